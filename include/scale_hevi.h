@@ -1,0 +1,256 @@
+/*
+ * scale_hevi.h -- C-ABI of the B200 implementation of SCALE-RM's HEVI short
+ * time step (libscale_hevi.so).
+ *
+ * Every entry point replaces one procedure of the reference dynamical core
+ * (hisashiyashiro/scale, SCALE 5.3.6) and keeps its argument list and order so
+ * that scale-rm's Fortran driver can bind it with ISO_C_BINDING (see
+ * INTEGRATION.md). Conventions follow what gfortran passes for those dummies:
+ *   - arrays are double* in Fortran column-major order with k fastest:
+ *     a (KA,IA,JA) field is element (k,i,j) at (k-1) + KA*((i-1) + IA*(j-1));
+ *   - intent(in) scalars are passed by reference (const double*, const int*);
+ *   - LOGICAL is a 4-byte int (0 = .false., nonzero = .true.).
+ * Entry points without the _dev suffix take HOST arrays: the library copies the
+ * inputs to the GPU, runs, and copies the outputs back before returning.
+ * Entry points with the _dev suffix take DEVICE pointers for every 2-D/3-D
+ * array and host pointers for the 1-D grid vectors and scalars; they enqueue
+ * work on the library's stream and return without synchronising.
+ *
+ * Every entry returns 0 on success or one of the SCALE_HEVI_ERR_* codes below;
+ * scale_hevi_last_error() then describes the failure. A Fortran shim maps a
+ * nonzero status to PRC_abort, as the reference aborts on errors.
+ *
+ * Supported configuration (checked, otherwise SCALE_HEVI_ERR_UNSUPPORTED):
+ * periodic lateral boundaries (BND_* = .false.), flat terrain (GSQRT = 1,
+ * J13G = J23G = 0, MAPF = 1, checked once per metric array), the default
+ * IBLOCK/JBLOCK (whole domain), flux schemes "UD3" and "CD4", ND_ORDER = 1,
+ * 4 <= KMAX <= 256, halo width 2. No additional prognostic variables (VA = 0).
+ *
+ * Concurrency: one library state per process (like the reference's module
+ * variables); calls are not re-entrant and must come from one host thread.
+ */
+#ifndef SCALE_HEVI_H
+#define SCALE_HEVI_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define SCALE_HEVI_OK                0
+#define SCALE_HEVI_ERR_ARG           1  /* inconsistent sizes or invalid argument       */
+#define SCALE_HEVI_ERR_NOT_SETUP     2  /* scale_hevi_setup() was not called            */
+#define SCALE_HEVI_ERR_CUDA          3  /* CUDA runtime error                            */
+#define SCALE_HEVI_ERR_NONFINITE     4  /* a prognostic output became NaN or Inf        */
+#define SCALE_HEVI_ERR_UNSUPPORTED   5  /* option outside the supported configuration   */
+#define SCALE_HEVI_ERR_ALLOC         6  /* device or pinned host allocation failed      */
+
+/* Index set of the local domain, the module variables of
+ * scalelib/src/atmosphere/grid/scale_atmos_grid_cartesC_index.F90:40-45,256-279 */
+typedef struct scale_hevi_index {
+    int KA, IA, JA;
+    int KS, KE, IS, IE, JS, JE;
+    int KMAX, IMAX, JMAX;
+    int KHALO, IHALO, JHALO;
+    int IBLOCK, JBLOCK;
+} scale_hevi_index;
+
+/* ---------------------------------------------------------------------------
+ * Library state
+ * ------------------------------------------------------------------------- */
+
+/* Setup of the index set and the flux schemes; replaces the module state set
+ * by ATMOS_GRID_CARTESC_INDEX_setup and ATMOS_DYN_FVM_flux_setup
+ * (scalelib/src/atmos-rm/dynamics/scale_atmos_dyn_fvm_flux.F90:276) for the
+ * HEVI short step (ATMOS_DYN_Tstep_short_fvm_hevi_setup,
+ * scale_atmos_dyn_tstep_short_fvm_hevi.F90:118). flux_type and
+ * flux_tracer_type are the ATMOS_DYN_FVM_FLUX_TYPE / _TRACER_TYPE names
+ * ("UD3", "CD4"). device is the CUDA ordinal to use. */
+int scale_hevi_setup(const scale_hevi_index *idx, const char *flux_type, const char *flux_tracer_type, int device);
+/* Frees every device buffer and the stream. */
+int scale_hevi_finalize(void);
+/* Text of the last error (empty when none). */
+const char *scale_hevi_last_error(void);
+/* The cudaStream_t the _dev entries enqueue on (as void*). */
+void *scale_hevi_stream(void);
+/* Waits for the stream and returns SCALE_HEVI_ERR_NONFINITE if any kernel
+ * since the last check saw a non-finite prognostic value (the device-side
+ * counterpart of the reference's UNDEF/NaN checks, scale_debug.F90:53-76). */
+int scale_hevi_check(void);
+/* Number of this library's kernels launched since setup (for profiling). */
+long long scale_hevi_kernel_launches(void);
+
+/* ---------------------------------------------------------------------------
+ * One HEVI stage. Replaces ATMOS_DYN_Tstep_short_fvm_hevi
+ * (scalelib/src/atmos-rm/dynamics/scale_atmos_dyn_tstep_short_fvm_hevi.F90:128-1089),
+ * the target of the ATMOS_DYN_Tstep_short procedure pointer
+ * (scale_atmos_dyn_tstep_short.F90:38-128,134). Same dummy arguments, same
+ * order. Outputs are written on the cells the reference writes; other cells of
+ * the output arrays keep their contents. PROG_RK/PROG0/PROG (VA = 0) and
+ * FLAG_FCT_* (unused by HEVI) are accepted and ignored; `last` only gates the
+ * reference's HIST_TEND output and is ignored.
+ * ------------------------------------------------------------------------- */
+#define SCALE_HEVI_TSTEP_SHORT_ARGS                                                                         \
+    double *DENS_RK, double *MOMZ_RK, double *MOMX_RK, double *MOMY_RK, double *RHOT_RK,                       \
+    double *PROG_RK, double *mflx_hi, double *tflx_hi,                                                         \
+    const double *DENS0, const double *MOMZ0, const double *MOMX0, const double *MOMY0, const double *RHOT0,   \
+    const double *DENS, const double *MOMZ, const double *MOMX, const double *MOMY, const double *RHOT,        \
+    const double *DENS_t, const double *MOMZ_t, const double *MOMX_t, const double *MOMY_t, const double *RHOT_t, \
+    const double *PROG0, const double *PROG,                                                                   \
+    const double *DPRES0, const double *RT2P, const double *CORIOLI,                                           \
+    const double *num_diff, const double *wdamp_coef, const double *divdmp_coef, const double *DDIV,           \
+    const int *FLAG_FCT_MOMENTUM, const int *FLAG_FCT_T, const int *FLAG_FCT_ALONG_STREAM,                     \
+    const double *CDZ, const double *FDZ, const double *FDX, const double *FDY,                                \
+    const double *RCDZ, const double *RCDX, const double *RCDY,                                                \
+    const double *RFDZ, const double *RFDX, const double *RFDY,                                                \
+    const double *PHI, const double *GSQRT, const double *J13G, const double *J23G, const double *J33G,        \
+    const double *MAPF, const double *REF_dens, const double *REF_rhot,                                        \
+    const int *BND_W, const int *BND_E, const int *BND_S, const int *BND_N,                                    \
+    const double *dtrk, const int *last
+
+int ATMOS_DYN_Tstep_short_fvm_hevi_b200(SCALE_HEVI_TSTEP_SHORT_ARGS);
+int ATMOS_DYN_Tstep_short_fvm_hevi_b200_dev(SCALE_HEVI_TSTEP_SHORT_ARGS);
+
+/* ---------------------------------------------------------------------------
+ * One short time step with the four-stage Runge-Kutta integrator. Replaces
+ * ATMOS_DYN_tinteg_short_rk4 (scale_atmos_dyn_tinteg_short_rk4.F90:199-650),
+ * target of ATMOS_DYN_Tinteg_short (scale_atmos_dyn_tinteg_short.F90:32-108).
+ * Same arguments in the same order (the reference names positions 21 and 48-49
+ * CVtot, REF_pres and REF_dens although the large step passes RT2P, REF_dens
+ * and REF_rhot; they are named here for what they receive). DENS..RHOT are
+ * updated in place on the interior; mflx_hi and tflx_hi receive the RK4
+ * averaged fluxes. The RK stage buffers stay on the device and the halo
+ * exchange between stages is done on the device.
+ * ------------------------------------------------------------------------- */
+#define SCALE_HEVI_TINTEG_SHORT_ARGS                                                                           \
+    double *DENS, double *MOMZ, double *MOMX, double *MOMY, double *RHOT, double *PROG,                        \
+    double *mflx_hi, double *tflx_hi,                                                                          \
+    const double *DENS_t, const double *MOMZ_t, const double *MOMX_t, const double *MOMY_t, const double *RHOT_t, \
+    const double *DPRES0, const double *RT2P, const double *CORIOLI,                                           \
+    const double *num_diff, const double *wdamp_coef, const double *divdmp_coef, const double *DDIV,           \
+    const int *FLAG_FCT_MOMENTUM, const int *FLAG_FCT_T, const int *FLAG_FCT_ALONG_STREAM,                     \
+    const double *CDZ, const double *FDZ, const double *FDX, const double *FDY,                                \
+    const double *RCDZ, const double *RCDX, const double *RCDY,                                                \
+    const double *RFDZ, const double *RFDX, const double *RFDY,                                                \
+    const double *PHI, const double *GSQRT, const double *J13G, const double *J23G, const double *J33G,        \
+    const double *MAPF, const double *REF_dens, const double *REF_rhot,                                        \
+    const int *BND_W, const int *BND_E, const int *BND_S, const int *BND_N,                                    \
+    const double *dt
+
+int ATMOS_DYN_Tinteg_short_rk4_b200(SCALE_HEVI_TINTEG_SHORT_ARGS);
+int ATMOS_DYN_Tinteg_short_rk4_b200_dev(SCALE_HEVI_TINTEG_SHORT_ARGS);
+
+/* ---------------------------------------------------------------------------
+ * Numerical filter coefficients. Replaces ATMOS_DYN_numfilter_coef
+ * (scalelib/src/atmos-rm/dynamics/scale_atmos_dyn_common.F90:385-985),
+ * including the halo exchange of the fifteen num_diff components.
+ * num_diff is (KA,IA,JA,5,3). ND_ORDER must be 1.
+ * ------------------------------------------------------------------------- */
+#define SCALE_HEVI_NUMFILTER_ARGS                                                                              \
+    double *num_diff,                                                                                          \
+    const double *DENS, const double *MOMZ, const double *MOMX, const double *MOMY, const double *RHOT,        \
+    const double *CDZ, const double *CDX, const double *CDY, const double *FDZ, const double *FDX,             \
+    const double *FDY, const double *DT, const double *REF_dens, const double *REF_pott,                       \
+    const double *ND_COEF, const int *ND_ORDER, const double *ND_SFC_FACT, const int *ND_USE_RS
+
+int ATMOS_DYN_numfilter_coef_b200(SCALE_HEVI_NUMFILTER_ARGS);
+int ATMOS_DYN_numfilter_coef_b200_dev(SCALE_HEVI_NUMFILTER_ARGS);
+
+/* ---------------------------------------------------------------------------
+ * Tracer advection. Replaces ATMOS_DYN_Tstep_tracer_fvm_heve
+ * (scalelib/src/atmos-rm/dynamics/scale_atmos_dyn_tstep_tracer_fvm_heve.F90:72-240,
+ * target of ATMOS_DYN_Tstep_tracer, scale_atmos_dyn_tstep_tracer.F90:32-68)
+ * and the three-stage integrator ATMOS_DYN_tinteg_tracer_rk3
+ * (scale_atmos_dyn_tinteg_tracer_rk3.F90:92-210), with the flux-corrected
+ * transport limiter ATMOS_DYN_fct (scale_atmos_dyn_common.F90:1922-2734).
+ * num_diff is (KA,IA,JA,3); GSQRT (KA,IA,JA,7); MAPF (IA,JA,2) at (x,y).
+ * QTRCo may be the same array as QTRC0. num_diff may be NULL for ND_COEF_Q = 0.
+ * ------------------------------------------------------------------------- */
+#define SCALE_HEVI_TSTEP_TRACER_ARGS                                                                           \
+    double *QTRCo, const double *QTRC, const double *QTRC0, const double *RHOQ_t,                              \
+    const double *DENS0, const double *DENS, const double *mflx_hi, const double *num_diff,                    \
+    const double *GSQRT, const double *MAPF,                                                                   \
+    const double *CDZ, const double *RCDZ, const double *RCDX, const double *RCDY,                             \
+    const double *dtl, const int *FLAG_FCT_TRACER, const int *FLAG_FCT_ALONG_STREAM
+
+int ATMOS_DYN_Tstep_tracer_fvm_heve_b200(SCALE_HEVI_TSTEP_TRACER_ARGS);
+int ATMOS_DYN_Tstep_tracer_fvm_heve_b200_dev(SCALE_HEVI_TSTEP_TRACER_ARGS);
+
+#define SCALE_HEVI_TINTEG_TRACER_ARGS                                                                          \
+    double *QTRC, const double *QTRC0, const double *RHOQ_t,                                                   \
+    const double *DENS0, const double *DENS, const double *mflx_hi, const double *num_diff,                    \
+    const double *GSQRT, const double *MAPF,                                                                   \
+    const double *CDZ, const double *RCDZ, const double *RCDX, const double *RCDY,                             \
+    const int *BND_W, const int *BND_E, const int *BND_S, const int *BND_N,                                    \
+    const double *dtl, const int *FLAG_FCT_TRACER, const int *FLAG_FCT_ALONG_STREAM
+
+int ATMOS_DYN_Tinteg_tracer_rk3_b200(SCALE_HEVI_TINTEG_TRACER_ARGS);
+int ATMOS_DYN_Tinteg_tracer_rk3_b200_dev(SCALE_HEVI_TINTEG_TRACER_ARGS);
+
+/* ---------------------------------------------------------------------------
+ * Periodic halo exchange of nfields consecutive (KA,IA,JA) device fields on
+ * one GPU. Replaces COMM_vars8 + COMM_wait of a periodic single-rank domain
+ * (scalelib/src/communication/scale_comm_cartesC.F90:345-397).
+ * ------------------------------------------------------------------------- */
+int COMM_vars8_b200_dev(double *var, const int *nfields);
+
+/* ---------------------------------------------------------------------------
+ * One large step of the dynamics on device-resident state. Replaces the
+ * dynamics part of ATMOS_DYN_Tstep_large_fvm_heve
+ * (scale_atmos_dyn_tstep_large_fvm_heve.F90:171-1130) for the supported
+ * configuration: no lateral damping (DAMP_alpha = 0), ND_COEF_Q = 0,
+ * USE_AVERAGE off, FLAG_TRACER_SPLIT_TEND off, EULER large-step integrator
+ * (QTRC0 = QTRC). Per large step: RT2P, DPRES0 and REF_rhot from the moist
+ * thermodynamics (:428-470); nstep = ceiling((DTLS-EPS)/DTSS) short steps, each
+ * numfilter + RK4 short step + vertical boundary values + halo exchange;
+ * then the RK3 tracer advection of every tracer with the short-step-averaged
+ * mass flux. Arrays are device pointers; QTRC and RHOQ_tp are (KA,IA,JA,QA),
+ * AQ_* are host arrays of length QA (QA <= 8). mflx_hi, tflx_hi and num_diff
+ * are outputs, as in the reference.
+ * ------------------------------------------------------------------------- */
+int ATMOS_DYN_Tstep_large_fvm_heve_b200_dev(
+    double *DENS, double *MOMZ, double *MOMX, double *MOMY, double *RHOT, double *QTRC, const int *QA,
+    double *mflx_hi, double *tflx_hi, double *num_diff,
+    const double *DENS_tp, const double *MOMZ_tp, const double *MOMX_tp, const double *MOMY_tp,
+    const double *RHOT_tp, const double *RHOQ_tp,
+    const double *CORIOLI,
+    const double *CDZ, const double *CDX, const double *CDY, const double *FDZ, const double *FDX, const double *FDY,
+    const double *RCDZ, const double *RCDX, const double *RCDY, const double *RFDZ, const double *RFDX, const double *RFDY,
+    const double *PHI, const double *GSQRT, const double *J13G, const double *J23G, const double *J33G, const double *MAPF,
+    const double *AQ_R, const double *AQ_CV, const double *AQ_CP, const double *AQ_MASS,
+    const double *REF_dens, const double *REF_pott, const double *REF_pres,
+    const double *ND_COEF, const int *ND_ORDER, const double *ND_SFC_FACT, const int *ND_USE_RS,
+    const double *wdamp_coef, const double *divdmp_coef,
+    const int *FLAG_FCT_TRACER, const int *FLAG_FCT_ALONG_STREAM,
+    const double *DTLS, const double *DTSS);
+
+/* Host-array variant of the large step: copies the state in, runs, copies the
+ * state, mflx_hi, tflx_hi and num_diff back. Same arguments. */
+int ATMOS_DYN_Tstep_large_fvm_heve_b200(
+    double *DENS, double *MOMZ, double *MOMX, double *MOMY, double *RHOT, double *QTRC, const int *QA,
+    double *mflx_hi, double *tflx_hi, double *num_diff,
+    const double *DENS_tp, const double *MOMZ_tp, const double *MOMX_tp, const double *MOMY_tp,
+    const double *RHOT_tp, const double *RHOQ_tp,
+    const double *CORIOLI,
+    const double *CDZ, const double *CDX, const double *CDY, const double *FDZ, const double *FDX, const double *FDY,
+    const double *RCDZ, const double *RCDX, const double *RCDY, const double *RFDZ, const double *RFDX, const double *RFDY,
+    const double *PHI, const double *GSQRT, const double *J13G, const double *J23G, const double *J33G, const double *MAPF,
+    const double *AQ_R, const double *AQ_CV, const double *AQ_CP, const double *AQ_MASS,
+    const double *REF_dens, const double *REF_pott, const double *REF_pres,
+    const double *ND_COEF, const int *ND_ORDER, const double *ND_SFC_FACT, const int *ND_USE_RS,
+    const double *wdamp_coef, const double *divdmp_coef,
+    const int *FLAG_FCT_TRACER, const int *FLAG_FCT_ALONG_STREAM,
+    const double *DTLS, const double *DTSS);
+
+/* ---------------------------------------------------------------------------
+ * FP64 domain budget: total = sum over the interior of var*CDZ*CDX*CDY, the
+ * mass total of check_mass (scalelib/src/atmos-rm/dynamics/scale_atmos_dyn.F90:530-688)
+ * computed on the device with a fixed reduction order. var is a device
+ * pointer, CDZ/CDX/CDY host arrays, total a host pointer. Synchronises.
+ * ------------------------------------------------------------------------- */
+int scale_hevi_domain_sum_dev(const double *var, const double *CDZ, const double *CDX, const double *CDY, double *total);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SCALE_HEVI_H */

@@ -1,0 +1,829 @@
+// C-ABI of libscale_hevi.so: library state, argument checks, host<->device
+// staging of the host-array entries, and the RK4 / tracer-RK3 / large-step
+// drivers that sequence the device kernels. Declarations and the reference
+// procedure each entry replaces are in include/scale_hevi.h.
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/scale_hevi.h"
+#include "grid_coef.h"
+#include "hevi_kernels.cuh"
+
+
+using namespace hevi;
+
+namespace {
+
+struct Ctx {
+    bool ready = false;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    scale_hevi_index idx{};
+    Grid g{};
+    int scheme = UD3, scheme_tracer = UD3;
+    size_t N3 = 0;
+    long long launches = 0;
+    // 1-D tables on the device: CDZ FDZ RCDZ RFDZ F2H1 F2H2 wdamp (KA each),
+    // FDX RCDX RFDX CDX (IA), FDY RCDY RFDY CDY (JA)
+    double *d_tab = nullptr;
+    std::vector<double> h_tab;
+    bool tab_valid = false;
+    double *d_wdamp = nullptr;
+    // numerical filter tables
+    double *d_nd = nullptr;
+    std::vector<double> nd_key;
+    NdCoef ndc{};
+    // scratch
+    double *adv = nullptr;          // 3*N3
+    double *rk[2] = {nullptr, nullptr}; // 5*N3 each
+    double *acc = nullptr;          // 5*N3
+    double *facc = nullptr;         // 6*N3
+    double *tr = nullptr;           // tracer: RK1, RK2, phi_lo, anti(3), rjp, rjm = 8*N3
+    double *lg = nullptr;           // large step: DENS00, RT2P, DPRES0, REF_rhot, mflx_av(3) = 7*N3
+    double *sum_part = nullptr, *sum_out = nullptr;
+    unsigned *status = nullptr;
+    unsigned long long *count = nullptr;
+    // metric check cache (pointer tuples already verified flat)
+    std::vector<std::vector<const void *>> flat_ok;
+    // staging buffers of the host-array entries
+    std::map<std::string, std::pair<double *, size_t>> stage;
+};
+
+Ctx C;
+std::string g_err;
+
+int fail(int code, const char *fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return code;
+}
+
+#define CU(call)                                                                              \
+    do {                                                                                      \
+        cudaError_t e_ = (call);                                                              \
+        if (e_ != cudaSuccess) return fail(SCALE_HEVI_ERR_CUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
+    } while (0)
+#define CK(expr)                      \
+    do {                              \
+        int rc_ = (expr);             \
+        if (rc_ != SCALE_HEVI_OK) return rc_; \
+    } while (0)
+
+int need_setup()
+{
+    if (!C.ready) return fail(SCALE_HEVI_ERR_NOT_SETUP, "scale_hevi_setup() has not been called");
+    return SCALE_HEVI_OK;
+}
+
+int dalloc(double **p, size_t n)
+{
+    if (cudaMalloc((void **)p, n * sizeof(double)) != cudaSuccess) {
+        *p = nullptr;
+        cudaGetLastError();
+        return fail(SCALE_HEVI_ERR_ALLOC, "cudaMalloc of %zu doubles failed", n);
+    }
+    return SCALE_HEVI_OK;
+}
+
+void free_all()
+{
+    double *bufs[] = {C.d_tab, C.d_nd, C.adv, C.rk[0], C.rk[1], C.acc, C.facc, C.tr, C.lg, C.sum_part, C.sum_out};
+    for (double *b : bufs) if (b) cudaFree(b);
+    for (auto &kv : C.stage) cudaFree(kv.second.first);
+    if (C.status) cudaFree(C.status);
+    if (C.count) cudaFree(C.count);
+    if (C.stream) cudaStreamDestroy(C.stream);
+    C = Ctx();
+}
+
+int parse_scheme(const char *s, int *out)
+{
+    if (!s) return fail(SCALE_HEVI_ERR_ARG, "flux scheme name is NULL");
+    std::string n(s);
+    while (!n.empty() && n.back() == ' ') n.pop_back(); // Fortran blank padding
+    if (n == "UD3") { *out = UD3; return SCALE_HEVI_OK; }
+    if (n == "CD4") { *out = CD4; return SCALE_HEVI_OK; }
+    return fail(SCALE_HEVI_ERR_UNSUPPORTED, "flux scheme '%s' is not supported (UD3, CD4)", n.c_str());
+}
+
+// host-array entries: a device buffer per argument role, grown on demand
+int stage_buf(const char *name, size_t n, double **out)
+{
+    auto &e = C.stage[name];
+    if (e.second < n) {
+        if (e.first) cudaFree(e.first);
+        e.first = nullptr;
+        e.second = 0;
+        CK(dalloc(&e.first, n));
+        e.second = n;
+    }
+    *out = e.first;
+    return SCALE_HEVI_OK;
+}
+int h2d(const char *name, const double *h, size_t n, double **d)
+{
+    CK(stage_buf(name, n, d));
+    CU(cudaMemcpyAsync(*d, h, n * sizeof(double), cudaMemcpyHostToDevice, C.stream));
+    return SCALE_HEVI_OK;
+}
+int d2h(double *h, const double *d, size_t n)
+{
+    CU(cudaMemcpyAsync(h, d, n * sizeof(double), cudaMemcpyDeviceToHost, C.stream));
+    return SCALE_HEVI_OK;
+}
+
+int check_bnd(const int *W, const int *E, const int *S, const int *N)
+{
+    if ((W && *W) || (E && *E) || (S && *S) || (N && *N))
+        return fail(SCALE_HEVI_ERR_UNSUPPORTED, "non-periodic lateral boundaries (BND_*=.true.) are not supported");
+    return SCALE_HEVI_OK;
+}
+
+// The kernels assume flat terrain. Verify GSQRT == 1, J13G == J23G == 0 and
+// MAPF == 1 once per distinct set of metric arrays.
+int check_flat(const double *GSQRT, const double *J13G, const double *J23G, const double *MAPF, bool on_device)
+{
+    std::vector<const void *> key = {GSQRT, J13G, J23G, MAPF, (const void *)(size_t)on_device};
+    for (auto &k : C.flat_ok) if (k == key) return SCALE_HEVI_OK;
+    const size_t n7 = 7 * C.N3, nm = (size_t)C.g.IA * C.g.JA * 2 * 4;
+    unsigned long long bad = 0;
+    if (on_device) {
+        CU(cudaMemsetAsync(C.count, 0, sizeof(unsigned long long), C.stream));
+        if (GSQRT) { count_not_equal(GSQRT, n7, 1.0, C.count, C.stream); ++C.launches; }
+        if (J13G) { count_not_equal(J13G, n7, 0.0, C.count, C.stream); ++C.launches; }
+        if (J23G) { count_not_equal(J23G, n7, 0.0, C.count, C.stream); ++C.launches; }
+        if (MAPF) { count_not_equal(MAPF, nm, 1.0, C.count, C.stream); ++C.launches; }
+        CU(cudaMemcpyAsync(&bad, C.count, sizeof bad, cudaMemcpyDeviceToHost, C.stream));
+        CU(cudaStreamSynchronize(C.stream));
+    } else {
+        for (size_t q = 0; GSQRT && q < n7; ++q) bad += GSQRT[q] != 1.0;
+        for (size_t q = 0; J13G && q < n7; ++q) bad += J13G[q] != 0.0;
+        for (size_t q = 0; J23G && q < n7; ++q) bad += J23G[q] != 0.0;
+        for (size_t q = 0; MAPF && q < nm; ++q) bad += MAPF[q] != 1.0;
+    }
+    if (bad)
+        return fail(SCALE_HEVI_ERR_UNSUPPORTED,
+                    "terrain-following metrics (%llu values of GSQRT/J13G/J23G/MAPF differ from flat terrain) are not supported", bad);
+    C.flat_ok.push_back(key);
+    return SCALE_HEVI_OK;
+}
+
+// Upload the 1-D grid vectors (host arrays) when they change and point the
+// Grid's table pointers at the device copies.
+int prepare_tables(const double *CDZ, const double *FDZ, const double *RCDZ, const double *RFDZ,
+                   const double *FDX, const double *RCDX, const double *RFDX,
+                   const double *FDY, const double *RCDY, const double *RFDY, const double *wdamp,
+                   const double *CDX, const double *CDY)
+{
+    const int KA = C.g.KA, IA = C.g.IA, JA = C.g.JA;
+    std::vector<double> h(7 * (size_t)KA + 4 * (size_t)IA + 4 * (size_t)JA, 0.0);
+    double *z = h.data(), *x = z + 7 * (size_t)KA, *y = x + 4 * (size_t)IA;
+    if (!CDZ || !FDZ || !RCDZ || !RFDZ || !FDX || !RCDX || !RFDX || !FDY || !RCDY || !RFDY)
+        return fail(SCALE_HEVI_ERR_ARG, "a 1-D grid vector is NULL");
+    std::memcpy(z, CDZ, KA * sizeof(double));
+    std::memcpy(z + KA, FDZ, (KA - 1) * sizeof(double));
+    std::memcpy(z + 2 * KA, RCDZ, KA * sizeof(double));
+    std::memcpy(z + 3 * KA, RFDZ, (KA - 1) * sizeof(double));
+    build_f2h(KA, CDZ, z + 4 * KA, z + 5 * KA);
+    if (wdamp) std::memcpy(z + 6 * KA, wdamp, KA * sizeof(double));
+    std::memcpy(x, FDX, (IA - 1) * sizeof(double));
+    std::memcpy(x + IA, RCDX, IA * sizeof(double));
+    std::memcpy(x + 2 * IA, RFDX, (IA - 1) * sizeof(double));
+    if (CDX) std::memcpy(x + 3 * IA, CDX, IA * sizeof(double));
+    std::memcpy(y, FDY, (JA - 1) * sizeof(double));
+    std::memcpy(y + JA, RCDY, JA * sizeof(double));
+    std::memcpy(y + 2 * JA, RFDY, (JA - 1) * sizeof(double));
+    if (CDY) std::memcpy(y + 3 * JA, CDY, JA * sizeof(double));
+    if (!C.tab_valid || h != C.h_tab) {
+        CU(cudaMemcpyAsync(C.d_tab, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice, C.stream));
+        CU(cudaStreamSynchronize(C.stream)); // the host vector is freed on return
+        C.h_tab.swap(h);
+        C.tab_valid = true;
+    }
+    double *dz = C.d_tab, *dx = dz + 7 * (size_t)KA, *dy = dx + 4 * (size_t)IA;
+    C.g.CDZ = dz; C.g.FDZ = dz + KA; C.g.RCDZ = dz + 2 * KA; C.g.RFDZ = dz + 3 * KA;
+    C.g.F2H1 = dz + 4 * KA; C.g.F2H2 = dz + 5 * KA; C.d_wdamp = dz + 6 * KA;
+    C.g.FDX = dx; C.g.RCDX = dx + IA; C.g.RFDX = dx + 2 * IA;
+    C.g.FDY = dy; C.g.RCDY = dy + JA; C.g.RFDY = dy + 2 * JA;
+    return SCALE_HEVI_OK;
+}
+const double *dev_CDX() { return C.d_tab + 7 * (size_t)C.g.KA + 3 * (size_t)C.g.IA; }
+const double *dev_CDY() { return C.d_tab + 7 * (size_t)C.g.KA + 4 * (size_t)C.g.IA + 3 * (size_t)C.g.JA; }
+
+int prepare_nd(const double *CDZ, const double *CDX, const double *CDY, const double *FDZ, const double *FDX,
+               const double *FDY, double DT, double ND_COEF, int ND_ORDER, double SFC)
+{
+    const int KA = C.g.KA, IA = C.g.IA, JA = C.g.JA;
+    std::vector<double> key;
+    key.insert(key.end(), CDZ, CDZ + KA); key.insert(key.end(), FDZ, FDZ + KA - 1);
+    key.insert(key.end(), CDX, CDX + IA); key.insert(key.end(), FDX, FDX + IA - 1);
+    key.insert(key.end(), CDY, CDY + JA); key.insert(key.end(), FDY, FDY + JA - 1);
+    key.push_back(DT); key.push_back(ND_COEF); key.push_back((double)ND_ORDER);
+    const size_t nz = 3 * (size_t)KA * 2, nx = 3 * (size_t)IA * 2, ny = 3 * (size_t)JA * 2;
+    if (key != C.nd_key) {
+        NdGrid gr{KA, IA, JA, C.g.KS, C.g.KE, C.g.IS, C.g.IE, C.g.JS, C.g.JE, CDZ, FDZ, CDX, FDX, CDY, FDY};
+        NdTables t;
+        build_nd_tables(gr, DT, ND_COEF, ND_ORDER, t);
+        std::vector<double> h;
+        for (auto *v : {&t.CNZ3, &t.CNX3, &t.CNY3, &t.cdz, &t.fdz, &t.cdx, &t.fdx, &t.cdy, &t.fdy})
+            h.insert(h.end(), v->begin(), v->end());
+        CU(cudaMemcpyAsync(C.d_nd, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice, C.stream));
+        CU(cudaStreamSynchronize(C.stream));
+        C.nd_key.swap(key);
+    }
+    const double *p = C.d_nd;
+    C.ndc.CNZ3 = p; p += nz;
+    C.ndc.CNX3 = p; p += nx;
+    C.ndc.CNY3 = p; p += ny;
+    C.ndc.cdz = p; p += KA;
+    C.ndc.fdz = p; p += KA;
+    C.ndc.cdx = p; p += IA;
+    C.ndc.fdx = p; p += IA;
+    C.ndc.cdy = p; p += JA;
+    C.ndc.fdy = p;
+    C.ndc.sfc = SFC;
+    return SCALE_HEVI_OK;
+}
+
+void halo(double *const *f, int n)
+{
+    periodic_halo(C.g, f, n, C.stream);
+    C.launches += (n + 15) / 16;
+}
+
+// ---- one stage ---------------------------------------------------------------
+struct StageIn {
+    const double *DENS0, *MOMZ0, *MOMX0, *MOMY0, *RHOT0;
+    const double *DENS, *MOMZ, *MOMX, *MOMY, *RHOT;
+    const double *DENS_t, *MOMZ_t, *MOMX_t, *MOMY_t, *RHOT_t;
+    const double *DPRES0, *RT2P, *CORIOLI, *num_diff, *DDIV, *REF_dens, *REF_rhot;
+    double divdmp, J33G;
+};
+
+int run_stage(const StageIn &in, double *const out[5], double *mflx, double *tflx, double dtrk, int mode)
+{
+    StageArgs a{};
+    a.DENS_RK = out[0]; a.MOMZ_RK = out[1]; a.MOMX_RK = out[2]; a.MOMY_RK = out[3]; a.RHOT_RK = out[4];
+    a.mflx = mflx; a.tflx = tflx;
+    a.DENS0 = in.DENS0; a.MOMZ0 = in.MOMZ0; a.MOMX0 = in.MOMX0; a.MOMY0 = in.MOMY0; a.RHOT0 = in.RHOT0;
+    a.DENS = in.DENS; a.MOMZ = in.MOMZ; a.MOMX = in.MOMX; a.MOMY = in.MOMY; a.RHOT = in.RHOT;
+    a.DENS_t = in.DENS_t; a.MOMZ_t = in.MOMZ_t; a.MOMX_t = in.MOMX_t; a.MOMY_t = in.MOMY_t; a.RHOT_t = in.RHOT_t;
+    a.DPRES0 = in.DPRES0; a.RT2P = in.RT2P; a.CORIOLI = in.CORIOLI; a.num_diff = in.num_diff;
+    a.wdamp = C.d_wdamp; a.DDIV = in.DDIV; a.REF_dens = in.REF_dens; a.REF_rhot = in.REF_rhot;
+    a.divdmp_coef = in.divdmp; a.J33G = in.J33G; a.dtrk = dtrk;
+    a.adv_r = C.adv; a.adv_w = C.adv + C.N3; a.adv_t = C.adv + 2 * C.N3;
+    a.rk_mode = mode; a.acc = C.acc; a.facc = C.facc; a.status = C.status;
+    CU(launch_hevi_stage(C.g, a, C.scheme, C.stream));
+    C.launches += 2;
+    return SCALE_HEVI_OK;
+}
+
+// RK4 short step on device arrays (tinteg_short_rk4.F90:199-650): stage s reads
+// the previous stage's buffer (halo filled on the device) and X0 = the input
+// state; the last stage writes the combined state in place.
+int run_rk4(double *X[5], double *mflx, double *tflx, const StageIn &base, double dt)
+{
+    StageIn in = base;
+    in.DENS0 = X[0]; in.MOMZ0 = X[1]; in.MOMX0 = X[2]; in.MOMY0 = X[3]; in.RHOT0 = X[4];
+    const double dts[4] = {dt / 2.0, dt / 2.0, dt, dt};
+    const double *src[5] = {X[0], X[1], X[2], X[3], X[4]};
+    for (int s = 0; s < 4; ++s) {
+        in.DENS = src[0]; in.MOMZ = src[1]; in.MOMX = src[2]; in.MOMY = src[3]; in.RHOT = src[4];
+        double *out[5];
+        if (s < 3) {
+            double *b = C.rk[s % 2];
+            for (int v = 0; v < 5; ++v) out[v] = b + (size_t)v * C.N3;
+        } else {
+            for (int v = 0; v < 5; ++v) out[v] = X[v];
+        }
+        CK(run_stage(in, out, mflx, tflx, dts[s], RK_STAGE1 + s));
+        if (s < 3) {
+            halo(out, 5); // COMM_vars8 of the stage buffers (rk4.F90:401-425)
+            for (int v = 0; v < 5; ++v) src[v] = out[v];
+        }
+    }
+    return SCALE_HEVI_OK;
+}
+
+int run_numfilter(double *num_diff, const double *DENS, const double *MOMZ, const double *MOMX, const double *MOMY,
+                  const double *RHOT, const double *REF_dens, const double *REF_pott)
+{
+    NdArgs a{num_diff, DENS, MOMZ, MOMX, MOMY, RHOT, REF_dens, REF_pott};
+    CU(launch_numfilter(C.g, C.ndc, a, C.stream));
+    ++C.launches;
+    double *f[15];
+    for (int q = 0; q < 15; ++q) f[q] = num_diff + (size_t)q * C.N3;
+    halo(f, 15);
+    return SCALE_HEVI_OK;
+}
+
+// RK3 tracer integrator (tinteg_tracer_rk3.F90:92-210) on device arrays
+int run_tracer_rk3(double *QTRC, const double *QTRC0, const double *RHOQ_t, const double *DENS0, const double *DENS,
+                   const double *mflx, const double *ndq, double dtl, bool fct, bool along)
+{
+    TracerArgs a{};
+    a.QTRC0 = QTRC0; a.RHOQ_t = RHOQ_t; a.DENS0 = DENS0; a.DENS = DENS; a.mflx = mflx; a.ndq = ndq;
+    a.phi_lo = C.tr + 2 * C.N3; a.anti = C.tr + 3 * C.N3; a.rjp = C.tr + 6 * C.N3; a.rjm = C.tr + 7 * C.N3;
+    a.along_stream = along ? 1 : 0;
+    double *rk1 = C.tr, *rk2 = C.tr + C.N3;
+    // stage 1: dt/3 with DENS0 + (DENS-DENS0)/3
+    a.QTRCo = rk1; a.QTRC = QTRC; a.dens_mode = 1; a.dtl = dtl / 3.0;
+    CU(launch_tracer_stage(C.g, a, C.scheme_tracer, false, C.stream));
+    ++C.launches;
+    halo(&rk1, 1);
+    // stage 2: dt/2 with DENS0 + (DENS-DENS0)*0.5
+    a.QTRCo = rk2; a.QTRC = rk1; a.dens_mode = 2; a.dtl = dtl / 2.0;
+    CU(launch_tracer_stage(C.g, a, C.scheme_tracer, false, C.stream));
+    ++C.launches;
+    halo(&rk2, 1);
+    // stage 3: dt with DENS, FCT when requested
+    a.QTRCo = QTRC; a.QTRC = rk2; a.dens_mode = 0; a.dtl = dtl;
+    CU(launch_tracer_stage(C.g, a, C.scheme_tracer, fct, C.stream));
+    C.launches += fct ? 4 : 1;
+    return SCALE_HEVI_OK;
+}
+
+size_t n3() { return C.N3; }
+
+}  // namespace
+
+// =============================================================================
+// exported entry points
+// =============================================================================
+extern "C" {
+
+int scale_hevi_setup(const scale_hevi_index *idx, const char *flux_type, const char *flux_tracer_type, int device)
+{
+    if (C.ready) free_all();
+    g_err.clear();
+    if (!idx) return fail(SCALE_HEVI_ERR_ARG, "index set is NULL");
+    const scale_hevi_index &x = *idx;
+    if (x.KHALO != 2 || x.IHALO != 2 || x.JHALO != 2) return fail(SCALE_HEVI_ERR_UNSUPPORTED, "halo width must be 2");
+    if (x.KA != x.KMAX + 2 * x.KHALO || x.IA != x.IMAX + 2 * x.IHALO || x.JA != x.JMAX + 2 * x.JHALO ||
+        x.KS != 1 + x.KHALO || x.KE != x.KMAX + x.KHALO || x.IS != 1 + x.IHALO || x.IE != x.IMAX + x.IHALO ||
+        x.JS != 1 + x.JHALO || x.JE != x.JMAX + x.JHALO)
+        return fail(SCALE_HEVI_ERR_ARG, "index set is inconsistent (KA=%d KMAX=%d KS=%d KE=%d IA=%d IMAX=%d JA=%d JMAX=%d)",
+                    x.KA, x.KMAX, x.KS, x.KE, x.IA, x.IMAX, x.JA, x.JMAX);
+    if (x.KMAX < 4 || x.KA > 260) return fail(SCALE_HEVI_ERR_UNSUPPORTED, "KMAX must be in 4..256 (got %d)", x.KMAX);
+    if (x.IMAX < 2 || x.JMAX < 2) return fail(SCALE_HEVI_ERR_ARG, "IMAX and JMAX must be >= IHALO, JHALO");
+    if ((x.IBLOCK > 0 && x.IBLOCK != x.IMAX) || (x.JBLOCK > 0 && x.JBLOCK != x.JMAX))
+        return fail(SCALE_HEVI_ERR_UNSUPPORTED, "only the default IBLOCK=IMAX, JBLOCK=JMAX blocking is supported");
+    int s1, s2;
+    CK(parse_scheme(flux_type, &s1));
+    CK(parse_scheme(flux_tracer_type, &s2));
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return fail(SCALE_HEVI_ERR_CUDA, "no CUDA device is available");
+    }
+    if (device < 0 || device >= ndev) return fail(SCALE_HEVI_ERR_ARG, "device %d out of range (%d devices)", device, ndev);
+    CU(cudaSetDevice(device));
+    C.device = device;
+    C.idx = x;
+    C.scheme = s1;
+    C.scheme_tracer = s2;
+    Grid &g = C.g;
+    g.KA = x.KA; g.IA = x.IA; g.JA = x.JA;
+    g.KS = x.KS; g.KE = x.KE; g.IS = x.IS; g.IE = x.IE; g.JS = x.JS; g.JE = x.JE;
+    g.KMAX = x.KMAX; g.IMAX = x.IMAX; g.JMAX = x.JMAX; g.IHALO = x.IHALO; g.JHALO = x.JHALO;
+    g.IEH = x.IE; g.JEH = x.JE; // BND_E = BND_N = .false.
+    C.N3 = (size_t)x.KA * x.IA * x.JA;
+    const size_t N3 = C.N3;
+    CU(cudaStreamCreateWithFlags(&C.stream, cudaStreamNonBlocking));
+    int rc = SCALE_HEVI_OK;
+    if ((rc = dalloc(&C.d_tab, 7 * (size_t)x.KA + 4 * (size_t)x.IA + 4 * (size_t)x.JA)) ||
+        (rc = dalloc(&C.d_nd, 8 * (size_t)x.KA + 8 * (size_t)x.IA + 8 * (size_t)x.JA)) ||
+        (rc = dalloc(&C.adv, 3 * N3)) || (rc = dalloc(&C.rk[0], 5 * N3)) || (rc = dalloc(&C.rk[1], 5 * N3)) ||
+        (rc = dalloc(&C.acc, 5 * N3)) || (rc = dalloc(&C.facc, 6 * N3)) ||
+        (rc = dalloc(&C.sum_part, (size_t)x.IMAX * x.JMAX)) || (rc = dalloc(&C.sum_out, 1))) {
+        free_all();
+        return rc;
+    }
+    if (cudaMalloc((void **)&C.status, sizeof(unsigned)) != cudaSuccess ||
+        cudaMalloc((void **)&C.count, sizeof(unsigned long long)) != cudaSuccess) {
+        free_all();
+        return fail(SCALE_HEVI_ERR_ALLOC, "cudaMalloc of status words failed");
+    }
+    cudaMemset(C.status, 0, sizeof(unsigned));
+    C.ready = true;
+    return SCALE_HEVI_OK;
+}
+
+int scale_hevi_finalize(void)
+{
+    if (C.ready && C.stream) cudaStreamSynchronize(C.stream);
+    free_all();
+    return SCALE_HEVI_OK;
+}
+
+const char *scale_hevi_last_error(void) { return g_err.c_str(); }
+void *scale_hevi_stream(void) { return (void *)C.stream; }
+long long scale_hevi_kernel_launches(void) { return C.launches; }
+
+int scale_hevi_check(void)
+{
+    CK(need_setup());
+    unsigned st = 0;
+    CU(cudaMemcpyAsync(&st, C.status, sizeof st, cudaMemcpyDeviceToHost, C.stream));
+    CU(cudaStreamSynchronize(C.stream));
+    CU(cudaMemsetAsync(C.status, 0, sizeof(unsigned), C.stream));
+    if (st & ST_NONFINITE) return fail(SCALE_HEVI_ERR_NONFINITE, "a prognostic output became NaN or Inf");
+    return SCALE_HEVI_OK;
+}
+
+// ---- HEVI stage --------------------------------------------------------------
+int ATMOS_DYN_Tstep_short_fvm_hevi_b200_dev(SCALE_HEVI_TSTEP_SHORT_ARGS)
+{
+    (void)PROG_RK; (void)PROG0; (void)PROG; (void)FLAG_FCT_MOMENTUM; (void)FLAG_FCT_T; (void)FLAG_FCT_ALONG_STREAM;
+    (void)last; (void)PHI;
+    CK(need_setup());
+    CK(check_bnd(BND_W, BND_E, BND_S, BND_N));
+    CK(check_flat(GSQRT, J13G, J23G, MAPF, true));
+    CK(prepare_tables(CDZ, FDZ, RCDZ, RFDZ, FDX, RCDX, RFDX, FDY, RCDY, RFDY, wdamp_coef, nullptr, nullptr));
+    StageIn in{DENS0, MOMZ0, MOMX0, MOMY0, RHOT0, DENS, MOMZ, MOMX, MOMY, RHOT,
+               DENS_t, MOMZ_t, MOMX_t, MOMY_t, RHOT_t, DPRES0, RT2P, CORIOLI, num_diff, DDIV, REF_dens, REF_rhot,
+               *divdmp_coef, *J33G};
+    double *out[5] = {DENS_RK, MOMZ_RK, MOMX_RK, MOMY_RK, RHOT_RK};
+    return run_stage(in, out, mflx_hi, tflx_hi, *dtrk, RK_PLAIN);
+}
+
+int ATMOS_DYN_Tstep_short_fvm_hevi_b200(SCALE_HEVI_TSTEP_SHORT_ARGS)
+{
+    CK(need_setup());
+    CK(check_bnd(BND_W, BND_E, BND_S, BND_N));
+    CK(check_flat(GSQRT, J13G, J23G, MAPF, false));
+    const size_t N3 = n3(), N2 = (size_t)C.g.IA * C.g.JA;
+    const bool use_div = *divdmp_coef != 0.0;
+    double *o[5], *mf, *tf, *i0[5], *iv[5], *it[5], *dp0, *rt, *cor, *nd, *ddiv = nullptr, *rd, *rr;
+    const double *hin0[5] = {DENS0, MOMZ0, MOMX0, MOMY0, RHOT0};
+    const double *hin[5] = {DENS, MOMZ, MOMX, MOMY, RHOT};
+    const double *htt[5] = {DENS_t, MOMZ_t, MOMX_t, MOMY_t, RHOT_t};
+    double *hout[5] = {DENS_RK, MOMZ_RK, MOMX_RK, MOMY_RK, RHOT_RK};
+    static const char *n_o[5] = {"o0", "o1", "o2", "o3", "o4"}, *n_0[5] = {"a0", "a1", "a2", "a3", "a4"};
+    static const char *n_v[5] = {"b0", "b1", "b2", "b3", "b4"}, *n_t[5] = {"t0", "t1", "t2", "t3", "t4"};
+    for (int v = 0; v < 5; ++v) {
+        CK(h2d(n_o[v], hout[v], N3, &o[v])); // cells the stage does not write keep their contents
+        CK(h2d(n_0[v], hin0[v], N3, &i0[v]));
+        CK(h2d(n_v[v], hin[v], N3, &iv[v]));
+        CK(h2d(n_t[v], htt[v], N3, &it[v]));
+    }
+    CK(h2d("mflx", mflx_hi, 3 * N3, &mf));
+    CK(h2d("tflx", tflx_hi, 3 * N3, &tf));
+    CK(h2d("DPRES0", DPRES0, N3, &dp0));
+    CK(h2d("RT2P", RT2P, N3, &rt));
+    CK(h2d("CORIOLI", CORIOLI, N2, &cor));
+    CK(h2d("num_diff", num_diff, 15 * N3, &nd));
+    if (use_div) CK(h2d("DDIV", DDIV, N3, &ddiv));
+    CK(h2d("REF_dens", REF_dens, N3, &rd));
+    CK(h2d("REF_rhot", REF_rhot, N3, &rr));
+    CK(prepare_tables(CDZ, FDZ, RCDZ, RFDZ, FDX, RCDX, RFDX, FDY, RCDY, RFDY, wdamp_coef, nullptr, nullptr));
+    StageIn in{i0[0], i0[1], i0[2], i0[3], i0[4], iv[0], iv[1], iv[2], iv[3], iv[4],
+               it[0], it[1], it[2], it[3], it[4], dp0, rt, cor, nd, ddiv, rd, rr, *divdmp_coef, *J33G};
+    CK(run_stage(in, o, mf, tf, *dtrk, RK_PLAIN));
+    for (int v = 0; v < 5; ++v) CK(d2h(hout[v], o[v], N3));
+    CK(d2h(mflx_hi, mf, 3 * N3));
+    CK(d2h(tflx_hi, tf, 3 * N3));
+    CU(cudaStreamSynchronize(C.stream));
+    (void)PROG_RK; (void)PROG0; (void)PROG; (void)FLAG_FCT_MOMENTUM; (void)FLAG_FCT_T; (void)FLAG_FCT_ALONG_STREAM; (void)last; (void)PHI;
+    return scale_hevi_check();
+}
+
+// ---- RK4 short step ------------------------------------------------------------
+int ATMOS_DYN_Tinteg_short_rk4_b200_dev(SCALE_HEVI_TINTEG_SHORT_ARGS)
+{
+    (void)PROG; (void)FLAG_FCT_MOMENTUM; (void)FLAG_FCT_T; (void)FLAG_FCT_ALONG_STREAM; (void)PHI;
+    CK(need_setup());
+    CK(check_bnd(BND_W, BND_E, BND_S, BND_N));
+    CK(check_flat(GSQRT, J13G, J23G, MAPF, true));
+    CK(prepare_tables(CDZ, FDZ, RCDZ, RFDZ, FDX, RCDX, RFDX, FDY, RCDY, RFDY, wdamp_coef, nullptr, nullptr));
+    double *X[5] = {DENS, MOMZ, MOMX, MOMY, RHOT};
+    StageIn base{nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
+                 DENS_t, MOMZ_t, MOMX_t, MOMY_t, RHOT_t, DPRES0, RT2P, CORIOLI, num_diff, DDIV, REF_dens, REF_rhot,
+                 *divdmp_coef, *J33G};
+    return run_rk4(X, mflx_hi, tflx_hi, base, *dt);
+}
+
+int ATMOS_DYN_Tinteg_short_rk4_b200(SCALE_HEVI_TINTEG_SHORT_ARGS)
+{
+    CK(need_setup());
+    CK(check_bnd(BND_W, BND_E, BND_S, BND_N));
+    CK(check_flat(GSQRT, J13G, J23G, MAPF, false));
+    const size_t N3 = n3(), N2 = (size_t)C.g.IA * C.g.JA;
+    double *hx[5] = {DENS, MOMZ, MOMX, MOMY, RHOT};
+    const double *htt[5] = {DENS_t, MOMZ_t, MOMX_t, MOMY_t, RHOT_t};
+    static const char *n_x[5] = {"x0", "x1", "x2", "x3", "x4"}, *n_t[5] = {"t0", "t1", "t2", "t3", "t4"};
+    double *X[5], *T[5], *mf, *tf, *dp0, *rt, *cor, *nd, *ddiv = nullptr, *rd, *rr;
+    for (int v = 0; v < 5; ++v) {
+        CK(h2d(n_x[v], hx[v], N3, &X[v]));
+        CK(h2d(n_t[v], htt[v], N3, &T[v]));
+    }
+    CK(h2d("mflx", mflx_hi, 3 * N3, &mf));
+    CK(h2d("tflx", tflx_hi, 3 * N3, &tf));
+    CK(h2d("DPRES0", DPRES0, N3, &dp0));
+    CK(h2d("RT2P", RT2P, N3, &rt));
+    CK(h2d("CORIOLI", CORIOLI, N2, &cor));
+    CK(h2d("num_diff", num_diff, 15 * N3, &nd));
+    if (*divdmp_coef != 0.0) CK(h2d("DDIV", DDIV, N3, &ddiv));
+    CK(h2d("REF_dens", REF_dens, N3, &rd));
+    CK(h2d("REF_rhot", REF_rhot, N3, &rr));
+    CK(prepare_tables(CDZ, FDZ, RCDZ, RFDZ, FDX, RCDX, RFDX, FDY, RCDY, RFDY, wdamp_coef, nullptr, nullptr));
+    StageIn base{nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
+                 T[0], T[1], T[2], T[3], T[4], dp0, rt, cor, nd, ddiv, rd, rr, *divdmp_coef, *J33G};
+    CK(run_rk4(X, mf, tf, base, *dt));
+    for (int v = 0; v < 5; ++v) CK(d2h(hx[v], X[v], N3));
+    CK(d2h(mflx_hi, mf, 3 * N3));
+    CK(d2h(tflx_hi, tf, 3 * N3));
+    CU(cudaStreamSynchronize(C.stream));
+    (void)PROG; (void)FLAG_FCT_MOMENTUM; (void)FLAG_FCT_T; (void)FLAG_FCT_ALONG_STREAM; (void)PHI;
+    return scale_hevi_check();
+}
+
+// ---- numerical filter --------------------------------------------------------
+int ATMOS_DYN_numfilter_coef_b200_dev(SCALE_HEVI_NUMFILTER_ARGS)
+{
+    CK(need_setup());
+    if (*ND_ORDER != 1) return fail(SCALE_HEVI_ERR_UNSUPPORTED, "ND_ORDER=%d is not supported (1 only)", *ND_ORDER);
+    if (!*ND_USE_RS) return fail(SCALE_HEVI_ERR_UNSUPPORTED, "ND_USE_RS=.false. is not supported");
+    CK(prepare_nd(CDZ, CDX, CDY, FDZ, FDX, FDY, *DT, *ND_COEF, *ND_ORDER, *ND_SFC_FACT));
+    return run_numfilter(num_diff, DENS, MOMZ, MOMX, MOMY, RHOT, REF_dens, REF_pott);
+}
+
+int ATMOS_DYN_numfilter_coef_b200(SCALE_HEVI_NUMFILTER_ARGS)
+{
+    CK(need_setup());
+    const size_t N3 = n3();
+    double *nd, *d[5], *rd, *rp;
+    const double *h[5] = {DENS, MOMZ, MOMX, MOMY, RHOT};
+    static const char *nm[5] = {"x0", "x1", "x2", "x3", "x4"};
+    for (int v = 0; v < 5; ++v) CK(h2d(nm[v], h[v], N3, &d[v]));
+    CK(h2d("REF_dens", REF_dens, N3, &rd));
+    CK(h2d("REF_pott", REF_pott, N3, &rp));
+    CK(stage_buf("num_diff", 15 * N3, &nd));
+    int rc = ATMOS_DYN_numfilter_coef_b200_dev(nd, d[0], d[1], d[2], d[3], d[4], CDZ, CDX, CDY, FDZ, FDX, FDY, DT, rd, rp,
+                                               ND_COEF, ND_ORDER, ND_SFC_FACT, ND_USE_RS);
+    if (rc) return rc;
+    CK(d2h(num_diff, nd, 15 * N3));
+    CU(cudaStreamSynchronize(C.stream));
+    return SCALE_HEVI_OK;
+}
+
+// ---- tracer ------------------------------------------------------------------
+static int tracer_common_checks(const double *GSQRT, const double *MAPF, bool on_device)
+{
+    CK(need_setup());
+    CK(check_flat(GSQRT, nullptr, nullptr, nullptr, on_device));
+    // MAPF here is the (IA,JA,2) slice at (x,y)
+    if (MAPF) {
+        std::vector<const void *> key = {MAPF, (const void *)(size_t)(on_device ? 3 : 2)};
+        bool ok = false;
+        for (auto &k : C.flat_ok) ok |= (k == key);
+        if (!ok) {
+            const size_t n = (size_t)C.g.IA * C.g.JA * 2;
+            unsigned long long bad = 0;
+            if (on_device) {
+                CU(cudaMemsetAsync(C.count, 0, sizeof bad, C.stream));
+                count_not_equal(MAPF, n, 1.0, C.count, C.stream);
+                ++C.launches;
+                CU(cudaMemcpyAsync(&bad, C.count, sizeof bad, cudaMemcpyDeviceToHost, C.stream));
+                CU(cudaStreamSynchronize(C.stream));
+            } else {
+                for (size_t q = 0; q < n; ++q) bad += MAPF[q] != 1.0;
+            }
+            if (bad) return fail(SCALE_HEVI_ERR_UNSUPPORTED, "map factors other than 1 are not supported");
+            C.flat_ok.push_back(key);
+        }
+    }
+    if (!C.tr) CK(dalloc(&C.tr, 8 * C.N3));
+    return SCALE_HEVI_OK;
+}
+
+int ATMOS_DYN_Tstep_tracer_fvm_heve_b200_dev(SCALE_HEVI_TSTEP_TRACER_ARGS)
+{
+    CK(tracer_common_checks(GSQRT, MAPF, true));
+    // the 1-D vectors this step needs; the others keep their last values
+    std::vector<double> one(C.g.KA > C.g.IA ? (C.g.KA > C.g.JA ? C.g.KA : C.g.JA) : (C.g.IA > C.g.JA ? C.g.IA : C.g.JA), 1.0);
+    CK(prepare_tables(CDZ, one.data(), RCDZ, one.data(), one.data(), RCDX, one.data(), one.data(), RCDY, one.data(),
+                      nullptr, nullptr, nullptr));
+    TracerArgs a{};
+    a.QTRCo = QTRCo; a.QTRC = QTRC; a.QTRC0 = QTRC0; a.RHOQ_t = RHOQ_t; a.DENS0 = DENS0; a.DENS = DENS;
+    a.dens_mode = 0; a.mflx = mflx_hi; a.ndq = num_diff; a.dtl = *dtl;
+    a.phi_lo = C.tr + 2 * C.N3; a.anti = C.tr + 3 * C.N3; a.rjp = C.tr + 6 * C.N3; a.rjm = C.tr + 7 * C.N3;
+    a.along_stream = *FLAG_FCT_ALONG_STREAM ? 1 : 0;
+    const bool fct = *FLAG_FCT_TRACER != 0;
+    CU(launch_tracer_stage(C.g, a, C.scheme_tracer, fct, C.stream));
+    C.launches += fct ? 4 : 1;
+    return SCALE_HEVI_OK;
+}
+
+int ATMOS_DYN_Tstep_tracer_fvm_heve_b200(SCALE_HEVI_TSTEP_TRACER_ARGS)
+{
+    CK(tracer_common_checks(GSQRT, MAPF, false));
+    const size_t N3 = n3();
+    double *qo, *q, *q0, *rq, *d0, *d, *mf, *nd = nullptr;
+    CK(h2d("q_out", QTRCo, N3, &qo));
+    CK(h2d("q_in", QTRC, N3, &q));
+    CK(h2d("q0", QTRC0, N3, &q0));
+    CK(h2d("rhoq_t", RHOQ_t, N3, &rq));
+    CK(h2d("DENS0", DENS0, N3, &d0));
+    CK(h2d("DENS", DENS, N3, &d));
+    CK(h2d("mflx", mflx_hi, 3 * N3, &mf));
+    if (num_diff) CK(h2d("ndq", num_diff, 3 * N3, &nd));
+    int rc = ATMOS_DYN_Tstep_tracer_fvm_heve_b200_dev(qo, q, (QTRC0 == QTRCo) ? qo : q0, rq, d0, d, mf, nd, nullptr, nullptr,
+                                                      CDZ, RCDZ, RCDX, RCDY, dtl, FLAG_FCT_TRACER, FLAG_FCT_ALONG_STREAM);
+    if (rc) return rc;
+    CK(d2h(QTRCo, qo, N3));
+    CU(cudaStreamSynchronize(C.stream));
+    return SCALE_HEVI_OK;
+}
+
+int ATMOS_DYN_Tinteg_tracer_rk3_b200_dev(SCALE_HEVI_TINTEG_TRACER_ARGS)
+{
+    CK(check_bnd(BND_W, BND_E, BND_S, BND_N));
+    CK(tracer_common_checks(GSQRT, MAPF, true));
+    std::vector<double> one(C.g.KA > C.g.IA ? (C.g.KA > C.g.JA ? C.g.KA : C.g.JA) : (C.g.IA > C.g.JA ? C.g.IA : C.g.JA), 1.0);
+    CK(prepare_tables(CDZ, one.data(), RCDZ, one.data(), one.data(), RCDX, one.data(), one.data(), RCDY, one.data(),
+                      nullptr, nullptr, nullptr));
+    return run_tracer_rk3(QTRC, QTRC0, RHOQ_t, DENS0, DENS, mflx_hi, num_diff, *dtl, *FLAG_FCT_TRACER != 0,
+                          *FLAG_FCT_ALONG_STREAM != 0);
+}
+
+int ATMOS_DYN_Tinteg_tracer_rk3_b200(SCALE_HEVI_TINTEG_TRACER_ARGS)
+{
+    CK(check_bnd(BND_W, BND_E, BND_S, BND_N));
+    CK(tracer_common_checks(GSQRT, MAPF, false));
+    const size_t N3 = n3();
+    double *q, *q0, *rq, *d0, *d, *mf, *nd = nullptr;
+    CK(h2d("q_out", QTRC, N3, &q));
+    CK(h2d("q0", QTRC0, N3, &q0));
+    CK(h2d("rhoq_t", RHOQ_t, N3, &rq));
+    CK(h2d("DENS0", DENS0, N3, &d0));
+    CK(h2d("DENS", DENS, N3, &d));
+    CK(h2d("mflx", mflx_hi, 3 * N3, &mf));
+    if (num_diff) CK(h2d("ndq", num_diff, 3 * N3, &nd));
+    int rc = ATMOS_DYN_Tinteg_tracer_rk3_b200_dev(q, (QTRC0 == QTRC) ? q : q0, rq, d0, d, mf, nd, nullptr, nullptr,
+                                                  CDZ, RCDZ, RCDX, RCDY, BND_W, BND_E, BND_S, BND_N, dtl,
+                                                  FLAG_FCT_TRACER, FLAG_FCT_ALONG_STREAM);
+    if (rc) return rc;
+    CK(d2h(QTRC, q, N3));
+    CU(cudaStreamSynchronize(C.stream));
+    return SCALE_HEVI_OK;
+}
+
+// ---- halo --------------------------------------------------------------------
+int COMM_vars8_b200_dev(double *var, const int *nfields)
+{
+    CK(need_setup());
+    if (!var || !nfields || *nfields < 1) return fail(SCALE_HEVI_ERR_ARG, "COMM_vars8: bad field list");
+    std::vector<double *> f(*nfields);
+    for (int q = 0; q < *nfields; ++q) f[q] = var + (size_t)q * C.N3;
+    halo(f.data(), *nfields);
+    return SCALE_HEVI_OK;
+}
+
+// ---- large step ----------------------------------------------------------------
+#define SCALE_HEVI_LARGE_ARGS                                                                                      \
+    double *DENS, double *MOMZ, double *MOMX, double *MOMY, double *RHOT, double *QTRC, const int *QA,             \
+        double *mflx_hi, double *tflx_hi, double *num_diff, const double *DENS_tp, const double *MOMZ_tp,          \
+        const double *MOMX_tp, const double *MOMY_tp, const double *RHOT_tp, const double *RHOQ_tp,                \
+        const double *CORIOLI, const double *CDZ, const double *CDX, const double *CDY, const double *FDZ,         \
+        const double *FDX, const double *FDY, const double *RCDZ, const double *RCDX, const double *RCDY,          \
+        const double *RFDZ, const double *RFDX, const double *RFDY, const double *PHI, const double *GSQRT,        \
+        const double *J13G, const double *J23G, const double *J33G, const double *MAPF, const double *AQ_R,        \
+        const double *AQ_CV, const double *AQ_CP, const double *AQ_MASS, const double *REF_dens,                   \
+        const double *REF_pott, const double *REF_pres, const double *ND_COEF, const int *ND_ORDER,                \
+        const double *ND_SFC_FACT, const int *ND_USE_RS, const double *wdamp_coef, const double *divdmp_coef,      \
+        const int *FLAG_FCT_TRACER, const int *FLAG_FCT_ALONG_STREAM, const double *DTLS, const double *DTSS
+
+int ATMOS_DYN_Tstep_large_fvm_heve_b200_dev(SCALE_HEVI_LARGE_ARGS)
+{
+    (void)PHI;
+    CK(need_setup());
+    const int qa = *QA;
+    if (qa < 0 || qa > 8) return fail(SCALE_HEVI_ERR_UNSUPPORTED, "QA=%d (0..8 supported)", qa);
+    if (*divdmp_coef > 0.0) return fail(SCALE_HEVI_ERR_UNSUPPORTED, "divergence damping (divdmp_coef > 0) is not supported in the large step");
+    if (*ND_COEF != 0.0 && *ND_ORDER != 1) return fail(SCALE_HEVI_ERR_UNSUPPORTED, "ND_ORDER=%d is not supported", *ND_ORDER);
+    if (*ND_COEF != 0.0 && !*ND_USE_RS) return fail(SCALE_HEVI_ERR_UNSUPPORTED, "ND_USE_RS=.false. is not supported");
+    CK(check_flat(GSQRT, J13G, J23G, MAPF, true));
+    const size_t N3 = C.N3;
+    if (!C.lg) CK(dalloc(&C.lg, 7 * N3));
+    if (!C.tr) CK(dalloc(&C.tr, 8 * N3));
+    double *DENS00 = C.lg, *RT2P = C.lg + N3, *DPRES0 = C.lg + 2 * N3, *REF_rhot = C.lg + 3 * N3, *mflx_av = C.lg + 4 * N3;
+
+    // time steps, :373-376
+    double dts = *DTSS;
+    const double dtl = *DTLS;
+    const int nstep = (int)std::ceil((dtl - EPS) / dts);
+    dts = dtl / nstep;
+
+    CU(cudaMemcpyAsync(DENS00, DENS, N3 * sizeof(double), cudaMemcpyDeviceToDevice, C.stream));
+    CU(cudaMemsetAsync(mflx_av, 0, 3 * N3 * sizeof(double), C.stream));
+    // RT2P / DPRES0 / REF_rhot, :428-470
+    PrepArgs pa{};
+    pa.RT2P = RT2P; pa.DPRES0 = DPRES0; pa.REF_rhot = REF_rhot; pa.RHOT = RHOT; pa.QTRC = QTRC; pa.REF_pres = REF_pres;
+    pa.QA = qa;
+    for (int q = 0; q < qa; ++q) { pa.AQ_R[q] = AQ_R[q]; pa.AQ_CV[q] = AQ_CV[q]; pa.AQ_CP[q] = AQ_CP[q]; pa.AQ_MASS[q] = AQ_MASS[q]; }
+    large_prep(C.g, pa, C.stream);
+    C.launches += 2;
+    CK(prepare_tables(CDZ, FDZ, RCDZ, RFDZ, FDX, RCDX, RFDX, FDY, RCDY, RFDY, wdamp_coef, CDX, CDY));
+    if (*ND_COEF != 0.0) CK(prepare_nd(CDZ, CDX, CDY, FDZ, FDX, FDY, dts, *ND_COEF, *ND_ORDER, *ND_SFC_FACT));
+
+    // With DAMP_alpha = 0 the tendencies of :606-839 equal the physics tendencies
+    // *_tp on every cell the short step reads, so *_tp are passed directly.
+    double *X[5] = {DENS, MOMZ, MOMX, MOMY, RHOT};
+    StageIn base{nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
+                 DENS_tp, MOMZ_tp, MOMX_tp, MOMY_tp, RHOT_tp, DPRES0, RT2P, CORIOLI, num_diff, nullptr,
+                 REF_dens, REF_rhot, 0.0, *J33G};
+    for (int step = 1; step <= nstep; ++step) {
+        if (*ND_COEF == 0.0) CU(cudaMemsetAsync(num_diff, 0, 15 * N3 * sizeof(double), C.stream));
+        else CK(run_numfilter(num_diff, DENS, MOMZ, MOMX, MOMY, RHOT, REF_dens, REF_pott));
+        CK(run_rk4(X, mflx_hi, tflx_hi, base, dts));
+        vertical_bc(C.g, DENS, MOMZ, MOMX, MOMY, RHOT, C.stream);
+        ++C.launches;
+        halo(X, 5);
+        mflx_accumulate(C.g, mflx_av, mflx_hi, C.stream);
+        ++C.launches;
+    }
+    if (qa > 0) {
+        mflx_average(C.g, mflx_hi, mflx_av, nstep, C.stream);
+        ++C.launches;
+        double *mf[3] = {mflx_hi, mflx_hi + N3, mflx_hi + 2 * N3};
+        halo(mf, 3);
+        for (int q = 0; q < qa; ++q) {
+            double *qt = QTRC + (size_t)q * N3;
+            CK(run_tracer_rk3(qt, qt, RHOQ_tp + (size_t)q * N3, DENS00, DENS, mflx_hi, nullptr, dtl,
+                              *FLAG_FCT_TRACER != 0, *FLAG_FCT_ALONG_STREAM != 0));
+            halo(&qt, 1);
+        }
+    }
+    return SCALE_HEVI_OK;
+}
+
+int ATMOS_DYN_Tstep_large_fvm_heve_b200(SCALE_HEVI_LARGE_ARGS)
+{
+    CK(need_setup());
+    CK(check_flat(GSQRT, J13G, J23G, MAPF, false));
+    const size_t N3 = n3(), N2 = (size_t)C.g.IA * C.g.JA;
+    const int qa = *QA;
+    double *X[5], *T[5], *q = nullptr, *rq = nullptr, *mf, *tf, *nd, *cor, *rd, *rp, *rpres;
+    double *hx[5] = {DENS, MOMZ, MOMX, MOMY, RHOT};
+    const double *ht[5] = {DENS_tp, MOMZ_tp, MOMX_tp, MOMY_tp, RHOT_tp};
+    static const char *n_x[5] = {"x0", "x1", "x2", "x3", "x4"}, *n_t[5] = {"t0", "t1", "t2", "t3", "t4"};
+    for (int v = 0; v < 5; ++v) {
+        CK(h2d(n_x[v], hx[v], N3, &X[v]));
+        CK(h2d(n_t[v], ht[v], N3, &T[v]));
+    }
+    if (qa > 0) {
+        CK(h2d("qtrc", QTRC, (size_t)qa * N3, &q));
+        CK(h2d("rhoq_tp", RHOQ_tp, (size_t)qa * N3, &rq));
+    }
+    CK(stage_buf("mflx", 3 * N3, &mf));
+    CK(stage_buf("tflx", 3 * N3, &tf));
+    CK(stage_buf("num_diff", 15 * N3, &nd));
+    CK(h2d("CORIOLI", CORIOLI, N2, &cor));
+    CK(h2d("REF_dens", REF_dens, N3, &rd));
+    CK(h2d("REF_pott", REF_pott, N3, &rp));
+    CK(h2d("REF_pres", REF_pres, N3, &rpres));
+    int rc = ATMOS_DYN_Tstep_large_fvm_heve_b200_dev(
+        X[0], X[1], X[2], X[3], X[4], q, QA, mf, tf, nd, T[0], T[1], T[2], T[3], T[4], rq, cor,
+        CDZ, CDX, CDY, FDZ, FDX, FDY, RCDZ, RCDX, RCDY, RFDZ, RFDX, RFDY, PHI, nullptr, nullptr, nullptr, J33G, nullptr,
+        AQ_R, AQ_CV, AQ_CP, AQ_MASS, rd, rp, rpres, ND_COEF, ND_ORDER, ND_SFC_FACT, ND_USE_RS, wdamp_coef, divdmp_coef,
+        FLAG_FCT_TRACER, FLAG_FCT_ALONG_STREAM, DTLS, DTSS);
+    if (rc) return rc;
+    for (int v = 0; v < 5; ++v) CK(d2h(hx[v], X[v], N3));
+    if (qa > 0) CK(d2h(QTRC, q, (size_t)qa * N3));
+    CK(d2h(mflx_hi, mf, 3 * N3));
+    CK(d2h(tflx_hi, tf, 3 * N3));
+    CK(d2h(num_diff, nd, 15 * N3));
+    CU(cudaStreamSynchronize(C.stream));
+    return scale_hevi_check();
+}
+
+int scale_hevi_domain_sum_dev(const double *var, const double *CDZ, const double *CDX, const double *CDY, double *total)
+{
+    CK(need_setup());
+    const int KA = C.g.KA, IA = C.g.IA, JA = C.g.JA;
+    std::vector<double> h(KA + IA + JA);
+    std::memcpy(h.data(), CDZ, KA * sizeof(double));
+    std::memcpy(h.data() + KA, CDX, IA * sizeof(double));
+    std::memcpy(h.data() + KA + IA, CDY, JA * sizeof(double));
+    double *d;
+    CK(stage_buf("sum_grid", h.size(), &d));
+    CU(cudaMemcpyAsync(d, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice, C.stream));
+    domain_sum(C.g, var, d + KA, d + KA + IA, d, C.sum_part, C.sum_out, C.stream);
+    C.launches += 2;
+    CU(cudaMemcpyAsync(total, C.sum_out, sizeof(double), cudaMemcpyDeviceToHost, C.stream));
+    CU(cudaStreamSynchronize(C.stream));
+    return SCALE_HEVI_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,94 @@
+// Shared device definitions for the B200 HEVI short-step kernels.
+//
+// Layout: every 3-D field is the reference's Fortran array (KA,IA,JA), k fastest,
+// halo width 2 in every direction (scale_atmos_grid_cartesC_index.F90:256-265).
+// Kernels use the reference's 1-based (k,i,j) indices so each expression can be
+// checked against the Fortran line it restates.
+//
+// Arithmetic: FP64, compiled with --fmad=false, and each expression keeps the
+// Fortran evaluation order, so the plain path reproduces the reference's
+// IEEE-754 results operation by operation. Flat terrain is assumed by these
+// kernels (GSQRT = 1, J13G = J23G = 0, MAPF = 1; checked by the host before any
+// launch): the metric factors then multiply or divide by exactly 1 and the
+// J13/J23 flux terms are exact zeros, so dropping them leaves every non-zero
+// value unchanged.
+#pragma once
+#include <cstddef>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace hevi {
+
+// flux schemes (ATMOS_DYN_FVM_FLUX_TYPE names)
+enum Scheme : int { UD3 = 1, CD4 = 2 };
+
+struct Grid {
+    int KA, IA, JA;
+    int KS, KE, IS, IE, JS, JE;
+    int KMAX, IMAX, JMAX;
+    int IHALO, JHALO;
+    int IEH, JEH;
+    // device 1-D tables, 0-based storage of the 1-based reference arrays
+    const double *CDZ, *FDZ, *RCDZ, *RFDZ;  // (KA), FDZ/RFDZ (KA-1)
+    const double *F2H1, *F2H2;              // face weights CDZ(k)/(CDZ(k)+CDZ(k+1)), CDZ(k+1)/(...)
+    const double *FDX, *RCDX, *RFDX;        // (IA)
+    const double *FDY, *RCDY, *RFDY;        // (JA)
+};
+
+__host__ __device__ __forceinline__ size_t idx3(const Grid &g, int k, int i, int j)
+{
+    return (size_t)(k - 1) + (size_t)g.KA * ((size_t)(i - 1) + (size_t)g.IA * (size_t)(j - 1));
+}
+__host__ __device__ __forceinline__ size_t n3(const Grid &g) { return (size_t)g.KA * g.IA * g.JA; }
+
+constexpr double GRAV = 9.80665;      // scale_const.F90:46
+constexpr double EPS = 2.220446049250313080847263336181640625e-16; // epsilon(0.0_RP)
+
+// SIGN(a,b) of Fortran = |a| with the sign bit of b
+__device__ __forceinline__ double fsign(double a, double b) { return copysign(fabs(a), b); }
+__device__ __forceinline__ double fmax2(double a, double b) { return a > b ? a : b; }
+__device__ __forceinline__ double fmin2(double a, double b) { return a < b ? a : b; }
+
+// ---- 4-point face interpolation of the flux schemes --------------------------
+// UD3: scale_atmos_dyn_fvm_flux_ud3.F90:87-89,124-125 ; CD4: ..._cd4.F90:87-88,123-124
+// The face lies between v0 and vp1.
+template <int S>
+__device__ __forceinline__ double ip4(double vel, double vm1, double v0, double vp1, double vp2)
+{
+    if (S == UD3) {
+        const double F31 = -1.0 / 12.0, F32 = 7.0 / 12.0, F33 = 3.0 / 12.0;
+        return (F31 * (vp2 + vm1) + F32 * (vp1 + v0)) - (F31 * (vp2 - vm1) + F33 * (vp1 - v0)) * fsign(1.0, vel);
+    } else {
+        const double F41 = 7.0 / 12.0, F42 = -1.0 / 12.0;
+        return F41 * (vp1 + v0) + F42 * (vp2 + vm1);
+    }
+}
+// value at the KS face from val(KS), val(KS+1), val(KS+2) (ud3.F90:142-145, cd4.F90:141)
+template <int S>
+__device__ __forceinline__ double ipL(double vel, double v0, double v1, double v2)
+{
+    if (S == UD3)
+        return 0.5 * (v1 + v0) * (0.5 + fsign(0.5, vel)) + (2.0 * v0 + 5.0 * v1 - v2) / 6.0 * (0.5 - fsign(0.5, vel));
+    else
+        return 0.5 * (v1 + v0);
+}
+// value at the KE-1 face from val(KE), val(KE-1), val(KE-2) (ud3.F90:146-149, cd4.F90:142)
+template <int S>
+__device__ __forceinline__ double ipH(double vel, double vE, double vE1, double vE2)
+{
+    if (S == UD3)
+        return (2.0 * vE + 5.0 * vE1 - vE2) / 6.0 * (0.5 + fsign(0.5, vel)) + 0.5 * (vE + vE1) * (0.5 - fsign(0.5, vel));
+    else
+        return 0.5 * (vE + vE1);
+}
+
+// read-only load through the non-coherent cache
+template <typename T>
+__device__ __forceinline__ T ld(const T *p) { return __ldg(p); }
+
+// device status word bits, read by the host after each call
+enum StatusBits : unsigned {
+    ST_NONFINITE = 1u << 0,   // a prognostic output is NaN/Inf
+};
+
+}  // namespace hevi

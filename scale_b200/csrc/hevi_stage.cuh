@@ -1,0 +1,46 @@
+// Argument block of one HEVI short-step stage on the device.
+#pragma once
+#include "hevi_common.cuh"
+
+namespace hevi {
+
+// RK4 accumulation performed in the stage epilogue. The four stages of
+// ATMOS_DYN_tinteg_short_rk4 (scale_atmos_dyn_tinteg_short_rk4.F90:376-560)
+// write their outputs to RK buffers and the combine (:562-650) forms
+//   X  = (RK1*2 + RK2*4 + RK3*2 + X4 - X0*3) / 6      (state, interior)
+//   F  = (F1 + F2*2 + F3*2 + F4) / 6                    (mflx_hi/tflx_hi, interior)
+// Accumulating the same sums left to right in the stage epilogues gives the
+// identical IEEE results without storing RK1..RK3 fluxes or a combine pass.
+enum RkMode : int {
+    RK_PLAIN = 0,  // one ATMOS_DYN_Tstep_short call: outputs only
+    RK_STAGE1 = 1, // acc = X*2, facc = F
+    RK_STAGE2 = 2, // acc += X*4, facc += F*2
+    RK_STAGE3 = 3, // acc += X*2, facc += F*2
+    RK_FINAL = 4,  // X = ((acc + X) - X0*3)/6, F = (facc + F)/6 over the interior
+};
+
+struct StageArgs {
+    // outputs (RK_FINAL: the state arrays themselves, updated in place)
+    double *DENS_RK, *MOMZ_RK, *MOMX_RK, *MOMY_RK, *RHOT_RK;
+    double *mflx; // mflx_hi(KA,IA,JA,3): Z, X, Y
+    double *tflx; // tflx_hi(KA,IA,JA,3)
+    // inputs
+    const double *DENS0, *MOMZ0, *MOMX0, *MOMY0, *RHOT0;
+    const double *DENS, *MOMZ, *MOMX, *MOMY, *RHOT;
+    const double *DENS_t, *MOMZ_t, *MOMX_t, *MOMY_t, *RHOT_t;
+    const double *DPRES0, *RT2P, *CORIOLI;
+    const double *num_diff; // (KA,IA,JA,5,3)
+    const double *wdamp;    // (KA)
+    const double *DDIV;
+    const double *REF_dens, *REF_rhot;
+    double divdmp_coef, J33G, dtrk;
+    // horizontal flux divergences handed from the 3-D kernel to the column kernel
+    double *adv_r, *adv_w, *adv_t;
+    // RK accumulation
+    int rk_mode;
+    double *acc;  // 5*N3: DENS, MOMZ, MOMX, MOMY, RHOT
+    double *facc; // 6*N3: mflx Z,X,Y then tflx Z,X,Y
+    unsigned *status;
+};
+
+}  // namespace hevi

@@ -1,0 +1,196 @@
+// Halo fill, vertical boundary fill, large-step preparation, metric check and
+// budget reduction kernels.
+#include "hevi_kernels.cuh"
+
+namespace hevi {
+
+// ---- periodic halo fill: COMM_vars8 + COMM_wait on a single periodic rank ----
+// (scalelib/src/communication/scale_comm_cartesC.F90:345-397, 1600-2043). Every
+// halo column takes all KA levels of its periodic image; corners included.
+struct FieldList {
+    double *f[16];
+};
+
+__global__ void k_halo(const Grid g, const FieldList fl)
+{
+    const int nA = 2 * g.JHALO * g.IA;      // halo rows j < JS and j > JE, all i
+    const int nB = 2 * g.IHALO * g.JMAX;    // halo columns i < IS and i > IE, interior j
+    const int h = blockIdx.x * blockDim.y + threadIdx.y;
+    if (h >= nA + nB) return;
+    int i, j;
+    if (h < nA) {
+        const int r = h / g.IA;
+        i = 1 + h % g.IA;
+        j = r < g.JHALO ? 1 + r : g.JE + 1 + (r - g.JHALO);
+    } else {
+        const int q = h - nA;
+        const int r = q / g.JMAX;
+        j = g.JS + q % g.JMAX;
+        i = r < g.IHALO ? 1 + r : g.IE + 1 + (r - g.IHALO);
+    }
+    const int si = i < g.IS ? i + g.IMAX : (i > g.IE ? i - g.IMAX : i);
+    const int sj = j < g.JS ? j + g.JMAX : (j > g.JE ? j - g.JMAX : j);
+    double *v = fl.f[blockIdx.y];
+    const size_t dst = idx3(g, 1, i, j), src = idx3(g, 1, si, sj);
+    for (int k = threadIdx.x; k < g.KA; k += 32) v[dst + k] = v[src + k];
+}
+
+void periodic_halo(const Grid &g, double *const *fields, int nf, cudaStream_t st)
+{
+    const int nh = 2 * g.JHALO * g.IA + 2 * g.IHALO * g.JMAX;
+    for (int base = 0; base < nf; base += 16) {
+        FieldList fl;
+        const int n = (nf - base) < 16 ? (nf - base) : 16;
+        for (int q = 0; q < n; ++q) fl.f[q] = fields[base + q];
+        dim3 b(32, 4), gr((nh + 3) / 4, n);
+        k_halo<<<gr, b, 0, st>>>(g, fl);
+    }
+}
+
+// ---- vertical boundary values after a short step (scale_atmos_dyn_tstep_large_fvm_heve.F90:910-926) ----
+__global__ void k_vbc(const Grid g, double *DENS, double *MOMZ, double *MOMX, double *MOMY, double *RHOT)
+{
+    const int i = g.IS + blockIdx.x * blockDim.y + threadIdx.y;
+    const int j = g.JS + blockIdx.y;
+    if (i > g.IE) return;
+    const size_t c = idx3(g, 1, i, j);
+    const int k = 1 + threadIdx.x;
+    if (k <= g.KS - 1) {
+        const size_t s = c + g.KS - 1, d = c + k - 1;
+        DENS[d] = DENS[s]; MOMZ[d] = 0.0; MOMX[d] = MOMX[s]; MOMY[d] = MOMY[s]; RHOT[d] = RHOT[s];
+    } else if (k <= g.KS - 1 + (g.KA - g.KE)) {
+        const int kk = g.KE + (k - (g.KS - 1));
+        const size_t s = c + g.KE - 1, d = c + kk - 1;
+        DENS[d] = DENS[s]; MOMZ[d] = 0.0; MOMX[d] = MOMX[s]; MOMY[d] = MOMY[s]; RHOT[d] = RHOT[s];
+    }
+}
+
+void vertical_bc(const Grid &g, double *DENS, double *MOMZ, double *MOMX, double *MOMY, double *RHOT, cudaStream_t st)
+{
+    dim3 b(32, 4), gr((g.IMAX + 3) / 4, g.JMAX);
+    k_vbc<<<gr, b, 0, st>>>(g, DENS, MOMZ, MOMX, MOMY, RHOT);
+}
+
+// ---- RT2P, DPRES0, REF_rhot once per large step (tstep_large_fvm_heve.F90:428-470, moist form) ----
+__global__ void k_large_prep(const Grid g, const PrepArgs a)
+{
+    const int i = 1 + blockIdx.x * blockDim.y + threadIdx.y;
+    const int j = 1 + blockIdx.y;
+    if (i > g.IA) return;
+    const size_t N3 = n3(g), col = idx3(g, 1, i, j);
+    const double P0 = 100000.0, Rdry = 287.04, CPdry = 1004.64, CVdry = CPdry - Rdry;
+    for (int k = g.KS + threadIdx.x; k <= g.KE; k += 32) {
+        const size_t c = col + k - 1;
+        double Rtot = 0.0, CVtot = 0.0, CPtot = 0.0, QDRY = 1.0;
+        for (int iq = 0; iq < a.QA; ++iq) {
+            const double q = a.QTRC[c + (size_t)iq * N3];
+            Rtot = Rtot + a.AQ_R[iq] * q;
+            CVtot = CVtot + a.AQ_CV[iq] * q;
+            CPtot = CPtot + a.AQ_CP[iq] * q;
+            QDRY = QDRY - q * a.AQ_MASS[iq];
+        }
+        Rtot = Rtot + Rdry * QDRY;
+        CVtot = CVtot + CVdry * QDRY;
+        CPtot = CPtot + CPdry * QDRY;
+        const double rhot = a.RHOT[c];
+        const double PRES = P0 * pow(Rtot * rhot / P0, CPtot / CVtot);
+        a.RT2P[c] = CPtot / CVtot * PRES / rhot;
+        a.DPRES0[c] = PRES - a.REF_pres[c];
+        a.REF_rhot[c] = rhot;
+    }
+}
+__global__ void k_large_prep_edge(const Grid g, const PrepArgs a)
+{
+    const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = 1 + blockIdx.y;
+    if (i > g.IA) return;
+    const size_t col = idx3(g, 1, i, j);
+    const int KS = g.KS, KE = g.KE;
+    a.DPRES0[col + KS - 2] = a.DPRES0[col + KS] + (a.REF_pres[col + KS] - a.REF_pres[col + KS - 2]);
+    a.DPRES0[col + KE] = a.DPRES0[col + KE - 2] + (a.REF_pres[col + KE - 2] - a.REF_pres[col + KE]);
+}
+
+void large_prep(const Grid &g, const PrepArgs &a, cudaStream_t st)
+{
+    dim3 b(32, 4), gr((g.IA + 3) / 4, g.JA);
+    k_large_prep<<<gr, b, 0, st>>>(g, a);
+    dim3 b2(128), g2((g.IA + 127) / 128, g.JA);
+    k_large_prep_edge<<<g2, b2, 0, st>>>(g, a);
+}
+
+// ---- flat-terrain check of the metric arrays --------------------------------
+__global__ void k_count_ne(const double *p, size_t n, double want, unsigned long long *count)
+{
+    unsigned long long local = 0;
+    for (size_t q = blockIdx.x * (size_t)blockDim.x + threadIdx.x; q < n; q += (size_t)gridDim.x * blockDim.x)
+        local += (p[q] != want);
+    if (local) atomicAdd(count, local);
+}
+
+void count_not_equal(const double *p, size_t n, double want, unsigned long long *count, cudaStream_t st)
+{
+    k_count_ne<<<148 * 8, 256, 0, st>>>(p, n, want, count);
+}
+
+// ---- FP64 domain budget: sum of var*CDZ*CDX*CDY over the interior ------------
+// Deterministic two-level reduction: one partial per column (k summed in order),
+// then a fixed-shape tree over columns.
+__global__ void k_col_sum(const Grid g, const double *var, const double *CDX, const double *CDY, const double *CDZ, double *part)
+{
+    const int i = g.IS + blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = g.JS + blockIdx.y;
+    if (i > g.IE) return;
+    const size_t col = idx3(g, 1, i, j);
+    double s = 0.0;
+    for (int k = g.KS; k <= g.KE; ++k) s += var[col + k - 1] * ld(CDZ + k - 1) * ld(CDX + i - 1) * ld(CDY + j - 1);
+    part[(size_t)(i - g.IS) + (size_t)g.IMAX * (j - g.JS)] = s;
+}
+__global__ void k_tree_sum(const double *part, size_t n, double *out)
+{
+    __shared__ double sh[1024];
+    double s = 0.0;
+    for (size_t q = threadIdx.x; q < n; q += blockDim.x) s += part[q];
+    sh[threadIdx.x] = s;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+        if ((int)threadIdx.x < w) sh[threadIdx.x] += sh[threadIdx.x + w];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) *out = sh[0];
+}
+
+void domain_sum(const Grid &g, const double *var, const double *CDX, const double *CDY, const double *CDZ,
+                double *part, double *out, cudaStream_t st)
+{
+    dim3 b(128), gr((g.IMAX + 127) / 128, g.JMAX);
+    k_col_sum<<<gr, b, 0, st>>>(g, var, CDX, CDY, CDZ, part);
+    k_tree_sum<<<1, 1024, 0, st>>>(part, (size_t)g.IMAX * g.JMAX, out);
+}
+
+// ---- short-step average of the mass flux for tracer advection
+// (tstep_large_fvm_heve.F90:960-967 and :1012-1019), interior cells ----
+__global__ void k_mflx_acc(const Grid g, double *av, const double *mflx, int nstep, int mode)
+{
+    const int i = g.IS + blockIdx.x * blockDim.y + threadIdx.y;
+    const int j = g.JS + blockIdx.y;
+    if (i > g.IE) return;
+    const size_t N3 = n3(g), col = idx3(g, 1, i, j);
+    for (int k = g.KS + threadIdx.x; k <= g.KE; k += 32)
+        for (int n = 0; n < 3; ++n) {
+            const size_t c = col + k - 1 + (size_t)n * N3;
+            if (mode == 0) av[c] = av[c] + mflx[c];
+            else ((double *)mflx)[c] = av[c] / nstep;
+        }
+}
+void mflx_accumulate(const Grid &g, double *av, const double *mflx, cudaStream_t st)
+{
+    dim3 b(32, 4), gr((g.IMAX + 3) / 4, g.JMAX);
+    k_mflx_acc<<<gr, b, 0, st>>>(g, av, mflx, 1, 0);
+}
+void mflx_average(const Grid &g, double *mflx, const double *av, int nstep, cudaStream_t st)
+{
+    dim3 b(32, 4), gr((g.IMAX + 3) / 4, g.JMAX);
+    k_mflx_acc<<<gr, b, 0, st>>>(g, (double *)av, mflx, nstep, 1);
+}
+
+}  // namespace hevi

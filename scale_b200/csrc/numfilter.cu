@@ -1,0 +1,190 @@
+// Numerical hyper-diffusion fluxes num_diff(KA,IA,JA,5,3) for ND_ORDER = 1
+// (ATMOS_DYN_numfilter_coef, scale_atmos_dyn_common.F90:385-985, with the
+// third-difference operator calc_diff3 :1600-1760 and its coefficients from
+// ATMOS_DYN_filter_setup :200-330).
+//
+// One thread per (k,i,j) of an interior column writes all 15 components at its
+// level, including the zero and mirrored values of the vertical halo, so the
+// seven inputs are streamed once and the fifteen outputs written once. The
+// lateral halo is filled afterwards by the periodic halo kernel, as COMM_vars8
+// does in the reference.
+#include "hevi_kernels.cuh"
+
+namespace hevi {
+
+#define CZ3(n, k, s) ld(c.CNZ3 + ((n) - 1) + 3 * ((size_t)((k) - 1) + (size_t)g.KA * ((s) - 1)))
+#define CX3(n, i, s) ld(c.CNX3 + ((n) - 1) + 3 * ((size_t)((i) - 1) + (size_t)g.IA * ((s) - 1)))
+#define CY3(n, j, s) ld(c.CNY3 + ((n) - 1) + 3 * ((size_t)((j) - 1) + (size_t)g.JA * ((s) - 1)))
+
+// The five filtered quantities, evaluated at any (k,i,j) the stencils need.
+// q: 0 DENS-REF_dens, 1 VELZ, 2 VELX, 3 VELY, 4 RHOT/DENS-REF_pott  (:538-547, 621-626, 715-720, 799-804, 876-883)
+struct Phi {
+    const Grid &g;
+    const NdArgs &a;
+    __device__ double operator()(int q, int k, int i, int j) const
+    {
+        const size_t c = idx3(g, k, i, j);
+        const long sI = g.KA, sJ = (long)g.KA * g.IA;
+        switch (q) {
+        case 0: return ld(a.DENS + c) - ld(a.REF_dens + c);
+        case 1: return 2.0 * ld(a.MOMZ + c) / (ld(a.DENS + c + 1) + ld(a.DENS + c));
+        case 2: return 2.0 * ld(a.MOMX + c) / (ld(a.DENS + c + sI) + ld(a.DENS + c));
+        case 3: return 2.0 * ld(a.MOMY + c) / (ld(a.DENS + c + sJ) + ld(a.DENS + c));
+        default: return ld(a.RHOT + c) / ld(a.DENS + c) - ld(a.REF_pott + c);
+        }
+    }
+};
+
+// calc_diff3 z-component with KO = 0 (:1617-1655) at level k (any k in 1..KA)
+__device__ double dz0(const Grid &g, const NdCoef &c, const Phi &phi, int q, int k, int i, int j)
+{
+    const int KS = g.KS, KE = g.KE;
+    auto inner = [&](int m) {
+        return (+CZ3(1, m + 1, 1) * phi(q, m + 2, i, j) - CZ3(2, m + 1, 1) * phi(q, m + 1, i, j)
+                + CZ3(3, m + 1, 1) * phi(q, m, i, j) - CZ3(1, m, 1) * phi(q, m - 1, i, j));
+    };
+    auto atKS = [&]() {
+        return (+CZ3(1, KS + 1, 1) * phi(q, KS + 2, i, j) - CZ3(2, KS + 1, 1) * phi(q, KS + 1, i, j)
+                + CZ3(3, KS + 1, 1) * phi(q, KS, i, j) - CZ3(1, KS, 1) * phi(q, KS + 1, i, j));
+    };
+    auto atKEm1 = [&]() {
+        return (+CZ3(1, KE, 1) * phi(q, KE - 1, i, j) - CZ3(2, KE, 1) * phi(q, KE, i, j)
+                + CZ3(3, KE, 1) * phi(q, KE - 1, i, j) - CZ3(1, KE - 1, 1) * phi(q, KE - 2, i, j));
+    };
+    if (k >= KS + 1 && k <= KE - 2) return inner(k);
+    if (k == KS) return atKS();
+    if (k == KS - 1) return -atKS();
+    if (k == KS - 2) return -inner(KS + 1);
+    if (k == KE - 1) return atKEm1();
+    if (k == KE) return -atKEm1();
+    if (k == KE + 1) return -inner(KE - 2);
+    return 0.0; // KE+2
+}
+
+// calc_diff3 z-component with KO = 1 (:1657-1705)
+__device__ double dz1(const Grid &g, const NdCoef &c, const Phi &phi, int q, int k, int i, int j)
+{
+    const int KS = g.KS, KE = g.KE;
+    auto inner = [&](int m) {
+        return (+CZ3(1, m, 2) * phi(q, m + 1, i, j) - CZ3(2, m, 2) * phi(q, m, i, j)
+                + CZ3(3, m, 2) * phi(q, m - 1, i, j) - CZ3(1, m - 1, 2) * phi(q, m - 2, i, j));
+    };
+    auto atKSp1 = [&]() {
+        return (+CZ3(1, KS + 1, 2) * phi(q, KS + 2, i, j) - CZ3(2, KS + 1, 2) * phi(q, KS + 1, i, j)
+                + CZ3(3, KS + 1, 2) * phi(q, KS, i, j) - CZ3(1, KS, 2) * phi(q, KS + 1, i, j));
+    };
+    auto atKEm1 = [&]() {
+        return (-CZ3(2, KE - 1, 2) * phi(q, KE - 1, i, j) + CZ3(3, KE - 1, 2) * phi(q, KE - 2, i, j)
+                - CZ3(1, KE - 2, 2) * phi(q, KE - 3, i, j));
+    };
+    auto atKE = [&]() {
+        return (+CZ3(1, KE, 2) * phi(q, KE - 1, i, j) + CZ3(3, KE, 2) * phi(q, KE - 1, i, j)
+                - CZ3(1, KE - 1, 2) * phi(q, KE - 2, i, j));
+    };
+    if (k >= KS + 2 && k <= KE - 2) return inner(k);
+    if (k == KS + 1) return atKSp1();
+    if (k == KS) return -atKSp1();
+    if (k == KS - 1) return -inner(KS + 2);
+    if (k == KS - 2) return -inner(KS + 3);
+    if (k == KE - 1) return atKEm1();
+    if (k == KE) return atKE();
+    if (k == KE + 1) return -atKE();
+    return -atKEm1(); // KE+2
+}
+
+// x and y components (:1707-1760); o selects IO/JO
+__device__ __forceinline__ double dx(const Grid &g, const NdCoef &c, const Phi &phi, int q, int o, int k, int i, int j)
+{
+    if (o == 0)
+        return (+CX3(1, i + 1, 1) * phi(q, k, i + 2, j) - CX3(2, i + 1, 1) * phi(q, k, i + 1, j)
+                + CX3(3, i + 1, 1) * phi(q, k, i, j) - CX3(1, i, 1) * phi(q, k, i - 1, j));
+    return (+CX3(1, i, 2) * phi(q, k, i + 1, j) - CX3(2, i, 2) * phi(q, k, i, j)
+            + CX3(3, i, 2) * phi(q, k, i - 1, j) - CX3(1, i - 1, 2) * phi(q, k, i - 2, j));
+}
+__device__ __forceinline__ double dy(const Grid &g, const NdCoef &c, const Phi &phi, int q, int o, int k, int i, int j)
+{
+    if (o == 0)
+        return (+CY3(1, j + 1, 1) * phi(q, k, i, j + 2) - CY3(2, j + 1, 1) * phi(q, k, i, j + 1)
+                + CY3(3, j + 1, 1) * phi(q, k, i, j) - CY3(1, j, 1) * phi(q, k, i, j - 1));
+    return (+CY3(1, j, 2) * phi(q, k, i, j + 1) - CY3(2, j, 2) * phi(q, k, i, j)
+            + CY3(3, j, 2) * phi(q, k, i, j - 1) - CY3(1, j - 1, 2) * phi(q, k, i, j - 2));
+}
+
+__global__ void __launch_bounds__(128) k_numfilter(const Grid g, const NdCoef c, const NdArgs a)
+{
+    const int i = g.IS + blockIdx.x * blockDim.y + threadIdx.y;
+    const int j = g.JS + blockIdx.y;
+    if (i > g.IE) return;
+    const size_t N3 = n3(g);
+    const int KS = g.KS, KE = g.KE;
+    const Phi phi{g, a};
+    const double *DN = a.DENS;
+    const long sI = g.KA, sJ = (long)g.KA * g.IA;
+    const double ncx = ld(c.cdx + i - 1), nfx = ld(c.fdx + i - 1), ncy = ld(c.cdy + j - 1), nfy = ld(c.fdy + j - 1);
+    const double sfc = c.sfc;
+    // surface-factor tail of every x/y component (:581-585 and the analogous blocks)
+    auto sfct = [&](int k, double v) {
+        if (k == KS) return v * sfc;
+        if (k == KS + 1) return v * (1.0 + sfc) * 0.5;
+        return v;
+    };
+    for (int k = 1 + threadIdx.x; k <= g.KA; k += 32) {
+        const size_t o = idx3(g, k, i, j);
+        const double ncz = (k >= KS - 1 && k <= KE) ? ld(c.cdz + k - 1) : 0.0;
+        double *ND = a.num_diff;
+        const bool kin = (k >= KS && k <= KE);
+        // ---- density (:553-610) ----
+        ND[o + N3 * 0] = (k >= KS - 1 && k <= KE) ? dz0(g, c, phi, 0, k, i, j) * ncz : 0.0;
+        ND[o + N3 * 5] = kin ? sfct(k, dx(g, c, phi, 0, 0, k, i, j) * ncx) : 0.0;
+        ND[o + N3 * 10] = kin ? sfct(k, dy(g, c, phi, 0, 0, k, i, j) * ncy) : 0.0;
+        // ---- z momentum (:628-698), phi = VELZ on KS..KE-1 ----
+        {
+            const bool kz = (k >= KS && k <= KE - 1);
+            const double nfz = (k >= KS + 1 && k <= KE - 1) ? ld(c.fdz + k - 1) : 0.0;
+            ND[o + N3 * 1] = (k >= KS + 1 && k <= KE - 1) ? dz1(g, c, phi, 1, k, i, j) * nfz * ld(DN + o) : 0.0;
+            ND[o + N3 * 6] = kz ? sfct(k, dx(g, c, phi, 1, 0, k, i, j) * ncx
+                                              * 0.25 * (ld(DN + o + 1 + sI) + ld(DN + o + 1) + ld(DN + o + sI) + ld(DN + o)))
+                                : 0.0;
+            ND[o + N3 * 11] = kz ? sfct(k, dy(g, c, phi, 1, 0, k, i, j) * ncy
+                                               * 0.25 * (ld(DN + o + 1 + sJ) + ld(DN + o + 1) + ld(DN + o + sJ) + ld(DN + o)))
+                                 : 0.0;
+        }
+        // ---- x momentum (:728-790), phi = VELX ----
+        ND[o + N3 * 2] = (k >= KS && k <= KE - 1)
+                             ? dz0(g, c, phi, 2, k, i, j) * ncz
+                                   * 0.25 * (ld(DN + o + 1 + sI) + ld(DN + o + 1) + ld(DN + o + sI) + ld(DN + o))
+                             : 0.0;
+        ND[o + N3 * 7] = kin ? sfct(k, dx(g, c, phi, 2, 1, k, i, j) * nfx * ld(DN + o)) : 0.0;
+        ND[o + N3 * 12] = kin ? sfct(k, dy(g, c, phi, 2, 0, k, i, j) * ncy
+                                            * 0.25 * (ld(DN + o + sI + sJ) + ld(DN + o + sI) + ld(DN + o + sJ) + ld(DN + o)))
+                              : 0.0;
+        // ---- y momentum (:812-870), phi = VELY ----
+        ND[o + N3 * 3] = (k >= KS && k <= KE - 1)
+                             ? dz0(g, c, phi, 3, k, i, j) * ncz
+                                   * 0.25 * (ld(DN + o + 1 + sJ) + ld(DN + o + 1) + ld(DN + o + sJ) + ld(DN + o))
+                             : 0.0;
+        ND[o + N3 * 8] = kin ? sfct(k, dx(g, c, phi, 3, 0, k, i, j) * ncx
+                                           * 0.25 * (ld(DN + o + sI + sJ) + ld(DN + o + sJ) + ld(DN + o + sI) + ld(DN + o)))
+                             : 0.0;
+        ND[o + N3 * 13] = kin ? sfct(k, dy(g, c, phi, 3, 1, k, i, j) * nfy * ld(DN + o)) : 0.0;
+        // ---- rho*theta (:885-960) ----
+        {
+            double v = 0.0;
+            if (k >= KS && k <= KE - 1) v = dz0(g, c, phi, 4, k, i, j) * ncz * 0.5 * (ld(DN + o + 1) + ld(DN + o));
+            else if (k == KS - 1) v = dz0(g, c, phi, 4, k, i, j) * ncz * ld(DN + idx3(g, KS, i, j));
+            else if (k == KE) v = dz0(g, c, phi, 4, k, i, j) * ncz * ld(DN + o);
+            ND[o + N3 * 4] = v;
+        }
+        ND[o + N3 * 9] = kin ? sfct(k, dx(g, c, phi, 4, 0, k, i, j) * ncx * 0.5 * (ld(DN + o + sI) + ld(DN + o))) : 0.0;
+        ND[o + N3 * 14] = kin ? sfct(k, dy(g, c, phi, 4, 0, k, i, j) * ncy * 0.5 * (ld(DN + o + sJ) + ld(DN + o))) : 0.0;
+    }
+}
+
+cudaError_t launch_numfilter(const Grid &g, const NdCoef &c, const NdArgs &a, cudaStream_t st)
+{
+    dim3 b(32, 4), gr((g.IMAX + 3) / 4, g.JMAX);
+    k_numfilter<<<gr, b, 0, st>>>(g, c, a);
+    return cudaGetLastError();
+}
+
+}  // namespace hevi

@@ -1,0 +1,229 @@
+"""Python binding of libscale_hevi.so.
+
+The functions below carry the names and argument lists of the reference
+procedures they replace (see include/scale_hevi.h). Arguments are passed by
+keyword, as the reference's dummy names; arrays may be numpy arrays (host
+entries) or torch CUDA tensors (device entries, ``*_dev`` functions), scalars
+are Python numbers. Everything is handed to the C-ABI by reference, as
+gfortran would. A nonzero status raises HeviError with the library's message,
+mirroring the reference's PRC_abort.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import re
+from pathlib import Path
+
+import numpy as np
+
+from .build import LIB, ROOT
+
+HEADER = ROOT / "include" / "scale_hevi.h"
+
+ERRORS = {
+    1: "SCALE_HEVI_ERR_ARG",
+    2: "SCALE_HEVI_ERR_NOT_SETUP",
+    3: "SCALE_HEVI_ERR_CUDA",
+    4: "SCALE_HEVI_ERR_NONFINITE",
+    5: "SCALE_HEVI_ERR_UNSUPPORTED",
+    6: "SCALE_HEVI_ERR_ALLOC",
+}
+
+
+class HeviError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{ERRORS.get(code, code)}: {msg}")
+        self.code = code
+
+
+class Index(C.Structure):
+    _fields_ = [(n, C.c_int) for n in ("KA", "IA", "JA", "KS", "KE", "IS", "IE", "JS", "JE", "KMAX", "IMAX", "JMAX",
+                                       "KHALO", "IHALO", "JHALO", "IBLOCK", "JBLOCK")]
+
+
+def header_functions() -> dict[str, list[str]]:
+    """Exported functions declared in the header and their parameter names."""
+    text = HEADER.read_text()
+    macros = {}
+    for m in re.finditer(r"#define\s+(SCALE_HEVI_\w+_ARGS)\s*\\\n((?:.*\\\n)*.*)\n", text):
+        body = m.group(2).replace("\\\n", " ")
+        macros[m.group(1)] = body
+    out = {}
+    for m in re.finditer(r"\n(?:int|void \*|const char \*|long long)\s*(\w+)\(([^;]*?)\);", text):
+        name, params = m.group(1), m.group(2)
+        for k, v in macros.items():
+            params = params.replace(k, v)
+        names = []
+        for p in params.split(","):
+            p = p.strip()
+            if not p or p == "void":
+                continue
+            names.append(re.split(r"[\s\*]+", p)[-1])
+        out[name] = names
+    return out
+
+
+_lib = None
+_sig = None
+
+
+def load(path: str | os.PathLike | None = None) -> C.CDLL:
+    """Load the in-tree library (raises if it has not been built)."""
+    global _lib, _sig
+    if _lib is not None:
+        return _lib
+    p = Path(path) if path else LIB
+    if not p.exists():
+        raise FileNotFoundError(f"{p} is missing: run `python -m scale_b200.build` (or __graft_entry__.build())")
+    lib = C.CDLL(str(p))
+    _sig = header_functions()
+    for name, params in _sig.items():
+        f = getattr(lib, name)
+        if name == "scale_hevi_last_error":
+            f.restype = C.c_char_p
+        elif name == "scale_hevi_stream":
+            f.restype = C.c_void_p
+        elif name == "scale_hevi_kernel_launches":
+            f.restype = C.c_longlong
+        else:
+            f.restype = C.c_int
+        if name == "scale_hevi_setup":
+            f.argtypes = [C.POINTER(Index), C.c_char_p, C.c_char_p, C.c_int]
+        else:
+            f.argtypes = [C.c_void_p] * len(params)
+    _lib = lib
+    return lib
+
+
+def last_error() -> str:
+    return load().scale_hevi_last_error().decode()
+
+
+def _check(rc: int) -> None:
+    if rc != 0:
+        raise HeviError(rc, last_error())
+
+
+class _Args:
+    """Marshals keyword arguments into by-reference C arguments, keeping the
+    temporaries alive for the duration of the call."""
+
+    def __init__(self):
+        self.keep = []
+
+    def ptr(self, v, ints: bool):
+        if v is None:
+            return None
+        if isinstance(v, np.ndarray):
+            if v.dtype == np.float64 and (v.flags.f_contiguous or v.flags.c_contiguous):
+                return v.ctypes.data
+            raise TypeError("arrays must be contiguous float64 in Fortran order")
+        if hasattr(v, "data_ptr"):  # torch tensor
+            return v.data_ptr()
+        if isinstance(v, (bool, np.bool_)) or (ints and isinstance(v, (int, np.integer))):
+            c = C.c_int(int(v))
+        else:
+            c = C.c_double(float(v))
+        self.keep.append(c)
+        return C.addressof(c)
+
+
+INT_ARGS = {"FLAG_FCT_MOMENTUM", "FLAG_FCT_T", "FLAG_FCT_ALONG_STREAM", "FLAG_FCT_TRACER", "BND_W", "BND_E",
+            "BND_S", "BND_N", "last", "ND_ORDER", "ND_USE_RS", "QA", "nfields"}
+
+
+def call(name: str, **kw) -> None:
+    """Call an exported entry by name with keyword arguments named as its dummies."""
+    lib = load()
+    params = _sig[name]
+    unknown = set(kw) - set(params)
+    if unknown:
+        raise TypeError(f"{name}: unknown arguments {sorted(unknown)}")
+    a = _Args()
+    args = [a.ptr(kw.get(p), p in INT_ARGS) for p in params]
+    _check(getattr(lib, name)(*args))
+
+
+# ---- library state ----------------------------------------------------------------
+def setup(index: dict, flux_type: str = "UD3", flux_tracer_type: str = "UD3", device: int = 0) -> None:
+    """ATMOS_DYN_FVM_flux_setup + index setup of the HEVI short step."""
+    lib = load()
+    idx = Index(**index)
+    _check(lib.scale_hevi_setup(C.byref(idx), flux_type.encode(), flux_tracer_type.encode(), int(device)))
+
+
+def finalize() -> None:
+    load().scale_hevi_finalize()
+
+
+def check() -> None:
+    _check(load().scale_hevi_check())
+
+
+def kernel_launches() -> int:
+    return int(load().scale_hevi_kernel_launches())
+
+
+def stream_handle() -> int:
+    return int(load().scale_hevi_stream() or 0)
+
+
+# ---- reference-named entries (host arrays) ---------------------------------------
+def ATMOS_DYN_Tstep_short_fvm_hevi(**kw):
+    call("ATMOS_DYN_Tstep_short_fvm_hevi_b200", **kw)
+
+
+def ATMOS_DYN_Tinteg_short_rk4(**kw):
+    call("ATMOS_DYN_Tinteg_short_rk4_b200", **kw)
+
+
+def ATMOS_DYN_numfilter_coef(**kw):
+    call("ATMOS_DYN_numfilter_coef_b200", **kw)
+
+
+def ATMOS_DYN_Tstep_tracer_fvm_heve(**kw):
+    call("ATMOS_DYN_Tstep_tracer_fvm_heve_b200", **kw)
+
+
+def ATMOS_DYN_Tinteg_tracer_rk3(**kw):
+    call("ATMOS_DYN_Tinteg_tracer_rk3_b200", **kw)
+
+
+def ATMOS_DYN_Tstep_large_fvm_heve(**kw):
+    call("ATMOS_DYN_Tstep_large_fvm_heve_b200", **kw)
+
+
+# ---- device-array entries -----------------------------------------------------------
+def ATMOS_DYN_Tstep_short_fvm_hevi_dev(**kw):
+    call("ATMOS_DYN_Tstep_short_fvm_hevi_b200_dev", **kw)
+
+
+def ATMOS_DYN_Tinteg_short_rk4_dev(**kw):
+    call("ATMOS_DYN_Tinteg_short_rk4_b200_dev", **kw)
+
+
+def ATMOS_DYN_numfilter_coef_dev(**kw):
+    call("ATMOS_DYN_numfilter_coef_b200_dev", **kw)
+
+
+def ATMOS_DYN_Tstep_tracer_fvm_heve_dev(**kw):
+    call("ATMOS_DYN_Tstep_tracer_fvm_heve_b200_dev", **kw)
+
+
+def ATMOS_DYN_Tinteg_tracer_rk3_dev(**kw):
+    call("ATMOS_DYN_Tinteg_tracer_rk3_b200_dev", **kw)
+
+
+def ATMOS_DYN_Tstep_large_fvm_heve_dev(**kw):
+    call("ATMOS_DYN_Tstep_large_fvm_heve_b200_dev", **kw)
+
+
+def COMM_vars8_dev(var, nfields: int):
+    call("COMM_vars8_b200_dev", var=var, nfields=nfields)
+
+
+def domain_sum_dev(var, CDZ, CDX, CDY) -> float:
+    out = np.zeros(1)
+    call("scale_hevi_domain_sum_dev", var=var, CDZ=CDZ, CDX=CDX, CDY=CDY, total=out)
+    return float(out[0])

@@ -1,0 +1,219 @@
+"""The oracle pinned by the reference's own tests of this path.
+
+The reference ships no golden vectors for the HEVI short step. Its tests are
+property tests (scalelib/test/unit/test_atmos_dyn.f90:307-763), the halo test
+(scalelib/test/unit/test_comm.f90:150-250) and the DEBUG self-check of the
+implicit solve (scale_atmos_dyn_tstep_short_fvm_hevi.F90:1131-1271). They are
+re-run here on the oracle with the HEVI scheme.
+"""
+import numpy as np
+import pytest
+
+import helpers
+import oracle
+from scale_b200 import mkinit
+
+STATE = ("DENS", "MOMZ", "MOMX", "MOMY", "RHOT")
+
+
+def _large(c, nlarge=1, fct=None, qa=None):
+    g = c.g
+    QA = c.QA if qa is None else qa
+    tp = {n: g.zeros() for n in ("DENS_tp", "MOMZ_tp", "MOMX_tp", "MOMY_tp", "RHOT_tp")}
+    if QA:
+        tp["RHOQ_tp"] = g.zeros(QA)
+    GS, J13, J23, MAPF = oracle.flat_metrics(g)
+    out = dict(mflx_hi=g.zeros(3), tflx_hi=g.zeros(3), num_diff=g.zeros(5, 3))
+    aq = mkinit.aq_props(QA) if QA else None
+    for _ in range(nlarge):
+        oracle.tstep_large(g, c.scheme, c.scheme_tracer, c.state, out, tp, c.ref, aq, GS, J13, J23, MAPF,
+                           np.zeros((g.IA, g.JA), order="F"), np.zeros(g.KA), c.dtl, c.dt, ND_COEF=c.nd_coef,
+                           fct=c.fct if fct is None else fct, QA=QA)
+    return out
+
+
+def _interior(a, g):
+    return a[g.KS - 1 : g.KE, g.IS - 1 : g.IE, g.JS - 1 : g.JE]
+
+
+@pytest.mark.parametrize("scheme", ["UD3", "CD4"])
+def test_const(scheme):
+    """test_const (test_atmos_dyn.f90:382-454): a horizontally uniform state stays uniform."""
+    g = helpers.small_grid(8, 6, 12)
+    c = mkinit.make_case("const", g, scheme, scheme, tracers=1, fct=True)
+    st = c.state
+    st["DENS"][...] = 1.0
+    st["MOMZ"][...] = 2.0
+    st["MOMX"][...] = 3.0
+    st["MOMY"][...] = 4.0
+    st["RHOT"][...] = 300.0
+    st["QTRC"][...] = 0.1
+    mkinit.vertical_fill(st, g)
+    c.ref["REF_dens"][...] = 1.0
+    c.ref["REF_pott"][...] = 300.0
+    c.ref["REF_pres"][...] = 1000.0
+    c.dtl, c.dt = 1.0, 1.0
+    _large(c)
+    for n in STATE:
+        x = _interior(st[n], g)
+        assert np.array_equal(x, np.broadcast_to(x[:, :1, :1], x.shape)), n
+    q = _interior(st["QTRC"][..., 0], g)
+    assert np.array_equal(q, np.broadcast_to(q[:, :1, :1], q.shape))
+
+
+@pytest.mark.parametrize("scheme", ["UD3", "CD4"])
+def test_conserve(scheme):
+    """test_conserve (test_atmos_dyn.f90:456-592): domain totals of DENS and RHOT
+    (weighted by the cell volume) are conserved to round-off."""
+    g = helpers.small_grid(10, 8, 14, stretched=True)
+    c = mkinit.make_case("conserve", g, scheme, scheme)
+    k, i, j = np.meshgrid(np.arange(1, g.KA + 1), np.arange(1, g.IA + 1), np.arange(1, g.JA + 1), indexing="ij")
+    st = c.state
+    st["MOMZ"][...] = (k + i + j) * 0.1
+    st["MOMX"][...] = (k * 2 + i + j) * 0.1
+    st["MOMY"][...] = (k + i * 2 + j) * 0.1
+    st["DENS"][...] = c.ref["REF_dens"] + (k * 2 + i * 2 + j) * 1e-3
+    st["RHOT"][...] = st["DENS"] * (300.0 + (k + i + j * 2) * 0.01)
+    for n in STATE:
+        mkinit.periodic_fill(st[n], g)
+    mkinit.vertical_fill(st, g)
+    m0 = oracle.domain_sum(g, st["DENS"])
+    t0 = oracle.domain_sum(g, st["RHOT"])
+    _large(c, 2)
+    assert abs(oracle.domain_sum(g, st["DENS"]) - m0) / m0 < 1e-13
+    assert abs(oracle.domain_sum(g, st["RHOT"]) - t0) / t0 < 1e-13
+
+
+def test_cwc():
+    """test_cwc (test_atmos_dyn.f90:594-670): uniform theta and tracer stay uniform
+    under random momenta (consistency with the continuity equation)."""
+    g = helpers.small_grid(10, 10, 14)
+    c = mkinit.make_case("cwc", g, "UD3", "UD3", tracers=1, fct=True)
+    rng = np.random.Generator(np.random.PCG64(3))
+    st = c.state
+    st["DENS"][...] = c.ref["REF_dens"] * (1.0 + 1e-3 * rng.uniform(-1, 1, size=g.shape))
+    st["MOMZ"][...] = rng.uniform(-1, 1, size=g.shape)
+    st["MOMX"][...] = rng.uniform(-3, 3, size=g.shape)
+    st["MOMY"][...] = rng.uniform(-3, 3, size=g.shape)
+    st["RHOT"][...] = st["DENS"] * 300.0
+    st["QTRC"][...] = 0.01
+    for n in STATE:
+        mkinit.periodic_fill(st[n], g)
+    mkinit.vertical_fill(st, g)
+    c.ref["REF_pott"][...] = 300.0
+    _large(c)
+    pott = _interior(st["RHOT"] / st["DENS"], g)
+    assert np.max(np.abs(pott - 300.0)) / 300.0 < 1e-12
+    q = _interior(st["QTRC"][..., 0], g)
+    assert np.max(np.abs(q - 0.01)) / 0.01 < 1e-12
+
+
+@pytest.mark.parametrize("along", [True, False])
+def test_fct_minmax(along):
+    """test_fctminmax (test_atmos_dyn.f90:672-763): with FCT the tracer stays
+    inside its initial range."""
+    g = helpers.small_grid(12, 12, 16)
+    c = helpers.small_case(g, "UD3", tracers=1, wind=5.0)
+    c.fct = True
+    rng = np.random.Generator(np.random.PCG64(9))
+    q = c.state["QTRC"]
+    q[..., 0] = np.where(rng.uniform(size=g.shape) > 0.5, 1.0e-3, 0.0)
+    mkinit.periodic_fill(q[..., 0], g)
+    qmin, qmax = 0.0, 1.0e-3
+    GS, _, _, MAPF = oracle.flat_metrics(g)
+    tp = {n: g.zeros() for n in ("DENS_tp", "MOMZ_tp", "MOMX_tp", "MOMY_tp", "RHOT_tp")}
+    tp["RHOQ_tp"] = g.zeros(1)
+    out = dict(mflx_hi=g.zeros(3), tflx_hi=g.zeros(3), num_diff=g.zeros(5, 3))
+    for _ in range(2):
+        oracle.tstep_large(g, "UD3", "UD3", c.state, out, tp, c.ref, mkinit.aq_props(1), GS, *oracle.flat_metrics(g)[1:3],
+                           MAPF, np.zeros((g.IA, g.JA), order="F"), np.zeros(g.KA), 5.0, 1.0, fct=True, along=along, QA=1)
+    x = _interior(q[..., 0], g)
+    eps = 1e-10
+    assert x.min() >= qmin - eps and x.max() <= qmax * (1.0 + eps)
+
+
+def test_no_undefined_values_leak():
+    """test_undef (test_atmos_dyn.f90:307-380): NaN in the vertical halo of the
+    state never reaches the interior (the short step reads only defined cells)."""
+    g = helpers.small_grid(10, 8, 14)
+    c = helpers.small_case(g)
+    helpers.perturb_state(c)
+    for n in STATE:
+        c.state[n][: g.KS - 1] = np.nan
+        c.state[n][g.KE :] = np.nan
+    _large(c, 1)
+    for n in STATE:
+        assert np.all(np.isfinite(_interior(c.state[n], g))), n
+
+
+def test_solver_residual_check():
+    """check_equation (tstep_short_fvm_hevi.F90:1131-1271) aborts above 1e-6; it
+    was written for CD4 face values and uniform dz."""
+    g = helpers.small_grid(10, 10, 20)
+    c = helpers.small_case(g, "CD4")
+    helpers.perturb_state(c)
+    RT2P, DPRES0, REF_rhot = mkinit.large_prep(c)
+    nd = g.zeros(5, 3)
+    oracle.numfilter(g, nd, c.state, c.ref, DT=1.0)
+    r = oracle.max_residual(g, "CD4", c.state, DPRES0, RT2P, nd, c.ref, REF_rhot, 0.5)
+    assert r < 1e-6
+
+
+def test_halo_fill_neighbours():
+    """test_comm.f90:150-250: the N/S/E/W and corner halos hold the periodic neighbours."""
+    g = helpers.small_grid(7, 5, 6)
+    k, i, j = np.meshgrid(np.arange(1, g.KA + 1), np.arange(1, g.IA + 1), np.arange(1, g.JA + 1), indexing="ij")
+    a = np.asfortranarray((k * 10000 + i * 100 + j).astype(np.float64))
+    oracle.halo(g, a)
+    wi = lambda ii: ii + g.IMAX if ii < g.IS else (ii - g.IMAX if ii > g.IE else ii)  # noqa: E731
+    wj = lambda jj: jj + g.JMAX if jj < g.JS else (jj - g.JMAX if jj > g.JE else jj)  # noqa: E731
+    for ii in range(1, g.IA + 1):
+        for jj in range(1, g.JA + 1):
+            exp = np.arange(1, g.KA + 1) * 10000 + wi(ii) * 100 + wj(jj)
+            assert np.array_equal(a[:, ii - 1, jj - 1], exp), (ii, jj)
+    b = a.copy(order="F")
+    mkinit.periodic_fill(b, g)
+    assert np.array_equal(a, b)
+
+
+def test_rk4_equals_four_stages():
+    """ATMOS_DYN_tinteg_short_rk4 restated twice: the oracle's integrator against
+    an explicit sequence of four oracle stages plus the combine (rk4.F90:376-650)."""
+    g = helpers.small_grid(9, 8, 12)
+    c = helpers.small_case(g)
+    helpers.perturb_state(c)
+    a = helpers.short_inputs(c, full=True)
+    for kk in ("DENS0", "MOMZ0", "MOMX0", "MOMY0", "RHOT0", "DENS", "MOMZ", "MOMX", "MOMY", "RHOT", "dtrk"):
+        a.pop(kk)
+    x = {n: c.state[n].copy(order="F") for n in STATE}
+    x["mflx_hi"] = g.zeros(3)
+    x["tflx_hi"] = g.zeros(3)
+    x0 = {n: v.copy(order="F") for n, v in x.items()}
+    oracle.tinteg_short_rk4(g, "UD3", x, dict(a, dt=1.0))
+    rk, fl = [], []
+    cur = {n: x0[n] for n in STATE}
+    for s, dtrk in enumerate((0.5, 0.5, 1.0, 1.0)):
+        o = helpers.stage_outputs(g, 0.0)
+        args = dict(a, dtrk=dtrk)
+        args.update({n + "0": x0[n] for n in STATE})
+        args.update(cur)
+        if s == 3:
+            o["mflx_hi"] = x0["mflx_hi"].copy(order="F")
+            o["tflx_hi"] = x0["tflx_hi"].copy(order="F")
+        oracle.tstep_short(g, "UD3", o, args)
+        st = {n: o[n + "_RK"] for n in STATE}
+        if s < 3:
+            for n in STATE:
+                oracle.halo(g, st[n])
+        rk.append(st)
+        fl.append((o["mflx_hi"], o["tflx_hi"]))
+        cur = st
+    sl = (slice(g.KS - 1, g.KE), slice(g.IS - 1, g.IE), slice(g.JS - 1, g.JE))
+    for n in STATE:
+        exp = (rk[0][n] * 2.0 + rk[1][n] * 4.0 + rk[2][n] * 2.0 + rk[3][n] - x0[n] * 3.0) / 6.0
+        ks = slice(g.KS - 1, g.KE - 1) if n == "MOMZ" else sl[0]
+        assert np.array_equal(x[n][ks, sl[1], sl[2]], exp[ks, sl[1], sl[2]]), n
+    for f in range(2):
+        exp = (fl[0][f] + fl[1][f] * 2.0 + fl[2][f] * 2.0 + fl[3][f]) / 6.0
+        got = x["mflx_hi" if f == 0 else "tflx_hi"]
+        assert np.array_equal(got[sl], exp[sl])
