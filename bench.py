@@ -1,0 +1,430 @@
+#!/usr/bin/env python
+"""Benchmark of the HEVI short step (SCALE-RM ATMOS_DYN_Tstep_short_fvm_hevi) on B200.
+
+Workload: the 512x512x128 configuration (dx = dy = 250 m, dz stretched 50 m to
+400 m, CD4 momentum/scalar flux, dt = 0.5 s, three moist tracers with FCT),
+synthetic seeded inputs (no public dataset is involved). One step is one
+iteration of the short-step loop of the large step
+(scale_atmos_dyn_tstep_large_fvm_heve.F90:600-944): the numerical filter
+coefficients, the RK4 short step (four HEVI stages with their device halo
+exchanges and the combine) and the boundary values + halo exchange of the
+state. The metric is interior cell-updates per second.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Under torchrun with N > 1 every rank runs its own replica of the workload on
+its GPU (the path is single-GPU by specification; no data-path collective) and
+the value is the aggregate over ranks divided by the slowest rank's time.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "HEVI short-step cell-updates/s on 1 B200, FP64 vs mixed at stated error; %HBM"
+UNIT = "cell-updates/s"
+L2_BYTES = 126 * 1024 * 1024
+# algorithmic bytes per interior cell: one HEVI stage reads 34
+# fields (DENS0..RHOT0, DENS..RHOT, *_t, DPRES0, RT2P, REF_dens, REF_rhot and the
+# 15 num_diff components; DDIV is not read because divdmp_coef = 0) and writes 11
+# (DENS_RK..RHOT_RK, mflx_hi(3), tflx_hi(3)); the filter reads 7 and writes 15.
+STAGE_BYTES = (34 + 11) * 8
+NUMFILTER_BYTES = (7 + 15) * 8
+STEP_BYTES = 4 * STAGE_BYTES + NUMFILTER_BYTES
+
+
+def rank_info():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("timestamp,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.window = None
+        self.path = Path(os.environ.get("TMPDIR", "/tmp")) / f"hevi_clocks_{os.getpid()}.csv"
+
+    def __enter__(self):
+        try:
+            self.fh = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.fh, stderr=subprocess.DEVNULL)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+            self.fh.close()
+
+    def mark(self, t0: float, t1: float):
+        """Host wall-clock bounds of the timed region."""
+        self.window = (t0, t1)
+
+    def summary(self):
+        if self.proc is None or not self.path.exists():
+            return None
+        from datetime import datetime
+
+        rows = []
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for line in self.path.read_text().splitlines():
+            p = [x.strip() for x in line.split(",")]
+            if len(p) < 9:
+                continue
+            try:
+                ts = datetime.strptime(p[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+                rows.append((ts, float(p[1]), float(p[2]), float(p[3]),
+                             [n for n, v in zip(names, p[5:9]) if v.lower() == "active"]))
+            except ValueError:
+                continue
+        self.path.unlink(missing_ok=True)
+        inside = [r for r in rows if self.window and self.window[0] <= r[0] <= self.window[1]]
+        used = inside or rows
+        if not used:
+            return None
+        return {"sm_mhz": statistics.median(r[1] for r in used), "sm_max_mhz": used[-1][2],
+                "power_w": statistics.median(r[3] for r in used),
+                "reasons": sorted({n for r in used for n in r[4]}), "samples": len(used),
+                "window": "timed region" if inside else "warm-up and timed region"}
+
+
+# ---------------------------------------------------------------------------
+# inputs
+# ---------------------------------------------------------------------------
+def make_inputs(scale: float):
+    from scale_b200 import mkinit
+
+    c = mkinit.config(2, scale=scale, seed=0)
+    RT2P, DPRES0, REF_rhot = mkinit.large_prep(c)
+    return c, RT2P, DPRES0, REF_rhot
+
+
+def to_dev(x, torch):
+    return torch.from_numpy(np.ravel(x, order="K")).cuda()
+
+
+# ---------------------------------------------------------------------------
+# the B200 arm
+# ---------------------------------------------------------------------------
+def run_b200(args):
+    import torch
+
+    from scale_b200 import hevi
+
+    rank, world, local = rank_info()
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    c, RT2P, DPRES0, REF_rhot = make_inputs(args.scale)
+    g = c.g
+    N3 = int(np.prod(g.shape))
+    cells = g.cells
+    hevi.setup(g.index_dict(), c.scheme, c.scheme_tracer, device=local)
+
+    # device-resident state and inputs (Fortran layout, one flat buffer each)
+    st = torch.empty((5, N3), dtype=torch.float64, device="cuda")
+    for v, n in enumerate(("DENS", "MOMZ", "MOMX", "MOMY", "RHOT")):
+        st[v].copy_(to_dev(c.state[n], torch))
+    X = dict(DENS=st[0], MOMZ=st[1], MOMX=st[2], MOMY=st[3], RHOT=st[4])
+    z = lambda k=1: torch.zeros(k * N3, dtype=torch.float64, device="cuda")  # noqa: E731
+    mflx, tflx, nd = z(3), z(3), z(15)
+    tend = {n: z() for n in ("DENS_t", "MOMZ_t", "MOMX_t", "MOMY_t", "RHOT_t")}
+    ref = {n: to_dev(v, torch) for n, v in c.ref.items()}
+    dp0, rt2p, refr = to_dev(DPRES0, torch), to_dev(RT2P, torch), to_dev(REF_rhot, torch)
+    GS = torch.ones(7 * N3, dtype=torch.float64, device="cuda")
+    J0 = torch.zeros(7 * N3, dtype=torch.float64, device="cuda")
+    MAPF = torch.ones(g.IA * g.JA * 8, dtype=torch.float64, device="cuda")
+    cor = torch.zeros(g.IA * g.JA, dtype=torch.float64, device="cuda")
+    wd = np.zeros(g.KA)
+    grid = dict(CDZ=g.CDZ, FDZ=g.FDZ, FDX=g.FDX, FDY=g.FDY, RCDZ=g.RCDZ, RCDX=g.RCDX, RCDY=g.RCDY, RFDZ=g.RFDZ,
+                RFDX=g.RFDX, RFDY=g.RFDY)
+    dts = c.dt
+
+    def step():
+        # numerical filter (tstep_large:847-858) on the state at the start of the short step
+        hevi.ATMOS_DYN_numfilter_coef_dev(num_diff=nd, CDZ=g.CDZ, CDX=g.CDX, CDY=g.CDY, FDZ=g.FDZ, FDX=g.FDX,
+                                          FDY=g.FDY, DT=dts, REF_dens=ref["REF_dens"], REF_pott=ref["REF_pott"],
+                                          ND_COEF=c.nd_coef, ND_ORDER=1, ND_SFC_FACT=1.0, ND_USE_RS=True, **X)
+        # RK4 short step (tstep_large:880-894)
+        hevi.ATMOS_DYN_Tinteg_short_rk4_dev(
+            PROG=None, mflx_hi=mflx, tflx_hi=tflx, DPRES0=dp0, RT2P=rt2p, CORIOLI=cor, num_diff=nd, wdamp_coef=wd,
+            divdmp_coef=0.0, DDIV=None, FLAG_FCT_MOMENTUM=False, FLAG_FCT_T=False, FLAG_FCT_ALONG_STREAM=True,
+            PHI=ref["PHI"], GSQRT=GS, J13G=J0, J23G=J0, J33G=1.0, MAPF=MAPF, REF_dens=ref["REF_dens"],
+            REF_rhot=refr, BND_W=False, BND_E=False, BND_S=False, BND_N=False, dt=dts, **X, **tend, **grid)
+        # vertical boundary values + halo exchange of the state (tstep_large:910-944)
+        hevi.boundary_dev(**X)
+
+    stream = torch.cuda.ExternalStream(hevi.stream_handle())
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        # warm-up (also keeps the GPU loaded while the clock sampler starts)
+        for _ in range(args.warmup):
+            step()
+        hevi.check()
+        m0 = hevi.domain_sum_dev(X["DENS"], g.CDZ, g.CDX, g.CDY)
+
+        # ---- timed region ----
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        hevi.profile(True)
+        launches0 = hevi.kernel_launches()
+        w0 = time.time()
+        t0.record(stream)
+        for _ in range(args.steps):
+            step()
+        t1.record(stream)
+        torch.cuda.synchronize()
+        clk.mark(w0, time.time())
+    launches = hevi.kernel_launches() - launches0
+    prof = hevi.profile_report()
+    hevi.profile(False)
+    elapsed_ms = t0.elapsed_time(t1)
+    if dist:
+        tt = torch.tensor([elapsed_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        elapsed_ms = float(tt.item())
+    hevi.check()
+    m1 = hevi.domain_sum_dev(X["DENS"], g.CDZ, g.CDX, g.CDY)
+    clocks = clk.summary()
+    ms_step = elapsed_ms / args.steps
+    value = world * cells * args.steps / (elapsed_ms * 1e-3)
+
+    # ---- roofline of the HEVI stage (k_hevi_horiz + k_hevi_column) ----
+    peaks = {}
+    pk = ROOT / "MEASURED_PEAKS.json"
+    if pk.exists():
+        peaks = json.loads(pk.read_text())
+    hbm = float(peaks.get("hbm_gbs", 6650.0))
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    nst = prof.get("hevi_horiz", (0, 0.0))[0]
+    stage_ms = (prof.get("hevi_horiz", (0, 0.0))[1] + prof.get("hevi_column", (0, 0.0))[1]) / max(nst, 1)
+    achieved = STAGE_BYTES * cells / (stage_ms * 1e-3) / 1e9 if stage_ms > 0 else None
+    traffic = read_traffic()
+    roofline = {"bound": "hbm", "kernel": "hevi_stage (k_hevi_horiz + k_hevi_column), one HEVI stage",
+                "achieved": achieved, "peak": hbm, "peak_source": peak_src, "unit": "GB/s",
+                "frac": (achieved / hbm) if achieved else None, "algorithmic_bytes_per_launch": STAGE_BYTES * cells,
+                "stage_ms": stage_ms, "traffic": traffic,
+                "step_frac": STEP_BYTES * cells / (ms_step * 1e-3) / 1e9 / hbm}
+
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded; no dataset involved)",
+        "config": {"workload": f"{g.IMAX}x{g.JMAX}x{g.KMAX} stretched dz 50-400 m, dx=250 m, CD4, dt=0.5 s, "
+                               "short step = numfilter + RK4 (4 HEVI stages) + boundary/halo",
+                   "cells": cells, "scheme": c.scheme, "integrator": "RK4", "precision": "fp64 (plain)",
+                   "l2": f"inputs larger than L2 ({N3 * 8 / 2**20:.0f} MiB per field > {L2_BYTES / 2**20:.0f} MiB)",
+                   "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
+        "roofline": roofline,
+        "sections_ms_per_step": {k: v[1] / args.steps for k, v in prof.items()},
+        "mass_drift_rel": abs(m1 - m0) / m0,
+        "gpu_launches": launches,
+        "clocks": clocks,
+    }
+
+    if rank == 0 and not args.no_e2e:
+        out["e2e"] = run_e2e(args, c, hevi, torch)
+    if rank == 0 and not args.no_cpu_baseline:
+        out["cpu_baseline"] = cpu_baseline(args)
+    hevi.finalize()
+    if dist:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+
+
+def read_traffic():
+    """DRAM bytes per HEVI stage from the committed ncu summary, if present."""
+    p = ROOT / "profiles" / "hevi_stage_512x512x128.md"
+    if not p.exists():
+        return None
+    for line in p.read_text().splitlines():
+        if line.startswith("traffic_bytes_per_stage_full_size:"):
+            try:
+                return float(line.split(":", 1)[1].split()[0])
+            except ValueError:
+                return None
+    return None
+
+
+def run_e2e(args, c, hevi, torch):
+    """Large steps through the host-array plugin entry (ATMOS_DYN_Tstep_large_fvm_heve),
+    pinned host buffers, copies inside the timed region."""
+    from scale_b200 import mkinit
+
+    g = c.g
+
+    def pinned(a):
+        t = torch.empty(a.size, dtype=torch.float64, pin_memory=True)
+        v = t.numpy()
+        v[:] = np.ravel(a, order="K")
+        return t, v.reshape(a.shape, order="F")
+
+    keep = []
+
+    def P(a):
+        t, v = pinned(a)
+        keep.append(t)
+        return v
+
+    st = {n: P(c.state[n]) for n in ("DENS", "MOMZ", "MOMX", "MOMY", "RHOT")}
+    q = P(c.state["QTRC"])
+    tp = {n: P(g.zeros()) for n in ("DENS_tp", "MOMZ_tp", "MOMX_tp", "MOMY_tp", "RHOT_tp")}
+    rq = P(g.zeros(c.QA))
+    mf, tf, nd = P(g.zeros(3)), P(g.zeros(3)), P(g.zeros(5, 3))
+    ref = {n: P(v) for n, v in c.ref.items()}
+    cor = P(np.zeros((g.IA, g.JA), order="F"))
+    GS = np.ones(g.shape + (7,), order="F")
+    J0 = np.zeros(g.shape + (7,), order="F")
+    MAPF = np.ones((g.IA, g.JA, 2, 4), order="F")
+    R, CV, CP, M = mkinit.aq_props(c.QA)
+    nstep = int(np.ceil((c.dtl - mkinit.EPS) / c.dt))
+
+    def call():
+        hevi.ATMOS_DYN_Tstep_large_fvm_heve(
+            QTRC=q, QA=c.QA, mflx_hi=mf, tflx_hi=tf, num_diff=nd, RHOQ_tp=rq, CORIOLI=cor, CDZ=g.CDZ, CDX=g.CDX,
+            CDY=g.CDY, FDZ=g.FDZ, FDX=g.FDX, FDY=g.FDY, RCDZ=g.RCDZ, RCDX=g.RCDX, RCDY=g.RCDY, RFDZ=g.RFDZ,
+            RFDX=g.RFDX, RFDY=g.RFDY, PHI=ref["PHI"], GSQRT=GS, J13G=J0, J23G=J0, J33G=1.0, MAPF=MAPF, AQ_R=R,
+            AQ_CV=CV, AQ_CP=CP, AQ_MASS=M, REF_dens=ref["REF_dens"], REF_pott=ref["REF_pott"],
+            REF_pres=ref["REF_pres"], ND_COEF=c.nd_coef, ND_ORDER=1, ND_SFC_FACT=1.0, ND_USE_RS=True,
+            wdamp_coef=np.zeros(g.KA), divdmp_coef=0.0, FLAG_FCT_TRACER=c.fct, FLAG_FCT_ALONG_STREAM=True,
+            DTLS=c.dtl, DTSS=c.dt, **st, **tp)
+
+    call()  # warm-up (first call also checks the metric arrays once)
+    stream = torch.cuda.ExternalStream(hevi.stream_handle())
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ncall = args.e2e_calls
+    torch.cuda.synchronize()
+    b0 = hevi.transfer_bytes()
+    e0.record(stream)
+    for _ in range(ncall):
+        call()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    b1 = hevi.transfer_bytes()
+    ms = e0.elapsed_time(e1) / ncall
+    h2d = (b1[0] - b0[0]) // ncall
+    d2h = (b1[1] - b0[1]) // ncall
+    return {"value": g.cells * nstep / (ms * 1e-3), "unit": UNIT, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+            "ms_per_step": ms, "step": f"one large step through the host-array entry ATMOS_DYN_Tstep_large_fvm_heve_b200 "
+                                      f"({nstep} short steps + RK3 advection of {c.QA} tracers with FCT), pinned host buffers",
+            "calls": ncall}
+
+
+# ---------------------------------------------------------------------------
+# CPU timings of the oracle (restatement of the reference's FP64 CPU code)
+# ---------------------------------------------------------------------------
+def oracle_short_step_rate(scale: float, steps: int, min_seconds: float = 0.0, max_steps: int = 100):
+    import oracle
+    from scale_b200 import mkinit
+
+    c, RT2P, DPRES0, REF_rhot = make_inputs(scale)
+    g = c.g
+    GS, J13, J23, MAPF = oracle.flat_metrics(g)
+    nd = g.zeros(5, 3)
+    x = {n: c.state[n] for n in ("DENS", "MOMZ", "MOMX", "MOMY", "RHOT")}
+    x["mflx_hi"], x["tflx_hi"] = g.zeros(3), g.zeros(3)
+    a = dict(DENS_t=g.zeros(), MOMZ_t=g.zeros(), MOMX_t=g.zeros(), MOMY_t=g.zeros(), RHOT_t=g.zeros(),
+             DPRES0=DPRES0, RT2P=RT2P, CORIOLI=np.zeros((g.IA, g.JA), order="F"), num_diff=nd,
+             wdamp_coef=np.zeros(g.KA), divdmp_coef=0.0, DDIV=g.zeros(), CDZ=g.CDZ, FDZ=g.FDZ, FDX=g.FDX, FDY=g.FDY,
+             RCDZ=g.RCDZ, RCDX=g.RCDX, RCDY=g.RCDY, RFDZ=g.RFDZ, RFDX=g.RFDX, RFDY=g.RFDY, PHI=c.ref["PHI"],
+             GSQRT=GS, J13G=J13, J23G=J23, J33G=1.0, MAPF=MAPF, REF_dens=c.ref["REF_dens"], REF_rhot=REF_rhot,
+             dt=c.dt)
+    times = []
+    while len(times) < steps or (sum(times) < min_seconds and len(times) < max_steps):
+        t = time.perf_counter()
+        oracle.numfilter(g, nd, x, c.ref, DT=c.dt, ND_COEF=c.nd_coef)
+        oracle.tinteg_short_rk4(g, c.scheme, x, a)
+        for n in ("DENS", "MOMZ", "MOMX", "MOMY", "RHOT"):
+            oracle.halo(g, x[n])
+        times.append(time.perf_counter() - t)
+    return g, times, oracle.num_threads()
+
+
+def cpu_baseline(args):
+    g, times, threads = oracle_short_step_rate(args.cpu_scale, 2, min_seconds=args.cpu_seconds)
+    rate = g.cells / statistics.median(times)
+    return {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{len(times)} short steps (numfilter + RK4 + halo) of the same configuration on a "
+                      f"{g.IMAX}x{g.JMAX}x{g.KMAX} horizontal sub-domain, FP64 C restatement with OpenMP; "
+                      f"median {statistics.median(times):.2f} s per step"}
+
+
+def run_reference(args):
+    rank, world, _ = rank_info()
+    if rank != 0:
+        return
+    g, times, threads = oracle_short_step_rate(args.cpu_scale, args.steps + args.warmup)
+    t = times[args.warmup:] or times
+    rate = g.cells / statistics.median(t)
+    out = {"impl": "reference", "metric": METRIC, "value": rate, "unit": UNIT, "n_gpus": world, "steps": len(t),
+           "warmup": args.warmup, "ms_per_step": 1e3 * statistics.median(t), "higher_is_better": True,
+           "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded; no dataset involved)",
+           "config": {"workload": f"512x512x128 CD4 short step sampled on a {g.IMAX}x{g.JMAX}x{g.KMAX} sub-domain",
+                      "cells": g.cells},
+           "cpu_baseline": {"value": rate, "unit": UNIT, "cores": threads, "kind": "port",
+                            "sample": f"short steps on a {g.IMAX}x{g.JMAX}x{g.KMAX} sub-domain of the same "
+                                      "configuration: FP64 C restatement of the reference Fortran (no Fortran "
+                                      "compiler in the image), OpenMP over all host threads"},
+           "e2e": {"value": rate, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(out), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--scale", type=float, default=1.0, help="horizontal scale of the workload (1 = 512x512)")
+    ap.add_argument("--cpu-scale", type=float, default=0.25, help="horizontal scale of the CPU sample")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="minimum CPU work of the baseline sample")
+    ap.add_argument("--e2e-calls", type=int, default=2)
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "b200":
+        log("warm-up raised to the minimum of 3 steps")
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_b200(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -79,6 +79,10 @@ void *scale_hevi_stream(void);
 int scale_hevi_check(void);
 /* Number of this library's kernels launched since setup (for profiling). */
 long long scale_hevi_kernel_launches(void);
+/* Bytes copied host->device and device->host by the host-array entries since
+ * setup (the staging copies of inputs and results). No counterpart in the
+ * reference; used to report the transfer volume of an end-to-end call. */
+int scale_hevi_transfer_bytes(long long *h2d_bytes, long long *d2h_bytes);
 
 /* ---------------------------------------------------------------------------
  * One HEVI stage. Replaces ATMOS_DYN_Tstep_short_fvm_hevi
@@ -241,6 +245,25 @@ int ATMOS_DYN_Tstep_large_fvm_heve_b200(
     const double *wdamp_coef, const double *divdmp_coef,
     const int *FLAG_FCT_TRACER, const int *FLAG_FCT_ALONG_STREAM,
     const double *DTLS, const double *DTSS);
+
+/* ---------------------------------------------------------------------------
+ * Boundary values after a short step: the vertical boundary copy of
+ * scale_atmos_dyn_tstep_large_fvm_heve.F90:910-926 followed by the periodic
+ * halo exchange of the five prognostic fields (:929-944). Device arrays.
+ * ------------------------------------------------------------------------- */
+int scale_hevi_boundary_dev(double *DENS, double *MOMZ, double *MOMX, double *MOMY, double *RHOT);
+
+/* ---------------------------------------------------------------------------
+ * Section timers, the counterpart of PROF_rapstart/PROF_rapend
+ * (scalelib/src/common/scale_prof.F90:156,209): when enabled, CUDA events on
+ * the library stream bracket each kernel section (hevi_horiz, hevi_column,
+ * numfilter, halo, boundary, tracer, tracer_fct, large_prep, mflx_average).
+ * scale_hevi_profile(1) enables and resets, scale_hevi_profile(0) disables;
+ * the report is a JSON object {"section": [launches, total_ms], ...} and
+ * synchronises the stream.
+ * ------------------------------------------------------------------------- */
+int scale_hevi_profile(int enable);
+const char *scale_hevi_profile_report(void);
 
 /* ---------------------------------------------------------------------------
  * FP64 domain budget: total = sum over the interior of var*CDZ*CDX*CDY, the

@@ -70,7 +70,7 @@ def build_cuda(force: bool = False, verbose: bool = False) -> Path:
         if src.endswith(".cu") and verbose:
             cmd += ["-Xptxas", "-v"]
         if src.endswith(".cpp"):
-            cmd = [nvcc, *common, "-x", "c++", "-c", str(CSRC / src), "-o", str(obj)]
+            cmd = [nvcc, *common, *ARCH, "-x", "c++", "-c", str(CSRC / src), "-o", str(obj)]
         _run(cmd)
         objs.append(str(obj))
     tmp = LIB.with_suffix(".so.tmp")

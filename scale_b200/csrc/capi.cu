@@ -28,6 +28,7 @@ struct Ctx {
     int scheme = UD3, scheme_tracer = UD3;
     size_t N3 = 0;
     long long launches = 0;
+    long long h2d_bytes = 0, d2h_bytes = 0; // host<->device copies of the host-array entries
     // 1-D tables on the device: CDZ FDZ RCDZ RFDZ F2H1 F2H2 wdamp (KA each),
     // FDX RCDX RFDX CDX (IA), FDY RCDY RFDY CDY (JA)
     double *d_tab = nullptr;
@@ -52,6 +53,12 @@ struct Ctx {
     std::vector<std::vector<const void *>> flat_ok;
     // staging buffers of the host-array entries
     std::map<std::string, std::pair<double *, size_t>> stage;
+    // section timers (scale_hevi_profile): event pairs recorded around launches
+    bool prof_on = false;
+    std::vector<cudaEvent_t> ev_pool;
+    size_t ev_used = 0;
+    std::vector<std::pair<std::string, size_t>> prof_marks; // name, index of the start event
+    std::string prof_text;
 };
 
 Ctx C;
@@ -85,6 +92,26 @@ int need_setup()
     return SCALE_HEVI_OK;
 }
 
+// Record a CUDA event pair around the launches of one section (the library's
+// counterpart of PROF_rapstart/PROF_rapend, scalelib/src/common/scale_prof.F90:156,209).
+template <class F>
+int timed(const char *name, F &&launch)
+{
+    if (!C.prof_on) return launch();
+    while (C.ev_pool.size() < C.ev_used + 2) {
+        cudaEvent_t e;
+        if (cudaEventCreate(&e) != cudaSuccess) return fail(SCALE_HEVI_ERR_CUDA, "cudaEventCreate failed");
+        C.ev_pool.push_back(e);
+    }
+    const size_t i0 = C.ev_used;
+    C.ev_used += 2;
+    cudaEventRecord(C.ev_pool[i0], C.stream);
+    int rc = launch();
+    cudaEventRecord(C.ev_pool[i0 + 1], C.stream);
+    C.prof_marks.emplace_back(name, i0);
+    return rc;
+}
+
 int dalloc(double **p, size_t n)
 {
     if (cudaMalloc((void **)p, n * sizeof(double)) != cudaSuccess) {
@@ -102,6 +129,7 @@ void free_all()
     for (auto &kv : C.stage) cudaFree(kv.second.first);
     if (C.status) cudaFree(C.status);
     if (C.count) cudaFree(C.count);
+    for (cudaEvent_t e : C.ev_pool) cudaEventDestroy(e);
     if (C.stream) cudaStreamDestroy(C.stream);
     C = Ctx();
 }
@@ -134,11 +162,13 @@ int h2d(const char *name, const double *h, size_t n, double **d)
 {
     CK(stage_buf(name, n, d));
     CU(cudaMemcpyAsync(*d, h, n * sizeof(double), cudaMemcpyHostToDevice, C.stream));
+    C.h2d_bytes += (long long)(n * sizeof(double));
     return SCALE_HEVI_OK;
 }
 int d2h(double *h, const double *d, size_t n)
 {
     CU(cudaMemcpyAsync(h, d, n * sizeof(double), cudaMemcpyDeviceToHost, C.stream));
+    C.d2h_bytes += (long long)(n * sizeof(double));
     return SCALE_HEVI_OK;
 }
 
@@ -217,8 +247,6 @@ int prepare_tables(const double *CDZ, const double *FDZ, const double *RCDZ, con
     C.g.FDY = dy; C.g.RCDY = dy + JA; C.g.RFDY = dy + 2 * JA;
     return SCALE_HEVI_OK;
 }
-const double *dev_CDX() { return C.d_tab + 7 * (size_t)C.g.KA + 3 * (size_t)C.g.IA; }
-const double *dev_CDY() { return C.d_tab + 7 * (size_t)C.g.KA + 4 * (size_t)C.g.IA + 3 * (size_t)C.g.JA; }
 
 int prepare_nd(const double *CDZ, const double *CDX, const double *CDY, const double *FDZ, const double *FDX,
                const double *FDY, double DT, double ND_COEF, int ND_ORDER, double SFC)
@@ -255,10 +283,13 @@ int prepare_nd(const double *CDZ, const double *CDX, const double *CDY, const do
     return SCALE_HEVI_OK;
 }
 
-void halo(double *const *f, int n)
+int halo(double *const *f, int n)
 {
-    periodic_halo(C.g, f, n, C.stream);
     C.launches += (n + 15) / 16;
+    return timed("halo", [&] {
+        periodic_halo(C.g, f, n, C.stream);
+        return SCALE_HEVI_OK;
+    });
 }
 
 // ---- one stage ---------------------------------------------------------------
@@ -272,6 +303,7 @@ struct StageIn {
 
 int run_stage(const StageIn &in, double *const out[5], double *mflx, double *tflx, double dtrk, int mode)
 {
+    if (in.divdmp != 0.0 && !in.DDIV) return fail(SCALE_HEVI_ERR_ARG, "divdmp_coef is nonzero but DDIV is NULL");
     StageArgs a{};
     a.DENS_RK = out[0]; a.MOMZ_RK = out[1]; a.MOMX_RK = out[2]; a.MOMY_RK = out[3]; a.RHOT_RK = out[4];
     a.mflx = mflx; a.tflx = tflx;
@@ -283,7 +315,14 @@ int run_stage(const StageIn &in, double *const out[5], double *mflx, double *tfl
     a.divdmp_coef = in.divdmp; a.J33G = in.J33G; a.dtrk = dtrk;
     a.adv_r = C.adv; a.adv_w = C.adv + C.N3; a.adv_t = C.adv + 2 * C.N3;
     a.rk_mode = mode; a.acc = C.acc; a.facc = C.facc; a.status = C.status;
-    CU(launch_hevi_stage(C.g, a, C.scheme, C.stream));
+    CK(timed("hevi_horiz", [&] {
+        CU(launch_hevi_horiz(C.g, a, C.scheme, C.stream));
+        return SCALE_HEVI_OK;
+    }));
+    CK(timed("hevi_column", [&] {
+        CU(launch_hevi_column(C.g, a, C.scheme, C.stream));
+        return SCALE_HEVI_OK;
+    }));
     C.launches += 2;
     return SCALE_HEVI_OK;
 }
@@ -308,7 +347,7 @@ int run_rk4(double *X[5], double *mflx, double *tflx, const StageIn &base, doubl
         }
         CK(run_stage(in, out, mflx, tflx, dts[s], RK_STAGE1 + s));
         if (s < 3) {
-            halo(out, 5); // COMM_vars8 of the stage buffers (rk4.F90:401-425)
+            CK(halo(out, 5)); // COMM_vars8 of the stage buffers (rk4.F90:401-425)
             for (int v = 0; v < 5; ++v) src[v] = out[v];
         }
     }
@@ -319,12 +358,14 @@ int run_numfilter(double *num_diff, const double *DENS, const double *MOMZ, cons
                   const double *RHOT, const double *REF_dens, const double *REF_pott)
 {
     NdArgs a{num_diff, DENS, MOMZ, MOMX, MOMY, RHOT, REF_dens, REF_pott};
-    CU(launch_numfilter(C.g, C.ndc, a, C.stream));
+    CK(timed("numfilter", [&] {
+        CU(launch_numfilter(C.g, C.ndc, a, C.stream));
+        return SCALE_HEVI_OK;
+    }));
     ++C.launches;
     double *f[15];
     for (int q = 0; q < 15; ++q) f[q] = num_diff + (size_t)q * C.N3;
-    halo(f, 15);
-    return SCALE_HEVI_OK;
+    return halo(f, 15);
 }
 
 // RK3 tracer integrator (tinteg_tracer_rk3.F90:92-210) on device arrays
@@ -338,17 +379,17 @@ int run_tracer_rk3(double *QTRC, const double *QTRC0, const double *RHOQ_t, cons
     double *rk1 = C.tr, *rk2 = C.tr + C.N3;
     // stage 1: dt/3 with DENS0 + (DENS-DENS0)/3
     a.QTRCo = rk1; a.QTRC = QTRC; a.dens_mode = 1; a.dtl = dtl / 3.0;
-    CU(launch_tracer_stage(C.g, a, C.scheme_tracer, false, C.stream));
+    CK(timed("tracer", [&] { CU(launch_tracer_stage(C.g, a, C.scheme_tracer, false, C.stream)); return SCALE_HEVI_OK; }));
     ++C.launches;
-    halo(&rk1, 1);
+    CK(halo(&rk1, 1));
     // stage 2: dt/2 with DENS0 + (DENS-DENS0)*0.5
     a.QTRCo = rk2; a.QTRC = rk1; a.dens_mode = 2; a.dtl = dtl / 2.0;
-    CU(launch_tracer_stage(C.g, a, C.scheme_tracer, false, C.stream));
+    CK(timed("tracer", [&] { CU(launch_tracer_stage(C.g, a, C.scheme_tracer, false, C.stream)); return SCALE_HEVI_OK; }));
     ++C.launches;
-    halo(&rk2, 1);
+    CK(halo(&rk2, 1));
     // stage 3: dt with DENS, FCT when requested
     a.QTRCo = QTRC; a.QTRC = rk2; a.dens_mode = 0; a.dtl = dtl;
-    CU(launch_tracer_stage(C.g, a, C.scheme_tracer, fct, C.stream));
+    CK(timed(fct ? "tracer_fct" : "tracer", [&] { CU(launch_tracer_stage(C.g, a, C.scheme_tracer, fct, C.stream)); return SCALE_HEVI_OK; }));
     C.launches += fct ? 4 : 1;
     return SCALE_HEVI_OK;
 }
@@ -429,6 +470,13 @@ int scale_hevi_finalize(void)
 const char *scale_hevi_last_error(void) { return g_err.c_str(); }
 void *scale_hevi_stream(void) { return (void *)C.stream; }
 long long scale_hevi_kernel_launches(void) { return C.launches; }
+
+int scale_hevi_transfer_bytes(long long *h2d_bytes, long long *d2h_bytes)
+{
+    if (h2d_bytes) *h2d_bytes = C.h2d_bytes;
+    if (d2h_bytes) *d2h_bytes = C.d2h_bytes;
+    return SCALE_HEVI_OK;
+}
 
 int scale_hevi_check(void)
 {
@@ -686,8 +734,7 @@ int COMM_vars8_b200_dev(double *var, const int *nfields)
     if (!var || !nfields || *nfields < 1) return fail(SCALE_HEVI_ERR_ARG, "COMM_vars8: bad field list");
     std::vector<double *> f(*nfields);
     for (int q = 0; q < *nfields; ++q) f[q] = var + (size_t)q * C.N3;
-    halo(f.data(), *nfields);
-    return SCALE_HEVI_OK;
+    return halo(f.data(), *nfields);
 }
 
 // ---- large step ----------------------------------------------------------------
@@ -732,7 +779,7 @@ int ATMOS_DYN_Tstep_large_fvm_heve_b200_dev(SCALE_HEVI_LARGE_ARGS)
     pa.RT2P = RT2P; pa.DPRES0 = DPRES0; pa.REF_rhot = REF_rhot; pa.RHOT = RHOT; pa.QTRC = QTRC; pa.REF_pres = REF_pres;
     pa.QA = qa;
     for (int q = 0; q < qa; ++q) { pa.AQ_R[q] = AQ_R[q]; pa.AQ_CV[q] = AQ_CV[q]; pa.AQ_CP[q] = AQ_CP[q]; pa.AQ_MASS[q] = AQ_MASS[q]; }
-    large_prep(C.g, pa, C.stream);
+    CK(timed("large_prep", [&] { large_prep(C.g, pa, C.stream); return SCALE_HEVI_OK; }));
     C.launches += 2;
     CK(prepare_tables(CDZ, FDZ, RCDZ, RFDZ, FDX, RCDX, RFDX, FDY, RCDY, RFDY, wdamp_coef, CDX, CDY));
     if (*ND_COEF != 0.0) CK(prepare_nd(CDZ, CDX, CDY, FDZ, FDX, FDY, dts, *ND_COEF, *ND_ORDER, *ND_SFC_FACT));
@@ -747,22 +794,22 @@ int ATMOS_DYN_Tstep_large_fvm_heve_b200_dev(SCALE_HEVI_LARGE_ARGS)
         if (*ND_COEF == 0.0) CU(cudaMemsetAsync(num_diff, 0, 15 * N3 * sizeof(double), C.stream));
         else CK(run_numfilter(num_diff, DENS, MOMZ, MOMX, MOMY, RHOT, REF_dens, REF_pott));
         CK(run_rk4(X, mflx_hi, tflx_hi, base, dts));
-        vertical_bc(C.g, DENS, MOMZ, MOMX, MOMY, RHOT, C.stream);
+        CK(timed("boundary", [&] { vertical_bc(C.g, DENS, MOMZ, MOMX, MOMY, RHOT, C.stream); return SCALE_HEVI_OK; }));
         ++C.launches;
-        halo(X, 5);
-        mflx_accumulate(C.g, mflx_av, mflx_hi, C.stream);
+        CK(halo(X, 5));
+        CK(timed("mflx_average", [&] { mflx_accumulate(C.g, mflx_av, mflx_hi, C.stream); return SCALE_HEVI_OK; }));
         ++C.launches;
     }
     if (qa > 0) {
         mflx_average(C.g, mflx_hi, mflx_av, nstep, C.stream);
         ++C.launches;
         double *mf[3] = {mflx_hi, mflx_hi + N3, mflx_hi + 2 * N3};
-        halo(mf, 3);
+        CK(halo(mf, 3));
         for (int q = 0; q < qa; ++q) {
             double *qt = QTRC + (size_t)q * N3;
             CK(run_tracer_rk3(qt, qt, RHOQ_tp + (size_t)q * N3, DENS00, DENS, mflx_hi, nullptr, dtl,
                               *FLAG_FCT_TRACER != 0, *FLAG_FCT_ALONG_STREAM != 0));
-            halo(&qt, 1);
+            CK(halo(&qt, 1));
         }
     }
     return SCALE_HEVI_OK;
@@ -806,6 +853,49 @@ int ATMOS_DYN_Tstep_large_fvm_heve_b200(SCALE_HEVI_LARGE_ARGS)
     CK(d2h(num_diff, nd, 15 * N3));
     CU(cudaStreamSynchronize(C.stream));
     return scale_hevi_check();
+}
+
+int scale_hevi_boundary_dev(double *DENS, double *MOMZ, double *MOMX, double *MOMY, double *RHOT)
+{
+    CK(need_setup());
+    CK(timed("boundary", [&] { vertical_bc(C.g, DENS, MOMZ, MOMX, MOMY, RHOT, C.stream); return SCALE_HEVI_OK; }));
+    ++C.launches;
+    double *X[5] = {DENS, MOMZ, MOMX, MOMY, RHOT};
+    return halo(X, 5);
+}
+
+int scale_hevi_profile(int enable)
+{
+    CK(need_setup());
+    CU(cudaStreamSynchronize(C.stream));
+    C.prof_on = enable != 0;
+    C.ev_used = 0;
+    C.prof_marks.clear();
+    return SCALE_HEVI_OK;
+}
+
+const char *scale_hevi_profile_report(void)
+{
+    C.prof_text = "{";
+    if (C.ready && cudaStreamSynchronize(C.stream) == cudaSuccess) {
+        std::map<std::string, std::pair<long, double>> acc;
+        for (auto &m : C.prof_marks) {
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, C.ev_pool[m.second], C.ev_pool[m.second + 1]);
+            auto &a = acc[m.first];
+            a.first += 1;
+            a.second += ms;
+        }
+        bool first = true;
+        for (auto &kv : acc) {
+            char buf[256];
+            snprintf(buf, sizeof buf, "%s\"%s\": [%ld, %.6f]", first ? "" : ", ", kv.first.c_str(), kv.second.first, kv.second.second);
+            C.prof_text += buf;
+            first = false;
+        }
+    }
+    C.prof_text += "}";
+    return C.prof_text.c_str();
 }
 
 int scale_hevi_domain_sum_dev(const double *var, const double *CDZ, const double *CDX, const double *CDY, double *total)

@@ -416,20 +416,22 @@ __global__ void __launch_bounds__(128) k_hevi_column(const Grid g, const StageAr
 }
 
 // ---- host launchers ---------------------------------------------------------
-cudaError_t launch_hevi_stage(const Grid &g, const StageArgs &a, int scheme, cudaStream_t st)
+cudaError_t launch_hevi_horiz(const Grid &g, const StageArgs &a, int scheme, cudaStream_t st)
 {
-    if (g.KA > MAXKA) return cudaErrorInvalidValue;
     dim3 bh(32, 4);
     dim3 gh((g.IMAX + 3) / 4, g.JMAX);
+    if (scheme == UD3) k_hevi_horiz<UD3><<<gh, bh, 0, st>>>(g, a);
+    else k_hevi_horiz<CD4><<<gh, bh, 0, st>>>(g, a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_hevi_column(const Grid &g, const StageArgs &a, int scheme, cudaStream_t st)
+{
+    if (g.KA > MAXKA) return cudaErrorInvalidValue;
     dim3 bc(128);
     dim3 gc((g.IMAX + 1 + 127) / 128, g.JMAX);
-    if (scheme == UD3) {
-        k_hevi_horiz<UD3><<<gh, bh, 0, st>>>(g, a);
-        k_hevi_column<UD3><<<gc, bc, 0, st>>>(g, a);
-    } else {
-        k_hevi_horiz<CD4><<<gh, bh, 0, st>>>(g, a);
-        k_hevi_column<CD4><<<gc, bc, 0, st>>>(g, a);
-    }
+    if (scheme == UD3) k_hevi_column<UD3><<<gc, bc, 0, st>>>(g, a);
+    else k_hevi_column<CD4><<<gc, bc, 0, st>>>(g, a);
     return cudaGetLastError();
 }
 

@@ -80,7 +80,7 @@ def load(path: str | os.PathLike | None = None) -> C.CDLL:
     _sig = header_functions()
     for name, params in _sig.items():
         f = getattr(lib, name)
-        if name == "scale_hevi_last_error":
+        if name in ("scale_hevi_last_error", "scale_hevi_profile_report"):
             f.restype = C.c_char_p
         elif name == "scale_hevi_stream":
             f.restype = C.c_void_p
@@ -90,6 +90,8 @@ def load(path: str | os.PathLike | None = None) -> C.CDLL:
             f.restype = C.c_int
         if name == "scale_hevi_setup":
             f.argtypes = [C.POINTER(Index), C.c_char_p, C.c_char_p, C.c_int]
+        elif name == "scale_hevi_profile":
+            f.argtypes = [C.c_int]
         else:
             f.argtypes = [C.c_void_p] * len(params)
     _lib = lib
@@ -163,6 +165,30 @@ def check() -> None:
 
 def kernel_launches() -> int:
     return int(load().scale_hevi_kernel_launches())
+
+
+def transfer_bytes() -> tuple[int, int]:
+    """(host->device, device->host) bytes staged by the host-array entries since setup."""
+    h, d = C.c_longlong(0), C.c_longlong(0)
+    _check(load().scale_hevi_transfer_bytes(C.byref(h), C.byref(d)))
+    return int(h.value), int(d.value)
+
+
+def profile(enable: bool) -> None:
+    """Enable (and reset) or disable the per-section CUDA-event timers."""
+    _check(load().scale_hevi_profile(1 if enable else 0))
+
+
+def profile_report() -> dict:
+    """{section: (launches, total_ms)} since the last profile(True)."""
+    import json
+
+    return {k: (int(v[0]), float(v[1])) for k, v in json.loads(load().scale_hevi_profile_report().decode()).items()}
+
+
+def boundary_dev(DENS, MOMZ, MOMX, MOMY, RHOT) -> None:
+    """Vertical boundary values and periodic halo of the five prognostic fields."""
+    call("scale_hevi_boundary_dev", DENS=DENS, MOMZ=MOMZ, MOMX=MOMX, MOMY=MOMY, RHOT=RHOT)
 
 
 def stream_handle() -> int:
