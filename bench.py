@@ -52,6 +52,23 @@ def log(*a):
     print(*a, file=sys.stderr, flush=True)
 
 
+def max_over_ranks(value: float, dist, device) -> float:
+    """The slowest rank's time (every rank takes part; returns the local value
+    without a process group)."""
+    if dist is None:
+        return float(value)
+    import torch
+
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def aggregate_rate(units_per_rank: int, world: int, steps: int, elapsed_ms: float) -> float:
+    """Whole-job throughput: the units all ranks processed over the slowest rank's time."""
+    return world * units_per_rank * steps / (elapsed_ms * 1e-3)
+
+
 # ---------------------------------------------------------------------------
 # clocks during the timed region
 # ---------------------------------------------------------------------------
@@ -211,16 +228,12 @@ def run_b200(args):
     launches = hevi.kernel_launches() - launches0
     prof = hevi.profile_report()
     hevi.profile(False)
-    elapsed_ms = t0.elapsed_time(t1)
-    if dist:
-        tt = torch.tensor([elapsed_ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        elapsed_ms = float(tt.item())
+    elapsed_ms = max_over_ranks(t0.elapsed_time(t1), dist, "cuda")
     hevi.check()
     m1 = hevi.domain_sum_dev(X["DENS"], g.CDZ, g.CDX, g.CDY)
     clocks = clk.summary()
     ms_step = elapsed_ms / args.steps
-    value = world * cells * args.steps / (elapsed_ms * 1e-3)
+    value = aggregate_rate(cells, world, args.steps, elapsed_ms)
 
     # ---- roofline of the HEVI stage (k_hevi_horiz + k_hevi_column) ----
     peaks = {}
