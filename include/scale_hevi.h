@@ -273,6 +273,32 @@ const char *scale_hevi_profile_report(void);
  * ------------------------------------------------------------------------- */
 int scale_hevi_domain_sum_dev(const double *var, const double *CDZ, const double *CDX, const double *CDY, double *total);
 
+/* ---------------------------------------------------------------------------
+ * One HEVI stage that allocates no device memory. This entry has no
+ * counterpart in the reference. It exists for callers that cannot let a
+ * library allocate GPU memory: a host model that owns the whole device budget
+ * and hands out pieces of it, where a library cudaMalloc in the middle of a
+ * run could fail or break its accounting, or a caller that cannot call
+ * scale_hevi_setup.
+ *
+ * Arguments: the index set and flux scheme that scale_hevi_setup would take,
+ * the cudaStream_t to run on (as void*), then the argument list of
+ * ATMOS_DYN_Tstep_short_fvm_hevi_b200_dev (device pointers for the 2-D/3-D
+ * arrays, host pointers for the 1-D vectors and scalars). It computes what
+ * that entry computes.
+ *
+ * Scratch: one fixed device array of SCALE_HEVI_NOALLOC_SCRATCH_BYTES inside
+ * the library. A domain must need no more than that:
+ * 256 + 8*(3*KA*IA*JA + 7*KA + 4*IA + 4*JA) bytes. A larger domain is rejected
+ * with SCALE_HEVI_ERR_ARG. The first call on a device looks up the array with
+ * that device current. Make that first call before any stream capture. All
+ * calls on a device share the array, so calls that overlap in time race. The
+ * entry synchronises the stream before it returns.
+ * ------------------------------------------------------------------------- */
+#define SCALE_HEVI_NOALLOC_SCRATCH_BYTES (32UL * 1024UL * 1024UL)
+int ATMOS_DYN_Tstep_short_fvm_hevi_b200_noalloc(const scale_hevi_index *idx, const char *flux_type, void *stream,
+                                                SCALE_HEVI_TSTEP_SHORT_ARGS);
+
 #ifdef __cplusplus
 }
 #endif

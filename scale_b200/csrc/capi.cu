@@ -398,6 +398,8 @@ size_t n3() { return C.N3; }
 
 }  // namespace
 
+void hevi::set_last_error(const char *msg) { g_err = msg ? msg : ""; }
+
 // =============================================================================
 // exported entry points
 // =============================================================================

@@ -54,4 +54,7 @@ void domain_sum(const Grid &g, const double *var, const double *CDX, const doubl
 void mflx_accumulate(const Grid &g, double *av, const double *mflx, cudaStream_t st);
 void mflx_average(const Grid &g, double *mflx, const double *av, int nstep, cudaStream_t st);
 
+// message returned by scale_hevi_last_error() (capi.cu)
+void set_last_error(const char *msg);
+
 }  // namespace hevi

@@ -133,6 +133,8 @@ class _Args:
 
 INT_ARGS = {"FLAG_FCT_MOMENTUM", "FLAG_FCT_T", "FLAG_FCT_ALONG_STREAM", "FLAG_FCT_TRACER", "BND_W", "BND_E",
             "BND_S", "BND_N", "last", "ND_ORDER", "ND_USE_RS", "QA", "nfields"}
+# arguments passed as they are (an address, a C string or a stream handle), not by reference
+RAW_ARGS = {"idx", "flux_type", "stream"}
 
 
 def call(name: str, **kw) -> None:
@@ -143,7 +145,7 @@ def call(name: str, **kw) -> None:
     if unknown:
         raise TypeError(f"{name}: unknown arguments {sorted(unknown)}")
     a = _Args()
-    args = [a.ptr(kw.get(p), p in INT_ARGS) for p in params]
+    args = [kw.get(p) if p in RAW_ARGS else a.ptr(kw.get(p), p in INT_ARGS) for p in params]
     _check(getattr(lib, name)(*args))
 
 
@@ -243,6 +245,14 @@ def ATMOS_DYN_Tinteg_tracer_rk3_dev(**kw):
 
 def ATMOS_DYN_Tstep_large_fvm_heve_dev(**kw):
     call("ATMOS_DYN_Tstep_large_fvm_heve_b200_dev", **kw)
+
+
+def ATMOS_DYN_Tstep_short_fvm_hevi_noalloc(index: dict, flux_type: str, stream: int, **kw):
+    """One HEVI stage that allocates no device memory (no scale_hevi_setup needed);
+    device arrays as in ATMOS_DYN_Tstep_short_fvm_hevi_dev, stream a cudaStream_t handle."""
+    idx = Index(**index)
+    call("ATMOS_DYN_Tstep_short_fvm_hevi_b200_noalloc", idx=C.addressof(idx), flux_type=flux_type.encode(),
+         stream=int(stream), **kw)
 
 
 def COMM_vars8_dev(var, nfields: int):
