@@ -236,182 +236,213 @@ __global__ void __launch_bounds__(128) k_hevi_horiz(const Grid g, const StageArg
 // =============================================================================
 // column kernel: vertical fluxes, sources, implicit solve, back-update
 // =============================================================================
-constexpr int MAXKA = 260; // largest KA (KMAX + 4) the column kernel accepts
+//
+// One CTA owns a tile of TC consecutive columns (i .. i+TC-1 at one j), all
+// levels. A column is KA contiguous doubles, so the tile of each field is one
+// contiguous block and warp w reads column w with its lanes along k (256-byte
+// coalesced accesses). The work runs in four phases over per-level arrays in
+// shared memory (one array per quantity, [column][level], odd row pitch):
+//   1. POTT = RHOT/DENS                                                 (k-parallel)
+//   2. PT (theta at w-faces, valueW_Z), tZ (fluxZ_XYZ), Sr, St, A       (k-parallel)
+//   3. right-hand side C of the tridiagonal system (:698-722)            (k-parallel)
+//   4. Thomas solve, solve_direct :1092-1127                             (one thread per column)
+//   5. back-update of DENS, RHOT, MOMZ and the vertical fluxes (:728-790) (k-parallel)
+// The arithmetic of every value keeps the reference's operation order, so
+// the results are bit-identical to the sequential formulation.
+constexpr int MAXKA = 260;    // largest KA (KMAX + 4) the column kernel accepts
+constexpr int COL_ARRAYS = 6; // per-level shared arrays
+
+enum ColArr : int { CA_C = 0, CA_PT = 1, CA_A = 2, CA_SR = 3, CA_ST = 4, CA_TZ = 5 };
+// CA_C holds POTT in phases 1-2, then the RHS C, then f, then the solution.
+// CA_A holds A(k), then e(k) once level k is eliminated.
+
+__host__ __device__ inline int col_pitch(int KA) { return KA | 1; }
 
 template <int S>
-__global__ void __launch_bounds__(128) k_hevi_column(const Grid g, const StageArgs a)
+__global__ void __launch_bounds__(512, 2) k_hevi_column(const Grid g, const StageArgs a)
 {
-    const int i = g.IS - 1 + blockIdx.x * blockDim.x + threadIdx.x;
+    extern __shared__ double sm[];
+    const int TC = blockDim.y;
+    const int lane = threadIdx.x, w = threadIdx.y;
+    const int i0 = g.IS + blockIdx.x * TC;
     const int j = g.JS + blockIdx.y;
-    if (i > g.IE) return;
+    const int i = i0 + w;           // this warp's column in the k-parallel phases
+    const bool col_ok = i <= g.IE;
     const size_t N3 = n3(g);
     const int KS = g.KS, KE = g.KE;
-    const size_t col = idx3(g, 1, i, j); // offset of level 1
+    const int KP = col_pitch(g.KA);
+    const size_t col = idx3(g, 1, i, j); // offset of level 1 of this warp's column
     const double *ndDZ = nd_slice(a, N3, 1, 1), *ndWZ = nd_slice(a, N3, 2, 1), *ndTZ = nd_slice(a, N3, 5, 1);
-#define CL(p, k) ld((p) + col + (k) - 1)
-
-    if (i == g.IS - 1) {
-        // hevi_mflx_z :369-393 also fills the halo column i = IS-1 with the
-        // explicit part of the vertical mass flux; the solver never updates it
-        if (a.rk_mode == RK_PLAIN || a.rk_mode == RK_FINAL) {
-            a.mflx[col + KS - 2] = 0.0;
-            for (int k = KS; k <= KE - 1; ++k) a.mflx[col + k - 1] = CL(ndDZ, k);
-            a.mflx[col + KE - 1] = 0.0;
-        }
-        return;
-    }
-
     const double dt = a.dtrk, J33G = a.J33G, dt2 = dt * dt;
     const bool use_div = a.divdmp_coef != 0.0;
     const double ddc = use_div ? a.divdmp_coef / dt : 0.0;
+    // shared arrays: SA(arr, c, L) for column c of the tile, level L (1-based)
+#define SA(arr, c, L) sm[((size_t)(arr) * TC + (c)) * KP + (L) - 1]
+#define CL(p, L) ld((p) + col + (L) - 1)
 
-    // per-level values kept for the back substitution and the final update
-    double e_[MAXKA], f_[MAXKA], pt_[MAXKA], sr_[MAXKA], st_[MAXKA], tz_[MAXKA];
+    // ---- phase 1: POTT(L) = RHOT/DENS, :586-600 ----
+    if (col_ok)
+        for (int L = KS + lane; L <= KE; L += 32) SA(CA_C, w, L) = CL(a.RHOT, L) / CL(a.DENS, L);
+    __syncthreads();
 
-    // sliding windows (suffix = level offset from the current level L)
-    double Pm1 = 0.0, P0, P1, P2 = 0.0;           // POTT(L-1..L+2)
-    double Mm2 = 0.0, Mm1 = 0.0, M0, M1 = 0.0;    // MOMZ(L-2..L+1)
-    double Dm1 = 0.0, D0;                         // DENS(L-1), DENS(L)
-    double Pd1, Pd2 = 0.0;                        // DENS(L+1), DENS(L+2) for POTT
-    double mZm1 = 0.0, tZm1 = 0.0, qZm1 = 0.0;    // mZ(L-1), tZ(L-1), qZ(L-2)
-    double PTm1 = 0.0, PTm2 = 0.0;                // PT(L-1), PT(L-2)
-    double Am1 = 0.0, DPm1 = 0.0, RPm1 = 0.0, RDm1 = 0.0, Srm1 = 0.0, Stm1 = 0.0;
-    double e_prev = 0.0, f_prev = 0.0, Cfin = 0.0;
-
-    D0 = CL(a.DENS, KS);
-    P0 = CL(a.RHOT, KS) / D0;
-    Pd1 = CL(a.DENS, KS + 1);
-    P1 = CL(a.RHOT, KS + 1) / Pd1;
-    M0 = CL(a.MOMZ, KS);
-
-    for (int L = KS; L <= KE; ++L) {
-        // advance the look-ahead windows
-        if (L + 2 <= KE) { Pd2 = CL(a.DENS, L + 2); P2 = CL(a.RHOT, L + 2) / Pd2; }
-        if (L + 1 <= KE) M1 = CL(a.MOMZ, L + 1);
-
-        // ---- level-L quantities ----
-        const double mZ = (L <= KE - 1) ? CL(ndDZ, L) : 0.0; // hevi_mflx_z :383-391 (flat terrain)
-        double PT = 0.0, tZ = 0.0;
-        if (L <= KE - 1) {
-            // valueW_Z (ud3.F90:98-153) and fluxZ_XYZ (ud3.F90:157-247)
+    // ---- phase 2: PT, tZ, Sr, St, A ----
+    if (col_ok) {
+        // valueW_Z (ud3.F90:98-153) with the w-momentum sign, and fluxZ_XYZ (ud3.F90:157-247)
+        auto pt_tz = [&](int L, double &pt, double &tz) {
+            if (L < KS || L > KE - 1) { pt = 0.0; tz = 0.0; return; }
+            const double mZ = CL(ndDZ, L); // hevi_mflx_z :383-391 (flat terrain)
+            const double M0 = CL(a.MOMZ, L);
             double pi, ti;
             if (L == KS) {
+                const double P0 = SA(CA_C, w, L), P1 = SA(CA_C, w, L + 1), P2 = SA(CA_C, w, L + 2);
                 pi = ipL<S>(M0, P0, P1, P2);
                 ti = ipL<S>(mZ, P0, P1, P2);
             } else if (L == KE - 1) {
+                const double Pm1 = SA(CA_C, w, L - 1), P0 = SA(CA_C, w, L), P1 = SA(CA_C, w, L + 1);
                 pi = ipH<S>(M0, P1, P0, Pm1);
                 ti = ipH<S>(mZ, P1, P0, Pm1);
             } else {
+                const double Pm1 = SA(CA_C, w, L - 1), P0 = SA(CA_C, w, L), P1 = SA(CA_C, w, L + 1), P2 = SA(CA_C, w, L + 2);
                 pi = ip4<S>(M0, Pm1, P0, P1, P2);
                 ti = ip4<S>(mZ, Pm1, P0, P1, P2);
             }
-            PT = pi;
-            tZ = mZ * ti + CL(ndTZ, L);
+            pt = pi;
+            tz = mZ * ti + CL(ndTZ, L);
+        };
+        for (int L = KS + lane; L <= KE; L += 32) {
+            double PT, tZ, PTm, tZm;
+            pt_tz(L, PT, tZ);
+            pt_tz(L - 1, PTm, tZm);
+            (void)PTm;
+            const double mZ = (L <= KE - 1) ? CL(ndDZ, L) : 0.0;
+            const double mZm1 = (L - 1 >= KS) ? CL(ndDZ, L - 1) : 0.0;
+            const double rcdz = ld(g.RCDZ + L - 1);
+            // hevi_sr :464-467 and hevi_st :646-649 (metric factors are 1)
+            const double Sr = (-(mZ - mZm1) * rcdz + CL(a.adv_r, L)) + CL(a.DENS_t, L);
+            const double St = (-(tZ - tZm) * rcdz + CL(a.adv_t, L)) + CL(a.RHOT_t, L);
+            const double RTL = CL(a.RT2P, L);
+            SA(CA_PT, w, L) = PT;
+            SA(CA_TZ, w, L) = tZ;
+            SA(CA_SR, w, L) = Sr;
+            SA(CA_ST, w, L) = St;
+            SA(CA_A, w, L) = dt2 * J33G * rcdz * RTL * J33G; // :696
         }
-        const double rcdz = ld(g.RCDZ + L - 1);
-        // hevi_sr :464-467 and hevi_st :646-649 (metric factors are 1)
-        const double Sr = (-(mZ - mZm1) * rcdz + CL(a.adv_r, L)) + CL(a.DENS_t, L);
-        const double St = (-(tZ - tZm1) * rcdz + CL(a.adv_t, L)) + CL(a.RHOT_t, L);
-        const double RTL = CL(a.RT2P, L);
-        const double RH = CL(a.RHOT, L);
-        const double DP = CL(a.DPRES0, L) + RTL * (RH - CL(a.REF_rhot, L)); // :355
-        const double A = dt2 * J33G * rcdz * RTL * J33G;                   // :696
-        const double RD = CL(a.REF_dens, L);
-        pt_[L - 1] = PT; sr_[L - 1] = Sr; st_[L - 1] = St; tz_[L - 1] = tZ;
+    }
+    __syncthreads();
 
-        if (L >= KS + 1) {
-            const int k = L - 1; // unknown level solved in this iteration
-            // vertical w-momentum flux at level k, fluxZ_XYW (ud3.F90:358-452, index shifted by -1)
-            double qZ = 0.0;
-            if (k <= KE - 2) {
-                const double vel = (0.5 * (Mm1 + M0)) / D0;
-                const double q = (k == KS) ? ipL<S>(vel, Mm1, M0, M1) : ip4<S>(vel, Mm2, Mm1, M0, M1);
-                qZ = J33G * vel * q + CL(ndWZ, k + 1);
-            }
+    // ---- phase 3: right-hand side C(k) of the unknown levels k = KS..KE-1, :698-722 ----
+    if (col_ok) {
+        // vertical w-momentum flux at the level k+1/2 ... , fluxZ_XYW (ud3.F90:358-452), zero outside KS..KE-2
+        auto qZ_at = [&](int k) -> double {
+            if (k < KS || k > KE - 2) return 0.0;
+            const double Mk = CL(a.MOMZ, k), Mk1 = CL(a.MOMZ, k + 1);
+            const double vel = (0.5 * (Mk + Mk1)) / CL(a.DENS, k + 1);
+            const double q = (k == KS) ? ipL<S>(vel, Mk, Mk1, CL(a.MOMZ, k + 2))
+                                       : ip4<S>(vel, CL(a.MOMZ, k - 1), Mk, Mk1, CL(a.MOMZ, k + 2));
+            return J33G * vel * q + CL(ndWZ, k + 1);
+        };
+        auto dpres = [&](int L) { return CL(a.DPRES0, L) + CL(a.RT2P, L) * (CL(a.RHOT, L) - CL(a.REF_rhot, L)); }; // :355
+        for (int k = KS + lane; k <= KE - 1; k += 32) {
             // hevi_sw :557-566
-            const double advcv = -(qZ - qZm1) * ld(g.RFDZ + k - 1);
+            const double advcv = -(qZ_at(k) - qZ_at(k - 1)) * ld(g.RFDZ + k - 1);
             const double wdmp = -ld(a.wdamp + k - 1) * CL(a.MOMZ0, k);
             const double div = use_div ? ddc * (CL(a.DDIV, k + 1) - CL(a.DDIV, k)) * ld(g.FDZ + k - 1) : 0.0;
             const double Sw = (advcv + CL(a.adv_w, k)) + wdmp + div + CL(a.MOMZ_t, k);
-            // coefficients :698-709
+            const double rfdz = ld(g.RFDZ + k - 1);
+            const double RTL1 = CL(a.RT2P, k + 1), RTL0 = CL(a.RT2P, k);
+            const double pg = -(dpres(k + 1) + RTL1 * dt * SA(CA_ST, w, k + 1) - dpres(k) - RTL0 * dt * SA(CA_ST, w, k)) * rfdz * J33G
+                              - GRAV * (ld(g.F2H1 + k - 1) * (CL(a.DENS, k + 1) - CL(a.REF_dens, k + 1) + SA(CA_SR, w, k + 1) * dt)
+                                        + ld(g.F2H2 + k - 1) * (CL(a.DENS, k) - CL(a.REF_dens, k) + SA(CA_SR, w, k) * dt));
+            SA(CA_C, w, k) = CL(a.MOMZ, k) + dt * (pg + Sw);
+        }
+    }
+    __syncthreads();
+
+    // ---- phase 4: Thomas solve, one thread per column (solve_direct :1110-1124) ----
+    if (w == 0 && lane < TC && i0 + lane <= g.IE) {
+        const int c = lane;
+        double e_prev = 0.0, f_prev = 0.0;
+        for (int k = KS; k <= KE - 1; ++k) {
             const double rfdz = ld(g.RFDZ + k - 1);
             const double B = GRAV * dt2 * J33G / (ld(g.CDZ + k) + ld(g.CDZ + k - 1));
-            const double F2 = 1.0 + (PTm1 * rfdz * (A + Am1));
-            // right-hand side :710-718
-            const double pg = -(DP + RTL * dt * St - DPm1 - RPm1 * dt * Stm1) * rfdz * J33G
-                              - GRAV * (ld(g.F2H1 + k - 1) * (D0 - RD + Sr * dt)
-                                        + ld(g.F2H2 + k - 1) * (Dm1 - RDm1 + Srm1 * dt));
-            const double C = Mm1 + dt * (pg + Sw);
-            // Thomas forward sweep, solve_direct :1110-1121
+            const double Ak = SA(CA_A, c, k), Ak1 = SA(CA_A, c, k + 1);
+            const double F2 = 1.0 + (SA(CA_PT, c, k) * rfdz * (Ak1 + Ak));
+            const double Ck = SA(CA_C, c, k);
             if (k == KS) {
-                const double F1 = -(PT * rfdz * A + B);
+                const double F1 = -(SA(CA_PT, c, k + 1) * rfdz * Ak1 + B);
                 const double rdenom = 1.0 / F2;
                 e_prev = -F1 * rdenom;
-                f_prev = C * rdenom;
-                e_[k - 1] = e_prev; f_[k - 1] = f_prev;
+                f_prev = Ck * rdenom;
             } else if (k <= KE - 2) {
-                const double F1 = -(PT * rfdz * A + B);
-                const double F3 = -(PTm2 * rfdz * Am1 - B);
+                const double F1 = -(SA(CA_PT, c, k + 1) * rfdz * Ak1 + B);
+                const double F3 = -(SA(CA_PT, c, k - 1) * rfdz * Ak - B);
                 const double rdenom = 1.0 / (F2 + F3 * e_prev);
                 e_prev = -F1 * rdenom;
-                f_prev = (C - F3 * f_prev) * rdenom;
-                e_[k - 1] = e_prev; f_[k - 1] = f_prev;
+                f_prev = (Ck - F3 * f_prev) * rdenom;
             } else {
-                const double F3 = -(PTm2 * rfdz * Am1 - B);
-                Cfin = (C - F3 * f_prev) / (F2 + F3 * e_prev);
+                const double F3 = -(SA(CA_PT, c, k - 1) * rfdz * Ak - B);
+                f_prev = (Ck - F3 * f_prev) / (F2 + F3 * e_prev); // the solution at KE-1
             }
-            qZm1 = qZ;
+            SA(CA_A, c, k) = e_prev;
+            SA(CA_C, c, k) = f_prev;
         }
-
-        // shift windows to L+1
-        Pm1 = P0; P0 = P1; P1 = P2;
-        Dm1 = D0; D0 = Pd1; Pd1 = Pd2;
-        Mm2 = Mm1; Mm1 = M0; M0 = M1;
-        mZm1 = mZ; tZm1 = tZ;
-        PTm2 = PTm1; PTm1 = PT;
-        Am1 = A; DPm1 = DP; RPm1 = RTL; RDm1 = RD; Srm1 = Sr; Stm1 = St;
+        // back substitution, C(k) = e(k) C(k+1) + f(k)
+        double Cnext = f_prev;
+        for (int k = KE - 2; k >= KS; --k) {
+            Cnext = SA(CA_A, c, k) * Cnext + SA(CA_C, c, k);
+            SA(CA_C, c, k) = Cnext;
+        }
+        SA(CA_C, c, KE) = 0.0;
+        SA(CA_C, c, KS - 1) = 0.0;
+        SA(CA_PT, c, KE) = 0.0;
+        SA(CA_PT, c, KS - 1) = 0.0;
     }
+    __syncthreads();
 
-    // ---- back substitution and update, :728-790 ----
-    const size_t c0 = col;
-    auto fin = [&](int m, double Cm, double Cm1) {
-        const size_t c = c0 + m - 1;
-        const double rcdz = ld(g.RCDZ + m - 1);
-        double adr, adt;
-        if (m == KE) {
-            adr = Cm1 * J33G * rcdz;
-            adt = Cm1 * pt_[KE - 2] * J33G * rcdz;
-        } else if (m == KS) {
-            adr = -Cm * J33G * rcdz;
-            adt = -Cm * pt_[KS - 1] * J33G * rcdz;
-        } else {
-            adr = -(Cm - Cm1) * J33G * rcdz;
-            adt = -(Cm * pt_[m - 1] - Cm1 * pt_[m - 2]) * J33G * rcdz;
+    // ---- phase 5: back-update, :728-790 ----
+    if (col_ok) {
+        for (int m = KS + lane; m <= KE; m += 32) {
+            const size_t c = col + m - 1;
+            const double rcdz = ld(g.RCDZ + m - 1);
+            const double Cm = SA(CA_C, w, m), Cm1 = SA(CA_C, w, m - 1);
+            double adr, adt;
+            if (m == KE) {
+                adr = Cm1 * J33G * rcdz;
+                adt = Cm1 * SA(CA_PT, w, KE - 1) * J33G * rcdz;
+            } else if (m == KS) {
+                adr = -Cm * J33G * rcdz;
+                adt = -Cm * SA(CA_PT, w, KS) * J33G * rcdz;
+            } else {
+                adr = -(Cm - Cm1) * J33G * rcdz;
+                adt = -(Cm * SA(CA_PT, w, m) - Cm1 * SA(CA_PT, w, m - 1)) * J33G * rcdz;
+            }
+            put_state(a, N3, 0, a.DENS_RK, a.DENS0, c, ld(a.DENS0 + c) + dt * (adr + SA(CA_SR, w, m)), true);
+            put_state(a, N3, 4, a.RHOT_RK, a.RHOT0, c, ld(a.RHOT0 + c) + dt * (adt + SA(CA_ST, w, m)), true);
+            if (m <= KE - 1) {
+                put_state(a, N3, 1, a.MOMZ_RK, a.MOMZ0, c, ld(a.MOMZ0 + c) + (Cm - ld(a.MOMZ + c)), true);
+                put_flux(a, N3, 0, c, ld(ndDZ + c) + J33G * Cm, true);
+                put_flux(a, N3, 3, c, SA(CA_TZ, w, m) + J33G * Cm * SA(CA_PT, w, m), true);
+            } else {
+                put_state(a, N3, 1, a.MOMZ_RK, a.MOMZ0, c, 0.0, false);
+                put_flux(a, N3, 0, c, 0.0, true);
+                put_flux(a, N3, 3, c, 0.0, true);
+            }
         }
-        put_state(a, N3, 0, a.DENS_RK, a.DENS0, c, ld(a.DENS0 + c) + dt * (adr + sr_[m - 1]), true);
-        put_state(a, N3, 4, a.RHOT_RK, a.RHOT0, c, ld(a.RHOT0 + c) + dt * (adt + st_[m - 1]), true);
-        if (m <= KE - 1) {
-            put_state(a, N3, 1, a.MOMZ_RK, a.MOMZ0, c, ld(a.MOMZ0 + c) + (Cm - ld(a.MOMZ + c)), true);
-            put_flux(a, N3, 0, c, ld(ndDZ + c) + J33G * Cm, true);
-            put_flux(a, N3, 3, c, tz_[m - 1] + J33G * Cm * pt_[m - 1], true);
-        } else {
-            put_state(a, N3, 1, a.MOMZ_RK, a.MOMZ0, c, 0.0, false);
-            put_flux(a, N3, 0, c, 0.0, true);
-            put_flux(a, N3, 3, c, 0.0, true);
+        if (lane == 0) {
+            // rigid-lid and surface values (:753-754) and the zero fluxes at KS-1 (:371, ud3.F90:222)
+            put_state(a, N3, 1, a.MOMZ_RK, a.MOMZ0, col + KS - 2, 0.0, false);
+            put_flux(a, N3, 0, col + KS - 2, 0.0, false);
+            put_flux(a, N3, 3, col + KS - 2, 0.0, false);
         }
-    };
-    double Cnext = Cfin;             // C at level KE-1
-    fin(KE, 0.0, Cnext);
-    for (int k = KE - 2; k >= KS; --k) {
-        const double Ck = e_[k - 1] * Cnext + f_[k - 1];
-        fin(k + 1, Cnext, Ck);
-        Cnext = Ck;
     }
-    fin(KS, Cnext, 0.0);
-    // rigid-lid and surface values (:753-754) and the zero fluxes at KS-1 (:371, ud3.F90:222)
-    put_state(a, N3, 1, a.MOMZ_RK, a.MOMZ0, c0 + KS - 2, 0.0, false);
-    put_flux(a, N3, 0, c0 + KS - 2, 0.0, false);
-    put_flux(a, N3, 3, c0 + KS - 2, 0.0, false);
+    // hevi_mflx_z :369-393 also fills the halo column i = IS-1 with the explicit
+    // part of the vertical mass flux; the solver never updates it
+    if (blockIdx.x == 0 && w == TC - 1 && (a.rk_mode == RK_PLAIN || a.rk_mode == RK_FINAL)) {
+        const size_t ch = idx3(g, 1, g.IS - 1, j);
+        for (int k = KS - 1 + lane; k <= KE; k += 32)
+            a.mflx[ch + k - 1] = (k >= KS && k <= KE - 1) ? ld(ndDZ + ch + k - 1) : 0.0;
+    }
+#undef SA
 #undef CL
 }
 
@@ -425,13 +456,22 @@ cudaError_t launch_hevi_horiz(const Grid &g, const StageArgs &a, int scheme, cud
     return cudaGetLastError();
 }
 
+// columns per CTA: 16 while two CTAs fit one SM's shared memory, else 8
+static int column_tile(int KA) { return (size_t)COL_ARRAYS * 16 * col_pitch(KA) * sizeof(double) <= 112 * 1024 ? 16 : 8; }
+
 cudaError_t launch_hevi_column(const Grid &g, const StageArgs &a, int scheme, cudaStream_t st)
 {
     if (g.KA > MAXKA) return cudaErrorInvalidValue;
-    dim3 bc(128);
-    dim3 gc((g.IMAX + 1 + 127) / 128, g.JMAX);
-    if (scheme == UD3) k_hevi_column<UD3><<<gc, bc, 0, st>>>(g, a);
-    else k_hevi_column<CD4><<<gc, bc, 0, st>>>(g, a);
+    const int TC = column_tile(g.KA);
+    const size_t smem = (size_t)COL_ARRAYS * TC * col_pitch(g.KA) * sizeof(double);
+    cudaError_t e = scheme == UD3
+        ? cudaFuncSetAttribute(k_hevi_column<UD3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)
+        : cudaFuncSetAttribute(k_hevi_column<CD4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    dim3 bc(32, TC);
+    dim3 gc((g.IMAX + TC - 1) / TC, g.JMAX);
+    if (scheme == UD3) k_hevi_column<UD3><<<gc, bc, smem, st>>>(g, a);
+    else k_hevi_column<CD4><<<gc, bc, smem, st>>>(g, a);
     return cudaGetLastError();
 }
 
