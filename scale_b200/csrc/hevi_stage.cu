@@ -17,6 +17,21 @@
 // reference HEVI file unless a flux file is named.
 #include "hevi_kernels.cuh"
 
+// Launch shapes. The defaults are the measured best on B200 for KMAX = 128;
+// they can be overridden at build time for tuning sweeps.
+#ifndef HEVI_HORIZ_COLS
+#define HEVI_HORIZ_COLS 4 // i-columns per block of k_hevi_horiz (blockDim = 32 x HEVI_HORIZ_COLS)
+#endif
+#ifndef HEVI_HORIZ_MINB
+#define HEVI_HORIZ_MINB 8 // minimum resident blocks per SM asked of the register allocator
+#endif
+#ifndef HEVI_COL_TC
+#define HEVI_COL_TC 16 // columns per CTA of k_hevi_column
+#endif
+#ifndef HEVI_COL_MINB
+#define HEVI_COL_MINB 2
+#endif
+
 namespace hevi {
 
 // num_diff(:,:,:,v,dir) slice offset; v: DENS=1..RHOT=5, dir: Z=1,X=2,Y=3
@@ -67,7 +82,7 @@ __device__ __forceinline__ void put_flux(const StageArgs &a, size_t N3, int f, s
 // 3-D kernel: horizontal fluxes and the u/v momentum updates
 // =============================================================================
 template <int S>
-__global__ void __launch_bounds__(128) k_hevi_horiz(const Grid g, const StageArgs a)
+__global__ void __launch_bounds__(32 * HEVI_HORIZ_COLS, HEVI_HORIZ_MINB) k_hevi_horiz(const Grid g, const StageArgs a)
 {
     const int i = g.IS + blockIdx.x * blockDim.y + threadIdx.y;
     const int j = g.JS + blockIdx.y;
@@ -259,7 +274,7 @@ enum ColArr : int { CA_C = 0, CA_PT = 1, CA_A = 2, CA_SR = 3, CA_ST = 4, CA_TZ =
 __host__ __device__ inline int col_pitch(int KA) { return KA | 1; }
 
 template <int S>
-__global__ void __launch_bounds__(512, 2) k_hevi_column(const Grid g, const StageArgs a)
+__global__ void __launch_bounds__(32 * HEVI_COL_TC, HEVI_COL_MINB) k_hevi_column(const Grid g, const StageArgs a)
 {
     extern __shared__ double sm[];
     const int TC = blockDim.y;
@@ -449,15 +464,20 @@ __global__ void __launch_bounds__(512, 2) k_hevi_column(const Grid g, const Stag
 // ---- host launchers ---------------------------------------------------------
 cudaError_t launch_hevi_horiz(const Grid &g, const StageArgs &a, int scheme, cudaStream_t st)
 {
-    dim3 bh(32, 4);
-    dim3 gh((g.IMAX + 3) / 4, g.JMAX);
+    dim3 bh(32, HEVI_HORIZ_COLS);
+    dim3 gh((g.IMAX + HEVI_HORIZ_COLS - 1) / HEVI_HORIZ_COLS, g.JMAX);
     if (scheme == UD3) k_hevi_horiz<UD3><<<gh, bh, 0, st>>>(g, a);
     else k_hevi_horiz<CD4><<<gh, bh, 0, st>>>(g, a);
     return cudaGetLastError();
 }
 
-// columns per CTA: 16 while two CTAs fit one SM's shared memory, else 8
-static int column_tile(int KA) { return (size_t)COL_ARRAYS * 16 * col_pitch(KA) * sizeof(double) <= 112 * 1024 ? 16 : 8; }
+// columns per CTA: HEVI_COL_TC, halved until HEVI_COL_MINB CTAs fit one SM's shared memory
+static int column_tile(int KA)
+{
+    int tc = HEVI_COL_TC;
+    while (tc > 1 && (size_t)COL_ARRAYS * tc * col_pitch(KA) * sizeof(double) > (size_t)224 * 1024 / HEVI_COL_MINB) tc /= 2;
+    return tc;
+}
 
 cudaError_t launch_hevi_column(const Grid &g, const StageArgs &a, int scheme, cudaStream_t st)
 {

@@ -110,7 +110,11 @@ __device__ __forceinline__ double dy(const Grid &g, const NdCoef &c, const Phi &
             + CY3(3, j, 2) * phi(q, k, i, j - 1) - CY3(1, j - 1, 2) * phi(q, k, i, j - 2));
 }
 
-__global__ void __launch_bounds__(128) k_numfilter(const Grid g, const NdCoef c, const NdArgs a)
+#ifndef HEVI_ND_MINB
+#define HEVI_ND_MINB 8 // minimum resident blocks per SM asked of the register allocator
+#endif
+
+__global__ void __launch_bounds__(128, HEVI_ND_MINB) k_numfilter(const Grid g, const NdCoef c, const NdArgs a)
 {
     const int i = g.IS + blockIdx.x * blockDim.y + threadIdx.y;
     const int j = g.JS + blockIdx.y;
