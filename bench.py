@@ -242,11 +242,11 @@ def run_b200(args):
         peaks = json.loads(pk.read_text())
     hbm = float(peaks.get("hbm_gbs", 6650.0))
     peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
-    nst = prof.get("hevi_horiz", (0, 0.0))[0]
-    stage_ms = (prof.get("hevi_horiz", (0, 0.0))[1] + prof.get("hevi_column", (0, 0.0))[1]) / max(nst, 1)
+    nst, stage_total = prof.get("hevi_stage", (0, 0.0))
+    stage_ms = stage_total / max(nst, 1)
     achieved = STAGE_BYTES * cells / (stage_ms * 1e-3) / 1e9 if stage_ms > 0 else None
     traffic = read_traffic()
-    roofline = {"bound": "hbm", "kernel": "hevi_stage (k_hevi_horiz + k_hevi_column), one HEVI stage",
+    roofline = {"bound": "hbm", "kernel": "k_hevi_stage (one HEVI stage)",
                 "achieved": achieved, "peak": hbm, "peak_source": peak_src, "unit": "GB/s",
                 "frac": (achieved / hbm) if achieved else None, "algorithmic_bytes_per_launch": STAGE_BYTES * cells,
                 "stage_ms": stage_ms, "traffic": traffic,

@@ -40,7 +40,6 @@ struct Ctx {
     std::vector<double> nd_key;
     NdCoef ndc{};
     // scratch
-    double *adv = nullptr;          // 3*N3
     double *rk[2] = {nullptr, nullptr}; // 5*N3 each
     double *acc = nullptr;          // 5*N3
     double *facc = nullptr;         // 6*N3
@@ -124,7 +123,7 @@ int dalloc(double **p, size_t n)
 
 void free_all()
 {
-    double *bufs[] = {C.d_tab, C.d_nd, C.adv, C.rk[0], C.rk[1], C.acc, C.facc, C.tr, C.lg, C.sum_part, C.sum_out};
+    double *bufs[] = {C.d_tab, C.d_nd, C.rk[0], C.rk[1], C.acc, C.facc, C.tr, C.lg, C.sum_part, C.sum_out};
     for (double *b : bufs) if (b) cudaFree(b);
     for (auto &kv : C.stage) cudaFree(kv.second.first);
     if (C.status) cudaFree(C.status);
@@ -313,17 +312,12 @@ int run_stage(const StageIn &in, double *const out[5], double *mflx, double *tfl
     a.DPRES0 = in.DPRES0; a.RT2P = in.RT2P; a.CORIOLI = in.CORIOLI; a.num_diff = in.num_diff;
     a.wdamp = C.d_wdamp; a.DDIV = in.DDIV; a.REF_dens = in.REF_dens; a.REF_rhot = in.REF_rhot;
     a.divdmp_coef = in.divdmp; a.J33G = in.J33G; a.dtrk = dtrk;
-    a.adv_r = C.adv; a.adv_w = C.adv + C.N3; a.adv_t = C.adv + 2 * C.N3;
     a.rk_mode = mode; a.acc = C.acc; a.facc = C.facc; a.status = C.status;
-    CK(timed("hevi_horiz", [&] {
-        CU(launch_hevi_horiz(C.g, a, C.scheme, C.stream));
+    CK(timed("hevi_stage", [&] {
+        CU(launch_hevi_stage(C.g, a, C.scheme, C.stream));
         return SCALE_HEVI_OK;
     }));
-    CK(timed("hevi_column", [&] {
-        CU(launch_hevi_column(C.g, a, C.scheme, C.stream));
-        return SCALE_HEVI_OK;
-    }));
-    C.launches += 2;
+    ++C.launches;
     return SCALE_HEVI_OK;
 }
 
@@ -446,7 +440,7 @@ int scale_hevi_setup(const scale_hevi_index *idx, const char *flux_type, const c
     int rc = SCALE_HEVI_OK;
     if ((rc = dalloc(&C.d_tab, 7 * (size_t)x.KA + 4 * (size_t)x.IA + 4 * (size_t)x.JA)) ||
         (rc = dalloc(&C.d_nd, 8 * (size_t)x.KA + 8 * (size_t)x.IA + 8 * (size_t)x.JA)) ||
-        (rc = dalloc(&C.adv, 3 * N3)) || (rc = dalloc(&C.rk[0], 5 * N3)) || (rc = dalloc(&C.rk[1], 5 * N3)) ||
+        (rc = dalloc(&C.rk[0], 5 * N3)) || (rc = dalloc(&C.rk[1], 5 * N3)) ||
         (rc = dalloc(&C.acc, 5 * N3)) || (rc = dalloc(&C.facc, 6 * N3)) ||
         (rc = dalloc(&C.sum_part, (size_t)x.IMAX * x.JMAX)) || (rc = dalloc(&C.sum_out, 1))) {
         free_all();

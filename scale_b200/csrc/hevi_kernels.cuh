@@ -35,8 +35,7 @@ struct TracerArgs {
 cudaError_t launch_tracer_stage(const Grid &g, const TracerArgs &a, int scheme, bool fct, cudaStream_t st);
 
 // ---- HEVI stage (hevi_stage.cu) ----
-cudaError_t launch_hevi_horiz(const Grid &g, const StageArgs &a, int scheme, cudaStream_t st);
-cudaError_t launch_hevi_column(const Grid &g, const StageArgs &a, int scheme, cudaStream_t st);
+cudaError_t launch_hevi_stage(const Grid &g, const StageArgs &a, int scheme, cudaStream_t st);
 
 // ---- utilities (misc.cu) ----
 void periodic_halo(const Grid &g, double *const *fields, int nf, cudaStream_t st);

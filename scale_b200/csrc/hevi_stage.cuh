@@ -34,8 +34,6 @@ struct StageArgs {
     const double *DDIV;
     const double *REF_dens, *REF_rhot;
     double divdmp_coef, J33G, dtrk;
-    // horizontal flux divergences handed from the 3-D kernel to the column kernel
-    double *adv_r, *adv_w, *adv_t;
     // RK accumulation
     int rk_mode;
     double *acc;  // 5*N3: DENS, MOMZ, MOMX, MOMY, RHOT

@@ -17,9 +17,10 @@
 //   - The scratch is shared by every call on a device, so calls that overlap in
 //     time (two host threads, or two streams in flight) race on it.
 //   - The entry synchronises its stream before it returns.
-//   - The domain must fit: 3*KA*IA*JA + 7*KA + 4*IA + 4*JA doubles plus a
-//     256-byte header, at most SCALE_HEVI_NOALLOC_SCRATCH_BYTES. Larger domains
-//     are rejected with SCALE_HEVI_ERR_ARG.
+//   - The scratch holds a 256-byte header (status word, terrain-check counter)
+//     and the 1-D grid tables, 7*KA + 4*IA + 4*JA doubles; at most
+//     SCALE_HEVI_NOALLOC_SCRATCH_BYTES. Larger domains are rejected with
+//     SCALE_HEVI_ERR_ARG.
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -118,7 +119,7 @@ extern "C" int ATMOS_DYN_Tstep_short_fvm_hevi_b200_noalloc(const scale_hevi_inde
     const int KA = x.KA, IA = x.IA, JA = x.JA;
     const size_t N3 = (size_t)KA * IA * JA;
     const size_t ntab = 7 * (size_t)KA + 4 * (size_t)IA + 4 * (size_t)JA;
-    const size_t need = kHeader + (3 * N3 + ntab) * sizeof(double);
+    const size_t need = kHeader + ntab * sizeof(double);
     if (need > kScratchBytes)
         return err(SCALE_HEVI_ERR_ARG,
                    "domain %dx%dx%d needs %zu bytes of scratch; the no-alloc entry holds at most %zu bytes",
@@ -129,8 +130,7 @@ extern "C" int ATMOS_DYN_Tstep_short_fvm_hevi_b200_noalloc(const scale_hevi_inde
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     unsigned *status = reinterpret_cast<unsigned *>(scr);
     unsigned long long *count = reinterpret_cast<unsigned long long *>(scr + 8);
-    double *adv = reinterpret_cast<double *>(scr + kHeader);
-    double *tab = adv + 3 * N3;
+    double *tab = reinterpret_cast<double *>(scr + kHeader);
 
     // flat terrain only, as the other entries (GSQRT = 1, J13G = J23G = 0, MAPF = 1)
     NA_CU(cudaMemsetAsync(scr, 0, kHeader, st)); // status and counter start at zero
@@ -179,11 +179,9 @@ extern "C" int ATMOS_DYN_Tstep_short_fvm_hevi_b200_noalloc(const scale_hevi_inde
     a.DPRES0 = DPRES0; a.RT2P = RT2P; a.CORIOLI = CORIOLI; a.num_diff = num_diff;
     a.wdamp = z + 6 * KA; a.DDIV = DDIV; a.REF_dens = REF_dens; a.REF_rhot = REF_rhot;
     a.divdmp_coef = *divdmp_coef; a.J33G = *J33G; a.dtrk = *dtrk;
-    a.adv_r = adv; a.adv_w = adv + N3; a.adv_t = adv + 2 * N3;
     a.rk_mode = RK_PLAIN; a.acc = nullptr; a.facc = nullptr; a.status = status;
 
-    NA_CU(launch_hevi_horiz(g, a, scheme, st));
-    NA_CU(launch_hevi_column(g, a, scheme, st));
+    NA_CU(launch_hevi_stage(g, a, scheme, st));
     unsigned flags = 0;
     NA_CU(cudaMemcpyAsync(&flags, status, sizeof flags, cudaMemcpyDeviceToHost, st));
     NA_CU(cudaStreamSynchronize(st));
