@@ -29,6 +29,15 @@
 #ifndef HEVI_COL_MINB
 #define HEVI_COL_MINB 2 // resident CTAs per SM the register allocator must allow
 #endif
+#ifndef HEVI_RASTER_J
+#define HEVI_RASTER_J 16 // rows of tiles launched together (2-D raster: a smaller L2 working set)
+#endif
+#ifndef HEVI_STREAM_HINTS
+#define HEVI_STREAM_HINTS 1 // evict-first loads/stores for data each cell touches once
+#endif
+#ifndef HEVI_L2_PREFETCH
+#define HEVI_L2_PREFETCH 0 // bulk L2 prefetch of the tile's columns one phase ahead
+#endif
 
 namespace hevi {
 
@@ -43,19 +52,30 @@ __device__ __forceinline__ void flag_nonfinite(const StageArgs &a, double v)
     if (!isfinite(v)) atomicOr(a.status, ST_NONFINITE);
 }
 
+// Data a cell reads or writes once (tendencies, stage-0 state, outputs, RK sums)
+// go through the cache-streaming path, so that L2 keeps the fields whose x/y
+// neighbours other tiles read again.
+#if HEVI_STREAM_HINTS
+__device__ __forceinline__ double lds(const double *p) { return __ldcs(p); }
+__device__ __forceinline__ void sts(double *p, double v) { __stcs(p, v); }
+#else
+__device__ __forceinline__ double lds(const double *p) { return __ldg(p); }
+__device__ __forceinline__ void sts(double *p, double v) { *p = v; }
+#endif
+
 // store one prognostic value of the stage, folding in the RK4 combine
 __device__ __forceinline__ void put_state(const StageArgs &a, size_t N3, int v, double *out, const double *x0,
                                           size_t c, double val, bool combine)
 {
     double *acc = a.acc + (size_t)v * N3 + c;
     switch (a.rk_mode) {
-    case RK_PLAIN: out[c] = val; flag_nonfinite(a, val); break;
-    case RK_STAGE1: out[c] = val; if (combine) *acc = val * 2.0; break;
-    case RK_STAGE2: out[c] = val; if (combine) *acc = *acc + val * 4.0; break;
-    case RK_STAGE3: out[c] = val; if (combine) *acc = *acc + val * 2.0; break;
+    case RK_PLAIN: sts(out + c, val); flag_nonfinite(a, val); break;
+    case RK_STAGE1: sts(out + c, val); if (combine) sts(acc, val * 2.0); break;
+    case RK_STAGE2: sts(out + c, val); if (combine) sts(acc, lds(acc) + val * 4.0); break;
+    case RK_STAGE3: sts(out + c, val); if (combine) sts(acc, lds(acc) + val * 2.0); break;
     default: {
-        double r = combine ? ((*acc + val) - x0[c] * 3.0) / 6.0 : val;
-        out[c] = r;
+        double r = combine ? ((lds(acc) + val) - lds(x0 + c) * 3.0) / 6.0 : val;
+        sts(out + c, r);
         flag_nonfinite(a, r);
     }
     }
@@ -68,12 +88,25 @@ __device__ __forceinline__ void put_flux(const StageArgs &a, size_t N3, int f, s
     double *out = (f < 3 ? a.mflx : a.tflx) + (size_t)(f % 3) * N3 + c;
     double *acc = a.facc + (size_t)f * N3 + c;
     switch (a.rk_mode) {
-    case RK_PLAIN: *out = val; break;
-    case RK_STAGE1: if (interior) *acc = val; break;
+    case RK_PLAIN: sts(out, val); break;
+    case RK_STAGE1: if (interior) sts(acc, val); break;
     case RK_STAGE2:
-    case RK_STAGE3: if (interior) *acc = *acc + val * 2.0; break;
-    default: *out = interior ? (*acc + val) / 6.0 : val;
+    case RK_STAGE3: if (interior) sts(acc, lds(acc) + val * 2.0); break;
+    default: sts(out, interior ? (lds(acc) + val) / 6.0 : val);
     }
+}
+
+// Bulk prefetch of n bytes at p into L2 (a hint: no completion to wait for).
+// The address must be 16-byte aligned and n a multiple of 16; misaligned
+// fields are simply not prefetched.
+__device__ __forceinline__ void l2_prefetch(const double *p, unsigned n)
+{
+#if HEVI_L2_PREFETCH
+    if (p && n && ((reinterpret_cast<uintptr_t>(p) & 15u) == 0) && (n & 15u) == 0)
+        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(n) : "memory");
+#else
+    (void)p; (void)n;
+#endif
 }
 
 // =============================================================================
@@ -159,7 +192,7 @@ __device__ __forceinline__ void update_momxy(const Grid &g, const StageArgs &a, 
             if (m == KS) q = ipL<S>(vel, AT(MX, dm, 0, 0), AT(MX, dm + 1, 0, 0), AT(MX, dm + 2, 0, 0));
             else if (m == KE - 1) q = ipH<S>(vel, AT(MX, dm + 1, 0, 0), AT(MX, dm, 0, 0), AT(MX, dm - 1, 0, 0));
             else q = ip4<S>(vel, AT(MX, dm - 1, 0, 0), AT(MX, dm, 0, 0), AT(MX, dm + 1, 0, 0), AT(MX, dm + 2, 0, 0));
-            return J33G * vel * q + AT(nd.UZ, dm, 0, 0);
+            return J33G * vel * q + lds(nd.UZ + c + dm);
         };
         const double U_m2 = AT(MX, 0, -2, 0), U_m1 = AT(MX, 0, -1, 0), U_00 = AT(MX, 0, 0, 0);
         const double U_p1 = AT(MX, 0, 1, 0), U_p2 = AT(MX, 0, 2, 0);
@@ -181,7 +214,7 @@ __device__ __forceinline__ void update_momxy(const Grid &g, const StageArgs &a, 
         const double pg = (DPe - DP00) * rfdx;
         const double cf = cor_u * (AT(MY, 0, 1, 0) + AT(MY, 0, 0, 0) + AT(MY, 0, 1, -1) + AT(MY, 0, 0, -1));
         const double div = use_div ? ddc * (AT(a.DDIV, 0, 1, 0) - AT(a.DDIV, 0, 0, 0)) * fdx : 0.0;
-        const double val = AT(a.MOMX0, 0, 0, 0) + dt * ((((advcv + advch) - pg) + cf) + div + AT(a.MOMX_t, 0, 0, 0));
+        const double val = lds(a.MOMX0 + c) + dt * ((((advcv + advch) - pg) + cf) + div + lds(a.MOMX_t + c));
         put_state(a, N3, 2, a.MOMX_RK, a.MOMX0, c, val, true);
     }
 
@@ -197,7 +230,7 @@ __device__ __forceinline__ void update_momxy(const Grid &g, const StageArgs &a, 
             if (m == KS) q = ipL<S>(vel, AT(MY, dm, 0, 0), AT(MY, dm + 1, 0, 0), AT(MY, dm + 2, 0, 0));
             else if (m == KE - 1) q = ipH<S>(vel, AT(MY, dm + 1, 0, 0), AT(MY, dm, 0, 0), AT(MY, dm - 1, 0, 0));
             else q = ip4<S>(vel, AT(MY, dm - 1, 0, 0), AT(MY, dm, 0, 0), AT(MY, dm + 1, 0, 0), AT(MY, dm + 2, 0, 0));
-            return J33G * vel * q + AT(nd.VZ, dm, 0, 0);
+            return J33G * vel * q + lds(nd.VZ + c + dm);
         };
         const double Y_m2 = AT(MY, 0, 0, -2), Y_m1 = AT(MY, 0, 0, -1), Y_00 = AT(MY, 0, 0, 0);
         const double Y_p1 = AT(MY, 0, 0, 1), Y_p2 = AT(MY, 0, 0, 2);
@@ -219,7 +252,7 @@ __device__ __forceinline__ void update_momxy(const Grid &g, const StageArgs &a, 
         const double pg = (DPn - DP00) * rfdy;
         const double cf = cor_v * (AT(MX, 0, 0, 1) + AT(MX, 0, 0, 0) + AT(MX, 0, -1, 1) + AT(MX, 0, -1, 0));
         const double div = use_div ? ddc * (AT(a.DDIV, 0, 0, 1) - AT(a.DDIV, 0, 0, 0)) * fdy : 0.0;
-        const double val = AT(a.MOMY0, 0, 0, 0) + dt * ((((advcv + advch) - pg) + cf) + div + AT(a.MOMY_t, 0, 0, 0));
+        const double val = lds(a.MOMY0 + c) + dt * ((((advcv + advch) - pg) + cf) + div + lds(a.MOMY_t + c));
         put_state(a, N3, 3, a.MOMY_RK, a.MOMY0, c, val, true);
     }
 }
@@ -242,8 +275,18 @@ __global__ void __launch_bounds__(32 * HEVI_COL_TC, HEVI_COL_MINB) k_hevi_stage(
     extern __shared__ double sm[];
     const int TC = blockDim.y;
     const int lane = threadIdx.x, w = threadIdx.y;
-    const int i0 = g.IS + blockIdx.x * TC;
-    const int j = g.JS + blockIdx.y;
+    // 2-D raster: consecutive CTAs walk down HEVI_RASTER_J rows of tiles, then
+    // step in i, so the CTAs resident together cover a compact patch
+    int ti, jj;
+    {
+        const int nti = gridDim.x, b = blockIdx.x + nti * blockIdx.y;
+        const int grp = b / (nti * HEVI_RASTER_J), rem = b - grp * (nti * HEVI_RASTER_J);
+        const int rows = min(HEVI_RASTER_J, g.JMAX - grp * HEVI_RASTER_J);
+        jj = grp * HEVI_RASTER_J + rem % rows;
+        ti = rem / rows;
+    }
+    const int i0 = g.IS + ti * TC;
+    const int j = g.JS + jj;
     const int i = i0 + w; // this warp's column in the k-parallel phases
     const bool col_ok = i <= g.IE;
     const size_t N3 = n3(g);
@@ -260,6 +303,22 @@ __global__ void __launch_bounds__(32 * HEVI_COL_TC, HEVI_COL_MINB) k_hevi_stage(
 #define SA(arr, cc, L) sm[((size_t)(arr) * TC + (cc)) * KP + (L) - 1]
 #define CL(p, L) ld((p) + col + (L) - 1)
 
+    // L2 prefetch of the tile's columns of the fields the next phase reads;
+    // the last warp issues one bulk prefetch per field (one lane each)
+    const size_t tile0 = idx3(g, 1, i0, j);
+    const unsigned tile_bytes = (unsigned)((size_t)min(TC, g.IE - i0 + 1) * g.KA * sizeof(double));
+    const bool rk_reads = a.rk_mode >= RK_STAGE2;
+    auto prefetch = [&](const double *const *f, int n) {
+        if (w == TC - 1 && lane < n) l2_prefetch(f[lane] ? f[lane] + tile0 : nullptr, tile_bytes);
+    };
+    {
+        const double *f[] = {a.RHOT, a.DENS, a.MOMX, a.MOMY, nd.DX, nd.DY, nd.DZ, a.DENS_t, a.RT2P,
+                             rk_reads ? a.facc + N3 : nullptr, rk_reads ? a.facc + 2 * N3 : nullptr,
+                             a.MOMZ, nd.TZ, nd.TX, nd.TY, a.RHOT_t,
+                             rk_reads ? a.facc + 4 * N3 : nullptr, rk_reads ? a.facc + 5 * N3 : nullptr};
+        prefetch(f, 18);
+    }
+
     // ---- phase 1: POTT (:586-600), x/y mass fluxes (:399-438), Sr (:443-479), A (:696) ----
     if (col_ok) {
         for (int L = KS + lane; L <= KE; L += 32) {
@@ -274,12 +333,17 @@ __global__ void __launch_bounds__(32 * HEVI_COL_TC, HEVI_COL_MINB) k_hevi_stage(
             const double mZ = (L <= KE - 1) ? ld(nd.DZ + c) : 0.0; // hevi_mflx_z :383-391 (flat terrain)
             const double mZm1 = (L - 1 >= KS) ? ld(nd.DZ + c - 1) : 0.0;
             const double rcdz = ld(g.RCDZ + L - 1);
-            SA(CA_SR, w, L) = (-(mZ - mZm1) * rcdz + adv_r) + ld(a.DENS_t + c);
+            SA(CA_SR, w, L) = (-(mZ - mZm1) * rcdz + adv_r) + lds(a.DENS_t + c);
             SA(CA_A, w, L) = dt2 * J33G * rcdz * ld(a.RT2P + c) * J33G;
         }
     }
     __syncthreads();
 
+    {
+        const double *f[] = {a.MOMZ0, a.MOMZ_t, a.DPRES0, a.REF_rhot, a.REF_dens, nd.WZ, nd.WX, nd.WY,
+                             use_div ? a.DDIV : nullptr};
+        prefetch(f, 9);
+    }
     // ---- phase 2: PT, tZ (valueW_Z ud3.F90:98-153, fluxZ_XYZ :157-247), x/y theta fluxes, St ----
     if (col_ok) {
         auto pt_tz = [&](int L, double &pt, double &tz) {
@@ -301,7 +365,7 @@ __global__ void __launch_bounds__(32 * HEVI_COL_TC, HEVI_COL_MINB) k_hevi_stage(
                 ti = ip4<S>(mZ, Pm1, P0, P1, P2);
             }
             pt = pi;
-            tz = mZ * ti + CL(nd.TZ, L);
+            tz = mZ * ti + lds(nd.TZ + col + L - 1);
         };
         for (int L = KS + lane; L <= KE; L += 32) {
             const size_t c = col + L - 1;
@@ -334,11 +398,16 @@ __global__ void __launch_bounds__(32 * HEVI_COL_TC, HEVI_COL_MINB) k_hevi_stage(
             const double rcdz = ld(g.RCDZ + L - 1);
             SA(CA_PT, w, L) = PT;
             SA(CA_TZ, w, L) = tZ;
-            SA(CA_ST, w, L) = (-(tZ - tZm) * rcdz + adv_t) + ld(a.RHOT_t + c); // hevi_st :646-649
+            SA(CA_ST, w, L) = (-(tZ - tZm) * rcdz + adv_t) + lds(a.RHOT_t + c); // hevi_st :646-649
         }
     }
     __syncthreads();
 
+    {
+        const double *f[] = {a.MOMX0, a.MOMY0, a.MOMX_t, a.MOMY_t, nd.UZ, nd.UX, nd.UY, nd.VZ, nd.VX, nd.VY,
+                             rk_reads ? a.acc + 2 * N3 : nullptr, rk_reads ? a.acc + 3 * N3 : nullptr};
+        prefetch(f, 12);
+    }
     // ---- phase 3: Sw (hevi_sw :528-578) and the right-hand side C(k), k = KS..KE-1 (:698-722) ----
     if (col_ok) {
         // vertical w-momentum flux above level k, fluxZ_XYW (ud3.F90:358-452), zero outside KS..KE-2
@@ -348,7 +417,7 @@ __global__ void __launch_bounds__(32 * HEVI_COL_TC, HEVI_COL_MINB) k_hevi_stage(
             const double vel = (0.5 * (Mk + Mk1)) / CL(a.DENS, k + 1);
             const double q = (k == KS) ? ipL<S>(vel, Mk, Mk1, CL(a.MOMZ, k + 2))
                                        : ip4<S>(vel, CL(a.MOMZ, k - 1), Mk, Mk1, CL(a.MOMZ, k + 2));
-            return J33G * vel * q + CL(nd.WZ, k + 1);
+            return J33G * vel * q + lds(nd.WZ + col + k);
         };
         auto dpres = [&](int L) { return CL(a.DPRES0, L) + CL(a.RT2P, L) * (CL(a.RHOT, L) - CL(a.REF_rhot, L)); }; // :355
         for (int k = KS + lane; k <= KE - 1; k += 32) {
@@ -357,17 +426,23 @@ __global__ void __launch_bounds__(32 * HEVI_COL_TC, HEVI_COL_MINB) k_hevi_stage(
             const double advcv = -(qZ_at(k) - qZ_at(k - 1)) * ld(g.RFDZ + k - 1);
             const double wdmp = -ld(a.wdamp + k - 1) * CL(a.MOMZ0, k);
             const double div = use_div ? ddc * (CL(a.DDIV, k + 1) - CL(a.DDIV, k)) * ld(g.FDZ + k - 1) : 0.0;
-            const double Sw = (advcv + adv_w) + wdmp + div + CL(a.MOMZ_t, k);
+            const double Sw = (advcv + adv_w) + wdmp + div + lds(a.MOMZ_t + c);
             const double rfdz = ld(g.RFDZ + k - 1);
             const double RTL1 = CL(a.RT2P, k + 1), RTL0 = CL(a.RT2P, k);
             const double pg = -(dpres(k + 1) + RTL1 * dt * SA(CA_ST, w, k + 1) - dpres(k) - RTL0 * dt * SA(CA_ST, w, k)) * rfdz * J33G
-                              - GRAV * (ld(g.F2H1 + k - 1) * (CL(a.DENS, k + 1) - CL(a.REF_dens, k + 1) + SA(CA_SR, w, k + 1) * dt)
-                                        + ld(g.F2H2 + k - 1) * (CL(a.DENS, k) - CL(a.REF_dens, k) + SA(CA_SR, w, k) * dt));
+                              - GRAV * (ld(g.F2H1 + k - 1) * (CL(a.DENS, k + 1) - lds(a.REF_dens + c + 1) + SA(CA_SR, w, k + 1) * dt)
+                                        + ld(g.F2H2 + k - 1) * (CL(a.DENS, k) - lds(a.REF_dens + c) + SA(CA_SR, w, k) * dt));
             SA(CA_C, w, k) = CL(a.MOMZ, k) + dt * (pg + Sw);
         }
     }
     __syncthreads();
 
+    {
+        const double *f[] = {a.DENS0, a.RHOT0, rk_reads ? a.acc : nullptr, rk_reads ? a.acc + N3 : nullptr,
+                             rk_reads ? a.acc + 4 * N3 : nullptr, rk_reads ? a.facc : nullptr,
+                             rk_reads ? a.facc + 3 * N3 : nullptr};
+        prefetch(f, 7);
+    }
     // ---- phase 4: Thomas solve (warp 0) while the other warps update rho*u, rho*v ----
     if (w == 0) {
         if (lane < TC && i0 + lane <= g.IE) {
@@ -436,8 +511,8 @@ __global__ void __launch_bounds__(32 * HEVI_COL_TC, HEVI_COL_MINB) k_hevi_stage(
                 adr = -(Cm - Cm1) * J33G * rcdz;
                 adt = -(Cm * SA(CA_PT, w, m) - Cm1 * SA(CA_PT, w, m - 1)) * J33G * rcdz;
             }
-            put_state(a, N3, 0, a.DENS_RK, a.DENS0, c, ld(a.DENS0 + c) + dt * (adr + SA(CA_SR, w, m)), true);
-            put_state(a, N3, 4, a.RHOT_RK, a.RHOT0, c, ld(a.RHOT0 + c) + dt * (adt + SA(CA_ST, w, m)), true);
+            put_state(a, N3, 0, a.DENS_RK, a.DENS0, c, lds(a.DENS0 + c) + dt * (adr + SA(CA_SR, w, m)), true);
+            put_state(a, N3, 4, a.RHOT_RK, a.RHOT0, c, lds(a.RHOT0 + c) + dt * (adt + SA(CA_ST, w, m)), true);
             if (m <= KE - 1) {
                 put_state(a, N3, 1, a.MOMZ_RK, a.MOMZ0, c, ld(a.MOMZ0 + c) + (Cm - ld(a.MOMZ + c)), true);
                 put_flux(a, N3, 0, c, ld(nd.DZ + c) + J33G * Cm, true);
@@ -457,7 +532,7 @@ __global__ void __launch_bounds__(32 * HEVI_COL_TC, HEVI_COL_MINB) k_hevi_stage(
     }
     // hevi_mflx_z :369-393 also fills the halo column i = IS-1 with the explicit
     // part of the vertical mass flux; the solver never updates it
-    if (blockIdx.x == 0 && w == TC - 1 && (a.rk_mode == RK_PLAIN || a.rk_mode == RK_FINAL)) {
+    if (ti == 0 && w == TC - 1 && (a.rk_mode == RK_PLAIN || a.rk_mode == RK_FINAL)) {
         const size_t ch = idx3(g, 1, g.IS - 1, j);
         for (int k = KS - 1 + lane; k <= KE; k += 32)
             a.mflx[ch + k - 1] = (k >= KS && k <= KE - 1) ? ld(nd.DZ + ch + k - 1) : 0.0;
