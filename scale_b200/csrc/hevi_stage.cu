@@ -35,6 +35,9 @@
 #ifndef HEVI_STREAM_HINTS
 #define HEVI_STREAM_HINTS 1 // evict-first loads/stores for data each cell touches once
 #endif
+#ifndef HEVI_SPLIT_ROLES
+#define HEVI_SPLIT_ROLES 0 // rho*u/rho*v in CTAs of their own, interleaved with the column CTAs
+#endif
 #ifndef HEVI_L2_PREFETCH
 #define HEVI_L2_PREFETCH 0 // bulk L2 prefetch of the tile's columns one phase ahead
 #endif
@@ -112,14 +115,28 @@ __device__ __forceinline__ void l2_prefetch(const double *p, unsigned n)
 // =============================================================================
 // per-cell pieces shared by the phases (c = offset of cell (k,i,j))
 // =============================================================================
+// num_diff components by (quantity, direction), computed at each use from the
+// kernel parameters so that no register holds fifteen pointers
 struct Nd {
-    const double *DX, *DY, *DZ, *WX, *WY, *WZ, *UZ, *UX, *UY, *VZ, *VX, *VY, *TX, *TY, *TZ;
-    __device__ Nd(const StageArgs &a, size_t N3)
-        : DX(nd_slice(a, N3, 1, 2)), DY(nd_slice(a, N3, 1, 3)), DZ(nd_slice(a, N3, 1, 1)),
-          WX(nd_slice(a, N3, 2, 2)), WY(nd_slice(a, N3, 2, 3)), WZ(nd_slice(a, N3, 2, 1)),
-          UZ(nd_slice(a, N3, 3, 1)), UX(nd_slice(a, N3, 3, 2)), UY(nd_slice(a, N3, 3, 3)),
-          VZ(nd_slice(a, N3, 4, 1)), VX(nd_slice(a, N3, 4, 2)), VY(nd_slice(a, N3, 4, 3)),
-          TX(nd_slice(a, N3, 5, 2)), TY(nd_slice(a, N3, 5, 3)), TZ(nd_slice(a, N3, 5, 1)) {}
+    const double *base;
+    size_t N3;
+    __device__ Nd(const StageArgs &a, size_t n) : base(a.num_diff), N3(n) {}
+    __device__ const double *q(int v, int dir) const { return base + N3 * (size_t)((v - 1) + 5 * (dir - 1)); }
+    __device__ const double *DZ() const { return q(1, 1); }
+    __device__ const double *DX() const { return q(1, 2); }
+    __device__ const double *DY() const { return q(1, 3); }
+    __device__ const double *WZ() const { return q(2, 1); }
+    __device__ const double *WX() const { return q(2, 2); }
+    __device__ const double *WY() const { return q(2, 3); }
+    __device__ const double *UZ() const { return q(3, 1); }
+    __device__ const double *UX() const { return q(3, 2); }
+    __device__ const double *UY() const { return q(3, 3); }
+    __device__ const double *VZ() const { return q(4, 1); }
+    __device__ const double *VX() const { return q(4, 2); }
+    __device__ const double *VY() const { return q(4, 3); }
+    __device__ const double *TZ() const { return q(5, 1); }
+    __device__ const double *TX() const { return q(5, 2); }
+    __device__ const double *TY() const { return q(5, 3); }
 };
 
 #define AT(p, dk, di, dj) ld((p) + c + (long)(dk) + (long)(di) * sI + (long)(dj) * sJ)
@@ -129,10 +146,10 @@ struct MassFlux { double Xe, Xw, Yn, Ys; };
 __device__ __forceinline__ MassFlux mass_flux(const StageArgs &a, const Nd &nd, size_t c, long sI, long sJ)
 {
     MassFlux m;
-    m.Xe = AT(a.MOMX, 0, 0, 0) + AT(nd.DX, 0, 0, 0);
-    m.Xw = AT(a.MOMX, 0, -1, 0) + AT(nd.DX, 0, -1, 0);
-    m.Yn = AT(a.MOMY, 0, 0, 0) + AT(nd.DY, 0, 0, 0);
-    m.Ys = AT(a.MOMY, 0, 0, -1) + AT(nd.DY, 0, 0, -1);
+    m.Xe = AT(a.MOMX, 0, 0, 0) + AT(nd.DX(), 0, 0, 0);
+    m.Xw = AT(a.MOMX, 0, -1, 0) + AT(nd.DX(), 0, -1, 0);
+    m.Yn = AT(a.MOMY, 0, 0, 0) + AT(nd.DY(), 0, 0, 0);
+    m.Ys = AT(a.MOMY, 0, 0, -1) + AT(nd.DY(), 0, 0, -1);
     return m;
 }
 
@@ -155,60 +172,88 @@ __device__ __forceinline__ double adv_w_h(const Grid &g, const StageArgs &a, con
     const double W_m2 = AT(MZ, 0, -2, 0), W_m1 = AT(MZ, 0, -1, 0), W_00 = AT(MZ, 0, 0, 0);
     const double W_p1 = AT(MZ, 0, 1, 0), W_p2 = AT(MZ, 0, 2, 0);
     const double V_m2 = AT(MZ, 0, 0, -2), V_m1 = AT(MZ, 0, 0, -1), V_p1 = AT(MZ, 0, 0, 1), V_p2 = AT(MZ, 0, 0, 2);
-    const double qXe = vXe * ip4<S>(vXe, W_m1, W_00, W_p1, W_p2) + AT(nd.WX, 0, 0, 0);
-    const double qXw = vXw * ip4<S>(vXw, W_m2, W_m1, W_00, W_p1) + AT(nd.WX, 0, -1, 0);
-    const double qYn = vYn * ip4<S>(vYn, V_m1, W_00, V_p1, V_p2) + AT(nd.WY, 0, 0, 0);
-    const double qYs = vYs * ip4<S>(vYs, V_m2, V_m1, W_00, V_p1) + AT(nd.WY, 0, 0, -1);
+    const double qXe = vXe * ip4<S>(vXe, W_m1, W_00, W_p1, W_p2) + AT(nd.WX(), 0, 0, 0);
+    const double qXw = vXw * ip4<S>(vXw, W_m2, W_m1, W_00, W_p1) + AT(nd.WX(), 0, -1, 0);
+    const double qYn = vYn * ip4<S>(vYn, V_m1, W_00, V_p1, V_p2) + AT(nd.WY(), 0, 0, 0);
+    const double qYs = vYs * ip4<S>(vYs, V_m2, V_m1, W_00, V_p1) + AT(nd.WY(), 0, 0, -1);
     return -((qXe - qXw) * rcdx + (qYn - qYs) * rcdy);
 }
 
-// rho*u and rho*v of cell (k,i,j), hevi_momx :814-928 and hevi_momy :934-1048
-template <int S>
-__device__ __forceinline__ void update_momxy(const Grid &g, const StageArgs &a, const Nd &nd, size_t N3, int k, int i, int j)
+// rho*u and rho*v of cell (k,i,j), hevi_momx :814-928 and hevi_momy :934-1048.
+// Called by all 32 lanes of a warp for 32 consecutive levels of one column;
+// 'valid' is false for lanes above KE. The z-face flux below a level is the
+// one above the level of the previous lane, passed by a warp shuffle.
+template <int S, int V>
+__device__ __forceinline__ void update_mom(const Grid &g, const StageArgs &a, const Nd &nd, size_t N3, int k, int i, int j,
+                                           bool valid)
 {
     const size_t c = idx3(g, k, i, j);
     const long sI = g.KA, sJ = (long)g.KA * g.IA;
     const double *MX = a.MOMX, *MY = a.MOMY, *MZ = a.MOMZ, *DN = a.DENS, *RT = a.RHOT;
-    const double rcdx = ld(g.RCDX + i - 1), rcdy = ld(g.RCDY + j - 1);
-    const double rfdx = ld(g.RFDX + i - 1), rfdy = ld(g.RFDY + j - 1);
-    const double fdx = ld(g.FDX + i - 1), fdy = ld(g.FDY + j - 1);
     const double dt = a.dtrk, J33G = a.J33G;
     const bool use_div = a.divdmp_coef != 0.0;
     const double ddc = use_div ? a.divdmp_coef / dt : 0.0;
     const int KS = g.KS, KE = g.KE;
+    const unsigned FULL = 0xffffffffu;
+
+    // z flux at (u,y,w), fluxZ_UYZ (ud3.F90:753-859); m is the lower level of the face
+    auto qZu = [&](int m) -> double {
+        if (m < KS || m > KE - 1) return 0.0;
+        const long dm = m - k;
+        const double den = ld(g.F2H1 + m - 1) * 0.5 * (AT(DN, dm + 1, 0, 0) + AT(DN, dm + 1, 1, 0))
+                           + ld(g.F2H2 + m - 1) * 0.5 * (AT(DN, dm, 0, 0) + AT(DN, dm, 1, 0));
+        const double vel = (0.5 * (AT(MZ, dm, 0, 0) + AT(MZ, dm, 1, 0))) / den;
+        double q;
+        if (m == KS) q = ipL<S>(vel, AT(MX, dm, 0, 0), AT(MX, dm + 1, 0, 0), AT(MX, dm + 2, 0, 0));
+        else if (m == KE - 1) q = ipH<S>(vel, AT(MX, dm + 1, 0, 0), AT(MX, dm, 0, 0), AT(MX, dm - 1, 0, 0));
+        else q = ip4<S>(vel, AT(MX, dm - 1, 0, 0), AT(MX, dm, 0, 0), AT(MX, dm + 1, 0, 0), AT(MX, dm + 2, 0, 0));
+        return J33G * vel * q + lds(nd.UZ() + c + dm);
+    };
+    // z flux at (x,v,w), fluxZ_XVZ (ud3.F90:1173-1279)
+    auto qZv = [&](int m) -> double {
+        if (m < KS || m > KE - 1) return 0.0;
+        const long dm = m - k;
+        const double den = ld(g.F2H1 + m - 1) * 0.5 * (AT(DN, dm + 1, 0, 0) + AT(DN, dm + 1, 0, 1))
+                           + ld(g.F2H2 + m - 1) * 0.5 * (AT(DN, dm, 0, 0) + AT(DN, dm, 0, 1));
+        const double vel = (0.5 * (AT(MZ, dm, 0, 0) + AT(MZ, dm, 0, 1))) / den;
+        double q;
+        if (m == KS) q = ipL<S>(vel, AT(MY, dm, 0, 0), AT(MY, dm + 1, 0, 0), AT(MY, dm + 2, 0, 0));
+        else if (m == KE - 1) q = ipH<S>(vel, AT(MY, dm + 1, 0, 0), AT(MY, dm, 0, 0), AT(MY, dm - 1, 0, 0));
+        else q = ip4<S>(vel, AT(MY, dm - 1, 0, 0), AT(MY, dm, 0, 0), AT(MY, dm + 1, 0, 0), AT(MY, dm + 2, 0, 0));
+        return J33G * vel * q + lds(nd.VZ() + c + dm);
+    };
+
+    // the flux through the face above this level; the one below comes from the
+    // lane of the level below (lane 0 computes it)
+    // V = 0: rho*u (the face is u-staggered), V = 1: rho*v
+    const bool do_u = V == 0 && i <= g.IEH, do_v = V == 1 && j <= g.JEH;
+    if (!do_u && !do_v) return; // warp-uniform
+    const double q_k = valid ? (V == 0 ? qZu(k) : qZv(k)) : 0.0;
+    double q_km = __shfl_up_sync(FULL, q_k, 1);
+    if (!valid) return;
+    if (threadIdx.x == 0) q_km = V == 0 ? qZu(k - 1) : qZv(k - 1);
+
     // pressure deviation at the cell and its +x/+y neighbours, hevi_pres :355
     const double DP00 = AT(a.DPRES0, 0, 0, 0) + AT(a.RT2P, 0, 0, 0) * (AT(RT, 0, 0, 0) - AT(a.REF_rhot, 0, 0, 0));
 
-    if (i <= g.IEH) {
+    if (do_u) {
+        const double rcdy = ld(g.RCDY + j - 1), rfdx = ld(g.RFDX + i - 1), fdx = ld(g.FDX + i - 1);
         const double cor_u = 0.125 * (ld(a.CORIOLI + (i) + (size_t)g.IA * (j - 1)) + ld(a.CORIOLI + (i - 1) + (size_t)g.IA * (j - 1)));
-        // z flux at (u,y,w), fluxZ_UYZ (ud3.F90:753-859); m is the lower level of the face
-        auto qZu = [&](int m) -> double {
-            if (m < KS || m > KE - 1) return 0.0;
-            const long dm = m - k;
-            const double den = ld(g.F2H1 + m - 1) * 0.5 * (AT(DN, dm + 1, 0, 0) + AT(DN, dm + 1, 1, 0))
-                               + ld(g.F2H2 + m - 1) * 0.5 * (AT(DN, dm, 0, 0) + AT(DN, dm, 1, 0));
-            const double vel = (0.5 * (AT(MZ, dm, 0, 0) + AT(MZ, dm, 1, 0))) / den;
-            double q;
-            if (m == KS) q = ipL<S>(vel, AT(MX, dm, 0, 0), AT(MX, dm + 1, 0, 0), AT(MX, dm + 2, 0, 0));
-            else if (m == KE - 1) q = ipH<S>(vel, AT(MX, dm + 1, 0, 0), AT(MX, dm, 0, 0), AT(MX, dm - 1, 0, 0));
-            else q = ip4<S>(vel, AT(MX, dm - 1, 0, 0), AT(MX, dm, 0, 0), AT(MX, dm + 1, 0, 0), AT(MX, dm + 2, 0, 0));
-            return J33G * vel * q + lds(nd.UZ + c + dm);
-        };
         const double U_m2 = AT(MX, 0, -2, 0), U_m1 = AT(MX, 0, -1, 0), U_00 = AT(MX, 0, 0, 0);
         const double U_p1 = AT(MX, 0, 1, 0), U_p2 = AT(MX, 0, 2, 0);
         // x flux at (x,y,z) with the index shift of fluxX_UYZ (ud3.F90:1053-1109)
         const double vE = (0.5 * (U_p1 + U_00)) / (AT(DN, 0, 1, 0));
-        const double qXe = vE * ip4<S>(vE, U_m1, U_00, U_p1, U_p2) + AT(nd.UX, 0, 1, 0);
+        const double qXe = vE * ip4<S>(vE, U_m1, U_00, U_p1, U_p2) + AT(nd.UX(), 0, 1, 0);
         const double vW = (0.5 * (U_00 + U_m1)) / (AT(DN, 0, 0, 0));
-        const double qXw = vW * ip4<S>(vW, U_m2, U_m1, U_00, U_p1) + AT(nd.UX, 0, 0, 0);
+        const double qXw = vW * ip4<S>(vW, U_m2, U_m1, U_00, U_p1) + AT(nd.UX(), 0, 0, 0);
         // y flux at (u,v,z), fluxY_UYZ (ud3.F90:1113-1167)
         const double vN = (0.5 * (AT(MY, 0, 0, 0) + AT(MY, 0, 1, 0)))
                           / (0.25 * (AT(DN, 0, 0, 0) + AT(DN, 0, 1, 0) + AT(DN, 0, 0, 1) + AT(DN, 0, 1, 1)));
-        const double qYn = vN * ip4<S>(vN, AT(MX, 0, 0, -1), U_00, AT(MX, 0, 0, 1), AT(MX, 0, 0, 2)) + AT(nd.UY, 0, 0, 0);
+        const double qYn = vN * ip4<S>(vN, AT(MX, 0, 0, -1), U_00, AT(MX, 0, 0, 1), AT(MX, 0, 0, 2)) + AT(nd.UY(), 0, 0, 0);
         const double vS = (0.5 * (AT(MY, 0, 0, -1) + AT(MY, 0, 1, -1)))
                           / (0.25 * (AT(DN, 0, 0, -1) + AT(DN, 0, 1, -1) + AT(DN, 0, 0, 0) + AT(DN, 0, 1, 0)));
-        const double qYs = vS * ip4<S>(vS, AT(MX, 0, 0, -2), AT(MX, 0, 0, -1), U_00, AT(MX, 0, 0, 1)) + AT(nd.UY, 0, 0, -1);
-        const double advcv = -(qZu(k) - qZu(k - 1)) * ld(g.RCDZ + k - 1);
+        const double qYs = vS * ip4<S>(vS, AT(MX, 0, 0, -2), AT(MX, 0, 0, -1), U_00, AT(MX, 0, 0, 1)) + AT(nd.UY(), 0, 0, -1);
+        const double advcv = -(q_k - q_km) * ld(g.RCDZ + k - 1);
         const double advch = -((qXe - qXw) * rfdx + (qYn - qYs) * rcdy);
         const double DPe = AT(a.DPRES0, 0, 1, 0) + AT(a.RT2P, 0, 1, 0) * (AT(RT, 0, 1, 0) - AT(a.REF_rhot, 0, 1, 0));
         const double pg = (DPe - DP00) * rfdx;
@@ -218,35 +263,24 @@ __device__ __forceinline__ void update_momxy(const Grid &g, const StageArgs &a, 
         put_state(a, N3, 2, a.MOMX_RK, a.MOMX0, c, val, true);
     }
 
-    if (j <= g.JEH) {
+    if (do_v) {
+        const double rcdx = ld(g.RCDX + i - 1), rfdy = ld(g.RFDY + j - 1), fdy = ld(g.FDY + j - 1);
         const double cor_v = -0.125 * (ld(a.CORIOLI + (i - 1) + (size_t)g.IA * (j)) + ld(a.CORIOLI + (i - 1) + (size_t)g.IA * (j - 1)));
-        auto qZv = [&](int m) -> double {
-            if (m < KS || m > KE - 1) return 0.0;
-            const long dm = m - k;
-            const double den = ld(g.F2H1 + m - 1) * 0.5 * (AT(DN, dm + 1, 0, 0) + AT(DN, dm + 1, 0, 1))
-                               + ld(g.F2H2 + m - 1) * 0.5 * (AT(DN, dm, 0, 0) + AT(DN, dm, 0, 1));
-            const double vel = (0.5 * (AT(MZ, dm, 0, 0) + AT(MZ, dm, 0, 1))) / den;
-            double q;
-            if (m == KS) q = ipL<S>(vel, AT(MY, dm, 0, 0), AT(MY, dm + 1, 0, 0), AT(MY, dm + 2, 0, 0));
-            else if (m == KE - 1) q = ipH<S>(vel, AT(MY, dm + 1, 0, 0), AT(MY, dm, 0, 0), AT(MY, dm - 1, 0, 0));
-            else q = ip4<S>(vel, AT(MY, dm - 1, 0, 0), AT(MY, dm, 0, 0), AT(MY, dm + 1, 0, 0), AT(MY, dm + 2, 0, 0));
-            return J33G * vel * q + lds(nd.VZ + c + dm);
-        };
         const double Y_m2 = AT(MY, 0, 0, -2), Y_m1 = AT(MY, 0, 0, -1), Y_00 = AT(MY, 0, 0, 0);
         const double Y_p1 = AT(MY, 0, 0, 1), Y_p2 = AT(MY, 0, 0, 2);
         // x flux at (u,v,z), fluxX_XVZ (ud3.F90:1473-1527)
         const double vE = (0.5 * (AT(MX, 0, 0, 0) + AT(MX, 0, 0, 1)))
                           / (0.25 * (AT(DN, 0, 0, 0) + AT(DN, 0, 1, 0) + AT(DN, 0, 0, 1) + AT(DN, 0, 1, 1)));
-        const double qXe = vE * ip4<S>(vE, AT(MY, 0, -1, 0), Y_00, AT(MY, 0, 1, 0), AT(MY, 0, 2, 0)) + AT(nd.VX, 0, 0, 0);
+        const double qXe = vE * ip4<S>(vE, AT(MY, 0, -1, 0), Y_00, AT(MY, 0, 1, 0), AT(MY, 0, 2, 0)) + AT(nd.VX(), 0, 0, 0);
         const double vW = (0.5 * (AT(MX, 0, -1, 0) + AT(MX, 0, -1, 1)))
                           / (0.25 * (AT(DN, 0, -1, 0) + AT(DN, 0, 0, 0) + AT(DN, 0, -1, 1) + AT(DN, 0, 0, 1)));
-        const double qXw = vW * ip4<S>(vW, AT(MY, 0, -2, 0), AT(MY, 0, -1, 0), Y_00, AT(MY, 0, 1, 0)) + AT(nd.VX, 0, -1, 0);
+        const double qXw = vW * ip4<S>(vW, AT(MY, 0, -2, 0), AT(MY, 0, -1, 0), Y_00, AT(MY, 0, 1, 0)) + AT(nd.VX(), 0, -1, 0);
         // y flux with the index shift of fluxY_XVZ (ud3.F90:1531-1587)
         const double vN = (0.5 * (Y_p1 + Y_00)) / (AT(DN, 0, 0, 1));
-        const double qYn = vN * ip4<S>(vN, Y_m1, Y_00, Y_p1, Y_p2) + AT(nd.VY, 0, 0, 1);
+        const double qYn = vN * ip4<S>(vN, Y_m1, Y_00, Y_p1, Y_p2) + AT(nd.VY(), 0, 0, 1);
         const double vS = (0.5 * (Y_00 + Y_m1)) / (AT(DN, 0, 0, 0));
-        const double qYs = vS * ip4<S>(vS, Y_m2, Y_m1, Y_00, Y_p1) + AT(nd.VY, 0, 0, 0);
-        const double advcv = -(qZv(k) - qZv(k - 1)) * ld(g.RCDZ + k - 1);
+        const double qYs = vS * ip4<S>(vS, Y_m2, Y_m1, Y_00, Y_p1) + AT(nd.VY(), 0, 0, 0);
+        const double advcv = -(q_k - q_km) * ld(g.RCDZ + k - 1);
         const double advch = -((qXe - qXw) * rcdx + (qYn - qYs) * rfdy);
         const double DPn = AT(a.DPRES0, 0, 0, 1) + AT(a.RT2P, 0, 0, 1) * (AT(RT, 0, 0, 1) - AT(a.REF_rhot, 0, 0, 1));
         const double pg = (DPn - DP00) * rfdy;
@@ -277,9 +311,14 @@ __global__ void __launch_bounds__(32 * HEVI_COL_TC, HEVI_COL_MINB) k_hevi_stage(
     const int lane = threadIdx.x, w = threadIdx.y;
     // 2-D raster: consecutive CTAs walk down HEVI_RASTER_J rows of tiles, then
     // step in i, so the CTAs resident together cover a compact patch
+    // With HEVI_SPLIT_ROLES the grid holds two CTAs per tile: even blockIdx.x
+    // runs the column work, odd blockIdx.x the rho*u/rho*v updates, so an SM
+    // holds both kinds and one kind's memory traffic covers the other's solve.
+    const bool mom_role = HEVI_SPLIT_ROLES && (blockIdx.x & 1);
+    const int bx = HEVI_SPLIT_ROLES ? (int)(blockIdx.x >> 1) : (int)blockIdx.x;
     int ti, jj;
     {
-        const int nti = gridDim.x, b = blockIdx.x + nti * blockIdx.y;
+        const int nti = HEVI_SPLIT_ROLES ? (int)(gridDim.x >> 1) : (int)gridDim.x, b = bx + nti * blockIdx.y;
         const int grp = b / (nti * HEVI_RASTER_J), rem = b - grp * (nti * HEVI_RASTER_J);
         const int rows = min(HEVI_RASTER_J, g.JMAX - grp * HEVI_RASTER_J);
         jj = grp * HEVI_RASTER_J + rem % rows;
@@ -312,11 +351,21 @@ __global__ void __launch_bounds__(32 * HEVI_COL_TC, HEVI_COL_MINB) k_hevi_stage(
         if (w == TC - 1 && lane < n) l2_prefetch(f[lane] ? f[lane] + tile0 : nullptr, tile_bytes);
     };
     {
-        const double *f[] = {a.RHOT, a.DENS, a.MOMX, a.MOMY, nd.DX, nd.DY, nd.DZ, a.DENS_t, a.RT2P,
+        const double *f[] = {a.RHOT, a.DENS, a.MOMX, a.MOMY, nd.DX(), nd.DY(), nd.DZ(), a.DENS_t, a.RT2P,
                              rk_reads ? a.facc + N3 : nullptr, rk_reads ? a.facc + 2 * N3 : nullptr,
-                             a.MOMZ, nd.TZ, nd.TX, nd.TY, a.RHOT_t,
+                             a.MOMZ, nd.TZ(), nd.TX(), nd.TY(), a.RHOT_t,
                              rk_reads ? a.facc + 4 * N3 : nullptr, rk_reads ? a.facc + 5 * N3 : nullptr};
         prefetch(f, 18);
+    }
+
+    if (mom_role) {
+        // rho*u and rho*v of this warp's column (hevi_momx :814-928, hevi_momy :934-1048)
+        if (col_ok)
+            for (int L0 = KS; L0 <= KE; L0 += 32) {
+                update_mom<S, 0>(g, a, nd, N3, L0 + lane, i, j, L0 + lane <= KE);
+                update_mom<S, 1>(g, a, nd, N3, L0 + lane, i, j, L0 + lane <= KE);
+            }
+        return;
     }
 
     // ---- phase 1: POTT (:586-600), x/y mass fluxes (:399-438), Sr (:443-479), A (:696) ----
@@ -330,8 +379,8 @@ __global__ void __launch_bounds__(32 * HEVI_COL_TC, HEVI_COL_MINB) k_hevi_stage(
             put_flux(a, N3, 2, c, m.Yn, true);
             if (i == g.IS) put_flux(a, N3, 1, c - sI, m.Xw, false);
             if (j == g.JS) put_flux(a, N3, 2, c - sJ, m.Ys, false);
-            const double mZ = (L <= KE - 1) ? ld(nd.DZ + c) : 0.0; // hevi_mflx_z :383-391 (flat terrain)
-            const double mZm1 = (L - 1 >= KS) ? ld(nd.DZ + c - 1) : 0.0;
+            const double mZ = (L <= KE - 1) ? ld(nd.DZ() + c) : 0.0; // hevi_mflx_z :383-391 (flat terrain)
+            const double mZm1 = (L - 1 >= KS) ? ld(nd.DZ() + c - 1) : 0.0;
             const double rcdz = ld(g.RCDZ + L - 1);
             SA(CA_SR, w, L) = (-(mZ - mZm1) * rcdz + adv_r) + lds(a.DENS_t + c);
             SA(CA_A, w, L) = dt2 * J33G * rcdz * ld(a.RT2P + c) * J33G;
@@ -340,7 +389,7 @@ __global__ void __launch_bounds__(32 * HEVI_COL_TC, HEVI_COL_MINB) k_hevi_stage(
     __syncthreads();
 
     {
-        const double *f[] = {a.MOMZ0, a.MOMZ_t, a.DPRES0, a.REF_rhot, a.REF_dens, nd.WZ, nd.WX, nd.WY,
+        const double *f[] = {a.MOMZ0, a.MOMZ_t, a.DPRES0, a.REF_rhot, a.REF_dens, nd.WZ(), nd.WX(), nd.WY(),
                              use_div ? a.DDIV : nullptr};
         prefetch(f, 9);
     }
@@ -348,7 +397,7 @@ __global__ void __launch_bounds__(32 * HEVI_COL_TC, HEVI_COL_MINB) k_hevi_stage(
     if (col_ok) {
         auto pt_tz = [&](int L, double &pt, double &tz) {
             if (L < KS || L > KE - 1) { pt = 0.0; tz = 0.0; return; }
-            const double mZ = CL(nd.DZ, L);
+            const double mZ = CL(nd.DZ(), L);
             const double M0 = CL(a.MOMZ, L);
             double pi, ti;
             if (L == KS) {
@@ -365,7 +414,7 @@ __global__ void __launch_bounds__(32 * HEVI_COL_TC, HEVI_COL_MINB) k_hevi_stage(
                 ti = ip4<S>(mZ, Pm1, P0, P1, P2);
             }
             pt = pi;
-            tz = mZ * ti + lds(nd.TZ + col + L - 1);
+            tz = mZ * ti + lds(nd.TZ() + col + L - 1);
         };
         for (int L = KS + lane; L <= KE; L += 32) {
             const size_t c = col + L - 1;
@@ -386,10 +435,10 @@ __global__ void __launch_bounds__(32 * HEVI_COL_TC, HEVI_COL_MINB) k_hevi_stage(
             const double Qp2 = AT(a.RHOT, 0, 0, 2) / AT(a.DENS, 0, 0, 2);
             const MassFlux m = mass_flux(a, nd, c, sI, sJ);
             // fluxX/Y_XYZ (ud3.F90:251-353)
-            const double tXe = m.Xe * ip4<S>(m.Xe, Pm1, P00, Pp1, Pp2) + AT(nd.TX, 0, 0, 0);
-            const double tXw = m.Xw * ip4<S>(m.Xw, Pm2, Pm1, P00, Pp1) + AT(nd.TX, 0, -1, 0);
-            const double tYn = m.Yn * ip4<S>(m.Yn, Qm1, P00, Qp1, Qp2) + AT(nd.TY, 0, 0, 0);
-            const double tYs = m.Ys * ip4<S>(m.Ys, Qm2, Qm1, P00, Qp1) + AT(nd.TY, 0, 0, -1);
+            const double tXe = m.Xe * ip4<S>(m.Xe, Pm1, P00, Pp1, Pp2) + AT(nd.TX(), 0, 0, 0);
+            const double tXw = m.Xw * ip4<S>(m.Xw, Pm2, Pm1, P00, Pp1) + AT(nd.TX(), 0, -1, 0);
+            const double tYn = m.Yn * ip4<S>(m.Yn, Qm1, P00, Qp1, Qp2) + AT(nd.TY(), 0, 0, 0);
+            const double tYs = m.Ys * ip4<S>(m.Ys, Qm2, Qm1, P00, Qp1) + AT(nd.TY(), 0, 0, -1);
             const double adv_t = -((tXe - tXw) * rcdx + (tYn - tYs) * rcdy); // hevi_st :646-648
             put_flux(a, N3, 4, c, tXe, true);
             put_flux(a, N3, 5, c, tYn, true);
@@ -404,7 +453,7 @@ __global__ void __launch_bounds__(32 * HEVI_COL_TC, HEVI_COL_MINB) k_hevi_stage(
     __syncthreads();
 
     {
-        const double *f[] = {a.MOMX0, a.MOMY0, a.MOMX_t, a.MOMY_t, nd.UZ, nd.UX, nd.UY, nd.VZ, nd.VX, nd.VY,
+        const double *f[] = {a.MOMX0, a.MOMY0, a.MOMX_t, a.MOMY_t, nd.UZ(), nd.UX(), nd.UY(), nd.VZ(), nd.VX(), nd.VY(),
                              rk_reads ? a.acc + 2 * N3 : nullptr, rk_reads ? a.acc + 3 * N3 : nullptr};
         prefetch(f, 12);
     }
@@ -417,13 +466,20 @@ __global__ void __launch_bounds__(32 * HEVI_COL_TC, HEVI_COL_MINB) k_hevi_stage(
             const double vel = (0.5 * (Mk + Mk1)) / CL(a.DENS, k + 1);
             const double q = (k == KS) ? ipL<S>(vel, Mk, Mk1, CL(a.MOMZ, k + 2))
                                        : ip4<S>(vel, CL(a.MOMZ, k - 1), Mk, Mk1, CL(a.MOMZ, k + 2));
-            return J33G * vel * q + lds(nd.WZ + col + k);
+            return J33G * vel * q + lds(nd.WZ() + col + k);
         };
         auto dpres = [&](int L) { return CL(a.DPRES0, L) + CL(a.RT2P, L) * (CL(a.RHOT, L) - CL(a.REF_rhot, L)); }; // :355
-        for (int k = KS + lane; k <= KE - 1; k += 32) {
+        for (int k0 = KS; k0 <= KE - 1; k0 += 32) {
+            const int k = k0 + lane;
+            const bool ok = k <= KE - 1;
+            // the flux above level k; the one below is the previous lane's (lane 0 computes it)
+            const double q_k = ok ? qZ_at(k) : 0.0;
+            double q_km = __shfl_up_sync(0xffffffffu, q_k, 1);
+            if (!ok) continue;
+            if (lane == 0) q_km = qZ_at(k - 1);
             const size_t c = col + k - 1;
             const double adv_w = adv_w_h<S>(g, a, nd, c, k, sI, sJ, rcdx, rcdy);
-            const double advcv = -(qZ_at(k) - qZ_at(k - 1)) * ld(g.RFDZ + k - 1);
+            const double advcv = -(q_k - q_km) * ld(g.RFDZ + k - 1);
             const double wdmp = -ld(a.wdamp + k - 1) * CL(a.MOMZ0, k);
             const double div = use_div ? ddc * (CL(a.DDIV, k + 1) - CL(a.DDIV, k)) * ld(g.FDZ + k - 1) : 0.0;
             const double Sw = (advcv + adv_w) + wdmp + div + lds(a.MOMZ_t + c);
@@ -483,13 +539,16 @@ __global__ void __launch_bounds__(32 * HEVI_COL_TC, HEVI_COL_MINB) k_hevi_stage(
             SA(CA_PT, cc, KS - 1) = 0.0;
         }
     }
-    if (w > 0 || TC == 1) {
-        // rho*u / rho*v of the tile: (column, 32-level chunk) items over the worker warps
+    if (!HEVI_SPLIT_ROLES && (w > 0 || TC == 1)) {
+        // rho*u / rho*v of the tile: (column, 32-level chunk, component) items over the worker warps
         const int nworkers = TC > 1 ? TC - 1 : 1, wid = TC > 1 ? w - 1 : 0;
         const int NL = (g.KMAX + 31) / 32;
-        for (int it = wid; it < TC * NL; it += nworkers) {
-            const int ii = i0 + it / NL, L = KS + (it % NL) * 32 + lane;
-            if (ii <= g.IE && L <= KE) update_momxy<S>(g, a, nd, N3, L, ii, j);
+        for (int it = wid; it < 2 * TC * NL; it += nworkers) {
+            const int item = it >> 1, ii = i0 + item / NL, L = KS + (item % NL) * 32 + lane;
+            if (ii <= g.IE) { // warp-uniform branch
+                if (it & 1) update_mom<S, 1>(g, a, nd, N3, L, ii, j, L <= KE);
+                else update_mom<S, 0>(g, a, nd, N3, L, ii, j, L <= KE);
+            }
         }
     }
     __syncthreads();
@@ -515,7 +574,7 @@ __global__ void __launch_bounds__(32 * HEVI_COL_TC, HEVI_COL_MINB) k_hevi_stage(
             put_state(a, N3, 4, a.RHOT_RK, a.RHOT0, c, lds(a.RHOT0 + c) + dt * (adt + SA(CA_ST, w, m)), true);
             if (m <= KE - 1) {
                 put_state(a, N3, 1, a.MOMZ_RK, a.MOMZ0, c, ld(a.MOMZ0 + c) + (Cm - ld(a.MOMZ + c)), true);
-                put_flux(a, N3, 0, c, ld(nd.DZ + c) + J33G * Cm, true);
+                put_flux(a, N3, 0, c, ld(nd.DZ() + c) + J33G * Cm, true);
                 put_flux(a, N3, 3, c, SA(CA_TZ, w, m) + J33G * Cm * SA(CA_PT, w, m), true);
             } else {
                 put_state(a, N3, 1, a.MOMZ_RK, a.MOMZ0, c, 0.0, false);
@@ -535,7 +594,7 @@ __global__ void __launch_bounds__(32 * HEVI_COL_TC, HEVI_COL_MINB) k_hevi_stage(
     if (ti == 0 && w == TC - 1 && (a.rk_mode == RK_PLAIN || a.rk_mode == RK_FINAL)) {
         const size_t ch = idx3(g, 1, g.IS - 1, j);
         for (int k = KS - 1 + lane; k <= KE; k += 32)
-            a.mflx[ch + k - 1] = (k >= KS && k <= KE - 1) ? ld(nd.DZ + ch + k - 1) : 0.0;
+            a.mflx[ch + k - 1] = (k >= KS && k <= KE - 1) ? ld(nd.DZ() + ch + k - 1) : 0.0;
     }
 #undef SA
 #undef CL
@@ -561,7 +620,7 @@ cudaError_t launch_hevi_stage(const Grid &g, const StageArgs &a, int scheme, cud
         : cudaFuncSetAttribute(k_hevi_stage<CD4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     dim3 bc(32, TC);
-    dim3 gc((g.IMAX + TC - 1) / TC, g.JMAX);
+    dim3 gc((g.IMAX + TC - 1) / TC * (HEVI_SPLIT_ROLES ? 2 : 1), g.JMAX);
     if (scheme == UD3) k_hevi_stage<UD3><<<gc, bc, smem, st>>>(g, a);
     else k_hevi_stage<CD4><<<gc, bc, smem, st>>>(g, a);
     return cudaGetLastError();
