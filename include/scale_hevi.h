@@ -288,14 +288,15 @@ int scale_hevi_domain_sum_dev(const double *var, const double *CDZ, const double
  * that entry computes.
  *
  * Scratch: one fixed device array of SCALE_HEVI_NOALLOC_SCRATCH_BYTES inside
- * the library holds the status words and the 1-D grid tables, which need
- * 256 + 8*(7*KA + 4*IA + 4*JA) bytes. A larger domain is rejected with
- * SCALE_HEVI_ERR_ARG. The first call on a device looks up the array with that
- * device current. Make that first call before any stream capture. All calls
- * on a device share the array, so calls that overlap in time race. The entry
- * synchronises the stream before it returns.
+ * the library holds the status words, three per-level fields of the column
+ * solve and the 1-D grid tables: 256 + 8*(3*KA*IA*JA + 7*KA + 4*IA + 4*JA)
+ * bytes. A larger domain is rejected with SCALE_HEVI_ERR_ARG. The first call
+ * on a device looks up the array with that device current. Make that first
+ * call before any stream capture. All calls on a device share the array, so
+ * calls that overlap in time race. The entry synchronises the stream before
+ * it returns.
  * ------------------------------------------------------------------------- */
-#define SCALE_HEVI_NOALLOC_SCRATCH_BYTES (1024UL * 1024UL)
+#define SCALE_HEVI_NOALLOC_SCRATCH_BYTES (32UL * 1024UL * 1024UL)
 int ATMOS_DYN_Tstep_short_fvm_hevi_b200_noalloc(const scale_hevi_index *idx, const char *flux_type, void *stream,
                                                 SCALE_HEVI_TSTEP_SHORT_ARGS);
 

@@ -43,6 +43,7 @@ struct Ctx {
     double *rk[2] = {nullptr, nullptr}; // 5*N3 each
     double *acc = nullptr;          // 5*N3
     double *facc = nullptr;         // 6*N3
+    double *colscr = nullptr;       // 3*N3 when HEVI_COL_SCRATCH
     double *tr = nullptr;           // tracer: RK1, RK2, phi_lo, anti(3), rjp, rjm = 8*N3
     double *lg = nullptr;           // large step: DENS00, RT2P, DPRES0, REF_rhot, mflx_av(3) = 7*N3
     double *sum_part = nullptr, *sum_out = nullptr;
@@ -123,7 +124,7 @@ int dalloc(double **p, size_t n)
 
 void free_all()
 {
-    double *bufs[] = {C.d_tab, C.d_nd, C.rk[0], C.rk[1], C.acc, C.facc, C.tr, C.lg, C.sum_part, C.sum_out};
+    double *bufs[] = {C.colscr, C.d_tab, C.d_nd, C.rk[0], C.rk[1], C.acc, C.facc, C.tr, C.lg, C.sum_part, C.sum_out};
     for (double *b : bufs) if (b) cudaFree(b);
     for (auto &kv : C.stage) cudaFree(kv.second.first);
     if (C.status) cudaFree(C.status);
@@ -312,7 +313,7 @@ int run_stage(const StageIn &in, double *const out[5], double *mflx, double *tfl
     a.DPRES0 = in.DPRES0; a.RT2P = in.RT2P; a.CORIOLI = in.CORIOLI; a.num_diff = in.num_diff;
     a.wdamp = C.d_wdamp; a.DDIV = in.DDIV; a.REF_dens = in.REF_dens; a.REF_rhot = in.REF_rhot;
     a.divdmp_coef = in.divdmp; a.J33G = in.J33G; a.dtrk = dtrk;
-    a.rk_mode = mode; a.acc = C.acc; a.facc = C.facc; a.status = C.status;
+    a.rk_mode = mode; a.acc = C.acc; a.facc = C.facc; a.status = C.status; a.colscr = C.colscr;
     CK(timed("hevi_stage", [&] {
         CU(launch_hevi_stage(C.g, a, C.scheme, C.stream));
         return SCALE_HEVI_OK;
@@ -442,6 +443,7 @@ int scale_hevi_setup(const scale_hevi_index *idx, const char *flux_type, const c
         (rc = dalloc(&C.d_nd, 8 * (size_t)x.KA + 8 * (size_t)x.IA + 8 * (size_t)x.JA)) ||
         (rc = dalloc(&C.rk[0], 5 * N3)) || (rc = dalloc(&C.rk[1], 5 * N3)) ||
         (rc = dalloc(&C.acc, 5 * N3)) || (rc = dalloc(&C.facc, 6 * N3)) ||
+        (HEVI_COL_SCRATCH && (rc = dalloc(&C.colscr, 3 * N3))) ||
         (rc = dalloc(&C.sum_part, (size_t)x.IMAX * x.JMAX)) || (rc = dalloc(&C.sum_out, 1))) {
         free_all();
         return rc;

@@ -295,7 +295,11 @@ __device__ __forceinline__ void update_mom(const Grid &g, const StageArgs &a, co
 // the stage kernel
 // =============================================================================
 constexpr int MAXKA = 260;    // largest KA (KMAX + 4) the kernel accepts
-constexpr int COL_ARRAYS = 6; // per-level shared arrays
+#if HEVI_COL_SCRATCH
+constexpr int COL_ARRAYS = 3; // per-level shared arrays
+#else
+constexpr int COL_ARRAYS = 6;
+#endif
 
 enum ColArr : int { CA_C = 0, CA_PT = 1, CA_A = 2, CA_SR = 3, CA_ST = 4, CA_TZ = 5 };
 // CA_C holds POTT in phases 1-2, then the RHS C, then f, then the solution.
@@ -341,6 +345,15 @@ __global__ void __launch_bounds__(32 * HEVI_COL_TC, HEVI_COL_MINB) k_hevi_stage(
     // shared arrays: SA(arr, cc, L) for column cc of the tile, level L (1-based)
 #define SA(arr, cc, L) sm[((size_t)(arr) * TC + (cc)) * KP + (L) - 1]
 #define CL(p, L) ld((p) + col + (L) - 1)
+#if HEVI_COL_SCRATCH
+    // Sr, St, tZ of this warp's column in the global scratch (written and read
+    // back by this CTA only; L2-cached loads see the block's own stores)
+#define XS_PUT(q, L, v) (a.colscr[(size_t)((q) - CA_SR) * N3 + col + (L) - 1] = (v))
+#define XS(q, L) __ldcg(a.colscr + (size_t)((q) - CA_SR) * N3 + col + (L) - 1)
+#else
+#define XS_PUT(q, L, v) (SA(q, w, L) = (v))
+#define XS(q, L) SA(q, w, L)
+#endif
 
     // L2 prefetch of the tile's columns of the fields the next phase reads;
     // the last warp issues one bulk prefetch per field (one lane each)
@@ -382,7 +395,7 @@ __global__ void __launch_bounds__(32 * HEVI_COL_TC, HEVI_COL_MINB) k_hevi_stage(
             const double mZ = (L <= KE - 1) ? ld(nd.DZ() + c) : 0.0; // hevi_mflx_z :383-391 (flat terrain)
             const double mZm1 = (L - 1 >= KS) ? ld(nd.DZ() + c - 1) : 0.0;
             const double rcdz = ld(g.RCDZ + L - 1);
-            SA(CA_SR, w, L) = (-(mZ - mZm1) * rcdz + adv_r) + lds(a.DENS_t + c);
+            XS_PUT(CA_SR, L, (-(mZ - mZm1) * rcdz + adv_r) + lds(a.DENS_t + c));
             SA(CA_A, w, L) = dt2 * J33G * rcdz * ld(a.RT2P + c) * J33G;
         }
     }
@@ -446,8 +459,8 @@ __global__ void __launch_bounds__(32 * HEVI_COL_TC, HEVI_COL_MINB) k_hevi_stage(
             if (j == g.JS) put_flux(a, N3, 5, c - sJ, tYs, false);
             const double rcdz = ld(g.RCDZ + L - 1);
             SA(CA_PT, w, L) = PT;
-            SA(CA_TZ, w, L) = tZ;
-            SA(CA_ST, w, L) = (-(tZ - tZm) * rcdz + adv_t) + lds(a.RHOT_t + c); // hevi_st :646-649
+            XS_PUT(CA_TZ, L, tZ);
+            XS_PUT(CA_ST, L, (-(tZ - tZm) * rcdz + adv_t) + lds(a.RHOT_t + c)); // hevi_st :646-649
         }
     }
     __syncthreads();
@@ -485,9 +498,9 @@ __global__ void __launch_bounds__(32 * HEVI_COL_TC, HEVI_COL_MINB) k_hevi_stage(
             const double Sw = (advcv + adv_w) + wdmp + div + lds(a.MOMZ_t + c);
             const double rfdz = ld(g.RFDZ + k - 1);
             const double RTL1 = CL(a.RT2P, k + 1), RTL0 = CL(a.RT2P, k);
-            const double pg = -(dpres(k + 1) + RTL1 * dt * SA(CA_ST, w, k + 1) - dpres(k) - RTL0 * dt * SA(CA_ST, w, k)) * rfdz * J33G
-                              - GRAV * (ld(g.F2H1 + k - 1) * (CL(a.DENS, k + 1) - lds(a.REF_dens + c + 1) + SA(CA_SR, w, k + 1) * dt)
-                                        + ld(g.F2H2 + k - 1) * (CL(a.DENS, k) - lds(a.REF_dens + c) + SA(CA_SR, w, k) * dt));
+            const double pg = -(dpres(k + 1) + RTL1 * dt * XS(CA_ST, k + 1) - dpres(k) - RTL0 * dt * XS(CA_ST, k)) * rfdz * J33G
+                              - GRAV * (ld(g.F2H1 + k - 1) * (CL(a.DENS, k + 1) - lds(a.REF_dens + c + 1) + XS(CA_SR, k + 1) * dt)
+                                        + ld(g.F2H2 + k - 1) * (CL(a.DENS, k) - lds(a.REF_dens + c) + XS(CA_SR, k) * dt));
             SA(CA_C, w, k) = CL(a.MOMZ, k) + dt * (pg + Sw);
         }
     }
@@ -570,12 +583,12 @@ __global__ void __launch_bounds__(32 * HEVI_COL_TC, HEVI_COL_MINB) k_hevi_stage(
                 adr = -(Cm - Cm1) * J33G * rcdz;
                 adt = -(Cm * SA(CA_PT, w, m) - Cm1 * SA(CA_PT, w, m - 1)) * J33G * rcdz;
             }
-            put_state(a, N3, 0, a.DENS_RK, a.DENS0, c, lds(a.DENS0 + c) + dt * (adr + SA(CA_SR, w, m)), true);
-            put_state(a, N3, 4, a.RHOT_RK, a.RHOT0, c, lds(a.RHOT0 + c) + dt * (adt + SA(CA_ST, w, m)), true);
+            put_state(a, N3, 0, a.DENS_RK, a.DENS0, c, lds(a.DENS0 + c) + dt * (adr + XS(CA_SR, m)), true);
+            put_state(a, N3, 4, a.RHOT_RK, a.RHOT0, c, lds(a.RHOT0 + c) + dt * (adt + XS(CA_ST, m)), true);
             if (m <= KE - 1) {
                 put_state(a, N3, 1, a.MOMZ_RK, a.MOMZ0, c, ld(a.MOMZ0 + c) + (Cm - ld(a.MOMZ + c)), true);
                 put_flux(a, N3, 0, c, ld(nd.DZ() + c) + J33G * Cm, true);
-                put_flux(a, N3, 3, c, SA(CA_TZ, w, m) + J33G * Cm * SA(CA_PT, w, m), true);
+                put_flux(a, N3, 3, c, XS(CA_TZ, m) + J33G * Cm * SA(CA_PT, w, m), true);
             } else {
                 put_state(a, N3, 1, a.MOMZ_RK, a.MOMZ0, c, 0.0, false);
                 put_flux(a, N3, 0, c, 0.0, true);
@@ -598,6 +611,8 @@ __global__ void __launch_bounds__(32 * HEVI_COL_TC, HEVI_COL_MINB) k_hevi_stage(
     }
 #undef SA
 #undef CL
+#undef XS
+#undef XS_PUT
 }
 #undef AT
 

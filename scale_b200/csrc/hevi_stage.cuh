@@ -19,6 +19,12 @@ enum RkMode : int {
     RK_FINAL = 4,  // X = ((acc + X) - X0*3)/6, F = (facc + F)/6 over the interior
 };
 
+// Per-level sources Sr, St and the vertical theta flux tZ of the implicit
+// column problem: in shared memory (0) or in a global scratch of 3 fields (1).
+#ifndef HEVI_COL_SCRATCH
+#define HEVI_COL_SCRATCH 1
+#endif
+
 struct StageArgs {
     // outputs (RK_FINAL: the state arrays themselves, updated in place)
     double *DENS_RK, *MOMZ_RK, *MOMX_RK, *MOMY_RK, *RHOT_RK;
@@ -39,6 +45,7 @@ struct StageArgs {
     double *acc;  // 5*N3: DENS, MOMZ, MOMX, MOMY, RHOT
     double *facc; // 6*N3: mflx Z,X,Y then tflx Z,X,Y
     unsigned *status;
+    double *colscr; // 3*N3 (HEVI_COL_SCRATCH): Sr, St, tZ
 };
 
 }  // namespace hevi

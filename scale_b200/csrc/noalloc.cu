@@ -17,8 +17,9 @@
 //   - The scratch is shared by every call on a device, so calls that overlap in
 //     time (two host threads, or two streams in flight) race on it.
 //   - The entry synchronises its stream before it returns.
-//   - The scratch holds a 256-byte header (status word, terrain-check counter)
-//     and the 1-D grid tables, 7*KA + 4*IA + 4*JA doubles; at most
+//   - The scratch holds a 256-byte header (status word, terrain-check counter),
+//     three per-level fields of the column solve (3*KA*IA*JA doubles) and the
+//     1-D grid tables (7*KA + 4*IA + 4*JA doubles); at most
 //     SCALE_HEVI_NOALLOC_SCRATCH_BYTES. Larger domains are rejected with
 //     SCALE_HEVI_ERR_ARG.
 #include <cstdarg>
@@ -119,7 +120,8 @@ extern "C" int ATMOS_DYN_Tstep_short_fvm_hevi_b200_noalloc(const scale_hevi_inde
     const int KA = x.KA, IA = x.IA, JA = x.JA;
     const size_t N3 = (size_t)KA * IA * JA;
     const size_t ntab = 7 * (size_t)KA + 4 * (size_t)IA + 4 * (size_t)JA;
-    const size_t need = kHeader + ntab * sizeof(double);
+    const size_t ncol = HEVI_COL_SCRATCH ? 3 * N3 : 0;
+    const size_t need = kHeader + (ncol + ntab) * sizeof(double);
     if (need > kScratchBytes)
         return err(SCALE_HEVI_ERR_ARG,
                    "domain %dx%dx%d needs %zu bytes of scratch; the no-alloc entry holds at most %zu bytes",
@@ -130,7 +132,8 @@ extern "C" int ATMOS_DYN_Tstep_short_fvm_hevi_b200_noalloc(const scale_hevi_inde
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     unsigned *status = reinterpret_cast<unsigned *>(scr);
     unsigned long long *count = reinterpret_cast<unsigned long long *>(scr + 8);
-    double *tab = reinterpret_cast<double *>(scr + kHeader);
+    double *colscr = reinterpret_cast<double *>(scr + kHeader);
+    double *tab = colscr + ncol;
 
     // flat terrain only, as the other entries (GSQRT = 1, J13G = J23G = 0, MAPF = 1)
     NA_CU(cudaMemsetAsync(scr, 0, kHeader, st)); // status and counter start at zero
@@ -180,6 +183,7 @@ extern "C" int ATMOS_DYN_Tstep_short_fvm_hevi_b200_noalloc(const scale_hevi_inde
     a.wdamp = z + 6 * KA; a.DDIV = DDIV; a.REF_dens = REF_dens; a.REF_rhot = REF_rhot;
     a.divdmp_coef = *divdmp_coef; a.J33G = *J33G; a.dtrk = *dtrk;
     a.rk_mode = RK_PLAIN; a.acc = nullptr; a.facc = nullptr; a.status = status;
+    a.colscr = HEVI_COL_SCRATCH ? colscr : nullptr;
 
     NA_CU(launch_hevi_stage(g, a, scheme, st));
     unsigned flags = 0;

@@ -65,8 +65,8 @@ def test_no_alloc_stage_matches_device_entry(gpu):
 def test_no_alloc_rejects_a_domain_beyond_its_scratch(gpu):
     g = helpers.small_grid(IMAX=16, JMAX=12, KMAX=20)
     idx = g.index_dict()
-    # 1-D tables of 4*(IA+JA) doubles above 1 MiB: the size check answers before any argument is read
-    n = 20000
+    # three (KA,IA,JA) fields above 32 MiB: the size check answers before any argument is read
+    n = 512
     idx.update(IMAX=n, JMAX=n, IA=n + 4, JA=n + 4, IE=n + 2, JE=n + 2, IBLOCK=n, JBLOCK=n)
     with pytest.raises(hevi.HeviError) as e:
         hevi.ATMOS_DYN_Tstep_short_fvm_hevi_noalloc(idx, "CD4", 0, divdmp_coef=0.0, CDZ=g.CDZ, FDZ=g.FDZ, FDX=g.FDX,
