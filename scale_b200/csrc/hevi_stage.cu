@@ -2,10 +2,10 @@
 // scalelib/src/atmos-rm/dynamics/scale_atmos_dyn_tstep_short_fvm_hevi.F90:128-1089)
 // as one kernel, k_hevi_stage.
 //
-// A CTA owns a tile of TC consecutive columns (i .. i+TC-1 at one j) over all
-// levels. A column is KA contiguous doubles, so warp w works on column w with
-// its lanes along k (256-byte coalesced accesses); horizontal neighbours are
-// other columns, read through L1/L2. Per-level values of the vertical implicit
+// A CTA owns a tile of TX x TY columns over all levels. A column is KA
+// contiguous doubles, so each warp works on one column with its lanes along k
+// (256-byte coalesced accesses); horizontal neighbours are other columns, read
+// through L1/L2, or from shared memory when they lie in the tile. Per-level values of the vertical implicit
 // problem live in shared memory ([quantity][column][level], odd pitch):
 //   1. POTT = RHOT/DENS; x/y mass fluxes and the mass source Sr; A(k)      (k-parallel)
 //   2. PT (theta at w-faces), vertical and x/y theta fluxes, St             (k-parallel)
@@ -23,9 +23,13 @@
 
 // Launch shape. The defaults are the measured best on B200 for KMAX = 128;
 // they can be overridden at build time for tuning sweeps.
-#ifndef HEVI_COL_TC
-#define HEVI_COL_TC 16 // columns per CTA (blockDim = 32 x HEVI_COL_TC)
+#ifndef HEVI_TILE_X
+#define HEVI_TILE_X 16 // columns per CTA along i
 #endif
+#ifndef HEVI_TILE_Y
+#define HEVI_TILE_Y 1 // columns per CTA along j (blockDim = 32 x HEVI_TILE_X*HEVI_TILE_Y)
+#endif
+#define HEVI_COL_TC (HEVI_TILE_X * HEVI_TILE_Y)
 #ifndef HEVI_COL_MINB
 #define HEVI_COL_MINB 2 // resident CTAs per SM the register allocator must allow
 #endif
@@ -35,12 +39,7 @@
 #ifndef HEVI_STREAM_HINTS
 #define HEVI_STREAM_HINTS 1 // evict-first loads/stores for data each cell touches once
 #endif
-#ifndef HEVI_SPLIT_ROLES
-#define HEVI_SPLIT_ROLES 0 // rho*u/rho*v in CTAs of their own, interleaved with the column CTAs
-#endif
-#ifndef HEVI_L2_PREFETCH
-#define HEVI_L2_PREFETCH 0 // bulk L2 prefetch of the tile's columns one phase ahead
-#endif
+
 
 namespace hevi {
 
@@ -97,19 +96,6 @@ __device__ __forceinline__ void put_flux(const StageArgs &a, size_t N3, int f, s
     case RK_STAGE3: if (interior) sts(acc, lds(acc) + val * 2.0); break;
     default: sts(out, interior ? (lds(acc) + val) / 6.0 : val);
     }
-}
-
-// Bulk prefetch of n bytes at p into L2 (a hint: no completion to wait for).
-// The address must be 16-byte aligned and n a multiple of 16; misaligned
-// fields are simply not prefetched.
-__device__ __forceinline__ void l2_prefetch(const double *p, unsigned n)
-{
-#if HEVI_L2_PREFETCH
-    if (p && n && ((reinterpret_cast<uintptr_t>(p) & 15u) == 0) && (n & 15u) == 0)
-        asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p), "r"(n) : "memory");
-#else
-    (void)p; (void)n;
-#endif
 }
 
 // =============================================================================
@@ -311,27 +297,22 @@ template <int S>
 __global__ void __launch_bounds__(32 * HEVI_COL_TC, HEVI_COL_MINB) k_hevi_stage(const Grid g, const StageArgs a)
 {
     extern __shared__ double sm[];
-    const int TC = blockDim.y;
+    constexpr int TX = HEVI_TILE_X, TY = HEVI_TILE_Y, TC = TX * TY;
     const int lane = threadIdx.x, w = threadIdx.y;
+    const int tx = w % TX, ty = w / TX; // this warp's column in the tile
     // 2-D raster: consecutive CTAs walk down HEVI_RASTER_J rows of tiles, then
     // step in i, so the CTAs resident together cover a compact patch
-    // With HEVI_SPLIT_ROLES the grid holds two CTAs per tile: even blockIdx.x
-    // runs the column work, odd blockIdx.x the rho*u/rho*v updates, so an SM
-    // holds both kinds and one kind's memory traffic covers the other's solve.
-    const bool mom_role = HEVI_SPLIT_ROLES && (blockIdx.x & 1);
-    const int bx = HEVI_SPLIT_ROLES ? (int)(blockIdx.x >> 1) : (int)blockIdx.x;
-    int ti, jj;
+    int ti, tj;
     {
-        const int nti = HEVI_SPLIT_ROLES ? (int)(gridDim.x >> 1) : (int)gridDim.x, b = bx + nti * blockIdx.y;
+        const int nti = gridDim.x, ntj = gridDim.y, b = blockIdx.x + nti * blockIdx.y;
         const int grp = b / (nti * HEVI_RASTER_J), rem = b - grp * (nti * HEVI_RASTER_J);
-        const int rows = min(HEVI_RASTER_J, g.JMAX - grp * HEVI_RASTER_J);
-        jj = grp * HEVI_RASTER_J + rem % rows;
+        const int rows = min(HEVI_RASTER_J, ntj - grp * HEVI_RASTER_J);
+        tj = grp * HEVI_RASTER_J + rem % rows;
         ti = rem / rows;
     }
-    const int i0 = g.IS + ti * TC;
-    const int j = g.JS + jj;
-    const int i = i0 + w; // this warp's column in the k-parallel phases
-    const bool col_ok = i <= g.IE;
+    const int i0 = g.IS + ti * TX, j0 = g.JS + tj * TY;
+    const int i = i0 + tx, j = j0 + ty; // this warp's column in the k-parallel phases
+    const bool col_ok = i <= g.IE && j <= g.JE;
     const size_t N3 = n3(g);
     const long sI = g.KA, sJ = (long)g.KA * g.IA;
     const int KS = g.KS, KE = g.KE;
@@ -341,7 +322,7 @@ __global__ void __launch_bounds__(32 * HEVI_COL_TC, HEVI_COL_MINB) k_hevi_stage(
     const double dt = a.dtrk, J33G = a.J33G, dt2 = dt * dt;
     const bool use_div = a.divdmp_coef != 0.0;
     const double ddc = use_div ? a.divdmp_coef / dt : 0.0;
-    const double rcdx = col_ok ? ld(g.RCDX + i - 1) : 0.0, rcdy = ld(g.RCDY + j - 1);
+    const double rcdx = col_ok ? ld(g.RCDX + i - 1) : 0.0, rcdy = col_ok ? ld(g.RCDY + j - 1) : 0.0;
     // shared arrays: SA(arr, cc, L) for column cc of the tile, level L (1-based)
 #define SA(arr, cc, L) sm[((size_t)(arr) * TC + (cc)) * KP + (L) - 1]
 #define CL(p, L) ld((p) + col + (L) - 1)
@@ -354,32 +335,6 @@ __global__ void __launch_bounds__(32 * HEVI_COL_TC, HEVI_COL_MINB) k_hevi_stage(
 #define XS_PUT(q, L, v) (SA(q, w, L) = (v))
 #define XS(q, L) SA(q, w, L)
 #endif
-
-    // L2 prefetch of the tile's columns of the fields the next phase reads;
-    // the last warp issues one bulk prefetch per field (one lane each)
-    const size_t tile0 = idx3(g, 1, i0, j);
-    const unsigned tile_bytes = (unsigned)((size_t)min(TC, g.IE - i0 + 1) * g.KA * sizeof(double));
-    const bool rk_reads = a.rk_mode >= RK_STAGE2;
-    auto prefetch = [&](const double *const *f, int n) {
-        if (w == TC - 1 && lane < n) l2_prefetch(f[lane] ? f[lane] + tile0 : nullptr, tile_bytes);
-    };
-    {
-        const double *f[] = {a.RHOT, a.DENS, a.MOMX, a.MOMY, nd.DX(), nd.DY(), nd.DZ(), a.DENS_t, a.RT2P,
-                             rk_reads ? a.facc + N3 : nullptr, rk_reads ? a.facc + 2 * N3 : nullptr,
-                             a.MOMZ, nd.TZ(), nd.TX(), nd.TY(), a.RHOT_t,
-                             rk_reads ? a.facc + 4 * N3 : nullptr, rk_reads ? a.facc + 5 * N3 : nullptr};
-        prefetch(f, 18);
-    }
-
-    if (mom_role) {
-        // rho*u and rho*v of this warp's column (hevi_momx :814-928, hevi_momy :934-1048)
-        if (col_ok)
-            for (int L0 = KS; L0 <= KE; L0 += 32) {
-                update_mom<S, 0>(g, a, nd, N3, L0 + lane, i, j, L0 + lane <= KE);
-                update_mom<S, 1>(g, a, nd, N3, L0 + lane, i, j, L0 + lane <= KE);
-            }
-        return;
-    }
 
     // ---- phase 1: POTT (:586-600), x/y mass fluxes (:399-438), Sr (:443-479), A (:696) ----
     if (col_ok) {
@@ -401,11 +356,6 @@ __global__ void __launch_bounds__(32 * HEVI_COL_TC, HEVI_COL_MINB) k_hevi_stage(
     }
     __syncthreads();
 
-    {
-        const double *f[] = {a.MOMZ0, a.MOMZ_t, a.DPRES0, a.REF_rhot, a.REF_dens, nd.WZ(), nd.WX(), nd.WY(),
-                             use_div ? a.DDIV : nullptr};
-        prefetch(f, 9);
-    }
     // ---- phase 2: PT, tZ (valueW_Z ud3.F90:98-153, fluxZ_XYZ :157-247), x/y theta fluxes, St ----
     if (col_ok) {
         auto pt_tz = [&](int L, double &pt, double &tz) {
@@ -437,15 +387,17 @@ __global__ void __launch_bounds__(32 * HEVI_COL_TC, HEVI_COL_MINB) k_hevi_stage(
             (void)PTm;
             // POTT at x-neighbours (from the tile when it holds them) and y-neighbours
             auto pott_x = [&](int d) -> double {
-                const int wd = w + d;
-                if (wd >= 0 && wd < TC && i + d <= g.IE) return SA(CA_C, wd, L);
+                const int td = tx + d;
+                if (td >= 0 && td < TX && i + d <= g.IE) return SA(CA_C, w + d, L);
                 return AT(a.RHOT, 0, d, 0) / AT(a.DENS, 0, d, 0);
             };
+            auto pott_y = [&](int d) -> double {
+                const int td = ty + d;
+                if (td >= 0 && td < TY && j + d <= g.JE) return SA(CA_C, w + d * TX, L);
+                return AT(a.RHOT, 0, 0, d) / AT(a.DENS, 0, 0, d);
+            };
             const double Pm2 = pott_x(-2), Pm1 = pott_x(-1), P00 = SA(CA_C, w, L), Pp1 = pott_x(1), Pp2 = pott_x(2);
-            const double Qm2 = AT(a.RHOT, 0, 0, -2) / AT(a.DENS, 0, 0, -2);
-            const double Qm1 = AT(a.RHOT, 0, 0, -1) / AT(a.DENS, 0, 0, -1);
-            const double Qp1 = AT(a.RHOT, 0, 0, 1) / AT(a.DENS, 0, 0, 1);
-            const double Qp2 = AT(a.RHOT, 0, 0, 2) / AT(a.DENS, 0, 0, 2);
+            const double Qm2 = pott_y(-2), Qm1 = pott_y(-1), Qp1 = pott_y(1), Qp2 = pott_y(2);
             const MassFlux m = mass_flux(a, nd, c, sI, sJ);
             // fluxX/Y_XYZ (ud3.F90:251-353)
             const double tXe = m.Xe * ip4<S>(m.Xe, Pm1, P00, Pp1, Pp2) + AT(nd.TX(), 0, 0, 0);
@@ -465,11 +417,6 @@ __global__ void __launch_bounds__(32 * HEVI_COL_TC, HEVI_COL_MINB) k_hevi_stage(
     }
     __syncthreads();
 
-    {
-        const double *f[] = {a.MOMX0, a.MOMY0, a.MOMX_t, a.MOMY_t, nd.UZ(), nd.UX(), nd.UY(), nd.VZ(), nd.VX(), nd.VY(),
-                             rk_reads ? a.acc + 2 * N3 : nullptr, rk_reads ? a.acc + 3 * N3 : nullptr};
-        prefetch(f, 12);
-    }
     // ---- phase 3: Sw (hevi_sw :528-578) and the right-hand side C(k), k = KS..KE-1 (:698-722) ----
     if (col_ok) {
         // vertical w-momentum flux above level k, fluxZ_XYW (ud3.F90:358-452), zero outside KS..KE-2
@@ -506,15 +453,9 @@ __global__ void __launch_bounds__(32 * HEVI_COL_TC, HEVI_COL_MINB) k_hevi_stage(
     }
     __syncthreads();
 
-    {
-        const double *f[] = {a.DENS0, a.RHOT0, rk_reads ? a.acc : nullptr, rk_reads ? a.acc + N3 : nullptr,
-                             rk_reads ? a.acc + 4 * N3 : nullptr, rk_reads ? a.facc : nullptr,
-                             rk_reads ? a.facc + 3 * N3 : nullptr};
-        prefetch(f, 7);
-    }
     // ---- phase 4: Thomas solve (warp 0) while the other warps update rho*u, rho*v ----
     if (w == 0) {
-        if (lane < TC && i0 + lane <= g.IE) {
+        if (lane < TC && i0 + lane % TX <= g.IE && j0 + lane / TX <= g.JE) {
             const int cc = lane;
             double e_prev = 0.0, f_prev = 0.0;
             for (int k = KS; k <= KE - 1; ++k) {
@@ -552,15 +493,16 @@ __global__ void __launch_bounds__(32 * HEVI_COL_TC, HEVI_COL_MINB) k_hevi_stage(
             SA(CA_PT, cc, KS - 1) = 0.0;
         }
     }
-    if (!HEVI_SPLIT_ROLES && (w > 0 || TC == 1)) {
+    if (w > 0 || TC == 1) {
         // rho*u / rho*v of the tile: (column, 32-level chunk, component) items over the worker warps
         const int nworkers = TC > 1 ? TC - 1 : 1, wid = TC > 1 ? w - 1 : 0;
         const int NL = (g.KMAX + 31) / 32;
         for (int it = wid; it < 2 * TC * NL; it += nworkers) {
-            const int item = it >> 1, ii = i0 + item / NL, L = KS + (item % NL) * 32 + lane;
-            if (ii <= g.IE) { // warp-uniform branch
-                if (it & 1) update_mom<S, 1>(g, a, nd, N3, L, ii, j, L <= KE);
-                else update_mom<S, 0>(g, a, nd, N3, L, ii, j, L <= KE);
+            const int item = it >> 1, cc = item / NL, L = KS + (item % NL) * 32 + lane;
+            const int ii = i0 + cc % TX, jj = j0 + cc / TX;
+            if (ii <= g.IE && jj <= g.JE) { // warp-uniform branch
+                if (it & 1) update_mom<S, 1>(g, a, nd, N3, L, ii, jj, L <= KE);
+                else update_mom<S, 0>(g, a, nd, N3, L, ii, jj, L <= KE);
             }
         }
     }
@@ -604,7 +546,7 @@ __global__ void __launch_bounds__(32 * HEVI_COL_TC, HEVI_COL_MINB) k_hevi_stage(
     }
     // hevi_mflx_z :369-393 also fills the halo column i = IS-1 with the explicit
     // part of the vertical mass flux; the solver never updates it
-    if (ti == 0 && w == TC - 1 && (a.rk_mode == RK_PLAIN || a.rk_mode == RK_FINAL)) {
+    if (ti == 0 && tx == 0 && col_ok && (a.rk_mode == RK_PLAIN || a.rk_mode == RK_FINAL)) {
         const size_t ch = idx3(g, 1, g.IS - 1, j);
         for (int k = KS - 1 + lane; k <= KE; k += 32)
             a.mflx[ch + k - 1] = (k >= KS && k <= KE - 1) ? ld(nd.DZ() + ch + k - 1) : 0.0;
@@ -617,25 +559,16 @@ __global__ void __launch_bounds__(32 * HEVI_COL_TC, HEVI_COL_MINB) k_hevi_stage(
 #undef AT
 
 // ---- host launcher ----------------------------------------------------------
-// columns per CTA: HEVI_COL_TC, halved until HEVI_COL_MINB CTAs fit one SM's shared memory
-static int column_tile(int KA)
-{
-    int tc = HEVI_COL_TC;
-    while (tc > 1 && (size_t)COL_ARRAYS * tc * col_pitch(KA) * sizeof(double) > (size_t)224 * 1024 / HEVI_COL_MINB) tc /= 2;
-    return tc;
-}
-
 cudaError_t launch_hevi_stage(const Grid &g, const StageArgs &a, int scheme, cudaStream_t st)
 {
     if (g.KA > MAXKA) return cudaErrorInvalidValue;
-    const int TC = column_tile(g.KA);
-    const size_t smem = (size_t)COL_ARRAYS * TC * col_pitch(g.KA) * sizeof(double);
+    const size_t smem = (size_t)COL_ARRAYS * HEVI_COL_TC * col_pitch(g.KA) * sizeof(double);
     cudaError_t e = scheme == UD3
         ? cudaFuncSetAttribute(k_hevi_stage<UD3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)
         : cudaFuncSetAttribute(k_hevi_stage<CD4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    dim3 bc(32, TC);
-    dim3 gc((g.IMAX + TC - 1) / TC * (HEVI_SPLIT_ROLES ? 2 : 1), g.JMAX);
+    dim3 bc(32, HEVI_COL_TC);
+    dim3 gc((g.IMAX + HEVI_TILE_X - 1) / HEVI_TILE_X, (g.JMAX + HEVI_TILE_Y - 1) / HEVI_TILE_Y);
     if (scheme == UD3) k_hevi_stage<UD3><<<gc, bc, smem, st>>>(g, a);
     else k_hevi_stage<CD4><<<gc, bc, smem, st>>>(g, a);
     return cudaGetLastError();
