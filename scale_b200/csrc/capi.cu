@@ -44,6 +44,7 @@ struct Ctx {
     double *acc = nullptr;          // 5*N3
     double *facc = nullptr;         // 6*N3
     double *colscr = nullptr;       // 3*N3 when HEVI_COL_SCRATCH
+    double *phi = nullptr;          // numerical filter: 5*N3 (allocated on first use)
     double *tr = nullptr;           // tracer: RK1, RK2, phi_lo, anti(3), rjp, rjm = 8*N3
     double *lg = nullptr;           // large step: DENS00, RT2P, DPRES0, REF_rhot, mflx_av(3) = 7*N3
     double *sum_part = nullptr, *sum_out = nullptr;
@@ -124,7 +125,7 @@ int dalloc(double **p, size_t n)
 
 void free_all()
 {
-    double *bufs[] = {C.colscr, C.d_tab, C.d_nd, C.rk[0], C.rk[1], C.acc, C.facc, C.tr, C.lg, C.sum_part, C.sum_out};
+    double *bufs[] = {C.phi, C.colscr, C.d_tab, C.d_nd, C.rk[0], C.rk[1], C.acc, C.facc, C.tr, C.lg, C.sum_part, C.sum_out};
     for (double *b : bufs) if (b) cudaFree(b);
     for (auto &kv : C.stage) cudaFree(kv.second.first);
     if (C.status) cudaFree(C.status);
@@ -352,12 +353,13 @@ int run_rk4(double *X[5], double *mflx, double *tflx, const StageIn &base, doubl
 int run_numfilter(double *num_diff, const double *DENS, const double *MOMZ, const double *MOMX, const double *MOMY,
                   const double *RHOT, const double *REF_dens, const double *REF_pott)
 {
-    NdArgs a{num_diff, DENS, MOMZ, MOMX, MOMY, RHOT, REF_dens, REF_pott};
+    if (!C.phi) CK(dalloc(&C.phi, 5 * C.N3));
+    NdArgs a{num_diff, DENS, MOMZ, MOMX, MOMY, RHOT, REF_dens, REF_pott, C.phi};
     CK(timed("numfilter", [&] {
         CU(launch_numfilter(C.g, C.ndc, a, C.stream));
         return SCALE_HEVI_OK;
     }));
-    ++C.launches;
+    C.launches += 2;
     double *f[15];
     for (int q = 0; q < 15; ++q) f[q] = num_diff + (size_t)q * C.N3;
     return halo(f, 15);

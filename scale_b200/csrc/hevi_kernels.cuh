@@ -15,6 +15,7 @@ struct NdCoef {
 struct NdArgs {
     double *num_diff;
     const double *DENS, *MOMZ, *MOMX, *MOMY, *RHOT, *REF_dens, *REF_pott;
+    double *phi; // 5*N3 scratch: the five filtered quantities at every point
 };
 cudaError_t launch_numfilter(const Grid &g, const NdCoef &c, const NdArgs &a, cudaStream_t st);
 

@@ -3,11 +3,13 @@
 // third-difference operator calc_diff3 :1600-1760 and its coefficients from
 // ATMOS_DYN_filter_setup :200-330).
 //
-// One thread per (k,i,j) of an interior column writes all 15 components at its
-// level, including the zero and mirrored values of the vertical halo, so the
-// seven inputs are streamed once and the fifteen outputs written once. The
-// lateral halo is filled afterwards by the periodic halo kernel, as COMM_vars8
-// does in the reference.
+// Two kernels. k_phi evaluates the five filtered quantities (density and
+// theta deviations, three velocities) once at every point into a scratch of
+// five fields, so no quotient is formed twice. k_numfilter then has one thread
+// per (k,i,j) of an interior column write all 15 components at its level,
+// including the zero and mirrored values of the vertical halo, reading the
+// quantities from the scratch. The lateral halo is filled afterwards by the
+// periodic halo kernel, as COMM_vars8 does in the reference.
 #include "hevi_kernels.cuh"
 
 namespace hevi {
@@ -16,22 +18,36 @@ namespace hevi {
 #define CX3(n, i, s) ld(c.CNX3 + ((n) - 1) + 3 * ((size_t)((i) - 1) + (size_t)g.IA * ((s) - 1)))
 #define CY3(n, j, s) ld(c.CNY3 + ((n) - 1) + 3 * ((size_t)((j) - 1) + (size_t)g.JA * ((s) - 1)))
 
-// The five filtered quantities, evaluated at any (k,i,j) the stencils need.
+// The five filtered quantities at one point.
 // q: 0 DENS-REF_dens, 1 VELZ, 2 VELX, 3 VELY, 4 RHOT/DENS-REF_pott  (:538-547, 621-626, 715-720, 799-804, 876-883)
+// A velocity needs the density one point above (VELZ), east (VELX) or north
+// (VELY); at the last point of the array in that direction, which no stencil
+// reads, it is stored as zero.
+__global__ void __launch_bounds__(128) k_phi(const Grid g, const NdArgs a)
+{
+    const int i = 1 + blockIdx.x * blockDim.y + threadIdx.y;
+    const int j = 1 + blockIdx.y;
+    if (i > g.IA) return;
+    const size_t N3 = n3(g);
+    const long sI = g.KA, sJ = (long)g.KA * g.IA;
+    for (int k = 1 + threadIdx.x; k <= g.KA; k += 32) {
+        const size_t c = idx3(g, k, i, j);
+        const double D = ld(a.DENS + c);
+        a.phi[c] = D - ld(a.REF_dens + c);
+        a.phi[c + N3] = k < g.KA ? 2.0 * ld(a.MOMZ + c) / (ld(a.DENS + c + 1) + D) : 0.0;
+        a.phi[c + 2 * N3] = i < g.IA ? 2.0 * ld(a.MOMX + c) / (ld(a.DENS + c + sI) + D) : 0.0;
+        a.phi[c + 3 * N3] = j < g.JA ? 2.0 * ld(a.MOMY + c) / (ld(a.DENS + c + sJ) + D) : 0.0;
+        a.phi[c + 4 * N3] = ld(a.RHOT + c) / D - ld(a.REF_pott + c);
+    }
+}
+
+// the quantities read back by the stencils
 struct Phi {
     const Grid &g;
     const NdArgs &a;
     __device__ double operator()(int q, int k, int i, int j) const
     {
-        const size_t c = idx3(g, k, i, j);
-        const long sI = g.KA, sJ = (long)g.KA * g.IA;
-        switch (q) {
-        case 0: return ld(a.DENS + c) - ld(a.REF_dens + c);
-        case 1: return 2.0 * ld(a.MOMZ + c) / (ld(a.DENS + c + 1) + ld(a.DENS + c));
-        case 2: return 2.0 * ld(a.MOMX + c) / (ld(a.DENS + c + sI) + ld(a.DENS + c));
-        case 3: return 2.0 * ld(a.MOMY + c) / (ld(a.DENS + c + sJ) + ld(a.DENS + c));
-        default: return ld(a.RHOT + c) / ld(a.DENS + c) - ld(a.REF_pott + c);
-        }
+        return __ldg(a.phi + (size_t)q * n3(g) + idx3(g, k, i, j));
     }
 };
 
@@ -186,8 +202,9 @@ __global__ void __launch_bounds__(128, HEVI_ND_MINB) k_numfilter(const Grid g, c
 
 cudaError_t launch_numfilter(const Grid &g, const NdCoef &c, const NdArgs &a, cudaStream_t st)
 {
-    dim3 b(32, 4), gr((g.IMAX + 3) / 4, g.JMAX);
-    k_numfilter<<<gr, b, 0, st>>>(g, c, a);
+    dim3 b(32, 4);
+    k_phi<<<dim3((g.IA + 3) / 4, g.JA), b, 0, st>>>(g, a);
+    k_numfilter<<<dim3((g.IMAX + 3) / 4, g.JMAX), b, 0, st>>>(g, c, a);
     return cudaGetLastError();
 }
 
