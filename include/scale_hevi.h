@@ -199,6 +199,20 @@ int ATMOS_DYN_Tinteg_tracer_rk3_b200_dev(SCALE_HEVI_TINTEG_TRACER_ARGS);
 int COMM_vars8_b200_dev(double *var, const int *nfields);
 
 /* ---------------------------------------------------------------------------
+ * 3-D divergence of the momentum for divergence damping. Replaces
+ * ATMOS_DYN_divergence (scale_atmos_dyn_common.F90:1437-1515), same arguments in
+ * the same order. DDIV is written on k = KS-1..KE+1, i = IS..IE+1, j = JS..JE+1;
+ * other cells keep their contents. Flat terrain only (checked).
+ * ------------------------------------------------------------------------- */
+#define SCALE_HEVI_DIVERGENCE_ARGS                                                                             \
+    double *DDIV, const double *MOMZ, const double *MOMX, const double *MOMY,                                  \
+    const double *GSQRT, const double *J13G, const double *J23G, const double *J33G, const double *MAPF,       \
+    const double *RCDZ, const double *RCDX, const double *RCDY, const double *RFDZ, const double *FDZ
+
+int ATMOS_DYN_divergence_b200(SCALE_HEVI_DIVERGENCE_ARGS);
+int ATMOS_DYN_divergence_b200_dev(SCALE_HEVI_DIVERGENCE_ARGS);
+
+/* ---------------------------------------------------------------------------
  * One large step of the dynamics on device-resident state. Replaces the
  * dynamics part of ATMOS_DYN_Tstep_large_fvm_heve
  * (scale_atmos_dyn_tstep_large_fvm_heve.F90:171-1130) for the supported
@@ -206,7 +220,8 @@ int COMM_vars8_b200_dev(double *var, const int *nfields);
  * USE_AVERAGE off, FLAG_TRACER_SPLIT_TEND off, EULER large-step integrator
  * (QTRC0 = QTRC). Per large step: RT2P, DPRES0 and REF_rhot from the moist
  * thermodynamics (:428-470); nstep = ceiling((DTLS-EPS)/DTSS) short steps, each
- * numfilter + RK4 short step + vertical boundary values + halo exchange;
+ * numfilter + divergence for the damping term when divdmp_coef > 0 (:860-871)
+ * + RK4 short step + vertical boundary values + halo exchange;
  * then the RK3 tracer advection of every tracer with the short-step-averaged
  * mass flux. Arrays are device pointers; QTRC and RHOQ_tp are (KA,IA,JA,QA),
  * AQ_* are host arrays of length QA (QA <= 8). mflx_hi, tflx_hi and num_diff

@@ -46,7 +46,7 @@ struct Ctx {
     double *colscr = nullptr;       // 3*N3 when HEVI_COL_SCRATCH
     double *phi = nullptr;          // numerical filter: 5*N3 (allocated on first use)
     double *tr = nullptr;           // tracer: RK1, RK2, phi_lo, anti(3), rjp, rjm = 8*N3
-    double *lg = nullptr;           // large step: DENS00, RT2P, DPRES0, REF_rhot, mflx_av(3) = 7*N3
+    double *lg = nullptr;           // large step: DENS00, RT2P, DPRES0, REF_rhot, mflx_av(3), DDIV = 8*N3
     double *sum_part = nullptr, *sum_out = nullptr;
     unsigned *status = nullptr;
     unsigned long long *count = nullptr;
@@ -363,6 +363,19 @@ int run_numfilter(double *num_diff, const double *DENS, const double *MOMZ, cons
     double *f[15];
     for (int q = 0; q < 15; ++q) f[q] = num_diff + (size_t)q * C.N3;
     return halo(f, 15);
+}
+
+// ATMOS_DYN_divergence on device arrays; RCDZ/RCDX/RCDY are device vectors
+int run_divergence(double *DDIV, const double *MOMZ, const double *MOMX, const double *MOMY, const double *RCDZ,
+                   const double *RCDX, const double *RCDY, double J33G)
+{
+    CK(timed("divergence", [&] {
+        divergence(C.g, DDIV, MOMZ, MOMX, MOMY, RCDZ, RCDX, RCDY, J33G, C.stream);
+        CU(cudaGetLastError());
+        return SCALE_HEVI_OK;
+    }));
+    ++C.launches;
+    return SCALE_HEVI_OK;
 }
 
 // RK3 tracer integrator (tinteg_tracer_rk3.F90:92-210) on device arrays
@@ -728,6 +741,40 @@ int ATMOS_DYN_Tinteg_tracer_rk3_b200(SCALE_HEVI_TINTEG_TRACER_ARGS)
 }
 
 // ---- halo --------------------------------------------------------------------
+// ---- divergence ------------------------------------------------------------------
+int ATMOS_DYN_divergence_b200_dev(SCALE_HEVI_DIVERGENCE_ARGS)
+{
+    (void)RFDZ;
+    CK(need_setup());
+    CK(check_flat(GSQRT, J13G, J23G, MAPF, true));
+    if (!RCDZ || !RCDX || !RCDY || !FDZ) return fail(SCALE_HEVI_ERR_ARG, "a 1-D grid vector is NULL");
+    const int KA = C.g.KA, IA = C.g.IA, JA = C.g.JA;
+    double *t;
+    CK(stage_buf("div_tab", (size_t)KA + IA + JA, &t));
+    CU(cudaMemcpyAsync(t, RCDZ, KA * sizeof(double), cudaMemcpyHostToDevice, C.stream));
+    CU(cudaMemcpyAsync(t + KA, RCDX, IA * sizeof(double), cudaMemcpyHostToDevice, C.stream));
+    CU(cudaMemcpyAsync(t + KA + IA, RCDY, JA * sizeof(double), cudaMemcpyHostToDevice, C.stream));
+    return run_divergence(DDIV, MOMZ, MOMX, MOMY, t, t + KA, t + KA + IA, *J33G);
+}
+
+int ATMOS_DYN_divergence_b200(SCALE_HEVI_DIVERGENCE_ARGS)
+{
+    CK(need_setup());
+    CK(check_flat(GSQRT, J13G, J23G, MAPF, false));
+    const size_t N3 = n3();
+    double *dd, *mz, *mx, *my;
+    CK(h2d("DDIV", DDIV, N3, &dd)); // cells the divergence does not write keep their contents
+    CK(h2d("x1", MOMZ, N3, &mz));
+    CK(h2d("x2", MOMX, N3, &mx));
+    CK(h2d("x3", MOMY, N3, &my));
+    int rc = ATMOS_DYN_divergence_b200_dev(dd, mz, mx, my, nullptr, nullptr, nullptr, J33G, nullptr, RCDZ, RCDX, RCDY,
+                                           RFDZ, FDZ);
+    if (rc) return rc;
+    CK(d2h(DDIV, dd, N3));
+    CU(cudaStreamSynchronize(C.stream));
+    return SCALE_HEVI_OK;
+}
+
 int COMM_vars8_b200_dev(double *var, const int *nfields)
 {
     CK(need_setup());
@@ -757,14 +804,15 @@ int ATMOS_DYN_Tstep_large_fvm_heve_b200_dev(SCALE_HEVI_LARGE_ARGS)
     CK(need_setup());
     const int qa = *QA;
     if (qa < 0 || qa > 8) return fail(SCALE_HEVI_ERR_UNSUPPORTED, "QA=%d (0..8 supported)", qa);
-    if (*divdmp_coef > 0.0) return fail(SCALE_HEVI_ERR_UNSUPPORTED, "divergence damping (divdmp_coef > 0) is not supported in the large step");
     if (*ND_COEF != 0.0 && *ND_ORDER != 1) return fail(SCALE_HEVI_ERR_UNSUPPORTED, "ND_ORDER=%d is not supported", *ND_ORDER);
     if (*ND_COEF != 0.0 && !*ND_USE_RS) return fail(SCALE_HEVI_ERR_UNSUPPORTED, "ND_USE_RS=.false. is not supported");
     CK(check_flat(GSQRT, J13G, J23G, MAPF, true));
     const size_t N3 = C.N3;
-    if (!C.lg) CK(dalloc(&C.lg, 7 * N3));
+    if (!C.lg) CK(dalloc(&C.lg, 8 * N3));
     if (!C.tr) CK(dalloc(&C.tr, 8 * N3));
     double *DENS00 = C.lg, *RT2P = C.lg + N3, *DPRES0 = C.lg + 2 * N3, *REF_rhot = C.lg + 3 * N3, *mflx_av = C.lg + 4 * N3;
+    double *DDIV = C.lg + 7 * N3;
+    const bool use_div = *divdmp_coef > 0.0;
 
     // time steps, :373-376
     double dts = *DTSS;
@@ -788,11 +836,13 @@ int ATMOS_DYN_Tstep_large_fvm_heve_b200_dev(SCALE_HEVI_LARGE_ARGS)
     // *_tp on every cell the short step reads, so *_tp are passed directly.
     double *X[5] = {DENS, MOMZ, MOMX, MOMY, RHOT};
     StageIn base{nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
-                 DENS_tp, MOMZ_tp, MOMX_tp, MOMY_tp, RHOT_tp, DPRES0, RT2P, CORIOLI, num_diff, nullptr,
-                 REF_dens, REF_rhot, 0.0, *J33G};
+                 DENS_tp, MOMZ_tp, MOMX_tp, MOMY_tp, RHOT_tp, DPRES0, RT2P, CORIOLI, num_diff, use_div ? DDIV : nullptr,
+                 REF_dens, REF_rhot, use_div ? *divdmp_coef : 0.0, *J33G};
     for (int step = 1; step <= nstep; ++step) {
         if (*ND_COEF == 0.0) CU(cudaMemsetAsync(num_diff, 0, 15 * N3 * sizeof(double), C.stream));
         else CK(run_numfilter(num_diff, DENS, MOMZ, MOMX, MOMY, RHOT, REF_dens, REF_pott));
+        // divergence for the damping term, :860-871
+        if (use_div) CK(run_divergence(DDIV, MOMZ, MOMX, MOMY, C.g.RCDZ, C.g.RCDX, C.g.RCDY, *J33G));
         CK(run_rk4(X, mflx_hi, tflx_hi, base, dts));
         CK(timed("boundary", [&] { vertical_bc(C.g, DENS, MOMZ, MOMX, MOMY, RHOT, C.stream); return SCALE_HEVI_OK; }));
         ++C.launches;

@@ -40,6 +40,8 @@ cudaError_t launch_hevi_stage(const Grid &g, const StageArgs &a, int scheme, cud
 
 // ---- utilities (misc.cu) ----
 void periodic_halo(const Grid &g, double *const *fields, int nf, cudaStream_t st);
+void divergence(const Grid &g, double *DDIV, const double *MOMZ, const double *MOMX, const double *MOMY,
+                const double *RCDZ, const double *RCDX, const double *RCDY, double J33G, cudaStream_t st);
 void vertical_bc(const Grid &g, double *DENS, double *MOMZ, double *MOMX, double *MOMY, double *RHOT, cudaStream_t st);
 struct PrepArgs {
     double *RT2P, *DPRES0, *REF_rhot;

@@ -71,6 +71,37 @@ void vertical_bc(const Grid &g, double *DENS, double *MOMZ, double *MOMX, double
     k_vbc<<<gr, b, 0, st>>>(g, DENS, MOMZ, MOMX, MOMY, RHOT);
 }
 
+// ---- 3-D divergence for divergence damping, ATMOS_DYN_divergence
+// (scale_atmos_dyn_common.F90:1437-1515) on k = KS-1..KE+1, i = IS..IE+1,
+// j = JS..JE+1 with the KS and KE rows of :1487-1506. Flat terrain: the J13G/J23G
+// terms are zeros and the GSQRT/MAPF factors are ones, which leaves every
+// non-zero value unchanged.
+__global__ void k_divergence(const Grid g, double *DDIV, const double *MOMZ, const double *MOMX, const double *MOMY,
+                             const double *RCDZ, const double *RCDX, const double *RCDY, double J33G)
+{
+    const int i = g.IS + blockIdx.x * blockDim.y + threadIdx.y;
+    const int j = g.JS + blockIdx.y;
+    if (i > g.IE + 1) return;
+    const long sI = g.KA, sJ = (long)g.KA * g.IA;
+    const double rcdx = ld(RCDX + i - 1), rcdy = ld(RCDY + j - 1);
+    for (int k = g.KS - 1 + threadIdx.x; k <= g.KE + 1; k += 32) {
+        const size_t c = idx3(g, k, i, j);
+        const double h = (ld(MOMX + c) - ld(MOMX + c - sI)) * rcdx + (ld(MOMY + c) - ld(MOMY + c - sJ)) * rcdy;
+        double v;
+        if (k == g.KS) v = J33G * (ld(MOMZ + c)) * ld(RCDZ + k - 1) + h;
+        else if (k == g.KE) v = J33G * (-ld(MOMZ + c - 1)) * ld(RCDZ + k - 1) + h;
+        else v = J33G * (ld(MOMZ + c) - ld(MOMZ + c - 1)) * ld(RCDZ + k - 1) + h;
+        DDIV[c] = v;
+    }
+}
+
+void divergence(const Grid &g, double *DDIV, const double *MOMZ, const double *MOMX, const double *MOMY,
+                const double *RCDZ, const double *RCDX, const double *RCDY, double J33G, cudaStream_t st)
+{
+    dim3 b(32, 4), gr((g.IMAX + 1 + 3) / 4, g.JMAX + 1);
+    k_divergence<<<gr, b, 0, st>>>(g, DDIV, MOMZ, MOMX, MOMY, RCDZ, RCDX, RCDY, J33G);
+}
+
 // ---- RT2P, DPRES0, REF_rhot once per large step (tstep_large_fvm_heve.F90:428-470, moist form) ----
 __global__ void k_large_prep(const Grid g, const PrepArgs a)
 {

@@ -222,6 +222,10 @@ def ATMOS_DYN_Tstep_large_fvm_heve(**kw):
     call("ATMOS_DYN_Tstep_large_fvm_heve_b200", **kw)
 
 
+def ATMOS_DYN_divergence(**kw):
+    call("ATMOS_DYN_divergence_b200", **kw)
+
+
 # ---- device-array entries -----------------------------------------------------------
 def ATMOS_DYN_Tstep_short_fvm_hevi_dev(**kw):
     call("ATMOS_DYN_Tstep_short_fvm_hevi_b200_dev", **kw)
@@ -253,6 +257,10 @@ def ATMOS_DYN_Tstep_short_fvm_hevi_noalloc(index: dict, flux_type: str, stream: 
     idx = Index(**index)
     call("ATMOS_DYN_Tstep_short_fvm_hevi_b200_noalloc", idx=C.addressof(idx), flux_type=flux_type.encode(),
          stream=int(stream), **kw)
+
+
+def ATMOS_DYN_divergence_dev(**kw):
+    call("ATMOS_DYN_divergence_b200_dev", **kw)
 
 
 def COMM_vars8_dev(var, nfields: int):

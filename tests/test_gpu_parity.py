@@ -178,7 +178,7 @@ def _large_inputs(c):
     return tp, GS, J13, J23, MAPF
 
 
-def _run_large_both(c, nlarge, lib):
+def _run_large_both(c, nlarge, lib, divdmp=0.0):
     g = c.g
     tp, GS, J13, J23, MAPF = _large_inputs(c)
     aq = mkinit.aq_props(c.QA) if c.QA else None
@@ -190,7 +190,7 @@ def _run_large_both(c, nlarge, lib):
     out_gpu = dict(mflx_hi=g.zeros(3), tflx_hi=g.zeros(3), num_diff=g.zeros(5, 3))
     for _ in range(nlarge):
         oracle.tstep_large(g, c.scheme, c.scheme_tracer, st_ref, out_ref, tp, c.ref, aq, GS, J13, J23, MAPF, cor, wd,
-                           c.dtl, c.dt, ND_COEF=c.nd_coef, fct=c.fct, QA=c.QA)
+                           c.dtl, c.dt, ND_COEF=c.nd_coef, divdmp=divdmp, fct=c.fct, QA=c.QA)
     lib.setup(g.index_dict(), c.scheme, c.scheme_tracer)
     R, CV, CP, M = aq if aq else (None, None, None, None)
     for _ in range(nlarge):
@@ -201,7 +201,7 @@ def _run_large_both(c, nlarge, lib):
             FDZ=g.FDZ, FDX=g.FDX, FDY=g.FDY, RCDZ=g.RCDZ, RCDX=g.RCDX, RCDY=g.RCDY, RFDZ=g.RFDZ, RFDX=g.RFDX,
             RFDY=g.RFDY, PHI=c.ref["PHI"], GSQRT=GS, J13G=J13, J23G=J23, J33G=1.0, MAPF=MAPF, AQ_R=R, AQ_CV=CV,
             AQ_CP=CP, AQ_MASS=M, REF_dens=c.ref["REF_dens"], REF_pott=c.ref["REF_pott"], REF_pres=c.ref["REF_pres"],
-            ND_COEF=c.nd_coef, ND_ORDER=1, ND_SFC_FACT=1.0, ND_USE_RS=True, wdamp_coef=wd, divdmp_coef=0.0,
+            ND_COEF=c.nd_coef, ND_ORDER=1, ND_SFC_FACT=1.0, ND_USE_RS=True, wdamp_coef=wd, divdmp_coef=divdmp,
             FLAG_FCT_TRACER=c.fct, FLAG_FCT_ALONG_STREAM=True, DTLS=c.dtl, DTSS=c.dt,
             **{k: v for k, v in tp.items() if k != "RHOQ_tp"})
     return st_ref, st_gpu
@@ -314,3 +314,27 @@ def test_warm_bubble_600_short_steps(lib):
     for st in (st_ref, st_gpu):
         m1 = oracle.domain_sum(g, st["DENS"])
         assert abs(m1 - m0) / m0 < 1e-12
+
+
+@pytest.mark.parametrize("stretched", [False, True])
+def test_divergence_bit_exact(lib, stretched):
+    g = helpers.small_grid(IMAX=13, JMAX=11, KMAX=17, stretched=stretched)
+    c = helpers.small_case(g)
+    helpers.perturb_state(c)
+    GS, J13, J23, MAPF = oracle.flat_metrics(g)
+    ref = np.full(g.shape, np.nan, order="F")
+    oracle.divergence(g, ref, c.state, GS, J13, J23, 1.0, MAPF)
+    got = np.full(g.shape, np.nan, order="F")
+    lib.setup(g.index_dict(), "UD3", "UD3")
+    lib.ATMOS_DYN_divergence(DDIV=got, MOMZ=c.state["MOMZ"], MOMX=c.state["MOMX"], MOMY=c.state["MOMY"], GSQRT=GS,
+                             J13G=J13, J23G=J23, J33G=1.0, MAPF=MAPF, RCDZ=g.RCDZ, RCDX=g.RCDX, RCDY=g.RCDY,
+                             RFDZ=g.RFDZ, FDZ=g.FDZ)
+    assert helpers.same(got, ref), f"max rel diff {helpers.max_rel(got, ref):.3e}"
+
+
+def test_large_step_with_divergence_damping(lib):
+    c = mkinit.config(1, scale=0.3)
+    st_ref, st_gpu = _run_large_both(c, 3, lib, divdmp=0.1)
+    for n in STATE:
+        err = _field_err(st_gpu[n], st_ref[n], c.g)
+        assert err <= 1e-10, f"{n}: {err:.3e}"
