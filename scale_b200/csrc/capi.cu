@@ -431,6 +431,8 @@ int scale_hevi_setup(const scale_hevi_index *idx, const char *flux_type, const c
     if (x.IMAX < 2 || x.JMAX < 2) return fail(SCALE_HEVI_ERR_ARG, "IMAX and JMAX must be >= IHALO, JHALO");
     if ((x.IBLOCK > 0 && x.IBLOCK != x.IMAX) || (x.JBLOCK > 0 && x.JBLOCK != x.JMAX))
         return fail(SCALE_HEVI_ERR_UNSUPPORTED, "only the default IBLOCK=IMAX, JBLOCK=JMAX blocking is supported");
+    if ((double)x.KA * x.IA * x.JA >= 2147483648.0)
+        return fail(SCALE_HEVI_ERR_UNSUPPORTED, "a field of %d x %d x %d points exceeds 2^31 points", x.KA, x.IA, x.JA);
     int s1, s2;
     CK(parse_scheme(flux_type, &s1));
     CK(parse_scheme(flux_tracer_type, &s2));

@@ -125,11 +125,12 @@ struct Nd {
     __device__ const double *TY() const { return q(5, 3); }
 };
 
-#define AT(p, dk, di, dj) ld((p) + c + (long)(dk) + (long)(di) * sI + (long)(dj) * sJ)
+// cell offsets are 32-bit (a field has fewer than 2^31 points, checked at setup)
+#define AT(p, dk, di, dj) ld((p) + (int)(c + (dk) + (di) * sI + (dj) * sJ))
 
 // mass fluxes at the u/v faces of cell c, hevi_mflx_x/y :399-438
 struct MassFlux { double Xe, Xw, Yn, Ys; };
-__device__ __forceinline__ MassFlux mass_flux(const StageArgs &a, const Nd &nd, size_t c, long sI, long sJ)
+__device__ __forceinline__ MassFlux mass_flux(const StageArgs &a, const Nd &nd, int c, int sI, int sJ)
 {
     MassFlux m;
     m.Xe = AT(a.MOMX, 0, 0, 0) + AT(nd.DX(), 0, 0, 0);
@@ -142,8 +143,8 @@ __device__ __forceinline__ MassFlux mass_flux(const StageArgs &a, const Nd &nd, 
 // horizontal w-momentum flux divergence at cell c (k <= KE-1),
 // fluxX/Y_XYW (ud3.F90:598-748), hevi_sw :560-562
 template <int S>
-__device__ __forceinline__ double adv_w_h(const Grid &g, const StageArgs &a, const Nd &nd, size_t c, int k,
-                                          long sI, long sJ, double rcdx, double rcdy)
+__device__ __forceinline__ double adv_w_h(const Grid &g, const StageArgs &a, const Nd &nd, int c, int k,
+                                          int sI, int sJ, double rcdx, double rcdy)
 {
     const double *MX = a.MOMX, *MY = a.MOMY, *MZ = a.MOMZ, *DN = a.DENS;
     const double f1 = ld(g.F2H1 + k - 1), f2 = ld(g.F2H2 + k - 1);
@@ -173,8 +174,8 @@ template <int S, int V>
 __device__ __forceinline__ void update_mom(const Grid &g, const StageArgs &a, const Nd &nd, size_t N3, int k, int i, int j,
                                            bool valid)
 {
-    const size_t c = idx3(g, k, i, j);
-    const long sI = g.KA, sJ = (long)g.KA * g.IA;
+    const int c = (int)idx3(g, k, i, j);
+    const int sI = g.KA, sJ = g.KA * g.IA;
     const double *MX = a.MOMX, *MY = a.MOMY, *MZ = a.MOMZ, *DN = a.DENS, *RT = a.RHOT;
     const double dt = a.dtrk, J33G = a.J33G;
     const bool use_div = a.divdmp_coef != 0.0;
@@ -314,10 +315,10 @@ __global__ void __launch_bounds__(32 * HEVI_COL_TC, HEVI_COL_MINB) k_hevi_stage(
     const int i = i0 + tx, j = j0 + ty; // this warp's column in the k-parallel phases
     const bool col_ok = i <= g.IE && j <= g.JE;
     const size_t N3 = n3(g);
-    const long sI = g.KA, sJ = (long)g.KA * g.IA;
+    const int sI = g.KA, sJ = g.KA * g.IA;
     const int KS = g.KS, KE = g.KE;
     const int KP = col_pitch(g.KA);
-    const size_t col = idx3(g, 1, i, j); // offset of level 1 of this warp's column
+    const int col = (int)idx3(g, 1, i, j); // offset of level 1 of this warp's column
     const Nd nd(a, N3);
     const double dt = a.dtrk, J33G = a.J33G, dt2 = dt * dt;
     const bool use_div = a.divdmp_coef != 0.0;
@@ -339,7 +340,7 @@ __global__ void __launch_bounds__(32 * HEVI_COL_TC, HEVI_COL_MINB) k_hevi_stage(
     // ---- phase 1: POTT (:586-600), x/y mass fluxes (:399-438), Sr (:443-479), A (:696) ----
     if (col_ok) {
         for (int L = KS + lane; L <= KE; L += 32) {
-            const size_t c = col + L - 1;
+            const int c = col + L - 1;
             SA(CA_C, w, L) = ld(a.RHOT + c) / ld(a.DENS + c);
             const MassFlux m = mass_flux(a, nd, c, sI, sJ);
             const double adv_r = -((m.Xe - m.Xw) * rcdx + (m.Yn - m.Ys) * rcdy);
@@ -380,7 +381,7 @@ __global__ void __launch_bounds__(32 * HEVI_COL_TC, HEVI_COL_MINB) k_hevi_stage(
             tz = mZ * ti + lds(nd.TZ() + col + L - 1);
         };
         for (int L = KS + lane; L <= KE; L += 32) {
-            const size_t c = col + L - 1;
+            const int c = col + L - 1;
             double PT, tZ, PTm, tZm;
             pt_tz(L, PT, tZ);
             pt_tz(L - 1, PTm, tZm);
@@ -437,7 +438,7 @@ __global__ void __launch_bounds__(32 * HEVI_COL_TC, HEVI_COL_MINB) k_hevi_stage(
             double q_km = __shfl_up_sync(0xffffffffu, q_k, 1);
             if (!ok) continue;
             if (lane == 0) q_km = qZ_at(k - 1);
-            const size_t c = col + k - 1;
+            const int c = col + k - 1;
             const double adv_w = adv_w_h<S>(g, a, nd, c, k, sI, sJ, rcdx, rcdy);
             const double advcv = -(q_k - q_km) * ld(g.RFDZ + k - 1);
             const double wdmp = -ld(a.wdamp + k - 1) * CL(a.MOMZ0, k);
@@ -511,7 +512,7 @@ __global__ void __launch_bounds__(32 * HEVI_COL_TC, HEVI_COL_MINB) k_hevi_stage(
     // ---- phase 5: back-update, :728-790 ----
     if (col_ok) {
         for (int m = KS + lane; m <= KE; m += 32) {
-            const size_t c = col + m - 1;
+            const int c = col + m - 1;
             const double rcdz = ld(g.RCDZ + m - 1);
             const double Cm = SA(CA_C, w, m), Cm1 = SA(CA_C, w, m - 1);
             double adr, adt;
