@@ -42,6 +42,10 @@ L2_BYTES = 126 * 1024 * 1024
 STAGE_BYTES = (34 + 11) * 8
 NUMFILTER_BYTES = (7 + 15) * 8
 STEP_BYTES = 4 * STAGE_BYTES + NUMFILTER_BYTES
+# mixed precision: the 19 state and base-state fields stay FP64, the flux-like
+# fields (num_diff 15, tendencies 5, mflx_hi 3, tflx_hi 3) are FP32
+MIXED_STAGE_BYTES = (5 + 5 + 4) * 8 + 5 * 8 + (15 + 5 + 3 + 3) * 4
+MIXED_NUMFILTER_BYTES = 7 * 8 + 15 * 4
 
 
 def rank_info():
@@ -175,6 +179,7 @@ def run_b200(args):
     for v, n in enumerate(("DENS", "MOMZ", "MOMX", "MOMY", "RHOT")):
         st[v].copy_(to_dev(c.state[n], torch))
     X = dict(DENS=st[0], MOMZ=st[1], MOMX=st[2], MOMY=st[3], RHOT=st[4])
+    st0 = st.clone() if not args.no_mixed else None
     z = lambda k=1: torch.zeros(k * N3, dtype=torch.float64, device="cuda")  # noqa: E731
     mflx, tflx, nd = z(3), z(3), z(15)
     tend = {n: z() for n in ("DENS_t", "MOMZ_t", "MOMX_t", "MOMY_t", "RHOT_t")}
@@ -267,6 +272,74 @@ def run_b200(args):
         "gpu_launches": launches,
         "clocks": clocks,
     }
+
+    if not args.no_mixed:
+        # the same workload from the same initial state on the mixed-precision path
+        st_fp64 = st.clone()
+        st.copy_(st0)
+        del st0
+        f32 = lambda k=1: torch.zeros(k * N3, dtype=torch.float32, device="cuda")  # noqa: E731
+        mflx32, tflx32, nd32 = f32(3), f32(3), f32(15)
+        tend32 = {n: f32() for n in ("DENS_t", "MOMZ_t", "MOMX_t", "MOMY_t", "RHOT_t")}
+
+        def step_mixed():
+            hevi.ATMOS_DYN_numfilter_coef_mixed_dev(num_diff=nd32, CDZ=g.CDZ, CDX=g.CDX, CDY=g.CDY, FDZ=g.FDZ,
+                                                    FDX=g.FDX, FDY=g.FDY, DT=dts, REF_dens=ref["REF_dens"],
+                                                    REF_pott=ref["REF_pott"], ND_COEF=c.nd_coef, ND_ORDER=1,
+                                                    ND_SFC_FACT=1.0, ND_USE_RS=True, **X)
+            hevi.ATMOS_DYN_Tinteg_short_rk4_mixed_dev(
+                PROG=None, mflx_hi=mflx32, tflx_hi=tflx32, DPRES0=dp0, RT2P=rt2p, CORIOLI=cor, num_diff=nd32,
+                wdamp_coef=wd, divdmp_coef=0.0, DDIV=None, FLAG_FCT_MOMENTUM=False, FLAG_FCT_T=False,
+                FLAG_FCT_ALONG_STREAM=True, PHI=ref["PHI"], GSQRT=GS, J13G=J0, J23G=J0, J33G=1.0, MAPF=MAPF,
+                REF_dens=ref["REF_dens"], REF_rhot=refr, BND_W=False, BND_E=False, BND_S=False, BND_N=False,
+                dt=dts, **X, **tend32, **grid)
+            hevi.boundary_dev(**X)
+
+        for _ in range(args.warmup):
+            step_mixed()
+        hevi.check()
+        m0x = hevi.domain_sum_dev(X["DENS"], g.CDZ, g.CDX, g.CDY)
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        hevi.profile(True)
+        t0.record(stream)
+        for _ in range(args.steps):
+            step_mixed()
+        t1.record(stream)
+        torch.cuda.synchronize()
+        profm = hevi.profile_report()
+        hevi.profile(False)
+        hevi.check()
+        m1x = hevi.domain_sum_dev(X["DENS"], g.CDZ, g.CDX, g.CDY)
+        ms_mixed = max_over_ranks(t0.elapsed_time(t1), dist, "cuda") / args.steps
+        nsm, tsm = profm.get("hevi_stage_mixed", (0, 0.0))
+        sm_ms = tsm / max(nsm, 1)
+        ach = MIXED_STAGE_BYTES * cells / (sm_ms * 1e-3) / 1e9 if sm_ms > 0 else None
+        # error of the mixed state against the FP64 state after the same steps,
+        # relative to each field's largest magnitude over the interior
+        sl = (slice(g.KS - 1, g.KE), slice(g.IS - 1, g.IE), slice(g.JS - 1, g.JE))
+        errs = {}
+        for v, n in enumerate(("DENS", "MOMZ", "MOMX", "MOMY", "RHOT")):
+            a64 = st_fp64[v].view(g.JA, g.IA, g.KA).permute(2, 1, 0)[sl[0], sl[1], sl[2]]
+            a32 = st[v].view(g.JA, g.IA, g.KA).permute(2, 1, 0)[sl[0], sl[1], sl[2]]
+            d = (a32 - a64).abs()
+            scale = float(a64.abs().max())
+            errs[n] = {"max": float(d.max()) / scale, "rms": float(d.pow(2).mean().sqrt()) / scale}
+        out["mixed"] = {
+            "value": aggregate_rate(cells, world, 1, ms_mixed), "unit": UNIT, "ms_per_step": ms_mixed,
+            "speedup_vs_fp64": ms_step / ms_mixed,
+            "precision": "FP32 flux and divergence arithmetic and FP32 num_diff/tendency/flux arrays; FP64 state, "
+                         "base-state deviations, right-hand side and tridiagonal solve",
+            "error_vs_fp64": {"steps": args.warmup + args.steps, "fields": errs},
+            "mass_drift_rel": abs(m1x - m0x) / m0x,
+            "roofline": {"bound": "hbm", "kernel": "k_hevi_stage<float> (one HEVI stage)", "achieved": ach,
+                         "peak": hbm, "unit": "GB/s", "frac": (ach / hbm) if ach else None,
+                         "algorithmic_bytes_per_launch": MIXED_STAGE_BYTES * cells, "stage_ms": sm_ms,
+                         "step_frac": (4 * MIXED_STAGE_BYTES + MIXED_NUMFILTER_BYTES) * cells / (ms_mixed * 1e-3) / 1e9 / hbm},
+            "sections_ms_per_step": {k: v[1] / args.steps for k, v in profm.items()},
+        }
+        del st_fp64
 
     if rank == 0 and not args.no_e2e:
         out["e2e"] = run_e2e(args, c, hevi, torch)
@@ -429,6 +502,7 @@ def main():
     ap.add_argument("--e2e-calls", type=int, default=2)
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision measurement")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "b200":
         log("warm-up raised to the minimum of 3 steps")

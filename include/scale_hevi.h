@@ -145,6 +145,43 @@ int ATMOS_DYN_Tinteg_short_rk4_b200(SCALE_HEVI_TINTEG_SHORT_ARGS);
 int ATMOS_DYN_Tinteg_short_rk4_b200_dev(SCALE_HEVI_TINTEG_SHORT_ARGS);
 
 /* ---------------------------------------------------------------------------
+ * Mixed-precision RK4 short step (device arrays). No counterpart in the
+ * reference, which is either all FP64 or, built with -DSINGLE, all FP32. Flux
+ * and divergence arithmetic runs in FP32. The state (DENS..RHOT), DPRES0, RT2P,
+ * REF_dens, REF_rhot, the deviations from the base state, the right-hand side
+ * and the tridiagonal solve stay FP64. The flux-like arrays are FP32 buffers:
+ * mflx_hi, tflx_hi, the tendencies DENS_t..RHOT_t, num_diff and DDIV. The
+ * arguments are otherwise those of ATMOS_DYN_Tinteg_short_rk4_b200_dev.
+ * ------------------------------------------------------------------------- */
+#define SCALE_HEVI_TINTEG_SHORT_MIXED_ARGS                                                                     \
+    double *DENS, double *MOMZ, double *MOMX, double *MOMY, double *RHOT, double *PROG,                        \
+    float *mflx_hi, float *tflx_hi,                                                                            \
+    const float *DENS_t, const float *MOMZ_t, const float *MOMX_t, const float *MOMY_t, const float *RHOT_t,   \
+    const double *DPRES0, const double *RT2P, const double *CORIOLI,                                           \
+    const float *num_diff, const double *wdamp_coef, const double *divdmp_coef, const float *DDIV,             \
+    const int *FLAG_FCT_MOMENTUM, const int *FLAG_FCT_T, const int *FLAG_FCT_ALONG_STREAM,                     \
+    const double *CDZ, const double *FDZ, const double *FDX, const double *FDY,                                \
+    const double *RCDZ, const double *RCDX, const double *RCDY,                                                \
+    const double *RFDZ, const double *RFDX, const double *RFDY,                                                \
+    const double *PHI, const double *GSQRT, const double *J13G, const double *J23G, const double *J33G,        \
+    const double *MAPF, const double *REF_dens, const double *REF_rhot,                                        \
+    const int *BND_W, const int *BND_E, const int *BND_S, const int *BND_N,                                    \
+    const double *dt
+
+int ATMOS_DYN_Tinteg_short_rk4_b200_mixed_dev(SCALE_HEVI_TINTEG_SHORT_MIXED_ARGS);
+
+/* Numerical filter of the mixed-precision path: as
+ * ATMOS_DYN_numfilter_coef_b200_dev, with num_diff an FP32 device array. */
+#define SCALE_HEVI_NUMFILTER_MIXED_ARGS                                                                        \
+    float *num_diff,                                                                                           \
+    const double *DENS, const double *MOMZ, const double *MOMX, const double *MOMY, const double *RHOT,        \
+    const double *CDZ, const double *CDX, const double *CDY, const double *FDZ, const double *FDX,             \
+    const double *FDY, const double *DT, const double *REF_dens, const double *REF_pott,                       \
+    const double *ND_COEF, const int *ND_ORDER, const double *ND_SFC_FACT, const int *ND_USE_RS
+
+int ATMOS_DYN_numfilter_coef_b200_mixed_dev(SCALE_HEVI_NUMFILTER_MIXED_ARGS);
+
+/* ---------------------------------------------------------------------------
  * Numerical filter coefficients. Replaces ATMOS_DYN_numfilter_coef
  * (scalelib/src/atmos-rm/dynamics/scale_atmos_dyn_common.F90:385-985),
  * including the halo exchange of the fifteen num_diff components.

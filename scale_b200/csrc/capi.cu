@@ -45,6 +45,9 @@ struct Ctx {
     double *facc = nullptr;         // 6*N3
     double *colscr = nullptr;       // 3*N3 when HEVI_COL_SCRATCH
     double *phi = nullptr;          // numerical filter: 5*N3 (allocated on first use)
+    // mixed-precision path (allocated on first use): flux RK sums, column-solve
+    // sources and the filtered quantities in FP32
+    float *facc_f = nullptr, *colscr_f = nullptr, *phi_f = nullptr;
     double *tr = nullptr;           // tracer: RK1, RK2, phi_lo, anti(3), rjp, rjm = 8*N3
     double *lg = nullptr;           // large step: DENS00, RT2P, DPRES0, REF_rhot, mflx_av(3), DDIV = 8*N3
     double *sum_part = nullptr, *sum_out = nullptr;
@@ -123,11 +126,22 @@ int dalloc(double **p, size_t n)
     return SCALE_HEVI_OK;
 }
 
+int falloc(float **p, size_t n)
+{
+    if (cudaMalloc((void **)p, n * sizeof(float)) != cudaSuccess) {
+        *p = nullptr;
+        cudaGetLastError();
+        return fail(SCALE_HEVI_ERR_ALLOC, "cudaMalloc of %zu floats failed", n);
+    }
+    return SCALE_HEVI_OK;
+}
+
 void free_all()
 {
     double *bufs[] = {C.phi, C.colscr, C.d_tab, C.d_nd, C.rk[0], C.rk[1], C.acc, C.facc, C.tr, C.lg, C.sum_part, C.sum_out};
     for (double *b : bufs) if (b) cudaFree(b);
     for (auto &kv : C.stage) cudaFree(kv.second.first);
+    for (float *b : {C.facc_f, C.colscr_f, C.phi_f}) if (b) cudaFree(b);
     if (C.status) cudaFree(C.status);
     if (C.count) cudaFree(C.count);
     for (cudaEvent_t e : C.ev_pool) cudaEventDestroy(e);
@@ -284,7 +298,8 @@ int prepare_nd(const double *CDZ, const double *CDX, const double *CDY, const do
     return SCALE_HEVI_OK;
 }
 
-int halo(double *const *f, int n)
+template <typename T>
+int halo(T *const *f, int n)
 {
     C.launches += (n + 15) / 16;
     return timed("halo", [&] {
@@ -294,18 +309,32 @@ int halo(double *const *f, int n)
 }
 
 // ---- one stage ---------------------------------------------------------------
-struct StageIn {
+// F: type of the flux-like arrays (double: plain path, float: mixed precision)
+template <typename F>
+struct StageInT {
     const double *DENS0, *MOMZ0, *MOMX0, *MOMY0, *RHOT0;
     const double *DENS, *MOMZ, *MOMX, *MOMY, *RHOT;
-    const double *DENS_t, *MOMZ_t, *MOMX_t, *MOMY_t, *RHOT_t;
-    const double *DPRES0, *RT2P, *CORIOLI, *num_diff, *DDIV, *REF_dens, *REF_rhot;
+    const F *DENS_t, *MOMZ_t, *MOMX_t, *MOMY_t, *RHOT_t;
+    const double *DPRES0, *RT2P, *CORIOLI;
+    const F *num_diff, *DDIV;
+    const double *REF_dens, *REF_rhot;
     double divdmp, J33G;
 };
+using StageIn = StageInT<double>;
 
-int run_stage(const StageIn &in, double *const out[5], double *mflx, double *tflx, double dtrk, int mode)
+// the flux RK sums and the column-solve scratch of each precision
+template <typename F> F *facc_buf();
+template <typename F> F *colscr_buf();
+template <> double *facc_buf<double>() { return C.facc; }
+template <> float *facc_buf<float>() { return C.facc_f; }
+template <> double *colscr_buf<double>() { return C.colscr; }
+template <> float *colscr_buf<float>() { return C.colscr_f; }
+
+template <typename F>
+int run_stage(const StageInT<F> &in, double *const out[5], F *mflx, F *tflx, double dtrk, int mode)
 {
     if (in.divdmp != 0.0 && !in.DDIV) return fail(SCALE_HEVI_ERR_ARG, "divdmp_coef is nonzero but DDIV is NULL");
-    StageArgs a{};
+    StageArgsT<F> a{};
     a.DENS_RK = out[0]; a.MOMZ_RK = out[1]; a.MOMX_RK = out[2]; a.MOMY_RK = out[3]; a.RHOT_RK = out[4];
     a.mflx = mflx; a.tflx = tflx;
     a.DENS0 = in.DENS0; a.MOMZ0 = in.MOMZ0; a.MOMX0 = in.MOMX0; a.MOMY0 = in.MOMY0; a.RHOT0 = in.RHOT0;
@@ -314,8 +343,8 @@ int run_stage(const StageIn &in, double *const out[5], double *mflx, double *tfl
     a.DPRES0 = in.DPRES0; a.RT2P = in.RT2P; a.CORIOLI = in.CORIOLI; a.num_diff = in.num_diff;
     a.wdamp = C.d_wdamp; a.DDIV = in.DDIV; a.REF_dens = in.REF_dens; a.REF_rhot = in.REF_rhot;
     a.divdmp_coef = in.divdmp; a.J33G = in.J33G; a.dtrk = dtrk;
-    a.rk_mode = mode; a.acc = C.acc; a.facc = C.facc; a.status = C.status; a.colscr = C.colscr;
-    CK(timed("hevi_stage", [&] {
+    a.rk_mode = mode; a.acc = C.acc; a.facc = facc_buf<F>(); a.status = C.status; a.colscr = colscr_buf<F>();
+    CK(timed(sizeof(F) == sizeof(double) ? "hevi_stage" : "hevi_stage_mixed", [&] {
         CU(launch_hevi_stage(C.g, a, C.scheme, C.stream));
         return SCALE_HEVI_OK;
     }));
@@ -326,9 +355,10 @@ int run_stage(const StageIn &in, double *const out[5], double *mflx, double *tfl
 // RK4 short step on device arrays (tinteg_short_rk4.F90:199-650): stage s reads
 // the previous stage's buffer (halo filled on the device) and X0 = the input
 // state; the last stage writes the combined state in place.
-int run_rk4(double *X[5], double *mflx, double *tflx, const StageIn &base, double dt)
+template <typename F>
+int run_rk4(double *X[5], F *mflx, F *tflx, const StageInT<F> &base, double dt)
 {
-    StageIn in = base;
+    StageInT<F> in = base;
     in.DENS0 = X[0]; in.MOMZ0 = X[1]; in.MOMX0 = X[2]; in.MOMY0 = X[3]; in.RHOT0 = X[4];
     const double dts[4] = {dt / 2.0, dt / 2.0, dt, dt};
     const double *src[5] = {X[0], X[1], X[2], X[3], X[4]};
@@ -350,17 +380,25 @@ int run_rk4(double *X[5], double *mflx, double *tflx, const StageIn &base, doubl
     return SCALE_HEVI_OK;
 }
 
-int run_numfilter(double *num_diff, const double *DENS, const double *MOMZ, const double *MOMX, const double *MOMY,
+template <typename R>
+int run_numfilter(R *num_diff, const double *DENS, const double *MOMZ, const double *MOMX, const double *MOMY,
                   const double *RHOT, const double *REF_dens, const double *REF_pott)
 {
-    if (!C.phi) CK(dalloc(&C.phi, 5 * C.N3));
-    NdArgs a{num_diff, DENS, MOMZ, MOMX, MOMY, RHOT, REF_dens, REF_pott, C.phi};
-    CK(timed("numfilter", [&] {
+    R *phi;
+    if (sizeof(R) == sizeof(double)) {
+        if (!C.phi) CK(dalloc(&C.phi, 5 * C.N3));
+        phi = reinterpret_cast<R *>(C.phi);
+    } else {
+        if (!C.phi_f) CK(falloc(&C.phi_f, 5 * C.N3));
+        phi = reinterpret_cast<R *>(C.phi_f);
+    }
+    NdArgsT<R> a{num_diff, DENS, MOMZ, MOMX, MOMY, RHOT, REF_dens, REF_pott, phi};
+    CK(timed(sizeof(R) == sizeof(double) ? "numfilter" : "numfilter_mixed", [&] {
         CU(launch_numfilter(C.g, C.ndc, a, C.stream));
         return SCALE_HEVI_OK;
     }));
     C.launches += 2;
-    double *f[15];
+    R *f[15];
     for (int q = 0; q < 15; ++q) f[q] = num_diff + (size_t)q * C.N3;
     return halo(f, 15);
 }
@@ -609,6 +647,32 @@ int ATMOS_DYN_Tinteg_short_rk4_b200(SCALE_HEVI_TINTEG_SHORT_ARGS)
     CU(cudaStreamSynchronize(C.stream));
     (void)PROG; (void)FLAG_FCT_MOMENTUM; (void)FLAG_FCT_T; (void)FLAG_FCT_ALONG_STREAM; (void)PHI;
     return scale_hevi_check();
+}
+
+// ---- mixed precision: FP32 flux arithmetic, FP64 state and solve -----------------
+int ATMOS_DYN_Tinteg_short_rk4_b200_mixed_dev(SCALE_HEVI_TINTEG_SHORT_MIXED_ARGS)
+{
+    (void)PROG; (void)FLAG_FCT_MOMENTUM; (void)FLAG_FCT_T; (void)FLAG_FCT_ALONG_STREAM; (void)PHI;
+    CK(need_setup());
+    CK(check_bnd(BND_W, BND_E, BND_S, BND_N));
+    CK(check_flat(GSQRT, J13G, J23G, MAPF, true));
+    CK(prepare_tables(CDZ, FDZ, RCDZ, RFDZ, FDX, RCDX, RFDX, FDY, RCDY, RFDY, wdamp_coef, nullptr, nullptr));
+    if (!C.facc_f) CK(falloc(&C.facc_f, 6 * C.N3));
+    if (HEVI_COL_SCRATCH && !C.colscr_f) CK(falloc(&C.colscr_f, 3 * C.N3));
+    double *X[5] = {DENS, MOMZ, MOMX, MOMY, RHOT};
+    StageInT<float> base{nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
+                         DENS_t, MOMZ_t, MOMX_t, MOMY_t, RHOT_t, DPRES0, RT2P, CORIOLI, num_diff, DDIV, REF_dens, REF_rhot,
+                         *divdmp_coef, *J33G};
+    return run_rk4(X, mflx_hi, tflx_hi, base, *dt);
+}
+
+int ATMOS_DYN_numfilter_coef_b200_mixed_dev(SCALE_HEVI_NUMFILTER_MIXED_ARGS)
+{
+    CK(need_setup());
+    if (*ND_ORDER != 1) return fail(SCALE_HEVI_ERR_UNSUPPORTED, "ND_ORDER=%d is not supported (1 only)", *ND_ORDER);
+    if (!*ND_USE_RS) return fail(SCALE_HEVI_ERR_UNSUPPORTED, "ND_USE_RS=.false. is not supported");
+    CK(prepare_nd(CDZ, CDX, CDY, FDZ, FDX, FDY, *DT, *ND_COEF, *ND_ORDER, *ND_SFC_FACT));
+    return run_numfilter(num_diff, DENS, MOMZ, MOMX, MOMY, RHOT, REF_dens, REF_pott);
 }
 
 // ---- numerical filter --------------------------------------------------------

@@ -45,41 +45,45 @@ constexpr double GRAV = 9.80665;      // scale_const.F90:46
 constexpr double EPS = 2.220446049250313080847263336181640625e-16; // epsilon(0.0_RP)
 
 // SIGN(a,b) of Fortran = |a| with the sign bit of b
-__device__ __forceinline__ double fsign(double a, double b) { return copysign(fabs(a), b); }
+template <typename R>
+__device__ __forceinline__ R fsign(R a, R b) { return copysign(fabs(a), b); }
 __device__ __forceinline__ double fmax2(double a, double b) { return a > b ? a : b; }
 __device__ __forceinline__ double fmin2(double a, double b) { return a < b ? a : b; }
 
 // ---- 4-point face interpolation of the flux schemes --------------------------
 // UD3: scale_atmos_dyn_fvm_flux_ud3.F90:87-89,124-125 ; CD4: ..._cd4.F90:87-88,123-124
-// The face lies between v0 and vp1.
-template <int S>
-__device__ __forceinline__ double ip4(double vel, double vm1, double v0, double vp1, double vp2)
+// The face lies between v0 and vp1. R is the arithmetic type (double on the
+// plain path; float for the flux arithmetic of the mixed-precision path).
+template <int S, typename R>
+__device__ __forceinline__ R ip4(R vel, R vm1, R v0, R vp1, R vp2)
 {
     if (S == UD3) {
-        const double F31 = -1.0 / 12.0, F32 = 7.0 / 12.0, F33 = 3.0 / 12.0;
-        return (F31 * (vp2 + vm1) + F32 * (vp1 + v0)) - (F31 * (vp2 - vm1) + F33 * (vp1 - v0)) * fsign(1.0, vel);
+        const R F31 = R(-1.0 / 12.0), F32 = R(7.0 / 12.0), F33 = R(3.0 / 12.0);
+        return (F31 * (vp2 + vm1) + F32 * (vp1 + v0)) - (F31 * (vp2 - vm1) + F33 * (vp1 - v0)) * fsign(R(1.0), vel);
     } else {
-        const double F41 = 7.0 / 12.0, F42 = -1.0 / 12.0;
+        const R F41 = R(7.0 / 12.0), F42 = R(-1.0 / 12.0);
         return F41 * (vp1 + v0) + F42 * (vp2 + vm1);
     }
 }
 // value at the KS face from val(KS), val(KS+1), val(KS+2) (ud3.F90:142-145, cd4.F90:141)
-template <int S>
-__device__ __forceinline__ double ipL(double vel, double v0, double v1, double v2)
+template <int S, typename R>
+__device__ __forceinline__ R ipL(R vel, R v0, R v1, R v2)
 {
     if (S == UD3)
-        return 0.5 * (v1 + v0) * (0.5 + fsign(0.5, vel)) + (2.0 * v0 + 5.0 * v1 - v2) / 6.0 * (0.5 - fsign(0.5, vel));
+        return R(0.5) * (v1 + v0) * (R(0.5) + fsign(R(0.5), vel))
+               + (R(2.0) * v0 + R(5.0) * v1 - v2) / R(6.0) * (R(0.5) - fsign(R(0.5), vel));
     else
-        return 0.5 * (v1 + v0);
+        return R(0.5) * (v1 + v0);
 }
 // value at the KE-1 face from val(KE), val(KE-1), val(KE-2) (ud3.F90:146-149, cd4.F90:142)
-template <int S>
-__device__ __forceinline__ double ipH(double vel, double vE, double vE1, double vE2)
+template <int S, typename R>
+__device__ __forceinline__ R ipH(R vel, R vE, R vE1, R vE2)
 {
     if (S == UD3)
-        return (2.0 * vE + 5.0 * vE1 - vE2) / 6.0 * (0.5 + fsign(0.5, vel)) + 0.5 * (vE + vE1) * (0.5 - fsign(0.5, vel));
+        return (R(2.0) * vE + R(5.0) * vE1 - vE2) / R(6.0) * (R(0.5) + fsign(R(0.5), vel))
+               + R(0.5) * (vE + vE1) * (R(0.5) - fsign(R(0.5), vel));
     else
-        return 0.5 * (vE + vE1);
+        return R(0.5) * (vE + vE1);
 }
 
 // read-only load through the non-coherent cache

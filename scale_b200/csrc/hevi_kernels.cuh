@@ -12,12 +12,15 @@ struct NdCoef {
     const double *cdz, *fdz, *cdx, *fdx, *cdy, *fdy; // DIFF4 * D**4 (nd_coef_cdz, ...)
     double sfc;                                      // ND_SFC_FACT
 };
-struct NdArgs {
-    double *num_diff;
+template <typename R>
+struct NdArgsT {
+    R *num_diff;
     const double *DENS, *MOMZ, *MOMX, *MOMY, *RHOT, *REF_dens, *REF_pott;
-    double *phi; // 5*N3 scratch: the five filtered quantities at every point
+    R *phi; // 5*N3 scratch: the five filtered quantities at every point
 };
-cudaError_t launch_numfilter(const Grid &g, const NdCoef &c, const NdArgs &a, cudaStream_t st);
+using NdArgs = NdArgsT<double>;
+template <typename R>
+cudaError_t launch_numfilter(const Grid &g, const NdCoef &c, const NdArgsT<R> &a, cudaStream_t st);
 
 // ---- tracer advection (tracer.cu) ----
 struct TracerArgs {
@@ -36,10 +39,12 @@ struct TracerArgs {
 cudaError_t launch_tracer_stage(const Grid &g, const TracerArgs &a, int scheme, bool fct, cudaStream_t st);
 
 // ---- HEVI stage (hevi_stage.cu) ----
-cudaError_t launch_hevi_stage(const Grid &g, const StageArgs &a, int scheme, cudaStream_t st);
+template <typename R>
+cudaError_t launch_hevi_stage(const Grid &g, const StageArgsT<R> &a, int scheme, cudaStream_t st);
 
 // ---- utilities (misc.cu) ----
-void periodic_halo(const Grid &g, double *const *fields, int nf, cudaStream_t st);
+template <typename T>
+void periodic_halo(const Grid &g, T *const *fields, int nf, cudaStream_t st);
 void divergence(const Grid &g, double *DDIV, const double *MOMZ, const double *MOMX, const double *MOMY,
                 const double *RCDZ, const double *RCDX, const double *RCDY, double J33G, cudaStream_t st);
 void vertical_bc(const Grid &g, double *DENS, double *MOMZ, double *MOMX, double *MOMY, double *RHOT, cudaStream_t st);

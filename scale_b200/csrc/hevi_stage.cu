@@ -17,6 +17,14 @@
 // Every value keeps the reference's operation order, so the stage is
 // bit-identical to the sequential formulation.
 //
+// The kernel is a template on R, the type of the flux arithmetic and of the
+// flux-like arrays (num_diff, tendencies, DDIV, mflx_hi/tflx_hi, their RK sums,
+// the column-solve sources). R = double is the plain path above. R = float is
+// the mixed-precision path: fluxes and divergences in FP32, while the state,
+// the pressure and density deviations from the base state, the right-hand
+// side and the Thomas solve stay FP64. Every FP64 operand is converted with
+// R(...) at its use, which is the identity for R = double.
+//
 // Flat terrain only (see hevi_common.cuh). Line numbers below refer to the
 // reference HEVI file unless a flux file is named.
 #include "hevi_kernels.cuh"
@@ -43,58 +51,54 @@
 
 namespace hevi {
 
-// num_diff(:,:,:,v,dir) slice offset; v: DENS=1..RHOT=5, dir: Z=1,X=2,Y=3
-__device__ __forceinline__ const double *nd_slice(const StageArgs &a, size_t N3, int v, int dir)
+__device__ __forceinline__ void flag_nonfinite(unsigned *status, double v)
 {
-    return a.num_diff + N3 * (size_t)((v - 1) + 5 * (dir - 1));
-}
-
-__device__ __forceinline__ void flag_nonfinite(const StageArgs &a, double v)
-{
-    if (!isfinite(v)) atomicOr(a.status, ST_NONFINITE);
+    if (!isfinite(v)) atomicOr(status, ST_NONFINITE);
 }
 
 // Data a cell reads or writes once (tendencies, stage-0 state, outputs, RK sums)
 // go through the cache-streaming path, so that L2 keeps the fields whose x/y
 // neighbours other tiles read again.
 #if HEVI_STREAM_HINTS
-__device__ __forceinline__ double lds(const double *p) { return __ldcs(p); }
-__device__ __forceinline__ void sts(double *p, double v) { __stcs(p, v); }
+template <typename T> __device__ __forceinline__ T lds(const T *p) { return __ldcs(p); }
+template <typename T> __device__ __forceinline__ void sts(T *p, T v) { __stcs(p, v); }
 #else
-__device__ __forceinline__ double lds(const double *p) { return __ldg(p); }
-__device__ __forceinline__ void sts(double *p, double v) { *p = v; }
+template <typename T> __device__ __forceinline__ T lds(const T *p) { return __ldg(p); }
+template <typename T> __device__ __forceinline__ void sts(T *p, T v) { *p = v; }
 #endif
 
 // store one prognostic value of the stage, folding in the RK4 combine
-__device__ __forceinline__ void put_state(const StageArgs &a, size_t N3, int v, double *out, const double *x0,
+template <typename F>
+__device__ __forceinline__ void put_state(const StageArgsT<F> &a, size_t N3, int v, double *out, const double *x0,
                                           size_t c, double val, bool combine)
 {
     double *acc = a.acc + (size_t)v * N3 + c;
     switch (a.rk_mode) {
-    case RK_PLAIN: sts(out + c, val); flag_nonfinite(a, val); break;
+    case RK_PLAIN: sts(out + c, val); flag_nonfinite(a.status, val); break;
     case RK_STAGE1: sts(out + c, val); if (combine) sts(acc, val * 2.0); break;
     case RK_STAGE2: sts(out + c, val); if (combine) sts(acc, lds(acc) + val * 4.0); break;
     case RK_STAGE3: sts(out + c, val); if (combine) sts(acc, lds(acc) + val * 2.0); break;
     default: {
         double r = combine ? ((lds(acc) + val) - lds(x0 + c) * 3.0) / 6.0 : val;
         sts(out + c, r);
-        flag_nonfinite(a, r);
+        flag_nonfinite(a.status, r);
     }
     }
 }
 
 // store one flux value (f: 0..2 mflx Z,X,Y; 3..5 tflx Z,X,Y); 'interior' marks the
 // cells the RK4 combine averages (k in KS:KE, i in IS:IE, j in JS:JE)
-__device__ __forceinline__ void put_flux(const StageArgs &a, size_t N3, int f, size_t c, double val, bool interior)
+template <typename F>
+__device__ __forceinline__ void put_flux(const StageArgsT<F> &a, size_t N3, int f, size_t c, F val, bool interior)
 {
-    double *out = (f < 3 ? a.mflx : a.tflx) + (size_t)(f % 3) * N3 + c;
-    double *acc = a.facc + (size_t)f * N3 + c;
+    F *out = (f < 3 ? a.mflx : a.tflx) + (size_t)(f % 3) * N3 + c;
+    F *acc = a.facc + (size_t)f * N3 + c;
     switch (a.rk_mode) {
     case RK_PLAIN: sts(out, val); break;
     case RK_STAGE1: if (interior) sts(acc, val); break;
     case RK_STAGE2:
-    case RK_STAGE3: if (interior) sts(acc, lds(acc) + val * 2.0); break;
-    default: sts(out, interior ? (lds(acc) + val) / 6.0 : val);
+    case RK_STAGE3: if (interior) sts(acc, lds(acc) + val * F(2.0)); break;
+    default: sts(out, interior ? (lds(acc) + val) / F(6.0) : val);
     }
 }
 
@@ -103,120 +107,126 @@ __device__ __forceinline__ void put_flux(const StageArgs &a, size_t N3, int f, s
 // =============================================================================
 // num_diff components by (quantity, direction), computed at each use from the
 // kernel parameters so that no register holds fifteen pointers
+template <typename F>
 struct Nd {
-    const double *base;
+    const F *base;
     size_t N3;
-    __device__ Nd(const StageArgs &a, size_t n) : base(a.num_diff), N3(n) {}
-    __device__ const double *q(int v, int dir) const { return base + N3 * (size_t)((v - 1) + 5 * (dir - 1)); }
-    __device__ const double *DZ() const { return q(1, 1); }
-    __device__ const double *DX() const { return q(1, 2); }
-    __device__ const double *DY() const { return q(1, 3); }
-    __device__ const double *WZ() const { return q(2, 1); }
-    __device__ const double *WX() const { return q(2, 2); }
-    __device__ const double *WY() const { return q(2, 3); }
-    __device__ const double *UZ() const { return q(3, 1); }
-    __device__ const double *UX() const { return q(3, 2); }
-    __device__ const double *UY() const { return q(3, 3); }
-    __device__ const double *VZ() const { return q(4, 1); }
-    __device__ const double *VX() const { return q(4, 2); }
-    __device__ const double *VY() const { return q(4, 3); }
-    __device__ const double *TZ() const { return q(5, 1); }
-    __device__ const double *TX() const { return q(5, 2); }
-    __device__ const double *TY() const { return q(5, 3); }
+    __device__ Nd(const StageArgsT<F> &a, size_t n) : base(a.num_diff), N3(n) {}
+    __device__ const F *q(int v, int dir) const { return base + N3 * (size_t)((v - 1) + 5 * (dir - 1)); }
+    __device__ const F *DZ() const { return q(1, 1); }
+    __device__ const F *DX() const { return q(1, 2); }
+    __device__ const F *DY() const { return q(1, 3); }
+    __device__ const F *WZ() const { return q(2, 1); }
+    __device__ const F *WX() const { return q(2, 2); }
+    __device__ const F *WY() const { return q(2, 3); }
+    __device__ const F *UZ() const { return q(3, 1); }
+    __device__ const F *UX() const { return q(3, 2); }
+    __device__ const F *UY() const { return q(3, 3); }
+    __device__ const F *VZ() const { return q(4, 1); }
+    __device__ const F *VX() const { return q(4, 2); }
+    __device__ const F *VY() const { return q(4, 3); }
+    __device__ const F *TZ() const { return q(5, 1); }
+    __device__ const F *TX() const { return q(5, 2); }
+    __device__ const F *TY() const { return q(5, 3); }
 };
 
 // cell offsets are 32-bit (a field has fewer than 2^31 points, checked at setup)
 #define AT(p, dk, di, dj) ld((p) + (int)(c + (dk) + (di) * sI + (dj) * sJ))
+// an FP64 field used in the flux arithmetic
+#define AR(p, dk, di, dj) R(AT(p, dk, di, dj))
 
 // mass fluxes at the u/v faces of cell c, hevi_mflx_x/y :399-438
-struct MassFlux { double Xe, Xw, Yn, Ys; };
-__device__ __forceinline__ MassFlux mass_flux(const StageArgs &a, const Nd &nd, int c, int sI, int sJ)
+template <typename R> struct MassFlux { R Xe, Xw, Yn, Ys; };
+template <typename R>
+__device__ __forceinline__ MassFlux<R> mass_flux(const StageArgsT<R> &a, const Nd<R> &nd, int c, int sI, int sJ)
 {
-    MassFlux m;
-    m.Xe = AT(a.MOMX, 0, 0, 0) + AT(nd.DX(), 0, 0, 0);
-    m.Xw = AT(a.MOMX, 0, -1, 0) + AT(nd.DX(), 0, -1, 0);
-    m.Yn = AT(a.MOMY, 0, 0, 0) + AT(nd.DY(), 0, 0, 0);
-    m.Ys = AT(a.MOMY, 0, 0, -1) + AT(nd.DY(), 0, 0, -1);
+    MassFlux<R> m;
+    m.Xe = AR(a.MOMX, 0, 0, 0) + AT(nd.DX(), 0, 0, 0);
+    m.Xw = AR(a.MOMX, 0, -1, 0) + AT(nd.DX(), 0, -1, 0);
+    m.Yn = AR(a.MOMY, 0, 0, 0) + AT(nd.DY(), 0, 0, 0);
+    m.Ys = AR(a.MOMY, 0, 0, -1) + AT(nd.DY(), 0, 0, -1);
     return m;
 }
 
 // horizontal w-momentum flux divergence at cell c (k <= KE-1),
 // fluxX/Y_XYW (ud3.F90:598-748), hevi_sw :560-562
-template <int S>
-__device__ __forceinline__ double adv_w_h(const Grid &g, const StageArgs &a, const Nd &nd, int c, int k,
-                                          int sI, int sJ, double rcdx, double rcdy)
+template <int S, typename R>
+__device__ __forceinline__ R adv_w_h(const Grid &g, const StageArgsT<R> &a, const Nd<R> &nd, int c, int k,
+                                     int sI, int sJ, R rcdx, R rcdy)
 {
     const double *MX = a.MOMX, *MY = a.MOMY, *MZ = a.MOMZ, *DN = a.DENS;
-    const double f1 = ld(g.F2H1 + k - 1), f2 = ld(g.F2H2 + k - 1);
-    const double vXe = (f1 * AT(MX, 1, 0, 0) + f2 * AT(MX, 0, 0, 0))
-                       / (f1 * 0.5 * (AT(DN, 1, 0, 0) + AT(DN, 1, 1, 0)) + f2 * 0.5 * (AT(DN, 0, 0, 0) + AT(DN, 0, 1, 0)));
-    const double vXw = (f1 * AT(MX, 1, -1, 0) + f2 * AT(MX, 0, -1, 0))
-                       / (f1 * 0.5 * (AT(DN, 1, -1, 0) + AT(DN, 1, 0, 0)) + f2 * 0.5 * (AT(DN, 0, -1, 0) + AT(DN, 0, 0, 0)));
-    const double vYn = (f1 * AT(MY, 1, 0, 0) + f2 * AT(MY, 0, 0, 0))
-                       / (f1 * 0.5 * (AT(DN, 1, 0, 0) + AT(DN, 1, 0, 1)) + f2 * 0.5 * (AT(DN, 0, 0, 0) + AT(DN, 0, 0, 1)));
-    const double vYs = (f1 * AT(MY, 1, 0, -1) + f2 * AT(MY, 0, 0, -1))
-                       / (f1 * 0.5 * (AT(DN, 1, 0, -1) + AT(DN, 1, 0, 0)) + f2 * 0.5 * (AT(DN, 0, 0, -1) + AT(DN, 0, 0, 0)));
-    const double W_m2 = AT(MZ, 0, -2, 0), W_m1 = AT(MZ, 0, -1, 0), W_00 = AT(MZ, 0, 0, 0);
-    const double W_p1 = AT(MZ, 0, 1, 0), W_p2 = AT(MZ, 0, 2, 0);
-    const double V_m2 = AT(MZ, 0, 0, -2), V_m1 = AT(MZ, 0, 0, -1), V_p1 = AT(MZ, 0, 0, 1), V_p2 = AT(MZ, 0, 0, 2);
-    const double qXe = vXe * ip4<S>(vXe, W_m1, W_00, W_p1, W_p2) + AT(nd.WX(), 0, 0, 0);
-    const double qXw = vXw * ip4<S>(vXw, W_m2, W_m1, W_00, W_p1) + AT(nd.WX(), 0, -1, 0);
-    const double qYn = vYn * ip4<S>(vYn, V_m1, W_00, V_p1, V_p2) + AT(nd.WY(), 0, 0, 0);
-    const double qYs = vYs * ip4<S>(vYs, V_m2, V_m1, W_00, V_p1) + AT(nd.WY(), 0, 0, -1);
+    const R f1 = R(ld(g.F2H1 + k - 1)), f2 = R(ld(g.F2H2 + k - 1)), h = R(0.5);
+    const R vXe = (f1 * AR(MX, 1, 0, 0) + f2 * AR(MX, 0, 0, 0))
+                  / (f1 * h * (AR(DN, 1, 0, 0) + AR(DN, 1, 1, 0)) + f2 * h * (AR(DN, 0, 0, 0) + AR(DN, 0, 1, 0)));
+    const R vXw = (f1 * AR(MX, 1, -1, 0) + f2 * AR(MX, 0, -1, 0))
+                  / (f1 * h * (AR(DN, 1, -1, 0) + AR(DN, 1, 0, 0)) + f2 * h * (AR(DN, 0, -1, 0) + AR(DN, 0, 0, 0)));
+    const R vYn = (f1 * AR(MY, 1, 0, 0) + f2 * AR(MY, 0, 0, 0))
+                  / (f1 * h * (AR(DN, 1, 0, 0) + AR(DN, 1, 0, 1)) + f2 * h * (AR(DN, 0, 0, 0) + AR(DN, 0, 0, 1)));
+    const R vYs = (f1 * AR(MY, 1, 0, -1) + f2 * AR(MY, 0, 0, -1))
+                  / (f1 * h * (AR(DN, 1, 0, -1) + AR(DN, 1, 0, 0)) + f2 * h * (AR(DN, 0, 0, -1) + AR(DN, 0, 0, 0)));
+    const R W_m2 = AR(MZ, 0, -2, 0), W_m1 = AR(MZ, 0, -1, 0), W_00 = AR(MZ, 0, 0, 0);
+    const R W_p1 = AR(MZ, 0, 1, 0), W_p2 = AR(MZ, 0, 2, 0);
+    const R V_m2 = AR(MZ, 0, 0, -2), V_m1 = AR(MZ, 0, 0, -1), V_p1 = AR(MZ, 0, 0, 1), V_p2 = AR(MZ, 0, 0, 2);
+    const R qXe = vXe * ip4<S>(vXe, W_m1, W_00, W_p1, W_p2) + AT(nd.WX(), 0, 0, 0);
+    const R qXw = vXw * ip4<S>(vXw, W_m2, W_m1, W_00, W_p1) + AT(nd.WX(), 0, -1, 0);
+    const R qYn = vYn * ip4<S>(vYn, V_m1, W_00, V_p1, V_p2) + AT(nd.WY(), 0, 0, 0);
+    const R qYs = vYs * ip4<S>(vYs, V_m2, V_m1, W_00, V_p1) + AT(nd.WY(), 0, 0, -1);
     return -((qXe - qXw) * rcdx + (qYn - qYs) * rcdy);
 }
 
-// rho*u and rho*v of cell (k,i,j), hevi_momx :814-928 and hevi_momy :934-1048.
+// rho*u (V = 0, hevi_momx :814-928) or rho*v (V = 1, hevi_momy :934-1048) of cell (k,i,j).
 // Called by all 32 lanes of a warp for 32 consecutive levels of one column;
 // 'valid' is false for lanes above KE. The z-face flux below a level is the
-// one above the level of the previous lane, passed by a warp shuffle.
-template <int S, int V>
-__device__ __forceinline__ void update_mom(const Grid &g, const StageArgs &a, const Nd &nd, size_t N3, int k, int i, int j,
-                                           bool valid)
+// one above the level of the previous lane, passed by a warp shuffle. The
+// advective and Coriolis terms are flux arithmetic (R); the pressure gradient
+// of the deviation from the base state and the update of the state are FP64.
+template <int S, int V, typename R>
+__device__ __forceinline__ void update_mom(const Grid &g, const StageArgsT<R> &a, const Nd<R> &nd, size_t N3, int k, int i,
+                                           int j, bool valid)
 {
     const int c = (int)idx3(g, k, i, j);
     const int sI = g.KA, sJ = g.KA * g.IA;
     const double *MX = a.MOMX, *MY = a.MOMY, *MZ = a.MOMZ, *DN = a.DENS, *RT = a.RHOT;
-    const double dt = a.dtrk, J33G = a.J33G;
+    const double dt = a.dtrk;
+    const R J33G = R(a.J33G), h = R(0.5), qr = R(0.25);
     const bool use_div = a.divdmp_coef != 0.0;
-    const double ddc = use_div ? a.divdmp_coef / dt : 0.0;
+    const R ddc = use_div ? R(a.divdmp_coef / dt) : R(0.0);
     const int KS = g.KS, KE = g.KE;
     const unsigned FULL = 0xffffffffu;
 
     // z flux at (u,y,w), fluxZ_UYZ (ud3.F90:753-859); m is the lower level of the face
-    auto qZu = [&](int m) -> double {
-        if (m < KS || m > KE - 1) return 0.0;
+    auto qZu = [&](int m) -> R {
+        if (m < KS || m > KE - 1) return R(0.0);
         const long dm = m - k;
-        const double den = ld(g.F2H1 + m - 1) * 0.5 * (AT(DN, dm + 1, 0, 0) + AT(DN, dm + 1, 1, 0))
-                           + ld(g.F2H2 + m - 1) * 0.5 * (AT(DN, dm, 0, 0) + AT(DN, dm, 1, 0));
-        const double vel = (0.5 * (AT(MZ, dm, 0, 0) + AT(MZ, dm, 1, 0))) / den;
-        double q;
-        if (m == KS) q = ipL<S>(vel, AT(MX, dm, 0, 0), AT(MX, dm + 1, 0, 0), AT(MX, dm + 2, 0, 0));
-        else if (m == KE - 1) q = ipH<S>(vel, AT(MX, dm + 1, 0, 0), AT(MX, dm, 0, 0), AT(MX, dm - 1, 0, 0));
-        else q = ip4<S>(vel, AT(MX, dm - 1, 0, 0), AT(MX, dm, 0, 0), AT(MX, dm + 1, 0, 0), AT(MX, dm + 2, 0, 0));
+        const R den = R(ld(g.F2H1 + m - 1)) * h * (AR(DN, dm + 1, 0, 0) + AR(DN, dm + 1, 1, 0))
+                      + R(ld(g.F2H2 + m - 1)) * h * (AR(DN, dm, 0, 0) + AR(DN, dm, 1, 0));
+        const R vel = (h * (AR(MZ, dm, 0, 0) + AR(MZ, dm, 1, 0))) / den;
+        R q;
+        if (m == KS) q = ipL<S>(vel, AR(MX, dm, 0, 0), AR(MX, dm + 1, 0, 0), AR(MX, dm + 2, 0, 0));
+        else if (m == KE - 1) q = ipH<S>(vel, AR(MX, dm + 1, 0, 0), AR(MX, dm, 0, 0), AR(MX, dm - 1, 0, 0));
+        else q = ip4<S>(vel, AR(MX, dm - 1, 0, 0), AR(MX, dm, 0, 0), AR(MX, dm + 1, 0, 0), AR(MX, dm + 2, 0, 0));
         return J33G * vel * q + lds(nd.UZ() + c + dm);
     };
     // z flux at (x,v,w), fluxZ_XVZ (ud3.F90:1173-1279)
-    auto qZv = [&](int m) -> double {
-        if (m < KS || m > KE - 1) return 0.0;
+    auto qZv = [&](int m) -> R {
+        if (m < KS || m > KE - 1) return R(0.0);
         const long dm = m - k;
-        const double den = ld(g.F2H1 + m - 1) * 0.5 * (AT(DN, dm + 1, 0, 0) + AT(DN, dm + 1, 0, 1))
-                           + ld(g.F2H2 + m - 1) * 0.5 * (AT(DN, dm, 0, 0) + AT(DN, dm, 0, 1));
-        const double vel = (0.5 * (AT(MZ, dm, 0, 0) + AT(MZ, dm, 0, 1))) / den;
-        double q;
-        if (m == KS) q = ipL<S>(vel, AT(MY, dm, 0, 0), AT(MY, dm + 1, 0, 0), AT(MY, dm + 2, 0, 0));
-        else if (m == KE - 1) q = ipH<S>(vel, AT(MY, dm + 1, 0, 0), AT(MY, dm, 0, 0), AT(MY, dm - 1, 0, 0));
-        else q = ip4<S>(vel, AT(MY, dm - 1, 0, 0), AT(MY, dm, 0, 0), AT(MY, dm + 1, 0, 0), AT(MY, dm + 2, 0, 0));
+        const R den = R(ld(g.F2H1 + m - 1)) * h * (AR(DN, dm + 1, 0, 0) + AR(DN, dm + 1, 0, 1))
+                      + R(ld(g.F2H2 + m - 1)) * h * (AR(DN, dm, 0, 0) + AR(DN, dm, 0, 1));
+        const R vel = (h * (AR(MZ, dm, 0, 0) + AR(MZ, dm, 0, 1))) / den;
+        R q;
+        if (m == KS) q = ipL<S>(vel, AR(MY, dm, 0, 0), AR(MY, dm + 1, 0, 0), AR(MY, dm + 2, 0, 0));
+        else if (m == KE - 1) q = ipH<S>(vel, AR(MY, dm + 1, 0, 0), AR(MY, dm, 0, 0), AR(MY, dm - 1, 0, 0));
+        else q = ip4<S>(vel, AR(MY, dm - 1, 0, 0), AR(MY, dm, 0, 0), AR(MY, dm + 1, 0, 0), AR(MY, dm + 2, 0, 0));
         return J33G * vel * q + lds(nd.VZ() + c + dm);
     };
 
     // the flux through the face above this level; the one below comes from the
     // lane of the level below (lane 0 computes it)
-    // V = 0: rho*u (the face is u-staggered), V = 1: rho*v
     const bool do_u = V == 0 && i <= g.IEH, do_v = V == 1 && j <= g.JEH;
     if (!do_u && !do_v) return; // warp-uniform
-    const double q_k = valid ? (V == 0 ? qZu(k) : qZv(k)) : 0.0;
-    double q_km = __shfl_up_sync(FULL, q_k, 1);
+    const R q_k = valid ? (V == 0 ? qZu(k) : qZv(k)) : R(0.0);
+    R q_km = __shfl_up_sync(FULL, q_k, 1);
     if (!valid) return;
     if (threadIdx.x == 0) q_km = V == 0 ? qZu(k - 1) : qZv(k - 1);
 
@@ -224,56 +234,58 @@ __device__ __forceinline__ void update_mom(const Grid &g, const StageArgs &a, co
     const double DP00 = AT(a.DPRES0, 0, 0, 0) + AT(a.RT2P, 0, 0, 0) * (AT(RT, 0, 0, 0) - AT(a.REF_rhot, 0, 0, 0));
 
     if (do_u) {
-        const double rcdy = ld(g.RCDY + j - 1), rfdx = ld(g.RFDX + i - 1), fdx = ld(g.FDX + i - 1);
-        const double cor_u = 0.125 * (ld(a.CORIOLI + (i) + (size_t)g.IA * (j - 1)) + ld(a.CORIOLI + (i - 1) + (size_t)g.IA * (j - 1)));
-        const double U_m2 = AT(MX, 0, -2, 0), U_m1 = AT(MX, 0, -1, 0), U_00 = AT(MX, 0, 0, 0);
-        const double U_p1 = AT(MX, 0, 1, 0), U_p2 = AT(MX, 0, 2, 0);
+        const R rcdy = R(ld(g.RCDY + j - 1)), fdx = R(ld(g.FDX + i - 1));
+        const double rfdx = ld(g.RFDX + i - 1);
+        const R cor_u = R(0.125) * (R(ld(a.CORIOLI + (i) + (size_t)g.IA * (j - 1))) + R(ld(a.CORIOLI + (i - 1) + (size_t)g.IA * (j - 1))));
+        const R U_m2 = AR(MX, 0, -2, 0), U_m1 = AR(MX, 0, -1, 0), U_00 = AR(MX, 0, 0, 0);
+        const R U_p1 = AR(MX, 0, 1, 0), U_p2 = AR(MX, 0, 2, 0);
         // x flux at (x,y,z) with the index shift of fluxX_UYZ (ud3.F90:1053-1109)
-        const double vE = (0.5 * (U_p1 + U_00)) / (AT(DN, 0, 1, 0));
-        const double qXe = vE * ip4<S>(vE, U_m1, U_00, U_p1, U_p2) + AT(nd.UX(), 0, 1, 0);
-        const double vW = (0.5 * (U_00 + U_m1)) / (AT(DN, 0, 0, 0));
-        const double qXw = vW * ip4<S>(vW, U_m2, U_m1, U_00, U_p1) + AT(nd.UX(), 0, 0, 0);
+        const R vE = (h * (U_p1 + U_00)) / (AR(DN, 0, 1, 0));
+        const R qXe = vE * ip4<S>(vE, U_m1, U_00, U_p1, U_p2) + AT(nd.UX(), 0, 1, 0);
+        const R vW = (h * (U_00 + U_m1)) / (AR(DN, 0, 0, 0));
+        const R qXw = vW * ip4<S>(vW, U_m2, U_m1, U_00, U_p1) + AT(nd.UX(), 0, 0, 0);
         // y flux at (u,v,z), fluxY_UYZ (ud3.F90:1113-1167)
-        const double vN = (0.5 * (AT(MY, 0, 0, 0) + AT(MY, 0, 1, 0)))
-                          / (0.25 * (AT(DN, 0, 0, 0) + AT(DN, 0, 1, 0) + AT(DN, 0, 0, 1) + AT(DN, 0, 1, 1)));
-        const double qYn = vN * ip4<S>(vN, AT(MX, 0, 0, -1), U_00, AT(MX, 0, 0, 1), AT(MX, 0, 0, 2)) + AT(nd.UY(), 0, 0, 0);
-        const double vS = (0.5 * (AT(MY, 0, 0, -1) + AT(MY, 0, 1, -1)))
-                          / (0.25 * (AT(DN, 0, 0, -1) + AT(DN, 0, 1, -1) + AT(DN, 0, 0, 0) + AT(DN, 0, 1, 0)));
-        const double qYs = vS * ip4<S>(vS, AT(MX, 0, 0, -2), AT(MX, 0, 0, -1), U_00, AT(MX, 0, 0, 1)) + AT(nd.UY(), 0, 0, -1);
-        const double advcv = -(q_k - q_km) * ld(g.RCDZ + k - 1);
-        const double advch = -((qXe - qXw) * rfdx + (qYn - qYs) * rcdy);
+        const R vN = (h * (AR(MY, 0, 0, 0) + AR(MY, 0, 1, 0)))
+                     / (qr * (AR(DN, 0, 0, 0) + AR(DN, 0, 1, 0) + AR(DN, 0, 0, 1) + AR(DN, 0, 1, 1)));
+        const R qYn = vN * ip4<S>(vN, AR(MX, 0, 0, -1), U_00, AR(MX, 0, 0, 1), AR(MX, 0, 0, 2)) + AT(nd.UY(), 0, 0, 0);
+        const R vS = (h * (AR(MY, 0, 0, -1) + AR(MY, 0, 1, -1)))
+                     / (qr * (AR(DN, 0, 0, -1) + AR(DN, 0, 1, -1) + AR(DN, 0, 0, 0) + AR(DN, 0, 1, 0)));
+        const R qYs = vS * ip4<S>(vS, AR(MX, 0, 0, -2), AR(MX, 0, 0, -1), U_00, AR(MX, 0, 0, 1)) + AT(nd.UY(), 0, 0, -1);
+        const R advcv = -(q_k - q_km) * R(ld(g.RCDZ + k - 1));
+        const R advch = -((qXe - qXw) * R(rfdx) + (qYn - qYs) * rcdy);
         const double DPe = AT(a.DPRES0, 0, 1, 0) + AT(a.RT2P, 0, 1, 0) * (AT(RT, 0, 1, 0) - AT(a.REF_rhot, 0, 1, 0));
         const double pg = (DPe - DP00) * rfdx;
-        const double cf = cor_u * (AT(MY, 0, 1, 0) + AT(MY, 0, 0, 0) + AT(MY, 0, 1, -1) + AT(MY, 0, 0, -1));
-        const double div = use_div ? ddc * (AT(a.DDIV, 0, 1, 0) - AT(a.DDIV, 0, 0, 0)) * fdx : 0.0;
-        const double val = lds(a.MOMX0 + c) + dt * ((((advcv + advch) - pg) + cf) + div + lds(a.MOMX_t + c));
+        const R cf = cor_u * (AR(MY, 0, 1, 0) + AR(MY, 0, 0, 0) + AR(MY, 0, 1, -1) + AR(MY, 0, 0, -1));
+        const R div = use_div ? ddc * (AT(a.DDIV, 0, 1, 0) - AT(a.DDIV, 0, 0, 0)) * fdx : R(0.0);
+        const double val = lds(a.MOMX0 + c) + dt * (((((double)(advcv + advch)) - pg) + (double)cf) + (double)div + (double)lds(a.MOMX_t + c));
         put_state(a, N3, 2, a.MOMX_RK, a.MOMX0, c, val, true);
     }
 
     if (do_v) {
-        const double rcdx = ld(g.RCDX + i - 1), rfdy = ld(g.RFDY + j - 1), fdy = ld(g.FDY + j - 1);
-        const double cor_v = -0.125 * (ld(a.CORIOLI + (i - 1) + (size_t)g.IA * (j)) + ld(a.CORIOLI + (i - 1) + (size_t)g.IA * (j - 1)));
-        const double Y_m2 = AT(MY, 0, 0, -2), Y_m1 = AT(MY, 0, 0, -1), Y_00 = AT(MY, 0, 0, 0);
-        const double Y_p1 = AT(MY, 0, 0, 1), Y_p2 = AT(MY, 0, 0, 2);
+        const R rcdx = R(ld(g.RCDX + i - 1)), fdy = R(ld(g.FDY + j - 1));
+        const double rfdy = ld(g.RFDY + j - 1);
+        const R cor_v = R(-0.125) * (R(ld(a.CORIOLI + (i - 1) + (size_t)g.IA * (j))) + R(ld(a.CORIOLI + (i - 1) + (size_t)g.IA * (j - 1))));
+        const R Y_m2 = AR(MY, 0, 0, -2), Y_m1 = AR(MY, 0, 0, -1), Y_00 = AR(MY, 0, 0, 0);
+        const R Y_p1 = AR(MY, 0, 0, 1), Y_p2 = AR(MY, 0, 0, 2);
         // x flux at (u,v,z), fluxX_XVZ (ud3.F90:1473-1527)
-        const double vE = (0.5 * (AT(MX, 0, 0, 0) + AT(MX, 0, 0, 1)))
-                          / (0.25 * (AT(DN, 0, 0, 0) + AT(DN, 0, 1, 0) + AT(DN, 0, 0, 1) + AT(DN, 0, 1, 1)));
-        const double qXe = vE * ip4<S>(vE, AT(MY, 0, -1, 0), Y_00, AT(MY, 0, 1, 0), AT(MY, 0, 2, 0)) + AT(nd.VX(), 0, 0, 0);
-        const double vW = (0.5 * (AT(MX, 0, -1, 0) + AT(MX, 0, -1, 1)))
-                          / (0.25 * (AT(DN, 0, -1, 0) + AT(DN, 0, 0, 0) + AT(DN, 0, -1, 1) + AT(DN, 0, 0, 1)));
-        const double qXw = vW * ip4<S>(vW, AT(MY, 0, -2, 0), AT(MY, 0, -1, 0), Y_00, AT(MY, 0, 1, 0)) + AT(nd.VX(), 0, -1, 0);
+        const R vE = (h * (AR(MX, 0, 0, 0) + AR(MX, 0, 0, 1)))
+                     / (qr * (AR(DN, 0, 0, 0) + AR(DN, 0, 1, 0) + AR(DN, 0, 0, 1) + AR(DN, 0, 1, 1)));
+        const R qXe = vE * ip4<S>(vE, AR(MY, 0, -1, 0), Y_00, AR(MY, 0, 1, 0), AR(MY, 0, 2, 0)) + AT(nd.VX(), 0, 0, 0);
+        const R vW = (h * (AR(MX, 0, -1, 0) + AR(MX, 0, -1, 1)))
+                     / (qr * (AR(DN, 0, -1, 0) + AR(DN, 0, 0, 0) + AR(DN, 0, -1, 1) + AR(DN, 0, 0, 1)));
+        const R qXw = vW * ip4<S>(vW, AR(MY, 0, -2, 0), AR(MY, 0, -1, 0), Y_00, AR(MY, 0, 1, 0)) + AT(nd.VX(), 0, -1, 0);
         // y flux with the index shift of fluxY_XVZ (ud3.F90:1531-1587)
-        const double vN = (0.5 * (Y_p1 + Y_00)) / (AT(DN, 0, 0, 1));
-        const double qYn = vN * ip4<S>(vN, Y_m1, Y_00, Y_p1, Y_p2) + AT(nd.VY(), 0, 0, 1);
-        const double vS = (0.5 * (Y_00 + Y_m1)) / (AT(DN, 0, 0, 0));
-        const double qYs = vS * ip4<S>(vS, Y_m2, Y_m1, Y_00, Y_p1) + AT(nd.VY(), 0, 0, 0);
-        const double advcv = -(q_k - q_km) * ld(g.RCDZ + k - 1);
-        const double advch = -((qXe - qXw) * rcdx + (qYn - qYs) * rfdy);
+        const R vN = (h * (Y_p1 + Y_00)) / (AR(DN, 0, 0, 1));
+        const R qYn = vN * ip4<S>(vN, Y_m1, Y_00, Y_p1, Y_p2) + AT(nd.VY(), 0, 0, 1);
+        const R vS = (h * (Y_00 + Y_m1)) / (AR(DN, 0, 0, 0));
+        const R qYs = vS * ip4<S>(vS, Y_m2, Y_m1, Y_00, Y_p1) + AT(nd.VY(), 0, 0, 0);
+        const R advcv = -(q_k - q_km) * R(ld(g.RCDZ + k - 1));
+        const R advch = -((qXe - qXw) * rcdx + (qYn - qYs) * R(rfdy));
         const double DPn = AT(a.DPRES0, 0, 0, 1) + AT(a.RT2P, 0, 0, 1) * (AT(RT, 0, 0, 1) - AT(a.REF_rhot, 0, 0, 1));
         const double pg = (DPn - DP00) * rfdy;
-        const double cf = cor_v * (AT(MX, 0, 0, 1) + AT(MX, 0, 0, 0) + AT(MX, 0, -1, 1) + AT(MX, 0, -1, 0));
-        const double div = use_div ? ddc * (AT(a.DDIV, 0, 0, 1) - AT(a.DDIV, 0, 0, 0)) * fdy : 0.0;
-        const double val = lds(a.MOMY0 + c) + dt * ((((advcv + advch) - pg) + cf) + div + lds(a.MOMY_t + c));
+        const R cf = cor_v * (AR(MX, 0, 0, 1) + AR(MX, 0, 0, 0) + AR(MX, 0, -1, 1) + AR(MX, 0, -1, 0));
+        const R div = use_div ? ddc * (AT(a.DDIV, 0, 0, 1) - AT(a.DDIV, 0, 0, 0)) * fdy : R(0.0);
+        const double val = lds(a.MOMY0 + c) + dt * (((((double)(advcv + advch)) - pg) + (double)cf) + (double)div + (double)lds(a.MOMY_t + c));
         put_state(a, N3, 3, a.MOMY_RK, a.MOMY0, c, val, true);
     }
 }
@@ -294,8 +306,8 @@ enum ColArr : int { CA_C = 0, CA_PT = 1, CA_A = 2, CA_SR = 3, CA_ST = 4, CA_TZ =
 
 __host__ __device__ inline int col_pitch(int KA) { return KA | 1; }
 
-template <int S>
-__global__ void __launch_bounds__(32 * HEVI_COL_TC, HEVI_COL_MINB) k_hevi_stage(const Grid g, const StageArgs a)
+template <int S, typename R>
+__global__ void __launch_bounds__(32 * HEVI_COL_TC, HEVI_COL_MINB) k_hevi_stage(const Grid g, const StageArgsT<R> a)
 {
     extern __shared__ double sm[];
     constexpr int TX = HEVI_TILE_X, TY = HEVI_TILE_Y, TC = TX * TY;
@@ -319,11 +331,11 @@ __global__ void __launch_bounds__(32 * HEVI_COL_TC, HEVI_COL_MINB) k_hevi_stage(
     const int KS = g.KS, KE = g.KE;
     const int KP = col_pitch(g.KA);
     const int col = (int)idx3(g, 1, i, j); // offset of level 1 of this warp's column
-    const Nd nd(a, N3);
+    const Nd<R> nd(a, N3);
     const double dt = a.dtrk, J33G = a.J33G, dt2 = dt * dt;
     const bool use_div = a.divdmp_coef != 0.0;
-    const double ddc = use_div ? a.divdmp_coef / dt : 0.0;
-    const double rcdx = col_ok ? ld(g.RCDX + i - 1) : 0.0, rcdy = col_ok ? ld(g.RCDY + j - 1) : 0.0;
+    const R ddc = use_div ? R(a.divdmp_coef / dt) : R(0.0);
+    const R rcdx = col_ok ? R(ld(g.RCDX + i - 1)) : R(0.0), rcdy = col_ok ? R(ld(g.RCDY + j - 1)) : R(0.0);
     // shared arrays: SA(arr, cc, L) for column cc of the tile, level L (1-based)
 #define SA(arr, cc, L) sm[((size_t)(arr) * TC + (cc)) * KP + (L) - 1]
 #define CL(p, L) ld((p) + col + (L) - 1)
@@ -334,46 +346,46 @@ __global__ void __launch_bounds__(32 * HEVI_COL_TC, HEVI_COL_MINB) k_hevi_stage(
 #define XS(q, L) __ldcg(a.colscr + (size_t)((q) - CA_SR) * N3 + col + (L) - 1)
 #else
 #define XS_PUT(q, L, v) (SA(q, w, L) = (v))
-#define XS(q, L) SA(q, w, L)
+#define XS(q, L) R(SA(q, w, L))
 #endif
 
     // ---- phase 1: POTT (:586-600), x/y mass fluxes (:399-438), Sr (:443-479), A (:696) ----
     if (col_ok) {
         for (int L = KS + lane; L <= KE; L += 32) {
             const int c = col + L - 1;
-            SA(CA_C, w, L) = ld(a.RHOT + c) / ld(a.DENS + c);
-            const MassFlux m = mass_flux(a, nd, c, sI, sJ);
-            const double adv_r = -((m.Xe - m.Xw) * rcdx + (m.Yn - m.Ys) * rcdy);
+            SA(CA_C, w, L) = R(ld(a.RHOT + c)) / R(ld(a.DENS + c));
+            const MassFlux<R> m = mass_flux(a, nd, c, sI, sJ);
+            const R adv_r = -((m.Xe - m.Xw) * rcdx + (m.Yn - m.Ys) * rcdy);
             put_flux(a, N3, 1, c, m.Xe, true);
             put_flux(a, N3, 2, c, m.Yn, true);
             if (i == g.IS) put_flux(a, N3, 1, c - sI, m.Xw, false);
             if (j == g.JS) put_flux(a, N3, 2, c - sJ, m.Ys, false);
-            const double mZ = (L <= KE - 1) ? ld(nd.DZ() + c) : 0.0; // hevi_mflx_z :383-391 (flat terrain)
-            const double mZm1 = (L - 1 >= KS) ? ld(nd.DZ() + c - 1) : 0.0;
-            const double rcdz = ld(g.RCDZ + L - 1);
+            const R mZ = (L <= KE - 1) ? ld(nd.DZ() + c) : R(0.0); // hevi_mflx_z :383-391 (flat terrain)
+            const R mZm1 = (L - 1 >= KS) ? ld(nd.DZ() + c - 1) : R(0.0);
+            const R rcdz = R(ld(g.RCDZ + L - 1));
             XS_PUT(CA_SR, L, (-(mZ - mZm1) * rcdz + adv_r) + lds(a.DENS_t + c));
-            SA(CA_A, w, L) = dt2 * J33G * rcdz * ld(a.RT2P + c) * J33G;
+            SA(CA_A, w, L) = dt2 * J33G * ld(g.RCDZ + L - 1) * ld(a.RT2P + c) * J33G;
         }
     }
     __syncthreads();
 
     // ---- phase 2: PT, tZ (valueW_Z ud3.F90:98-153, fluxZ_XYZ :157-247), x/y theta fluxes, St ----
     if (col_ok) {
-        auto pt_tz = [&](int L, double &pt, double &tz) {
-            if (L < KS || L > KE - 1) { pt = 0.0; tz = 0.0; return; }
-            const double mZ = CL(nd.DZ(), L);
-            const double M0 = CL(a.MOMZ, L);
-            double pi, ti;
+        auto pt_tz = [&](int L, R &pt, R &tz) {
+            if (L < KS || L > KE - 1) { pt = R(0.0); tz = R(0.0); return; }
+            const R mZ = CL(nd.DZ(), L);
+            const R M0 = R(CL(a.MOMZ, L));
+            R pi, ti;
             if (L == KS) {
-                const double P0 = SA(CA_C, w, L), P1 = SA(CA_C, w, L + 1), P2 = SA(CA_C, w, L + 2);
+                const R P0 = R(SA(CA_C, w, L)), P1 = R(SA(CA_C, w, L + 1)), P2 = R(SA(CA_C, w, L + 2));
                 pi = ipL<S>(M0, P0, P1, P2);
                 ti = ipL<S>(mZ, P0, P1, P2);
             } else if (L == KE - 1) {
-                const double Pm1 = SA(CA_C, w, L - 1), P0 = SA(CA_C, w, L), P1 = SA(CA_C, w, L + 1);
+                const R Pm1 = R(SA(CA_C, w, L - 1)), P0 = R(SA(CA_C, w, L)), P1 = R(SA(CA_C, w, L + 1));
                 pi = ipH<S>(M0, P1, P0, Pm1);
                 ti = ipH<S>(mZ, P1, P0, Pm1);
             } else {
-                const double Pm1 = SA(CA_C, w, L - 1), P0 = SA(CA_C, w, L), P1 = SA(CA_C, w, L + 1), P2 = SA(CA_C, w, L + 2);
+                const R Pm1 = R(SA(CA_C, w, L - 1)), P0 = R(SA(CA_C, w, L)), P1 = R(SA(CA_C, w, L + 1)), P2 = R(SA(CA_C, w, L + 2));
                 pi = ip4<S>(M0, Pm1, P0, P1, P2);
                 ti = ip4<S>(mZ, Pm1, P0, P1, P2);
             }
@@ -382,35 +394,35 @@ __global__ void __launch_bounds__(32 * HEVI_COL_TC, HEVI_COL_MINB) k_hevi_stage(
         };
         for (int L = KS + lane; L <= KE; L += 32) {
             const int c = col + L - 1;
-            double PT, tZ, PTm, tZm;
+            R PT, tZ, PTm, tZm;
             pt_tz(L, PT, tZ);
             pt_tz(L - 1, PTm, tZm);
             (void)PTm;
             // POTT at x-neighbours (from the tile when it holds them) and y-neighbours
-            auto pott_x = [&](int d) -> double {
+            auto pott_x = [&](int d) -> R {
                 const int td = tx + d;
-                if (td >= 0 && td < TX && i + d <= g.IE) return SA(CA_C, w + d, L);
-                return AT(a.RHOT, 0, d, 0) / AT(a.DENS, 0, d, 0);
+                if (td >= 0 && td < TX && i + d <= g.IE) return R(SA(CA_C, w + d, L));
+                return AR(a.RHOT, 0, d, 0) / AR(a.DENS, 0, d, 0);
             };
-            auto pott_y = [&](int d) -> double {
+            auto pott_y = [&](int d) -> R {
                 const int td = ty + d;
-                if (td >= 0 && td < TY && j + d <= g.JE) return SA(CA_C, w + d * TX, L);
-                return AT(a.RHOT, 0, 0, d) / AT(a.DENS, 0, 0, d);
+                if (td >= 0 && td < TY && j + d <= g.JE) return R(SA(CA_C, w + d * TX, L));
+                return AR(a.RHOT, 0, 0, d) / AR(a.DENS, 0, 0, d);
             };
-            const double Pm2 = pott_x(-2), Pm1 = pott_x(-1), P00 = SA(CA_C, w, L), Pp1 = pott_x(1), Pp2 = pott_x(2);
-            const double Qm2 = pott_y(-2), Qm1 = pott_y(-1), Qp1 = pott_y(1), Qp2 = pott_y(2);
-            const MassFlux m = mass_flux(a, nd, c, sI, sJ);
+            const R Pm2 = pott_x(-2), Pm1 = pott_x(-1), P00 = R(SA(CA_C, w, L)), Pp1 = pott_x(1), Pp2 = pott_x(2);
+            const R Qm2 = pott_y(-2), Qm1 = pott_y(-1), Qp1 = pott_y(1), Qp2 = pott_y(2);
+            const MassFlux<R> m = mass_flux(a, nd, c, sI, sJ);
             // fluxX/Y_XYZ (ud3.F90:251-353)
-            const double tXe = m.Xe * ip4<S>(m.Xe, Pm1, P00, Pp1, Pp2) + AT(nd.TX(), 0, 0, 0);
-            const double tXw = m.Xw * ip4<S>(m.Xw, Pm2, Pm1, P00, Pp1) + AT(nd.TX(), 0, -1, 0);
-            const double tYn = m.Yn * ip4<S>(m.Yn, Qm1, P00, Qp1, Qp2) + AT(nd.TY(), 0, 0, 0);
-            const double tYs = m.Ys * ip4<S>(m.Ys, Qm2, Qm1, P00, Qp1) + AT(nd.TY(), 0, 0, -1);
-            const double adv_t = -((tXe - tXw) * rcdx + (tYn - tYs) * rcdy); // hevi_st :646-648
+            const R tXe = m.Xe * ip4<S>(m.Xe, Pm1, P00, Pp1, Pp2) + AT(nd.TX(), 0, 0, 0);
+            const R tXw = m.Xw * ip4<S>(m.Xw, Pm2, Pm1, P00, Pp1) + AT(nd.TX(), 0, -1, 0);
+            const R tYn = m.Yn * ip4<S>(m.Yn, Qm1, P00, Qp1, Qp2) + AT(nd.TY(), 0, 0, 0);
+            const R tYs = m.Ys * ip4<S>(m.Ys, Qm2, Qm1, P00, Qp1) + AT(nd.TY(), 0, 0, -1);
+            const R adv_t = -((tXe - tXw) * rcdx + (tYn - tYs) * rcdy); // hevi_st :646-648
             put_flux(a, N3, 4, c, tXe, true);
             put_flux(a, N3, 5, c, tYn, true);
             if (i == g.IS) put_flux(a, N3, 4, c - sI, tXw, false);
             if (j == g.JS) put_flux(a, N3, 5, c - sJ, tYs, false);
-            const double rcdz = ld(g.RCDZ + L - 1);
+            const R rcdz = R(ld(g.RCDZ + L - 1));
             SA(CA_PT, w, L) = PT;
             XS_PUT(CA_TZ, L, tZ);
             XS_PUT(CA_ST, L, (-(tZ - tZm) * rcdz + adv_t) + lds(a.RHOT_t + c)); // hevi_st :646-649
@@ -420,36 +432,37 @@ __global__ void __launch_bounds__(32 * HEVI_COL_TC, HEVI_COL_MINB) k_hevi_stage(
 
     // ---- phase 3: Sw (hevi_sw :528-578) and the right-hand side C(k), k = KS..KE-1 (:698-722) ----
     if (col_ok) {
+        const R J33R = R(J33G);
         // vertical w-momentum flux above level k, fluxZ_XYW (ud3.F90:358-452), zero outside KS..KE-2
-        auto qZ_at = [&](int k) -> double {
-            if (k < KS || k > KE - 2) return 0.0;
-            const double Mk = CL(a.MOMZ, k), Mk1 = CL(a.MOMZ, k + 1);
-            const double vel = (0.5 * (Mk + Mk1)) / CL(a.DENS, k + 1);
-            const double q = (k == KS) ? ipL<S>(vel, Mk, Mk1, CL(a.MOMZ, k + 2))
-                                       : ip4<S>(vel, CL(a.MOMZ, k - 1), Mk, Mk1, CL(a.MOMZ, k + 2));
-            return J33G * vel * q + lds(nd.WZ() + col + k);
+        auto qZ_at = [&](int k) -> R {
+            if (k < KS || k > KE - 2) return R(0.0);
+            const R Mk = R(CL(a.MOMZ, k)), Mk1 = R(CL(a.MOMZ, k + 1));
+            const R vel = (R(0.5) * (Mk + Mk1)) / R(CL(a.DENS, k + 1));
+            const R q = (k == KS) ? ipL<S>(vel, Mk, Mk1, R(CL(a.MOMZ, k + 2)))
+                                  : ip4<S>(vel, R(CL(a.MOMZ, k - 1)), Mk, Mk1, R(CL(a.MOMZ, k + 2)));
+            return J33R * vel * q + lds(nd.WZ() + col + k);
         };
         auto dpres = [&](int L) { return CL(a.DPRES0, L) + CL(a.RT2P, L) * (CL(a.RHOT, L) - CL(a.REF_rhot, L)); }; // :355
         for (int k0 = KS; k0 <= KE - 1; k0 += 32) {
             const int k = k0 + lane;
             const bool ok = k <= KE - 1;
             // the flux above level k; the one below is the previous lane's (lane 0 computes it)
-            const double q_k = ok ? qZ_at(k) : 0.0;
-            double q_km = __shfl_up_sync(0xffffffffu, q_k, 1);
+            const R q_k = ok ? qZ_at(k) : R(0.0);
+            R q_km = __shfl_up_sync(0xffffffffu, q_k, 1);
             if (!ok) continue;
             if (lane == 0) q_km = qZ_at(k - 1);
             const int c = col + k - 1;
-            const double adv_w = adv_w_h<S>(g, a, nd, c, k, sI, sJ, rcdx, rcdy);
-            const double advcv = -(q_k - q_km) * ld(g.RFDZ + k - 1);
-            const double wdmp = -ld(a.wdamp + k - 1) * CL(a.MOMZ0, k);
-            const double div = use_div ? ddc * (CL(a.DDIV, k + 1) - CL(a.DDIV, k)) * ld(g.FDZ + k - 1) : 0.0;
-            const double Sw = (advcv + adv_w) + wdmp + div + lds(a.MOMZ_t + c);
+            const R adv_w = adv_w_h<S>(g, a, nd, c, k, sI, sJ, rcdx, rcdy);
+            const R advcv = -(q_k - q_km) * R(ld(g.RFDZ + k - 1));
+            const R wdmp = -R(ld(a.wdamp + k - 1)) * R(CL(a.MOMZ0, k));
+            const R div = use_div ? ddc * (CL(a.DDIV, k + 1) - CL(a.DDIV, k)) * R(ld(g.FDZ + k - 1)) : R(0.0);
+            const R Sw = (advcv + adv_w) + wdmp + div + lds(a.MOMZ_t + c);
             const double rfdz = ld(g.RFDZ + k - 1);
             const double RTL1 = CL(a.RT2P, k + 1), RTL0 = CL(a.RT2P, k);
-            const double pg = -(dpres(k + 1) + RTL1 * dt * XS(CA_ST, k + 1) - dpres(k) - RTL0 * dt * XS(CA_ST, k)) * rfdz * J33G
-                              - GRAV * (ld(g.F2H1 + k - 1) * (CL(a.DENS, k + 1) - lds(a.REF_dens + c + 1) + XS(CA_SR, k + 1) * dt)
-                                        + ld(g.F2H2 + k - 1) * (CL(a.DENS, k) - lds(a.REF_dens + c) + XS(CA_SR, k) * dt));
-            SA(CA_C, w, k) = CL(a.MOMZ, k) + dt * (pg + Sw);
+            const double pg = -(dpres(k + 1) + RTL1 * dt * (double)XS(CA_ST, k + 1) - dpres(k) - RTL0 * dt * (double)XS(CA_ST, k)) * rfdz * J33G
+                              - GRAV * (ld(g.F2H1 + k - 1) * (CL(a.DENS, k + 1) - lds(a.REF_dens + c + 1) + (double)XS(CA_SR, k + 1) * dt)
+                                        + ld(g.F2H2 + k - 1) * (CL(a.DENS, k) - lds(a.REF_dens + c) + (double)XS(CA_SR, k) * dt));
+            SA(CA_C, w, k) = CL(a.MOMZ, k) + dt * (pg + (double)Sw);
         }
     }
     __syncthreads();
@@ -526,23 +539,23 @@ __global__ void __launch_bounds__(32 * HEVI_COL_TC, HEVI_COL_MINB) k_hevi_stage(
                 adr = -(Cm - Cm1) * J33G * rcdz;
                 adt = -(Cm * SA(CA_PT, w, m) - Cm1 * SA(CA_PT, w, m - 1)) * J33G * rcdz;
             }
-            put_state(a, N3, 0, a.DENS_RK, a.DENS0, c, lds(a.DENS0 + c) + dt * (adr + XS(CA_SR, m)), true);
-            put_state(a, N3, 4, a.RHOT_RK, a.RHOT0, c, lds(a.RHOT0 + c) + dt * (adt + XS(CA_ST, m)), true);
+            put_state(a, N3, 0, a.DENS_RK, a.DENS0, c, lds(a.DENS0 + c) + dt * (adr + (double)XS(CA_SR, m)), true);
+            put_state(a, N3, 4, a.RHOT_RK, a.RHOT0, c, lds(a.RHOT0 + c) + dt * (adt + (double)XS(CA_ST, m)), true);
             if (m <= KE - 1) {
                 put_state(a, N3, 1, a.MOMZ_RK, a.MOMZ0, c, ld(a.MOMZ0 + c) + (Cm - ld(a.MOMZ + c)), true);
-                put_flux(a, N3, 0, c, ld(nd.DZ() + c) + J33G * Cm, true);
-                put_flux(a, N3, 3, c, XS(CA_TZ, m) + J33G * Cm * SA(CA_PT, w, m), true);
+                put_flux(a, N3, 0, c, R((double)ld(nd.DZ() + c) + J33G * Cm), true);
+                put_flux(a, N3, 3, c, R((double)XS(CA_TZ, m) + J33G * Cm * SA(CA_PT, w, m)), true);
             } else {
                 put_state(a, N3, 1, a.MOMZ_RK, a.MOMZ0, c, 0.0, false);
-                put_flux(a, N3, 0, c, 0.0, true);
-                put_flux(a, N3, 3, c, 0.0, true);
+                put_flux(a, N3, 0, c, R(0.0), true);
+                put_flux(a, N3, 3, c, R(0.0), true);
             }
         }
         if (lane == 0) {
             // rigid-lid and surface values (:753-754) and the zero fluxes at KS-1 (:371, ud3.F90:222)
             put_state(a, N3, 1, a.MOMZ_RK, a.MOMZ0, col + KS - 2, 0.0, false);
-            put_flux(a, N3, 0, col + KS - 2, 0.0, false);
-            put_flux(a, N3, 3, col + KS - 2, 0.0, false);
+            put_flux(a, N3, 0, col + KS - 2, R(0.0), false);
+            put_flux(a, N3, 3, col + KS - 2, R(0.0), false);
         }
     }
     // hevi_mflx_z :369-393 also fills the halo column i = IS-1 with the explicit
@@ -550,7 +563,7 @@ __global__ void __launch_bounds__(32 * HEVI_COL_TC, HEVI_COL_MINB) k_hevi_stage(
     if (ti == 0 && tx == 0 && col_ok && (a.rk_mode == RK_PLAIN || a.rk_mode == RK_FINAL)) {
         const size_t ch = idx3(g, 1, g.IS - 1, j);
         for (int k = KS - 1 + lane; k <= KE; k += 32)
-            a.mflx[ch + k - 1] = (k >= KS && k <= KE - 1) ? ld(nd.DZ() + ch + k - 1) : 0.0;
+            a.mflx[ch + k - 1] = (k >= KS && k <= KE - 1) ? ld(nd.DZ() + ch + k - 1) : R(0.0);
     }
 #undef SA
 #undef CL
@@ -558,21 +571,25 @@ __global__ void __launch_bounds__(32 * HEVI_COL_TC, HEVI_COL_MINB) k_hevi_stage(
 #undef XS_PUT
 }
 #undef AT
+#undef AR
 
 // ---- host launcher ----------------------------------------------------------
-cudaError_t launch_hevi_stage(const Grid &g, const StageArgs &a, int scheme, cudaStream_t st)
+template <typename R>
+cudaError_t launch_hevi_stage(const Grid &g, const StageArgsT<R> &a, int scheme, cudaStream_t st)
 {
     if (g.KA > MAXKA) return cudaErrorInvalidValue;
     const size_t smem = (size_t)COL_ARRAYS * HEVI_COL_TC * col_pitch(g.KA) * sizeof(double);
     cudaError_t e = scheme == UD3
-        ? cudaFuncSetAttribute(k_hevi_stage<UD3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)
-        : cudaFuncSetAttribute(k_hevi_stage<CD4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        ? cudaFuncSetAttribute(k_hevi_stage<UD3, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)
+        : cudaFuncSetAttribute(k_hevi_stage<CD4, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     dim3 bc(32, HEVI_COL_TC);
     dim3 gc((g.IMAX + HEVI_TILE_X - 1) / HEVI_TILE_X, (g.JMAX + HEVI_TILE_Y - 1) / HEVI_TILE_Y);
-    if (scheme == UD3) k_hevi_stage<UD3><<<gc, bc, smem, st>>>(g, a);
-    else k_hevi_stage<CD4><<<gc, bc, smem, st>>>(g, a);
+    if (scheme == UD3) k_hevi_stage<UD3, R><<<gc, bc, smem, st>>>(g, a);
+    else k_hevi_stage<CD4, R><<<gc, bc, smem, st>>>(g, a);
     return cudaGetLastError();
 }
+template cudaError_t launch_hevi_stage<double>(const Grid &, const StageArgsT<double> &, int, cudaStream_t);
+template cudaError_t launch_hevi_stage<float>(const Grid &, const StageArgsT<float> &, int, cudaStream_t);
 
 }  // namespace hevi

@@ -25,27 +25,33 @@ enum RkMode : int {
 #define HEVI_COL_SCRATCH 1
 #endif
 
-struct StageArgs {
+// F is the storage and arithmetic type of the flux-like arrays (num_diff, the
+// tendencies, DDIV, the fluxes and their RK sums, the column-solve sources):
+// double on the plain path, float on the mixed-precision path. The state, the
+// base state and the pressure deviation are always double.
+template <typename F>
+struct StageArgsT {
     // outputs (RK_FINAL: the state arrays themselves, updated in place)
     double *DENS_RK, *MOMZ_RK, *MOMX_RK, *MOMY_RK, *RHOT_RK;
-    double *mflx; // mflx_hi(KA,IA,JA,3): Z, X, Y
-    double *tflx; // tflx_hi(KA,IA,JA,3)
+    F *mflx; // mflx_hi(KA,IA,JA,3): Z, X, Y
+    F *tflx; // tflx_hi(KA,IA,JA,3)
     // inputs
     const double *DENS0, *MOMZ0, *MOMX0, *MOMY0, *RHOT0;
     const double *DENS, *MOMZ, *MOMX, *MOMY, *RHOT;
-    const double *DENS_t, *MOMZ_t, *MOMX_t, *MOMY_t, *RHOT_t;
+    const F *DENS_t, *MOMZ_t, *MOMX_t, *MOMY_t, *RHOT_t;
     const double *DPRES0, *RT2P, *CORIOLI;
-    const double *num_diff; // (KA,IA,JA,5,3)
-    const double *wdamp;    // (KA)
-    const double *DDIV;
+    const F *num_diff;   // (KA,IA,JA,5,3)
+    const double *wdamp; // (KA)
+    const F *DDIV;
     const double *REF_dens, *REF_rhot;
     double divdmp_coef, J33G, dtrk;
     // RK accumulation
     int rk_mode;
-    double *acc;  // 5*N3: DENS, MOMZ, MOMX, MOMY, RHOT
-    double *facc; // 6*N3: mflx Z,X,Y then tflx Z,X,Y
+    double *acc; // 5*N3: DENS, MOMZ, MOMX, MOMY, RHOT
+    F *facc;     // 6*N3: mflx Z,X,Y then tflx Z,X,Y
     unsigned *status;
-    double *colscr; // 3*N3 (HEVI_COL_SCRATCH): Sr, St, tZ
+    F *colscr; // 3*N3 (HEVI_COL_SCRATCH): Sr, St, tZ
 };
+using StageArgs = StageArgsT<double>;
 
 }  // namespace hevi

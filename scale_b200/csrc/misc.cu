@@ -7,11 +7,13 @@ namespace hevi {
 // ---- periodic halo fill: COMM_vars8 + COMM_wait on a single periodic rank ----
 // (scalelib/src/communication/scale_comm_cartesC.F90:345-397, 1600-2043). Every
 // halo column takes all KA levels of its periodic image; corners included.
+template <typename T>
 struct FieldList {
-    double *f[16];
+    T *f[16];
 };
 
-__global__ void k_halo(const Grid g, const FieldList fl)
+template <typename T>
+__global__ void k_halo(const Grid g, const FieldList<T> fl)
 {
     const int nA = 2 * g.JHALO * g.IA;      // halo rows j < JS and j > JE, all i
     const int nB = 2 * g.IHALO * g.JMAX;    // halo columns i < IS and i > IE, interior j
@@ -30,22 +32,25 @@ __global__ void k_halo(const Grid g, const FieldList fl)
     }
     const int si = i < g.IS ? i + g.IMAX : (i > g.IE ? i - g.IMAX : i);
     const int sj = j < g.JS ? j + g.JMAX : (j > g.JE ? j - g.JMAX : j);
-    double *v = fl.f[blockIdx.y];
+    T *v = fl.f[blockIdx.y];
     const size_t dst = idx3(g, 1, i, j), src = idx3(g, 1, si, sj);
     for (int k = threadIdx.x; k < g.KA; k += 32) v[dst + k] = v[src + k];
 }
 
-void periodic_halo(const Grid &g, double *const *fields, int nf, cudaStream_t st)
+template <typename T>
+void periodic_halo(const Grid &g, T *const *fields, int nf, cudaStream_t st)
 {
     const int nh = 2 * g.JHALO * g.IA + 2 * g.IHALO * g.JMAX;
     for (int base = 0; base < nf; base += 16) {
-        FieldList fl;
+        FieldList<T> fl;
         const int n = (nf - base) < 16 ? (nf - base) : 16;
         for (int q = 0; q < n; ++q) fl.f[q] = fields[base + q];
         dim3 b(32, 4), gr((nh + 3) / 4, n);
-        k_halo<<<gr, b, 0, st>>>(g, fl);
+        k_halo<T><<<gr, b, 0, st>>>(g, fl);
     }
 }
+template void periodic_halo<double>(const Grid &, double *const *, int, cudaStream_t);
+template void periodic_halo<float>(const Grid &, float *const *, int, cudaStream_t);
 
 // ---- vertical boundary values after a short step (scale_atmos_dyn_tstep_large_fvm_heve.F90:910-926) ----
 __global__ void k_vbc(const Grid g, double *DENS, double *MOMZ, double *MOMX, double *MOMY, double *RHOT)

@@ -10,20 +10,25 @@
 // including the zero and mirrored values of the vertical halo, reading the
 // quantities from the scratch. The lateral halo is filled afterwards by the
 // periodic halo kernel, as COMM_vars8 does in the reference.
+//
+// R is the output and arithmetic type: double on the plain path, float on the
+// mixed-precision path (the deviations from the base state and the quotients
+// of k_phi are formed in FP64 and then stored as R).
 #include "hevi_kernels.cuh"
 
 namespace hevi {
 
-#define CZ3(n, k, s) ld(c.CNZ3 + ((n) - 1) + 3 * ((size_t)((k) - 1) + (size_t)g.KA * ((s) - 1)))
-#define CX3(n, i, s) ld(c.CNX3 + ((n) - 1) + 3 * ((size_t)((i) - 1) + (size_t)g.IA * ((s) - 1)))
-#define CY3(n, j, s) ld(c.CNY3 + ((n) - 1) + 3 * ((size_t)((j) - 1) + (size_t)g.JA * ((s) - 1)))
+#define CZ3(n, k, s) (R)ld(c.CNZ3 + ((n) - 1) + 3 * ((size_t)((k) - 1) + (size_t)g.KA * ((s) - 1)))
+#define CX3(n, i, s) (R)ld(c.CNX3 + ((n) - 1) + 3 * ((size_t)((i) - 1) + (size_t)g.IA * ((s) - 1)))
+#define CY3(n, j, s) (R)ld(c.CNY3 + ((n) - 1) + 3 * ((size_t)((j) - 1) + (size_t)g.JA * ((s) - 1)))
 
 // The five filtered quantities at one point.
 // q: 0 DENS-REF_dens, 1 VELZ, 2 VELX, 3 VELY, 4 RHOT/DENS-REF_pott  (:538-547, 621-626, 715-720, 799-804, 876-883)
 // A velocity needs the density one point above (VELZ), east (VELX) or north
 // (VELY); at the last point of the array in that direction, which no stencil
 // reads, it is stored as zero.
-__global__ void __launch_bounds__(128) k_phi(const Grid g, const NdArgs a)
+template <typename R>
+__global__ void __launch_bounds__(128) k_phi(const Grid g, const NdArgsT<R> a)
 {
     const int i = 1 + blockIdx.x * blockDim.y + threadIdx.y;
     const int j = 1 + blockIdx.y;
@@ -33,26 +38,28 @@ __global__ void __launch_bounds__(128) k_phi(const Grid g, const NdArgs a)
     for (int k = 1 + threadIdx.x; k <= g.KA; k += 32) {
         const size_t c = idx3(g, k, i, j);
         const double D = ld(a.DENS + c);
-        a.phi[c] = D - ld(a.REF_dens + c);
-        a.phi[c + N3] = k < g.KA ? 2.0 * ld(a.MOMZ + c) / (ld(a.DENS + c + 1) + D) : 0.0;
-        a.phi[c + 2 * N3] = i < g.IA ? 2.0 * ld(a.MOMX + c) / (ld(a.DENS + c + sI) + D) : 0.0;
-        a.phi[c + 3 * N3] = j < g.JA ? 2.0 * ld(a.MOMY + c) / (ld(a.DENS + c + sJ) + D) : 0.0;
-        a.phi[c + 4 * N3] = ld(a.RHOT + c) / D - ld(a.REF_pott + c);
+        a.phi[c] = R(D - ld(a.REF_dens + c));
+        a.phi[c + N3] = R(k < g.KA ? 2.0 * ld(a.MOMZ + c) / (ld(a.DENS + c + 1) + D) : 0.0);
+        a.phi[c + 2 * N3] = R(i < g.IA ? 2.0 * ld(a.MOMX + c) / (ld(a.DENS + c + sI) + D) : 0.0);
+        a.phi[c + 3 * N3] = R(j < g.JA ? 2.0 * ld(a.MOMY + c) / (ld(a.DENS + c + sJ) + D) : 0.0);
+        a.phi[c + 4 * N3] = R(ld(a.RHOT + c) / D - ld(a.REF_pott + c));
     }
 }
 
 // the quantities read back by the stencils
+template <typename R>
 struct Phi {
     const Grid &g;
-    const NdArgs &a;
-    __device__ double operator()(int q, int k, int i, int j) const
+    const NdArgsT<R> &a;
+    __device__ R operator()(int q, int k, int i, int j) const
     {
         return __ldg(a.phi + (size_t)q * n3(g) + idx3(g, k, i, j));
     }
 };
 
 // calc_diff3 z-component with KO = 0 (:1617-1655) at level k (any k in 1..KA)
-__device__ double dz0(const Grid &g, const NdCoef &c, const Phi &phi, int q, int k, int i, int j)
+template <typename R>
+__device__ R dz0(const Grid &g, const NdCoef &c, const Phi<R> &phi, int q, int k, int i, int j)
 {
     const int KS = g.KS, KE = g.KE;
     auto inner = [&](int m) {
@@ -74,11 +81,12 @@ __device__ double dz0(const Grid &g, const NdCoef &c, const Phi &phi, int q, int
     if (k == KE - 1) return atKEm1();
     if (k == KE) return -atKEm1();
     if (k == KE + 1) return -inner(KE - 2);
-    return 0.0; // KE+2
+    return R(0.0); // KE+2
 }
 
 // calc_diff3 z-component with KO = 1 (:1657-1705)
-__device__ double dz1(const Grid &g, const NdCoef &c, const Phi &phi, int q, int k, int i, int j)
+template <typename R>
+__device__ R dz1(const Grid &g, const NdCoef &c, const Phi<R> &phi, int q, int k, int i, int j)
 {
     const int KS = g.KS, KE = g.KE;
     auto inner = [&](int m) {
@@ -109,7 +117,8 @@ __device__ double dz1(const Grid &g, const NdCoef &c, const Phi &phi, int q, int
 }
 
 // x and y components (:1707-1760); o selects IO/JO
-__device__ __forceinline__ double dx(const Grid &g, const NdCoef &c, const Phi &phi, int q, int o, int k, int i, int j)
+template <typename R>
+__device__ __forceinline__ R dx(const Grid &g, const NdCoef &c, const Phi<R> &phi, int q, int o, int k, int i, int j)
 {
     if (o == 0)
         return (+CX3(1, i + 1, 1) * phi(q, k, i + 2, j) - CX3(2, i + 1, 1) * phi(q, k, i + 1, j)
@@ -117,7 +126,8 @@ __device__ __forceinline__ double dx(const Grid &g, const NdCoef &c, const Phi &
     return (+CX3(1, i, 2) * phi(q, k, i + 1, j) - CX3(2, i, 2) * phi(q, k, i, j)
             + CX3(3, i, 2) * phi(q, k, i - 1, j) - CX3(1, i - 1, 2) * phi(q, k, i - 2, j));
 }
-__device__ __forceinline__ double dy(const Grid &g, const NdCoef &c, const Phi &phi, int q, int o, int k, int i, int j)
+template <typename R>
+__device__ __forceinline__ R dy(const Grid &g, const NdCoef &c, const Phi<R> &phi, int q, int o, int k, int i, int j)
 {
     if (o == 0)
         return (+CY3(1, j + 1, 1) * phi(q, k, i, j + 2) - CY3(2, j + 1, 1) * phi(q, k, i, j + 1)
@@ -130,82 +140,86 @@ __device__ __forceinline__ double dy(const Grid &g, const NdCoef &c, const Phi &
 #define HEVI_ND_MINB 8 // minimum resident blocks per SM asked of the register allocator
 #endif
 
-__global__ void __launch_bounds__(128, HEVI_ND_MINB) k_numfilter(const Grid g, const NdCoef c, const NdArgs a)
+template <typename R>
+__global__ void __launch_bounds__(128, HEVI_ND_MINB) k_numfilter(const Grid g, const NdCoef c, const NdArgsT<R> a)
 {
     const int i = g.IS + blockIdx.x * blockDim.y + threadIdx.y;
     const int j = g.JS + blockIdx.y;
     if (i > g.IE) return;
     const size_t N3 = n3(g);
     const int KS = g.KS, KE = g.KE;
-    const Phi phi{g, a};
+    const Phi<R> phi{g, a};
     const double *DN = a.DENS;
     const long sI = g.KA, sJ = (long)g.KA * g.IA;
-    const double ncx = ld(c.cdx + i - 1), nfx = ld(c.fdx + i - 1), ncy = ld(c.cdy + j - 1), nfy = ld(c.fdy + j - 1);
-    const double sfc = c.sfc;
+    const R ncx = R(ld(c.cdx + i - 1)), nfx = R(ld(c.fdx + i - 1)), ncy = R(ld(c.cdy + j - 1)), nfy = R(ld(c.fdy + j - 1));
+    const R sfc = R(c.sfc);
     // surface-factor tail of every x/y component (:581-585 and the analogous blocks)
-    auto sfct = [&](int k, double v) {
+    auto sfct = [&](int k, R v) {
         if (k == KS) return v * sfc;
-        if (k == KS + 1) return v * (1.0 + sfc) * 0.5;
+        if (k == KS + 1) return v * (R(1.0) + sfc) * R(0.5);
         return v;
     };
     for (int k = 1 + threadIdx.x; k <= g.KA; k += 32) {
         const size_t o = idx3(g, k, i, j);
-        const double ncz = (k >= KS - 1 && k <= KE) ? ld(c.cdz + k - 1) : 0.0;
-        double *ND = a.num_diff;
+        const R ncz = (k >= KS - 1 && k <= KE) ? R(ld(c.cdz + k - 1)) : R(0.0);
+        R *ND = a.num_diff;
         const bool kin = (k >= KS && k <= KE);
         // ---- density (:553-610) ----
-        ND[o + N3 * 0] = (k >= KS - 1 && k <= KE) ? dz0(g, c, phi, 0, k, i, j) * ncz : 0.0;
-        ND[o + N3 * 5] = kin ? sfct(k, dx(g, c, phi, 0, 0, k, i, j) * ncx) : 0.0;
-        ND[o + N3 * 10] = kin ? sfct(k, dy(g, c, phi, 0, 0, k, i, j) * ncy) : 0.0;
+        ND[o + N3 * 0] = (k >= KS - 1 && k <= KE) ? dz0(g, c, phi, 0, k, i, j) * ncz : R(0.0);
+        ND[o + N3 * 5] = kin ? sfct(k, dx(g, c, phi, 0, 0, k, i, j) * ncx) : R(0.0);
+        ND[o + N3 * 10] = kin ? sfct(k, dy(g, c, phi, 0, 0, k, i, j) * ncy) : R(0.0);
         // ---- z momentum (:628-698), phi = VELZ on KS..KE-1 ----
         {
             const bool kz = (k >= KS && k <= KE - 1);
-            const double nfz = (k >= KS + 1 && k <= KE - 1) ? ld(c.fdz + k - 1) : 0.0;
-            ND[o + N3 * 1] = (k >= KS + 1 && k <= KE - 1) ? dz1(g, c, phi, 1, k, i, j) * nfz * ld(DN + o) : 0.0;
+            const R nfz = (k >= KS + 1 && k <= KE - 1) ? R(ld(c.fdz + k - 1)) : R(0.0);
+            ND[o + N3 * 1] = (k >= KS + 1 && k <= KE - 1) ? dz1(g, c, phi, 1, k, i, j) * nfz * R(ld(DN + o)) : R(0.0);
             ND[o + N3 * 6] = kz ? sfct(k, dx(g, c, phi, 1, 0, k, i, j) * ncx
-                                              * 0.25 * (ld(DN + o + 1 + sI) + ld(DN + o + 1) + ld(DN + o + sI) + ld(DN + o)))
-                                : 0.0;
+                                              * R(0.25) * (R(ld(DN + o + 1 + sI)) + R(ld(DN + o + 1)) + R(ld(DN + o + sI)) + R(ld(DN + o))))
+                                : R(0.0);
             ND[o + N3 * 11] = kz ? sfct(k, dy(g, c, phi, 1, 0, k, i, j) * ncy
-                                               * 0.25 * (ld(DN + o + 1 + sJ) + ld(DN + o + 1) + ld(DN + o + sJ) + ld(DN + o)))
-                                 : 0.0;
+                                               * R(0.25) * (R(ld(DN + o + 1 + sJ)) + R(ld(DN + o + 1)) + R(ld(DN + o + sJ)) + R(ld(DN + o))))
+                                 : R(0.0);
         }
         // ---- x momentum (:728-790), phi = VELX ----
         ND[o + N3 * 2] = (k >= KS && k <= KE - 1)
                              ? dz0(g, c, phi, 2, k, i, j) * ncz
-                                   * 0.25 * (ld(DN + o + 1 + sI) + ld(DN + o + 1) + ld(DN + o + sI) + ld(DN + o))
-                             : 0.0;
-        ND[o + N3 * 7] = kin ? sfct(k, dx(g, c, phi, 2, 1, k, i, j) * nfx * ld(DN + o)) : 0.0;
+                                   * R(0.25) * (R(ld(DN + o + 1 + sI)) + R(ld(DN + o + 1)) + R(ld(DN + o + sI)) + R(ld(DN + o)))
+                             : R(0.0);
+        ND[o + N3 * 7] = kin ? sfct(k, dx(g, c, phi, 2, 1, k, i, j) * nfx * R(ld(DN + o))) : R(0.0);
         ND[o + N3 * 12] = kin ? sfct(k, dy(g, c, phi, 2, 0, k, i, j) * ncy
-                                            * 0.25 * (ld(DN + o + sI + sJ) + ld(DN + o + sI) + ld(DN + o + sJ) + ld(DN + o)))
-                              : 0.0;
+                                            * R(0.25) * (R(ld(DN + o + sI + sJ)) + R(ld(DN + o + sI)) + R(ld(DN + o + sJ)) + R(ld(DN + o))))
+                              : R(0.0);
         // ---- y momentum (:812-870), phi = VELY ----
         ND[o + N3 * 3] = (k >= KS && k <= KE - 1)
                              ? dz0(g, c, phi, 3, k, i, j) * ncz
-                                   * 0.25 * (ld(DN + o + 1 + sJ) + ld(DN + o + 1) + ld(DN + o + sJ) + ld(DN + o))
-                             : 0.0;
+                                   * R(0.25) * (R(ld(DN + o + 1 + sJ)) + R(ld(DN + o + 1)) + R(ld(DN + o + sJ)) + R(ld(DN + o)))
+                             : R(0.0);
         ND[o + N3 * 8] = kin ? sfct(k, dx(g, c, phi, 3, 0, k, i, j) * ncx
-                                           * 0.25 * (ld(DN + o + sI + sJ) + ld(DN + o + sJ) + ld(DN + o + sI) + ld(DN + o)))
-                             : 0.0;
-        ND[o + N3 * 13] = kin ? sfct(k, dy(g, c, phi, 3, 1, k, i, j) * nfy * ld(DN + o)) : 0.0;
+                                           * R(0.25) * (R(ld(DN + o + sI + sJ)) + R(ld(DN + o + sJ)) + R(ld(DN + o + sI)) + R(ld(DN + o))))
+                             : R(0.0);
+        ND[o + N3 * 13] = kin ? sfct(k, dy(g, c, phi, 3, 1, k, i, j) * nfy * R(ld(DN + o))) : R(0.0);
         // ---- rho*theta (:885-960) ----
         {
-            double v = 0.0;
-            if (k >= KS && k <= KE - 1) v = dz0(g, c, phi, 4, k, i, j) * ncz * 0.5 * (ld(DN + o + 1) + ld(DN + o));
-            else if (k == KS - 1) v = dz0(g, c, phi, 4, k, i, j) * ncz * ld(DN + idx3(g, KS, i, j));
-            else if (k == KE) v = dz0(g, c, phi, 4, k, i, j) * ncz * ld(DN + o);
+            R v = R(0.0);
+            if (k >= KS && k <= KE - 1) v = dz0(g, c, phi, 4, k, i, j) * ncz * R(0.5) * (R(ld(DN + o + 1)) + R(ld(DN + o)));
+            else if (k == KS - 1) v = dz0(g, c, phi, 4, k, i, j) * ncz * R(R(ld(DN + idx3(g, KS, i, j))));
+            else if (k == KE) v = dz0(g, c, phi, 4, k, i, j) * ncz * R(ld(DN + o));
             ND[o + N3 * 4] = v;
         }
-        ND[o + N3 * 9] = kin ? sfct(k, dx(g, c, phi, 4, 0, k, i, j) * ncx * 0.5 * (ld(DN + o + sI) + ld(DN + o))) : 0.0;
-        ND[o + N3 * 14] = kin ? sfct(k, dy(g, c, phi, 4, 0, k, i, j) * ncy * 0.5 * (ld(DN + o + sJ) + ld(DN + o))) : 0.0;
+        ND[o + N3 * 9] = kin ? sfct(k, dx(g, c, phi, 4, 0, k, i, j) * ncx * R(0.5) * (R(ld(DN + o + sI)) + R(ld(DN + o)))) : R(0.0);
+        ND[o + N3 * 14] = kin ? sfct(k, dy(g, c, phi, 4, 0, k, i, j) * ncy * R(0.5) * (R(ld(DN + o + sJ)) + R(ld(DN + o)))) : R(0.0);
     }
 }
 
-cudaError_t launch_numfilter(const Grid &g, const NdCoef &c, const NdArgs &a, cudaStream_t st)
+template <typename R>
+cudaError_t launch_numfilter(const Grid &g, const NdCoef &c, const NdArgsT<R> &a, cudaStream_t st)
 {
     dim3 b(32, 4);
-    k_phi<<<dim3((g.IA + 3) / 4, g.JA), b, 0, st>>>(g, a);
-    k_numfilter<<<dim3((g.IMAX + 3) / 4, g.JMAX), b, 0, st>>>(g, c, a);
+    k_phi<R><<<dim3((g.IA + 3) / 4, g.JA), b, 0, st>>>(g, a);
+    k_numfilter<R><<<dim3((g.IMAX + 3) / 4, g.JMAX), b, 0, st>>>(g, c, a);
     return cudaGetLastError();
 }
+template cudaError_t launch_numfilter<double>(const Grid &, const NdCoef &, const NdArgsT<double> &, cudaStream_t);
+template cudaError_t launch_numfilter<float>(const Grid &, const NdCoef &, const NdArgsT<float> &, cudaStream_t);
 
 }  // namespace hevi

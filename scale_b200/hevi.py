@@ -263,6 +263,16 @@ def ATMOS_DYN_divergence_dev(**kw):
     call("ATMOS_DYN_divergence_b200_dev", **kw)
 
 
+def ATMOS_DYN_Tinteg_short_rk4_mixed_dev(**kw):
+    """Mixed-precision RK4 short step; mflx_hi, tflx_hi, *_t, num_diff, DDIV are float32 device tensors."""
+    call("ATMOS_DYN_Tinteg_short_rk4_b200_mixed_dev", **kw)
+
+
+def ATMOS_DYN_numfilter_coef_mixed_dev(**kw):
+    """Numerical filter with a float32 num_diff device tensor."""
+    call("ATMOS_DYN_numfilter_coef_b200_mixed_dev", **kw)
+
+
 def COMM_vars8_dev(var, nfields: int):
     call("COMM_vars8_b200_dev", var=var, nfields=nfields)
 
