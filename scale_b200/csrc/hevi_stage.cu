@@ -508,11 +508,13 @@ __global__ void __launch_bounds__(32 * HEVI_COL_TC, HEVI_COL_MINB) k_hevi_stage(
         }
     }
     if (w > 0 || TC == 1) {
-        // rho*u / rho*v of the tile: (column, 32-level chunk, component) items over the worker warps
+        // rho*u / rho*v of the tile: (32-level chunk, column, component) items over
+        // the worker warps, chunk-major so that the warps work on one chunk of the
+        // tile at a time and share its neighbour data in L1
         const int nworkers = TC > 1 ? TC - 1 : 1, wid = TC > 1 ? w - 1 : 0;
         const int NL = (g.KMAX + 31) / 32;
         for (int it = wid; it < 2 * TC * NL; it += nworkers) {
-            const int item = it >> 1, cc = item / NL, L = KS + (item % NL) * 32 + lane;
+            const int item = it >> 1, cc = item % TC, L = KS + (item / TC) * 32 + lane;
             const int ii = i0 + cc % TX, jj = j0 + cc / TX;
             if (ii <= g.IE && jj <= g.JE) { // warp-uniform branch
                 if (it & 1) update_mom<S, 1>(g, a, nd, N3, L, ii, jj, L <= KE);
