@@ -318,6 +318,20 @@ int scale_hevi_profile(int enable);
 const char *scale_hevi_profile_report(void);
 
 /* ---------------------------------------------------------------------------
+ * CUDA graph of a call sequence on the library's stream; no counterpart in the
+ * reference. Between scale_hevi_capture_begin() and scale_hevi_capture_end()
+ * the _dev entries are recorded instead of run; scale_hevi_replay(&n) then
+ * launches the recorded sequence n times. The entries must have run once
+ * eagerly with the same arguments before the capture, so that their one-time
+ * checks and table uploads (which synchronise) are already done. A new capture
+ * replaces the previous graph; the graph keeps the pointers it was recorded
+ * with.
+ * ------------------------------------------------------------------------- */
+int scale_hevi_capture_begin(void);
+int scale_hevi_capture_end(void);
+int scale_hevi_replay(const int *n);
+
+/* ---------------------------------------------------------------------------
  * FP64 domain budget: total = sum over the interior of var*CDZ*CDX*CDY, the
  * mass total of check_mass (scalelib/src/atmos-rm/dynamics/scale_atmos_dyn.F90:530-688)
  * computed on the device with a fixed reduction order. var is a device

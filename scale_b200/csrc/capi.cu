@@ -63,6 +63,10 @@ struct Ctx {
     size_t ev_used = 0;
     std::vector<std::pair<std::string, size_t>> prof_marks; // name, index of the start event
     std::string prof_text;
+    // CUDA graph of a captured call sequence (scale_hevi_capture_*)
+    cudaGraphExec_t graph_exec = nullptr;
+    bool capturing = false;
+    long long capture_from = 0, graph_launches = 0; // kernel launches recorded in the graph
 };
 
 Ctx C;
@@ -145,6 +149,12 @@ void free_all()
     if (C.status) cudaFree(C.status);
     if (C.count) cudaFree(C.count);
     for (cudaEvent_t e : C.ev_pool) cudaEventDestroy(e);
+    if (C.capturing) {
+        cudaGraph_t g = nullptr;
+        if (cudaStreamEndCapture(C.stream, &g) == cudaSuccess && g) cudaGraphDestroy(g);
+        cudaGetLastError();
+    }
+    if (C.graph_exec) cudaGraphExecDestroy(C.graph_exec);
     if (C.stream) cudaStreamDestroy(C.stream);
     C = Ctx();
 }
@@ -978,6 +988,55 @@ int scale_hevi_boundary_dev(double *DENS, double *MOMZ, double *MOMX, double *MO
     ++C.launches;
     double *X[5] = {DENS, MOMZ, MOMX, MOMY, RHOT};
     return halo(X, 5);
+}
+
+int scale_hevi_capture_begin(void)
+{
+    CK(need_setup());
+    if (C.capturing) return fail(SCALE_HEVI_ERR_ARG, "a capture is already open");
+    if (C.prof_on) return fail(SCALE_HEVI_ERR_ARG, "section timers are on; turn them off before a capture");
+    CU(cudaStreamSynchronize(C.stream));
+    CU(cudaStreamBeginCapture(C.stream, cudaStreamCaptureModeThreadLocal));
+    C.capturing = true;
+    C.capture_from = C.launches;
+    return SCALE_HEVI_OK;
+}
+
+int scale_hevi_capture_end(void)
+{
+    CK(need_setup());
+    if (!C.capturing) return fail(SCALE_HEVI_ERR_ARG, "no capture is open");
+    C.capturing = false;
+    const long long recorded = C.launches - C.capture_from;
+    C.launches = C.capture_from; // recorded, not launched
+    cudaGraph_t graph = nullptr;
+    cudaError_t e = cudaStreamEndCapture(C.stream, &graph);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(SCALE_HEVI_ERR_CUDA,
+                    "the capture failed (%s): a call inside it synchronised or allocated; warm up with one eager call first",
+                    cudaGetErrorString(e));
+    }
+    if (C.graph_exec) {
+        cudaGraphExecDestroy(C.graph_exec);
+        C.graph_exec = nullptr;
+    }
+    e = cudaGraphInstantiate(&C.graph_exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return fail(SCALE_HEVI_ERR_CUDA, "cudaGraphInstantiate: %s", cudaGetErrorString(e));
+    C.graph_launches = recorded;
+    return SCALE_HEVI_OK;
+}
+
+int scale_hevi_replay(const int *n)
+{
+    CK(need_setup());
+    if (!C.graph_exec) return fail(SCALE_HEVI_ERR_ARG, "nothing has been captured");
+    for (int q = 0; q < (n ? *n : 1); ++q) {
+        CU(cudaGraphLaunch(C.graph_exec, C.stream));
+        C.launches += C.graph_launches;
+    }
+    return SCALE_HEVI_OK;
 }
 
 int scale_hevi_profile(int enable)

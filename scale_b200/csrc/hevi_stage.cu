@@ -581,10 +581,22 @@ cudaError_t launch_hevi_stage(const Grid &g, const StageArgsT<R> &a, int scheme,
 {
     if (g.KA > MAXKA) return cudaErrorInvalidValue;
     const size_t smem = (size_t)COL_ARRAYS * HEVI_COL_TC * col_pitch(g.KA) * sizeof(double);
-    cudaError_t e = scheme == UD3
-        ? cudaFuncSetAttribute(k_hevi_stage<UD3, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)
-        : cudaFuncSetAttribute(k_hevi_stage<CD4, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    // the shared-memory limit of each instantiation is raised once per device
+    // (also keeps launches free of non-stream calls inside a graph capture)
+    static int attr_dev[2] = {-1, -1};
+    static size_t attr_smem[2] = {0, 0};
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
+    const int s = scheme == UD3 ? 0 : 1;
+    if (attr_dev[s] != dev || attr_smem[s] < smem) {
+        const int lim = 227 * 1024;
+        e = scheme == UD3 ? cudaFuncSetAttribute(k_hevi_stage<UD3, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim)
+                          : cudaFuncSetAttribute(k_hevi_stage<CD4, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
+        if (e != cudaSuccess) return e;
+        attr_dev[s] = dev;
+        attr_smem[s] = lim;
+    }
     dim3 bc(32, HEVI_COL_TC);
     dim3 gc((g.IMAX + HEVI_TILE_X - 1) / HEVI_TILE_X, (g.JMAX + HEVI_TILE_Y - 1) / HEVI_TILE_Y);
     if (scheme == UD3) k_hevi_stage<UD3, R><<<gc, bc, smem, st>>>(g, a);

@@ -92,6 +92,8 @@ def load(path: str | os.PathLike | None = None) -> C.CDLL:
             f.argtypes = [C.POINTER(Index), C.c_char_p, C.c_char_p, C.c_int]
         elif name == "scale_hevi_profile":
             f.argtypes = [C.c_int]
+        elif name in ("scale_hevi_capture_begin", "scale_hevi_capture_end"):
+            f.argtypes = []
         else:
             f.argtypes = [C.c_void_p] * len(params)
     _lib = lib
@@ -132,7 +134,7 @@ class _Args:
 
 
 INT_ARGS = {"FLAG_FCT_MOMENTUM", "FLAG_FCT_T", "FLAG_FCT_ALONG_STREAM", "FLAG_FCT_TRACER", "BND_W", "BND_E",
-            "BND_S", "BND_N", "last", "ND_ORDER", "ND_USE_RS", "QA", "nfields"}
+            "BND_S", "BND_N", "last", "ND_ORDER", "ND_USE_RS", "QA", "nfields", "n"}
 # arguments passed as they are (an address, a C string or a stream handle), not by reference
 RAW_ARGS = {"idx", "flux_type", "stream"}
 
@@ -174,6 +176,20 @@ def transfer_bytes() -> tuple[int, int]:
     h, d = C.c_longlong(0), C.c_longlong(0)
     _check(load().scale_hevi_transfer_bytes(C.byref(h), C.byref(d)))
     return int(h.value), int(d.value)
+
+
+def capture_begin() -> None:
+    """Start recording the _dev calls on the library stream into a CUDA graph."""
+    _check(load().scale_hevi_capture_begin())
+
+
+def capture_end() -> None:
+    _check(load().scale_hevi_capture_end())
+
+
+def replay(n: int = 1) -> None:
+    """Launch the captured graph n times on the library stream."""
+    call("scale_hevi_replay", n=n)
 
 
 def profile(enable: bool) -> None:
