@@ -318,6 +318,44 @@ int scale_hevi_profile(int enable);
 const char *scale_hevi_profile_report(void);
 
 /* ---------------------------------------------------------------------------
+ * Ensembles; no counterpart in the reference, where each member is a separate
+ * run. n members of possibly different sizes (each its own index set, same
+ * flux schemes) share one library state; every kernel of the short step then
+ * advances all members in one launch. After scale_hevi_ensemble_setup the
+ * short-step _dev entries (ATMOS_DYN_Tstep_short_fvm_hevi_b200_dev,
+ * ATMOS_DYN_Tinteg_short_rk4_b200[_mixed]_dev,
+ * ATMOS_DYN_numfilter_coef_b200[_mixed]_dev, scale_hevi_boundary_dev,
+ * COMM_vars8_b200_dev) take POOLED arrays:
+ *   - a 3-D field holds member m's (KA,IA,JA) array at point cell0[m]; a
+ *     multi-component array (num_diff(...,15), mflx_hi(...,3), GSQRT(...,7))
+ *     holds component q of member m at q*cell0[n] + cell0[m];
+ *   - a 2-D field (CORIOLI) holds member m's (IA,JA) array at col0[m]
+ *     (MAPF: component q at q*col0[n] + col0[m]);
+ *   - a 1-D z vector (CDZ, FDZ, RCDZ, RFDZ, wdamp_coef) holds member m's KA
+ *     values at z0[m] (FDZ/RFDZ use KA-1 of the KA slots); x and y vectors
+ *     likewise at x0[m] (IA slots) and y0[m] (JA slots).
+ * The time step and the filter and damping coefficients are common to all
+ * members; divergence damping, the tracer, large-step, divergence and
+ * domain-sum entries and the host-array entries need a single domain
+ * (SCALE_HEVI_ERR_UNSUPPORTED otherwise). scale_hevi_setup(idx, ...) is
+ * scale_hevi_ensemble_setup(1, idx, ...). At most 64 members.
+ * scale_hevi_ensemble_layout fills arrays of n+1 entries with those offsets;
+ * entry n holds the pooled totals. Any pointer may be NULL.
+ * ------------------------------------------------------------------------- */
+int scale_hevi_ensemble_setup(int n, const scale_hevi_index *idx, const char *flux_type,
+                              const char *flux_tracer_type, int device);
+int scale_hevi_ensemble_layout(long long *cell0, long long *col0, long long *z0, long long *x0, long long *y0);
+
+/* ---------------------------------------------------------------------------
+ * Launch shape of the stage kernel; no counterpart in the reference. A CTA
+ * owns 16 columns as a tile of tile_x x (16/tile_x) columns (tile_x one of
+ * 16, 8, 4) and CTAs are issued in raster groups of `raster` tile rows.
+ * 0 selects the default (16, 16). The shape changes the speed only: results
+ * are identical for every shape.
+ * ------------------------------------------------------------------------- */
+int scale_hevi_stage_shape(int tile_x, int raster);
+
+/* ---------------------------------------------------------------------------
  * CUDA graph of a call sequence on the library's stream; no counterpart in the
  * reference. Between scale_hevi_capture_begin() and scale_hevi_capture_end()
  * the _dev entries are recorded instead of run; scale_hevi_replay(&n) then

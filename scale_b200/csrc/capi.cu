@@ -26,7 +26,13 @@ struct Ctx {
     scale_hevi_index idx{};
     Grid g{};
     int scheme = UD3, scheme_tracer = UD3;
-    size_t N3 = 0;
+    size_t N3 = 0;   // points of one 3-D field (all members)
+    // ensemble members sharing the pooled arrays (one entry for a single domain)
+    std::vector<MemberGeom> members;
+    std::vector<scale_hevi_index> member_idx;
+    size_t N2 = 0;                   // points of one 2-D field (all members)
+    int ZT = 0, XT = 0, YT = 0;      // lengths of the pooled z/x/y vectors
+    StageShape shape;                // stage tile shape (autotuned or set)
     long long launches = 0;
     long long h2d_bytes = 0, d2h_bytes = 0; // host<->device copies of the host-array entries
     // 1-D tables on the device: CDZ FDZ RCDZ RFDZ F2H1 F2H2 wdamp (KA each),
@@ -97,6 +103,18 @@ int fail(int code, const char *fmt, ...)
 int need_setup()
 {
     if (!C.ready) return fail(SCALE_HEVI_ERR_NOT_SETUP, "scale_hevi_setup() has not been called");
+    return SCALE_HEVI_OK;
+}
+
+Members mem() { return Members{C.members.data(), (int)C.members.size()}; }
+
+// entries that only a single domain supports
+int need_single(const char *what)
+{
+    CK(need_setup());
+    if (C.members.size() > 1)
+        return fail(SCALE_HEVI_ERR_UNSUPPORTED, "%s is not available for an ensemble (%zu members)", what,
+                    C.members.size());
     return SCALE_HEVI_OK;
 }
 
@@ -210,7 +228,7 @@ int check_flat(const double *GSQRT, const double *J13G, const double *J23G, cons
 {
     std::vector<const void *> key = {GSQRT, J13G, J23G, MAPF, (const void *)(size_t)on_device};
     for (auto &k : C.flat_ok) if (k == key) return SCALE_HEVI_OK;
-    const size_t n7 = 7 * C.N3, nm = (size_t)C.g.IA * C.g.JA * 2 * 4;
+    const size_t n7 = 7 * C.N3, nm = C.N2 * 2 * 4;
     unsigned long long bad = 0;
     if (on_device) {
         CU(cudaMemsetAsync(C.count, 0, sizeof(unsigned long long), C.stream));
@@ -240,70 +258,78 @@ int prepare_tables(const double *CDZ, const double *FDZ, const double *RCDZ, con
                    const double *FDY, const double *RCDY, const double *RFDY, const double *wdamp,
                    const double *CDX, const double *CDY)
 {
-    const int KA = C.g.KA, IA = C.g.IA, JA = C.g.JA;
-    std::vector<double> h(7 * (size_t)KA + 4 * (size_t)IA + 4 * (size_t)JA, 0.0);
-    double *z = h.data(), *x = z + 7 * (size_t)KA, *y = x + 4 * (size_t)IA;
+    // pooled layout: table t of the z vectors at t*ZT, member m's values at z0
+    // of it (KA slots; FDZ/RFDZ use KA-1); likewise x (IA) and y (JA)
+    const size_t ZT = C.ZT, XT = C.XT, YT = C.YT;
+    std::vector<double> h(7 * ZT + 4 * XT + 4 * YT, 0.0);
+    double *z = h.data(), *x = z + 7 * ZT, *y = x + 4 * XT;
     if (!CDZ || !FDZ || !RCDZ || !RFDZ || !FDX || !RCDX || !RFDX || !FDY || !RCDY || !RFDY)
         return fail(SCALE_HEVI_ERR_ARG, "a 1-D grid vector is NULL");
-    std::memcpy(z, CDZ, KA * sizeof(double));
-    std::memcpy(z + KA, FDZ, (KA - 1) * sizeof(double));
-    std::memcpy(z + 2 * KA, RCDZ, KA * sizeof(double));
-    std::memcpy(z + 3 * KA, RFDZ, (KA - 1) * sizeof(double));
-    build_f2h(KA, CDZ, z + 4 * KA, z + 5 * KA);
-    if (wdamp) std::memcpy(z + 6 * KA, wdamp, KA * sizeof(double));
-    std::memcpy(x, FDX, (IA - 1) * sizeof(double));
-    std::memcpy(x + IA, RCDX, IA * sizeof(double));
-    std::memcpy(x + 2 * IA, RFDX, (IA - 1) * sizeof(double));
-    if (CDX) std::memcpy(x + 3 * IA, CDX, IA * sizeof(double));
-    std::memcpy(y, FDY, (JA - 1) * sizeof(double));
-    std::memcpy(y + JA, RCDY, JA * sizeof(double));
-    std::memcpy(y + 2 * JA, RFDY, (JA - 1) * sizeof(double));
-    if (CDY) std::memcpy(y + 3 * JA, CDY, JA * sizeof(double));
+    for (const MemberGeom &m : C.members) {
+        const int KA = m.KMAX + 4, IA = m.IMAX + 4, JA = m.JMAX + 4, z0 = m.z0, x0 = m.x0, y0 = m.y0;
+        std::memcpy(z + z0, CDZ + z0, KA * sizeof(double));
+        std::memcpy(z + ZT + z0, FDZ + z0, (KA - 1) * sizeof(double));
+        std::memcpy(z + 2 * ZT + z0, RCDZ + z0, KA * sizeof(double));
+        std::memcpy(z + 3 * ZT + z0, RFDZ + z0, (KA - 1) * sizeof(double));
+        build_f2h(KA, CDZ + z0, z + 4 * ZT + z0, z + 5 * ZT + z0);
+        if (wdamp) std::memcpy(z + 6 * ZT + z0, wdamp + z0, KA * sizeof(double));
+        std::memcpy(x + x0, FDX + x0, (IA - 1) * sizeof(double));
+        std::memcpy(x + XT + x0, RCDX + x0, IA * sizeof(double));
+        std::memcpy(x + 2 * XT + x0, RFDX + x0, (IA - 1) * sizeof(double));
+        if (CDX) std::memcpy(x + 3 * XT + x0, CDX + x0, IA * sizeof(double));
+        std::memcpy(y + y0, FDY + y0, (JA - 1) * sizeof(double));
+        std::memcpy(y + YT + y0, RCDY + y0, JA * sizeof(double));
+        std::memcpy(y + 2 * YT + y0, RFDY + y0, (JA - 1) * sizeof(double));
+        if (CDY) std::memcpy(y + 3 * YT + y0, CDY + y0, JA * sizeof(double));
+    }
     if (!C.tab_valid || h != C.h_tab) {
         CU(cudaMemcpyAsync(C.d_tab, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice, C.stream));
         CU(cudaStreamSynchronize(C.stream)); // the host vector is freed on return
         C.h_tab.swap(h);
         C.tab_valid = true;
     }
-    double *dz = C.d_tab, *dx = dz + 7 * (size_t)KA, *dy = dx + 4 * (size_t)IA;
-    C.g.CDZ = dz; C.g.FDZ = dz + KA; C.g.RCDZ = dz + 2 * KA; C.g.RFDZ = dz + 3 * KA;
-    C.g.F2H1 = dz + 4 * KA; C.g.F2H2 = dz + 5 * KA; C.d_wdamp = dz + 6 * KA;
-    C.g.FDX = dx; C.g.RCDX = dx + IA; C.g.RFDX = dx + 2 * IA;
-    C.g.FDY = dy; C.g.RCDY = dy + JA; C.g.RFDY = dy + 2 * JA;
+    double *dz = C.d_tab, *dx = dz + 7 * ZT, *dy = dx + 4 * XT;
+    C.g.CDZ = dz; C.g.FDZ = dz + ZT; C.g.RCDZ = dz + 2 * ZT; C.g.RFDZ = dz + 3 * ZT;
+    C.g.F2H1 = dz + 4 * ZT; C.g.F2H2 = dz + 5 * ZT; C.d_wdamp = dz + 6 * ZT;
+    C.g.FDX = dx; C.g.RCDX = dx + XT; C.g.RFDX = dx + 2 * XT;
+    C.g.FDY = dy; C.g.RCDY = dy + YT; C.g.RFDY = dy + 2 * YT;
     return SCALE_HEVI_OK;
 }
 
 int prepare_nd(const double *CDZ, const double *CDX, const double *CDY, const double *FDZ, const double *FDX,
                const double *FDY, double DT, double ND_COEF, int ND_ORDER, double SFC)
 {
-    const int KA = C.g.KA, IA = C.g.IA, JA = C.g.JA;
+    const size_t ZT = C.ZT, XT = C.XT, YT = C.YT;
     std::vector<double> key;
-    key.insert(key.end(), CDZ, CDZ + KA); key.insert(key.end(), FDZ, FDZ + KA - 1);
-    key.insert(key.end(), CDX, CDX + IA); key.insert(key.end(), FDX, FDX + IA - 1);
-    key.insert(key.end(), CDY, CDY + JA); key.insert(key.end(), FDY, FDY + JA - 1);
+    key.insert(key.end(), CDZ, CDZ + ZT); key.insert(key.end(), FDZ, FDZ + ZT - 1);
+    key.insert(key.end(), CDX, CDX + XT); key.insert(key.end(), FDX, FDX + XT - 1);
+    key.insert(key.end(), CDY, CDY + YT); key.insert(key.end(), FDY, FDY + YT - 1);
     key.push_back(DT); key.push_back(ND_COEF); key.push_back((double)ND_ORDER);
-    const size_t nz = 3 * (size_t)KA * 2, nx = 3 * (size_t)IA * 2, ny = 3 * (size_t)JA * 2;
+    // pooled layout: CNZ3 (6 values per level), CNX3, CNY3, then cdz fdz (ZT
+    // each), cdx fdx (XT), cdy fdy (YT); member m at 6*z0 / z0 / ...
+    const size_t oX3 = 6 * ZT, oY3 = oX3 + 6 * XT, ocdz = oY3 + 6 * YT, ofdz = ocdz + ZT, ocdx = ofdz + ZT,
+                 ofdx = ocdx + XT, ocdy = ofdx + XT, ofdy = ocdy + YT;
     if (key != C.nd_key) {
-        NdGrid gr{KA, IA, JA, C.g.KS, C.g.KE, C.g.IS, C.g.IE, C.g.JS, C.g.JE, CDZ, FDZ, CDX, FDX, CDY, FDY};
-        NdTables t;
-        build_nd_tables(gr, DT, ND_COEF, ND_ORDER, t);
-        std::vector<double> h;
-        for (auto *v : {&t.CNZ3, &t.CNX3, &t.CNY3, &t.cdz, &t.fdz, &t.cdx, &t.fdx, &t.cdy, &t.fdy})
-            h.insert(h.end(), v->begin(), v->end());
+        std::vector<double> h(ofdy + YT, 0.0);
+        for (const MemberGeom &m : C.members) {
+            const int KA = m.KMAX + 4, IA = m.IMAX + 4, JA = m.JMAX + 4, z0 = m.z0, x0 = m.x0, y0 = m.y0;
+            NdGrid gr{KA, IA, JA, 3, m.KMAX + 2, 3, m.IMAX + 2, 3, m.JMAX + 2,
+                      CDZ + z0, FDZ + z0, CDX + x0, FDX + x0, CDY + y0, FDY + y0};
+            NdTables t;
+            build_nd_tables(gr, DT, ND_COEF, ND_ORDER, t);
+            auto put = [&](const std::vector<double> &v, size_t at) { std::copy(v.begin(), v.end(), h.begin() + at); };
+            put(t.CNZ3, 6 * (size_t)z0); put(t.CNX3, oX3 + 6 * (size_t)x0); put(t.CNY3, oY3 + 6 * (size_t)y0);
+            put(t.cdz, ocdz + z0); put(t.fdz, ofdz + z0); put(t.cdx, ocdx + x0); put(t.fdx, ofdx + x0);
+            put(t.cdy, ocdy + y0); put(t.fdy, ofdy + y0);
+        }
         CU(cudaMemcpyAsync(C.d_nd, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice, C.stream));
         CU(cudaStreamSynchronize(C.stream));
         C.nd_key.swap(key);
     }
     const double *p = C.d_nd;
-    C.ndc.CNZ3 = p; p += nz;
-    C.ndc.CNX3 = p; p += nx;
-    C.ndc.CNY3 = p; p += ny;
-    C.ndc.cdz = p; p += KA;
-    C.ndc.fdz = p; p += KA;
-    C.ndc.cdx = p; p += IA;
-    C.ndc.fdx = p; p += IA;
-    C.ndc.cdy = p; p += JA;
-    C.ndc.fdy = p;
+    C.ndc.CNZ3 = p; C.ndc.CNX3 = p + oX3; C.ndc.CNY3 = p + oY3;
+    C.ndc.cdz = p + ocdz; C.ndc.fdz = p + ofdz; C.ndc.cdx = p + ocdx; C.ndc.fdx = p + ofdx;
+    C.ndc.cdy = p + ocdy; C.ndc.fdy = p + ofdy;
     C.ndc.sfc = SFC;
     return SCALE_HEVI_OK;
 }
@@ -313,7 +339,7 @@ int halo(T *const *f, int n)
 {
     C.launches += (n + 15) / 16;
     return timed("halo", [&] {
-        periodic_halo(C.g, f, n, C.stream);
+        periodic_halo(C.g, mem(), f, n, C.stream);
         return SCALE_HEVI_OK;
     });
 }
@@ -344,6 +370,8 @@ template <typename F>
 int run_stage(const StageInT<F> &in, double *const out[5], F *mflx, F *tflx, double dtrk, int mode)
 {
     if (in.divdmp != 0.0 && !in.DDIV) return fail(SCALE_HEVI_ERR_ARG, "divdmp_coef is nonzero but DDIV is NULL");
+    if (in.divdmp != 0.0 && C.members.size() > 1)
+        return fail(SCALE_HEVI_ERR_UNSUPPORTED, "divergence damping is not available for an ensemble");
     StageArgsT<F> a{};
     a.DENS_RK = out[0]; a.MOMZ_RK = out[1]; a.MOMX_RK = out[2]; a.MOMY_RK = out[3]; a.RHOT_RK = out[4];
     a.mflx = mflx; a.tflx = tflx;
@@ -355,7 +383,7 @@ int run_stage(const StageInT<F> &in, double *const out[5], F *mflx, F *tflx, dou
     a.divdmp_coef = in.divdmp; a.J33G = in.J33G; a.dtrk = dtrk;
     a.rk_mode = mode; a.acc = C.acc; a.facc = facc_buf<F>(); a.status = C.status; a.colscr = colscr_buf<F>();
     CK(timed(sizeof(F) == sizeof(double) ? "hevi_stage" : "hevi_stage_mixed", [&] {
-        CU(launch_hevi_stage(C.g, a, C.scheme, C.stream));
+        CU(launch_hevi_stage(C.g, mem(), a, C.scheme, C.shape, C.stream));
         return SCALE_HEVI_OK;
     }));
     ++C.launches;
@@ -404,7 +432,7 @@ int run_numfilter(R *num_diff, const double *DENS, const double *MOMZ, const dou
     }
     NdArgsT<R> a{num_diff, DENS, MOMZ, MOMX, MOMY, RHOT, REF_dens, REF_pott, phi};
     CK(timed(sizeof(R) == sizeof(double) ? "numfilter" : "numfilter_mixed", [&] {
-        CU(launch_numfilter(C.g, C.ndc, a, C.stream));
+        CU(launch_numfilter(C.g, mem(), C.ndc, a, C.stream));
         return SCALE_HEVI_OK;
     }));
     C.launches += 2;
@@ -463,12 +491,9 @@ void hevi::set_last_error(const char *msg) { g_err = msg ? msg : ""; }
 // =============================================================================
 extern "C" {
 
-int scale_hevi_setup(const scale_hevi_index *idx, const char *flux_type, const char *flux_tracer_type, int device)
+// checks of one index set (of a domain or an ensemble member)
+static int check_index(const scale_hevi_index &x)
 {
-    if (C.ready) free_all();
-    g_err.clear();
-    if (!idx) return fail(SCALE_HEVI_ERR_ARG, "index set is NULL");
-    const scale_hevi_index &x = *idx;
     if (x.KHALO != 2 || x.IHALO != 2 || x.JHALO != 2) return fail(SCALE_HEVI_ERR_UNSUPPORTED, "halo width must be 2");
     if (x.KA != x.KMAX + 2 * x.KHALO || x.IA != x.IMAX + 2 * x.IHALO || x.JA != x.JMAX + 2 * x.JHALO ||
         x.KS != 1 + x.KHALO || x.KE != x.KMAX + x.KHALO || x.IS != 1 + x.IHALO || x.IE != x.IMAX + x.IHALO ||
@@ -479,8 +504,29 @@ int scale_hevi_setup(const scale_hevi_index *idx, const char *flux_type, const c
     if (x.IMAX < 2 || x.JMAX < 2) return fail(SCALE_HEVI_ERR_ARG, "IMAX and JMAX must be >= IHALO, JHALO");
     if ((x.IBLOCK > 0 && x.IBLOCK != x.IMAX) || (x.JBLOCK > 0 && x.JBLOCK != x.JMAX))
         return fail(SCALE_HEVI_ERR_UNSUPPORTED, "only the default IBLOCK=IMAX, JBLOCK=JMAX blocking is supported");
-    if ((double)x.KA * x.IA * x.JA >= 2147483648.0)
-        return fail(SCALE_HEVI_ERR_UNSUPPORTED, "a field of %d x %d x %d points exceeds 2^31 points", x.KA, x.IA, x.JA);
+    return SCALE_HEVI_OK;
+}
+
+int scale_hevi_ensemble_setup(int n, const scale_hevi_index *idx, const char *flux_type, const char *flux_tracer_type,
+                              int device)
+{
+    if (C.ready) free_all();
+    g_err.clear();
+    if (!idx) return fail(SCALE_HEVI_ERR_ARG, "index set is NULL");
+    if (n < 1 || n > HEVI_MAX_MEMBERS) return fail(SCALE_HEVI_ERR_ARG, "ensemble of %d members (1..%d)", n, HEVI_MAX_MEMBERS);
+    std::vector<MemberGeom> mem(n);
+    size_t N3 = 0, N2 = 0;
+    long long ZT = 0, XT = 0, YT = 0;
+    for (int m = 0; m < n; ++m) {
+        const scale_hevi_index &x = idx[m];
+        CK(check_index(x));
+        mem[m] = MemberGeom{x.KMAX, x.IMAX, x.JMAX, (int)ZT, (int)XT, (int)YT, (int)N3, (int)N2};
+        N3 += (size_t)x.KA * x.IA * x.JA;
+        N2 += (size_t)x.IA * x.JA;
+        ZT += x.KA; XT += x.IA; YT += x.JA;
+        if ((double)N3 >= 2147483648.0)
+            return fail(SCALE_HEVI_ERR_UNSUPPORTED, "the fields of the domain%s exceed 2^31 points", n > 1 ? "s" : "");
+    }
     int s1, s2;
     CK(parse_scheme(flux_type, &s1));
     CK(parse_scheme(flux_tracer_type, &s2));
@@ -492,7 +538,10 @@ int scale_hevi_setup(const scale_hevi_index *idx, const char *flux_type, const c
     if (device < 0 || device >= ndev) return fail(SCALE_HEVI_ERR_ARG, "device %d out of range (%d devices)", device, ndev);
     CU(cudaSetDevice(device));
     C.device = device;
+    const scale_hevi_index &x = idx[0];
     C.idx = x;
+    C.member_idx.assign(idx, idx + n);
+    C.members = mem;
     C.scheme = s1;
     C.scheme_tracer = s2;
     Grid &g = C.g;
@@ -500,12 +549,15 @@ int scale_hevi_setup(const scale_hevi_index *idx, const char *flux_type, const c
     g.KS = x.KS; g.KE = x.KE; g.IS = x.IS; g.IE = x.IE; g.JS = x.JS; g.JE = x.JE;
     g.KMAX = x.KMAX; g.IMAX = x.IMAX; g.JMAX = x.JMAX; g.IHALO = x.IHALO; g.JHALO = x.JHALO;
     g.IEH = x.IE; g.JEH = x.JE; // BND_E = BND_N = .false.
-    C.N3 = (size_t)x.KA * x.IA * x.JA;
-    const size_t N3 = C.N3;
+    g.cell0 = g.c2 = g.z0 = g.x0 = g.y0 = 0;
+    g.stride = N3;
+    C.N3 = N3;
+    C.N2 = N2;
+    C.ZT = (int)ZT; C.XT = (int)XT; C.YT = (int)YT;
     CU(cudaStreamCreateWithFlags(&C.stream, cudaStreamNonBlocking));
     int rc = SCALE_HEVI_OK;
-    if ((rc = dalloc(&C.d_tab, 7 * (size_t)x.KA + 4 * (size_t)x.IA + 4 * (size_t)x.JA)) ||
-        (rc = dalloc(&C.d_nd, 8 * (size_t)x.KA + 8 * (size_t)x.IA + 8 * (size_t)x.JA)) ||
+    if ((rc = dalloc(&C.d_tab, 7 * (size_t)ZT + 4 * (size_t)XT + 4 * (size_t)YT)) ||
+        (rc = dalloc(&C.d_nd, 8 * (size_t)ZT + 8 * (size_t)XT + 8 * (size_t)YT)) ||
         (rc = dalloc(&C.rk[0], 5 * N3)) || (rc = dalloc(&C.rk[1], 5 * N3)) ||
         (rc = dalloc(&C.acc, 5 * N3)) || (rc = dalloc(&C.facc, 6 * N3)) ||
         (HEVI_COL_SCRATCH && (rc = dalloc(&C.colscr, 3 * N3))) ||
@@ -520,6 +572,38 @@ int scale_hevi_setup(const scale_hevi_index *idx, const char *flux_type, const c
     }
     cudaMemset(C.status, 0, sizeof(unsigned));
     C.ready = true;
+    return SCALE_HEVI_OK;
+}
+
+int scale_hevi_setup(const scale_hevi_index *idx, const char *flux_type, const char *flux_tracer_type, int device)
+{
+    return scale_hevi_ensemble_setup(1, idx, flux_type, flux_tracer_type, device);
+}
+
+int scale_hevi_ensemble_layout(long long *cell0, long long *col0, long long *z0, long long *x0, long long *y0)
+{
+    CK(need_setup());
+    const size_t n = C.members.size();
+    for (size_t m = 0; m <= n; ++m) {
+        const bool end = m == n;
+        const MemberGeom &g = C.members[end ? 0 : m];
+        if (cell0) cell0[m] = end ? (long long)C.N3 : g.cell0;
+        if (col0) col0[m] = end ? (long long)C.N2 : g.c2;
+        if (z0) z0[m] = end ? C.ZT : g.z0;
+        if (x0) x0[m] = end ? C.XT : g.x0;
+        if (y0) y0[m] = end ? C.YT : g.y0;
+    }
+    return SCALE_HEVI_OK;
+}
+
+int scale_hevi_stage_shape(int tile_x, int raster)
+{
+    CK(need_setup());
+    bool ok = tile_x == 0;
+    for (int t : STAGE_TILE_XS) ok |= tile_x == t;
+    if (!ok || raster < 0) return fail(SCALE_HEVI_ERR_ARG, "tile width %d / raster %d is not a compiled shape", tile_x, raster);
+    C.shape.tile_x = tile_x;
+    C.shape.raster = raster;
     return SCALE_HEVI_OK;
 }
 
@@ -570,7 +654,7 @@ int ATMOS_DYN_Tstep_short_fvm_hevi_b200_dev(SCALE_HEVI_TSTEP_SHORT_ARGS)
 
 int ATMOS_DYN_Tstep_short_fvm_hevi_b200(SCALE_HEVI_TSTEP_SHORT_ARGS)
 {
-    CK(need_setup());
+    CK(need_single("the host-array stage entry"));
     CK(check_bnd(BND_W, BND_E, BND_S, BND_N));
     CK(check_flat(GSQRT, J13G, J23G, MAPF, false));
     const size_t N3 = n3(), N2 = (size_t)C.g.IA * C.g.JA;
@@ -626,7 +710,7 @@ int ATMOS_DYN_Tinteg_short_rk4_b200_dev(SCALE_HEVI_TINTEG_SHORT_ARGS)
 
 int ATMOS_DYN_Tinteg_short_rk4_b200(SCALE_HEVI_TINTEG_SHORT_ARGS)
 {
-    CK(need_setup());
+    CK(need_single("the host-array RK4 entry"));
     CK(check_bnd(BND_W, BND_E, BND_S, BND_N));
     CK(check_flat(GSQRT, J13G, J23G, MAPF, false));
     const size_t N3 = n3(), N2 = (size_t)C.g.IA * C.g.JA;
@@ -697,7 +781,7 @@ int ATMOS_DYN_numfilter_coef_b200_dev(SCALE_HEVI_NUMFILTER_ARGS)
 
 int ATMOS_DYN_numfilter_coef_b200(SCALE_HEVI_NUMFILTER_ARGS)
 {
-    CK(need_setup());
+    CK(need_single("the host-array numerical filter"));
     const size_t N3 = n3();
     double *nd, *d[5], *rd, *rp;
     const double *h[5] = {DENS, MOMZ, MOMX, MOMY, RHOT};
@@ -717,7 +801,7 @@ int ATMOS_DYN_numfilter_coef_b200(SCALE_HEVI_NUMFILTER_ARGS)
 // ---- tracer ------------------------------------------------------------------
 static int tracer_common_checks(const double *GSQRT, const double *MAPF, bool on_device)
 {
-    CK(need_setup());
+    CK(need_single("tracer advection"));
     CK(check_flat(GSQRT, nullptr, nullptr, nullptr, on_device));
     // MAPF here is the (IA,JA,2) slice at (x,y)
     if (MAPF) {
@@ -821,7 +905,7 @@ int ATMOS_DYN_Tinteg_tracer_rk3_b200(SCALE_HEVI_TINTEG_TRACER_ARGS)
 int ATMOS_DYN_divergence_b200_dev(SCALE_HEVI_DIVERGENCE_ARGS)
 {
     (void)RFDZ;
-    CK(need_setup());
+    CK(need_single("the divergence"));
     CK(check_flat(GSQRT, J13G, J23G, MAPF, true));
     if (!RCDZ || !RCDX || !RCDY || !FDZ) return fail(SCALE_HEVI_ERR_ARG, "a 1-D grid vector is NULL");
     const int KA = C.g.KA, IA = C.g.IA, JA = C.g.JA;
@@ -835,7 +919,7 @@ int ATMOS_DYN_divergence_b200_dev(SCALE_HEVI_DIVERGENCE_ARGS)
 
 int ATMOS_DYN_divergence_b200(SCALE_HEVI_DIVERGENCE_ARGS)
 {
-    CK(need_setup());
+    CK(need_single("the divergence"));
     CK(check_flat(GSQRT, J13G, J23G, MAPF, false));
     const size_t N3 = n3();
     double *dd, *mz, *mx, *my;
@@ -877,7 +961,7 @@ int COMM_vars8_b200_dev(double *var, const int *nfields)
 int ATMOS_DYN_Tstep_large_fvm_heve_b200_dev(SCALE_HEVI_LARGE_ARGS)
 {
     (void)PHI;
-    CK(need_setup());
+    CK(need_single("the large step"));
     const int qa = *QA;
     if (qa < 0 || qa > 8) return fail(SCALE_HEVI_ERR_UNSUPPORTED, "QA=%d (0..8 supported)", qa);
     if (*ND_COEF != 0.0 && *ND_ORDER != 1) return fail(SCALE_HEVI_ERR_UNSUPPORTED, "ND_ORDER=%d is not supported", *ND_ORDER);
@@ -920,7 +1004,7 @@ int ATMOS_DYN_Tstep_large_fvm_heve_b200_dev(SCALE_HEVI_LARGE_ARGS)
         // divergence for the damping term, :860-871
         if (use_div) CK(run_divergence(DDIV, MOMZ, MOMX, MOMY, C.g.RCDZ, C.g.RCDX, C.g.RCDY, *J33G));
         CK(run_rk4(X, mflx_hi, tflx_hi, base, dts));
-        CK(timed("boundary", [&] { vertical_bc(C.g, DENS, MOMZ, MOMX, MOMY, RHOT, C.stream); return SCALE_HEVI_OK; }));
+        CK(timed("boundary", [&] { vertical_bc(C.g, mem(), DENS, MOMZ, MOMX, MOMY, RHOT, C.stream); return SCALE_HEVI_OK; }));
         ++C.launches;
         CK(halo(X, 5));
         CK(timed("mflx_average", [&] { mflx_accumulate(C.g, mflx_av, mflx_hi, C.stream); return SCALE_HEVI_OK; }));
@@ -943,7 +1027,7 @@ int ATMOS_DYN_Tstep_large_fvm_heve_b200_dev(SCALE_HEVI_LARGE_ARGS)
 
 int ATMOS_DYN_Tstep_large_fvm_heve_b200(SCALE_HEVI_LARGE_ARGS)
 {
-    CK(need_setup());
+    CK(need_single("the large step"));
     CK(check_flat(GSQRT, J13G, J23G, MAPF, false));
     const size_t N3 = n3(), N2 = (size_t)C.g.IA * C.g.JA;
     const int qa = *QA;
@@ -984,7 +1068,7 @@ int ATMOS_DYN_Tstep_large_fvm_heve_b200(SCALE_HEVI_LARGE_ARGS)
 int scale_hevi_boundary_dev(double *DENS, double *MOMZ, double *MOMX, double *MOMY, double *RHOT)
 {
     CK(need_setup());
-    CK(timed("boundary", [&] { vertical_bc(C.g, DENS, MOMZ, MOMX, MOMY, RHOT, C.stream); return SCALE_HEVI_OK; }));
+    CK(timed("boundary", [&] { vertical_bc(C.g, mem(), DENS, MOMZ, MOMX, MOMY, RHOT, C.stream); return SCALE_HEVI_OK; }));
     ++C.launches;
     double *X[5] = {DENS, MOMZ, MOMX, MOMY, RHOT};
     return halo(X, 5);
@@ -1075,7 +1159,7 @@ const char *scale_hevi_profile_report(void)
 
 int scale_hevi_domain_sum_dev(const double *var, const double *CDZ, const double *CDX, const double *CDY, double *total)
 {
-    CK(need_setup());
+    CK(need_single("the domain sum"));
     const int KA = C.g.KA, IA = C.g.IA, JA = C.g.JA;
     std::vector<double> h(KA + IA + JA);
     std::memcpy(h.data(), CDZ, KA * sizeof(double));

@@ -33,13 +33,79 @@ struct Grid {
     const double *F2H1, *F2H2;              // face weights CDZ(k)/(CDZ(k)+CDZ(k+1)), CDZ(k+1)/(...)
     const double *FDX, *RCDX, *RFDX;        // (IA)
     const double *FDY, *RCDY, *RFDY;        // (JA)
+    // Ensemble pooling (all zero offsets for a single domain): the domain's
+    // (KA,IA,JA) fields start at point cell0 of pooled arrays whose components
+    // (num_diff(...,15), mflx_hi(...,3), ...) lie `stride` points apart; its
+    // (IA,JA) fields start at c2 and its 1-D vectors at z0/x0/y0 of pooled
+    // tables that hold each member's KA/IA/JA values back to back.
+    int cell0, c2, z0, x0, y0;
+    size_t stride;
 };
 
 __host__ __device__ __forceinline__ size_t idx3(const Grid &g, int k, int i, int j)
 {
-    return (size_t)(k - 1) + (size_t)g.KA * ((size_t)(i - 1) + (size_t)g.IA * (size_t)(j - 1));
+    return (size_t)g.cell0 + (size_t)(k - 1) + (size_t)g.KA * ((size_t)(i - 1) + (size_t)g.IA * (size_t)(j - 1));
 }
-__host__ __device__ __forceinline__ size_t n3(const Grid &g) { return (size_t)g.KA * g.IA * g.JA; }
+// distance between the components of a multi-field array
+__host__ __device__ __forceinline__ size_t n3(const Grid &g) { return g.stride; }
+
+// ---- ensembles: members of different sizes advanced by the same launches ----
+// Every kernel flattens its per-domain grid of blocks to one dimension and
+// concatenates the members' block ranges; a block finds its member by a
+// binary search over the range starts (kernel parameters, so the search reads
+// the constant bank). NM = 1 compiles the single-domain form without it.
+#ifndef HEVI_MAX_MEMBERS
+#define HEVI_MAX_MEMBERS 64
+#endif
+struct MemberGeom {
+    int KMAX, IMAX, JMAX;
+    int z0, x0, y0;  // offsets of the member's 1-D vectors in the pooled tables
+    int cell0, c2;   // offsets of its 3-D and 2-D fields in the pooled arrays
+};
+template <int NM>
+struct BatchT {
+    static constexpr int NMAX = NM;
+    int n;             // members in this launch
+    int first[NM + 1]; // first block of each member; first[n] = all blocks
+    MemberGeom m[NM];
+};
+
+// the member's Grid: sizes, offsets and table pointers of member M (halo 2)
+__host__ __device__ __forceinline__ Grid member_grid(const Grid &t, const MemberGeom &M)
+{
+    Grid g = t;
+    g.KMAX = M.KMAX; g.IMAX = M.IMAX; g.JMAX = M.JMAX;
+    g.KA = M.KMAX + 4; g.IA = M.IMAX + 4; g.JA = M.JMAX + 4;
+    g.KS = 3; g.KE = M.KMAX + 2; g.IS = 3; g.IE = M.IMAX + 2; g.JS = 3; g.JE = M.JMAX + 2;
+    g.IHALO = 2; g.JHALO = 2; g.IEH = g.IE; g.JEH = g.JE;
+    g.cell0 = M.cell0; g.c2 = M.c2; g.z0 = M.z0; g.x0 = M.x0; g.y0 = M.y0;
+    g.CDZ = t.CDZ + M.z0; g.FDZ = t.FDZ + M.z0; g.RCDZ = t.RCDZ + M.z0; g.RFDZ = t.RFDZ + M.z0;
+    g.F2H1 = t.F2H1 + M.z0; g.F2H2 = t.F2H2 + M.z0;
+    g.FDX = t.FDX + M.x0; g.RCDX = t.RCDX + M.x0; g.RFDX = t.RFDX + M.x0;
+    g.FDY = t.FDY + M.y0; g.RCDY = t.RCDY + M.y0; g.RFDY = t.RFDY + M.y0;
+    return g;
+}
+
+// This block's domain and its block index b within that domain.
+template <int NM>
+__device__ __forceinline__ Grid block_domain(const Grid &t, const BatchT<NM> &B, int &b)
+{
+    if constexpr (NM == 1) {
+        // a single domain has zero offsets; stating them lets them fold away
+        b = blockIdx.x;
+        Grid g = t;
+        g.cell0 = 0; g.c2 = 0; g.z0 = 0; g.x0 = 0; g.y0 = 0;
+        return g;
+    } else {
+        const int x = blockIdx.x;
+        int lo = 0;
+#pragma unroll
+        for (int step = NM / 2; step > 0; step >>= 1)
+            if (lo + step < B.n && B.first[lo + step] <= x) lo += step;
+        b = x - B.first[lo];
+        return member_grid(t, B.m[lo]);
+    }
+}
 
 constexpr double GRAV = 9.80665;      // scale_const.F90:46
 constexpr double EPS = 2.220446049250313080847263336181640625e-16; // epsilon(0.0_RP)

@@ -1,8 +1,51 @@
 // Argument blocks and host launchers of every device kernel of the library.
 #pragma once
+#include <type_traits>
+#include <utility>
 #include "hevi_stage.cuh"
 
 namespace hevi {
+
+// ---- ensemble members on the host ----
+// The members that share the pooled arrays of one library state; a single
+// domain is one member with zero offsets (or no list at all). The launchers
+// below run every member in the same launch. A view: the caller owns the array.
+struct Members {
+    const MemberGeom *m = nullptr;
+    int n = 0;
+};
+
+// Calls launch(B, nblocks) with the block map of the members for a kernel
+// whose per-domain block count is nblocks_of(member Grid): the single-domain
+// form BatchT<1> for one member, BatchT<HEVI_MAX_MEMBERS> otherwise.
+template <class NB, class L>
+cudaError_t with_batch(const Grid &g, const Members &mem, NB nblocks_of, L launch)
+{
+    if (mem.n <= 1) {
+        BatchT<1> B{};
+        B.n = 1;
+        B.first[0] = 0;
+        B.first[1] = nblocks_of(g);
+        if (mem.n == 1) B.m[0] = mem.m[0];
+        return B.first[1] > 0 ? launch(B, B.first[1]) : cudaSuccess;
+    }
+    if (mem.n > HEVI_MAX_MEMBERS) return cudaErrorInvalidValue;
+    BatchT<HEVI_MAX_MEMBERS> B{};
+    B.n = mem.n;
+    long long total = 0;
+    for (int q = 0; q < B.n; ++q) {
+        B.first[q] = (int)total;
+        B.m[q] = mem.m[q];
+        total += nblocks_of(member_grid(g, mem.m[q]));
+    }
+    if (total >= (1LL << 31)) return cudaErrorInvalidValue;
+    for (int q = B.n; q <= HEVI_MAX_MEMBERS; ++q) B.first[q] = (int)total;
+    return launch(B, (int)total);
+}
+
+// per-member block index b -> (bx, by) of a kernel whose per-domain grid is gx wide
+struct Block2 { int x, y; };
+__device__ __forceinline__ Block2 split_block(int b, int gx) { return {b % gx, b / gx}; }
 
 // ---- numerical filter (numfilter.cu) ----
 // coefficient tables built on the host (grid_coef.cpp), 0-based storage of
@@ -20,7 +63,16 @@ struct NdArgsT {
 };
 using NdArgs = NdArgsT<double>;
 template <typename R>
-cudaError_t launch_numfilter(const Grid &g, const NdCoef &c, const NdArgsT<R> &a, cudaStream_t st);
+cudaError_t launch_numfilter(const Grid &g, const Members &mem, const NdCoef &c, const NdArgsT<R> &a, cudaStream_t st);
+// the member's coefficient tables in the pooled ones (per member: CN*3 hold
+// 6 values per level or point, the nd_coef_* vectors one)
+__host__ __device__ __forceinline__ NdCoef member_nd(const NdCoef &c, const Grid &g)
+{
+    NdCoef m = c;
+    m.CNZ3 += 6 * (size_t)g.z0; m.CNX3 += 6 * (size_t)g.x0; m.CNY3 += 6 * (size_t)g.y0;
+    m.cdz += g.z0; m.fdz += g.z0; m.cdx += g.x0; m.fdx += g.x0; m.cdy += g.y0; m.fdy += g.y0;
+    return m;
+}
 
 // ---- tracer advection (tracer.cu) ----
 struct TracerArgs {
@@ -39,15 +91,25 @@ struct TracerArgs {
 cudaError_t launch_tracer_stage(const Grid &g, const TracerArgs &a, int scheme, bool fct, cudaStream_t st);
 
 // ---- HEVI stage (hevi_stage.cu) ----
+// tile width (columns along i; the CTA's HEVI_COL_TC columns make the tile)
+// and raster height of the stage launch; 0 selects the defaults
+struct StageShape {
+    int tile_x = 0, raster = 0;
+};
+constexpr int STAGE_TILE_XS[3] = {16, 8, 4};
+constexpr int STAGE_TILE_X_DEFAULT = 16;
+constexpr int STAGE_RASTER_DEFAULT = 16;
 template <typename R>
-cudaError_t launch_hevi_stage(const Grid &g, const StageArgsT<R> &a, int scheme, cudaStream_t st);
+cudaError_t launch_hevi_stage(const Grid &g, const Members &mem, const StageArgsT<R> &a, int scheme, StageShape shape,
+                              cudaStream_t st);
 
 // ---- utilities (misc.cu) ----
 template <typename T>
-void periodic_halo(const Grid &g, T *const *fields, int nf, cudaStream_t st);
+void periodic_halo(const Grid &g, const Members &mem, T *const *fields, int nf, cudaStream_t st);
 void divergence(const Grid &g, double *DDIV, const double *MOMZ, const double *MOMX, const double *MOMY,
                 const double *RCDZ, const double *RCDX, const double *RCDY, double J33G, cudaStream_t st);
-void vertical_bc(const Grid &g, double *DENS, double *MOMZ, double *MOMX, double *MOMY, double *RHOT, cudaStream_t st);
+void vertical_bc(const Grid &g, const Members &mem, double *DENS, double *MOMZ, double *MOMX, double *MOMY, double *RHOT,
+                 cudaStream_t st);
 struct PrepArgs {
     double *RT2P, *DPRES0, *REF_rhot;
     const double *RHOT, *QTRC, *REF_pres;

@@ -29,20 +29,15 @@
 // reference HEVI file unless a flux file is named.
 #include "hevi_kernels.cuh"
 
-// Launch shape. The defaults are the measured best on B200 for KMAX = 128;
-// they can be overridden at build time for tuning sweeps.
-#ifndef HEVI_TILE_X
-#define HEVI_TILE_X 16 // columns per CTA along i
+// Launch shape. A CTA is HEVI_COL_TC warps, one column each; the tile is
+// TX x (HEVI_COL_TC/TX) columns with TX one of the compiled widths
+// STAGE_TILE_XS, chosen per workload (the default is the measured best on B200
+// for KMAX = 128, or the autotuner's pick), as is the raster height.
+#ifndef HEVI_COL_TC
+#define HEVI_COL_TC 16 // columns (warps) per CTA
 #endif
-#ifndef HEVI_TILE_Y
-#define HEVI_TILE_Y 1 // columns per CTA along j (blockDim = 32 x HEVI_TILE_X*HEVI_TILE_Y)
-#endif
-#define HEVI_COL_TC (HEVI_TILE_X * HEVI_TILE_Y)
 #ifndef HEVI_COL_MINB
 #define HEVI_COL_MINB 2 // resident CTAs per SM the register allocator must allow
-#endif
-#ifndef HEVI_RASTER_J
-#define HEVI_RASTER_J 16 // rows of tiles launched together (2-D raster: a smaller L2 working set)
 #endif
 #ifndef HEVI_STREAM_HINTS
 #define HEVI_STREAM_HINTS 1 // evict-first loads/stores for data each cell touches once
@@ -236,7 +231,7 @@ __device__ __forceinline__ void update_mom(const Grid &g, const StageArgsT<R> &a
     if (do_u) {
         const R rcdy = R(ld(g.RCDY + j - 1)), fdx = R(ld(g.FDX + i - 1));
         const double rfdx = ld(g.RFDX + i - 1);
-        const R cor_u = R(0.125) * (R(ld(a.CORIOLI + (i) + (size_t)g.IA * (j - 1))) + R(ld(a.CORIOLI + (i - 1) + (size_t)g.IA * (j - 1))));
+        const R cor_u = R(0.125) * (R(ld(a.CORIOLI + g.c2 + (i) + (size_t)g.IA * (j - 1))) + R(ld(a.CORIOLI + g.c2 + (i - 1) + (size_t)g.IA * (j - 1))));
         const R U_m2 = AR(MX, 0, -2, 0), U_m1 = AR(MX, 0, -1, 0), U_00 = AR(MX, 0, 0, 0);
         const R U_p1 = AR(MX, 0, 1, 0), U_p2 = AR(MX, 0, 2, 0);
         // x flux at (x,y,z) with the index shift of fluxX_UYZ (ud3.F90:1053-1109)
@@ -264,7 +259,7 @@ __device__ __forceinline__ void update_mom(const Grid &g, const StageArgsT<R> &a
     if (do_v) {
         const R rcdx = R(ld(g.RCDX + i - 1)), fdy = R(ld(g.FDY + j - 1));
         const double rfdy = ld(g.RFDY + j - 1);
-        const R cor_v = R(-0.125) * (R(ld(a.CORIOLI + (i - 1) + (size_t)g.IA * (j))) + R(ld(a.CORIOLI + (i - 1) + (size_t)g.IA * (j - 1))));
+        const R cor_v = R(-0.125) * (R(ld(a.CORIOLI + g.c2 + (i - 1) + (size_t)g.IA * (j))) + R(ld(a.CORIOLI + g.c2 + (i - 1) + (size_t)g.IA * (j - 1))));
         const R Y_m2 = AR(MY, 0, 0, -2), Y_m1 = AR(MY, 0, 0, -1), Y_00 = AR(MY, 0, 0, 0);
         const R Y_p1 = AR(MY, 0, 0, 1), Y_p2 = AR(MY, 0, 0, 2);
         // x flux at (u,v,z), fluxX_XVZ (ud3.F90:1473-1527)
@@ -306,21 +301,25 @@ enum ColArr : int { CA_C = 0, CA_PT = 1, CA_A = 2, CA_SR = 3, CA_ST = 4, CA_TZ =
 
 __host__ __device__ inline int col_pitch(int KA) { return KA | 1; }
 
-template <int S, typename R>
-__global__ void __launch_bounds__(32 * HEVI_COL_TC, HEVI_COL_MINB) k_hevi_stage(const Grid g, const StageArgsT<R> a)
+template <int S, typename R, int TX, int NM>
+__global__ void __launch_bounds__(32 * HEVI_COL_TC, HEVI_COL_MINB)
+    k_hevi_stage(const Grid gt, const StageArgsT<R> a, const BatchT<NM> B)
 {
     extern __shared__ double sm[];
-    constexpr int TX = HEVI_TILE_X, TY = HEVI_TILE_Y, TC = TX * TY;
+    constexpr int TC = HEVI_COL_TC, TY = TC / TX;
+    static_assert(TX * TY == TC, "the tile width must divide the CTA's column count");
+    int b;
+    const Grid g = block_domain(gt, B, b); // this CTA's ensemble member (the domain itself when NM = 1)
     const int lane = threadIdx.x, w = threadIdx.y;
     const int tx = w % TX, ty = w / TX; // this warp's column in the tile
-    // 2-D raster: consecutive CTAs walk down HEVI_RASTER_J rows of tiles, then
-    // step in i, so the CTAs resident together cover a compact patch
+    // 2-D raster: consecutive CTAs walk down a.raster rows of tiles, then step
+    // in i, so the CTAs resident together cover a compact patch
     int ti, tj;
     {
-        const int nti = gridDim.x, ntj = gridDim.y, b = blockIdx.x + nti * blockIdx.y;
-        const int grp = b / (nti * HEVI_RASTER_J), rem = b - grp * (nti * HEVI_RASTER_J);
-        const int rows = min(HEVI_RASTER_J, ntj - grp * HEVI_RASTER_J);
-        tj = grp * HEVI_RASTER_J + rem % rows;
+        const int nti = (g.IMAX + TX - 1) / TX, ntj = (g.JMAX + TY - 1) / TY, RJ = a.raster;
+        const int grp = b / (nti * RJ), rem = b - grp * (nti * RJ);
+        const int rows = min(RJ, ntj - grp * RJ);
+        tj = grp * RJ + rem % rows;
         ti = rem / rows;
     }
     const int i0 = g.IS + ti * TX, j0 = g.JS + tj * TY;
@@ -454,7 +453,7 @@ __global__ void __launch_bounds__(32 * HEVI_COL_TC, HEVI_COL_MINB) k_hevi_stage(
             const int c = col + k - 1;
             const R adv_w = adv_w_h<S>(g, a, nd, c, k, sI, sJ, rcdx, rcdy);
             const R advcv = -(q_k - q_km) * R(ld(g.RFDZ + k - 1));
-            const R wdmp = -R(ld(a.wdamp + k - 1)) * R(CL(a.MOMZ0, k));
+            const R wdmp = -R(ld(a.wdamp + g.z0 + k - 1)) * R(CL(a.MOMZ0, k));
             const R div = use_div ? ddc * (CL(a.DDIV, k + 1) - CL(a.DDIV, k)) * R(ld(g.FDZ + k - 1)) : R(0.0);
             const R Sw = (advcv + adv_w) + wdmp + div + lds(a.MOMZ_t + c);
             const double rfdz = ld(g.RFDZ + k - 1);
@@ -576,34 +575,65 @@ __global__ void __launch_bounds__(32 * HEVI_COL_TC, HEVI_COL_MINB) k_hevi_stage(
 #undef AR
 
 // ---- host launcher ----------------------------------------------------------
-template <typename R>
-cudaError_t launch_hevi_stage(const Grid &g, const StageArgsT<R> &a, int scheme, cudaStream_t st)
+// Opens the dynamic shared memory of a kernel instantiation to the per-CTA
+// maximum, once per device (keeps later launches free of non-stream calls,
+// e.g. inside a graph capture).
+template <class K>
+static cudaError_t allow_smem(K kern)
 {
-    if (g.KA > MAXKA) return cudaErrorInvalidValue;
-    const size_t smem = (size_t)COL_ARRAYS * HEVI_COL_TC * col_pitch(g.KA) * sizeof(double);
-    // the shared-memory limit of each instantiation is raised once per device
-    // (also keeps launches free of non-stream calls inside a graph capture)
-    static int attr_dev[2] = {-1, -1};
-    static size_t attr_smem[2] = {0, 0};
+    static std::pair<const void *, int> done[64];
+    static int ndone = 0;
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
-    const int s = scheme == UD3 ? 0 : 1;
-    if (attr_dev[s] != dev || attr_smem[s] < smem) {
-        const int lim = 227 * 1024;
-        e = scheme == UD3 ? cudaFuncSetAttribute(k_hevi_stage<UD3, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim)
-                          : cudaFuncSetAttribute(k_hevi_stage<CD4, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, lim);
-        if (e != cudaSuccess) return e;
-        attr_dev[s] = dev;
-        attr_smem[s] = lim;
-    }
-    dim3 bc(32, HEVI_COL_TC);
-    dim3 gc((g.IMAX + HEVI_TILE_X - 1) / HEVI_TILE_X, (g.JMAX + HEVI_TILE_Y - 1) / HEVI_TILE_Y);
-    if (scheme == UD3) k_hevi_stage<UD3, R><<<gc, bc, smem, st>>>(g, a);
-    else k_hevi_stage<CD4, R><<<gc, bc, smem, st>>>(g, a);
+    for (int q = 0; q < ndone; ++q)
+        if (done[q].first == (const void *)kern && done[q].second == dev) return cudaSuccess;
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    if (e == cudaSuccess && ndone < 64) done[ndone++] = {(const void *)kern, dev};
+    return e;
+}
+
+template <int S, typename R, int TX, int NM>
+static cudaError_t launch_one(const Grid &g, StageArgsT<R> a, const BatchT<NM> &B, int nblocks, size_t smem,
+                              int raster, cudaStream_t st)
+{
+    auto kern = k_hevi_stage<S, R, TX, NM>;
+    cudaError_t e = allow_smem(kern);
+    if (e != cudaSuccess) return e;
+    a.raster = raster > 0 ? raster : STAGE_RASTER_DEFAULT;
+    kern<<<nblocks, dim3(32, HEVI_COL_TC), smem, st>>>(g, a, B);
     return cudaGetLastError();
 }
-template cudaError_t launch_hevi_stage<double>(const Grid &, const StageArgsT<double> &, int, cudaStream_t);
-template cudaError_t launch_hevi_stage<float>(const Grid &, const StageArgsT<float> &, int, cudaStream_t);
+
+template <typename R>
+cudaError_t launch_hevi_stage(const Grid &g, const Members &mem, const StageArgsT<R> &a, int scheme,
+                              StageShape shape, cudaStream_t st)
+{
+    int maxKA = g.KA;
+    for (int q = 0; q < mem.n; ++q) maxKA = mem.m[q].KMAX + 4 > maxKA ? mem.m[q].KMAX + 4 : maxKA;
+    if (maxKA > MAXKA) return cudaErrorInvalidValue;
+    const size_t smem = (size_t)COL_ARRAYS * HEVI_COL_TC * col_pitch(maxKA) * sizeof(double);
+    const int tx = shape.tile_x > 0 ? shape.tile_x : STAGE_TILE_X_DEFAULT;
+    auto go = [&](auto tile, const auto &B, int nb) -> cudaError_t {
+        constexpr int TX = decltype(tile)::value, NM = std::decay_t<decltype(B)>::NMAX;
+        return scheme == UD3 ? launch_one<UD3, R, TX, NM>(g, a, B, nb, smem, shape.raster, st)
+                             : launch_one<CD4, R, TX, NM>(g, a, B, nb, smem, shape.raster, st);
+    };
+    auto dispatch = [&](auto tile) {
+        constexpr int TX = decltype(tile)::value, TY = HEVI_COL_TC / TX;
+        auto nblocks = [](const Grid &m) { return ((m.IMAX + TX - 1) / TX) * ((m.JMAX + TY - 1) / TY); };
+        return with_batch(g, mem, nblocks, [&](const auto &B, int nb) { return go(tile, B, nb); });
+    };
+    switch (tx) {
+    case 16: return dispatch(std::integral_constant<int, 16>{});
+    case 8: return dispatch(std::integral_constant<int, 8>{});
+    case 4: return dispatch(std::integral_constant<int, 4>{});
+    default: return cudaErrorInvalidValue;
+    }
+}
+template cudaError_t launch_hevi_stage<double>(const Grid &, const Members &, const StageArgsT<double> &, int,
+                                               StageShape, cudaStream_t);
+template cudaError_t launch_hevi_stage<float>(const Grid &, const Members &, const StageArgsT<float> &, int,
+                                              StageShape, cudaStream_t);
 
 }  // namespace hevi

@@ -51,6 +51,7 @@ struct StageArgsT {
     F *facc;     // 6*N3: mflx Z,X,Y then tflx Z,X,Y
     unsigned *status;
     F *colscr; // 3*N3 (HEVI_COL_SCRATCH): Sr, St, tZ
+    int raster; // rows of tiles per raster group (set by the launcher)
 };
 using StageArgs = StageArgsT<double>;
 

@@ -12,12 +12,14 @@ struct FieldList {
     T *f[16];
 };
 
-template <typename T>
-__global__ void k_halo(const Grid g, const FieldList<T> fl)
+template <typename T, int NM>
+__global__ void k_halo(const Grid gt, const FieldList<T> fl, const BatchT<NM> B)
 {
+    int b;
+    const Grid g = block_domain(gt, B, b);
     const int nA = 2 * g.JHALO * g.IA;      // halo rows j < JS and j > JE, all i
     const int nB = 2 * g.IHALO * g.JMAX;    // halo columns i < IS and i > IE, interior j
-    const int h = blockIdx.x * blockDim.y + threadIdx.y;
+    const int h = b * blockDim.y + threadIdx.y;
     if (h >= nA + nB) return;
     int i, j;
     if (h < nA) {
@@ -38,25 +40,33 @@ __global__ void k_halo(const Grid g, const FieldList<T> fl)
 }
 
 template <typename T>
-void periodic_halo(const Grid &g, T *const *fields, int nf, cudaStream_t st)
+void periodic_halo(const Grid &g, const Members &mem, T *const *fields, int nf, cudaStream_t st)
 {
-    const int nh = 2 * g.JHALO * g.IA + 2 * g.IHALO * g.JMAX;
+    auto nblocks = [](const Grid &m) { return (2 * m.JHALO * m.IA + 2 * m.IHALO * m.JMAX + 3) / 4; };
     for (int base = 0; base < nf; base += 16) {
         FieldList<T> fl;
         const int n = (nf - base) < 16 ? (nf - base) : 16;
         for (int q = 0; q < n; ++q) fl.f[q] = fields[base + q];
-        dim3 b(32, 4), gr((nh + 3) / 4, n);
-        k_halo<T><<<gr, b, 0, st>>>(g, fl);
+        with_batch(g, mem, nblocks, [&](const auto &B, int nb) {
+            constexpr int NM = std::decay_t<decltype(B)>::NMAX;
+            k_halo<T, NM><<<dim3(nb, n), dim3(32, 4), 0, st>>>(g, fl, B);
+            return cudaSuccess;
+        });
     }
 }
-template void periodic_halo<double>(const Grid &, double *const *, int, cudaStream_t);
-template void periodic_halo<float>(const Grid &, float *const *, int, cudaStream_t);
+template void periodic_halo<double>(const Grid &, const Members &, double *const *, int, cudaStream_t);
+template void periodic_halo<float>(const Grid &, const Members &, float *const *, int, cudaStream_t);
 
 // ---- vertical boundary values after a short step (scale_atmos_dyn_tstep_large_fvm_heve.F90:910-926) ----
-__global__ void k_vbc(const Grid g, double *DENS, double *MOMZ, double *MOMX, double *MOMY, double *RHOT)
+template <int NM>
+__global__ void k_vbc(const Grid gt, double *DENS, double *MOMZ, double *MOMX, double *MOMY, double *RHOT,
+                      const BatchT<NM> B)
 {
-    const int i = g.IS + blockIdx.x * blockDim.y + threadIdx.y;
-    const int j = g.JS + blockIdx.y;
+    int b;
+    const Grid g = block_domain(gt, B, b);
+    const Block2 p = split_block(b, (g.IMAX + 3) / 4);
+    const int i = g.IS + p.x * blockDim.y + threadIdx.y;
+    const int j = g.JS + p.y;
     if (i > g.IE) return;
     const size_t c = idx3(g, 1, i, j);
     const int k = 1 + threadIdx.x;
@@ -70,10 +80,15 @@ __global__ void k_vbc(const Grid g, double *DENS, double *MOMZ, double *MOMX, do
     }
 }
 
-void vertical_bc(const Grid &g, double *DENS, double *MOMZ, double *MOMX, double *MOMY, double *RHOT, cudaStream_t st)
+void vertical_bc(const Grid &g, const Members &mem, double *DENS, double *MOMZ, double *MOMX, double *MOMY, double *RHOT,
+                 cudaStream_t st)
 {
-    dim3 b(32, 4), gr((g.IMAX + 3) / 4, g.JMAX);
-    k_vbc<<<gr, b, 0, st>>>(g, DENS, MOMZ, MOMX, MOMY, RHOT);
+    auto nblocks = [](const Grid &m) { return ((m.IMAX + 3) / 4) * m.JMAX; };
+    with_batch(g, mem, nblocks, [&](const auto &B, int nb) {
+        constexpr int NM = std::decay_t<decltype(B)>::NMAX;
+        k_vbc<NM><<<nb, dim3(32, 4), 0, st>>>(g, DENS, MOMZ, MOMX, MOMY, RHOT, B);
+        return cudaSuccess;
+    });
 }
 
 // ---- 3-D divergence for divergence damping, ATMOS_DYN_divergence

@@ -172,6 +172,7 @@ extern "C" int ATMOS_DYN_Tstep_short_fvm_hevi_b200_noalloc(const scale_hevi_inde
     g.CDZ = z; g.FDZ = z + KA; g.RCDZ = z + 2 * KA; g.RFDZ = z + 3 * KA; g.F2H1 = z + 4 * KA; g.F2H2 = z + 5 * KA;
     g.FDX = xs; g.RCDX = xs + IA; g.RFDX = xs + 2 * IA;
     g.FDY = ys; g.RCDY = ys + JA; g.RFDY = ys + 2 * JA;
+    g.stride = (size_t)KA * IA * JA;
 
     StageArgs a{};
     a.DENS_RK = DENS_RK; a.MOMZ_RK = MOMZ_RK; a.MOMX_RK = MOMX_RK; a.MOMY_RK = MOMY_RK; a.RHOT_RK = RHOT_RK;
@@ -185,7 +186,7 @@ extern "C" int ATMOS_DYN_Tstep_short_fvm_hevi_b200_noalloc(const scale_hevi_inde
     a.rk_mode = RK_PLAIN; a.acc = nullptr; a.facc = nullptr; a.status = status;
     a.colscr = HEVI_COL_SCRATCH ? colscr : nullptr;
 
-    NA_CU(launch_hevi_stage(g, a, scheme, st));
+    NA_CU(launch_hevi_stage(g, Members{}, a, scheme, StageShape{}, st));
     unsigned flags = 0;
     NA_CU(cudaMemcpyAsync(&flags, status, sizeof flags, cudaMemcpyDeviceToHost, st));
     NA_CU(cudaStreamSynchronize(st));

@@ -27,11 +27,14 @@ namespace hevi {
 // A velocity needs the density one point above (VELZ), east (VELX) or north
 // (VELY); at the last point of the array in that direction, which no stencil
 // reads, it is stored as zero.
-template <typename R>
-__global__ void __launch_bounds__(128) k_phi(const Grid g, const NdArgsT<R> a)
+template <typename R, int NM>
+__global__ void __launch_bounds__(128) k_phi(const Grid gt, const NdArgsT<R> a, const BatchT<NM> B)
 {
-    const int i = 1 + blockIdx.x * blockDim.y + threadIdx.y;
-    const int j = 1 + blockIdx.y;
+    int b;
+    const Grid g = block_domain(gt, B, b);
+    const Block2 p = split_block(b, (g.IA + 3) / 4);
+    const int i = 1 + p.x * blockDim.y + threadIdx.y;
+    const int j = 1 + p.y;
     if (i > g.IA) return;
     const size_t N3 = n3(g);
     const long sI = g.KA, sJ = (long)g.KA * g.IA;
@@ -140,11 +143,16 @@ __device__ __forceinline__ R dy(const Grid &g, const NdCoef &c, const Phi<R> &ph
 #define HEVI_ND_MINB 8 // minimum resident blocks per SM asked of the register allocator
 #endif
 
-template <typename R>
-__global__ void __launch_bounds__(128, HEVI_ND_MINB) k_numfilter(const Grid g, const NdCoef c, const NdArgsT<R> a)
+template <typename R, int NM>
+__global__ void __launch_bounds__(128, HEVI_ND_MINB)
+    k_numfilter(const Grid gt, const NdCoef ct, const NdArgsT<R> a, const BatchT<NM> B)
 {
-    const int i = g.IS + blockIdx.x * blockDim.y + threadIdx.y;
-    const int j = g.JS + blockIdx.y;
+    int b;
+    const Grid g = block_domain(gt, B, b);
+    const NdCoef c = NM == 1 ? ct : member_nd(ct, g);
+    const Block2 p = split_block(b, (g.IMAX + 3) / 4);
+    const int i = g.IS + p.x * blockDim.y + threadIdx.y;
+    const int j = g.JS + p.y;
     if (i > g.IE) return;
     const size_t N3 = n3(g);
     const int KS = g.KS, KE = g.KE;
@@ -212,14 +220,23 @@ __global__ void __launch_bounds__(128, HEVI_ND_MINB) k_numfilter(const Grid g, c
 }
 
 template <typename R>
-cudaError_t launch_numfilter(const Grid &g, const NdCoef &c, const NdArgsT<R> &a, cudaStream_t st)
+cudaError_t launch_numfilter(const Grid &g, const Members &mem, const NdCoef &c, const NdArgsT<R> &a, cudaStream_t st)
 {
-    dim3 b(32, 4);
-    k_phi<R><<<dim3((g.IA + 3) / 4, g.JA), b, 0, st>>>(g, a);
-    k_numfilter<R><<<dim3((g.IMAX + 3) / 4, g.JMAX), b, 0, st>>>(g, c, a);
+    auto nb_phi = [](const Grid &m) { return ((m.IA + 3) / 4) * m.JA; };
+    auto nb_nd = [](const Grid &m) { return ((m.IMAX + 3) / 4) * m.JMAX; };
+    with_batch(g, mem, nb_phi, [&](const auto &B, int nb) {
+        k_phi<R, std::decay_t<decltype(B)>::NMAX><<<nb, dim3(32, 4), 0, st>>>(g, a, B);
+        return cudaSuccess;
+    });
+    with_batch(g, mem, nb_nd, [&](const auto &B, int nb) {
+        k_numfilter<R, std::decay_t<decltype(B)>::NMAX><<<nb, dim3(32, 4), 0, st>>>(g, c, a, B);
+        return cudaSuccess;
+    });
     return cudaGetLastError();
 }
-template cudaError_t launch_numfilter<double>(const Grid &, const NdCoef &, const NdArgsT<double> &, cudaStream_t);
-template cudaError_t launch_numfilter<float>(const Grid &, const NdCoef &, const NdArgsT<float> &, cudaStream_t);
+template cudaError_t launch_numfilter<double>(const Grid &, const Members &, const NdCoef &, const NdArgsT<double> &,
+                                              cudaStream_t);
+template cudaError_t launch_numfilter<float>(const Grid &, const Members &, const NdCoef &, const NdArgsT<float> &,
+                                             cudaStream_t);
 
 }  // namespace hevi

@@ -285,7 +285,7 @@ cudaError_t launch_tracer_stage(const Grid &g, const TracerArgs &a, int scheme, 
     else k_fct_lo<CD4><<<gl, b, 0, st>>>(g, a);
     k_fct_r<<<gr, b, 0, st>>>(g, a);
     double *rr[2] = {a.rjp, a.rjm};
-    periodic_halo(g, rr, 2, st);
+    periodic_halo(g, Members{}, rr, 2, st);
     if (scheme == UD3) k_fct_apply<UD3><<<gr, b, 0, st>>>(g, a);
     else k_fct_apply<CD4><<<gr, b, 0, st>>>(g, a);
     return cudaGetLastError();

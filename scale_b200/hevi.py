@@ -90,6 +90,10 @@ def load(path: str | os.PathLike | None = None) -> C.CDLL:
             f.restype = C.c_int
         if name == "scale_hevi_setup":
             f.argtypes = [C.POINTER(Index), C.c_char_p, C.c_char_p, C.c_int]
+        elif name == "scale_hevi_ensemble_setup":
+            f.argtypes = [C.c_int, C.POINTER(Index), C.c_char_p, C.c_char_p, C.c_int]
+        elif name == "scale_hevi_stage_shape":
+            f.argtypes = [C.c_int, C.c_int]
         elif name == "scale_hevi_profile":
             f.argtypes = [C.c_int]
         elif name in ("scale_hevi_capture_begin", "scale_hevi_capture_end"):
@@ -157,6 +161,62 @@ def setup(index: dict, flux_type: str = "UD3", flux_tracer_type: str = "UD3", de
     lib = load()
     idx = Index(**index)
     _check(lib.scale_hevi_setup(C.byref(idx), flux_type.encode(), flux_tracer_type.encode(), int(device)))
+
+
+def ensemble_setup(indices: list[dict], flux_type: str = "UD3", flux_tracer_type: str = "UD3",
+                   device: int = 0) -> dict[str, np.ndarray]:
+    """Set up an ensemble of len(indices) members; returns its pooled layout
+    (ensemble_layout())."""
+    lib = load()
+    arr = (Index * len(indices))(*[Index(**d) for d in indices])
+    _check(lib.scale_hevi_ensemble_setup(len(indices), arr, flux_type.encode(), flux_tracer_type.encode(),
+                                         int(device)))
+    return ensemble_layout(len(indices))
+
+
+def ensemble_layout(n: int) -> dict[str, np.ndarray]:
+    """Offsets of each member in the pooled arrays: cell0 (3-D fields), col0
+    (2-D fields), z0/x0/y0 (1-D vectors); n+1 entries, the last the totals."""
+    out = {k: np.zeros(n + 1, dtype=np.int64) for k in ("cell0", "col0", "z0", "x0", "y0")}
+    ptr = lambda v: v.ctypes.data_as(C.POINTER(C.c_longlong))  # noqa: E731
+    _check(load().scale_hevi_ensemble_layout(*(ptr(out[k]) for k in ("cell0", "col0", "z0", "x0", "y0"))))
+    return out
+
+
+def pool(arrays: list[np.ndarray], offsets: np.ndarray, ncomp: int = 1, slots: list[int] | None = None) -> np.ndarray:
+    """Pooled array of per-member arrays (Fortran order): component q of member
+    m at q*offsets[-1] + offsets[m]. For 1-D vectors, `slots` gives each
+    member's length in the pool (a shorter vector leaves its last slot zero)."""
+    total = int(offsets[-1])
+    out = np.zeros(ncomp * total)
+    for m, a in enumerate(arrays):
+        flat = np.ravel(a, order="F")
+        n = flat.size // ncomp
+        if slots is not None and n > slots[m]:
+            raise ValueError(f"member {m}: {n} values for {slots[m]} slots")
+        for q in range(ncomp):
+            o = q * total + int(offsets[m])
+            out[o:o + n] = flat[q * n:(q + 1) * n]
+    return out
+
+
+def unpool(pooled: np.ndarray, offsets: np.ndarray, shapes: list[tuple], ncomp: int = 1) -> list[np.ndarray]:
+    """Per-member arrays (Fortran order, shape shapes[m] + (ncomp,) when
+    ncomp > 1) of a pooled array."""
+    total = int(offsets[-1])
+    flat = np.asarray(pooled).ravel()
+    out = []
+    for m, shp in enumerate(shapes):
+        n = int(np.prod(shp))
+        comps = [flat[q * total + int(offsets[m]): q * total + int(offsets[m]) + n] for q in range(ncomp)]
+        v = np.concatenate(comps) if ncomp > 1 else comps[0].copy()
+        out.append(v.reshape(tuple(shp) + ((ncomp,) if ncomp > 1 else ()), order="F"))
+    return out
+
+
+def stage_shape(tile_x: int = 0, raster: int = 0) -> None:
+    """Tile width and raster height of the stage kernel (0: defaults)."""
+    _check(load().scale_hevi_stage_shape(int(tile_x), int(raster)))
 
 
 def finalize() -> None:

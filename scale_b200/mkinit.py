@@ -356,3 +356,30 @@ def config(n: int, scale: float = 1.0, seed: int = 0) -> Case:
                          bubbles=[(Lx / 2, Ly / 2, 2000.0, 4000.0, 4000.0, 4000.0, 3.0)],
                          theta_noise=0.01, seed=seed)
     raise ValueError(f"unknown configuration {n}")
+
+
+# ---------------------------------------------------------------------------
+# the uneven ensemble
+# ---------------------------------------------------------------------------
+# 48 members of three sizes (IMAX, JMAX, KMAX), all at dx = dy = 500 m with
+# the tutorial's 250 m levels
+ENSEMBLE_SIZES = [(64, 64, 64)] * 16 + [(128, 128, 96)] * 16 + [(256, 256, 96)] * 16
+
+
+def ensemble_member(IMAX: int, JMAX: int, KMAX: int, m: int, seed: int = 0) -> Case:
+    """Member m: one warm bubble at a seeded position with a seeded amplitude
+    in [1, 4] K, and its own seeded +-0.01 K theta noise."""
+    g = uniform_grid(IMAX, JMAX, KMAX, 500.0, 500.0, 250.0)
+    rng = np.random.Generator(np.random.PCG64(seed + 3000 + m))
+    Lx, Ly = g.IMAX * 500.0, g.JMAX * 500.0
+    bub = [(rng.uniform(0.0, Lx), rng.uniform(0.0, Ly), 2000.0, 4000.0, 4000.0, 4000.0, rng.uniform(1.0, 4.0))]
+    return make_case(f"ensemble member {m} {IMAX}x{JMAX}x{KMAX}", g, "UD3", "UD3", dt=1.0, dtl=5.0, bubbles=bub,
+                     theta_noise=0.01, noise_kind="uniform", seed=seed + 100 + m)
+
+
+def ensemble(scale: float = 1.0, seed: int = 0, sizes=None) -> list[Case]:
+    """The members of the uneven ensemble (scale < 1 shrinks the horizontal
+    sizes, for tests; sizes replaces the member list)."""
+    sizes = ENSEMBLE_SIZES if sizes is None else sizes
+    return [ensemble_member(max(8, int(round(I * scale))), max(8, int(round(J * scale))), K, m, seed)
+            for m, (I, J, K) in enumerate(sizes)]

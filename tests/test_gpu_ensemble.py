@@ -1,0 +1,106 @@
+"""Uneven ensembles: members of different sizes advanced together (every
+kernel launch covers all members) give, member by member, the same state bit
+for bit as each member advanced alone by the single-domain path, which the
+parity tests compare with the oracle. Also across the stage kernel's tile
+shapes, with the step replayed as a CUDA graph, and on the mixed-precision
+path."""
+import numpy as np
+import pytest
+
+from scale_b200 import hevi, mkinit
+from scale_b200.ensemble import STATE, Ensemble
+
+pytestmark = pytest.mark.gpu
+
+SIZES = [(16, 12, 20), (24, 20, 24), (8, 10, 16), (33, 17, 12)]
+NSTEPS = 6
+
+
+def _alone(cases, nsteps, mixed=False):
+    out = []
+    for c in cases:
+        e = Ensemble([c], mixed=mixed)
+        try:
+            e.run(nsteps)
+            out.append(e.members()[0])
+        finally:
+            e.close()
+    return out
+
+
+def _together(cases, nsteps, mixed=False, tile_x=0, raster=0, graph=False):
+    e = Ensemble(cases, mixed=mixed)
+    try:
+        hevi.stage_shape(tile_x, raster)
+        if graph:
+            e.capture(1)  # one eager step, then the recorded one
+            e.run(nsteps - 1)
+        else:
+            e.run(nsteps)
+        launches = hevi.kernel_launches()
+        return e.members(), launches
+    finally:
+        e.close()
+
+
+def _same(a, b):
+    for m, (x, y) in enumerate(zip(a, b)):
+        for n in STATE:
+            assert np.array_equal(x[n], y[n]), f"member {m} {n}: max diff {np.max(np.abs(x[n] - y[n])):.3e}"
+
+
+@pytest.fixture(scope="module")
+def cases():
+    return mkinit.ensemble(sizes=SIZES)
+
+
+@pytest.fixture(scope="module")
+def alone(cases):
+    return _alone(cases, NSTEPS)
+
+
+def test_ensemble_matches_members_alone(cases, alone):
+    got, _ = _together(cases, NSTEPS)
+    _same(got, alone)
+    for st in got:
+        assert all(np.isfinite(st[n]).all() for n in STATE)
+
+
+@pytest.mark.parametrize("tile_x,raster", [(8, 4), (4, 1), (16, 64)])
+def test_ensemble_tile_shapes_give_identical_results(cases, alone, tile_x, raster):
+    got, _ = _together(cases, NSTEPS, tile_x=tile_x, raster=raster)
+    _same(got, alone)
+
+
+def test_ensemble_graph_replay(cases, alone):
+    got, _ = _together(cases, NSTEPS, graph=True)
+    _same(got, alone)
+
+
+def test_ensemble_one_launch_per_kernel(cases):
+    # the launch count of a step does not depend on the number of members
+    _, l4 = _together(cases, 2)
+    _, l1 = _together(cases[:1], 2)
+    assert l4 == l1
+
+
+def test_ensemble_mixed_precision_matches_members_alone(cases):
+    _same(_together(cases, 4, mixed=True)[0], _alone(cases, 4, mixed=True))
+
+
+def test_ensemble_rejects_single_domain_entries(cases):
+    e = Ensemble(cases[:2])
+    try:
+        with pytest.raises(hevi.HeviError, match="ensemble"):
+            hevi.ATMOS_DYN_Tinteg_short_rk4_dev(
+                PROG=None, mflx_hi=e.mflx, tflx_hi=e.tflx, DPRES0=e.DPRES0, RT2P=e.RT2P, CORIOLI=e.CORIOLI,
+                num_diff=e.num_diff, wdamp_coef=e.wdamp, divdmp_coef=0.1, DDIV=e.tend["DENS_t"],
+                FLAG_FCT_MOMENTUM=False, FLAG_FCT_T=False, FLAG_FCT_ALONG_STREAM=True, PHI=e.ref["PHI"],
+                GSQRT=e.GSQRT, J13G=e.J0, J23G=e.J0, J33G=1.0, MAPF=e.MAPF, REF_dens=e.ref["REF_dens"],
+                REF_rhot=e.REF_rhot, BND_W=False, BND_E=False, BND_S=False, BND_N=False, dt=1.0, **e.X, **e.tend,
+                **{k: e.grid[k] for k in ("CDZ", "FDZ", "FDX", "FDY", "RCDZ", "RCDX", "RCDY", "RFDZ", "RFDX",
+                                          "RFDY")})
+        with pytest.raises(hevi.HeviError, match="ensemble"):
+            hevi.domain_sum_dev(e.X["DENS"], e.grid["CDZ"], e.grid["CDX"], e.grid["CDY"])
+    finally:
+        e.close()
