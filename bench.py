@@ -173,6 +173,7 @@ def run_b200(args):
     N3 = int(np.prod(g.shape))
     cells = g.cells
     hevi.setup(g.index_dict(), c.scheme, c.scheme_tracer, device=local)
+    hevi.stage_autotune(True)  # the first warm-up step picks the stage tile shape
 
     # device-resident state and inputs (Fortran layout, one flat buffer each)
     st = torch.empty((5, N3), dtype=torch.float64, device="cuda")
@@ -271,6 +272,7 @@ def run_b200(args):
         "mass_drift_rel": abs(m1 - m0) / m0,
         "gpu_launches": launches,
         "clocks": clocks,
+        "autotune": hevi.autotune_report(),
     }
 
     if not args.no_mixed:
@@ -346,11 +348,59 @@ def run_b200(args):
     if rank == 0 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(args)
     hevi.finalize()
+    if world == 1 and not args.no_ensemble:
+        del st, X, mflx, tflx, nd, tend, ref, dp0, rt2p, refr, GS, J0, MAPF, cor
+        torch.cuda.empty_cache()
+        out["ensemble"] = run_ensemble(args, hevi, torch)
     if dist:
         dist.barrier()
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(out), flush=True)
+
+
+def run_ensemble(args, hevi, torch):
+    """The 48-member uneven ensemble (16 each of 64x64x64, 128x128x96 and
+    256x256x96): every kernel of a short step launched once over all members,
+    the step replayed as a CUDA graph, the stage shape autotuned."""
+    from scale_b200 import mkinit
+    from scale_b200.ensemble import Ensemble
+
+    w0 = time.time()
+    cases = mkinit.ensemble(scale=args.ensemble_scale)
+    prep_s = time.time() - w0
+    cells = sum(c.g.cells for c in cases)
+    sizes = {}
+    for c in cases:
+        k = f"{c.g.IMAX}x{c.g.JMAX}x{c.g.KMAX}"
+        sizes[k] = sizes.get(k, 0) + 1
+    e = Ensemble(cases)
+    del cases
+    try:
+        hevi.stage_autotune(True)
+        e.capture(1)  # one eager step (tunes the stage shape), then one recorded step
+        e.run(max(3, args.warmup))
+        hevi.check()
+        stream = torch.cuda.ExternalStream(hevi.stream_handle())
+        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        k = args.ensemble_steps
+        torch.cuda.synchronize()
+        l0 = hevi.kernel_launches()
+        t0.record(stream)
+        e.run(k)
+        t1.record(stream)
+        torch.cuda.synchronize()
+        ms = t0.elapsed_time(t1)
+        launches = hevi.kernel_launches() - l0
+        hevi.check()
+        shape = hevi.stage_shape_get()
+        return {"value": cells * k / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms / k, "steps": k,
+                "members": len(e.shapes), "sizes": sizes, "cells": cells,
+                "kernel_launches_per_step": launches / k, "cuda_graph": True,
+                "stage_shape": {"tile_x": shape[0], "raster": shape[1]}, "autotune": hevi.autotune_report(),
+                "input_prep_s": prep_s, "l2": "inputs larger than L2"}
+    finally:
+        e.close()
 
 
 def read_traffic():
@@ -503,6 +553,9 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision measurement")
+    ap.add_argument("--no-ensemble", action="store_true", help="skip the 48-member ensemble measurement")
+    ap.add_argument("--ensemble-steps", type=int, default=20)
+    ap.add_argument("--ensemble-scale", type=float, default=1.0, help="horizontal scale of the ensemble members")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "b200":
         log("warm-up raised to the minimum of 3 steps")

@@ -354,6 +354,18 @@ int scale_hevi_ensemble_layout(long long *cell0, long long *col0, long long *z0,
  * are identical for every shape.
  * ------------------------------------------------------------------------- */
 int scale_hevi_stage_shape(int tile_x, int raster);
+/* Autotuner of that shape. With enable != 0, the next short-step call of each
+ * path (FP64, mixed precision) outside a graph capture first times every
+ * compiled tile width at raster heights 4, 16 and 64 on its own inputs (a
+ * plain stage per candidate, outputs to library scratch; the caller's arrays
+ * are not written) and keeps the fastest. scale_hevi_stage_shape() replaces
+ * the choice and turns the tuner off. */
+int scale_hevi_stage_autotune(int enable);
+/* The shape in use on the FP64 (mixed = 0) or mixed-precision path. */
+int scale_hevi_stage_shape_get(int *tile_x, int *raster, int mixed);
+/* JSON record of the last tuning: {"path", "chosen": [tile_x, raster, ms],
+ * "candidates": [[tile_x, raster, ms], ...]}; empty before one ran. */
+const char *scale_hevi_autotune_report(void);
 
 /* ---------------------------------------------------------------------------
  * CUDA graph of a call sequence on the library's stream; no counterpart in the

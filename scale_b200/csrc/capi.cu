@@ -32,7 +32,10 @@ struct Ctx {
     std::vector<scale_hevi_index> member_idx;
     size_t N2 = 0;                   // points of one 2-D field (all members)
     int ZT = 0, XT = 0, YT = 0;      // lengths of the pooled z/x/y vectors
-    StageShape shape;                // stage tile shape (autotuned or set)
+    StageShape shape[2];             // stage launch shape, FP64 [0] and mixed [1] path (tuned or set)
+    int autotune = 0;                // tune the shape at the next short-step call (per path)
+    bool tuned[2] = {false, false};
+    std::string tune_text;           // JSON record of the last tuning
     long long launches = 0;
     long long h2d_bytes = 0, d2h_bytes = 0; // host<->device copies of the host-array entries
     // 1-D tables on the device: CDZ FDZ RCDZ RFDZ F2H1 F2H2 wdamp (KA each),
@@ -367,11 +370,8 @@ template <> double *colscr_buf<double>() { return C.colscr; }
 template <> float *colscr_buf<float>() { return C.colscr_f; }
 
 template <typename F>
-int run_stage(const StageInT<F> &in, double *const out[5], F *mflx, F *tflx, double dtrk, int mode)
+StageArgsT<F> stage_args(const StageInT<F> &in, double *const out[5], F *mflx, F *tflx, double dtrk, int mode)
 {
-    if (in.divdmp != 0.0 && !in.DDIV) return fail(SCALE_HEVI_ERR_ARG, "divdmp_coef is nonzero but DDIV is NULL");
-    if (in.divdmp != 0.0 && C.members.size() > 1)
-        return fail(SCALE_HEVI_ERR_UNSUPPORTED, "divergence damping is not available for an ensemble");
     StageArgsT<F> a{};
     a.DENS_RK = out[0]; a.MOMZ_RK = out[1]; a.MOMX_RK = out[2]; a.MOMY_RK = out[3]; a.RHOT_RK = out[4];
     a.mflx = mflx; a.tflx = tflx;
@@ -382,8 +382,75 @@ int run_stage(const StageInT<F> &in, double *const out[5], F *mflx, F *tflx, dou
     a.wdamp = C.d_wdamp; a.DDIV = in.DDIV; a.REF_dens = in.REF_dens; a.REF_rhot = in.REF_rhot;
     a.divdmp_coef = in.divdmp; a.J33G = in.J33G; a.dtrk = dtrk;
     a.rk_mode = mode; a.acc = C.acc; a.facc = facc_buf<F>(); a.status = C.status; a.colscr = colscr_buf<F>();
+    return a;
+}
+
+// Stage-shape autotuner: times every compiled tile width at three raster
+// heights on the caller's own inputs (one plain stage whose outputs go to
+// the library's scratch: the RK buffer, the flux RK sums, the column scratch;
+// nothing the caller holds is written) and keeps the fastest for this path.
+template <typename F>
+int autotune_stage(const StageInT<F> &in, double dtrk)
+{
+    const int p = sizeof(F) == sizeof(double) ? 0 : 1;
+    double *out[5];
+    for (int v = 0; v < 5; ++v) out[v] = C.rk[0] + (size_t)v * C.N3;
+    F *fs = facc_buf<F>();
+    const StageArgsT<F> a = stage_args(in, out, fs, fs + 3 * C.N3, dtrk, RK_PLAIN);
+    cudaEvent_t e0, e1;
+    CU(cudaEventCreate(&e0));
+    CU(cudaEventCreate(&e1));
+    constexpr int RASTERS[3] = {4, 16, 64}, REPS = 3;
+    StageShape best{};
+    float best_ms = 1e30f;
+    std::string rows;
+    int rc = SCALE_HEVI_OK;
+    for (int tx : STAGE_TILE_XS) {
+        for (int r : RASTERS) {
+            const StageShape sh{tx, r};
+            cudaError_t e = launch_hevi_stage(C.g, mem(), a, C.scheme, sh, C.stream); // warm-up
+            cudaEventRecord(e0, C.stream);
+            for (int q = 0; q < REPS && e == cudaSuccess; ++q) e = launch_hevi_stage(C.g, mem(), a, C.scheme, sh, C.stream);
+            cudaEventRecord(e1, C.stream);
+            if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+            float ms = 0.f;
+            if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+            if (e != cudaSuccess) {
+                rc = fail(SCALE_HEVI_ERR_CUDA, "stage autotune (tile %d, raster %d): %s", tx, r, cudaGetErrorString(e));
+                break;
+            }
+            ms /= REPS;
+            C.launches += 1 + REPS;
+            char buf[96];
+            snprintf(buf, sizeof buf, "%s[%d, %d, %.4f]", rows.empty() ? "" : ", ", tx, r, ms);
+            rows += buf;
+            if (ms < best_ms) { best_ms = ms; best = sh; }
+        }
+        if (rc != SCALE_HEVI_OK) break;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc != SCALE_HEVI_OK) return rc;
+    C.shape[p] = best;
+    C.tuned[p] = true;
+    char head[160];
+    snprintf(head, sizeof head, "{\"path\": \"%s\", \"chosen\": [%d, %d, %.4f], \"candidates\": [",
+             p ? "mixed" : "fp64", best.tile_x, best.raster, best_ms);
+    C.tune_text = std::string(head) + rows + "]}";
+    return SCALE_HEVI_OK;
+}
+
+template <typename F>
+int run_stage(const StageInT<F> &in, double *const out[5], F *mflx, F *tflx, double dtrk, int mode)
+{
+    if (in.divdmp != 0.0 && !in.DDIV) return fail(SCALE_HEVI_ERR_ARG, "divdmp_coef is nonzero but DDIV is NULL");
+    if (in.divdmp != 0.0 && C.members.size() > 1)
+        return fail(SCALE_HEVI_ERR_UNSUPPORTED, "divergence damping is not available for an ensemble");
+    const int p = sizeof(F) == sizeof(double) ? 0 : 1;
+    if (C.autotune && !C.tuned[p] && !C.capturing) CK(autotune_stage(in, dtrk));
+    const StageArgsT<F> a = stage_args(in, out, mflx, tflx, dtrk, mode);
     CK(timed(sizeof(F) == sizeof(double) ? "hevi_stage" : "hevi_stage_mixed", [&] {
-        CU(launch_hevi_stage(C.g, mem(), a, C.scheme, C.shape, C.stream));
+        CU(launch_hevi_stage(C.g, mem(), a, C.scheme, C.shape[p], C.stream));
         return SCALE_HEVI_OK;
     }));
     ++C.launches;
@@ -602,8 +669,26 @@ int scale_hevi_stage_shape(int tile_x, int raster)
     bool ok = tile_x == 0;
     for (int t : STAGE_TILE_XS) ok |= tile_x == t;
     if (!ok || raster < 0) return fail(SCALE_HEVI_ERR_ARG, "tile width %d / raster %d is not a compiled shape", tile_x, raster);
-    C.shape.tile_x = tile_x;
-    C.shape.raster = raster;
+    C.shape[0] = C.shape[1] = StageShape{tile_x, raster};
+    C.autotune = 0;
+    return SCALE_HEVI_OK;
+}
+
+int scale_hevi_stage_autotune(int enable)
+{
+    CK(need_setup());
+    C.autotune = enable != 0;
+    C.tuned[0] = C.tuned[1] = false;
+    C.tune_text.clear();
+    return SCALE_HEVI_OK;
+}
+
+int scale_hevi_stage_shape_get(int *tile_x, int *raster, int mixed)
+{
+    CK(need_setup());
+    const StageShape &s = C.shape[mixed ? 1 : 0];
+    if (tile_x) *tile_x = s.tile_x > 0 ? s.tile_x : STAGE_TILE_X_DEFAULT;
+    if (raster) *raster = s.raster > 0 ? s.raster : STAGE_RASTER_DEFAULT;
     return SCALE_HEVI_OK;
 }
 
@@ -1122,6 +1207,8 @@ int scale_hevi_replay(const int *n)
     }
     return SCALE_HEVI_OK;
 }
+
+const char *scale_hevi_autotune_report(void) { return C.tune_text.c_str(); }
 
 int scale_hevi_profile(int enable)
 {

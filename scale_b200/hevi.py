@@ -80,7 +80,7 @@ def load(path: str | os.PathLike | None = None) -> C.CDLL:
     _sig = header_functions()
     for name, params in _sig.items():
         f = getattr(lib, name)
-        if name in ("scale_hevi_last_error", "scale_hevi_profile_report"):
+        if name in ("scale_hevi_last_error", "scale_hevi_profile_report", "scale_hevi_autotune_report"):
             f.restype = C.c_char_p
         elif name == "scale_hevi_stream":
             f.restype = C.c_void_p
@@ -94,6 +94,10 @@ def load(path: str | os.PathLike | None = None) -> C.CDLL:
             f.argtypes = [C.c_int, C.POINTER(Index), C.c_char_p, C.c_char_p, C.c_int]
         elif name == "scale_hevi_stage_shape":
             f.argtypes = [C.c_int, C.c_int]
+        elif name == "scale_hevi_stage_autotune":
+            f.argtypes = [C.c_int]
+        elif name == "scale_hevi_stage_shape_get":
+            f.argtypes = [C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_int]
         elif name == "scale_hevi_profile":
             f.argtypes = [C.c_int]
         elif name in ("scale_hevi_capture_begin", "scale_hevi_capture_end"):
@@ -217,6 +221,24 @@ def unpool(pooled: np.ndarray, offsets: np.ndarray, shapes: list[tuple], ncomp: 
 def stage_shape(tile_x: int = 0, raster: int = 0) -> None:
     """Tile width and raster height of the stage kernel (0: defaults)."""
     _check(load().scale_hevi_stage_shape(int(tile_x), int(raster)))
+
+
+def stage_autotune(enable: bool = True) -> None:
+    """Tune the stage shape at the next short-step call of each path."""
+    _check(load().scale_hevi_stage_autotune(int(bool(enable))))
+
+
+def stage_shape_get(mixed: bool = False) -> tuple[int, int]:
+    tx, r = C.c_int(), C.c_int()
+    _check(load().scale_hevi_stage_shape_get(C.byref(tx), C.byref(r), int(bool(mixed))))
+    return tx.value, r.value
+
+
+def autotune_report() -> dict:
+    import json
+
+    t = load().scale_hevi_autotune_report().decode()
+    return json.loads(t) if t else {}
 
 
 def finalize() -> None:

@@ -104,3 +104,19 @@ def test_ensemble_rejects_single_domain_entries(cases):
             hevi.domain_sum_dev(e.X["DENS"], e.grid["CDZ"], e.grid["CDX"], e.grid["CDY"])
     finally:
         e.close()
+
+
+def test_autotuned_shape_gives_identical_results(cases, alone):
+    e = Ensemble(cases)
+    try:
+        hevi.stage_autotune(True)
+        e.run(NSTEPS)
+        got = e.members()
+        rep = hevi.autotune_report()
+        tx, r = hevi.stage_shape_get()
+    finally:
+        e.close()
+    _same(got, alone)
+    assert rep["path"] == "fp64" and len(rep["candidates"]) == 9
+    assert [tx, r] == rep["chosen"][:2]
+    assert min(c[2] for c in rep["candidates"]) == rep["chosen"][2]
