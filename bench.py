@@ -352,6 +352,8 @@ def run_b200(args):
         del st, X, mflx, tflx, nd, tend, ref, dp0, rt2p, refr, GS, J0, MAPF, cor
         torch.cuda.empty_cache()
         out["ensemble"] = run_ensemble(args, hevi, torch)
+    if world == 1 and not args.no_adjoint:
+        out["adjoint"] = run_adjoint(args, hevi, torch)
     if dist:
         dist.barrier()
         dist.destroy_process_group()
@@ -401,6 +403,66 @@ def run_ensemble(args, hevi, torch):
                 "input_prep_s": prep_s, "l2": "inputs larger than L2"}
     finally:
         e.close()
+
+
+def run_adjoint(args, hevi, torch):
+    """Gradient of the warm-bubble cost (128x128x64, UD3): J = 1/2 sum of
+    (theta - theta_base)^2 vol over x, y in [20, 44] km, z in [2, 6] km after
+    120 short steps, with respect to the initial theta, MOMX and MOMY, by the
+    adjoint with a checkpoint every 10 steps; checked against central finite
+    differences (eps = 1e-6) along 8 seeded directions and by the
+    tangent-linear dot-product test. The differentiated window starts after
+    10 short steps of spin-up from rest (at rest every face velocity is
+    exactly zero, where the UD3 upwind switches have no derivative)."""
+    from scale_b200 import adjoint, mkinit
+
+    out = {}
+    for scheme in ("UD3", "CD4"):
+        c = mkinit.config(5)
+        c.scheme = scheme
+        hevi.setup(c.g.index_dict(), c.scheme, c.scheme_tracer)
+        try:
+            p = adjoint.Problem(c, nsteps=args.adjoint_steps, K=10, spinup=10)
+            torch.cuda.synchronize()
+            w0 = time.time()
+            J, _ = p.value_and_grad()
+            torch.cuda.synchronize()
+            t_grad = time.time() - w0
+            X = p.model.state()
+            p.model.boundary(X)
+            t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            lam = torch.ones_like(X)
+            p.model.adjoint(X, lam)  # warm
+            t0.record()
+            for _ in range(5):
+                p.model.adjoint(X, lam)
+            t1.record()
+            torch.cuda.synchronize()
+            ms_adj = t0.elapsed_time(t1) / 5
+            t0.record()
+            for _ in range(5):
+                p.model.step(X)
+            t1.record()
+            torch.cuda.synchronize()
+            ms_fwd = t0.elapsed_time(t1) / 5
+            hevi.check()
+            eps_list = (1e-6, 1e-5, 1e-4)
+            r = adjoint.gradient_check(p, ndirs=8, eps=eps_list)
+            X = p.model.state()
+            p.model.boundary(X)
+            dp = adjoint.dot_product_test(p.model, X, 3)
+            fd = {}
+            for e in eps_list:
+                errs = sorted(d[f"rel_err_{e:g}"] for d in r["directions"])
+                fd[f"{e:g}"] = {"max": errs[-1], "median": errs[len(errs) // 2]}
+            out[scheme] = {"J": J, "gradient_s": t_grad, "steps": args.adjoint_steps, "checkpoint_every": 10,
+                           "ms_per_adjoint_step": ms_adj, "ms_per_forward_step": ms_fwd,
+                           "fd_rel_err_by_eps": fd, "directions": len(r["directions"]),
+                           "dot_product_rel_diff": dp["rel_diff"]}
+        finally:
+            hevi.finalize()
+    out["workload"] = "warm bubble 128x128x64, dx=500 m, dt=1 s; J over x,y in [20,44] km, z in [2,6] km"
+    return out
 
 
 def read_traffic():
@@ -556,6 +618,8 @@ def main():
     ap.add_argument("--no-ensemble", action="store_true", help="skip the 48-member ensemble measurement")
     ap.add_argument("--ensemble-steps", type=int, default=20)
     ap.add_argument("--ensemble-scale", type=float, default=1.0, help="horizontal scale of the ensemble members")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint gradient measurement")
+    ap.add_argument("--adjoint-steps", type=int, default=120)
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "b200":
         log("warm-up raised to the minimum of 3 steps")

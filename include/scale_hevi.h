@@ -71,7 +71,10 @@ int scale_hevi_setup(const scale_hevi_index *idx, const char *flux_type, const c
 int scale_hevi_finalize(void);
 /* Text of the last error (empty when none). */
 const char *scale_hevi_last_error(void);
-/* The cudaStream_t the _dev entries enqueue on (as void*). */
+/* The cudaStream_t the _dev entries enqueue on (as void*). It is a blocking
+ * stream: work on the legacy default stream is ordered with it both ways, so
+ * arrays produced or consumed there need no further synchronisation; a caller
+ * on another stream orders its work with events. */
 void *scale_hevi_stream(void);
 /* Waits for the stream and returns SCALE_HEVI_ERR_NONFINITE if any kernel
  * since the last check saw a non-finite prognostic value (the device-side
@@ -366,6 +369,42 @@ int scale_hevi_stage_shape_get(int *tile_x, int *raster, int mixed);
 /* JSON record of the last tuning: {"path", "chosen": [tile_x, raster, ms],
  * "candidates": [[tile_x, raster, ms], ...]}; empty before one ran. */
 const char *scale_hevi_autotune_report(void);
+
+/* ---------------------------------------------------------------------------
+ * Differentiated short step; no counterpart in the reference. The model is one
+ * short step of a single flat-terrain domain as ATMOS_DYN_Tstep_large_fvm_heve
+ * runs it (scale_atmos_dyn_tstep_large_fvm_heve.F90:847-944): the numerical
+ * filter (ND_ORDER = 1) of the step's start state, the RK4 short integrator of
+ * four HEVI stages without divergence damping, then the vertical boundary
+ * values and the periodic halo. The large-step quantities (DPRES0, RT2P,
+ * REF_rhot) and the base state are fixed parameters and the tendencies are
+ * zero. A state X is one device buffer of 5*KA*IA*JA doubles: DENS, MOMZ,
+ * MOMX, MOMY, RHOT.
+ *   scale_hevi_adjoint_setup      parameters (device arrays, kept by pointer;
+ *                                 1-D vectors and scalars on the host, copied)
+ *   scale_hevi_short_step_dev     forward: X advanced one step (the fused kernels)
+ *   scale_hevi_short_step_passes_dev
+ *                                 the same step through the pass form the
+ *                                 tangent-linear and adjoint linearise
+ *   scale_hevi_short_step_tlm_dev X and its tangent dX advanced one step
+ *   scale_hevi_short_step_adjoint_dev
+ *                                 lam, the adjoint of the state after a step
+ *                                 from X, replaced by the adjoint of X
+ *   scale_hevi_boundary_adjoint_dev
+ *                                 adjoint of scale_hevi_boundary_dev (on the
+ *                                 5 fields of lam)
+ * ------------------------------------------------------------------------- */
+int scale_hevi_adjoint_setup(const double *DPRES0, const double *RT2P, const double *REF_rhot, const double *REF_dens,
+                             const double *REF_pott, const double *PHI, const double *CORIOLI, const double *CDZ,
+                             const double *CDX, const double *CDY, const double *FDZ, const double *FDX,
+                             const double *FDY, const double *RCDZ, const double *RCDX, const double *RCDY,
+                             const double *RFDZ, const double *RFDX, const double *RFDY, const double *wdamp_coef,
+                             const double *dt, const double *ND_COEF, const double *ND_SFC_FACT, const double *J33G);
+int scale_hevi_short_step_dev(double *X);
+int scale_hevi_short_step_passes_dev(double *X);
+int scale_hevi_short_step_tlm_dev(double *X, double *dX);
+int scale_hevi_short_step_adjoint_dev(const double *X, double *lam);
+int scale_hevi_boundary_adjoint_dev(double *lam);
 
 /* ---------------------------------------------------------------------------
  * CUDA graph of a call sequence on the library's stream; no counterpart in the

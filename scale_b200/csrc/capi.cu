@@ -11,6 +11,7 @@
 #include <vector>
 
 #include "../../include/scale_hevi.h"
+#include "adjoint.cuh"
 #include "grid_coef.h"
 #include "hevi_kernels.cuh"
 
@@ -76,6 +77,13 @@ struct Ctx {
     cudaGraphExec_t graph_exec = nullptr;
     bool capturing = false;
     long long capture_from = 0, graph_launches = 0; // kernel launches recorded in the graph
+    // differentiated short step (scale_hevi_adjoint_setup)
+    bool ad_ready = false;
+    ad::Model adm{};
+    double *ad_scratch = nullptr, *ad_zero = nullptr, *ad_nd = nullptr, *ad_flx = nullptr;
+    std::vector<double> ad_vec[12]; // CDZ CDX CDY FDZ FDX FDY RCDZ RCDX RCDY RFDZ RFDX RFDY
+    std::vector<double> ad_wdamp;
+    double ad_ndcoef = 0.0, ad_sfc = 1.0;
 };
 
 Ctx C;
@@ -167,6 +175,7 @@ void free_all()
     for (double *b : bufs) if (b) cudaFree(b);
     for (auto &kv : C.stage) cudaFree(kv.second.first);
     for (float *b : {C.facc_f, C.colscr_f, C.phi_f}) if (b) cudaFree(b);
+    for (double *b : {C.ad_scratch, C.ad_zero, C.ad_nd, C.ad_flx}) if (b) cudaFree(b);
     if (C.status) cudaFree(C.status);
     if (C.count) cudaFree(C.count);
     for (cudaEvent_t e : C.ev_pool) cudaEventDestroy(e);
@@ -621,7 +630,10 @@ int scale_hevi_ensemble_setup(int n, const scale_hevi_index *idx, const char *fl
     C.N3 = N3;
     C.N2 = N2;
     C.ZT = (int)ZT; C.XT = (int)XT; C.YT = (int)YT;
-    CU(cudaStreamCreateWithFlags(&C.stream, cudaStreamNonBlocking));
+    // a blocking stream: its work is ordered with the legacy default stream,
+    // on which callers such as torch enqueue the producers and consumers of
+    // the device arrays handed to the _dev entries
+    CU(cudaStreamCreate(&C.stream));
     int rc = SCALE_HEVI_OK;
     if ((rc = dalloc(&C.d_tab, 7 * (size_t)ZT + 4 * (size_t)XT + 4 * (size_t)YT)) ||
         (rc = dalloc(&C.d_nd, 8 * (size_t)ZT + 8 * (size_t)XT + 8 * (size_t)YT)) ||
@@ -718,6 +730,7 @@ int scale_hevi_check(void)
     CU(cudaStreamSynchronize(C.stream));
     CU(cudaMemsetAsync(C.status, 0, sizeof(unsigned), C.stream));
     if (st & ST_NONFINITE) return fail(SCALE_HEVI_ERR_NONFINITE, "a prognostic output became NaN or Inf");
+    if (st & (1u << 4)) return fail(SCALE_HEVI_ERR_CUDA, "an adjoint pass loaded more inputs than its derivative slots");
     return SCALE_HEVI_OK;
 }
 
@@ -1157,6 +1170,110 @@ int scale_hevi_boundary_dev(double *DENS, double *MOMZ, double *MOMX, double *MO
     ++C.launches;
     double *X[5] = {DENS, MOMZ, MOMX, MOMY, RHOT};
     return halo(X, 5);
+}
+
+// ---- the differentiated short step ------------------------------------------------
+int scale_hevi_adjoint_setup(const double *DPRES0, const double *RT2P, const double *REF_rhot, const double *REF_dens,
+                             const double *REF_pott, const double *PHI, const double *CORIOLI, const double *CDZ,
+                             const double *CDX, const double *CDY, const double *FDZ, const double *FDX,
+                             const double *FDY, const double *RCDZ, const double *RCDX, const double *RCDY,
+                             const double *RFDZ, const double *RFDX, const double *RFDY, const double *wdamp_coef,
+                             const double *dt, const double *ND_COEF, const double *ND_SFC_FACT, const double *J33G)
+{
+    CK(need_single("the differentiated short step"));
+    const double *v[12] = {CDZ, CDX, CDY, FDZ, FDX, FDY, RCDZ, RCDX, RCDY, RFDZ, RFDX, RFDY};
+    const int len[12] = {C.g.KA, C.g.IA, C.g.JA, C.g.KA - 1, C.g.IA - 1, C.g.JA - 1,
+                         C.g.KA, C.g.IA, C.g.JA, C.g.KA - 1, C.g.IA - 1, C.g.JA - 1};
+    for (int q = 0; q < 12; ++q) {
+        if (!v[q]) return fail(SCALE_HEVI_ERR_ARG, "a 1-D grid vector is NULL");
+        C.ad_vec[q].assign(v[q], v[q] + len[q]);
+    }
+    if (!DPRES0 || !RT2P || !REF_rhot || !REF_dens || !REF_pott || !PHI || !CORIOLI || !dt || !ND_COEF || !ND_SFC_FACT || !J33G)
+        return fail(SCALE_HEVI_ERR_ARG, "an argument of the differentiated short step is NULL");
+    C.ad_wdamp.assign((size_t)C.g.KA, 0.0);
+    if (wdamp_coef) C.ad_wdamp.assign(wdamp_coef, wdamp_coef + C.g.KA);
+    C.ad_ndcoef = *ND_COEF;
+    C.ad_sfc = *ND_SFC_FACT;
+    const size_t N3 = C.N3;
+    if (!C.ad_scratch) {
+        CK(dalloc(&C.ad_scratch, ad::scratch_fields() * N3));
+        CK(dalloc(&C.ad_zero, N3));
+        CK(dalloc(&C.ad_nd, 15 * N3));
+        CK(dalloc(&C.ad_flx, 6 * N3));
+        CU(cudaMemsetAsync(C.ad_scratch, 0, ad::scratch_fields() * N3 * sizeof(double), C.stream));
+        CU(cudaMemsetAsync(C.ad_zero, 0, N3 * sizeof(double), C.stream));
+        CU(cudaMemsetAsync(C.ad_nd, 0, 15 * N3 * sizeof(double), C.stream));
+    }
+    ad::Model &M = C.adm;
+    M.dt = *dt;
+    M.J33G = *J33G;
+    M.status = C.status;
+    M.DPRES0 = DPRES0; M.RT2P = RT2P; M.REF_rhot = REF_rhot; M.REF_dens = REF_dens; M.REF_pott = REF_pott;
+    M.PHI = PHI; M.CORIOLI = CORIOLI; M.zero = C.ad_zero; M.scratch = C.ad_scratch;
+    M.scheme = C.scheme;
+    M.stream = C.stream;
+    C.ad_ready = true;
+    return SCALE_HEVI_OK;
+}
+
+// tables of the differentiated model (cached: no transfer unless they changed)
+static int ad_prepare()
+{
+    CK(need_single("the differentiated short step"));
+    if (!C.ad_ready) return fail(SCALE_HEVI_ERR_NOT_SETUP, "scale_hevi_adjoint_setup() has not been called");
+    const auto &v = C.ad_vec;
+    CK(prepare_tables(v[0].data(), v[3].data(), v[6].data(), v[9].data(), v[4].data(), v[7].data(), v[10].data(),
+                      v[5].data(), v[8].data(), v[11].data(), C.ad_wdamp.data(), nullptr, nullptr));
+    CK(prepare_nd(v[0].data(), v[1].data(), v[2].data(), v[3].data(), v[4].data(), v[5].data(), C.adm.dt, C.ad_ndcoef, 1,
+                  C.ad_sfc));
+    C.adm.g = C.g;
+    C.adm.nd = C.ndc;
+    C.adm.wdamp = C.d_wdamp;
+    return SCALE_HEVI_OK;
+}
+
+int scale_hevi_short_step_dev(double *X)
+{
+    CK(ad_prepare());
+    const size_t N3 = C.N3;
+    double *Xv[5] = {X, X + N3, X + 2 * N3, X + 3 * N3, X + 4 * N3};
+    const ad::Model &M = C.adm;
+    CK(run_numfilter<double>(C.ad_nd, Xv[0], Xv[1], Xv[2], Xv[3], Xv[4], M.REF_dens, M.REF_pott));
+    StageIn base{nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
+                 M.zero, M.zero, M.zero, M.zero, M.zero, M.DPRES0, M.RT2P, M.CORIOLI, C.ad_nd, nullptr, M.REF_dens,
+                 M.REF_rhot, 0.0, M.J33G};
+    CK(run_rk4(Xv, C.ad_flx, C.ad_flx + 3 * N3, base, M.dt));
+    return scale_hevi_boundary_dev(Xv[0], Xv[1], Xv[2], Xv[3], Xv[4]);
+}
+
+int scale_hevi_short_step_passes_dev(double *X)
+{
+    CK(ad_prepare());
+    CU(ad::step_forward(C.adm, X));
+    return SCALE_HEVI_OK;
+}
+
+int scale_hevi_short_step_tlm_dev(double *X, double *dX)
+{
+    CK(ad_prepare());
+    if (!X || !dX) return fail(SCALE_HEVI_ERR_ARG, "X or dX is NULL");
+    CU(ad::step_tlm(C.adm, X, dX));
+    return SCALE_HEVI_OK;
+}
+
+int scale_hevi_short_step_adjoint_dev(const double *X, double *lam)
+{
+    CK(ad_prepare());
+    if (!X || !lam) return fail(SCALE_HEVI_ERR_ARG, "X or lam is NULL");
+    CU(ad::step_adjoint(C.adm, X, lam));
+    return SCALE_HEVI_OK;
+}
+
+int scale_hevi_boundary_adjoint_dev(double *lam)
+{
+    CK(ad_prepare());
+    CU(ad::boundary_adjoint(C.adm, lam));
+    return SCALE_HEVI_OK;
 }
 
 int scale_hevi_capture_begin(void)
