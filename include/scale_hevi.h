@@ -65,7 +65,9 @@ typedef struct scale_hevi_index {
  * HEVI short step (ATMOS_DYN_Tstep_short_fvm_hevi_setup,
  * scale_atmos_dyn_tstep_short_fvm_hevi.F90:118). flux_type and
  * flux_tracer_type are the ATMOS_DYN_FVM_FLUX_TYPE / _TRACER_TYPE names
- * ("UD3", "CD4"). device is the CUDA ordinal to use. */
+ * ("UD3", "CD4"; the tracer scheme may also be "UD3KOREN1993",
+ * scale_atmos_dyn_fvm_flux_ud3Koren1993.F90:163-373, the reference's default
+ * tracer flux). device is the CUDA ordinal to use. */
 int scale_hevi_setup(const scale_hevi_index *idx, const char *flux_type, const char *flux_tracer_type, int device);
 /* Frees every device buffer and the stream. */
 int scale_hevi_finalize(void);

@@ -15,8 +15,9 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 LIB = HERE / "build" / "liboracle.so"
-UD3, CD4 = 1, 2
-SCHEMES = {"UD3": UD3, "CD4": CD4}
+UD3, CD4, KOREN = 1, 2, 3
+# "UD3KOREN1993" is a tracer scheme only
+SCHEMES = {"UD3": UD3, "CD4": CD4, "UD3KOREN1993": KOREN}
 
 
 class Dims(C.Structure):

@@ -70,6 +70,24 @@ static inline double og_ipH(int scheme, double vel, double vE, double vE1, doubl
     return F2_ * (vE + vE1);
 }
 
+/* Koren (1993) limiter of the UD3KOREN1993 tracer flux,
+ * scale_atmos_dyn_fvm_flux_ud3Koren1993.F90:1690-1710 */
+static inline double og_koren_phi(double v1, double v2, double v3)
+{
+    const double EPS = OG_EPS;
+    const double zerosw1 = EPS - og_sign(EPS, fabs(v1 - v2) - EPS);
+    const double zerosw2 = EPS - og_sign(EPS, fabs(v2 - v3) - EPS);
+    const double r2 = 2.0 * (v1 - v2 + zerosw1 * zerosw2) / (v2 - v3 + zerosw2);
+    return og_max(0.0, og_min(r2, og_min((1.0 + r2) / 3.0, 2.0)));
+}
+/* limited face value with the upwind switch: vm1 v0 | vp1 vp2, the face
+ * between v0 and vp1 (ud3Koren1993.F90:200-206, 298-305, 355-362) */
+static inline double og_koren_face(double vel, double vm1, double v0, double vp1, double vp2)
+{
+    return (v0 + 0.5 * og_koren_phi(vp1, v0, vm1) * (v0 - vm1)) * (0.5 + og_sign(0.5, vel))
+           + (vp1 + 0.5 * og_koren_phi(v0, vp1, vp2) * (vp1 - vp2)) * (0.5 - og_sign(0.5, vel));
+}
+
 /* ---- flux family (19 routines), one generic restatement per reference routine ---- */
 typedef struct {
     int IIS, IIE, JJS, JJE;

@@ -20,7 +20,7 @@
 namespace hevi {
 
 // flux schemes (ATMOS_DYN_FVM_FLUX_TYPE names)
-enum Scheme : int { UD3 = 1, CD4 = 2 };
+enum Scheme : int { UD3 = 1, CD4 = 2, KOREN = 3 }; // KOREN: UD3KOREN1993, tracer fluxes only
 
 struct Grid {
     int KA, IA, JA;
@@ -150,6 +150,32 @@ __device__ __forceinline__ R ipH(R vel, R vE, R vE1, R vE2)
                + R(0.5) * (vE + vE1) * (R(0.5) - fsign(R(0.5), vel));
     else
         return R(0.5) * (vE + vE1);
+}
+
+// ---- UD3KOREN1993 tracer flux (scale_atmos_dyn_fvm_flux_ud3Koren1993.F90) ----
+// the Koren (1993) limiter phi (:1690-1710)
+__device__ __forceinline__ double koren_phi(double v1, double v2, double v3)
+{
+    const double zerosw1 = EPS - fsign(EPS, fabs(v1 - v2) - EPS);
+    const double zerosw2 = EPS - fsign(EPS, fabs(v2 - v3) - EPS);
+    const double r2 = 2.0 * (v1 - v2 + zerosw1 * zerosw2) / (v2 - v3 + zerosw2);
+    return fmax2(0.0, fmin2(r2, fmin2((1.0 + r2) / 3.0, 2.0)));
+}
+// limited value at the face between v0 and vp1 with the upwind switch
+// (:200-206 for z, :298-305 for x, :355-362 for y)
+__device__ __forceinline__ double koren_face(double vel, double vm1, double v0, double vp1, double vp2)
+{
+    return (v0 + 0.5 * koren_phi(vp1, v0, vm1) * (v0 - vm1)) * (0.5 + fsign(0.5, vel))
+           + (vp1 + 0.5 * koren_phi(v0, vp1, vp2) * (vp1 - vp2)) * (0.5 - fsign(0.5, vel));
+}
+// the one-sided faces above KS (:236-241) and below KE (:243-249)
+__device__ __forceinline__ double koren_face_KS(double vel, double q0, double q1, double q2)
+{
+    return q0 * (0.5 + fsign(0.5, vel)) + (q1 + 0.5 * koren_phi(q0, q1, q2) * (q1 - q2)) * (0.5 - fsign(0.5, vel));
+}
+__device__ __forceinline__ double koren_face_KE(double vel, double e2, double e1, double e0)
+{
+    return (e1 + 0.5 * koren_phi(e2, e1, e0) * (e1 - e0)) * (0.5 + fsign(0.5, vel)) + e0 * (0.5 - fsign(0.5, vel));
 }
 
 // read-only load through the non-coherent cache

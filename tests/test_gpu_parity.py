@@ -134,7 +134,7 @@ def _tracer_inputs(g, c, seed=5):
     return q0, q, dens0, dens, mflx, rhoq, GS, np.asfortranarray(MAPF[..., 0])
 
 
-@pytest.mark.parametrize("scheme", ["UD3", "CD4"])
+@pytest.mark.parametrize("scheme", ["UD3", "CD4", "UD3KOREN1993"])
 @pytest.mark.parametrize("fct,along", [(False, True), (True, True), (True, False)])
 def test_tracer_step_bit_exact(lib, scheme, fct, along):
     g = helpers.small_grid(IMAX=12, JMAX=14, KMAX=16)
@@ -144,7 +144,7 @@ def test_tracer_step_bit_exact(lib, scheme, fct, along):
     ref = np.full(g.shape, np.nan, order="F")
     oracle.tstep_tracer(g, scheme, ref, q, q0, rhoq, d0, d, mflx, g.zeros(3), GS, MAPF, 2.5, fct, along)
     got = np.full(g.shape, np.nan, order="F")
-    lib.setup(g.index_dict(), scheme, scheme)
+    lib.setup(g.index_dict(), "UD3" if scheme == "UD3KOREN1993" else scheme, scheme)
     lib.ATMOS_DYN_Tstep_tracer_fvm_heve(QTRCo=got, QTRC=q, QTRC0=q0, RHOQ_t=rhoq, DENS0=d0, DENS=d, mflx_hi=mflx,
                                         num_diff=g.zeros(3), GSQRT=GS, MAPF=MAPF, CDZ=g.CDZ, RCDZ=g.RCDZ,
                                         RCDX=g.RCDX, RCDY=g.RCDY, dtl=2.5, FLAG_FCT_TRACER=fct,
@@ -152,16 +152,17 @@ def test_tracer_step_bit_exact(lib, scheme, fct, along):
     assert helpers.same(got, ref), f"max rel diff {helpers.max_rel(got, ref):.3e}"
 
 
+@pytest.mark.parametrize("tscheme", ["UD3", "UD3KOREN1993"])
 @pytest.mark.parametrize("fct", [False, True])
-def test_tracer_rk3_bit_exact(lib, fct):
+def test_tracer_rk3_bit_exact(lib, fct, tscheme):
     g = helpers.small_grid(IMAX=10, JMAX=12, KMAX=18, stretched=True)
     c = helpers.small_case(g)
     helpers.perturb_state(c)
     q0, q, d0, d, mflx, rhoq, GS, MAPF = _tracer_inputs(g, c)
     ref = q0.copy(order="F")
-    oracle.tinteg_tracer_rk3(g, "UD3", ref, ref, rhoq, d0, d, mflx, g.zeros(3), GS, MAPF, 5.0, fct, True)
+    oracle.tinteg_tracer_rk3(g, tscheme, ref, ref, rhoq, d0, d, mflx, g.zeros(3), GS, MAPF, 5.0, fct, True)
     got = q0.copy(order="F")
-    lib.setup(g.index_dict(), "UD3", "UD3")
+    lib.setup(g.index_dict(), "UD3", tscheme)
     lib.ATMOS_DYN_Tinteg_tracer_rk3(QTRC=got, QTRC0=got, RHOQ_t=rhoq, DENS0=d0, DENS=d, mflx_hi=mflx,
                                     num_diff=g.zeros(3), GSQRT=GS, MAPF=MAPF, CDZ=g.CDZ, RCDZ=g.RCDZ, RCDX=g.RCDX,
                                     RCDY=g.RCDY, BND_W=False, BND_E=False, BND_S=False, BND_N=False, dtl=5.0,

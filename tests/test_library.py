@@ -78,3 +78,13 @@ def test_fortran_blank_padded_scheme_names_are_accepted():
     with pytest.raises(hevi.HeviError) as e:
         hevi.setup(_index(), flux_type="CD4     ", flux_tracer_type="UD3 ")
     assert e.value.code == 3
+
+
+def test_koren_only_as_tracer_scheme():
+    """UD3KOREN1993 is accepted as the tracer flux scheme and rejected, before
+    any device work, as the dynamics flux scheme."""
+    from scale_b200 import hevi, mkinit
+
+    g = mkinit.uniform_grid(8, 8, 8, 500.0, 500.0, 250.0)
+    with pytest.raises(hevi.HeviError, match="tracer flux scheme only"):
+        hevi.setup(g.index_dict(), "UD3KOREN1993", "UD3")

@@ -217,3 +217,54 @@ def test_rk4_equals_four_stages():
         exp = (fl[0][f] + fl[1][f] * 2.0 + fl[2][f] * 2.0 + fl[3][f]) / 6.0
         got = x["mflx_hi" if f == 0 else "tflx_hi"]
         assert np.array_equal(got[sl], exp[sl])
+
+
+@pytest.mark.parametrize("fct", [False, True])
+def test_koren_tracer_keeps_uniform_tracer(fct):
+    """test_cwc with the UD3KOREN1993 tracer flux (the reference's default
+    tracer scheme): a uniform tracer stays uniform under random momenta."""
+    g = helpers.small_grid(10, 10, 14)
+    c = mkinit.make_case("cwc koren", g, "UD3", "UD3KOREN1993", tracers=1, fct=fct)
+    rng = np.random.Generator(np.random.PCG64(5))
+    st = c.state
+    st["DENS"][...] = c.ref["REF_dens"] * (1.0 + 1e-3 * rng.uniform(-1, 1, size=g.shape))
+    st["MOMZ"][...] = rng.uniform(-1, 1, size=g.shape)
+    st["MOMX"][...] = rng.uniform(-3, 3, size=g.shape)
+    st["MOMY"][...] = rng.uniform(-3, 3, size=g.shape)
+    st["RHOT"][...] = st["DENS"] * 300.0
+    st["QTRC"][...] = 0.01
+    for n in STATE:
+        mkinit.periodic_fill(st[n], g)
+    mkinit.vertical_fill(st, g)
+    c.ref["REF_pott"][...] = 300.0
+    _large(c)
+    q = _interior(st["QTRC"][..., 0], g)
+    assert np.max(np.abs(q - 0.01)) / 0.01 < 1e-12
+
+
+def _step_advection(scheme, g, cfl=0.2):
+    """One tracer stage of a step function in x under a uniform x mass flux."""
+    q = g.zeros()
+    x = np.arange(g.IA)
+    q[:, (x >= g.IS - 1 + g.IMAX // 4) & (x < g.IS - 1 + g.IMAX // 2), :] = 1.0
+    mkinit.periodic_fill(q, g)
+    d = np.asfortranarray(np.ones(g.shape))
+    mflx = g.zeros(3)
+    mflx[..., 1] = 1.0
+    dtl = cfl * g.DX
+    GS, _, _, MAPF = oracle.flat_metrics(g)
+    out = np.full(g.shape, np.nan, order="F")
+    oracle.tstep_tracer(g, scheme, out, q, q, g.zeros(), d, d, mflx, g.zeros(3), GS, np.asfortranarray(MAPF[..., 0]),
+                        dtl, False, True)
+    return _interior(out, g)
+
+
+def test_koren_limiter_keeps_step_bounded():
+    """The Koren (1993) limiter is total-variation diminishing: advecting a
+    step function with UD3KOREN1993 (no FCT) creates no new extrema, while the
+    unlimited UD3 flux over- and undershoots."""
+    g = helpers.small_grid(32, 4, 6)
+    qk = _step_advection("UD3KOREN1993", g)
+    assert qk.min() >= -1e-15 and qk.max() <= 1.0 + 1e-15
+    qu = _step_advection("UD3", g)
+    assert qu.min() < -1e-3 or qu.max() > 1.0 + 1e-3
