@@ -23,7 +23,8 @@
  * Supported configuration (checked, otherwise SCALE_HEVI_ERR_UNSUPPORTED):
  * periodic lateral boundaries (BND_* = .false.), flat terrain (GSQRT = 1,
  * J13G = J23G = 0, MAPF = 1, checked once per metric array), the default
- * IBLOCK/JBLOCK (whole domain), flux schemes "UD3" and "CD4", ND_ORDER = 1,
+ * IBLOCK/JBLOCK (whole domain), flux schemes "UD3", "CD4", "CD2" and
+ * "UD3KOREN1993", ND_ORDER = 1,
  * 4 <= KMAX <= 256, halo width 2. No additional prognostic variables (VA = 0).
  *
  * Concurrency: one library state per process (like the reference's module
@@ -65,9 +66,9 @@ typedef struct scale_hevi_index {
  * HEVI short step (ATMOS_DYN_Tstep_short_fvm_hevi_setup,
  * scale_atmos_dyn_tstep_short_fvm_hevi.F90:118). flux_type and
  * flux_tracer_type are the ATMOS_DYN_FVM_FLUX_TYPE / _TRACER_TYPE names
- * ("UD3", "CD4"; the tracer scheme may also be "UD3KOREN1993",
- * scale_atmos_dyn_fvm_flux_ud3Koren1993.F90:163-373, the reference's default
- * tracer flux). device is the CUDA ordinal to use. */
+ * ("UD3", "CD4", "CD2" or "UD3KOREN1993": scale_atmos_dyn_fvm_flux_ud3.F90,
+ * _cd4.F90, _cd2.F90, _ud3Koren1993.F90; UD3KOREN1993 is the reference's
+ * default tracer flux). device is the CUDA ordinal to use. */
 int scale_hevi_setup(const scale_hevi_index *idx, const char *flux_type, const char *flux_tracer_type, int device);
 /* Frees every device buffer and the stream. */
 int scale_hevi_finalize(void);

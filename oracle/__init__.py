@@ -15,9 +15,8 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 LIB = HERE / "build" / "liboracle.so"
-UD3, CD4, KOREN = 1, 2, 3
-# "UD3KOREN1993" is a tracer scheme only
-SCHEMES = {"UD3": UD3, "CD4": CD4, "UD3KOREN1993": KOREN}
+UD3, CD4, KOREN, CD2 = 1, 2, 3, 4
+SCHEMES = {"UD3": UD3, "CD4": CD4, "UD3KOREN1993": KOREN, "CD2": CD2}
 
 
 class Dims(C.Structure):

@@ -34,28 +34,6 @@ void og_fluxZ_XYZ(const og_dims *d, int scheme, double *flux, const double *mflx
 #pragma omp parallel for collapse(2)
     for (int j = b.JJS; j <= b.JJE; ++j)
         for (int i = b.IIS; i <= b.IIE; ++i) {
-            if (scheme == OG_KOREN) {
-                /* ud3Koren1993.F90:186-255 */
-                for (int k = KS + 1; k <= KE - 2; ++k) {
-                    double vel = mflx[I3(k, i, j)];
-                    flux[I3(k, i, j)] = vel * og_koren_face(vel, val[I3(k - 1, i, j)], val[I3(k, i, j)],
-                                                            val[I3(k + 1, i, j)], val[I3(k + 2, i, j)])
-                                        + GSQRT[I3(k, i, j)] * nd[I3(k, i, j)];
-                }
-                flux[I3(KS - 1, i, j)] = 0.0;
-                double vel = mflx[I3(KS, i, j)];
-                const double q0 = val[I3(KS, i, j)], q1 = val[I3(KS + 1, i, j)], q2 = val[I3(KS + 2, i, j)];
-                flux[I3(KS, i, j)] = vel * (q0 * (0.5 + og_sign(0.5, vel))
-                                            + (q1 + 0.5 * og_koren_phi(q0, q1, q2) * (q1 - q2)) * (0.5 - og_sign(0.5, vel)))
-                                     + GSQRT[I3(KS, i, j)] * nd[I3(KS, i, j)];
-                vel = mflx[I3(KE - 1, i, j)];
-                const double e2 = val[I3(KE - 2, i, j)], e1 = val[I3(KE - 1, i, j)], e0 = val[I3(KE, i, j)];
-                flux[I3(KE - 1, i, j)] = vel * ((e1 + 0.5 * og_koren_phi(e2, e1, e0) * (e1 - e0)) * (0.5 + og_sign(0.5, vel))
-                                                + e0 * (0.5 - og_sign(0.5, vel)))
-                                         + GSQRT[I3(KE - 1, i, j)] * nd[I3(KE - 1, i, j)];
-                flux[I3(KE, i, j)] = 0.0;
-                continue;
-            }
             for (int k = KS + 1; k <= KE - 2; ++k) {
                 double vel = mflx[I3(k, i, j)];
                 flux[I3(k, i, j)] = vel * og_ip4(scheme, vel, val[I3(k - 1, i, j)], val[I3(k, i, j)],
@@ -83,11 +61,8 @@ void og_fluxX_XYZ(const og_dims *d, int scheme, double *flux, const double *mflx
         for (int i = b.IIS - 1; i <= b.IIE; ++i)
             for (int k = KS; k <= KE; ++k) {
                 double vel = mflx[I3(k, i, j)];
-                const double vm1 = val[I3(k, i - 1, j)], v0 = val[I3(k, i, j)], vp1 = val[I3(k, i + 1, j)],
-                             vp2 = val[I3(k, i + 2, j)];
-                /* ud3Koren1993.F90:298-305 for OG_KOREN */
-                flux[I3(k, i, j)] = vel * (scheme == OG_KOREN ? og_koren_face(vel, vm1, v0, vp1, vp2)
-                                                              : og_ip4(scheme, vel, vm1, v0, vp1, vp2))
+                flux[I3(k, i, j)] = vel * og_ip4(scheme, vel, val[I3(k, i - 1, j)], val[I3(k, i, j)],
+                                                 val[I3(k, i + 1, j)], val[I3(k, i + 2, j)])
                                     + GSQRT[I3(k, i, j)] * nd[I3(k, i, j)];
             }
 }
@@ -102,11 +77,8 @@ void og_fluxY_XYZ(const og_dims *d, int scheme, double *flux, const double *mflx
         for (int i = b.IIS; i <= b.IIE; ++i)
             for (int k = KS; k <= KE; ++k) {
                 double vel = mflx[I3(k, i, j)];
-                const double vm1 = val[I3(k, i, j - 1)], v0 = val[I3(k, i, j)], vp1 = val[I3(k, i, j + 1)],
-                             vp2 = val[I3(k, i, j + 2)];
-                /* ud3Koren1993.F90:355-362 for OG_KOREN */
-                flux[I3(k, i, j)] = vel * (scheme == OG_KOREN ? og_koren_face(vel, vm1, v0, vp1, vp2)
-                                                              : og_ip4(scheme, vel, vm1, v0, vp1, vp2))
+                flux[I3(k, i, j)] = vel * og_ip4(scheme, vel, val[I3(k, i, j - 1)], val[I3(k, i, j)],
+                                                 val[I3(k, i, j + 1)], val[I3(k, i, j + 2)])
                                     + GSQRT[I3(k, i, j)] * nd[I3(k, i, j)];
             }
 }

@@ -39,9 +39,21 @@ static inline double og_sign(double a, double b) { return copysign(fabs(a), b); 
 static inline double og_max(double a, double b) { return a > b ? a : b; }
 static inline double og_min(double a, double b) { return a < b ? a : b; }
 
+/* Koren (1993) limiter of UD3KOREN1993, scale_atmos_dyn_fvm_flux_ud3Koren1993.F90:1690-1710 */
+static inline double og_koren_phi(double v1, double v2, double v3)
+{
+    const double EPS = OG_EPS;
+    const double zerosw1 = EPS - og_sign(EPS, fabs(v1 - v2) - EPS);
+    const double zerosw2 = EPS - og_sign(EPS, fabs(v2 - v3) - EPS);
+    const double r2 = 2.0 * (v1 - v2 + zerosw1 * zerosw2) / (v2 - v3 + zerosw2);
+    return og_max(0.0, og_min(r2, og_min((1.0 + r2) / 3.0, 2.0)));
+}
+
 /* flux scheme kernels (UD3: scale_atmos_dyn_fvm_flux_ud3.F90:84-89,124-149;
- * CD4: scale_atmos_dyn_fvm_flux_cd4.F90:87-88,123-142). The face lies between
- * v0 and vp1; vm1/vp2 are the outer points. */
+ * CD4: scale_atmos_dyn_fvm_flux_cd4.F90:87-88,123-142; CD2: ..._cd2.F90, the
+ * same F2*(v0+vp1) at every face; UD3KOREN1993: the limited upwind value of
+ * ..._ud3Koren1993.F90:200-206 (interior), :236-241 (above KS), :243-249
+ * (below KE)). The face lies between v0 and vp1; vm1/vp2 are the outer points. */
 #define F2_  0.5
 #define F31 (-1.0 / 12.0)
 #define F32 (7.0 / 12.0)
@@ -53,6 +65,11 @@ static inline double og_ip4(int scheme, double vel, double vm1, double v0, doubl
 {
     if (scheme == OG_UD3)
         return (F31 * (vp2 + vm1) + F32 * (vp1 + v0)) - (F31 * (vp2 - vm1) + F33 * (vp1 - v0)) * og_sign(1.0, vel);
+    if (scheme == OG_CD2)
+        return F2_ * (vp1 + v0);
+    if (scheme == OG_KOREN)
+        return (v0 + 0.5 * og_koren_phi(vp1, v0, vm1) * (v0 - vm1)) * (0.5 + og_sign(0.5, vel))
+               + (vp1 + 0.5 * og_koren_phi(v0, vp1, vp2) * (vp1 - vp2)) * (0.5 - og_sign(0.5, vel));
     return F41 * (vp1 + v0) + F42 * (vp2 + vm1);
 }
 /* one-sided value at the KS face from val(KS), val(KS+1), val(KS+2) */
@@ -60,6 +77,8 @@ static inline double og_ipL(int scheme, double vel, double v0, double v1, double
 {
     if (scheme == OG_UD3)
         return F2_ * (v1 + v0) * (0.5 + og_sign(0.5, vel)) + (2.0 * v0 + 5.0 * v1 - v2) / 6.0 * (0.5 - og_sign(0.5, vel));
+    if (scheme == OG_KOREN)
+        return v0 * (0.5 + og_sign(0.5, vel)) + (v1 + 0.5 * og_koren_phi(v0, v1, v2) * (v1 - v2)) * (0.5 - og_sign(0.5, vel));
     return F2_ * (v1 + v0);
 }
 /* one-sided value at the KE-1 face from val(KE), val(KE-1), val(KE-2) */
@@ -67,25 +86,9 @@ static inline double og_ipH(int scheme, double vel, double vE, double vE1, doubl
 {
     if (scheme == OG_UD3)
         return (2.0 * vE + 5.0 * vE1 - vE2) / 6.0 * (0.5 + og_sign(0.5, vel)) + F2_ * (vE + vE1) * (0.5 - og_sign(0.5, vel));
+    if (scheme == OG_KOREN)
+        return (vE1 + 0.5 * og_koren_phi(vE2, vE1, vE) * (vE1 - vE)) * (0.5 + og_sign(0.5, vel)) + vE * (0.5 - og_sign(0.5, vel));
     return F2_ * (vE + vE1);
-}
-
-/* Koren (1993) limiter of the UD3KOREN1993 tracer flux,
- * scale_atmos_dyn_fvm_flux_ud3Koren1993.F90:1690-1710 */
-static inline double og_koren_phi(double v1, double v2, double v3)
-{
-    const double EPS = OG_EPS;
-    const double zerosw1 = EPS - og_sign(EPS, fabs(v1 - v2) - EPS);
-    const double zerosw2 = EPS - og_sign(EPS, fabs(v2 - v3) - EPS);
-    const double r2 = 2.0 * (v1 - v2 + zerosw1 * zerosw2) / (v2 - v3 + zerosw2);
-    return og_max(0.0, og_min(r2, og_min((1.0 + r2) / 3.0, 2.0)));
-}
-/* limited face value with the upwind switch: vm1 v0 | vp1 vp2, the face
- * between v0 and vp1 (ud3Koren1993.F90:200-206, 298-305, 355-362) */
-static inline double og_koren_face(double vel, double vm1, double v0, double vp1, double vp2)
-{
-    return (v0 + 0.5 * og_koren_phi(vp1, v0, vm1) * (v0 - vm1)) * (0.5 + og_sign(0.5, vel))
-           + (vp1 + 0.5 * og_koren_phi(v0, vp1, vp2) * (vp1 - vp2)) * (0.5 - og_sign(0.5, vel));
 }
 
 /* ---- flux family (19 routines), one generic restatement per reference routine ---- */

@@ -18,6 +18,7 @@ import os
 import shutil
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 from pathlib import Path
 
 PKG = Path(__file__).resolve().parent
@@ -63,7 +64,7 @@ def build_cuda(force: bool = False, verbose: bool = False) -> Path:
     nvcc = _nvcc()
     common = ["-O3", "-std=c++17", "--fmad=false", "-lineinfo", "-ccbin", _host_cxx(),
               "-Xcompiler", "-fPIC,-ffp-contract=off", "-I", str(ROOT / "include")]
-    objs = []
+    objs, cmds = [], []
     for src in CU_SOURCES + CPP_SOURCES:
         obj = objdir / (Path(src).stem + ".o")
         cmd = [nvcc, *common, *ARCH, "-c", str(CSRC / src), "-o", str(obj)]
@@ -71,8 +72,13 @@ def build_cuda(force: bool = False, verbose: bool = False) -> Path:
             cmd += ["-Xptxas", "-v"]
         if src.endswith(".cpp"):
             cmd = [nvcc, *common, *ARCH, "-x", "c++", "-c", str(CSRC / src), "-o", str(obj)]
-        _run(cmd)
+        cmds.append(cmd)
         objs.append(str(obj))
+    # the translation units compile independently; the kernel templates make
+    # some of them long, so they run side by side
+    with ThreadPoolExecutor(max_workers=min(len(cmds), os.cpu_count() or 1)) as pool:
+        for f in [pool.submit(_run, c) for c in cmds]:
+            f.result()
     tmp = LIB.with_suffix(".so.tmp")
     _run([nvcc, *ARCH, "-shared", "-cudart", "static", "-o", str(tmp), *objs])
     tmp.replace(LIB)

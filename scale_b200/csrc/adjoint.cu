@@ -51,6 +51,7 @@ struct Dual {
     }
     friend __device__ Dual operator-(const Dual &a) { return {-a.v, -a.t}; }
     friend __device__ Dual operator+(const Dual &a) { return a; }
+    friend __device__ double vof(const Dual &a) { return a.v; }
     friend __device__ Dual fabs(const Dual &a) { return {::fabs(a.v), signbit(a.v) ? -a.t : a.t}; }
     friend __device__ Dual copysign(const Dual &a, const Dual &b)
     {
@@ -108,6 +109,7 @@ struct Jet {
         return r;
     }
     friend __device__ Jet operator+(const Jet &a) { return a; }
+    friend __device__ double vof(const Jet &a) { return a.v; }
     friend __device__ Jet fabs(const Jet &a)
     {
         Jet r = signbit(a.v) ? -a : a;
@@ -1293,17 +1295,29 @@ static cudaError_t step_adj_impl(const Model &M, const double *X_in, double *lam
     return cudaGetLastError();
 }
 
+// the model's flux scheme as a template argument
+template <class F>
+static cudaError_t by_scheme(int scheme, F f)
+{
+    switch (scheme) {
+    case UD3: return f(std::integral_constant<int, UD3>{});
+    case CD4: return f(std::integral_constant<int, CD4>{});
+    case KOREN: return f(std::integral_constant<int, KOREN>{});
+    case CD2: return f(std::integral_constant<int, CD2>{});
+    default: return cudaErrorInvalidValue;
+    }
+}
 cudaError_t step_forward(const Model &M, double *X)
 {
-    return M.scheme == UD3 ? step_tlm_impl<UD3>(M, X, nullptr, false) : step_tlm_impl<CD4>(M, X, nullptr, false);
+    return by_scheme(M.scheme, [&](auto s) { return step_tlm_impl<decltype(s)::value>(M, X, nullptr, false); });
 }
 cudaError_t step_tlm(const Model &M, double *X, double *dX)
 {
-    return M.scheme == UD3 ? step_tlm_impl<UD3>(M, X, dX, true) : step_tlm_impl<CD4>(M, X, dX, true);
+    return by_scheme(M.scheme, [&](auto s) { return step_tlm_impl<decltype(s)::value>(M, X, dX, true); });
 }
 cudaError_t step_adjoint(const Model &M, const double *X, double *lam)
 {
-    return M.scheme == UD3 ? step_adj_impl<UD3>(M, X, lam) : step_adj_impl<CD4>(M, X, lam);
+    return by_scheme(M.scheme, [&](auto s) { return step_adj_impl<decltype(s)::value>(M, X, lam); });
 }
 cudaError_t boundary_adjoint(const Model &M, double *lam)
 {

@@ -197,7 +197,8 @@ int parse_scheme(const char *s, int *out)
     if (n == "UD3") { *out = UD3; return SCALE_HEVI_OK; }
     if (n == "CD4") { *out = CD4; return SCALE_HEVI_OK; }
     if (n == "UD3KOREN1993") { *out = KOREN; return SCALE_HEVI_OK; }
-    return fail(SCALE_HEVI_ERR_UNSUPPORTED, "flux scheme '%s' is not supported (UD3, CD4; UD3KOREN1993 for tracers)",
+    if (n == "CD2") { *out = CD2; return SCALE_HEVI_OK; }
+    return fail(SCALE_HEVI_ERR_UNSUPPORTED, "flux scheme '%s' is not supported (UD3, CD4, UD3KOREN1993, CD2)",
                 n.c_str());
 }
 
@@ -608,8 +609,6 @@ int scale_hevi_ensemble_setup(int n, const scale_hevi_index *idx, const char *fl
     int s1, s2;
     CK(parse_scheme(flux_type, &s1));
     CK(parse_scheme(flux_tracer_type, &s2));
-    if (s1 == KOREN)
-        return fail(SCALE_HEVI_ERR_UNSUPPORTED, "UD3KOREN1993 is supported as the tracer flux scheme only");
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
         cudaGetLastError();

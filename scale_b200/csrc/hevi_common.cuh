@@ -20,7 +20,8 @@
 namespace hevi {
 
 // flux schemes (ATMOS_DYN_FVM_FLUX_TYPE names)
-enum Scheme : int { UD3 = 1, CD4 = 2, KOREN = 3 }; // KOREN: UD3KOREN1993, tracer fluxes only
+// (ATMOS_DYN_FVM_FLUX_TYPE / _TRACER_TYPE names: UD3, CD4, UD3KOREN1993, CD2)
+enum Scheme : int { UD3 = 1, CD4 = 2, KOREN = 3, CD2 = 4 };
 
 struct Grid {
     int KA, IA, JA;
@@ -116,28 +117,59 @@ __device__ __forceinline__ R fsign(R a, R b) { return copysign(fabs(a), b); }
 __device__ __forceinline__ double fmax2(double a, double b) { return a > b ? a : b; }
 __device__ __forceinline__ double fmin2(double a, double b) { return a < b ? a : b; }
 
-// ---- 4-point face interpolation of the flux schemes --------------------------
-// UD3: scale_atmos_dyn_fvm_flux_ud3.F90:87-89,124-125 ; CD4: ..._cd4.F90:87-88,123-124
-// The face lies between v0 and vp1. R is the arithmetic type (double on the
-// plain path; float for the flux arithmetic of the mixed-precision path).
+// value of a scalar of any arithmetic type of the kernels, for comparisons
+template <typename R>
+__device__ __forceinline__ double vof(const R &x) { return (double)x; }
+template <typename R>
+__device__ __forceinline__ R rmax(R a, R b) { return vof(a) > vof(b) ? a : b; }
+template <typename R>
+__device__ __forceinline__ R rmin(R a, R b) { return vof(a) < vof(b) ? a : b; }
+
+// ---- UD3KOREN1993 (scale_atmos_dyn_fvm_flux_ud3Koren1993.F90) ----
+// the Koren (1993) limiter phi (:1690-1710)
+template <typename R>
+__device__ __forceinline__ R koren_phi(R v1, R v2, R v3)
+{
+    const R eps = R(EPS);
+    const R zerosw1 = eps - fsign(eps, fabs(v1 - v2) - eps);
+    const R zerosw2 = eps - fsign(eps, fabs(v2 - v3) - eps);
+    const R r2 = R(2.0) * (v1 - v2 + zerosw1 * zerosw2) / (v2 - v3 + zerosw2);
+    return rmax(R(0.0), rmin(r2, rmin((R(1.0) + r2) / R(3.0), R(2.0))));
+}
+
+// ---- face interpolation of the flux schemes ----------------------------------
+// UD3: scale_atmos_dyn_fvm_flux_ud3.F90:87-89,124-125 ; CD4: ..._cd4.F90:87-88,123-124;
+// CD2: ..._cd2.F90 (F2*(v0+vp1) at every face); UD3KOREN1993: the limited
+// upwind value of ..._ud3Koren1993.F90 (:200-206 interior, :236-241 above KS,
+// :243-249 below KE). The face lies between v0 and vp1. R is the arithmetic
+// type (double on the plain path; float for the flux arithmetic of the
+// mixed-precision path; dual numbers and jets in the differentiated step).
 template <int S, typename R>
 __device__ __forceinline__ R ip4(R vel, R vm1, R v0, R vp1, R vp2)
 {
-    if (S == UD3) {
+    if constexpr (S == UD3) {
         const R F31 = R(-1.0 / 12.0), F32 = R(7.0 / 12.0), F33 = R(3.0 / 12.0);
         return (F31 * (vp2 + vm1) + F32 * (vp1 + v0)) - (F31 * (vp2 - vm1) + F33 * (vp1 - v0)) * fsign(R(1.0), vel);
-    } else {
+    } else if constexpr (S == CD4) {
         const R F41 = R(7.0 / 12.0), F42 = R(-1.0 / 12.0);
         return F41 * (vp1 + v0) + F42 * (vp2 + vm1);
+    } else if constexpr (S == CD2) {
+        return R(0.5) * (vp1 + v0);
+    } else {
+        return (v0 + R(0.5) * koren_phi(vp1, v0, vm1) * (v0 - vm1)) * (R(0.5) + fsign(R(0.5), vel))
+               + (vp1 + R(0.5) * koren_phi(v0, vp1, vp2) * (vp1 - vp2)) * (R(0.5) - fsign(R(0.5), vel));
     }
 }
 // value at the KS face from val(KS), val(KS+1), val(KS+2) (ud3.F90:142-145, cd4.F90:141)
 template <int S, typename R>
 __device__ __forceinline__ R ipL(R vel, R v0, R v1, R v2)
 {
-    if (S == UD3)
+    if constexpr (S == UD3)
         return R(0.5) * (v1 + v0) * (R(0.5) + fsign(R(0.5), vel))
                + (R(2.0) * v0 + R(5.0) * v1 - v2) / R(6.0) * (R(0.5) - fsign(R(0.5), vel));
+    else if constexpr (S == KOREN)
+        return v0 * (R(0.5) + fsign(R(0.5), vel))
+               + (v1 + R(0.5) * koren_phi(v0, v1, v2) * (v1 - v2)) * (R(0.5) - fsign(R(0.5), vel));
     else
         return R(0.5) * (v1 + v0);
 }
@@ -145,37 +177,14 @@ __device__ __forceinline__ R ipL(R vel, R v0, R v1, R v2)
 template <int S, typename R>
 __device__ __forceinline__ R ipH(R vel, R vE, R vE1, R vE2)
 {
-    if (S == UD3)
+    if constexpr (S == UD3)
         return (R(2.0) * vE + R(5.0) * vE1 - vE2) / R(6.0) * (R(0.5) + fsign(R(0.5), vel))
                + R(0.5) * (vE + vE1) * (R(0.5) - fsign(R(0.5), vel));
+    else if constexpr (S == KOREN)
+        return (vE1 + R(0.5) * koren_phi(vE2, vE1, vE) * (vE1 - vE)) * (R(0.5) + fsign(R(0.5), vel))
+               + vE * (R(0.5) - fsign(R(0.5), vel));
     else
         return R(0.5) * (vE + vE1);
-}
-
-// ---- UD3KOREN1993 tracer flux (scale_atmos_dyn_fvm_flux_ud3Koren1993.F90) ----
-// the Koren (1993) limiter phi (:1690-1710)
-__device__ __forceinline__ double koren_phi(double v1, double v2, double v3)
-{
-    const double zerosw1 = EPS - fsign(EPS, fabs(v1 - v2) - EPS);
-    const double zerosw2 = EPS - fsign(EPS, fabs(v2 - v3) - EPS);
-    const double r2 = 2.0 * (v1 - v2 + zerosw1 * zerosw2) / (v2 - v3 + zerosw2);
-    return fmax2(0.0, fmin2(r2, fmin2((1.0 + r2) / 3.0, 2.0)));
-}
-// limited value at the face between v0 and vp1 with the upwind switch
-// (:200-206 for z, :298-305 for x, :355-362 for y)
-__device__ __forceinline__ double koren_face(double vel, double vm1, double v0, double vp1, double vp2)
-{
-    return (v0 + 0.5 * koren_phi(vp1, v0, vm1) * (v0 - vm1)) * (0.5 + fsign(0.5, vel))
-           + (vp1 + 0.5 * koren_phi(v0, vp1, vp2) * (vp1 - vp2)) * (0.5 - fsign(0.5, vel));
-}
-// the one-sided faces above KS (:236-241) and below KE (:243-249)
-__device__ __forceinline__ double koren_face_KS(double vel, double q0, double q1, double q2)
-{
-    return q0 * (0.5 + fsign(0.5, vel)) + (q1 + 0.5 * koren_phi(q0, q1, q2) * (q1 - q2)) * (0.5 - fsign(0.5, vel));
-}
-__device__ __forceinline__ double koren_face_KE(double vel, double e2, double e1, double e0)
-{
-    return (e1 + 0.5 * koren_phi(e2, e1, e0) * (e1 - e0)) * (0.5 + fsign(0.5, vel)) + e0 * (0.5 - fsign(0.5, vel));
 }
 
 // read-only load through the non-coherent cache

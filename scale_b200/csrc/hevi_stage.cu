@@ -616,8 +616,13 @@ cudaError_t launch_hevi_stage(const Grid &g, const Members &mem, const StageArgs
     const int tx = shape.tile_x > 0 ? shape.tile_x : STAGE_TILE_X_DEFAULT;
     auto go = [&](auto tile, const auto &B, int nb) -> cudaError_t {
         constexpr int TX = decltype(tile)::value, NM = std::decay_t<decltype(B)>::NMAX;
-        return scheme == UD3 ? launch_one<UD3, R, TX, NM>(g, a, B, nb, smem, shape.raster, st)
-                             : launch_one<CD4, R, TX, NM>(g, a, B, nb, smem, shape.raster, st);
+        switch (scheme) {
+        case UD3: return launch_one<UD3, R, TX, NM>(g, a, B, nb, smem, shape.raster, st);
+        case CD4: return launch_one<CD4, R, TX, NM>(g, a, B, nb, smem, shape.raster, st);
+        case KOREN: return launch_one<KOREN, R, TX, NM>(g, a, B, nb, smem, shape.raster, st);
+        case CD2: return launch_one<CD2, R, TX, NM>(g, a, B, nb, smem, shape.raster, st);
+        default: return cudaErrorInvalidValue;
+        }
     };
     auto dispatch = [&](auto tile) {
         constexpr int TX = decltype(tile)::value, TY = HEVI_COL_TC / TX;

@@ -38,15 +38,9 @@ __device__ double hflux_z(const Grid &g, const TracerArgs &a, size_t N3, size_t 
     const double *q = a.QTRC + col - 1;
     const double vel = ld(a.mflx + col + m - 1);
     double v;
-    if constexpr (S == KOREN) {
-        if (m == g.KS) v = koren_face_KS(vel, ld(q + m), ld(q + m + 1), ld(q + m + 2));
-        else if (m == g.KE - 1) v = koren_face_KE(vel, ld(q + m - 1), ld(q + m), ld(q + m + 1));
-        else v = koren_face(vel, ld(q + m - 1), ld(q + m), ld(q + m + 1), ld(q + m + 2));
-    } else {
-        if (m == g.KS) v = ipL<S>(vel, ld(q + m), ld(q + m + 1), ld(q + m + 2));
-        else if (m == g.KE - 1) v = ipH<S>(vel, ld(q + m + 1), ld(q + m), ld(q + m - 1));
-        else v = ip4<S>(vel, ld(q + m - 1), ld(q + m), ld(q + m + 1), ld(q + m + 2));
-    }
+    if (m == g.KS) v = ipL<S>(vel, ld(q + m), ld(q + m + 1), ld(q + m + 2));
+    else if (m == g.KE - 1) v = ipH<S>(vel, ld(q + m + 1), ld(q + m), ld(q + m - 1));
+    else v = ip4<S>(vel, ld(q + m - 1), ld(q + m), ld(q + m + 1), ld(q + m + 2));
     return vel * v + ndq_at(a, N3, 0, col + m - 1);
 }
 // high-order flux at the face between c and c+s (fluxX/Y_XYZ, ud3.F90:251-353); dir 1 = x, 2 = y
@@ -55,10 +49,7 @@ __device__ __forceinline__ double hflux_h(const TracerArgs &a, size_t N3, int di
 {
     const double vel = ld(a.mflx + (size_t)dir * N3 + c);
     const double *q = a.QTRC + c;
-    if constexpr (S == KOREN)
-        return vel * koren_face(vel, ld(q - s), ld(q), ld(q + s), ld(q + 2 * s)) + ndq_at(a, N3, dir, c);
-    else
-        return vel * ip4<S>(vel, ld(q - s), ld(q), ld(q + s), ld(q + 2 * s)) + ndq_at(a, N3, dir, c);
+    return vel * ip4<S>(vel, ld(q - s), ld(q), ld(q + s), ld(q + 2 * s)) + ndq_at(a, N3, dir, c);
 }
 // donor-cell flux at the face between c and c+s (ud1.F90:155-165)
 __device__ __forceinline__ double lflux(const TracerArgs &a, size_t N3, int dir, size_t c, long s)
@@ -281,26 +272,32 @@ __global__ void __launch_bounds__(128) k_fct_apply(const Grid g, const TracerArg
     }
 }
 
-cudaError_t launch_tracer_stage(const Grid &g, const TracerArgs &a, int scheme, bool fct, cudaStream_t st)
+template <int S>
+static cudaError_t tracer_stage(const Grid &g, const TracerArgs &a, bool fct, cudaStream_t st)
 {
     dim3 b(32, 4), gr((g.IMAX + 3) / 4, g.JMAX);
     if (!fct) {
-        if (scheme == UD3) k_tracer_plain<UD3><<<gr, b, 0, st>>>(g, a);
-        else if (scheme == CD4) k_tracer_plain<CD4><<<gr, b, 0, st>>>(g, a);
-        else k_tracer_plain<KOREN><<<gr, b, 0, st>>>(g, a);
+        k_tracer_plain<S><<<gr, b, 0, st>>>(g, a);
         return cudaGetLastError();
     }
     dim3 gl((g.IMAX + 2 + 3) / 4, g.JMAX + 2);
-    if (scheme == UD3) k_fct_lo<UD3><<<gl, b, 0, st>>>(g, a);
-    else if (scheme == CD4) k_fct_lo<CD4><<<gl, b, 0, st>>>(g, a);
-    else k_fct_lo<KOREN><<<gl, b, 0, st>>>(g, a);
+    k_fct_lo<S><<<gl, b, 0, st>>>(g, a);
     k_fct_r<<<gr, b, 0, st>>>(g, a);
     double *rr[2] = {a.rjp, a.rjm};
     periodic_halo(g, Members{}, rr, 2, st);
-    if (scheme == UD3) k_fct_apply<UD3><<<gr, b, 0, st>>>(g, a);
-    else if (scheme == CD4) k_fct_apply<CD4><<<gr, b, 0, st>>>(g, a);
-    else k_fct_apply<KOREN><<<gr, b, 0, st>>>(g, a);
+    k_fct_apply<S><<<gr, b, 0, st>>>(g, a);
     return cudaGetLastError();
+}
+
+cudaError_t launch_tracer_stage(const Grid &g, const TracerArgs &a, int scheme, bool fct, cudaStream_t st)
+{
+    switch (scheme) {
+    case UD3: return tracer_stage<UD3>(g, a, fct, st);
+    case CD4: return tracer_stage<CD4>(g, a, fct, st);
+    case KOREN: return tracer_stage<KOREN>(g, a, fct, st);
+    case CD2: return tracer_stage<CD2>(g, a, fct, st);
+    default: return cudaErrorInvalidValue;
+    }
 }
 
 }  // namespace hevi

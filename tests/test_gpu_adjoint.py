@@ -79,6 +79,28 @@ def test_tangent_linear_matches_finite_differences(model):
     assert med < 1e-8, med
 
 
+@pytest.mark.parametrize("scheme", ["UD3KOREN1993", "CD2"])
+def test_adjoint_dot_product_other_schemes(scheme):
+    c = _case(scheme)
+    hevi.setup(c.g.index_dict(), c.scheme, c.scheme_tracer)
+    try:
+        m = adjoint.Model(c)
+        X = m.state()
+        m.boundary(X)
+        for _ in range(3):
+            m.step(X)
+        r = adjoint.dot_product_test(m, X, 2)
+        assert r["rel_diff"] < 1e-11, r
+        # the pass form reproduces the fused step for this scheme as well
+        Xa, Xb = X.clone(), X.clone()
+        m.step(Xa)
+        m.step_passes(Xb)
+        hevi.check()
+        assert (Xa - Xb).abs().max().item() <= 1e-12 * Xa.abs().max().item()
+    finally:
+        hevi.finalize()
+
+
 def test_adjoint_dot_product(model):
     X = model.state()
     model.boundary(X)

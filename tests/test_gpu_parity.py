@@ -34,7 +34,7 @@ def _stage_call_args(a, o):
     return kw
 
 
-@pytest.mark.parametrize("scheme", ["UD3", "CD4"])
+@pytest.mark.parametrize("scheme", ["UD3", "CD4", "UD3KOREN1993", "CD2"])
 @pytest.mark.parametrize("stretched", [False, True])
 @pytest.mark.parametrize("full", [False, True])
 def test_stage_bit_exact(lib, scheme, stretched, full):
@@ -74,7 +74,7 @@ def test_stage_device_entry_matches_host_entry(lib):
         assert np.array_equal(got, v), n
 
 
-@pytest.mark.parametrize("scheme", ["UD3", "CD4"])
+@pytest.mark.parametrize("scheme", ["UD3", "CD4", "UD3KOREN1993", "CD2"])
 def test_rk4_short_step_bit_exact(lib, scheme):
     g = helpers.small_grid(IMAX=14, JMAX=11, KMAX=18, stretched=(scheme == "CD4"))
     c = helpers.small_case(g, scheme)
@@ -134,7 +134,7 @@ def _tracer_inputs(g, c, seed=5):
     return q0, q, dens0, dens, mflx, rhoq, GS, np.asfortranarray(MAPF[..., 0])
 
 
-@pytest.mark.parametrize("scheme", ["UD3", "CD4", "UD3KOREN1993"])
+@pytest.mark.parametrize("scheme", ["UD3", "CD4", "UD3KOREN1993", "CD2"])
 @pytest.mark.parametrize("fct,along", [(False, True), (True, True), (True, False)])
 def test_tracer_step_bit_exact(lib, scheme, fct, along):
     g = helpers.small_grid(IMAX=12, JMAX=14, KMAX=16)
@@ -144,7 +144,7 @@ def test_tracer_step_bit_exact(lib, scheme, fct, along):
     ref = np.full(g.shape, np.nan, order="F")
     oracle.tstep_tracer(g, scheme, ref, q, q0, rhoq, d0, d, mflx, g.zeros(3), GS, MAPF, 2.5, fct, along)
     got = np.full(g.shape, np.nan, order="F")
-    lib.setup(g.index_dict(), "UD3" if scheme == "UD3KOREN1993" else scheme, scheme)
+    lib.setup(g.index_dict(), scheme, scheme)
     lib.ATMOS_DYN_Tstep_tracer_fvm_heve(QTRCo=got, QTRC=q, QTRC0=q0, RHOQ_t=rhoq, DENS0=d0, DENS=d, mflx_hi=mflx,
                                         num_diff=g.zeros(3), GSQRT=GS, MAPF=MAPF, CDZ=g.CDZ, RCDZ=g.RCDZ,
                                         RCDX=g.RCDX, RCDY=g.RCDY, dtl=2.5, FLAG_FCT_TRACER=fct,

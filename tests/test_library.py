@@ -80,11 +80,12 @@ def test_fortran_blank_padded_scheme_names_are_accepted():
     assert e.value.code == 3
 
 
-def test_koren_only_as_tracer_scheme():
-    """UD3KOREN1993 is accepted as the tracer flux scheme and rejected, before
-    any device work, as the dynamics flux scheme."""
+def test_unknown_flux_scheme_rejected_before_device_work():
+    """Scheme names outside UD3, CD4, UD3KOREN1993 and CD2 (for example the
+    halo-3 schemes UD5 and CD6) are refused before any device work."""
     from scale_b200 import hevi, mkinit
 
     g = mkinit.uniform_grid(8, 8, 8, 500.0, 500.0, 250.0)
-    with pytest.raises(hevi.HeviError, match="tracer flux scheme only"):
-        hevi.setup(g.index_dict(), "UD3KOREN1993", "UD3")
+    for name in ("UD5", "CD6"):
+        with pytest.raises(hevi.HeviError, match="not supported"):
+            hevi.setup(g.index_dict(), name, "UD3")

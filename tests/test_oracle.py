@@ -36,7 +36,7 @@ def _interior(a, g):
     return a[g.KS - 1 : g.KE, g.IS - 1 : g.IE, g.JS - 1 : g.JE]
 
 
-@pytest.mark.parametrize("scheme", ["UD3", "CD4"])
+@pytest.mark.parametrize("scheme", ["UD3", "CD4", "UD3KOREN1993", "CD2"])
 def test_const(scheme):
     """test_const (test_atmos_dyn.f90:382-454): a horizontally uniform state stays uniform."""
     g = helpers.small_grid(8, 6, 12)
@@ -61,7 +61,7 @@ def test_const(scheme):
     assert np.array_equal(q, np.broadcast_to(q[:, :1, :1], q.shape))
 
 
-@pytest.mark.parametrize("scheme", ["UD3", "CD4"])
+@pytest.mark.parametrize("scheme", ["UD3", "CD4", "UD3KOREN1993", "CD2"])
 def test_conserve(scheme):
     """test_conserve (test_atmos_dyn.f90:456-592): domain totals of DENS and RHOT
     (weighted by the cell volume) are conserved to round-off."""
