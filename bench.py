@@ -348,9 +348,13 @@ def run_b200(args):
     if rank == 0 and not args.no_cpu_baseline:
         out["cpu_baseline"] = cpu_baseline(args)
     hevi.finalize()
-    if world == 1 and not args.no_ensemble:
+    if world == 1 and not (args.no_ensemble and args.no_mixed_large):
         del st, X, mflx, tflx, nd, tend, ref, dp0, rt2p, refr, GS, J0, MAPF, cor
         torch.cuda.empty_cache()
+    if world == 1 and not args.no_mixed_large:
+        out["mixed_1024x1024x96"] = run_mixed_large(args, hevi, torch)
+        torch.cuda.empty_cache()
+    if world == 1 and not args.no_ensemble:
         out["ensemble"] = run_ensemble(args, hevi, torch)
     if world == 1 and not args.no_adjoint:
         out["adjoint"] = run_adjoint(args, hevi, torch)
@@ -359,6 +363,110 @@ def run_b200(args):
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(out), flush=True)
+
+
+def run_mixed_large(args, hevi, torch):
+    """The multi-bubble configuration at its full 1024x1024x96 size: the same
+    short steps (numfilter + RK4 + boundary/halo) from the same initial state
+    in FP64 and in mixed precision, timed on the library stream; errors of the
+    mixed state against the FP64 state after the same steps, relative to each
+    field's largest magnitude over the interior."""
+    from scale_b200 import mkinit
+
+    w0 = time.time()
+    c = mkinit.config(4, scale=args.mixed_scale)
+    RT2P, DPRES0, REF_rhot = mkinit.large_prep(c)
+    prep_s = time.time() - w0
+    g = c.g
+    N3 = int(np.prod(g.shape))
+    cells = g.cells
+    hevi.setup(g.index_dict(), c.scheme, c.scheme_tracer)
+    try:
+        hevi.stage_autotune(True)
+        st0 = torch.empty((5, N3), dtype=torch.float64, device="cuda")
+        for v, n in enumerate(("DENS", "MOMZ", "MOMX", "MOMY", "RHOT")):
+            st0[v].copy_(to_dev(c.state[n], torch))
+        ref = {n: to_dev(v, torch) for n, v in c.ref.items()}
+        dp0, rt2p, refr = to_dev(DPRES0, torch), to_dev(RT2P, torch), to_dev(REF_rhot, torch)
+        del RT2P, DPRES0, REF_rhot
+        GS = torch.ones(7 * N3, dtype=torch.float64, device="cuda")
+        J0 = torch.zeros(7 * N3, dtype=torch.float64, device="cuda")
+        MAPF = torch.ones(g.IA * g.JA * 8, dtype=torch.float64, device="cuda")
+        cor = torch.zeros(g.IA * g.JA, dtype=torch.float64, device="cuda")
+        wd = np.zeros(g.KA)
+        grid = dict(CDZ=g.CDZ, FDZ=g.FDZ, FDX=g.FDX, FDY=g.FDY, RCDZ=g.RCDZ, RCDX=g.RCDX, RCDY=g.RCDY,
+                    RFDZ=g.RFDZ, RFDX=g.RFDX, RFDY=g.RFDY)
+        stream = torch.cuda.ExternalStream(hevi.stream_handle())
+        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        k, warm = args.mixed_large_steps, max(3, args.warmup)
+
+        def run(mixed):
+            ft = torch.float32 if mixed else torch.float64
+            st = st0.clone()
+            X = dict(DENS=st[0], MOMZ=st[1], MOMX=st[2], MOMY=st[3], RHOT=st[4])
+            z = lambda q=1: torch.zeros(q * N3, dtype=ft, device="cuda")  # noqa: E731
+            mflx, tflx, nd = z(3), z(3), z(15)
+            tend = {n: z() for n in ("DENS_t", "MOMZ_t", "MOMX_t", "MOMY_t", "RHOT_t")}
+            nf = hevi.ATMOS_DYN_numfilter_coef_mixed_dev if mixed else hevi.ATMOS_DYN_numfilter_coef_dev
+            rk = hevi.ATMOS_DYN_Tinteg_short_rk4_mixed_dev if mixed else hevi.ATMOS_DYN_Tinteg_short_rk4_dev
+
+            def step():
+                nf(num_diff=nd, CDZ=g.CDZ, CDX=g.CDX, CDY=g.CDY, FDZ=g.FDZ, FDX=g.FDX, FDY=g.FDY, DT=c.dt,
+                   REF_dens=ref["REF_dens"], REF_pott=ref["REF_pott"], ND_COEF=c.nd_coef, ND_ORDER=1,
+                   ND_SFC_FACT=1.0, ND_USE_RS=True, **X)
+                rk(PROG=None, mflx_hi=mflx, tflx_hi=tflx, DPRES0=dp0, RT2P=rt2p, CORIOLI=cor, num_diff=nd,
+                   wdamp_coef=wd, divdmp_coef=0.0, DDIV=None, FLAG_FCT_MOMENTUM=False, FLAG_FCT_T=False,
+                   FLAG_FCT_ALONG_STREAM=True, PHI=ref["PHI"], GSQRT=GS, J13G=J0, J23G=J0, J33G=1.0, MAPF=MAPF,
+                   REF_dens=ref["REF_dens"], REF_rhot=refr, BND_W=False, BND_E=False, BND_S=False, BND_N=False,
+                   dt=c.dt, **X, **tend, **grid)
+                hevi.boundary_dev(**X)
+
+            for _ in range(warm):
+                step()
+            hevi.check()
+            torch.cuda.synchronize()
+            hevi.profile(True)
+            t0.record(stream)
+            for _ in range(k):
+                step()
+            t1.record(stream)
+            torch.cuda.synchronize()
+            prof = hevi.profile_report()
+            hevi.profile(False)
+            hevi.check()
+            del mflx, tflx, nd, tend
+            return st, t0.elapsed_time(t1) / k, prof
+
+        st64, ms64, prof64 = run(False)
+        st32, ms32, prof32 = run(True)
+        sl = (slice(g.KS - 1, g.KE), slice(g.IS - 1, g.IE), slice(g.JS - 1, g.JE))
+        errs = {}
+        for v, n in enumerate(("DENS", "MOMZ", "MOMX", "MOMY", "RHOT")):
+            a64 = st64[v].view(g.JA, g.IA, g.KA).permute(2, 1, 0)[sl[0], sl[1], sl[2]]
+            a32 = st32[v].view(g.JA, g.IA, g.KA).permute(2, 1, 0)[sl[0], sl[1], sl[2]]
+            d = (a32 - a64).abs()
+            scale = float(a64.abs().max())
+            errs[n] = {"max": float(d.max()) / scale, "rms": float(d.pow(2).mean().sqrt()) / scale}
+        peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+        hbm = float(peaks.get("hbm_gbs", 6650.0))
+        n64, t64 = prof64.get("hevi_stage", (0, 0.0))
+        n32, t32 = prof32.get("hevi_stage_mixed", (0, 0.0))
+        s64, s32 = t64 / max(n64, 1), t32 / max(n32, 1)
+        return {
+            "workload": f"{g.IMAX}x{g.JMAX}x{g.KMAX} multi-bubble (32 seeded bubbles +1..3 K), dx=dz=200 m, UD3, dt=0.4 s",
+            "cells": cells, "steps": k, "input_prep_s": prep_s,
+            "fp64": {"value": cells / (ms64 * 1e-3), "ms_per_step": ms64, "stage_ms": s64,
+                     "stage_frac_of_measured_hbm": STAGE_BYTES * cells / (s64 * 1e-3) / 1e9 / hbm if s64 else None},
+            "mixed": {"value": cells / (ms32 * 1e-3), "ms_per_step": ms32, "stage_ms": s32,
+                      "stage_frac_of_measured_hbm": MIXED_STAGE_BYTES * cells / (s32 * 1e-3) / 1e9 / hbm if s32 else None,
+                      "step_frac_of_measured_hbm": (4 * MIXED_STAGE_BYTES + MIXED_NUMFILTER_BYTES) * cells
+                      / (ms32 * 1e-3) / 1e9 / hbm},
+            "speedup_mixed_vs_fp64": ms64 / ms32,
+            "error_vs_fp64": {"steps": warm + k, "fields": errs},
+            "autotune": hevi.autotune_report(),
+        }
+    finally:
+        hevi.finalize()
 
 
 def run_ensemble(args, hevi, torch):
@@ -619,6 +727,9 @@ def main():
     ap.add_argument("--ensemble-steps", type=int, default=20)
     ap.add_argument("--ensemble-scale", type=float, default=1.0, help="horizontal scale of the ensemble members")
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint gradient measurement")
+    ap.add_argument("--no-mixed-large", action="store_true", help="skip FP64 vs mixed on 1024x1024x96")
+    ap.add_argument("--mixed-large-steps", type=int, default=20)
+    ap.add_argument("--mixed-scale", type=float, default=1.0, help="horizontal scale of the 1024x1024x96 leg")
     ap.add_argument("--adjoint-steps", type=int, default=120)
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "b200":

@@ -176,6 +176,27 @@ def bubble(g: Grid, cx, cy, cz, rx, ry, rz):
     return np.asfortranarray(np.cos(0.5 * np.pi * np.sqrt(np.minimum(dist, 1.0))) ** 2)
 
 
+def add_bubble(theta: np.ndarray, g: Grid, cx, cy, cz, rx, ry, rz, amp) -> np.ndarray:
+    """theta + amp * bubble(...), evaluated only on the bubble's support.
+
+    Outside the support the cos**2 term is cos(pi/2)**2, about 4e-33, which
+    leaves a potential temperature of a few hundred K unchanged in FP64; so
+    the result equals the full-domain sum bit for bit (checked by the tests),
+    at a fraction of the cost on large domains."""
+    Lx = g.IMAX * g.DX
+    Ly = g.JMAX * g.DY
+    dz = ((g.CZ - cz) / rz) ** 2
+    dx = np.minimum(np.minimum(((g.CX - cx) / rx) ** 2, ((g.CX - cx - Lx) / rx) ** 2), ((g.CX - cx + Lx) / rx) ** 2)
+    dy = np.minimum(np.minimum(((g.CY - cy) / ry) ** 2, ((g.CY - cy - Ly) / ry) ** 2), ((g.CY - cy + Ly) / ry) ** 2)
+    kk, ii, jj = np.nonzero(dz < 1.0)[0], np.nonzero(dx < 1.0)[0], np.nonzero(dy < 1.0)[0]
+    if len(kk) == 0 or len(ii) == 0 or len(jj) == 0:
+        return theta
+    dist = dz[kk][:, None, None] + dx[ii][None, :, None] + dy[jj][None, None, :]
+    sel = np.ix_(kk, ii, jj)
+    theta[sel] = theta[sel] + amp * np.cos(0.5 * np.pi * np.sqrt(np.minimum(dist, 1.0))) ** 2
+    return theta
+
+
 def periodic_fill(a: np.ndarray, g: Grid):
     """Periodic lateral halo of one (KA,IA,JA) field (all k)."""
     I, J = g.IMAX, g.JMAX
@@ -235,7 +256,7 @@ def make_case(name: str, g: Grid, scheme="UD3", scheme_tracer="UD3", dt=1.0, dtl
     DENS = _bcast(base["dens"], g)
     theta = _bcast(base["pott"], g)
     for (cx, cy, cz, rx, ry, rz, amp) in bubbles:
-        theta = theta + amp * bubble(g, cx, cy, cz, rx, ry, rz)
+        theta = add_bubble(theta, g, cx, cy, cz, rx, ry, rz, amp)
     shp = g.shape
     low = (g.CZ <= noise_top)[:, None, None]
     if theta_noise > 0.0:

@@ -58,3 +58,21 @@ def test_ensemble_setup_argument_checks():
     bad = dict(idx, KE=idx["KE"] + 1)
     with pytest.raises(hevi.HeviError, match="inconsistent"):
         hevi.ensemble_setup([idx, bad])
+
+
+def test_bubble_on_its_support_equals_full_domain_sum():
+    """The input generator adds each warm bubble only where it is nonzero; the
+    state equals the full-domain formula bit for bit."""
+    rng = np.random.default_rng(3)
+    for g in (mkinit.uniform_grid(40, 40, 80, 500.0, 500.0, 250.0),
+              mkinit.stretched_grid(24, 20, 30, 250.0, 250.0, 50.0, 400.0)):
+        base = mkinit.base_state(g)
+        full = mkinit._bcast(base["pott"], g)
+        part = full.copy(order="F")
+        Lx, Ly = g.IMAX * g.DX, g.JMAX * g.DY
+        for _ in range(6):
+            b = (rng.uniform(0, Lx), rng.uniform(0, Ly), rng.uniform(500, 4000), rng.uniform(1e3, 6e3),
+                 rng.uniform(1e3, 6e3), rng.uniform(1e3, 4e3), rng.uniform(1, 4))
+            full = full + b[6] * mkinit.bubble(g, *b[:6])
+            part = mkinit.add_bubble(part, g, *b)
+        assert np.array_equal(full, part)
