@@ -24,7 +24,7 @@
  * periodic lateral boundaries (BND_* = .false.), flat terrain (GSQRT = 1,
  * J13G = J23G = 0, MAPF = 1, checked once per metric array), the default
  * IBLOCK/JBLOCK (whole domain), flux schemes "UD3", "CD4", "CD2" and
- * "UD3KOREN1993", ND_ORDER = 1,
+ * "UD3KOREN1993", ND_ORDER >= 1 (above 1 on the FP64 path of one domain),
  * 4 <= KMAX <= 256, halo width 2. No additional prognostic variables (VA = 0).
  *
  * Concurrency: one library state per process (like the reference's module
@@ -191,7 +191,8 @@ int ATMOS_DYN_numfilter_coef_b200_mixed_dev(SCALE_HEVI_NUMFILTER_MIXED_ARGS);
  * Numerical filter coefficients. Replaces ATMOS_DYN_numfilter_coef
  * (scalelib/src/atmos-rm/dynamics/scale_atmos_dyn_common.F90:385-985),
  * including the halo exchange of the fifteen num_diff components.
- * num_diff is (KA,IA,JA,5,3). ND_ORDER must be 1.
+ * num_diff is (KA,IA,JA,5,3). ND_ORDER 1..8; above 1 the differences are
+ * iterated with calc_diff4 (scale_atmos_dyn_common.F90:1518-1573, 1810-1918).
  * ------------------------------------------------------------------------- */
 #define SCALE_HEVI_NUMFILTER_ARGS                                                                              \
     double *num_diff,                                                                                          \

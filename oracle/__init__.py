@@ -159,7 +159,7 @@ def tinteg_tracer_rk3(g, scheme, QTRC, QTRC0, RHOQ_t, DENS0, DENS, mflx_hi, num_
 
 
 def tstep_large(g, scheme, scheme_tracer, st, out, tp, ref, aq, GSQRT, J13G, J23G, MAPF, CORIOLI, wdamp, dtl, dts,
-                ND_COEF=1e-4, divdmp=0.0, fct=False, along=True, QA=0):
+                ND_COEF=1e-4, divdmp=0.0, fct=False, along=True, QA=0, ND_ORDER=1):
     """Large step of the dynamics; st (DENS..RHOT, QTRC) is advanced in place."""
     QTRC = st.get("QTRC") if QA else None
     R, CV, CP, M = aq if QA else (None, None, None, None)
@@ -169,7 +169,8 @@ def tstep_large(g, scheme, scheme_tracer, st, out, tp, ref, aq, GSQRT, J13G, J23
                  tp["DENS_tp"], tp["MOMZ_tp"], tp["MOMX_tp"], tp["MOMY_tp"], tp["RHOT_tp"], tp.get("RHOQ_tp"),
                  CORIOLI, g.CDZ, g.CDX, g.CDY, g.FDZ, g.FDX, g.FDY, g.RCDZ, g.RCDX, g.RCDY, g.RFDZ, g.RFDX, g.RFDY,
                  ref["PHI"], GSQRT, J13G, J23G, 1.0, MAPF, R, CV, CP, M,
-                 ref["REF_dens"], ref["REF_pott"], ref["REF_pres"], float(ND_COEF), 1, 1.0, 1, wdamp, float(divdmp),
+                 ref["REF_dens"], ref["REF_pott"], ref["REF_pres"], float(ND_COEF), int(ND_ORDER), 1.0, 1, wdamp,
+                 float(divdmp),
                  int(fct), int(along), float(dtl), float(dts))
 
 

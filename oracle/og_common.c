@@ -1,9 +1,9 @@
 /*
  * Oracle restatement of the dynamics helpers in
  * scalelib/src/atmos-rm/dynamics/scale_atmos_dyn_common.F90:
- *   ATMOS_DYN_filter_setup (CNZ3/CNX3/CNY3)  :100-330
+ *   ATMOS_DYN_filter_setup (CNZ3/CNX3/CNY3, CNZ4/CNX4/CNY4) :100-330
  *   ATMOS_DYN_numfilter_coef                 :385-985
- *   calc_numdiff / calc_diff3                :1518-1760
+ *   calc_numdiff / calc_diff3 / calc_diff4   :1518-1918
  *   ATMOS_DYN_divergence                     :1437-1515
  *   ATMOS_DYN_fct / get_fact_fct             :1922-2734
  */
@@ -24,10 +24,14 @@ static double og_powi(double x, int m)
 /* ---------------- filter_setup: third-order difference coefficients ---------------- */
 typedef struct {
     double *CNZ3, *CNX3, *CNY3; /* (3,KA,2) (3,IA,2) (3,JA,2), 1-based */
+    double *CNZ4, *CNX4, *CNY4; /* (5,KA,2) (5,IA,2) (5,JA,2) */
 } cn3_t;
 #define CZ3(c, n, k, s) (c).CNZ3[((n) - 1) + 3 * ((size_t)((k) - 1) + (size_t)KA * ((s) - 1))]
 #define CX3(c, n, i, s) (c).CNX3[((n) - 1) + 3 * ((size_t)((i) - 1) + (size_t)IA * ((s) - 1))]
 #define CY3(c, n, j, s) (c).CNY3[((n) - 1) + 3 * ((size_t)((j) - 1) + (size_t)JA * ((s) - 1))]
+#define CZ4(c, n, k, s) (c).CNZ4[((n) - 1) + 5 * ((size_t)((k) - 1) + (size_t)KA * ((s) - 1))]
+#define CX4(c, n, i, s) (c).CNX4[((n) - 1) + 5 * ((size_t)((i) - 1) + (size_t)IA * ((s) - 1))]
+#define CY4(c, n, j, s) (c).CNY4[((n) - 1) + 5 * ((size_t)((j) - 1) + (size_t)JA * ((s) - 1))]
 
 static int cn3_setup(const og_dims *d, cn3_t *c, const double *CDZ, const double *CDX, const double *CDY,
                      const double *FDZ, const double *FDX, const double *FDY)
@@ -36,7 +40,10 @@ static int cn3_setup(const og_dims *d, cn3_t *c, const double *CDZ, const double
     c->CNZ3 = og_alloc_undef(3 * (size_t)KA * 2);
     c->CNX3 = og_alloc_undef(3 * (size_t)IA * 2);
     c->CNY3 = og_alloc_undef(3 * (size_t)JA * 2);
-    if (!c->CNZ3 || !c->CNX3 || !c->CNY3) return -1;
+    c->CNZ4 = og_alloc_undef(5 * (size_t)KA * 2);
+    c->CNX4 = og_alloc_undef(5 * (size_t)IA * 2);
+    c->CNY4 = og_alloc_undef(5 * (size_t)JA * 2);
+    if (!c->CNZ3 || !c->CNX3 || !c->CNY3 || !c->CNZ4 || !c->CNX4 || !c->CNY4) return -1;
     cn3_t C = *c;
 #define cdz(k) CDZ[(k) - 1]
 #define fdz(k) FDZ[(k) - 1]
@@ -125,6 +132,35 @@ static int cn3_setup(const og_dims *d, cn3_t *c, const double *CDZ, const double
         CY3(C, 3, j, 2) = 1.0 / (cdy(j) * fdy(j) * cdy(j)) + 1.0 / (cdy(j) * fdy(j - 1) * cdy(j))
                           + 1.0 / (cdy(j) * fdy(j - 1) * cdy(j - 1));
     }
+    /* fourth-order coefficients (:186-193, :253-263, :281-297, :309-317): the
+     * second kind of z, x and y divides by FDZ/FDX/FDY, the first by CDZ/CDX/CDY */
+    for (int s = 1; s <= 2; ++s)
+        for (int k = KS; k <= KE - 1; ++k) {
+            const double den = s == 1 ? cdz(k) : fdz(k);
+            CZ4(C, 1, k, s) = (CZ3(C, 1, k + 1, s)) / den;
+            CZ4(C, 2, k, s) = (CZ3(C, 2, k + 1, s) + CZ3(C, 1, k, s)) / den;
+            CZ4(C, 3, k, s) = (CZ3(C, 3, k + 1, s) + CZ3(C, 2, k, s)) / den;
+            CZ4(C, 4, k, s) = (CZ3(C, 1, k, s) + CZ3(C, 3, k, s)) / den;
+            CZ4(C, 5, k, s) = (CZ3(C, 1, k - 1, s)) / den;
+        }
+    for (int s = 1; s <= 2; ++s)
+        for (int i = IS; i <= IE; ++i) {
+            const double den = s == 1 ? cdx(i) : fdx(i);
+            CX4(C, 1, i, s) = (CX3(C, 1, i + 1, s)) / den;
+            CX4(C, 2, i, s) = (CX3(C, 2, i + 1, s) + CX3(C, 1, i, s)) / den;
+            CX4(C, 3, i, s) = (CX3(C, 3, i + 1, s) + CX3(C, 2, i, s)) / den;
+            CX4(C, 4, i, s) = (CX3(C, 1, i, s) + CX3(C, 3, i, s)) / den;
+            CX4(C, 5, i, s) = (CX3(C, 1, i - 1, s)) / den;
+        }
+    for (int s = 1; s <= 2; ++s)
+        for (int j = JS; j <= JE; ++j) {
+            const double den = s == 1 ? cdy(j) : fdy(j);
+            CY4(C, 1, j, s) = (CY3(C, 1, j + 1, s)) / den;
+            CY4(C, 2, j, s) = (CY3(C, 2, j + 1, s) + CY3(C, 1, j, s)) / den;
+            CY4(C, 3, j, s) = (CY3(C, 3, j + 1, s) + CY3(C, 2, j, s)) / den;
+            CY4(C, 4, j, s) = (CY3(C, 1, j, s) + CY3(C, 3, j, s)) / den;
+            CY4(C, 5, j, s) = (CY3(C, 1, j - 1, s)) / den;
+        }
 #undef cdz
 #undef fdz
 #undef cdx
@@ -133,7 +169,11 @@ static int cn3_setup(const og_dims *d, cn3_t *c, const double *CDZ, const double
 #undef fdy
     return 0;
 }
-static void cn3_free(cn3_t *c) { free(c->CNZ3); free(c->CNX3); free(c->CNY3); }
+static void cn3_free(cn3_t *c)
+{
+    free(c->CNZ3); free(c->CNX3); free(c->CNY3);
+    free(c->CNZ4); free(c->CNX4); free(c->CNY4);
+}
 
 /* calc_diff3, :1600-1760; diff is (KA,IA,JA,3) */
 static void calc_diff3(const og_dims *d, const cn3_t *c, double *diff, const double *phi, int KO, int IO, int JO)
@@ -215,8 +255,56 @@ static void calc_diff3(const og_dims *d, const cn3_t *c, double *diff, const dou
         }
 }
 
-/* numfilter_coef, :385-985. Only ND_ORDER = 1 (the model default) is restated:
- * calc_numdiff then reduces to calc_diff3. Returns -2 for other orders. */
+/* calc_diff4, :1810-1918: out = fourth difference of in, z on KS..KE-1 with the
+ * mirrored levels KS-1, KS-2, KE, KE+1, x and y on KS..K1; interior columns */
+static void calc_diff4(const og_dims *d, const cn3_t *c, double *out, const double *in, int KO, int IO, int JO, int K1)
+{
+    OG_DIMS(d);
+    const cn3_t C = *c;
+    double *oZ = out, *oX = out + N3, *oY = out + 2 * N3;
+    const double *iZ = in, *iX = in + N3, *iY = in + 2 * N3;
+    const int sz = 1 + KO, sx = 1 + IO, sy = 1 + JO;
+#pragma omp parallel for collapse(2)
+    for (int j = JS; j <= JE; ++j)
+        for (int i = IS; i <= IE; ++i) {
+            for (int k = KS; k <= KE - 1; ++k)
+                oZ[I3(k, i, j)] = (CZ4(C, 1, k, sz) * iZ[I3(k + 2, i, j)] - CZ4(C, 2, k, sz) * iZ[I3(k + 1, i, j)]
+                                   + CZ4(C, 3, k, sz) * iZ[I3(k, i, j)] - CZ4(C, 4, k, sz) * iZ[I3(k - 1, i, j)]
+                                   + CZ4(C, 5, k, sz) * iZ[I3(k - 2, i, j)]);
+            oZ[I3(KS - 1, i, j)] = -oZ[I3(KS, i, j)];
+            oZ[I3(KS - 2, i, j)] = -oZ[I3(KS + 1, i, j)];
+            oZ[I3(KE, i, j)] = -oZ[I3(KE - 1, i, j)];
+            oZ[I3(KE + 1, i, j)] = -oZ[I3(KE - 2, i, j)];
+            for (int k = KS; k <= K1; ++k) {
+                oX[I3(k, i, j)] = (CX4(C, 1, i, sx) * iX[I3(k, i + 2, j)] - CX4(C, 2, i, sx) * iX[I3(k, i + 1, j)]
+                                   + CX4(C, 3, i, sx) * iX[I3(k, i, j)] - CX4(C, 4, i, sx) * iX[I3(k, i - 1, j)]
+                                   + CX4(C, 5, i, sx) * iX[I3(k, i - 2, j)]);
+                oY[I3(k, i, j)] = (CY4(C, 1, j, sy) * iY[I3(k, i, j + 2)] - CY4(C, 2, j, sy) * iY[I3(k, i, j + 1)]
+                                   + CY4(C, 3, j, sy) * iY[I3(k, i, j)] - CY4(C, 4, j, sy) * iY[I3(k, i, j - 1)]
+                                   + CY4(C, 5, j, sy) * iY[I3(k, i, j - 2)]);
+            }
+        }
+}
+
+/* calc_numdiff, :1518-1573: calc_diff3, then nd_order-1 times the periodic halo
+ * of the three components (COMM_vars8, one rank) and calc_diff4. Returns the
+ * buffer (w1 or w2) that holds the result. */
+static double *calc_numdiff(const og_dims *d, const cn3_t *c, double *w1, double *w2, const double *data, int nd_order,
+                            int KO, int IO, int JO)
+{
+    calc_diff3(d, c, w1, data, KO, IO, JO);
+    double *in = w1, *out = w2;
+    for (int no = 2; no <= nd_order; ++no) {
+        og_halo_periodic(d, in, 3);
+        calc_diff4(d, c, out, in, KO, IO, JO, d->KE - KO);
+        double *t = in;
+        in = out;
+        out = t;
+    }
+    return in;
+}
+
+/* numfilter_coef, :385-985, for any ND_ORDER >= 1. */
 int og_numfilter_coef(
     const og_dims *d, double *num_diff,
     const double *DENS, const double *MOMZ, const double *MOMX, const double *MOMY, const double *RHOT,
@@ -226,14 +314,15 @@ int og_numfilter_coef(
     double ND_COEF, int ND_ORDER, double ND_SFC_FACT, int ND_USE_RS)
 {
     OG_DIMS(d);
-    if (ND_ORDER != 1) return -2;
+    if (ND_ORDER < 1) return -2;
     cn3_t cn;
     if (cn3_setup(d, &cn, CDZ, CDX, CDY, FDZ, FDX, FDY)) { cn3_free(&cn); return -1; }
-    double *work = og_alloc_undef(3 * N3), *tmp = og_alloc_undef(N3), *tmp2 = og_alloc_undef(N3);
+    double *work = og_alloc_undef(3 * N3), *work2 = og_alloc_undef(3 * N3), *tmp = og_alloc_undef(N3),
+           *tmp2 = og_alloc_undef(N3);
     double *ncz = og_alloc_undef(KA), *nfz = og_alloc_undef(KA), *ncx = og_alloc_undef(IA), *nfx = og_alloc_undef(IA);
     double *ncy = og_alloc_undef(JA), *nfy = og_alloc_undef(JA);
-    if (!work || !tmp || !tmp2 || !ncz || !nfz || !ncx || !nfx || !ncy || !nfy) {
-        free(work); free(tmp); free(tmp2); free(ncz); free(nfz); free(ncx); free(nfx); free(ncy); free(nfy);
+    if (!work || !work2 || !tmp || !tmp2 || !ncz || !nfz || !ncx || !nfx || !ncy || !nfy) {
+        free(work); free(work2); free(tmp); free(tmp2); free(ncz); free(nfz); free(ncx); free(nfx); free(ncy); free(nfy);
         cn3_free(&cn);
         return -1;
     }
@@ -249,7 +338,12 @@ int og_numfilter_coef(
         ncy[j - 1] = DIFF4 * og_powi(CDY[j - 1], nd_order4);
         nfy[j - 1] = DIFF4 * og_powi(FDY[j - 1], nd_order4);
     }
-    double *wZ = work, *wX = work + N3, *wY = work + 2 * N3;
+    double *wZ = work, *wX = work + N3, *wY = work + 2 * N3, *wres = work;
+#define NUMDIFF(data, KO, IO, JO)                                                    \
+    do {                                                                             \
+        wres = calc_numdiff(d, &cn, work, work2, (data), ND_ORDER, (KO), (IO), (JO)); \
+        wZ = wres; wX = wres + N3; wY = wres + 2 * N3;                               \
+    } while (0)
 #define NDF(v, dir) ND(num_diff, v, dir)
     /* lateral zeroing and surface factors shared by the x/y components */
 #define SFC_TAIL(nd, kzero_top)                                                   \
@@ -301,7 +395,7 @@ int og_numfilter_coef(
     }
 
     /* ---- density :552-610 ---- */
-    calc_diff3(d, &cn, work, dens_diff, 0, 0, 0);
+    NUMDIFF(dens_diff, 0, 0, 0);
     {
         double *nz = NDF(I_DENS, ZDIR), *nx = NDF(I_DENS, XDIR), *ny = NDF(I_DENS, YDIR);
 #pragma omp parallel for collapse(2)
@@ -326,7 +420,7 @@ int og_numfilter_coef(
             for (int i = IS - 2; i <= IE + 2; ++i)
                 for (int k = KS; k <= KE - 1; ++k)
                     VELZ[I3(k, i, j)] = 2.0 * MOMZ[I3(k, i, j)] / (DENS[I3(k + 1, i, j)] + DENS[I3(k, i, j)]);
-        calc_diff3(d, &cn, work, VELZ, 1, 0, 0);
+        NUMDIFF(VELZ, 1, 0, 0);
         double *nz = NDF(I_MOMZ, ZDIR), *nx = NDF(I_MOMZ, XDIR), *ny = NDF(I_MOMZ, YDIR);
 #pragma omp parallel for collapse(2)
         for (int j = JS; j <= JE; ++j)
@@ -354,7 +448,7 @@ int og_numfilter_coef(
             for (int i = IS - 2; i <= IE + 1; ++i)
                 for (int k = KS; k <= KE; ++k)
                     VELX[I3(k, i, j)] = 2.0 * MOMX[I3(k, i, j)] / (DENS[I3(k, i + 1, j)] + DENS[I3(k, i, j)]);
-        calc_diff3(d, &cn, work, VELX, 0, 1, 0);
+        NUMDIFF(VELX, 0, 1, 0);
         double *nz = NDF(I_MOMX, ZDIR), *nx = NDF(I_MOMX, XDIR), *ny = NDF(I_MOMX, YDIR);
 #pragma omp parallel for collapse(2)
         for (int j = JS; j <= JE; ++j)
@@ -382,7 +476,7 @@ int og_numfilter_coef(
             for (int i = IS - 2; i <= IE + 2; ++i)
                 for (int k = KS; k <= KE; ++k)
                     VELY[I3(k, i, j)] = 2.0 * MOMY[I3(k, i, j)] / (DENS[I3(k, i, j + 1)] + DENS[I3(k, i, j)]);
-        calc_diff3(d, &cn, work, VELY, 0, 0, 1);
+        NUMDIFF(VELY, 0, 0, 1);
         double *nz = NDF(I_MOMY, ZDIR), *nx = NDF(I_MOMY, XDIR), *ny = NDF(I_MOMY, YDIR);
 #pragma omp parallel for collapse(2)
         for (int j = JS; j <= JE; ++j)
@@ -410,7 +504,7 @@ int og_numfilter_coef(
                 for (int k = KS; k <= KE; ++k)
                     pott_diff[I3(k, i, j)] = RHOT[I3(k, i, j)] / DENS[I3(k, i, j)] - REF_pott[I3(k, i, j)];
     }
-    calc_diff3(d, &cn, work, pott_diff, 0, 0, 0);
+    NUMDIFF(pott_diff, 0, 0, 0);
     {
         double *nz = NDF(I_RHOT, ZDIR), *nx = NDF(I_RHOT, XDIR), *ny = NDF(I_RHOT, YDIR);
 #pragma omp parallel for collapse(2)
@@ -433,7 +527,9 @@ int og_numfilter_coef(
     }
 #undef SFC_TAIL
 #undef NDF
-    free(work); free(tmp); free(tmp2); free(ncz); free(nfz); free(ncx); free(nfx); free(ncy); free(nfy);
+#undef NUMDIFF
+    (void)wres;
+    free(work); free(work2); free(tmp); free(tmp2); free(ncz); free(nfz); free(ncx); free(nfx); free(ncy); free(nfy);
     cn3_free(&cn);
     return 0;
 }

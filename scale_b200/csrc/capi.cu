@@ -55,6 +55,7 @@ struct Ctx {
     double *facc = nullptr;         // 6*N3
     double *colscr = nullptr;       // 3*N3 when HEVI_COL_SCRATCH
     double *phi = nullptr;          // numerical filter: 5*N3 (allocated on first use)
+    double *ndw = nullptr;          // numerical filter at ND_ORDER > 1: 2 x 15*N3 work (on first use)
     // mixed-precision path (allocated on first use): flux RK sums, column-solve
     // sources and the filtered quantities in FP32
     float *facc_f = nullptr, *colscr_f = nullptr, *phi_f = nullptr;
@@ -171,7 +172,7 @@ int falloc(float **p, size_t n)
 
 void free_all()
 {
-    double *bufs[] = {C.phi, C.colscr, C.d_tab, C.d_nd, C.rk[0], C.rk[1], C.acc, C.facc, C.tr, C.lg, C.sum_part, C.sum_out};
+    double *bufs[] = {C.phi, C.ndw, C.colscr, C.d_tab, C.d_nd, C.rk[0], C.rk[1], C.acc, C.facc, C.tr, C.lg, C.sum_part, C.sum_out};
     for (double *b : bufs) if (b) cudaFree(b);
     for (auto &kv : C.stage) cudaFree(kv.second.first);
     for (float *b : {C.facc_f, C.colscr_f, C.phi_f}) if (b) cudaFree(b);
@@ -324,8 +325,10 @@ int prepare_nd(const double *CDZ, const double *CDX, const double *CDY, const do
     // each), cdx fdx (XT), cdy fdy (YT); member m at 6*z0 / z0 / ...
     const size_t oX3 = 6 * ZT, oY3 = oX3 + 6 * XT, ocdz = oY3 + 6 * YT, ofdz = ocdz + ZT, ocdx = ofdz + ZT,
                  ofdx = ocdx + XT, ocdy = ofdx + XT, ofdy = ocdy + YT;
+    // then the calc_diff4 coefficients CNZ4, CNX4, CNY4 (10 values per level or point)
+    const size_t oZ4 = ofdy + YT, oX4 = oZ4 + 10 * ZT, oY4 = oX4 + 10 * XT, oend = oY4 + 10 * YT;
     if (key != C.nd_key) {
-        std::vector<double> h(ofdy + YT, 0.0);
+        std::vector<double> h(oend, 0.0);
         for (const MemberGeom &m : C.members) {
             const int KA = m.KMAX + 4, IA = m.IMAX + 4, JA = m.JMAX + 4, z0 = m.z0, x0 = m.x0, y0 = m.y0;
             NdGrid gr{KA, IA, JA, 3, m.KMAX + 2, 3, m.IMAX + 2, 3, m.JMAX + 2,
@@ -336,6 +339,7 @@ int prepare_nd(const double *CDZ, const double *CDX, const double *CDY, const do
             put(t.CNZ3, 6 * (size_t)z0); put(t.CNX3, oX3 + 6 * (size_t)x0); put(t.CNY3, oY3 + 6 * (size_t)y0);
             put(t.cdz, ocdz + z0); put(t.fdz, ofdz + z0); put(t.cdx, ocdx + x0); put(t.fdx, ofdx + x0);
             put(t.cdy, ocdy + y0); put(t.fdy, ofdy + y0);
+            put(t.CNZ4, oZ4 + 10 * (size_t)z0); put(t.CNX4, oX4 + 10 * (size_t)x0); put(t.CNY4, oY4 + 10 * (size_t)y0);
         }
         CU(cudaMemcpyAsync(C.d_nd, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice, C.stream));
         CU(cudaStreamSynchronize(C.stream));
@@ -346,6 +350,8 @@ int prepare_nd(const double *CDZ, const double *CDX, const double *CDY, const do
     C.ndc.cdz = p + ocdz; C.ndc.fdz = p + ofdz; C.ndc.cdx = p + ocdx; C.ndc.fdx = p + ofdx;
     C.ndc.cdy = p + ocdy; C.ndc.fdy = p + ofdy;
     C.ndc.sfc = SFC;
+    C.ndc.CNZ4 = p + oZ4; C.ndc.CNX4 = p + oX4; C.ndc.CNY4 = p + oY4;
+    C.ndc.order = ND_ORDER;
     return SCALE_HEVI_OK;
 }
 
@@ -509,6 +515,22 @@ int run_numfilter(R *num_diff, const double *DENS, const double *MOMZ, const dou
         if (!C.phi_f) CK(falloc(&C.phi_f, 5 * C.N3));
         phi = reinterpret_cast<R *>(C.phi_f);
     }
+    if (C.ndc.order > 1) {
+        if (sizeof(R) != sizeof(double))
+            return fail(SCALE_HEVI_ERR_UNSUPPORTED, "ND_ORDER > 1 is supported on the FP64 path only");
+        if (C.members.size() > 1) return fail(SCALE_HEVI_ERR_UNSUPPORTED, "ND_ORDER > 1 is not available for an ensemble");
+        if (!C.ndw) CK(dalloc(&C.ndw, 30 * C.N3));
+        NdArgs ah{reinterpret_cast<double *>(num_diff), DENS, MOMZ, MOMX, MOMY, RHOT, REF_dens, REF_pott,
+                  reinterpret_cast<double *>(phi)};
+        CK(timed("numfilter", [&] {
+            CU(launch_numfilter_high(C.g, C.ndc, ah, C.ndw, C.ndw + 15 * C.N3, C.stream));
+            return SCALE_HEVI_OK;
+        }));
+        C.launches += 3 + 2 * (C.ndc.order - 1);
+        R *f[15];
+        for (int q = 0; q < 15; ++q) f[q] = num_diff + (size_t)q * C.N3;
+        return halo(f, 15);
+    }
     NdArgsT<R> a{num_diff, DENS, MOMZ, MOMX, MOMY, RHOT, REF_dens, REF_pott, phi};
     CK(timed(sizeof(R) == sizeof(double) ? "numfilter" : "numfilter_mixed", [&] {
         CU(launch_numfilter(C.g, mem(), C.ndc, a, C.stream));
@@ -639,7 +661,7 @@ int scale_hevi_ensemble_setup(int n, const scale_hevi_index *idx, const char *fl
     CU(cudaStreamCreate(&C.stream));
     int rc = SCALE_HEVI_OK;
     if ((rc = dalloc(&C.d_tab, 7 * (size_t)ZT + 4 * (size_t)XT + 4 * (size_t)YT)) ||
-        (rc = dalloc(&C.d_nd, 8 * (size_t)ZT + 8 * (size_t)XT + 8 * (size_t)YT)) ||
+        (rc = dalloc(&C.d_nd, 18 * (size_t)ZT + 18 * (size_t)XT + 18 * (size_t)YT)) ||
         (rc = dalloc(&C.rk[0], 5 * N3)) || (rc = dalloc(&C.rk[1], 5 * N3)) ||
         (rc = dalloc(&C.acc, 5 * N3)) || (rc = dalloc(&C.facc, 6 * N3)) ||
         (HEVI_COL_SCRATCH && (rc = dalloc(&C.colscr, 3 * N3))) ||
@@ -874,7 +896,7 @@ int ATMOS_DYN_numfilter_coef_b200_mixed_dev(SCALE_HEVI_NUMFILTER_MIXED_ARGS)
 int ATMOS_DYN_numfilter_coef_b200_dev(SCALE_HEVI_NUMFILTER_ARGS)
 {
     CK(need_setup());
-    if (*ND_ORDER != 1) return fail(SCALE_HEVI_ERR_UNSUPPORTED, "ND_ORDER=%d is not supported (1 only)", *ND_ORDER);
+    if (*ND_ORDER < 1 || *ND_ORDER > 8) return fail(SCALE_HEVI_ERR_UNSUPPORTED, "ND_ORDER=%d is not supported (1..8)", *ND_ORDER);
     if (!*ND_USE_RS) return fail(SCALE_HEVI_ERR_UNSUPPORTED, "ND_USE_RS=.false. is not supported");
     CK(prepare_nd(CDZ, CDX, CDY, FDZ, FDX, FDY, *DT, *ND_COEF, *ND_ORDER, *ND_SFC_FACT));
     return run_numfilter(num_diff, DENS, MOMZ, MOMX, MOMY, RHOT, REF_dens, REF_pott);
@@ -1065,7 +1087,8 @@ int ATMOS_DYN_Tstep_large_fvm_heve_b200_dev(SCALE_HEVI_LARGE_ARGS)
     CK(need_single("the large step"));
     const int qa = *QA;
     if (qa < 0 || qa > 8) return fail(SCALE_HEVI_ERR_UNSUPPORTED, "QA=%d (0..8 supported)", qa);
-    if (*ND_COEF != 0.0 && *ND_ORDER != 1) return fail(SCALE_HEVI_ERR_UNSUPPORTED, "ND_ORDER=%d is not supported", *ND_ORDER);
+    if (*ND_COEF != 0.0 && (*ND_ORDER < 1 || *ND_ORDER > 8))
+        return fail(SCALE_HEVI_ERR_UNSUPPORTED, "ND_ORDER=%d is not supported (1..8)", *ND_ORDER);
     if (*ND_COEF != 0.0 && !*ND_USE_RS) return fail(SCALE_HEVI_ERR_UNSUPPORTED, "ND_USE_RS=.false. is not supported");
     CK(check_flat(GSQRT, J13G, J23G, MAPF, true));
     const size_t N3 = C.N3;

@@ -121,6 +121,41 @@ void build_nd_tables(const NdGrid &gr, double DT, double ND_COEF, int ND_ORDER, 
         cy(3, j, 2) = 1.0 / (CDY(j) * FDY(j) * CDY(j)) + 1.0 / (CDY(j) * FDY(j - 1) * CDY(j)) + 1.0 / (CDY(j) * FDY(j - 1) * CDY(j - 1));
     }
 
+    // fourth-order coefficients of calc_diff4 (:186-193, :253-263, :281-297, :309-317):
+    // the first kind divides by CDZ/CDX/CDY, the second by FDZ/FDX/FDY
+    t.CNZ4.assign(5 * (size_t)KA * 2, 0.0);
+    t.CNX4.assign(5 * (size_t)IA * 2, 0.0);
+    t.CNY4.assign(5 * (size_t)JA * 2, 0.0);
+    auto c4 = [](std::vector<double> &v, int N, int n, int p, int s) -> double & {
+        return v[(n - 1) + 5 * ((size_t)(p - 1) + (size_t)N * (s - 1))];
+    };
+    for (int s = 1; s <= 2; ++s) {
+        for (int k = KS; k <= KE - 1; ++k) {
+            const double den = s == 1 ? CDZ(k) : FDZ(k);
+            c4(t.CNZ4, KA, 1, k, s) = (cz(1, k + 1, s)) / den;
+            c4(t.CNZ4, KA, 2, k, s) = (cz(2, k + 1, s) + cz(1, k, s)) / den;
+            c4(t.CNZ4, KA, 3, k, s) = (cz(3, k + 1, s) + cz(2, k, s)) / den;
+            c4(t.CNZ4, KA, 4, k, s) = (cz(1, k, s) + cz(3, k, s)) / den;
+            c4(t.CNZ4, KA, 5, k, s) = (cz(1, k - 1, s)) / den;
+        }
+        for (int i = IS; i <= IE; ++i) {
+            const double den = s == 1 ? CDX(i) : FDX(i);
+            c4(t.CNX4, IA, 1, i, s) = (cx(1, i + 1, s)) / den;
+            c4(t.CNX4, IA, 2, i, s) = (cx(2, i + 1, s) + cx(1, i, s)) / den;
+            c4(t.CNX4, IA, 3, i, s) = (cx(3, i + 1, s) + cx(2, i, s)) / den;
+            c4(t.CNX4, IA, 4, i, s) = (cx(1, i, s) + cx(3, i, s)) / den;
+            c4(t.CNX4, IA, 5, i, s) = (cx(1, i - 1, s)) / den;
+        }
+        for (int j = JS; j <= JE; ++j) {
+            const double den = s == 1 ? CDY(j) : FDY(j);
+            c4(t.CNY4, JA, 1, j, s) = (cy(1, j + 1, s)) / den;
+            c4(t.CNY4, JA, 2, j, s) = (cy(2, j + 1, s) + cy(1, j, s)) / den;
+            c4(t.CNY4, JA, 3, j, s) = (cy(3, j + 1, s) + cy(2, j, s)) / den;
+            c4(t.CNY4, JA, 4, j, s) = (cy(1, j, s) + cy(3, j, s)) / den;
+            c4(t.CNY4, JA, 5, j, s) = (cy(1, j - 1, s)) / den;
+        }
+    }
+
     // nd_coef_* (:444-463): DIFF4 = ND_COEF / (2**(4*order) * DT), coef = DIFF4 * D**(4*order)
     const int n4 = ND_ORDER * 4;
     const double DIFF4 = ND_COEF / (powi(2.0, n4) * DT);

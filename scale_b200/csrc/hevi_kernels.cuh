@@ -52,8 +52,10 @@ __device__ __forceinline__ Block2 split_block(int b, int gx) { return {b % gx, b
 // CNZ3(3,KA,2), CNX3(3,IA,2), CNY3(3,JA,2) and the nd_coef_* vectors
 struct NdCoef {
     const double *CNZ3, *CNX3, *CNY3;
-    const double *cdz, *fdz, *cdx, *fdx, *cdy, *fdy; // DIFF4 * D**4 (nd_coef_cdz, ...)
+    const double *cdz, *fdz, *cdx, *fdx, *cdy, *fdy; // DIFF4 * D**(4*order) (nd_coef_cdz, ...)
     double sfc;                                      // ND_SFC_FACT
+    const double *CNZ4, *CNX4, *CNY4;                // calc_diff4 coefficients (5,KA,2) ...
+    int order;                                       // ND_ORDER
 };
 template <typename R>
 struct NdArgsT {
@@ -64,6 +66,12 @@ struct NdArgsT {
 using NdArgs = NdArgsT<double>;
 template <typename R>
 cudaError_t launch_numfilter(const Grid &g, const Members &mem, const NdCoef &c, const NdArgsT<R> &a, cudaStream_t st);
+// ND_ORDER > 1 (FP64, one domain): the differences of the five quantities go
+// through work buffers w1/w2 (15 fields each; component 3*q + dir, dir 0 z,
+// 1 x, 2 y) and ND_ORDER-1 applications of calc_diff4 with the periodic halo
+// before each; num_diff is then formed from the last one
+cudaError_t launch_numfilter_high(const Grid &g, const NdCoef &c, const NdArgs &a, double *w1, double *w2,
+                                  cudaStream_t st);
 // the member's coefficient tables in the pooled ones (per member: CN*3 hold
 // 6 values per level or point, the nd_coef_* vectors one)
 __host__ __device__ __forceinline__ NdCoef member_nd(const NdCoef &c, const Grid &g)
@@ -71,6 +79,7 @@ __host__ __device__ __forceinline__ NdCoef member_nd(const NdCoef &c, const Grid
     NdCoef m = c;
     m.CNZ3 += 6 * (size_t)g.z0; m.CNX3 += 6 * (size_t)g.x0; m.CNY3 += 6 * (size_t)g.y0;
     m.cdz += g.z0; m.fdz += g.z0; m.cdx += g.x0; m.fdx += g.x0; m.cdy += g.y0; m.fdy += g.y0;
+    m.CNZ4 += 10 * (size_t)g.z0; m.CNX4 += 10 * (size_t)g.x0; m.CNY4 += 10 * (size_t)g.y0;
     return m;
 }
 

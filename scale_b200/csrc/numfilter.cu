@@ -143,9 +143,11 @@ __device__ __forceinline__ R dy(const Grid &g, const NdCoef &c, const Phi<R> &ph
 #define HEVI_ND_MINB 8 // minimum resident blocks per SM asked of the register allocator
 #endif
 
-template <typename R, int NM>
+// FW: the differences come from the calc_numdiff work buffer W (ND_ORDER > 1)
+// instead of being formed from phi here (ND_ORDER = 1)
+template <typename R, int NM, bool FW = false>
 __global__ void __launch_bounds__(128, HEVI_ND_MINB)
-    k_numfilter(const Grid gt, const NdCoef ct, const NdArgsT<R> a, const BatchT<NM> B)
+    k_numfilter(const Grid gt, const NdCoef ct, const NdArgsT<R> a, const BatchT<NM> B, const double *W = nullptr)
 {
     int b;
     const Grid g = block_domain(gt, B, b);
@@ -169,54 +171,149 @@ __global__ void __launch_bounds__(128, HEVI_ND_MINB)
     };
     for (int k = 1 + threadIdx.x; k <= g.KA; k += 32) {
         const size_t o = idx3(g, k, i, j);
+        // the difference of quantity q in a direction: formed here from phi, or
+        // read from the work buffer (the expression is then not evaluated)
+#define DZ(q, expr) (FW ? R(ld(W + (size_t)(3 * (q) + 0) * N3 + o)) : (expr))
+#define DX(q, expr) (FW ? R(ld(W + (size_t)(3 * (q) + 1) * N3 + o)) : (expr))
+#define DY(q, expr) (FW ? R(ld(W + (size_t)(3 * (q) + 2) * N3 + o)) : (expr))
         const R ncz = (k >= KS - 1 && k <= KE) ? R(ld(c.cdz + k - 1)) : R(0.0);
         R *ND = a.num_diff;
         const bool kin = (k >= KS && k <= KE);
         // ---- density (:553-610) ----
-        ND[o + N3 * 0] = (k >= KS - 1 && k <= KE) ? dz0(g, c, phi, 0, k, i, j) * ncz : R(0.0);
-        ND[o + N3 * 5] = kin ? sfct(k, dx(g, c, phi, 0, 0, k, i, j) * ncx) : R(0.0);
-        ND[o + N3 * 10] = kin ? sfct(k, dy(g, c, phi, 0, 0, k, i, j) * ncy) : R(0.0);
+        ND[o + N3 * 0] = (k >= KS - 1 && k <= KE) ? DZ(0, dz0(g, c, phi, 0, k, i, j)) * ncz : R(0.0);
+        ND[o + N3 * 5] = kin ? sfct(k, DX(0, dx(g, c, phi, 0, 0, k, i, j)) * ncx) : R(0.0);
+        ND[o + N3 * 10] = kin ? sfct(k, DY(0, dy(g, c, phi, 0, 0, k, i, j)) * ncy) : R(0.0);
         // ---- z momentum (:628-698), phi = VELZ on KS..KE-1 ----
         {
             const bool kz = (k >= KS && k <= KE - 1);
             const R nfz = (k >= KS + 1 && k <= KE - 1) ? R(ld(c.fdz + k - 1)) : R(0.0);
-            ND[o + N3 * 1] = (k >= KS + 1 && k <= KE - 1) ? dz1(g, c, phi, 1, k, i, j) * nfz * R(ld(DN + o)) : R(0.0);
-            ND[o + N3 * 6] = kz ? sfct(k, dx(g, c, phi, 1, 0, k, i, j) * ncx
+            ND[o + N3 * 1] = (k >= KS + 1 && k <= KE - 1) ? DZ(1, dz1(g, c, phi, 1, k, i, j)) * nfz * R(ld(DN + o)) : R(0.0);
+            ND[o + N3 * 6] = kz ? sfct(k, DX(1, dx(g, c, phi, 1, 0, k, i, j)) * ncx
                                               * R(0.25) * (R(ld(DN + o + 1 + sI)) + R(ld(DN + o + 1)) + R(ld(DN + o + sI)) + R(ld(DN + o))))
                                 : R(0.0);
-            ND[o + N3 * 11] = kz ? sfct(k, dy(g, c, phi, 1, 0, k, i, j) * ncy
+            ND[o + N3 * 11] = kz ? sfct(k, DY(1, dy(g, c, phi, 1, 0, k, i, j)) * ncy
                                                * R(0.25) * (R(ld(DN + o + 1 + sJ)) + R(ld(DN + o + 1)) + R(ld(DN + o + sJ)) + R(ld(DN + o))))
                                  : R(0.0);
         }
         // ---- x momentum (:728-790), phi = VELX ----
         ND[o + N3 * 2] = (k >= KS && k <= KE - 1)
-                             ? dz0(g, c, phi, 2, k, i, j) * ncz
+                             ? DZ(2, dz0(g, c, phi, 2, k, i, j)) * ncz
                                    * R(0.25) * (R(ld(DN + o + 1 + sI)) + R(ld(DN + o + 1)) + R(ld(DN + o + sI)) + R(ld(DN + o)))
                              : R(0.0);
-        ND[o + N3 * 7] = kin ? sfct(k, dx(g, c, phi, 2, 1, k, i, j) * nfx * R(ld(DN + o))) : R(0.0);
-        ND[o + N3 * 12] = kin ? sfct(k, dy(g, c, phi, 2, 0, k, i, j) * ncy
+        ND[o + N3 * 7] = kin ? sfct(k, DX(2, dx(g, c, phi, 2, 1, k, i, j)) * nfx * R(ld(DN + o))) : R(0.0);
+        ND[o + N3 * 12] = kin ? sfct(k, DY(2, dy(g, c, phi, 2, 0, k, i, j)) * ncy
                                             * R(0.25) * (R(ld(DN + o + sI + sJ)) + R(ld(DN + o + sI)) + R(ld(DN + o + sJ)) + R(ld(DN + o))))
                               : R(0.0);
         // ---- y momentum (:812-870), phi = VELY ----
         ND[o + N3 * 3] = (k >= KS && k <= KE - 1)
-                             ? dz0(g, c, phi, 3, k, i, j) * ncz
+                             ? DZ(3, dz0(g, c, phi, 3, k, i, j)) * ncz
                                    * R(0.25) * (R(ld(DN + o + 1 + sJ)) + R(ld(DN + o + 1)) + R(ld(DN + o + sJ)) + R(ld(DN + o)))
                              : R(0.0);
-        ND[o + N3 * 8] = kin ? sfct(k, dx(g, c, phi, 3, 0, k, i, j) * ncx
+        ND[o + N3 * 8] = kin ? sfct(k, DX(3, dx(g, c, phi, 3, 0, k, i, j)) * ncx
                                            * R(0.25) * (R(ld(DN + o + sI + sJ)) + R(ld(DN + o + sJ)) + R(ld(DN + o + sI)) + R(ld(DN + o))))
                              : R(0.0);
-        ND[o + N3 * 13] = kin ? sfct(k, dy(g, c, phi, 3, 1, k, i, j) * nfy * R(ld(DN + o))) : R(0.0);
+        ND[o + N3 * 13] = kin ? sfct(k, DY(3, dy(g, c, phi, 3, 1, k, i, j)) * nfy * R(ld(DN + o))) : R(0.0);
         // ---- rho*theta (:885-960) ----
         {
             R v = R(0.0);
-            if (k >= KS && k <= KE - 1) v = dz0(g, c, phi, 4, k, i, j) * ncz * R(0.5) * (R(ld(DN + o + 1)) + R(ld(DN + o)));
-            else if (k == KS - 1) v = dz0(g, c, phi, 4, k, i, j) * ncz * R(R(ld(DN + idx3(g, KS, i, j))));
-            else if (k == KE) v = dz0(g, c, phi, 4, k, i, j) * ncz * R(ld(DN + o));
+            if (k >= KS && k <= KE - 1) v = DZ(4, dz0(g, c, phi, 4, k, i, j)) * ncz * R(0.5) * (R(ld(DN + o + 1)) + R(ld(DN + o)));
+            else if (k == KS - 1) v = DZ(4, dz0(g, c, phi, 4, k, i, j)) * ncz * R(R(ld(DN + idx3(g, KS, i, j))));
+            else if (k == KE) v = DZ(4, dz0(g, c, phi, 4, k, i, j)) * ncz * R(ld(DN + o));
             ND[o + N3 * 4] = v;
         }
-        ND[o + N3 * 9] = kin ? sfct(k, dx(g, c, phi, 4, 0, k, i, j) * ncx * R(0.5) * (R(ld(DN + o + sI)) + R(ld(DN + o)))) : R(0.0);
-        ND[o + N3 * 14] = kin ? sfct(k, dy(g, c, phi, 4, 0, k, i, j) * ncy * R(0.5) * (R(ld(DN + o + sJ)) + R(ld(DN + o)))) : R(0.0);
+        ND[o + N3 * 9] = kin ? sfct(k, DX(4, dx(g, c, phi, 4, 0, k, i, j)) * ncx * R(0.5) * (R(ld(DN + o + sI)) + R(ld(DN + o)))) : R(0.0);
+        ND[o + N3 * 14] = kin ? sfct(k, DY(4, dy(g, c, phi, 4, 0, k, i, j)) * ncy * R(0.5) * (R(ld(DN + o + sJ)) + R(ld(DN + o)))) : R(0.0);
     }
+}
+
+#undef DZ
+#undef DX
+#undef DY
+
+// ---- ND_ORDER > 1: calc_numdiff (scale_atmos_dyn_common.F90:1518-1573) -----------
+// calc_diff3 of the five quantities (q: 0 density, 1 VELZ, 2 VELX, 3 VELY, 4
+// theta) into the work buffer, at every level of the interior columns; the
+// horizontal components on KS..KE-KO only, zero elsewhere (:1600-1760)
+__global__ void __launch_bounds__(128) k_nd_diff3(const Grid g, const NdCoef c, const NdArgs a, double *W)
+{
+    const int i = g.IS + blockIdx.x * blockDim.y + threadIdx.y;
+    const int j = g.JS + blockIdx.y;
+    if (i > g.IE) return;
+    const size_t N3 = n3(g);
+    const Phi<double> phi{g, a};
+    for (int k = 1 + threadIdx.x; k <= g.KA; k += 32) {
+        const size_t o = idx3(g, k, i, j);
+        for (int q = 0; q < 5; ++q) {
+            const int KO = q == 1, IO = q == 2, JO = q == 3, KEE = g.KE - KO;
+            W[(size_t)(3 * q + 0) * N3 + o] = KO ? dz1(g, c, phi, q, k, i, j) : dz0(g, c, phi, q, k, i, j);
+            const bool kin = k >= g.KS && k <= KEE;
+            W[(size_t)(3 * q + 1) * N3 + o] = kin ? dx(g, c, phi, q, IO, k, i, j) : 0.0;
+            W[(size_t)(3 * q + 2) * N3 + o] = kin ? dy(g, c, phi, q, JO, k, i, j) : 0.0;
+        }
+    }
+}
+
+// calc_diff4 (:1810-1918): z on KS..KE-1 and the mirrored levels KS-1, KS-2,
+// KE, KE+1 (written by the lane of the level they mirror, after a warp-wide
+// pass over the levels); x and y on KS..KE-KO
+__global__ void __launch_bounds__(128) k_nd_diff4(const Grid g, const NdCoef c, const double *Win, double *Wout)
+{
+    const int i = g.IS + blockIdx.x * blockDim.y + threadIdx.y;
+    const int j = g.JS + blockIdx.y;
+    if (i > g.IE) return;
+    const size_t N3 = n3(g), sI = (size_t)g.KA, sJ = (size_t)g.KA * g.IA;
+    const int KS = g.KS, KE = g.KE;
+    const size_t c1 = idx3(g, 1, i, j);
+    for (int q = 0; q < 5; ++q) {
+        const int KO = q == 1, IO = q == 2, JO = q == 3, K1 = KE - KO;
+        const double *CZ = c.CNZ4 + 5 * (size_t)g.KA * KO, *CX = c.CNX4 + 5 * (size_t)g.IA * IO,
+                     *CY = c.CNY4 + 5 * (size_t)g.JA * JO;
+        const double *iz = Win + (size_t)(3 * q) * N3, *ix = iz + N3, *iy = iz + 2 * N3;
+        double *oz = Wout + (size_t)(3 * q) * N3, *ox = oz + N3, *oy = oz + 2 * N3;
+        auto zval = [&](int k) {
+            const size_t o = c1 + k - 1;
+            const double *cz = CZ + 5 * (size_t)(k - 1);
+            return (ld(cz) * ld(iz + o + 2) - ld(cz + 1) * ld(iz + o + 1) + ld(cz + 2) * ld(iz + o) - ld(cz + 3) * ld(iz + o - 1)
+                    + ld(cz + 4) * ld(iz + o - 2));
+        };
+        for (int k = 1 + threadIdx.x; k <= g.KA; k += 32) {
+            const size_t o = c1 + k - 1;
+            if (k >= KS && k <= KE - 1) oz[o] = zval(k);
+            else if (k == KS - 1) oz[o] = -zval(KS);
+            else if (k == KS - 2) oz[o] = -zval(KS + 1);
+            else if (k == KE) oz[o] = -zval(KE - 1);
+            else if (k == KE + 1) oz[o] = -zval(KE - 2);
+            if (k >= KS && k <= K1) {
+                const double *cx = CX + 5 * (size_t)(i - 1), *cy = CY + 5 * (size_t)(j - 1);
+                ox[o] = (ld(cx) * ld(ix + o + 2 * sI) - ld(cx + 1) * ld(ix + o + sI) + ld(cx + 2) * ld(ix + o)
+                         - ld(cx + 3) * ld(ix + o - sI) + ld(cx + 4) * ld(ix + o - 2 * sI));
+                oy[o] = (ld(cy) * ld(iy + o + 2 * sJ) - ld(cy + 1) * ld(iy + o + sJ) + ld(cy + 2) * ld(iy + o)
+                         - ld(cy + 3) * ld(iy + o - sJ) + ld(cy + 4) * ld(iy + o - 2 * sJ));
+            }
+        }
+    }
+}
+
+cudaError_t launch_numfilter_high(const Grid &g, const NdCoef &c, const NdArgs &a, double *w1, double *w2,
+                                  cudaStream_t st)
+{
+    dim3 b(32, 4), gr((g.IMAX + 3) / 4, g.JMAX);
+    const BatchT<1> one{1, {0, ((g.IA + 3) / 4) * g.JA}, {}};
+    k_phi<double, 1><<<one.first[1], b, 0, st>>>(g, a, one);
+    k_nd_diff3<<<gr, b, 0, st>>>(g, c, a, w1);
+    double *in = w1, *out = w2;
+    for (int no = 2; no <= c.order; ++no) {
+        double *f[15];
+        for (int q = 0; q < 15; ++q) f[q] = in + (size_t)q * n3(g);
+        periodic_halo(g, Members{}, f, 15, st); // COMM_vars8 of the work (:1557-1563)
+        k_nd_diff4<<<gr, b, 0, st>>>(g, c, in, out);
+        double *t = in;
+        in = out;
+        out = t;
+    }
+    const BatchT<1> oneN{1, {0, ((g.IMAX + 3) / 4) * g.JMAX}, {}};
+    k_numfilter<double, 1, true><<<oneN.first[1], b, 0, st>>>(g, c, a, oneN, in);
+    return cudaGetLastError();
 }
 
 template <typename R>
@@ -229,7 +326,7 @@ cudaError_t launch_numfilter(const Grid &g, const Members &mem, const NdCoef &c,
         return cudaSuccess;
     });
     with_batch(g, mem, nb_nd, [&](const auto &B, int nb) {
-        k_numfilter<R, std::decay_t<decltype(B)>::NMAX><<<nb, dim3(32, 4), 0, st>>>(g, c, a, B);
+        k_numfilter<R, std::decay_t<decltype(B)>::NMAX><<<nb, dim3(32, 4), 0, st>>>(g, c, a, B, nullptr);
         return cudaSuccess;
     });
     return cudaGetLastError();

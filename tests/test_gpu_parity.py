@@ -96,19 +96,21 @@ def test_rk4_short_step_bit_exact(lib, scheme):
         assert helpers.same(xg[n], xs[n]), f"{n}: max rel diff {helpers.max_rel(xg[n], xs[n]):.3e}"
 
 
+@pytest.mark.parametrize("order", [1, 2, 3])
 @pytest.mark.parametrize("stretched", [False, True])
-def test_numfilter_bit_exact(lib, stretched):
+def test_numfilter_bit_exact(lib, stretched, order):
     g = helpers.small_grid(IMAX=15, JMAX=10, KMAX=19, stretched=stretched)
     c = helpers.small_case(g)
     helpers.perturb_state(c)
     ref_nd = g.zeros(5, 3)
-    oracle.numfilter(g, ref_nd, c.state, c.ref, DT=0.5, ND_COEF=1e-3, ND_SFC_FACT=0.7)
+    oracle.numfilter(g, ref_nd, c.state, c.ref, DT=0.5, ND_COEF=1e-3, ND_ORDER=order, ND_SFC_FACT=0.7)
     got = np.full(g.shape + (5, 3), np.nan, order="F")
     lib.setup(g.index_dict(), "UD3", "UD3")
     lib.ATMOS_DYN_numfilter_coef(num_diff=got, DENS=c.state["DENS"], MOMZ=c.state["MOMZ"], MOMX=c.state["MOMX"],
                                  MOMY=c.state["MOMY"], RHOT=c.state["RHOT"], CDZ=g.CDZ, CDX=g.CDX, CDY=g.CDY,
                                  FDZ=g.FDZ, FDX=g.FDX, FDY=g.FDY, DT=0.5, REF_dens=c.ref["REF_dens"],
-                                 REF_pott=c.ref["REF_pott"], ND_COEF=1e-3, ND_ORDER=1, ND_SFC_FACT=0.7, ND_USE_RS=True)
+                                 REF_pott=c.ref["REF_pott"], ND_COEF=1e-3, ND_ORDER=order, ND_SFC_FACT=0.7,
+                                 ND_USE_RS=True)
     for v in range(5):
         for d in range(3):
             assert helpers.same(got[..., v, d], ref_nd[..., v, d]), f"num_diff(:,:,:,{v+1},{d+1})"
@@ -179,7 +181,7 @@ def _large_inputs(c):
     return tp, GS, J13, J23, MAPF
 
 
-def _run_large_both(c, nlarge, lib, divdmp=0.0):
+def _run_large_both(c, nlarge, lib, divdmp=0.0, nd_order=1):
     g = c.g
     tp, GS, J13, J23, MAPF = _large_inputs(c)
     aq = mkinit.aq_props(c.QA) if c.QA else None
@@ -191,7 +193,7 @@ def _run_large_both(c, nlarge, lib, divdmp=0.0):
     out_gpu = dict(mflx_hi=g.zeros(3), tflx_hi=g.zeros(3), num_diff=g.zeros(5, 3))
     for _ in range(nlarge):
         oracle.tstep_large(g, c.scheme, c.scheme_tracer, st_ref, out_ref, tp, c.ref, aq, GS, J13, J23, MAPF, cor, wd,
-                           c.dtl, c.dt, ND_COEF=c.nd_coef, divdmp=divdmp, fct=c.fct, QA=c.QA)
+                           c.dtl, c.dt, ND_COEF=c.nd_coef, divdmp=divdmp, fct=c.fct, QA=c.QA, ND_ORDER=nd_order)
     lib.setup(g.index_dict(), c.scheme, c.scheme_tracer)
     R, CV, CP, M = aq if aq else (None, None, None, None)
     for _ in range(nlarge):
@@ -202,7 +204,7 @@ def _run_large_both(c, nlarge, lib, divdmp=0.0):
             FDZ=g.FDZ, FDX=g.FDX, FDY=g.FDY, RCDZ=g.RCDZ, RCDX=g.RCDX, RCDY=g.RCDY, RFDZ=g.RFDZ, RFDX=g.RFDX,
             RFDY=g.RFDY, PHI=c.ref["PHI"], GSQRT=GS, J13G=J13, J23G=J23, J33G=1.0, MAPF=MAPF, AQ_R=R, AQ_CV=CV,
             AQ_CP=CP, AQ_MASS=M, REF_dens=c.ref["REF_dens"], REF_pott=c.ref["REF_pott"], REF_pres=c.ref["REF_pres"],
-            ND_COEF=c.nd_coef, ND_ORDER=1, ND_SFC_FACT=1.0, ND_USE_RS=True, wdamp_coef=wd, divdmp_coef=divdmp,
+            ND_COEF=c.nd_coef, ND_ORDER=nd_order, ND_SFC_FACT=1.0, ND_USE_RS=True, wdamp_coef=wd, divdmp_coef=divdmp,
             FLAG_FCT_TRACER=c.fct, FLAG_FCT_ALONG_STREAM=True, DTLS=c.dtl, DTSS=c.dt,
             **{k: v for k, v in tp.items() if k != "RHOQ_tp"})
     return st_ref, st_gpu
@@ -218,6 +220,15 @@ def _field_err(a, b, g):
 def test_large_step_dry_parity(lib):
     c = mkinit.config(1, scale=0.3)
     st_ref, st_gpu = _run_large_both(c, 4, lib)
+    for n in STATE:
+        err = _field_err(st_gpu[n], st_ref[n], c.g)
+        assert err <= 1e-10, f"{n}: {err:.3e}"
+
+
+def test_large_step_higher_order_filter_parity(lib):
+    # the numerical filter at ND_ORDER = 2 inside the device large step
+    c = mkinit.config(1, scale=0.3)
+    st_ref, st_gpu = _run_large_both(c, 2, lib, nd_order=2)
     for n in STATE:
         err = _field_err(st_gpu[n], st_ref[n], c.g)
         assert err <= 1e-10, f"{n}: {err:.3e}"

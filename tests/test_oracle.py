@@ -268,3 +268,35 @@ def test_koren_limiter_keeps_step_bounded():
     assert qk.min() >= -1e-15 and qk.max() <= 1.0 + 1e-15
     qu = _step_advection("UD3", g)
     assert qu.min() < -1e-3 or qu.max() > 1.0 + 1e-3
+
+
+def test_numfilter_higher_orders_damp_the_two_grid_wave_alike():
+    """The filter coefficient DIFF4 * dx**(4*order) / 2**(4*order) normalises
+    every order (calc_numdiff with calc_diff4, scale_atmos_dyn_common.F90:
+    444-460, 1518-1918) so that a 2-dx wave is damped the same: for a density
+    anomaly alternating along x on a uniform grid, num_diff(DENS, x) agrees
+    for ND_ORDER 1, 2 and 3; a uniform state gives zero at every order."""
+    g = mkinit.uniform_grid(16, 8, 12, 500.0, 500.0, 250.0)
+    c = mkinit.make_case("2dx", g, "UD3", "UD3")
+    st = c.state
+    i = np.arange(g.IA)
+    st["DENS"][...] = c.ref["REF_dens"] + 1e-3 * np.where(i % 2 == 0, 1.0, -1.0)[None, :, None]
+    st["RHOT"][...] = st["DENS"] * c.ref["REF_pott"]
+    for n in ("MOMZ", "MOMX", "MOMY"):
+        st[n][...] = 0.0
+    out = {}
+    for order in (1, 2, 3):
+        nd = g.zeros(5, 3)
+        assert oracle.numfilter(g, nd, st, c.ref, DT=1.0, ND_COEF=1e-2, ND_ORDER=order) == 0
+        out[order] = _interior(nd[..., 0, 1], g)
+    scale = np.max(np.abs(out[1]))
+    assert scale > 0.0
+    for order in (2, 3):
+        assert np.max(np.abs(out[order] - out[1])) <= 1e-12 * scale, order
+    # uniform state: no diffusion at any order
+    st["DENS"][...] = c.ref["REF_dens"]
+    st["RHOT"][...] = st["DENS"] * c.ref["REF_pott"]
+    for order in (2, 3):
+        nd = g.zeros(5, 3)
+        oracle.numfilter(g, nd, st, c.ref, DT=1.0, ND_COEF=1e-2, ND_ORDER=order)
+        assert np.max(np.abs(_interior(nd[..., 0, 1], g))) < 1e-14
