@@ -288,7 +288,12 @@ int ATMOS_DYN_Tstep_large_fvm_heve_b200_dev(
     const double *DTLS, const double *DTSS);
 
 /* Host-array variant of the large step: copies the state in, runs, copies the
- * state, mflx_hi, tflx_hi and num_diff back. Same arguments. */
+ * state, QTRC, mflx_hi, tflx_hi and num_diff back. Same arguments and results
+ * as the device entry. The copies run on a second stream, inputs in the order
+ * of first use and each output group as soon as it is final, so that with
+ * page-locked host arrays they overlap the kernels; the call returns when all
+ * copies have landed. Not capturable in a CUDA graph (rejected while a capture
+ * is open). */
 int ATMOS_DYN_Tstep_large_fvm_heve_b200(
     double *DENS, double *MOMZ, double *MOMX, double *MOMY, double *RHOT, double *QTRC, const int *QA,
     double *mflx_hi, double *tflx_hi, double *num_diff,

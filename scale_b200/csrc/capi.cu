@@ -6,6 +6,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <functional>
 #include <map>
 #include <string>
 #include <vector>
@@ -19,6 +20,8 @@
 using namespace hevi;
 
 namespace {
+
+struct LargeHooks;
 
 struct Ctx {
     bool ready = false;
@@ -68,6 +71,11 @@ struct Ctx {
     std::vector<std::vector<const void *>> flat_ok;
     // staging buffers of the host-array entries
     std::map<std::string, std::pair<double *, size_t>> stage;
+    // host-array large step: a second stream carries the host<->device copies so
+    // that they overlap the kernels on `stream` (created on first use)
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t copy_ev[6] = {};
+    LargeHooks *large_hooks = nullptr; // set only inside the host-array large step
     // section timers (scale_hevi_profile): event pairs recorded around launches
     bool prof_on = false;
     std::vector<cudaEvent_t> ev_pool;
@@ -180,6 +188,8 @@ void free_all()
     if (C.status) cudaFree(C.status);
     if (C.count) cudaFree(C.count);
     for (cudaEvent_t e : C.ev_pool) cudaEventDestroy(e);
+    for (cudaEvent_t e : C.copy_ev) if (e) cudaEventDestroy(e);
+    if (C.copy_stream) cudaStreamDestroy(C.copy_stream);
     if (C.capturing) {
         cudaGraph_t g = nullptr;
         if (cudaStreamEndCapture(C.stream, &g) == cudaSuccess && g) cudaGraphDestroy(g);
@@ -217,16 +227,17 @@ int stage_buf(const char *name, size_t n, double **out)
     *out = e.first;
     return SCALE_HEVI_OK;
 }
-int h2d(const char *name, const double *h, size_t n, double **d)
+// copies on `st`, or on the library stream when st is null
+int h2d(const char *name, const double *h, size_t n, double **d, cudaStream_t st = nullptr)
 {
     CK(stage_buf(name, n, d));
-    CU(cudaMemcpyAsync(*d, h, n * sizeof(double), cudaMemcpyHostToDevice, C.stream));
+    CU(cudaMemcpyAsync(*d, h, n * sizeof(double), cudaMemcpyHostToDevice, st ? st : C.stream));
     C.h2d_bytes += (long long)(n * sizeof(double));
     return SCALE_HEVI_OK;
 }
-int d2h(double *h, const double *d, size_t n)
+int d2h(double *h, const double *d, size_t n, cudaStream_t st = nullptr)
 {
-    CU(cudaMemcpyAsync(h, d, n * sizeof(double), cudaMemcpyDeviceToHost, C.stream));
+    CU(cudaMemcpyAsync(h, d, n * sizeof(double), cudaMemcpyDeviceToHost, st ? st : C.stream));
     C.d2h_bytes += (long long)(n * sizeof(double));
     return SCALE_HEVI_OK;
 }
@@ -1081,6 +1092,20 @@ int COMM_vars8_b200_dev(double *var, const int *nfields)
         const double *ND_SFC_FACT, const int *ND_USE_RS, const double *wdamp_coef, const double *divdmp_coef,      \
         const int *FLAG_FCT_TRACER, const int *FLAG_FCT_ALONG_STREAM, const double *DTLS, const double *DTSS
 
+// Copy/compute overlap of the host-array large step. The device body waits on
+// in[g] before the first use of input group g (0: DENS RHOT QTRC REF_pres for
+// the preparation; 1: MOMZ MOMX MOMY REF_dens REF_pott for the filter; 2: the
+// tendencies and CORIOLI for the short steps; 3: RHOQ_tp for the tracers) and
+// calls done() as soon as a group of outputs holds its final values (0:
+// num_diff after the last filter; 1: the state and tflx_hi after the last
+// short step; 2: mflx_hi; 3: tracer q after its advection and halo).
+namespace {
+struct LargeHooks {
+    cudaEvent_t in[4] = {};
+    std::function<int(int what, int q)> done;
+};
+}  // namespace
+
 int ATMOS_DYN_Tstep_large_fvm_heve_b200_dev(SCALE_HEVI_LARGE_ARGS)
 {
     (void)PHI;
@@ -1104,6 +1129,14 @@ int ATMOS_DYN_Tstep_large_fvm_heve_b200_dev(SCALE_HEVI_LARGE_ARGS)
     const int nstep = (int)std::ceil((dtl - EPS) / dts);
     dts = dtl / nstep;
 
+    LargeHooks *hk = C.large_hooks;
+    auto wait_in = [&](int grp) -> int {
+        if (hk && hk->in[grp]) CU(cudaStreamWaitEvent(C.stream, hk->in[grp], 0));
+        return SCALE_HEVI_OK;
+    };
+    auto done = [&](int what, int q) -> int { return hk ? hk->done(what, q) : SCALE_HEVI_OK; };
+
+    CK(wait_in(0));
     CU(cudaMemcpyAsync(DENS00, DENS, N3 * sizeof(double), cudaMemcpyDeviceToDevice, C.stream));
     CU(cudaMemsetAsync(mflx_av, 0, 3 * N3 * sizeof(double), C.stream));
     // RT2P / DPRES0 / REF_rhot, :428-470
@@ -1123,10 +1156,13 @@ int ATMOS_DYN_Tstep_large_fvm_heve_b200_dev(SCALE_HEVI_LARGE_ARGS)
                  DENS_tp, MOMZ_tp, MOMX_tp, MOMY_tp, RHOT_tp, DPRES0, RT2P, CORIOLI, num_diff, use_div ? DDIV : nullptr,
                  REF_dens, REF_rhot, use_div ? *divdmp_coef : 0.0, *J33G};
     for (int step = 1; step <= nstep; ++step) {
+        if (step == 1) CK(wait_in(1));
         if (*ND_COEF == 0.0) CU(cudaMemsetAsync(num_diff, 0, 15 * N3 * sizeof(double), C.stream));
         else CK(run_numfilter(num_diff, DENS, MOMZ, MOMX, MOMY, RHOT, REF_dens, REF_pott));
+        if (step == nstep) CK(done(0, 0));
         // divergence for the damping term, :860-871
         if (use_div) CK(run_divergence(DDIV, MOMZ, MOMX, MOMY, C.g.RCDZ, C.g.RCDX, C.g.RCDY, *J33G));
+        if (step == 1) CK(wait_in(2));
         CK(run_rk4(X, mflx_hi, tflx_hi, base, dts));
         CK(timed("boundary", [&] { vertical_bc(C.g, mem(), DENS, MOMZ, MOMX, MOMY, RHOT, C.stream); return SCALE_HEVI_OK; }));
         ++C.launches;
@@ -1134,58 +1170,102 @@ int ATMOS_DYN_Tstep_large_fvm_heve_b200_dev(SCALE_HEVI_LARGE_ARGS)
         CK(timed("mflx_average", [&] { mflx_accumulate(C.g, mflx_av, mflx_hi, C.stream); return SCALE_HEVI_OK; }));
         ++C.launches;
     }
+    if (nstep < 1) CK(done(0, 0));
+    CK(done(1, 0));
     if (qa > 0) {
         mflx_average(C.g, mflx_hi, mflx_av, nstep, C.stream);
         ++C.launches;
         double *mf[3] = {mflx_hi, mflx_hi + N3, mflx_hi + 2 * N3};
         CK(halo(mf, 3));
+        CK(done(2, 0));
+        CK(wait_in(3));
         for (int q = 0; q < qa; ++q) {
             double *qt = QTRC + (size_t)q * N3;
             CK(run_tracer_rk3(qt, qt, RHOQ_tp + (size_t)q * N3, DENS00, DENS, mflx_hi, nullptr, dtl,
                               *FLAG_FCT_TRACER != 0, *FLAG_FCT_ALONG_STREAM != 0));
             CK(halo(&qt, 1));
+            CK(done(3, q));
         }
+    } else {
+        CK(done(2, 0));
     }
     return SCALE_HEVI_OK;
 }
 
+// Host-array form: inputs are copied in on a second stream in the order the
+// device body first needs them, and each group of outputs is copied back as
+// soon as it is final, so that the copies overlap the kernels. Results are
+// those of the device entry; the call returns when every copy has landed.
 int ATMOS_DYN_Tstep_large_fvm_heve_b200(SCALE_HEVI_LARGE_ARGS)
 {
     CK(need_single("the large step"));
+    if (C.capturing) return fail(SCALE_HEVI_ERR_ARG, "the host-array large step cannot be captured");
     CK(check_flat(GSQRT, J13G, J23G, MAPF, false));
     const size_t N3 = n3(), N2 = (size_t)C.g.IA * C.g.JA;
     const int qa = *QA;
+    if (qa < 0 || qa > 8) return fail(SCALE_HEVI_ERR_UNSUPPORTED, "QA=%d (0..8 supported)", qa);
+    if (!C.copy_stream) {
+        CU(cudaStreamCreate(&C.copy_stream));
+        for (cudaEvent_t &e : C.copy_ev) CU(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    }
+    cudaStream_t cs = C.copy_stream;
+    // the copies start after the work already queued on the library stream
+    CU(cudaEventRecord(C.copy_ev[5], C.stream));
+    CU(cudaStreamWaitEvent(cs, C.copy_ev[5], 0));
+
     double *X[5], *T[5], *q = nullptr, *rq = nullptr, *mf, *tf, *nd, *cor, *rd, *rp, *rpres;
     double *hx[5] = {DENS, MOMZ, MOMX, MOMY, RHOT};
     const double *ht[5] = {DENS_tp, MOMZ_tp, MOMX_tp, MOMY_tp, RHOT_tp};
     static const char *n_x[5] = {"x0", "x1", "x2", "x3", "x4"}, *n_t[5] = {"t0", "t1", "t2", "t3", "t4"};
-    for (int v = 0; v < 5; ++v) {
-        CK(h2d(n_x[v], hx[v], N3, &X[v]));
-        CK(h2d(n_t[v], ht[v], N3, &T[v]));
-    }
+    LargeHooks hk;
+    // group 0: DENS RHOT QTRC REF_pres
+    CK(h2d(n_x[0], hx[0], N3, &X[0], cs));
+    CK(h2d(n_x[4], hx[4], N3, &X[4], cs));
+    if (qa > 0) CK(h2d("qtrc", QTRC, (size_t)qa * N3, &q, cs));
+    CK(h2d("REF_pres", REF_pres, N3, &rpres, cs));
+    CU(cudaEventRecord(C.copy_ev[0], cs));
+    // group 1: MOMZ MOMX MOMY REF_dens REF_pott
+    for (int v = 1; v < 4; ++v) CK(h2d(n_x[v], hx[v], N3, &X[v], cs));
+    CK(h2d("REF_dens", REF_dens, N3, &rd, cs));
+    CK(h2d("REF_pott", REF_pott, N3, &rp, cs));
+    CU(cudaEventRecord(C.copy_ev[1], cs));
+    // group 2: tendencies, CORIOLI
+    for (int v = 0; v < 5; ++v) CK(h2d(n_t[v], ht[v], N3, &T[v], cs));
+    CK(h2d("CORIOLI", CORIOLI, N2, &cor, cs));
+    CU(cudaEventRecord(C.copy_ev[2], cs));
+    // group 3: tracer tendencies
     if (qa > 0) {
-        CK(h2d("qtrc", QTRC, (size_t)qa * N3, &q));
-        CK(h2d("rhoq_tp", RHOQ_tp, (size_t)qa * N3, &rq));
+        CK(h2d("rhoq_tp", RHOQ_tp, (size_t)qa * N3, &rq, cs));
+        CU(cudaEventRecord(C.copy_ev[3], cs));
     }
+    for (int g = 0; g < 4; ++g) hk.in[g] = (g < 3 || qa > 0) ? C.copy_ev[g] : nullptr;
     CK(stage_buf("mflx", 3 * N3, &mf));
     CK(stage_buf("tflx", 3 * N3, &tf));
     CK(stage_buf("num_diff", 15 * N3, &nd));
-    CK(h2d("CORIOLI", CORIOLI, N2, &cor));
-    CK(h2d("REF_dens", REF_dens, N3, &rd));
-    CK(h2d("REF_pott", REF_pott, N3, &rp));
-    CK(h2d("REF_pres", REF_pres, N3, &rpres));
+    hk.done = [&](int what, int iq) -> int {
+        CU(cudaEventRecord(C.copy_ev[4], C.stream));
+        CU(cudaStreamWaitEvent(cs, C.copy_ev[4], 0));
+        switch (what) {
+        case 0: return d2h(num_diff, nd, 15 * N3, cs);
+        case 1:
+            for (int v = 0; v < 5; ++v) CK(d2h(hx[v], X[v], N3, cs));
+            return d2h(tflx_hi, tf, 3 * N3, cs);
+        case 2: return d2h(mflx_hi, mf, 3 * N3, cs);
+        default: return d2h(QTRC + (size_t)iq * N3, q + (size_t)iq * N3, N3, cs);
+        }
+    };
+    C.large_hooks = &hk;
     int rc = ATMOS_DYN_Tstep_large_fvm_heve_b200_dev(
         X[0], X[1], X[2], X[3], X[4], q, QA, mf, tf, nd, T[0], T[1], T[2], T[3], T[4], rq, cor,
         CDZ, CDX, CDY, FDZ, FDX, FDY, RCDZ, RCDX, RCDY, RFDZ, RFDX, RFDY, PHI, nullptr, nullptr, nullptr, J33G, nullptr,
         AQ_R, AQ_CV, AQ_CP, AQ_MASS, rd, rp, rpres, ND_COEF, ND_ORDER, ND_SFC_FACT, ND_USE_RS, wdamp_coef, divdmp_coef,
         FLAG_FCT_TRACER, FLAG_FCT_ALONG_STREAM, DTLS, DTSS);
+    C.large_hooks = nullptr;
+    // both streams drain before the host arrays are handed back, also on failure
+    const cudaError_t e1 = cudaStreamSynchronize(cs), e2 = cudaStreamSynchronize(C.stream);
     if (rc) return rc;
-    for (int v = 0; v < 5; ++v) CK(d2h(hx[v], X[v], N3));
-    if (qa > 0) CK(d2h(QTRC, q, (size_t)qa * N3));
-    CK(d2h(mflx_hi, mf, 3 * N3));
-    CK(d2h(tflx_hi, tf, 3 * N3));
-    CK(d2h(num_diff, nd, 15 * N3));
-    CU(cudaStreamSynchronize(C.stream));
+    CU(e1);
+    CU(e2);
     return scale_hevi_check();
 }
 
