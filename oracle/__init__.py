@@ -15,8 +15,9 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 LIB = HERE / "build" / "liboracle.so"
-UD3, CD4, KOREN, CD2 = 1, 2, 3, 4
-SCHEMES = {"UD3": UD3, "CD4": CD4, "UD3KOREN1993": KOREN, "CD2": CD2}
+UD3, CD4, KOREN, CD2, UD5, CD6 = 1, 2, 3, 4, 5, 6
+SCHEMES = {"UD3": UD3, "CD4": CD4, "UD3KOREN1993": KOREN, "CD2": CD2, "UD5": UD5, "CD6": CD6}
+WIDE = ("UD5", "CD6")  # 6-point schemes: IHALO = JHALO = 3
 
 
 class Dims(C.Structure):
@@ -73,7 +74,7 @@ def load() -> C.CDLL:
 
 def dims(g) -> Dims:
     return Dims(KA=g.KA, IA=g.IA, JA=g.JA, KS=g.KS, KE=g.KE, IS=g.IS, IE=g.IE, JS=g.JS, JE=g.JE, KMAX=g.KMAX,
-                IMAX=g.IMAX, JMAX=g.JMAX, IHALO=2, JHALO=2, IEH=g.IE, JEH=g.JE)
+                IMAX=g.IMAX, JMAX=g.JMAX, IHALO=g.IS - 1, JHALO=g.JS - 1, IEH=g.IE, JEH=g.JE)
 
 
 def _p(a):

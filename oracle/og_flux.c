@@ -5,9 +5,15 @@
  * reference routine of the same name in
  *   scalelib/src/atmos-rm/dynamics/scale_atmos_dyn_fvm_flux_ud3.F90 (UD3)
  *   scalelib/src/atmos-rm/dynamics/scale_atmos_dyn_fvm_flux_cd4.F90 (CD4)
- * The two files are generated from one template (scale_atmos_dyn_fvm_flux_udcd.F90.erb)
- * and differ only in the 4-point interpolation and the near-wall formulas, which
- * are og_ip4 / og_ipL / og_ipH. Line numbers cite the UD3 file.
+ *   ..._cd2.F90, ..._ud5.F90, ..._cd6.F90 (CD2, UD5, CD6)
+ *   ..._ud3Koren1993.F90 (UD3KOREN1993)
+ * The UD/CD files are generated from one template (scale_atmos_dyn_fvm_flux_udcd.F90.erb)
+ * and differ only in the face interpolation and the near-wall formulas: og_hface
+ * along x and y, og_zface along z (og_internal.h). Each z routine loops over all
+ * its faces; the reference's separate statements at KS and KE-1 (and, for the
+ * 6-point schemes, KS+1 and KE-2) use the same velocity formula as its interior
+ * loop and differ only in the face value, which og_zface selects by level.
+ * Line numbers cite the UD3 file.
  */
 #include "og_internal.h"
 
@@ -20,10 +26,7 @@
 void og_valueW_Z(const og_dims *d, int scheme, double *valW, const double *mflx, const double *val)
 {
     const int KS = d->KS, KE = d->KE;
-    for (int k = KS + 1; k <= KE - 2; ++k)
-        valW[k - 1] = og_ip4(scheme, mflx[k - 1], val[k - 2], val[k - 1], val[k], val[k + 1]);
-    valW[KS - 1] = og_ipL(scheme, mflx[KS - 1], val[KS - 1], val[KS], val[KS + 1]);
-    valW[KE - 2] = og_ipH(scheme, mflx[KE - 2], val[KE - 1], val[KE - 2], val[KE - 3]);
+    for (int m = KS; m <= KE - 1; ++m) valW[m - 1] = og_zface(scheme, mflx[m - 1], val, m, KS, KE);
 }
 
 /* ud3.F90:157-247 */
@@ -34,19 +37,12 @@ void og_fluxZ_XYZ(const og_dims *d, int scheme, double *flux, const double *mflx
 #pragma omp parallel for collapse(2)
     for (int j = b.JJS; j <= b.JJE; ++j)
         for (int i = b.IIS; i <= b.IIE; ++i) {
-            for (int k = KS + 1; k <= KE - 2; ++k) {
+            for (int k = KS; k <= KE - 1; ++k) {
                 double vel = mflx[I3(k, i, j)];
-                flux[I3(k, i, j)] = vel * og_ip4(scheme, vel, val[I3(k - 1, i, j)], val[I3(k, i, j)],
-                                                 val[I3(k + 1, i, j)], val[I3(k + 2, i, j)])
+                flux[I3(k, i, j)] = vel * og_zface(scheme, vel, &val[I3(1, i, j)], k, KS, KE)
                                     + GSQRT[I3(k, i, j)] * nd[I3(k, i, j)];
             }
             flux[I3(KS - 1, i, j)] = 0.0;
-            double vel = mflx[I3(KS, i, j)];
-            flux[I3(KS, i, j)] = vel * og_ipL(scheme, vel, val[I3(KS, i, j)], val[I3(KS + 1, i, j)], val[I3(KS + 2, i, j)])
-                                 + GSQRT[I3(KS, i, j)] * nd[I3(KS, i, j)];
-            vel = mflx[I3(KE - 1, i, j)];
-            flux[I3(KE - 1, i, j)] = vel * og_ipH(scheme, vel, val[I3(KE, i, j)], val[I3(KE - 1, i, j)], val[I3(KE - 2, i, j)])
-                                     + GSQRT[I3(KE - 1, i, j)] * nd[I3(KE - 1, i, j)];
             flux[I3(KE, i, j)] = 0.0;
         }
 }
@@ -61,8 +57,7 @@ void og_fluxX_XYZ(const og_dims *d, int scheme, double *flux, const double *mflx
         for (int i = b.IIS - 1; i <= b.IIE; ++i)
             for (int k = KS; k <= KE; ++k) {
                 double vel = mflx[I3(k, i, j)];
-                flux[I3(k, i, j)] = vel * og_ip4(scheme, vel, val[I3(k, i - 1, j)], val[I3(k, i, j)],
-                                                 val[I3(k, i + 1, j)], val[I3(k, i + 2, j)])
+                flux[I3(k, i, j)] = vel * og_hface(scheme, vel, &val[I3(k, i, j)], (long)KA)
                                     + GSQRT[I3(k, i, j)] * nd[I3(k, i, j)];
             }
 }
@@ -77,8 +72,7 @@ void og_fluxY_XYZ(const og_dims *d, int scheme, double *flux, const double *mflx
         for (int i = b.IIS; i <= b.IIE; ++i)
             for (int k = KS; k <= KE; ++k) {
                 double vel = mflx[I3(k, i, j)];
-                flux[I3(k, i, j)] = vel * og_ip4(scheme, vel, val[I3(k, i, j - 1)], val[I3(k, i, j)],
-                                                 val[I3(k, i, j + 1)], val[I3(k, i, j + 2)])
+                flux[I3(k, i, j)] = vel * og_hface(scheme, vel, &val[I3(k, i, j)], (long)KA * IA)
                                     + GSQRT[I3(k, i, j)] * nd[I3(k, i, j)];
             }
 }
@@ -91,16 +85,14 @@ void og_fluxZ_XYW(const og_dims *d, int scheme, double *flux, const double *mom,
 #pragma omp parallel for collapse(2)
     for (int j = b.JJS; j <= b.JJE; ++j)
         for (int i = b.IIS; i <= b.IIE; ++i) {
-            for (int k = KS + 2; k <= KE - 1; ++k) {
+            /* flux(k-1) for k = KS+1..KE-1: the KS face (ud3.F90:424-432) and the
+             * interior loop (:376-402) share the same velocity formula */
+            for (int k = KS + 1; k <= KE - 1; ++k) {
                 double vel = (0.5 * (mom[I3(k - 1, i, j)] + mom[I3(k, i, j)])) / DENS[I3(k, i, j)];
-                flux[I3(k - 1, i, j)] = J33G * vel * og_ip4(scheme, vel, val[I3(k - 2, i, j)], val[I3(k - 1, i, j)],
-                                                            val[I3(k, i, j)], val[I3(k + 1, i, j)])
+                flux[I3(k - 1, i, j)] = J33G * vel * og_zface(scheme, vel, &val[I3(1, i, j)], k - 1, KS, KE)
                                         + GSQRT[I3(k, i, j)] * nd[I3(k, i, j)];
             }
             flux[I3(KS - 1, i, j)] = 0.0;
-            double vel = (0.5 * (mom[I3(KS, i, j)] + mom[I3(KS + 1, i, j)])) / DENS[I3(KS + 1, i, j)];
-            flux[I3(KS, i, j)] = J33G * vel * og_ipL(scheme, vel, val[I3(KS, i, j)], val[I3(KS + 1, i, j)], val[I3(KS + 2, i, j)])
-                                 + GSQRT[I3(KS + 1, i, j)] * nd[I3(KS + 1, i, j)];
             flux[I3(KE - 1, i, j)] = 0.0;
             flux[I3(KE, i, j)] = 0.0;
         }
@@ -111,15 +103,21 @@ void og_fluxJ13_XYW(const og_dims *d, int scheme, double *flux, const double *mo
                     const double *DENS, const double *J13G, const double *MAPF, og_blk b)
 {
     OG_DIMS(d);
+    /* 4-point schemes: flux(k-1) for k = KS+2..KE-1 (ud3.F90); 6-point ones: for
+     * k = KS+2..KE-2 from val(k-3..k+2), and at KE-2 the 3-point form of the KE-1
+     * face one level lower (ud5.F90:604-657, cd6.F90) */
+    const int wide = og_wide(scheme), kend = wide ? KE - 2 : KE - 1;
 #pragma omp parallel for collapse(2)
     for (int j = b.JJS; j <= b.JJE; ++j)
         for (int i = b.IIS; i <= b.IIE; ++i) {
-            for (int k = KS + 2; k <= KE - 1; ++k) {
+            for (int k = KS + 2; k <= kend; ++k) {
                 double vel = (0.5 * (mom[I3(k, i, j)] + mom[I3(k, i - 1, j)])) / DENS[I3(k, i, j)];
                 vel = vel * J13G[I3(k, i, j)];
-                flux[I3(k - 1, i, j)] = vel / MP(MAPF, i, j, 2)
-                                        * og_ip4(scheme, vel, val[I3(k - 2, i, j)], val[I3(k - 1, i, j)],
-                                                 val[I3(k, i, j)], val[I3(k + 1, i, j)]);
+                const double q = wide ? og_ip6(scheme, vel, val[I3(k - 3, i, j)], val[I3(k - 2, i, j)], val[I3(k - 1, i, j)],
+                                               val[I3(k, i, j)], val[I3(k + 1, i, j)], val[I3(k + 2, i, j)])
+                                      : og_ip4(scheme, vel, val[I3(k - 2, i, j)], val[I3(k - 1, i, j)],
+                                               val[I3(k, i, j)], val[I3(k + 1, i, j)]);
+                flux[I3(k - 1, i, j)] = vel / MP(MAPF, i, j, 2) * q;
             }
             flux[I3(KS - 1, i, j)] = 0.0;
             double vel = ((0.5 * (mom[I3(KS + 1, i, j)] + mom[I3(KS + 1, i - 1, j)])) / DENS[I3(KS + 1, i, j)]
@@ -127,6 +125,12 @@ void og_fluxJ13_XYW(const og_dims *d, int scheme, double *flux, const double *mo
             vel = vel * J13G[I3(KS + 1, i, j)];
             flux[I3(KS, i, j)] = vel / MP(MAPF, i, j, 2)
                                  * og_ipL(scheme, vel, val[I3(KS, i, j)], val[I3(KS + 1, i, j)], val[I3(KS + 2, i, j)]);
+            if (wide) {
+                vel = (0.5 * (mom[I3(KE - 1, i, j)] + mom[I3(KE - 1, i - 1, j)])) / DENS[I3(KE - 1, i, j)];
+                vel = vel * J13G[I3(KE - 1, i, j)];
+                flux[I3(KE - 2, i, j)] = vel / MP(MAPF, i, j, 2)
+                                         * og_ipH(scheme, vel, val[I3(KE - 1, i, j)], val[I3(KE - 2, i, j)], val[I3(KE - 3, i, j)]);
+            }
             flux[I3(KE - 1, i, j)] = 0.0;
         }
 }
@@ -136,15 +140,21 @@ void og_fluxJ23_XYW(const og_dims *d, int scheme, double *flux, const double *mo
                     const double *DENS, const double *J23G, const double *MAPF, og_blk b)
 {
     OG_DIMS(d);
+    /* 4-point schemes: flux(k-1) for k = KS+2..KE-1 (ud3.F90); 6-point ones: for
+     * k = KS+2..KE-2 from val(k-3..k+2), and at KE-2 the 3-point form of the KE-1
+     * face one level lower (ud5.F90:604-657, cd6.F90) */
+    const int wide = og_wide(scheme), kend = wide ? KE - 2 : KE - 1;
 #pragma omp parallel for collapse(2)
     for (int j = b.JJS; j <= b.JJE; ++j)
         for (int i = b.IIS; i <= b.IIE; ++i) {
-            for (int k = KS + 2; k <= KE - 1; ++k) {
+            for (int k = KS + 2; k <= kend; ++k) {
                 double vel = (0.5 * (mom[I3(k, i, j)] + mom[I3(k, i, j - 1)])) / DENS[I3(k, i, j)];
                 vel = vel * J23G[I3(k, i, j)];
-                flux[I3(k - 1, i, j)] = vel / MP(MAPF, i, j, 1)
-                                        * og_ip4(scheme, vel, val[I3(k - 2, i, j)], val[I3(k - 1, i, j)],
-                                                 val[I3(k, i, j)], val[I3(k + 1, i, j)]);
+                const double q = wide ? og_ip6(scheme, vel, val[I3(k - 3, i, j)], val[I3(k - 2, i, j)], val[I3(k - 1, i, j)],
+                                               val[I3(k, i, j)], val[I3(k + 1, i, j)], val[I3(k + 2, i, j)])
+                                      : og_ip4(scheme, vel, val[I3(k - 2, i, j)], val[I3(k - 1, i, j)],
+                                               val[I3(k, i, j)], val[I3(k + 1, i, j)]);
+                flux[I3(k - 1, i, j)] = vel / MP(MAPF, i, j, 1) * q;
             }
             flux[I3(KS - 1, i, j)] = 0.0;
             double vel = ((0.5 * (mom[I3(KS + 1, i, j)] + mom[I3(KS + 1, i, j - 1)])) / DENS[I3(KS + 1, i, j)]
@@ -152,6 +162,12 @@ void og_fluxJ23_XYW(const og_dims *d, int scheme, double *flux, const double *mo
             vel = vel * J23G[I3(KS + 1, i, j)];
             flux[I3(KS, i, j)] = vel / MP(MAPF, i, j, 1)
                                  * og_ipL(scheme, vel, val[I3(KS, i, j)], val[I3(KS + 1, i, j)], val[I3(KS + 2, i, j)]);
+            if (wide) {
+                vel = (0.5 * (mom[I3(KE - 1, i, j)] + mom[I3(KE - 1, i, j - 1)])) / DENS[I3(KE - 1, i, j)];
+                vel = vel * J23G[I3(KE - 1, i, j)];
+                flux[I3(KE - 2, i, j)] = vel / MP(MAPF, i, j, 1)
+                                         * og_ipH(scheme, vel, val[I3(KE - 1, i, j)], val[I3(KE - 2, i, j)], val[I3(KE - 3, i, j)]);
+            }
             flux[I3(KE - 1, i, j)] = 0.0;
         }
 }
@@ -170,8 +186,7 @@ void og_fluxX_XYW(const og_dims *d, int scheme, double *flux, const double *mom,
                              / (F2H(k, 1) * 0.5 * (DENS[I3(k + 1, i, j)] + DENS[I3(k + 1, i + 1, j)])
                                 + F2H(k, 2) * 0.5 * (DENS[I3(k, i, j)] + DENS[I3(k, i + 1, j)]));
                 flux[I3(k, i, j)] = GSQRT[I3(k, i, j)] / MP(MAPF, i, j, 2) * vel
-                                    * og_ip4(scheme, vel, val[I3(k, i - 1, j)], val[I3(k, i, j)],
-                                             val[I3(k, i + 1, j)], val[I3(k, i + 2, j)])
+                                    * og_hface(scheme, vel, &val[I3(k, i, j)], (long)KA)
                                     + GSQRT[I3(k, i, j)] * nd[I3(k, i, j)];
             }
             flux[I3(KE, i, j)] = 0.0;
@@ -192,8 +207,7 @@ void og_fluxY_XYW(const og_dims *d, int scheme, double *flux, const double *mom,
                              / (F2H(k, 1) * 0.5 * (DENS[I3(k + 1, i, j)] + DENS[I3(k + 1, i, j + 1)])
                                 + F2H(k, 2) * 0.5 * (DENS[I3(k, i, j)] + DENS[I3(k, i, j + 1)]));
                 flux[I3(k, i, j)] = GSQRT[I3(k, i, j)] / MP(MAPF, i, j, 1) * vel
-                                    * og_ip4(scheme, vel, val[I3(k, i, j - 1)], val[I3(k, i, j)],
-                                             val[I3(k, i, j + 1)], val[I3(k, i, j + 2)])
+                                    * og_hface(scheme, vel, &val[I3(k, i, j)], (long)KA * IA)
                                     + GSQRT[I3(k, i, j)] * nd[I3(k, i, j)];
             }
             flux[I3(KE, i, j)] = 0.0;
@@ -215,19 +229,12 @@ void og_fluxZ_UYZ(const og_dims *d, int scheme, double *flux, const double *mom,
 #pragma omp parallel for collapse(2)
     for (int j = b.JJS; j <= b.JJE; ++j)
         for (int i = b.IIS; i <= b.IIE; ++i) {
-            for (int k = KS + 1; k <= KE - 2; ++k) {
+            for (int k = KS; k <= KE - 1; ++k) {
                 double vel = (0.5 * (mom[I3(k, i, j)] + mom[I3(k, i + 1, j)])) / DEN_UYZ(k);
-                flux[I3(k, i, j)] = J33G * vel * og_ip4(scheme, vel, val[I3(k - 1, i, j)], val[I3(k, i, j)],
-                                                        val[I3(k + 1, i, j)], val[I3(k + 2, i, j)])
+                flux[I3(k, i, j)] = J33G * vel * og_zface(scheme, vel, &val[I3(1, i, j)], k, KS, KE)
                                     + GSQRT[I3(k, i, j)] * nd[I3(k, i, j)];
             }
             flux[I3(KS - 1, i, j)] = 0.0;
-            double vel = (0.5 * (mom[I3(KS, i, j)] + mom[I3(KS, i + 1, j)])) / DEN_UYZ(KS);
-            flux[I3(KS, i, j)] = J33G * vel * og_ipL(scheme, vel, val[I3(KS, i, j)], val[I3(KS + 1, i, j)], val[I3(KS + 2, i, j)])
-                                 + GSQRT[I3(KS, i, j)] * nd[I3(KS, i, j)];
-            vel = (0.5 * (mom[I3(KE - 1, i, j)] + mom[I3(KE - 1, i + 1, j)])) / DEN_UYZ(KE - 1);
-            flux[I3(KE - 1, i, j)] = J33G * vel * og_ipH(scheme, vel, val[I3(KE, i, j)], val[I3(KE - 1, i, j)], val[I3(KE - 2, i, j)])
-                                     + GSQRT[I3(KE - 1, i, j)] * nd[I3(KE - 1, i, j)];
             flux[I3(KE, i, j)] = 0.0;
         }
 }
@@ -241,22 +248,13 @@ void og_fluxJ13_UYZ(const og_dims *d, int scheme, double *flux, const double *mo
 #pragma omp parallel for collapse(2)
     for (int j = b.JJS; j <= b.JJE; ++j)
         for (int i = b.IIS; i <= b.IIE; ++i) {
-            for (int k = KS + 1; k <= KE - 2; ++k) {
+            for (int k = KS; k <= KE - 1; ++k) {
                 double vel = (F2H(k, 1) * mom[I3(k + 1, i, j)] + F2H(k, 2) * mom[I3(k, i, j)]) / DEN_UYZ(k);
                 vel = vel * J13G[I3(k, i, j)];
                 flux[I3(k, i, j)] = vel / MP(MAPF, i, j, 2)
-                                    * og_ip4(scheme, vel, val[I3(k - 1, i, j)], val[I3(k, i, j)],
-                                             val[I3(k + 1, i, j)], val[I3(k + 2, i, j)]);
+                                    * og_zface(scheme, vel, &val[I3(1, i, j)], k, KS, KE);
             }
             flux[I3(KS - 1, i, j)] = 0.0;
-            double vel = (F2H(KS, 1) * mom[I3(KS + 1, i, j)] + F2H(KS, 2) * mom[I3(KS, i, j)]) / DEN_UYZ(KS);
-            vel = vel * J13G[I3(KS, i, j)];
-            flux[I3(KS, i, j)] = vel / MP(MAPF, i, j, 2)
-                                 * og_ipL(scheme, vel, val[I3(KS, i, j)], val[I3(KS + 1, i, j)], val[I3(KS + 2, i, j)]);
-            vel = (F2H(KE - 1, 1) * mom[I3(KE, i, j)] + F2H(KE - 1, 2) * mom[I3(KE - 1, i, j)]) / DEN_UYZ(KE - 1);
-            vel = vel * J13G[I3(KE - 1, i, j)];
-            flux[I3(KE - 1, i, j)] = vel / MP(MAPF, i, j, 2)
-                                     * og_ipH(scheme, vel, val[I3(KE, i, j)], val[I3(KE - 1, i, j)], val[I3(KE - 2, i, j)]);
             flux[I3(KE, i, j)] = 0.0;
         }
 }
@@ -273,22 +271,13 @@ void og_fluxJ23_UYZ(const og_dims *d, int scheme, double *flux, const double *mo
 #pragma omp parallel for collapse(2)
     for (int j = b.JJS; j <= b.JJE; ++j)
         for (int i = b.IIS; i <= b.IIE; ++i) {
-            for (int k = KS + 1; k <= KE - 2; ++k) {
+            for (int k = KS; k <= KE - 1; ++k) {
                 double vel = (F2H(k, 1) * AVG4_UV(mom, k + 1) + F2H(k, 2) * AVG4_UV(mom, k)) / DEN_UYZ(k);
                 vel = vel * J23G[I3(k, i, j)];
                 flux[I3(k, i, j)] = vel / MP(MAPF, i, j, 1)
-                                    * og_ip4(scheme, vel, val[I3(k - 1, i, j)], val[I3(k, i, j)],
-                                             val[I3(k + 1, i, j)], val[I3(k + 2, i, j)]);
+                                    * og_zface(scheme, vel, &val[I3(1, i, j)], k, KS, KE);
             }
             flux[I3(KS - 1, i, j)] = 0.0;
-            double vel = (F2H(KS, 1) * AVG4_UV(mom, KS + 1) + F2H(KS, 2) * AVG4_UV(mom, KS)) / DEN_UYZ(KS);
-            vel = vel * J23G[I3(KS, i, j)];
-            flux[I3(KS, i, j)] = vel / MP(MAPF, i, j, 1)
-                                 * og_ipL(scheme, vel, val[I3(KS, i, j)], val[I3(KS + 1, i, j)], val[I3(KS + 2, i, j)]);
-            vel = (F2H(KE - 1, 1) * AVG4_UV(mom, KE) + F2H(KE - 1, 2) * AVG4_UV(mom, KE - 1)) / DEN_UYZ(KE - 1);
-            vel = vel * J23G[I3(KE - 1, i, j)];
-            flux[I3(KE - 1, i, j)] = vel / MP(MAPF, i, j, 1)
-                                     * og_ipH(scheme, vel, val[I3(KE, i, j)], val[I3(KE - 1, i, j)], val[I3(KE - 2, i, j)]);
             flux[I3(KE, i, j)] = 0.0;
         }
 }
@@ -304,8 +293,7 @@ void og_fluxX_UYZ(const og_dims *d, int scheme, double *flux, const double *mom,
             for (int k = KS; k <= KE; ++k) {
                 double vel = (0.5 * (mom[I3(k, i, j)] + mom[I3(k, i - 1, j)])) / (DENS[I3(k, i, j)]);
                 flux[I3(k, i - 1, j)] = GSQRT[I3(k, i, j)] / MP(MAPF, i, j, 2) * vel
-                                        * og_ip4(scheme, vel, val[I3(k, i - 2, j)], val[I3(k, i - 1, j)],
-                                                 val[I3(k, i, j)], val[I3(k, i + 1, j)])
+                                        * og_hface(scheme, vel, &val[I3(k, i - 1, j)], (long)KA)
                                         + GSQRT[I3(k, i, j)] * nd[I3(k, i, j)];
             }
 }
@@ -322,8 +310,7 @@ void og_fluxY_UYZ(const og_dims *d, int scheme, double *flux, const double *mom,
                 double vel = (0.5 * (mom[I3(k, i, j)] + mom[I3(k, i + 1, j)]))
                              / (0.25 * (DENS[I3(k, i, j)] + DENS[I3(k, i + 1, j)] + DENS[I3(k, i, j + 1)] + DENS[I3(k, i + 1, j + 1)]));
                 flux[I3(k, i, j)] = GSQRT[I3(k, i, j)] / MP(MAPF, i, j, 1) * vel
-                                    * og_ip4(scheme, vel, val[I3(k, i, j - 1)], val[I3(k, i, j)],
-                                             val[I3(k, i, j + 1)], val[I3(k, i, j + 2)])
+                                    * og_hface(scheme, vel, &val[I3(k, i, j)], (long)KA * IA)
                                     + GSQRT[I3(k, i, j)] * nd[I3(k, i, j)];
             }
 }
@@ -337,19 +324,12 @@ void og_fluxZ_XVZ(const og_dims *d, int scheme, double *flux, const double *mom,
 #pragma omp parallel for collapse(2)
     for (int j = b.JJS; j <= b.JJE; ++j)
         for (int i = b.IIS; i <= b.IIE; ++i) {
-            for (int k = KS + 1; k <= KE - 2; ++k) {
+            for (int k = KS; k <= KE - 1; ++k) {
                 double vel = (0.5 * (mom[I3(k, i, j)] + mom[I3(k, i, j + 1)])) / DEN_XVZ(k);
-                flux[I3(k, i, j)] = J33G * vel * og_ip4(scheme, vel, val[I3(k - 1, i, j)], val[I3(k, i, j)],
-                                                        val[I3(k + 1, i, j)], val[I3(k + 2, i, j)])
+                flux[I3(k, i, j)] = J33G * vel * og_zface(scheme, vel, &val[I3(1, i, j)], k, KS, KE)
                                     + GSQRT[I3(k, i, j)] * nd[I3(k, i, j)];
             }
             flux[I3(KS - 1, i, j)] = 0.0;
-            double vel = (0.5 * (mom[I3(KS, i, j)] + mom[I3(KS, i, j + 1)])) / DEN_XVZ(KS);
-            flux[I3(KS, i, j)] = J33G * vel * og_ipL(scheme, vel, val[I3(KS, i, j)], val[I3(KS + 1, i, j)], val[I3(KS + 2, i, j)])
-                                 + GSQRT[I3(KS, i, j)] * nd[I3(KS, i, j)];
-            vel = (0.5 * (mom[I3(KE - 1, i, j)] + mom[I3(KE - 1, i, j + 1)])) / DEN_XVZ(KE - 1);
-            flux[I3(KE - 1, i, j)] = J33G * vel * og_ipH(scheme, vel, val[I3(KE, i, j)], val[I3(KE - 1, i, j)], val[I3(KE - 2, i, j)])
-                                     + GSQRT[I3(KE - 1, i, j)] * nd[I3(KE - 1, i, j)];
             flux[I3(KE, i, j)] = 0.0;
         }
 }
@@ -365,22 +345,13 @@ void og_fluxJ13_XVZ(const og_dims *d, int scheme, double *flux, const double *mo
 #pragma omp parallel for collapse(2)
     for (int j = b.JJS; j <= b.JJE; ++j)
         for (int i = b.IIS; i <= b.IIE; ++i) {
-            for (int k = KS + 1; k <= KE - 2; ++k) {
+            for (int k = KS; k <= KE - 1; ++k) {
                 double vel = (F2H(k, 1) * AVG4_XV(mom, k + 1) + F2H(k, 2) * AVG4_XV(mom, k)) / DEN_XVZ(k);
                 vel = vel * J13G[I3(k, i, j)];
                 flux[I3(k, i, j)] = vel / MP(MAPF, i, j, 2)
-                                    * og_ip4(scheme, vel, val[I3(k - 1, i, j)], val[I3(k, i, j)],
-                                             val[I3(k + 1, i, j)], val[I3(k + 2, i, j)]);
+                                    * og_zface(scheme, vel, &val[I3(1, i, j)], k, KS, KE);
             }
             flux[I3(KS - 1, i, j)] = 0.0;
-            double vel = (F2H(KS, 1) * AVG4_XV(mom, KS + 1) + F2H(KS, 2) * AVG4_XV(mom, KS)) / DEN_XVZ(KS);
-            vel = vel * J13G[I3(KS, i, j)];
-            flux[I3(KS, i, j)] = vel / MP(MAPF, i, j, 2)
-                                 * og_ipL(scheme, vel, val[I3(KS, i, j)], val[I3(KS + 1, i, j)], val[I3(KS + 2, i, j)]);
-            vel = (F2H(KE - 1, 1) * AVG4_XV(mom, KE) + F2H(KE - 1, 2) * AVG4_XV(mom, KE - 1)) / DEN_XVZ(KE - 1);
-            vel = vel * J13G[I3(KE - 1, i, j)];
-            flux[I3(KE - 1, i, j)] = vel / MP(MAPF, i, j, 2)
-                                     * og_ipH(scheme, vel, val[I3(KE, i, j)], val[I3(KE - 1, i, j)], val[I3(KE - 2, i, j)]);
             flux[I3(KE, i, j)] = 0.0;
         }
 }
@@ -394,22 +365,13 @@ void og_fluxJ23_XVZ(const og_dims *d, int scheme, double *flux, const double *mo
 #pragma omp parallel for collapse(2)
     for (int j = b.JJS; j <= b.JJE; ++j)
         for (int i = b.IIS; i <= b.IIE; ++i) {
-            for (int k = KS + 1; k <= KE - 2; ++k) {
+            for (int k = KS; k <= KE - 1; ++k) {
                 double vel = (F2H(k, 1) * mom[I3(k + 1, i, j)] + F2H(k, 2) * mom[I3(k, i, j)]) / DEN_XVZ(k);
                 vel = vel * J23G[I3(k, i, j)];
                 flux[I3(k, i, j)] = vel / MP(MAPF, i, j, 1)
-                                    * og_ip4(scheme, vel, val[I3(k - 1, i, j)], val[I3(k, i, j)],
-                                             val[I3(k + 1, i, j)], val[I3(k + 2, i, j)]);
+                                    * og_zface(scheme, vel, &val[I3(1, i, j)], k, KS, KE);
             }
             flux[I3(KS - 1, i, j)] = 0.0;
-            double vel = (F2H(KS, 1) * mom[I3(KS + 1, i, j)] + F2H(KS, 2) * mom[I3(KS, i, j)]) / DEN_XVZ(KS);
-            vel = vel * J23G[I3(KS, i, j)];
-            flux[I3(KS, i, j)] = vel / MP(MAPF, i, j, 1)
-                                 * og_ipL(scheme, vel, val[I3(KS, i, j)], val[I3(KS + 1, i, j)], val[I3(KS + 2, i, j)]);
-            vel = (F2H(KE - 1, 1) * mom[I3(KE, i, j)] + F2H(KE - 1, 2) * mom[I3(KE - 1, i, j)]) / DEN_XVZ(KE - 1);
-            vel = vel * J23G[I3(KE - 1, i, j)];
-            flux[I3(KE - 1, i, j)] = vel / MP(MAPF, i, j, 1)
-                                     * og_ipH(scheme, vel, val[I3(KE, i, j)], val[I3(KE - 1, i, j)], val[I3(KE - 2, i, j)]);
             flux[I3(KE, i, j)] = 0.0;
         }
 }
@@ -426,8 +388,7 @@ void og_fluxX_XVZ(const og_dims *d, int scheme, double *flux, const double *mom,
                 double vel = (0.5 * (mom[I3(k, i, j)] + mom[I3(k, i, j + 1)]))
                              / (0.25 * (DENS[I3(k, i, j)] + DENS[I3(k, i + 1, j)] + DENS[I3(k, i, j + 1)] + DENS[I3(k, i + 1, j + 1)]));
                 flux[I3(k, i, j)] = GSQRT[I3(k, i, j)] / MP(MAPF, i, j, 2) * vel
-                                    * og_ip4(scheme, vel, val[I3(k, i - 1, j)], val[I3(k, i, j)],
-                                             val[I3(k, i + 1, j)], val[I3(k, i + 2, j)])
+                                    * og_hface(scheme, vel, &val[I3(k, i, j)], (long)KA)
                                     + GSQRT[I3(k, i, j)] * nd[I3(k, i, j)];
             }
 }
@@ -443,8 +404,7 @@ void og_fluxY_XVZ(const og_dims *d, int scheme, double *flux, const double *mom,
             for (int k = KS; k <= KE; ++k) {
                 double vel = (0.5 * (mom[I3(k, i, j)] + mom[I3(k, i, j - 1)])) / (DENS[I3(k, i, j)]);
                 flux[I3(k, i, j - 1)] = GSQRT[I3(k, i, j)] / MP(MAPF, i, j, 1) * vel
-                                        * og_ip4(scheme, vel, val[I3(k, i, j - 2)], val[I3(k, i, j - 1)],
-                                                 val[I3(k, i, j)], val[I3(k, i, j + 1)])
+                                        * og_hface(scheme, vel, &val[I3(k, i, j - 1)], (long)KA * IA)
                                         + GSQRT[I3(k, i, j)] * nd[I3(k, i, j)];
             }
 }

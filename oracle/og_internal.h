@@ -75,7 +75,7 @@ static inline double og_ip4(int scheme, double vel, double vm1, double v0, doubl
 /* one-sided value at the KS face from val(KS), val(KS+1), val(KS+2) */
 static inline double og_ipL(int scheme, double vel, double v0, double v1, double v2)
 {
-    if (scheme == OG_UD3)
+    if (scheme == OG_UD3 || scheme == OG_UD5)
         return F2_ * (v1 + v0) * (0.5 + og_sign(0.5, vel)) + (2.0 * v0 + 5.0 * v1 - v2) / 6.0 * (0.5 - og_sign(0.5, vel));
     if (scheme == OG_KOREN)
         return v0 * (0.5 + og_sign(0.5, vel)) + (v1 + 0.5 * og_koren_phi(v0, v1, v2) * (v1 - v2)) * (0.5 - og_sign(0.5, vel));
@@ -84,11 +84,81 @@ static inline double og_ipL(int scheme, double vel, double v0, double v1, double
 /* one-sided value at the KE-1 face from val(KE), val(KE-1), val(KE-2) */
 static inline double og_ipH(int scheme, double vel, double vE, double vE1, double vE2)
 {
-    if (scheme == OG_UD3)
+    if (scheme == OG_UD3 || scheme == OG_UD5)
         return (2.0 * vE + 5.0 * vE1 - vE2) / 6.0 * (0.5 + og_sign(0.5, vel)) + F2_ * (vE + vE1) * (0.5 - og_sign(0.5, vel));
     if (scheme == OG_KOREN)
         return (vE1 + 0.5 * og_koren_phi(vE2, vE1, vE) * (vE1 - vE)) * (0.5 + og_sign(0.5, vel)) + vE * (0.5 - og_sign(0.5, vel));
     return F2_ * (vE + vE1);
+}
+
+/* ---- 6-point schemes (scale_atmos_dyn_fvm_flux_ud5.F90, ..._cd6.F90; one
+ * generator template, scale_atmos_dyn_fvm_flux_udcd.F90.erb). The interior face
+ * value uses two points more on each side (IHALO = JHALO = 3); in z, where the
+ * halo is 2, the faces KS+1 and KE-2 take the forms og_ipL2/og_ipH2 and the
+ * faces KS and KE-1 the UD3 (UD5) or F2 (CD6) forms of og_ipL/og_ipH. */
+#define F51 (1.0 / 60.0)
+#define F52 (-8.0 / 60.0)
+#define F53 (37.0 / 60.0)
+#define F54 (-5.0 / 60.0)
+#define F55 (10.0 / 60.0)
+#define F61 (37.0 / 60.0)
+#define F62 (-8.0 / 60.0)
+#define F63 (1.0 / 60.0)
+
+static inline int og_wide(int scheme) { return scheme == OG_UD5 || scheme == OG_CD6; }
+
+/* ud5.F90:92-96,133-138 ; cd6.F90:89-91,130-132. The face lies between v0 and vp1. */
+static inline double og_ip6(int scheme, double vel, double vm2, double vm1, double v0, double vp1, double vp2,
+                            double vp3)
+{
+    if (scheme == OG_UD5)
+        return (F51 * (vp3 + vm2) + F52 * (vp2 + vm1) + F53 * (vp1 + v0))
+               - (F51 * (vp3 - vm2) + F54 * (vp2 - vm1) + F55 * (vp1 - v0)) * og_sign(1.0, vel);
+    if (scheme == OG_CD6)
+        return F61 * (vp1 + v0) + F62 * (vp2 + vm1) + F63 * (vp3 + vm2);
+    return og_ip4(scheme, vel, vm1, v0, vp1, vp2);
+}
+/* the KS+1 face from val(KS..KS+4): ud5.F90:171-177, cd6.F90:159-160 */
+static inline double og_ipL2(int scheme, double vel, double v0, double v1, double v2, double v3, double v4)
+{
+    if (scheme == OG_UD5)
+        return (2.0 * v2 + 5.0 * v1 - v0) / 6.0 * (0.5 + og_sign(0.5, vel))
+               + (-3.0 * v0 + 27.0 * v1 + 47.0 * v2 - 13.0 * v3 + 2.0 * v4) / 60.0 * (0.5 - og_sign(0.5, vel));
+    return F41 * (v2 + v1) + F42 * (v3 + v0);
+}
+/* the KE-2 face from val(KE), val(KE-1), ..., val(KE-4): ud5.F90:179-185, cd6.F90:161-162 */
+static inline double og_ipH2(int scheme, double vel, double vE, double vE1, double vE2, double vE3, double vE4)
+{
+    if (scheme == OG_UD5)
+        return (-3.0 * vE + 27.0 * vE1 + 47.0 * vE2 - 13.0 * vE3 + 2.0 * vE4) / 60.0 * (0.5 + og_sign(0.5, vel))
+               + (2.0 * vE2 + 5.0 * vE1 - vE) / 6.0 * (0.5 - og_sign(0.5, vel));
+    return F41 * (vE1 + vE2) + F42 * (vE + vE3);
+}
+
+/* Face value between p[0] and p[s] along a horizontal direction of stride s:
+ * the 4-point value from p[-s..2s], or the 6-point one from p[-2s..3s]. */
+static inline double og_hface(int scheme, double vel, const double *p, long s)
+{
+    if (og_wide(scheme)) return og_ip6(scheme, vel, p[-2 * s], p[-s], p[0], p[s], p[2 * s], p[3 * s]);
+    return og_ip4(scheme, vel, p[-s], p[0], p[s], p[2 * s]);
+}
+
+/* Face value at the w-level m (between levels m and m+1) of a column whose
+ * level l is col[l-1], with the near-wall forms of the scheme: og_ipL at KS,
+ * og_ipH at KE-1, and for the 6-point schemes og_ipL2 at KS+1, og_ipH2 at KE-2
+ * (the k-loops KS+1..KE-2 of ud3.F90 and KS+2..KE-3 of ud5.F90/cd6.F90). */
+static inline double og_zface(int scheme, double vel, const double *col, int m, int KS, int KE)
+{
+#define V_(l) col[(l) - 1]
+    if (m == KS) return og_ipL(scheme, vel, V_(KS), V_(KS + 1), V_(KS + 2));
+    if (m == KE - 1) return og_ipH(scheme, vel, V_(KE), V_(KE - 1), V_(KE - 2));
+    if (og_wide(scheme)) {
+        if (m == KS + 1) return og_ipL2(scheme, vel, V_(KS), V_(KS + 1), V_(KS + 2), V_(KS + 3), V_(KS + 4));
+        if (m == KE - 2) return og_ipH2(scheme, vel, V_(KE), V_(KE - 1), V_(KE - 2), V_(KE - 3), V_(KE - 4));
+        return og_ip6(scheme, vel, V_(m - 2), V_(m - 1), V_(m), V_(m + 1), V_(m + 2), V_(m + 3));
+    }
+    return og_ip4(scheme, vel, V_(m - 1), V_(m), V_(m + 1), V_(m + 2));
+#undef V_
 }
 
 /* ---- flux family (19 routines), one generic restatement per reference routine ---- */

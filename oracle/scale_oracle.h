@@ -43,7 +43,8 @@ typedef struct {
 } og_dims;
 
 /* flux scheme ids (scale_atmos_dyn_fvm_flux.F90:276 setup by name) */
-enum { OG_UD3 = 1, OG_CD4 = 2, OG_KOREN = 3, OG_CD2 = 4 }; /* OG_KOREN: UD3KOREN1993 */
+enum { OG_UD3 = 1, OG_CD4 = 2, OG_KOREN = 3, OG_CD2 = 4, OG_UD5 = 5, OG_CD6 = 6 }; /* OG_KOREN: UD3KOREN1993;
+ * OG_UD5 and OG_CD6 need IHALO = JHALO = 3 */
 
 /* physical constants, scale_const.F90 */
 #define OG_GRAV   9.80665

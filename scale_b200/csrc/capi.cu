@@ -209,8 +209,10 @@ int parse_scheme(const char *s, int *out)
     if (n == "CD4") { *out = CD4; return SCALE_HEVI_OK; }
     if (n == "UD3KOREN1993") { *out = KOREN; return SCALE_HEVI_OK; }
     if (n == "CD2") { *out = CD2; return SCALE_HEVI_OK; }
-    return fail(SCALE_HEVI_ERR_UNSUPPORTED, "flux scheme '%s' is not supported (UD3, CD4, UD3KOREN1993, CD2)",
-                n.c_str());
+    if (n == "UD5") { *out = UD5; return SCALE_HEVI_OK; }
+    if (n == "CD6") { *out = CD6; return SCALE_HEVI_OK; }
+    return fail(SCALE_HEVI_ERR_UNSUPPORTED,
+                "flux scheme '%s' is not supported (UD3, CD4, UD3KOREN1993, CD2, UD5, CD6)", n.c_str());
 }
 
 // host-array entries: a device buffer per argument role, grown on demand
@@ -292,8 +294,9 @@ int prepare_tables(const double *CDZ, const double *FDZ, const double *RCDZ, con
     double *z = h.data(), *x = z + 7 * ZT, *y = x + 4 * XT;
     if (!CDZ || !FDZ || !RCDZ || !RFDZ || !FDX || !RCDX || !RFDX || !FDY || !RCDY || !RFDY)
         return fail(SCALE_HEVI_ERR_ARG, "a 1-D grid vector is NULL");
+    const int H = C.g.IHALO; // lateral halo of every member
     for (const MemberGeom &m : C.members) {
-        const int KA = m.KMAX + 4, IA = m.IMAX + 4, JA = m.JMAX + 4, z0 = m.z0, x0 = m.x0, y0 = m.y0;
+        const int KA = m.KMAX + 4, IA = m.IMAX + 2 * H, JA = m.JMAX + 2 * H, z0 = m.z0, x0 = m.x0, y0 = m.y0;
         std::memcpy(z + z0, CDZ + z0, KA * sizeof(double));
         std::memcpy(z + ZT + z0, FDZ + z0, (KA - 1) * sizeof(double));
         std::memcpy(z + 2 * ZT + z0, RCDZ + z0, KA * sizeof(double));
@@ -340,9 +343,10 @@ int prepare_nd(const double *CDZ, const double *CDX, const double *CDY, const do
     const size_t oZ4 = ofdy + YT, oX4 = oZ4 + 10 * ZT, oY4 = oX4 + 10 * XT, oend = oY4 + 10 * YT;
     if (key != C.nd_key) {
         std::vector<double> h(oend, 0.0);
+        const int H = C.g.IHALO; // lateral halo of every member
         for (const MemberGeom &m : C.members) {
-            const int KA = m.KMAX + 4, IA = m.IMAX + 4, JA = m.JMAX + 4, z0 = m.z0, x0 = m.x0, y0 = m.y0;
-            NdGrid gr{KA, IA, JA, 3, m.KMAX + 2, 3, m.IMAX + 2, 3, m.JMAX + 2,
+            const int KA = m.KMAX + 4, IA = m.IMAX + 2 * H, JA = m.JMAX + 2 * H, z0 = m.z0, x0 = m.x0, y0 = m.y0;
+            NdGrid gr{KA, IA, JA, 3, m.KMAX + 2, H + 1, m.IMAX + H, H + 1, m.JMAX + H,
                       CDZ + z0, FDZ + z0, CDX + x0, FDX + x0, CDY + y0, FDY + y0};
             NdTables t;
             build_nd_tables(gr, DT, ND_COEF, ND_ORDER, t);
@@ -606,14 +610,16 @@ extern "C" {
 // checks of one index set (of a domain or an ensemble member)
 static int check_index(const scale_hevi_index &x)
 {
-    if (x.KHALO != 2 || x.IHALO != 2 || x.JHALO != 2) return fail(SCALE_HEVI_ERR_UNSUPPORTED, "halo width must be 2");
+    if (x.KHALO != 2 || x.IHALO != x.JHALO || x.IHALO < 2 || x.IHALO > 3)
+        return fail(SCALE_HEVI_ERR_UNSUPPORTED, "halo widths must be KHALO = 2 and IHALO = JHALO = 2 or 3 (got %d, %d, %d)",
+                    x.KHALO, x.IHALO, x.JHALO);
     if (x.KA != x.KMAX + 2 * x.KHALO || x.IA != x.IMAX + 2 * x.IHALO || x.JA != x.JMAX + 2 * x.JHALO ||
         x.KS != 1 + x.KHALO || x.KE != x.KMAX + x.KHALO || x.IS != 1 + x.IHALO || x.IE != x.IMAX + x.IHALO ||
         x.JS != 1 + x.JHALO || x.JE != x.JMAX + x.JHALO)
         return fail(SCALE_HEVI_ERR_ARG, "index set is inconsistent (KA=%d KMAX=%d KS=%d KE=%d IA=%d IMAX=%d JA=%d JMAX=%d)",
                     x.KA, x.KMAX, x.KS, x.KE, x.IA, x.IMAX, x.JA, x.JMAX);
     if (x.KMAX < 4 || x.KA > 260) return fail(SCALE_HEVI_ERR_UNSUPPORTED, "KMAX must be in 4..256 (got %d)", x.KMAX);
-    if (x.IMAX < 2 || x.JMAX < 2) return fail(SCALE_HEVI_ERR_ARG, "IMAX and JMAX must be >= IHALO, JHALO");
+    if (x.IMAX < x.IHALO || x.JMAX < x.JHALO) return fail(SCALE_HEVI_ERR_ARG, "IMAX and JMAX must be >= IHALO, JHALO");
     if ((x.IBLOCK > 0 && x.IBLOCK != x.IMAX) || (x.JBLOCK > 0 && x.JBLOCK != x.JMAX))
         return fail(SCALE_HEVI_ERR_UNSUPPORTED, "only the default IBLOCK=IMAX, JBLOCK=JMAX blocking is supported");
     return SCALE_HEVI_OK;
@@ -632,6 +638,7 @@ int scale_hevi_ensemble_setup(int n, const scale_hevi_index *idx, const char *fl
     for (int m = 0; m < n; ++m) {
         const scale_hevi_index &x = idx[m];
         CK(check_index(x));
+        if (x.IHALO != idx[0].IHALO) return fail(SCALE_HEVI_ERR_ARG, "ensemble members must share one halo width");
         mem[m] = MemberGeom{x.KMAX, x.IMAX, x.JMAX, (int)ZT, (int)XT, (int)YT, (int)N3, (int)N2};
         N3 += (size_t)x.KA * x.IA * x.JA;
         N2 += (size_t)x.IA * x.JA;
@@ -642,6 +649,13 @@ int scale_hevi_ensemble_setup(int n, const scale_hevi_index *idx, const char *fl
     int s1, s2;
     CK(parse_scheme(flux_type, &s1));
     CK(parse_scheme(flux_tracer_type, &s2));
+    // the 6-point schemes read three points on each side (scale_atmos_dyn_fvm_flux.F90:742-749)
+    if ((wide_scheme(s1) || wide_scheme(s2)) && idx[0].IHALO < 3)
+        return fail(SCALE_HEVI_ERR_ARG, "the UD5 and CD6 schemes need IHALO = JHALO = 3 (got %d)", idx[0].IHALO);
+    // their near-wall forms at KS+1 and KE-2 read five levels of the interior
+    for (int m = 0; m < n; ++m)
+        if ((wide_scheme(s1) || wide_scheme(s2)) && idx[m].KMAX < 5)
+            return fail(SCALE_HEVI_ERR_UNSUPPORTED, "the UD5 and CD6 schemes need KMAX >= 5 (got %d)", idx[m].KMAX);
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
         cudaGetLastError();
@@ -1287,6 +1301,8 @@ int scale_hevi_adjoint_setup(const double *DPRES0, const double *RT2P, const dou
                              const double *dt, const double *ND_COEF, const double *ND_SFC_FACT, const double *J33G)
 {
     CK(need_single("the differentiated short step"));
+    if (wide_scheme(C.scheme))
+        return fail(SCALE_HEVI_ERR_UNSUPPORTED, "the differentiated short step supports UD3, CD4, UD3KOREN1993 and CD2");
     const double *v[12] = {CDZ, CDX, CDY, FDZ, FDX, FDY, RCDZ, RCDX, RCDY, RFDZ, RFDX, RFDY};
     const int len[12] = {C.g.KA, C.g.IA, C.g.JA, C.g.KA - 1, C.g.IA - 1, C.g.JA - 1,
                          C.g.KA, C.g.IA, C.g.JA, C.g.KA - 1, C.g.IA - 1, C.g.JA - 1};

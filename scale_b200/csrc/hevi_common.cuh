@@ -21,7 +21,9 @@ namespace hevi {
 
 // flux schemes (ATMOS_DYN_FVM_FLUX_TYPE names)
 // (ATMOS_DYN_FVM_FLUX_TYPE / _TRACER_TYPE names: UD3, CD4, UD3KOREN1993, CD2)
-enum Scheme : int { UD3 = 1, CD4 = 2, KOREN = 3, CD2 = 4 };
+enum Scheme : int { UD3 = 1, CD4 = 2, KOREN = 3, CD2 = 4, UD5 = 5, CD6 = 6 };
+// the 6-point schemes, which read three points on each side (IHALO = JHALO = 3)
+__host__ __device__ constexpr bool wide_scheme(int s) { return s == UD5 || s == CD6; }
 
 struct Grid {
     int KA, IA, JA;
@@ -71,14 +73,16 @@ struct BatchT {
     MemberGeom m[NM];
 };
 
-// the member's Grid: sizes, offsets and table pointers of member M (halo 2)
+// the member's Grid: sizes, offsets and table pointers of member M (vertical
+// halo 2; the lateral halo IHALO = JHALO of the pooled grid t, common to all members)
 __host__ __device__ __forceinline__ Grid member_grid(const Grid &t, const MemberGeom &M)
 {
     Grid g = t;
+    const int H = t.IHALO;
     g.KMAX = M.KMAX; g.IMAX = M.IMAX; g.JMAX = M.JMAX;
-    g.KA = M.KMAX + 4; g.IA = M.IMAX + 4; g.JA = M.JMAX + 4;
-    g.KS = 3; g.KE = M.KMAX + 2; g.IS = 3; g.IE = M.IMAX + 2; g.JS = 3; g.JE = M.JMAX + 2;
-    g.IHALO = 2; g.JHALO = 2; g.IEH = g.IE; g.JEH = g.JE;
+    g.KA = M.KMAX + 4; g.IA = M.IMAX + 2 * H; g.JA = M.JMAX + 2 * H;
+    g.KS = 3; g.KE = M.KMAX + 2; g.IS = H + 1; g.IE = M.IMAX + H; g.JS = H + 1; g.JE = M.JMAX + H;
+    g.IHALO = H; g.JHALO = H; g.IEH = g.IE; g.JEH = g.JE;
     g.cell0 = M.cell0; g.c2 = M.c2; g.z0 = M.z0; g.x0 = M.x0; g.y0 = M.y0;
     g.CDZ = t.CDZ + M.z0; g.FDZ = t.FDZ + M.z0; g.RCDZ = t.RCDZ + M.z0; g.RFDZ = t.RFDZ + M.z0;
     g.F2H1 = t.F2H1 + M.z0; g.F2H2 = t.F2H2 + M.z0;
@@ -160,11 +164,12 @@ __device__ __forceinline__ R ip4(R vel, R vm1, R v0, R vp1, R vp2)
                + (vp1 + R(0.5) * koren_phi(v0, vp1, vp2) * (vp1 - vp2)) * (R(0.5) - fsign(R(0.5), vel));
     }
 }
-// value at the KS face from val(KS), val(KS+1), val(KS+2) (ud3.F90:142-145, cd4.F90:141)
+// value at the KS face from val(KS), val(KS+1), val(KS+2) (ud3.F90:142-145, cd4.F90:141;
+// UD5 and CD6 use the UD3 and the F2 form, ud5.F90:162-165, cd6.F90:156)
 template <int S, typename R>
 __device__ __forceinline__ R ipL(R vel, R v0, R v1, R v2)
 {
-    if constexpr (S == UD3)
+    if constexpr (S == UD3 || S == UD5)
         return R(0.5) * (v1 + v0) * (R(0.5) + fsign(R(0.5), vel))
                + (R(2.0) * v0 + R(5.0) * v1 - v2) / R(6.0) * (R(0.5) - fsign(R(0.5), vel));
     else if constexpr (S == KOREN)
@@ -173,11 +178,12 @@ __device__ __forceinline__ R ipL(R vel, R v0, R v1, R v2)
     else
         return R(0.5) * (v1 + v0);
 }
-// value at the KE-1 face from val(KE), val(KE-1), val(KE-2) (ud3.F90:146-149, cd4.F90:142)
+// value at the KE-1 face from val(KE), val(KE-1), val(KE-2) (ud3.F90:146-149, cd4.F90:142;
+// ud5.F90:166-169, cd6.F90:157)
 template <int S, typename R>
 __device__ __forceinline__ R ipH(R vel, R vE, R vE1, R vE2)
 {
-    if constexpr (S == UD3)
+    if constexpr (S == UD3 || S == UD5)
         return (R(2.0) * vE + R(5.0) * vE1 - vE2) / R(6.0) * (R(0.5) + fsign(R(0.5), vel))
                + R(0.5) * (vE + vE1) * (R(0.5) - fsign(R(0.5), vel));
     else if constexpr (S == KOREN)
@@ -185,6 +191,68 @@ __device__ __forceinline__ R ipH(R vel, R vE, R vE1, R vE2)
                + vE * (R(0.5) - fsign(R(0.5), vel));
     else
         return R(0.5) * (vE + vE1);
+}
+
+// ---- 6-point schemes: UD5 (scale_atmos_dyn_fvm_flux_ud5.F90) and CD6 (..._cd6.F90),
+// from the same generator template as UD3/CD4. Interior face value from two
+// more points on each side (ud5.F90:92-96,133-138; cd6.F90:89-91,130-132); for
+// the 4-point schemes ip6 is ip4 of the inner four points, whose callers then
+// never read the outer two (they are compile-time dead).
+template <int S, typename R>
+__device__ __forceinline__ R ip6(R vel, R vm2, R vm1, R v0, R vp1, R vp2, R vp3)
+{
+    if constexpr (S == UD5) {
+        const R F51 = R(1.0 / 60.0), F52 = R(-8.0 / 60.0), F53 = R(37.0 / 60.0), F54 = R(-5.0 / 60.0),
+                F55 = R(10.0 / 60.0);
+        return (F51 * (vp3 + vm2) + F52 * (vp2 + vm1) + F53 * (vp1 + v0))
+               - (F51 * (vp3 - vm2) + F54 * (vp2 - vm1) + F55 * (vp1 - v0)) * fsign(R(1.0), vel);
+    } else if constexpr (S == CD6) {
+        const R F61 = R(37.0 / 60.0), F62 = R(-8.0 / 60.0), F63 = R(1.0 / 60.0);
+        return F61 * (vp1 + v0) + F62 * (vp2 + vm1) + F63 * (vp3 + vm2);
+    } else {
+        return ip4<S>(vel, vm1, v0, vp1, vp2);
+    }
+}
+// the KS+1 face of the 6-point schemes from val(KS..KS+4) (ud5.F90:171-177, cd6.F90:159-160)
+template <int S, typename R>
+__device__ __forceinline__ R ipL2(R vel, R v0, R v1, R v2, R v3, R v4)
+{
+    if constexpr (S == UD5)
+        return (R(2.0) * v2 + R(5.0) * v1 - v0) / R(6.0) * (R(0.5) + fsign(R(0.5), vel))
+               + (R(-3.0) * v0 + R(27.0) * v1 + R(47.0) * v2 - R(13.0) * v3 + R(2.0) * v4) / R(60.0)
+                     * (R(0.5) - fsign(R(0.5), vel));
+    else
+        return R(7.0 / 12.0) * (v2 + v1) + R(-1.0 / 12.0) * (v3 + v0);
+}
+// the KE-2 face of the 6-point schemes from val(KE), ..., val(KE-4) (ud5.F90:179-185, cd6.F90:161-162)
+template <int S, typename R>
+__device__ __forceinline__ R ipH2(R vel, R vE, R vE1, R vE2, R vE3, R vE4)
+{
+    if constexpr (S == UD5)
+        return (R(-3.0) * vE + R(27.0) * vE1 + R(47.0) * vE2 - R(13.0) * vE3 + R(2.0) * vE4) / R(60.0)
+                   * (R(0.5) + fsign(R(0.5), vel))
+               + (R(2.0) * vE2 + R(5.0) * vE1 - vE) / R(6.0) * (R(0.5) - fsign(R(0.5), vel));
+    else
+        return R(7.0 / 12.0) * (vE1 + vE2) + R(-1.0 / 12.0) * (vE + vE3);
+}
+
+// Face value at w-level m (between levels m and m+1) of a column; v(l) returns
+// the value at level l. The near-wall forms: ipL at KS, ipH at KE-1, and for
+// the 6-point schemes ipL2 at KS+1 and ipH2 at KE-2 (the interior loops are
+// KS+1..KE-2 in ud3.F90/cd4.F90 and KS+2..KE-3 in ud5.F90/cd6.F90). Only the
+// levels the chosen form needs are read.
+template <int S, typename R, typename V>
+__device__ __forceinline__ R zface(R vel, int m, int KS, int KE, const V &v)
+{
+    if (m == KS) return ipL<S>(vel, v(KS), v(KS + 1), v(KS + 2));
+    if (m == KE - 1) return ipH<S>(vel, v(KE), v(KE - 1), v(KE - 2));
+    if constexpr (wide_scheme(S)) {
+        if (m == KS + 1) return ipL2<S>(vel, v(KS), v(KS + 1), v(KS + 2), v(KS + 3), v(KS + 4));
+        if (m == KE - 2) return ipH2<S>(vel, v(KE), v(KE - 1), v(KE - 2), v(KE - 3), v(KE - 4));
+        return ip6<S>(vel, v(m - 2), v(m - 1), v(m), v(m + 1), v(m + 2), v(m + 3));
+    } else {
+        return ip4<S>(vel, v(m - 1), v(m), v(m + 1), v(m + 2));
+    }
 }
 
 // read-only load through the non-coherent cache

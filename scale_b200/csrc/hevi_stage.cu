@@ -159,13 +159,16 @@ __device__ __forceinline__ R adv_w_h(const Grid &g, const StageArgsT<R> &a, cons
                   / (f1 * h * (AR(DN, 1, 0, 0) + AR(DN, 1, 0, 1)) + f2 * h * (AR(DN, 0, 0, 0) + AR(DN, 0, 0, 1)));
     const R vYs = (f1 * AR(MY, 1, 0, -1) + f2 * AR(MY, 0, 0, -1))
                   / (f1 * h * (AR(DN, 1, 0, -1) + AR(DN, 1, 0, 0)) + f2 * h * (AR(DN, 0, 0, -1) + AR(DN, 0, 0, 0)));
+    constexpr bool W6 = wide_scheme(S); // the third points are read by the 6-point schemes only
     const R W_m2 = AR(MZ, 0, -2, 0), W_m1 = AR(MZ, 0, -1, 0), W_00 = AR(MZ, 0, 0, 0);
     const R W_p1 = AR(MZ, 0, 1, 0), W_p2 = AR(MZ, 0, 2, 0);
     const R V_m2 = AR(MZ, 0, 0, -2), V_m1 = AR(MZ, 0, 0, -1), V_p1 = AR(MZ, 0, 0, 1), V_p2 = AR(MZ, 0, 0, 2);
-    const R qXe = vXe * ip4<S>(vXe, W_m1, W_00, W_p1, W_p2) + AT(nd.WX(), 0, 0, 0);
-    const R qXw = vXw * ip4<S>(vXw, W_m2, W_m1, W_00, W_p1) + AT(nd.WX(), 0, -1, 0);
-    const R qYn = vYn * ip4<S>(vYn, V_m1, W_00, V_p1, V_p2) + AT(nd.WY(), 0, 0, 0);
-    const R qYs = vYs * ip4<S>(vYs, V_m2, V_m1, W_00, V_p1) + AT(nd.WY(), 0, 0, -1);
+    const R W_m3 = W6 ? AR(MZ, 0, -3, 0) : R(0.0), W_p3 = W6 ? AR(MZ, 0, 3, 0) : R(0.0);
+    const R V_m3 = W6 ? AR(MZ, 0, 0, -3) : R(0.0), V_p3 = W6 ? AR(MZ, 0, 0, 3) : R(0.0);
+    const R qXe = vXe * ip6<S>(vXe, W_m2, W_m1, W_00, W_p1, W_p2, W_p3) + AT(nd.WX(), 0, 0, 0);
+    const R qXw = vXw * ip6<S>(vXw, W_m3, W_m2, W_m1, W_00, W_p1, W_p2) + AT(nd.WX(), 0, -1, 0);
+    const R qYn = vYn * ip6<S>(vYn, V_m2, V_m1, W_00, V_p1, V_p2, V_p3) + AT(nd.WY(), 0, 0, 0);
+    const R qYs = vYs * ip6<S>(vYs, V_m3, V_m2, V_m1, W_00, V_p1, V_p2) + AT(nd.WY(), 0, 0, -1);
     return -((qXe - qXw) * rcdx + (qYn - qYs) * rcdy);
 }
 
@@ -188,6 +191,7 @@ __device__ __forceinline__ void update_mom(const Grid &g, const StageArgsT<R> &a
     const R ddc = use_div ? R(a.divdmp_coef / dt) : R(0.0);
     const int KS = g.KS, KE = g.KE;
     const unsigned FULL = 0xffffffffu;
+    constexpr bool W6 = wide_scheme(S); // the third points are read by the 6-point schemes only
 
     // z flux at (u,y,w), fluxZ_UYZ (ud3.F90:753-859); m is the lower level of the face
     auto qZu = [&](int m) -> R {
@@ -196,10 +200,7 @@ __device__ __forceinline__ void update_mom(const Grid &g, const StageArgsT<R> &a
         const R den = R(ld(g.F2H1 + m - 1)) * h * (AR(DN, dm + 1, 0, 0) + AR(DN, dm + 1, 1, 0))
                       + R(ld(g.F2H2 + m - 1)) * h * (AR(DN, dm, 0, 0) + AR(DN, dm, 1, 0));
         const R vel = (h * (AR(MZ, dm, 0, 0) + AR(MZ, dm, 1, 0))) / den;
-        R q;
-        if (m == KS) q = ipL<S>(vel, AR(MX, dm, 0, 0), AR(MX, dm + 1, 0, 0), AR(MX, dm + 2, 0, 0));
-        else if (m == KE - 1) q = ipH<S>(vel, AR(MX, dm + 1, 0, 0), AR(MX, dm, 0, 0), AR(MX, dm - 1, 0, 0));
-        else q = ip4<S>(vel, AR(MX, dm - 1, 0, 0), AR(MX, dm, 0, 0), AR(MX, dm + 1, 0, 0), AR(MX, dm + 2, 0, 0));
+        const R q = zface<S>(vel, m, KS, KE, [&](int l) { return AR(MX, l - k, 0, 0); });
         return J33G * vel * q + lds(nd.UZ() + c + dm);
     };
     // z flux at (x,v,w), fluxZ_XVZ (ud3.F90:1173-1279)
@@ -209,10 +210,7 @@ __device__ __forceinline__ void update_mom(const Grid &g, const StageArgsT<R> &a
         const R den = R(ld(g.F2H1 + m - 1)) * h * (AR(DN, dm + 1, 0, 0) + AR(DN, dm + 1, 0, 1))
                       + R(ld(g.F2H2 + m - 1)) * h * (AR(DN, dm, 0, 0) + AR(DN, dm, 0, 1));
         const R vel = (h * (AR(MZ, dm, 0, 0) + AR(MZ, dm, 0, 1))) / den;
-        R q;
-        if (m == KS) q = ipL<S>(vel, AR(MY, dm, 0, 0), AR(MY, dm + 1, 0, 0), AR(MY, dm + 2, 0, 0));
-        else if (m == KE - 1) q = ipH<S>(vel, AR(MY, dm + 1, 0, 0), AR(MY, dm, 0, 0), AR(MY, dm - 1, 0, 0));
-        else q = ip4<S>(vel, AR(MY, dm - 1, 0, 0), AR(MY, dm, 0, 0), AR(MY, dm + 1, 0, 0), AR(MY, dm + 2, 0, 0));
+        const R q = zface<S>(vel, m, KS, KE, [&](int l) { return AR(MY, l - k, 0, 0); });
         return J33G * vel * q + lds(nd.VZ() + c + dm);
     };
 
@@ -236,16 +234,19 @@ __device__ __forceinline__ void update_mom(const Grid &g, const StageArgsT<R> &a
         const R U_p1 = AR(MX, 0, 1, 0), U_p2 = AR(MX, 0, 2, 0);
         // x flux at (x,y,z) with the index shift of fluxX_UYZ (ud3.F90:1053-1109)
         const R vE = (h * (U_p1 + U_00)) / (AR(DN, 0, 1, 0));
-        const R qXe = vE * ip4<S>(vE, U_m1, U_00, U_p1, U_p2) + AT(nd.UX(), 0, 1, 0);
+        const R U_m3 = W6 ? AR(MX, 0, -3, 0) : R(0.0), U_p3 = W6 ? AR(MX, 0, 3, 0) : R(0.0);
+        const R qXe = vE * ip6<S>(vE, U_m2, U_m1, U_00, U_p1, U_p2, U_p3) + AT(nd.UX(), 0, 1, 0);
         const R vW = (h * (U_00 + U_m1)) / (AR(DN, 0, 0, 0));
-        const R qXw = vW * ip4<S>(vW, U_m2, U_m1, U_00, U_p1) + AT(nd.UX(), 0, 0, 0);
+        const R qXw = vW * ip6<S>(vW, U_m3, U_m2, U_m1, U_00, U_p1, U_p2) + AT(nd.UX(), 0, 0, 0);
         // y flux at (u,v,z), fluxY_UYZ (ud3.F90:1113-1167)
         const R vN = (h * (AR(MY, 0, 0, 0) + AR(MY, 0, 1, 0)))
                      / (qr * (AR(DN, 0, 0, 0) + AR(DN, 0, 1, 0) + AR(DN, 0, 0, 1) + AR(DN, 0, 1, 1)));
-        const R qYn = vN * ip4<S>(vN, AR(MX, 0, 0, -1), U_00, AR(MX, 0, 0, 1), AR(MX, 0, 0, 2)) + AT(nd.UY(), 0, 0, 0);
+        const R qYn = vN * ip6<S>(vN, W6 ? AR(MX, 0, 0, -2) : R(0.0), AR(MX, 0, 0, -1), U_00, AR(MX, 0, 0, 1),
+                                  AR(MX, 0, 0, 2), W6 ? AR(MX, 0, 0, 3) : R(0.0)) + AT(nd.UY(), 0, 0, 0);
         const R vS = (h * (AR(MY, 0, 0, -1) + AR(MY, 0, 1, -1)))
                      / (qr * (AR(DN, 0, 0, -1) + AR(DN, 0, 1, -1) + AR(DN, 0, 0, 0) + AR(DN, 0, 1, 0)));
-        const R qYs = vS * ip4<S>(vS, AR(MX, 0, 0, -2), AR(MX, 0, 0, -1), U_00, AR(MX, 0, 0, 1)) + AT(nd.UY(), 0, 0, -1);
+        const R qYs = vS * ip6<S>(vS, W6 ? AR(MX, 0, 0, -3) : R(0.0), AR(MX, 0, 0, -2), AR(MX, 0, 0, -1), U_00,
+                                  AR(MX, 0, 0, 1), W6 ? AR(MX, 0, 0, 2) : R(0.0)) + AT(nd.UY(), 0, 0, -1);
         const R advcv = -(q_k - q_km) * R(ld(g.RCDZ + k - 1));
         const R advch = -((qXe - qXw) * R(rfdx) + (qYn - qYs) * rcdy);
         const double DPe = AT(a.DPRES0, 0, 1, 0) + AT(a.RT2P, 0, 1, 0) * (AT(RT, 0, 1, 0) - AT(a.REF_rhot, 0, 1, 0));
@@ -265,15 +266,18 @@ __device__ __forceinline__ void update_mom(const Grid &g, const StageArgsT<R> &a
         // x flux at (u,v,z), fluxX_XVZ (ud3.F90:1473-1527)
         const R vE = (h * (AR(MX, 0, 0, 0) + AR(MX, 0, 0, 1)))
                      / (qr * (AR(DN, 0, 0, 0) + AR(DN, 0, 1, 0) + AR(DN, 0, 0, 1) + AR(DN, 0, 1, 1)));
-        const R qXe = vE * ip4<S>(vE, AR(MY, 0, -1, 0), Y_00, AR(MY, 0, 1, 0), AR(MY, 0, 2, 0)) + AT(nd.VX(), 0, 0, 0);
+        const R qXe = vE * ip6<S>(vE, W6 ? AR(MY, 0, -2, 0) : R(0.0), AR(MY, 0, -1, 0), Y_00, AR(MY, 0, 1, 0),
+                                  AR(MY, 0, 2, 0), W6 ? AR(MY, 0, 3, 0) : R(0.0)) + AT(nd.VX(), 0, 0, 0);
         const R vW = (h * (AR(MX, 0, -1, 0) + AR(MX, 0, -1, 1)))
                      / (qr * (AR(DN, 0, -1, 0) + AR(DN, 0, 0, 0) + AR(DN, 0, -1, 1) + AR(DN, 0, 0, 1)));
-        const R qXw = vW * ip4<S>(vW, AR(MY, 0, -2, 0), AR(MY, 0, -1, 0), Y_00, AR(MY, 0, 1, 0)) + AT(nd.VX(), 0, -1, 0);
+        const R qXw = vW * ip6<S>(vW, W6 ? AR(MY, 0, -3, 0) : R(0.0), AR(MY, 0, -2, 0), AR(MY, 0, -1, 0), Y_00,
+                                  AR(MY, 0, 1, 0), W6 ? AR(MY, 0, 2, 0) : R(0.0)) + AT(nd.VX(), 0, -1, 0);
         // y flux with the index shift of fluxY_XVZ (ud3.F90:1531-1587)
         const R vN = (h * (Y_p1 + Y_00)) / (AR(DN, 0, 0, 1));
-        const R qYn = vN * ip4<S>(vN, Y_m1, Y_00, Y_p1, Y_p2) + AT(nd.VY(), 0, 0, 1);
+        const R Y_m3 = W6 ? AR(MY, 0, 0, -3) : R(0.0), Y_p3 = W6 ? AR(MY, 0, 0, 3) : R(0.0);
+        const R qYn = vN * ip6<S>(vN, Y_m2, Y_m1, Y_00, Y_p1, Y_p2, Y_p3) + AT(nd.VY(), 0, 0, 1);
         const R vS = (h * (Y_00 + Y_m1)) / (AR(DN, 0, 0, 0));
-        const R qYs = vS * ip4<S>(vS, Y_m2, Y_m1, Y_00, Y_p1) + AT(nd.VY(), 0, 0, 0);
+        const R qYs = vS * ip6<S>(vS, Y_m3, Y_m2, Y_m1, Y_00, Y_p1, Y_p2) + AT(nd.VY(), 0, 0, 0);
         const R advcv = -(q_k - q_km) * R(ld(g.RCDZ + k - 1));
         const R advch = -((qXe - qXw) * rcdx + (qYn - qYs) * R(rfdy));
         const double DPn = AT(a.DPRES0, 0, 0, 1) + AT(a.RT2P, 0, 0, 1) * (AT(RT, 0, 0, 1) - AT(a.REF_rhot, 0, 0, 1));
@@ -374,20 +378,8 @@ __global__ void __launch_bounds__(32 * HEVI_COL_TC, HEVI_COL_MINB)
             if (L < KS || L > KE - 1) { pt = R(0.0); tz = R(0.0); return; }
             const R mZ = CL(nd.DZ(), L);
             const R M0 = R(CL(a.MOMZ, L));
-            R pi, ti;
-            if (L == KS) {
-                const R P0 = R(SA(CA_C, w, L)), P1 = R(SA(CA_C, w, L + 1)), P2 = R(SA(CA_C, w, L + 2));
-                pi = ipL<S>(M0, P0, P1, P2);
-                ti = ipL<S>(mZ, P0, P1, P2);
-            } else if (L == KE - 1) {
-                const R Pm1 = R(SA(CA_C, w, L - 1)), P0 = R(SA(CA_C, w, L)), P1 = R(SA(CA_C, w, L + 1));
-                pi = ipH<S>(M0, P1, P0, Pm1);
-                ti = ipH<S>(mZ, P1, P0, Pm1);
-            } else {
-                const R Pm1 = R(SA(CA_C, w, L - 1)), P0 = R(SA(CA_C, w, L)), P1 = R(SA(CA_C, w, L + 1)), P2 = R(SA(CA_C, w, L + 2));
-                pi = ip4<S>(M0, Pm1, P0, P1, P2);
-                ti = ip4<S>(mZ, Pm1, P0, P1, P2);
-            }
+            auto P = [&](int l) { return R(SA(CA_C, w, l)); };
+            const R pi = zface<S>(M0, L, KS, KE, P), ti = zface<S>(mZ, L, KS, KE, P);
             pt = pi;
             tz = mZ * ti + lds(nd.TZ() + col + L - 1);
         };
@@ -408,14 +400,17 @@ __global__ void __launch_bounds__(32 * HEVI_COL_TC, HEVI_COL_MINB)
                 if (td >= 0 && td < TY && j + d <= g.JE) return R(SA(CA_C, w + d * TX, L));
                 return AR(a.RHOT, 0, 0, d) / AR(a.DENS, 0, 0, d);
             };
+            constexpr bool W6 = wide_scheme(S);
             const R Pm2 = pott_x(-2), Pm1 = pott_x(-1), P00 = R(SA(CA_C, w, L)), Pp1 = pott_x(1), Pp2 = pott_x(2);
             const R Qm2 = pott_y(-2), Qm1 = pott_y(-1), Qp1 = pott_y(1), Qp2 = pott_y(2);
+            const R Pm3 = W6 ? pott_x(-3) : R(0.0), Pp3 = W6 ? pott_x(3) : R(0.0);
+            const R Qm3 = W6 ? pott_y(-3) : R(0.0), Qp3 = W6 ? pott_y(3) : R(0.0);
             const MassFlux<R> m = mass_flux(a, nd, c, sI, sJ);
             // fluxX/Y_XYZ (ud3.F90:251-353)
-            const R tXe = m.Xe * ip4<S>(m.Xe, Pm1, P00, Pp1, Pp2) + AT(nd.TX(), 0, 0, 0);
-            const R tXw = m.Xw * ip4<S>(m.Xw, Pm2, Pm1, P00, Pp1) + AT(nd.TX(), 0, -1, 0);
-            const R tYn = m.Yn * ip4<S>(m.Yn, Qm1, P00, Qp1, Qp2) + AT(nd.TY(), 0, 0, 0);
-            const R tYs = m.Ys * ip4<S>(m.Ys, Qm2, Qm1, P00, Qp1) + AT(nd.TY(), 0, 0, -1);
+            const R tXe = m.Xe * ip6<S>(m.Xe, Pm2, Pm1, P00, Pp1, Pp2, Pp3) + AT(nd.TX(), 0, 0, 0);
+            const R tXw = m.Xw * ip6<S>(m.Xw, Pm3, Pm2, Pm1, P00, Pp1, Pp2) + AT(nd.TX(), 0, -1, 0);
+            const R tYn = m.Yn * ip6<S>(m.Yn, Qm2, Qm1, P00, Qp1, Qp2, Qp3) + AT(nd.TY(), 0, 0, 0);
+            const R tYs = m.Ys * ip6<S>(m.Ys, Qm3, Qm2, Qm1, P00, Qp1, Qp2) + AT(nd.TY(), 0, 0, -1);
             const R adv_t = -((tXe - tXw) * rcdx + (tYn - tYs) * rcdy); // hevi_st :646-648
             put_flux(a, N3, 4, c, tXe, true);
             put_flux(a, N3, 5, c, tYn, true);
@@ -437,8 +432,8 @@ __global__ void __launch_bounds__(32 * HEVI_COL_TC, HEVI_COL_MINB)
             if (k < KS || k > KE - 2) return R(0.0);
             const R Mk = R(CL(a.MOMZ, k)), Mk1 = R(CL(a.MOMZ, k + 1));
             const R vel = (R(0.5) * (Mk + Mk1)) / R(CL(a.DENS, k + 1));
-            const R q = (k == KS) ? ipL<S>(vel, Mk, Mk1, R(CL(a.MOMZ, k + 2)))
-                                  : ip4<S>(vel, R(CL(a.MOMZ, k - 1)), Mk, Mk1, R(CL(a.MOMZ, k + 2)));
+            // fluxZ_XYW writes flux(k) for k = KS..KE-2 (ud3.F90:376-432, ud5.F90:479-571)
+            const R q = zface<S>(vel, k, KS, KE, [&](int l) { return R(CL(a.MOMZ, l)); });
             return J33R * vel * q + lds(nd.WZ() + col + k);
         };
         auto dpres = [&](int L) { return CL(a.DPRES0, L) + CL(a.RT2P, L) * (CL(a.RHOT, L) - CL(a.REF_rhot, L)); }; // :355
@@ -621,6 +616,8 @@ cudaError_t launch_hevi_stage(const Grid &g, const Members &mem, const StageArgs
         case CD4: return launch_one<CD4, R, TX, NM>(g, a, B, nb, smem, shape.raster, st);
         case KOREN: return launch_one<KOREN, R, TX, NM>(g, a, B, nb, smem, shape.raster, st);
         case CD2: return launch_one<CD2, R, TX, NM>(g, a, B, nb, smem, shape.raster, st);
+        case UD5: return launch_one<UD5, R, TX, NM>(g, a, B, nb, smem, shape.raster, st);
+        case CD6: return launch_one<CD6, R, TX, NM>(g, a, B, nb, smem, shape.raster, st);
         default: return cudaErrorInvalidValue;
         }
     };

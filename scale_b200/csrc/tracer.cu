@@ -30,17 +30,14 @@ __device__ __forceinline__ double ndq_at(const TracerArgs &a, size_t N3, int dir
     return a.ndq ? ld(a.ndq + (size_t)dir * N3 + c) : 0.0;
 }
 
-// high-order z flux at the face above level m (fluxZ_XYZ, ud3.F90:157-247)
+// high-order z flux at the face above level m (fluxZ_XYZ, ud3.F90:157-247, ud5.F90:194-321)
 template <int S>
 __device__ double hflux_z(const Grid &g, const TracerArgs &a, size_t N3, size_t col, int m)
 {
     if (m < g.KS || m > g.KE - 1) return 0.0;
     const double *q = a.QTRC + col - 1;
     const double vel = ld(a.mflx + col + m - 1);
-    double v;
-    if (m == g.KS) v = ipL<S>(vel, ld(q + m), ld(q + m + 1), ld(q + m + 2));
-    else if (m == g.KE - 1) v = ipH<S>(vel, ld(q + m + 1), ld(q + m), ld(q + m - 1));
-    else v = ip4<S>(vel, ld(q + m - 1), ld(q + m), ld(q + m + 1), ld(q + m + 2));
+    const double v = zface<S>(vel, m, g.KS, g.KE, [&](int l) { return ld(q + l); });
     return vel * v + ndq_at(a, N3, 0, col + m - 1);
 }
 // high-order flux at the face between c and c+s (fluxX/Y_XYZ, ud3.F90:251-353); dir 1 = x, 2 = y
@@ -49,7 +46,9 @@ __device__ __forceinline__ double hflux_h(const TracerArgs &a, size_t N3, int di
 {
     const double vel = ld(a.mflx + (size_t)dir * N3 + c);
     const double *q = a.QTRC + c;
-    return vel * ip4<S>(vel, ld(q - s), ld(q), ld(q + s), ld(q + 2 * s)) + ndq_at(a, N3, dir, c);
+    constexpr bool W6 = wide_scheme(S);
+    return vel * ip6<S>(vel, W6 ? ld(q - 2 * s) : 0.0, ld(q - s), ld(q), ld(q + s), ld(q + 2 * s), W6 ? ld(q + 3 * s) : 0.0)
+           + ndq_at(a, N3, dir, c);
 }
 // donor-cell flux at the face between c and c+s (ud1.F90:155-165)
 __device__ __forceinline__ double lflux(const TracerArgs &a, size_t N3, int dir, size_t c, long s)
@@ -296,6 +295,8 @@ cudaError_t launch_tracer_stage(const Grid &g, const TracerArgs &a, int scheme, 
     case CD4: return tracer_stage<CD4>(g, a, fct, st);
     case KOREN: return tracer_stage<KOREN>(g, a, fct, st);
     case CD2: return tracer_stage<CD2>(g, a, fct, st);
+    case UD5: return tracer_stage<UD5>(g, a, fct, st);
+    case CD6: return tracer_stage<CD6>(g, a, fct, st);
     default: return cudaErrorInvalidValue;
     }
 }

@@ -36,6 +36,12 @@ CVVAP = CPVAP - RVAP
 CL = 4218.0
 EPS = float(np.finfo(np.float64).eps)
 HALO = 2
+WIDE_SCHEMES = ("UD5", "CD6")  # 6-point flux schemes: IHALO = JHALO = 3
+
+
+def halo_for(*schemes) -> int:
+    """The lateral halo the flux schemes need (scale_atmos_dyn_fvm_flux.F90:742-749)."""
+    return 3 if any(s in WIDE_SCHEMES for s in schemes) else HALO
 
 
 @dataclass
@@ -48,12 +54,14 @@ class Grid:
     DX: float
     DY: float
     FZ: np.ndarray  # face heights of the interior levels KS..KE (KMAX values)
+    halo: int = HALO  # IHALO = JHALO (3 for the UD5/CD6 flux schemes); KHALO is always 2
 
     def __post_init__(self):
-        self.KA, self.IA, self.JA = self.KMAX + 2 * HALO, self.IMAX + 2 * HALO, self.JMAX + 2 * HALO
+        H = self.halo
+        self.KA, self.IA, self.JA = self.KMAX + 2 * HALO, self.IMAX + 2 * H, self.JMAX + 2 * H
         self.KS, self.KE = 1 + HALO, self.KMAX + HALO
-        self.IS, self.IE = 1 + HALO, self.IMAX + HALO
-        self.JS, self.JE = 1 + HALO, self.JMAX + HALO
+        self.IS, self.IE = 1 + H, self.IMAX + H
+        self.JS, self.JE = 1 + H, self.JMAX + H
         KA, KS, KE = self.KA, self.KS, self.KE
         fz = np.zeros(KA + 1)  # FZ(0:KA)
         fz[KS - 1] = 0.0
@@ -96,18 +104,18 @@ class Grid:
     def index_dict(self):
         return dict(KA=self.KA, IA=self.IA, JA=self.JA, KS=self.KS, KE=self.KE, IS=self.IS, IE=self.IE,
                     JS=self.JS, JE=self.JE, KMAX=self.KMAX, IMAX=self.IMAX, JMAX=self.JMAX,
-                    KHALO=HALO, IHALO=HALO, JHALO=HALO, IBLOCK=self.IMAX, JBLOCK=self.JMAX)
+                    KHALO=HALO, IHALO=self.halo, JHALO=self.halo, IBLOCK=self.IMAX, JBLOCK=self.JMAX)
 
 
-def uniform_grid(IMAX, JMAX, KMAX, DX, DY, DZ) -> Grid:
-    return Grid(IMAX, JMAX, KMAX, DX, DY, DZ * np.arange(1, KMAX + 1, dtype=np.float64))
+def uniform_grid(IMAX, JMAX, KMAX, DX, DY, DZ, halo=HALO) -> Grid:
+    return Grid(IMAX, JMAX, KMAX, DX, DY, DZ * np.arange(1, KMAX + 1, dtype=np.float64), halo)
 
 
-def stretched_grid(IMAX, JMAX, KMAX, DX, DY, dz_bottom, dz_top) -> Grid:
+def stretched_grid(IMAX, JMAX, KMAX, DX, DY, dz_bottom, dz_top, halo=HALO) -> Grid:
     """Face heights whose spacing grows geometrically from dz_bottom to dz_top."""
     r = (dz_top / dz_bottom) ** (1.0 / (KMAX - 1))
     dz = dz_bottom * r ** np.arange(KMAX)
-    return Grid(IMAX, JMAX, KMAX, DX, DY, np.cumsum(dz))
+    return Grid(IMAX, JMAX, KMAX, DX, DY, np.cumsum(dz), halo)
 
 
 # ---------------------------------------------------------------------------
@@ -387,20 +395,20 @@ def config(n: int, scale: float = 1.0, seed: int = 0) -> Case:
 ENSEMBLE_SIZES = [(64, 64, 64)] * 16 + [(128, 128, 96)] * 16 + [(256, 256, 96)] * 16
 
 
-def ensemble_member(IMAX: int, JMAX: int, KMAX: int, m: int, seed: int = 0) -> Case:
+def ensemble_member(IMAX: int, JMAX: int, KMAX: int, m: int, seed: int = 0, scheme: str = "UD3") -> Case:
     """Member m: one warm bubble at a seeded position with a seeded amplitude
     in [1, 4] K, and its own seeded +-0.01 K theta noise."""
-    g = uniform_grid(IMAX, JMAX, KMAX, 500.0, 500.0, 250.0)
+    g = uniform_grid(IMAX, JMAX, KMAX, 500.0, 500.0, 250.0, halo=halo_for(scheme))
     rng = np.random.Generator(np.random.PCG64(seed + 3000 + m))
     Lx, Ly = g.IMAX * 500.0, g.JMAX * 500.0
     bub = [(rng.uniform(0.0, Lx), rng.uniform(0.0, Ly), 2000.0, 4000.0, 4000.0, 4000.0, rng.uniform(1.0, 4.0))]
-    return make_case(f"ensemble member {m} {IMAX}x{JMAX}x{KMAX}", g, "UD3", "UD3", dt=1.0, dtl=5.0, bubbles=bub,
+    return make_case(f"ensemble member {m} {IMAX}x{JMAX}x{KMAX}", g, scheme, scheme, dt=1.0, dtl=5.0, bubbles=bub,
                      theta_noise=0.01, noise_kind="uniform", seed=seed + 100 + m)
 
 
-def ensemble(scale: float = 1.0, seed: int = 0, sizes=None) -> list[Case]:
+def ensemble(scale: float = 1.0, seed: int = 0, sizes=None, scheme: str = "UD3") -> list[Case]:
     """The members of the uneven ensemble (scale < 1 shrinks the horizontal
     sizes, for tests; sizes replaces the member list)."""
     sizes = ENSEMBLE_SIZES if sizes is None else sizes
-    return [ensemble_member(max(8, int(round(I * scale))), max(8, int(round(J * scale))), K, m, seed)
+    return [ensemble_member(max(8, int(round(I * scale))), max(8, int(round(J * scale))), K, m, seed, scheme)
             for m, (I, J, K) in enumerate(sizes)]

@@ -7,10 +7,15 @@ import oracle
 from scale_b200 import mkinit
 
 
-def small_grid(IMAX=12, JMAX=10, KMAX=16, DX=500.0, DY=400.0, DZ=250.0, stretched=False):
+def small_grid(IMAX=12, JMAX=10, KMAX=16, DX=500.0, DY=400.0, DZ=250.0, stretched=False, halo=2):
     if stretched:
-        return mkinit.stretched_grid(IMAX, JMAX, KMAX, DX, DY, 60.0, 400.0)
-    return mkinit.uniform_grid(IMAX, JMAX, KMAX, DX, DY, DZ)
+        return mkinit.stretched_grid(IMAX, JMAX, KMAX, DX, DY, 60.0, 400.0, halo=halo)
+    return mkinit.uniform_grid(IMAX, JMAX, KMAX, DX, DY, DZ, halo=halo)
+
+
+def halo_of(scheme):
+    """IHALO = JHALO a flux scheme needs (scale_atmos_dyn_fvm_flux.F90:742-749 for UD5/CD6)."""
+    return mkinit.halo_for(scheme)
 
 
 def small_case(g, scheme="UD3", seed=1, tracers=0, wind=2.0):

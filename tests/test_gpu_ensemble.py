@@ -120,3 +120,11 @@ def test_autotuned_shape_gives_identical_results(cases, alone):
     assert rep["path"] == "fp64" and len(rep["candidates"]) == 9
     assert [tx, r] == rep["chosen"][:2]
     assert min(c[2] for c in rep["candidates"]) == rep["chosen"][2]
+
+
+@pytest.mark.parametrize("scheme", ["UD5", "CD6"])
+def test_six_point_ensemble_matches_members_alone(scheme):
+    # members on a lateral halo of 3, advanced together and alone
+    cases = mkinit.ensemble(sizes=SIZES[:3], scheme=scheme)
+    assert all(c.g.IS == 4 for c in cases)
+    _same(_together(cases, 4)[0], _alone(cases, 4))

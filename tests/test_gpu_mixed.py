@@ -87,3 +87,16 @@ def test_mixed_precision_conserves_mass():
     drift = abs(m1 - m0) / m0
     print(f"mixed-precision mass drift after 50 short steps: {drift:.3e}")
     assert drift < 1e-8
+
+
+@pytest.mark.parametrize("scheme", ["UD5", "CD6"])
+def test_mixed_precision_six_point_schemes(scheme):
+    # a warm bubble on a lateral halo of 3, 100 short steps, FP32 fluxes against FP64
+    g = mkinit.uniform_grid(32, 32, 32, 200.0, 200.0, 200.0, halo=3)
+    c = mkinit.make_case("mixed six-point", g, scheme, scheme, dt=0.4, dtl=2.0,
+                         bubbles=[(3200.0, 3200.0, 2000.0, 1500.0, 1500.0, 1000.0, 2.0)], theta_noise=0.01, seed=7)
+    st64 = run_short_steps(c, 100, mixed=False)
+    st32 = run_short_steps(c, 100, mixed=True)
+    for n in STATE:
+        emax, erms = field_errors(st32[n], st64[n], c.g)
+        assert emax <= 1e-5, f"{n}: max {emax:.3e} rms {erms:.3e}"

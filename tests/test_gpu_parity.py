@@ -34,11 +34,14 @@ def _stage_call_args(a, o):
     return kw
 
 
-@pytest.mark.parametrize("scheme", ["UD3", "CD4", "UD3KOREN1993", "CD2"])
+SCHEMES = ["UD3", "CD4", "UD3KOREN1993", "CD2", "UD5", "CD6"]
+
+
+@pytest.mark.parametrize("scheme", SCHEMES)
 @pytest.mark.parametrize("stretched", [False, True])
 @pytest.mark.parametrize("full", [False, True])
 def test_stage_bit_exact(lib, scheme, stretched, full):
-    g = helpers.small_grid(IMAX=13, JMAX=9, KMAX=17, stretched=stretched)
+    g = helpers.small_grid(IMAX=13, JMAX=9, KMAX=17, stretched=stretched, halo=helpers.halo_of(scheme))
     c = helpers.small_case(g, scheme)
     helpers.perturb_state(c)
     a = helpers.short_inputs(c, dtrk=0.5, full=full)
@@ -74,9 +77,9 @@ def test_stage_device_entry_matches_host_entry(lib):
         assert np.array_equal(got, v), n
 
 
-@pytest.mark.parametrize("scheme", ["UD3", "CD4", "UD3KOREN1993", "CD2"])
+@pytest.mark.parametrize("scheme", SCHEMES)
 def test_rk4_short_step_bit_exact(lib, scheme):
-    g = helpers.small_grid(IMAX=14, JMAX=11, KMAX=18, stretched=(scheme == "CD4"))
+    g = helpers.small_grid(IMAX=14, JMAX=11, KMAX=18, stretched=scheme in ("CD4", "UD5"), halo=helpers.halo_of(scheme))
     c = helpers.small_case(g, scheme)
     helpers.perturb_state(c)
     a = helpers.short_inputs(c, full=True)
@@ -96,10 +99,10 @@ def test_rk4_short_step_bit_exact(lib, scheme):
         assert helpers.same(xg[n], xs[n]), f"{n}: max rel diff {helpers.max_rel(xg[n], xs[n]):.3e}"
 
 
-@pytest.mark.parametrize("order", [1, 2, 3])
+@pytest.mark.parametrize("order,halo", [(1, 2), (2, 2), (3, 2), (1, 3), (2, 3)])
 @pytest.mark.parametrize("stretched", [False, True])
-def test_numfilter_bit_exact(lib, stretched, order):
-    g = helpers.small_grid(IMAX=15, JMAX=10, KMAX=19, stretched=stretched)
+def test_numfilter_bit_exact(lib, stretched, order, halo):
+    g = helpers.small_grid(IMAX=15, JMAX=10, KMAX=19, stretched=stretched, halo=halo)
     c = helpers.small_case(g)
     helpers.perturb_state(c)
     ref_nd = g.zeros(5, 3)
@@ -136,10 +139,10 @@ def _tracer_inputs(g, c, seed=5):
     return q0, q, dens0, dens, mflx, rhoq, GS, np.asfortranarray(MAPF[..., 0])
 
 
-@pytest.mark.parametrize("scheme", ["UD3", "CD4", "UD3KOREN1993", "CD2"])
+@pytest.mark.parametrize("scheme", SCHEMES)
 @pytest.mark.parametrize("fct,along", [(False, True), (True, True), (True, False)])
 def test_tracer_step_bit_exact(lib, scheme, fct, along):
-    g = helpers.small_grid(IMAX=12, JMAX=14, KMAX=16)
+    g = helpers.small_grid(IMAX=12, JMAX=14, KMAX=16, halo=helpers.halo_of(scheme))
     c = helpers.small_case(g)
     helpers.perturb_state(c)
     q0, q, d0, d, mflx, rhoq, GS, MAPF = _tracer_inputs(g, c)
@@ -237,6 +240,23 @@ def test_large_step_higher_order_filter_parity(lib):
 def test_large_step_moist_fct_parity(lib):
     c = mkinit.config(2, scale=0.04)
     st_ref, st_gpu = _run_large_both(c, 2, lib)
+    for n in STATE:
+        err = _field_err(st_gpu[n], st_ref[n], c.g)
+        assert err <= 1e-10, f"{n}: {err:.3e}"
+    for iq in range(c.QA):
+        err = _field_err(st_gpu["QTRC"][..., iq], st_ref["QTRC"][..., iq], c.g)
+        assert err <= 1e-10, f"QTRC[{iq}]: {err:.3e}"
+
+
+@pytest.mark.parametrize("scheme", ["UD5", "CD6"])
+def test_large_step_six_point_schemes_parity(lib, scheme):
+    # dynamics and tracers (FCT) with a 6-point scheme, on a lateral halo of 3,
+    # through the host-array large step
+    g = helpers.small_grid(IMAX=14, JMAX=12, KMAX=20, stretched=True, halo=3)
+    c = mkinit.make_case("wide", g, scheme, scheme, dt=1.0, dtl=5.0,
+                         bubbles=[(3000.0, 2500.0, 1500.0, 2000.0, 2000.0, 1500.0, 3.0)], theta_noise=0.05,
+                         noise_kind="normal", wind_noise=2.0, tracers=2, fct=True, seed=4, u0=3.0, v0=-2.0)
+    st_ref, st_gpu = _run_large_both(c, 2, lib, divdmp=0.05)
     for n in STATE:
         err = _field_err(st_gpu[n], st_ref[n], c.g)
         assert err <= 1e-10, f"{n}: {err:.3e}"

@@ -39,8 +39,11 @@ def test_setup_rejects_inconsistent_index_set():
 
 def test_setup_rejects_unsupported_options():
     with pytest.raises(hevi.HeviError) as e:
-        hevi.setup(_index(), flux_type="UD5")
+        hevi.setup(_index(), flux_type="UD7")
     assert e.value.code == 5
+    with pytest.raises(hevi.HeviError) as e:
+        hevi.setup(_index(KA=24, IA=24, JA=20, IS=5, IE=20, JS=5, JE=16, IHALO=4, JHALO=4))
+    assert e.value.code == 5 and "halo" in str(e.value)
     with pytest.raises(hevi.HeviError) as e:
         hevi.setup(_index(IBLOCK=8))
     assert e.value.code == 5
@@ -81,11 +84,28 @@ def test_fortran_blank_padded_scheme_names_are_accepted():
 
 
 def test_unknown_flux_scheme_rejected_before_device_work():
-    """Scheme names outside UD3, CD4, UD3KOREN1993 and CD2 (for example the
-    halo-3 schemes UD5 and CD6) are refused before any device work."""
+    """Scheme names outside UD3, CD4, UD3KOREN1993, CD2, UD5 and CD6 are
+    refused before any device work."""
     from scale_b200 import hevi, mkinit
 
     g = mkinit.uniform_grid(8, 8, 8, 500.0, 500.0, 250.0)
-    for name in ("UD5", "CD6"):
+    for name in ("UD1", "UD7", "CD8"):
         with pytest.raises(hevi.HeviError, match="not supported"):
             hevi.setup(g.index_dict(), name, "UD3")
+
+
+def test_six_point_schemes_need_a_halo_of_three():
+    """UD5 and CD6 read three points on each side: with IHALO = JHALO = 2 the
+    setup fails before any device work (scale_atmos_dyn_fvm_flux.F90:742-749),
+    for the dynamics and for the tracer scheme alike."""
+    from scale_b200 import hevi, mkinit
+
+    g2 = mkinit.uniform_grid(8, 8, 8, 500.0, 500.0, 250.0)
+    for dyn, trc in (("UD5", "UD3"), ("CD6", "UD3"), ("UD3", "UD5")):
+        with pytest.raises(hevi.HeviError, match="IHALO = JHALO = 3"):
+            hevi.setup(g2.index_dict(), dyn, trc)
+    g3 = mkinit.uniform_grid(8, 8, 8, 500.0, 500.0, 250.0, halo=3)
+    assert (g3.IA, g3.IS, g3.IE) == (14, 4, 11)
+    ens = [g3.index_dict(), g2.index_dict()]
+    with pytest.raises(hevi.HeviError, match="one halo width"):
+        hevi.ensemble_setup(ens, "UD3", "UD3")

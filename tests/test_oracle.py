@@ -36,10 +36,13 @@ def _interior(a, g):
     return a[g.KS - 1 : g.KE, g.IS - 1 : g.IE, g.JS - 1 : g.JE]
 
 
-@pytest.mark.parametrize("scheme", ["UD3", "CD4", "UD3KOREN1993", "CD2"])
+SCHEMES = ["UD3", "CD4", "UD3KOREN1993", "CD2", "UD5", "CD6"]
+
+
+@pytest.mark.parametrize("scheme", SCHEMES)
 def test_const(scheme):
     """test_const (test_atmos_dyn.f90:382-454): a horizontally uniform state stays uniform."""
-    g = helpers.small_grid(8, 6, 12)
+    g = helpers.small_grid(8, 6, 12, halo=helpers.halo_of(scheme))
     c = mkinit.make_case("const", g, scheme, scheme, tracers=1, fct=True)
     st = c.state
     st["DENS"][...] = 1.0
@@ -61,11 +64,11 @@ def test_const(scheme):
     assert np.array_equal(q, np.broadcast_to(q[:, :1, :1], q.shape))
 
 
-@pytest.mark.parametrize("scheme", ["UD3", "CD4", "UD3KOREN1993", "CD2"])
+@pytest.mark.parametrize("scheme", SCHEMES)
 def test_conserve(scheme):
     """test_conserve (test_atmos_dyn.f90:456-592): domain totals of DENS and RHOT
     (weighted by the cell volume) are conserved to round-off."""
-    g = helpers.small_grid(10, 8, 14, stretched=True)
+    g = helpers.small_grid(10, 8, 14, stretched=True, halo=helpers.halo_of(scheme))
     c = mkinit.make_case("conserve", g, scheme, scheme)
     k, i, j = np.meshgrid(np.arange(1, g.KA + 1), np.arange(1, g.IA + 1), np.arange(1, g.JA + 1), indexing="ij")
     st = c.state
@@ -84,11 +87,12 @@ def test_conserve(scheme):
     assert abs(oracle.domain_sum(g, st["RHOT"]) - t0) / t0 < 1e-13
 
 
-def test_cwc():
+@pytest.mark.parametrize("scheme", ["UD3", "UD5", "CD6"])
+def test_cwc(scheme):
     """test_cwc (test_atmos_dyn.f90:594-670): uniform theta and tracer stay uniform
     under random momenta (consistency with the continuity equation)."""
-    g = helpers.small_grid(10, 10, 14)
-    c = mkinit.make_case("cwc", g, "UD3", "UD3", tracers=1, fct=True)
+    g = helpers.small_grid(10, 10, 14, halo=helpers.halo_of(scheme))
+    c = mkinit.make_case("cwc", g, scheme, scheme, tracers=1, fct=True)
     rng = np.random.Generator(np.random.PCG64(3))
     st = c.state
     st["DENS"][...] = c.ref["REF_dens"] * (1.0 + 1e-3 * rng.uniform(-1, 1, size=g.shape))
