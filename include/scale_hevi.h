@@ -23,9 +23,10 @@
  * Supported configuration (checked, otherwise SCALE_HEVI_ERR_UNSUPPORTED):
  * periodic lateral boundaries (BND_* = .false.), flat terrain (GSQRT = 1,
  * J13G = J23G = 0, MAPF = 1, checked once per metric array), the default
- * IBLOCK/JBLOCK (whole domain), flux schemes "UD3", "CD4", "CD2" and
- * "UD3KOREN1993", ND_ORDER >= 1 (above 1 on the FP64 path of one domain),
- * 4 <= KMAX <= 256, halo width 2. No additional prognostic variables (VA = 0).
+ * IBLOCK/JBLOCK (whole domain), flux schemes "UD3", "CD4", "CD2",
+ * "UD3KOREN1993", "UD5" and "CD6", ND_ORDER >= 1 (above 1 on the FP64 path of
+ * one domain), 4 <= KMAX <= 256 (5 for UD5/CD6), KHALO = 2 and IHALO = JHALO
+ * = 2 or 3 (3 for UD5/CD6). No additional prognostic variables (VA = 0).
  *
  * Concurrency: one library state per process (like the reference's module
  * variables); calls are not re-entrant and must come from one host thread.
@@ -66,9 +67,11 @@ typedef struct scale_hevi_index {
  * HEVI short step (ATMOS_DYN_Tstep_short_fvm_hevi_setup,
  * scale_atmos_dyn_tstep_short_fvm_hevi.F90:118). flux_type and
  * flux_tracer_type are the ATMOS_DYN_FVM_FLUX_TYPE / _TRACER_TYPE names
- * ("UD3", "CD4", "CD2" or "UD3KOREN1993": scale_atmos_dyn_fvm_flux_ud3.F90,
- * _cd4.F90, _cd2.F90, _ud3Koren1993.F90; UD3KOREN1993 is the reference's
- * default tracer flux). device is the CUDA ordinal to use. */
+ * ("UD3", "CD4", "CD2", "UD3KOREN1993", "UD5" or "CD6":
+ * scale_atmos_dyn_fvm_flux_ud3.F90, _cd4.F90, _cd2.F90, _ud3Koren1993.F90,
+ * _ud5.F90, _cd6.F90; UD3KOREN1993 is the reference's default tracer flux;
+ * UD5 and CD6 need IHALO = JHALO = 3, as scale_atmos_dyn_fvm_flux.F90:742-749
+ * requires). device is the CUDA ordinal to use. */
 int scale_hevi_setup(const scale_hevi_index *idx, const char *flux_type, const char *flux_tracer_type, int device);
 /* Frees every device buffer and the stream. */
 int scale_hevi_finalize(void);
