@@ -25,7 +25,7 @@
  * J13G = J23G = 0, MAPF = 1, checked once per metric array), the default
  * IBLOCK/JBLOCK (whole domain), flux schemes "UD3", "CD4", "CD2",
  * "UD3KOREN1993", "UD5" and "CD6", ND_ORDER >= 1 (above 1 on the FP64 path of
- * one domain), 4 <= KMAX <= 256 (5 for UD5/CD6), KHALO = 2 and IHALO = JHALO
+ * one domain with KMAX >= 6), 4 <= KMAX <= 256 (5 for UD5/CD6), KHALO = 2 and IHALO = JHALO
  * = 2 or 3 (3 for UD5/CD6). No additional prognostic variables (VA = 0).
  *
  * Concurrency: one library state per process (like the reference's module

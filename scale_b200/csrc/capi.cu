@@ -329,6 +329,14 @@ int prepare_tables(const double *CDZ, const double *FDZ, const double *RCDZ, con
 int prepare_nd(const double *CDZ, const double *CDX, const double *CDY, const double *FDZ, const double *FDX,
                const double *FDY, double DT, double ND_COEF, int ND_ORDER, double SFC)
 {
+    // calc_diff3 of the w-point quantity mirrors levels KS+2 and KS+3 into KS-1
+    // and KS-2 (scale_atmos_dyn_common.F90:1695-1696) before it writes them when
+    // KMAX < 6, so the result there would depend on what the work array held;
+    // calc_diff4 (ND_ORDER > 1) reads those levels
+    if (ND_ORDER > 1)
+        for (const MemberGeom &m : C.members)
+            if (m.KMAX < 6)
+                return fail(SCALE_HEVI_ERR_UNSUPPORTED, "ND_ORDER > 1 needs KMAX >= 6 (got %d)", m.KMAX);
     const size_t ZT = C.ZT, XT = C.XT, YT = C.YT;
     std::vector<double> key;
     key.insert(key.end(), CDZ, CDZ + ZT); key.insert(key.end(), FDZ, FDZ + ZT - 1);
