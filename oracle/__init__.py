@@ -121,9 +121,23 @@ def tstep_short(g, scheme, o, a):
                  float(a["dtrk"]))
 
 
-def tinteg_short_rk4(g, scheme, x, a):
-    """RK4 short step; x holds DENS..RHOT, mflx_hi, tflx_hi (updated in place)."""
-    return _call("og_tinteg_short_rk4", g, SCHEMES[scheme],
+def tstep_short_heve(g, scheme, o, a):
+    """One HEVE stage (fully explicit), same arguments as tstep_short."""
+    return _call("og_tstep_short_fvm_heve", g, SCHEMES[scheme],
+                 o["DENS_RK"], o["MOMZ_RK"], o["MOMX_RK"], o["MOMY_RK"], o["RHOT_RK"], o["mflx_hi"], o["tflx_hi"],
+                 a["DENS0"], a["MOMZ0"], a["MOMX0"], a["MOMY0"], a["RHOT0"],
+                 a["DENS"], a["MOMZ"], a["MOMX"], a["MOMY"], a["RHOT"],
+                 a["DENS_t"], a["MOMZ_t"], a["MOMX_t"], a["MOMY_t"], a["RHOT_t"],
+                 a["DPRES0"], a["RT2P"], a["CORIOLI"], a["num_diff"], a["wdamp_coef"], float(a["divdmp_coef"]), a["DDIV"],
+                 a["CDZ"], a["FDZ"], a["FDX"], a["FDY"], a["RCDZ"], a["RCDX"], a["RCDY"], a["RFDZ"], a["RFDX"], a["RFDY"],
+                 a["PHI"], a["GSQRT"], a["J13G"], a["J23G"], float(a["J33G"]), a["MAPF"], a["REF_dens"], a["REF_rhot"],
+                 float(a["dtrk"]))
+
+
+def tinteg_short_rk4(g, scheme, x, a, short="HEVI"):
+    """RK4 short step; x holds DENS..RHOT, mflx_hi, tflx_hi (updated in place).
+    short selects the registered short step, "HEVI" or "HEVE"."""
+    return _call({"HEVI": "og_tinteg_short_rk4", "HEVE": "og_tinteg_short_rk4_heve"}[short], g, SCHEMES[scheme],
                  x["DENS"], x["MOMZ"], x["MOMX"], x["MOMY"], x["RHOT"], x["mflx_hi"], x["tflx_hi"],
                  a["DENS_t"], a["MOMZ_t"], a["MOMX_t"], a["MOMY_t"], a["RHOT_t"],
                  a["DPRES0"], a["RT2P"], a["CORIOLI"], a["num_diff"], a["wdamp_coef"], float(a["divdmp_coef"]), a["DDIV"],

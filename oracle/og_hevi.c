@@ -38,11 +38,7 @@ static void solve_direct(int KS, int KE, int KMAX, double *C, const double *F1, 
         C[k - 1] = e[k - 1] * C[k] + f[k - 1];
 }
 
-typedef struct {
-    double *POTT, *DPRES, *qflx_hi, *qflx_J13, *qflx_J23, *Sr, *Sw, *St;
-} hevi_work;
-
-static int work_alloc(hevi_work *w, size_t N3)
+int og_stage_work_alloc(og_stage_work *w, size_t N3)
 {
     w->POTT = og_alloc_undef(N3);
     w->DPRES = og_alloc_undef(N3);
@@ -54,7 +50,7 @@ static int work_alloc(hevi_work *w, size_t N3)
     w->St = og_alloc_undef(N3);
     return (w->POTT && w->DPRES && w->qflx_hi && w->qflx_J13 && w->qflx_J23 && w->Sr && w->Sw && w->St) ? 0 : -1;
 }
-static void work_free(hevi_work *w)
+void og_stage_work_free(og_stage_work *w)
 {
     free(w->POTT); free(w->DPRES); free(w->qflx_hi); free(w->qflx_J13); free(w->qflx_J23);
     free(w->Sr); free(w->Sw); free(w->St);
@@ -62,7 +58,7 @@ static void work_free(hevi_work *w)
 
 /* The stage body; the solver's vertical momentum C(:,i,j) can be exported for the residual check. */
 static int hevi_stage(
-    const og_dims *d, int scheme, hevi_work *w, double *Cout,
+    const og_dims *d, int scheme, og_stage_work *w, double *Cout,
     double *DENS_RK, double *MOMZ_RK, double *MOMX_RK, double *MOMY_RK, double *RHOT_RK,
     double *mflx_hi, double *tflx_hi,
     const double *DENS0, const double *MOMZ0, const double *MOMX0, const double *MOMY0, const double *RHOT0,
@@ -358,14 +354,14 @@ int og_tstep_short_fvm_hevi(
     double dtrk)
 {
     OG_DIMS(d);
-    hevi_work w;
-    if (work_alloc(&w, N3)) { work_free(&w); return -1; }
+    og_stage_work w;
+    if (og_stage_work_alloc(&w, N3)) { og_stage_work_free(&w); return -1; }
     int rc = hevi_stage(d, scheme, &w, NULL, DENS_RK, MOMZ_RK, MOMX_RK, MOMY_RK, RHOT_RK, mflx_hi, tflx_hi,
                         DENS0, MOMZ0, MOMX0, MOMY0, RHOT0, DENS, MOMZ, MOMX, MOMY, RHOT,
                         DENS_t, MOMZ_t, MOMX_t, MOMY_t, RHOT_t, DPRES0, RT2P, CORIOLI,
                         num_diff, wdamp_coef, divdmp_coef, DDIV, CDZ, FDZ, FDX, FDY, RCDZ, RCDX, RCDY,
                         RFDZ, RFDX, RFDY, PHI, GSQRT, J13G, J23G, J33G, MAPF, REF_dens, REF_rhot, dtrk);
-    work_free(&w);
+    og_stage_work_free(&w);
     return rc;
 }
 
@@ -388,9 +384,34 @@ void og_halo_periodic(const og_dims *d, double *var, int nfields)
     }
 }
 
-/* RK4 short integrator, tinteg_short_rk4.F90:199-650, periodic (Copy_boundary is a no-op) */
-int og_tinteg_short_rk4(
-    const og_dims *d, int scheme,
+/* the HEVI stage body with the signature of og_heve_stage */
+static int hevi_stage_fn(
+    const og_dims *d, int scheme, og_stage_work *w,
+    double *DENS_RK, double *MOMZ_RK, double *MOMX_RK, double *MOMY_RK, double *RHOT_RK,
+    double *mflx_hi, double *tflx_hi,
+    const double *DENS0, const double *MOMZ0, const double *MOMX0, const double *MOMY0, const double *RHOT0,
+    const double *DENS, const double *MOMZ, const double *MOMX, const double *MOMY, const double *RHOT,
+    const double *DENS_t, const double *MOMZ_t, const double *MOMX_t, const double *MOMY_t, const double *RHOT_t,
+    const double *DPRES0, const double *RT2P, const double *CORIOLI,
+    const double *num_diff, const double *wdamp_coef, double divdmp_coef, const double *DDIV,
+    const double *CDZ, const double *FDZ, const double *FDX, const double *FDY,
+    const double *RCDZ, const double *RCDX, const double *RCDY,
+    const double *RFDZ, const double *RFDX, const double *RFDY,
+    const double *PHI, const double *GSQRT, const double *J13G, const double *J23G, double J33G,
+    const double *MAPF, const double *REF_dens, const double *REF_rhot,
+    double dtrk)
+{
+    return hevi_stage(d, scheme, w, NULL, DENS_RK, MOMZ_RK, MOMX_RK, MOMY_RK, RHOT_RK, mflx_hi, tflx_hi,
+                      DENS0, MOMZ0, MOMX0, MOMY0, RHOT0, DENS, MOMZ, MOMX, MOMY, RHOT,
+                      DENS_t, MOMZ_t, MOMX_t, MOMY_t, RHOT_t, DPRES0, RT2P, CORIOLI,
+                      num_diff, wdamp_coef, divdmp_coef, DDIV, CDZ, FDZ, FDX, FDY, RCDZ, RCDX, RCDY,
+                      RFDZ, RFDX, RFDY, PHI, GSQRT, J13G, J23G, J33G, MAPF, REF_dens, REF_rhot, dtrk);
+}
+
+/* RK4 short integrator, tinteg_short_rk4.F90:199-650, periodic (Copy_boundary is a no-op);
+ * stage is the registered short step (ATMOS_DYN_Tstep_short: HEVI or HEVE) */
+static int tinteg_short_rk4(
+    og_stage_fn stage, const og_dims *d, int scheme,
     double *DENS, double *MOMZ, double *MOMX, double *MOMY, double *RHOT,
     double *mflx_hi, double *tflx_hi,
     const double *DENS_t, const double *MOMZ_t, const double *MOMX_t, const double *MOMY_t, const double *RHOT_t,
@@ -409,11 +430,11 @@ int og_tinteg_short_rk4(
     for (int s = 0; s < 3; ++s) RK[s] = og_alloc_undef(5 * N3);
     double *S0 = og_alloc(5 * N3);
     double *mRK = og_alloc_undef(3 * 3 * N3), *tRK = og_alloc_undef(3 * 3 * N3);
-    hevi_work w;
-    int bad = work_alloc(&w, N3) || !RK[0] || !RK[1] || !RK[2] || !S0 || !mRK || !tRK;
+    og_stage_work w;
+    int bad = og_stage_work_alloc(&w, N3) || !RK[0] || !RK[1] || !RK[2] || !S0 || !mRK || !tRK;
     if (bad) {
         for (int s = 0; s < 3; ++s) free(RK[s]);
-        free(S0); free(mRK); free(tRK); work_free(&w);
+        free(S0); free(mRK); free(tRK); og_stage_work_free(&w);
         return -1;
     }
     double *X[5] = {DENS, MOMZ, MOMX, MOMY, RHOT};
@@ -436,7 +457,7 @@ int og_tinteg_short_rk4(
         }
         if (s == 0) for (int v = 0; v < 5; ++v) in[v] = X[v];
         else for (int v = 0; v < 5; ++v) in[v] = RK[s - 1] + v * N3;
-        hevi_stage(d, scheme, &w, NULL, out[0], out[1], out[2], out[3], out[4], mo, to,
+        stage(d, scheme, &w, out[0], out[1], out[2], out[3], out[4], mo, to,
                    X0[0], X0[1], X0[2], X0[3], X0[4], in[0], in[1], in[2], in[3], in[4],
                    DENS_t, MOMZ_t, MOMX_t, MOMY_t, RHOT_t, DPRES0, RT2P, CORIOLI,
                    num_diff, wdamp_coef, divdmp_coef, DDIV, CDZ, FDZ, FDX, FDY, RCDZ, RCDX, RCDY,
@@ -468,8 +489,49 @@ int og_tinteg_short_rk4(
                 }
     }
     for (int s = 0; s < 3; ++s) free(RK[s]);
-    free(S0); free(mRK); free(tRK); work_free(&w);
+    free(S0); free(mRK); free(tRK); og_stage_work_free(&w);
     return 0;
+}
+
+int og_tinteg_short_rk4(
+    const og_dims *d, int scheme,
+    double *DENS, double *MOMZ, double *MOMX, double *MOMY, double *RHOT,
+    double *mflx_hi, double *tflx_hi,
+    const double *DENS_t, const double *MOMZ_t, const double *MOMX_t, const double *MOMY_t, const double *RHOT_t,
+    const double *DPRES0, const double *RT2P, const double *CORIOLI,
+    const double *num_diff, const double *wdamp_coef, double divdmp_coef, const double *DDIV,
+    const double *CDZ, const double *FDZ, const double *FDX, const double *FDY,
+    const double *RCDZ, const double *RCDX, const double *RCDY,
+    const double *RFDZ, const double *RFDX, const double *RFDY,
+    const double *PHI, const double *GSQRT, const double *J13G, const double *J23G, double J33G,
+    const double *MAPF, const double *REF_dens, const double *REF_rhot,
+    double dt)
+{
+    return tinteg_short_rk4(hevi_stage_fn, d, scheme, DENS, MOMZ, MOMX, MOMY, RHOT, mflx_hi, tflx_hi, DENS_t, MOMZ_t, MOMX_t, MOMY_t,
+                            RHOT_t, DPRES0, RT2P, CORIOLI, num_diff, wdamp_coef, divdmp_coef, DDIV, CDZ, FDZ, FDX, FDY,
+                            RCDZ, RCDX, RCDY, RFDZ, RFDX, RFDY, PHI, GSQRT, J13G, J23G, J33G, MAPF, REF_dens,
+                            REF_rhot, dt);
+}
+
+/* the same RK4 with the HEVE short step registered (ATMOS_DYN_TSTEP_SHORT_TYPE = "HEVE") */
+int og_tinteg_short_rk4_heve(
+    const og_dims *d, int scheme,
+    double *DENS, double *MOMZ, double *MOMX, double *MOMY, double *RHOT,
+    double *mflx_hi, double *tflx_hi,
+    const double *DENS_t, const double *MOMZ_t, const double *MOMX_t, const double *MOMY_t, const double *RHOT_t,
+    const double *DPRES0, const double *RT2P, const double *CORIOLI,
+    const double *num_diff, const double *wdamp_coef, double divdmp_coef, const double *DDIV,
+    const double *CDZ, const double *FDZ, const double *FDX, const double *FDY,
+    const double *RCDZ, const double *RCDX, const double *RCDY,
+    const double *RFDZ, const double *RFDX, const double *RFDY,
+    const double *PHI, const double *GSQRT, const double *J13G, const double *J23G, double J33G,
+    const double *MAPF, const double *REF_dens, const double *REF_rhot,
+    double dt)
+{
+    return tinteg_short_rk4(og_heve_stage, d, scheme, DENS, MOMZ, MOMX, MOMY, RHOT, mflx_hi, tflx_hi, DENS_t, MOMZ_t, MOMX_t, MOMY_t,
+                            RHOT_t, DPRES0, RT2P, CORIOLI, num_diff, wdamp_coef, divdmp_coef, DDIV, CDZ, FDZ, FDX, FDY,
+                            RCDZ, RCDX, RCDY, RFDZ, RFDX, RFDY, PHI, GSQRT, J13G, J23G, J33G, MAPF, REF_dens,
+                            REF_rhot, dt);
 }
 
 /* check_equation port: returns the largest |error| the reference's DEBUG check
@@ -492,10 +554,10 @@ double og_hevi_max_residual(
     double *wd = (double *)calloc(KA, sizeof(double));
     double *out = og_alloc(5 * N3), *mflx = (double *)calloc(3 * N3, sizeof(double)), *tflx = (double *)calloc(3 * N3, sizeof(double));
     double *C = (double *)calloc(N3, sizeof(double));
-    hevi_work w;
+    og_stage_work w;
     memset(&w, 0, sizeof(w));
     double worst = 0.0;
-    if (!zero || !one || !jz || !mapf || !cor || !wd || !out || !mflx || !tflx || !C || work_alloc(&w, N3)) {
+    if (!zero || !one || !jz || !mapf || !cor || !wd || !out || !mflx || !tflx || !C || og_stage_work_alloc(&w, N3)) {
         worst = INFINITY;
         goto done;
     }
@@ -549,6 +611,6 @@ double og_hevi_max_residual(
         }
 done:
     free(zero); free(one); free(jz); free(mapf); free(cor); free(wd); free(out); free(mflx); free(tflx); free(C);
-    work_free(&w);
+    og_stage_work_free(&w);
     return worst;
 }

@@ -161,6 +161,43 @@ static inline double og_zface(int scheme, double vel, const double *col, int m, 
 #undef V_
 }
 
+/* ---- work arrays and the stage bodies (og_hevi.c, og_heve.c) ---- */
+typedef struct {
+    double *POTT, *DPRES, *qflx_hi, *qflx_J13, *qflx_J23, *Sr, *Sw, *St;
+} og_stage_work;
+int og_stage_work_alloc(og_stage_work *w, size_t N3);
+void og_stage_work_free(og_stage_work *w);
+typedef int (*og_stage_fn)(
+    const og_dims *d, int scheme, og_stage_work *w,
+    double *DENS_RK, double *MOMZ_RK, double *MOMX_RK, double *MOMY_RK, double *RHOT_RK,
+    double *mflx_hi, double *tflx_hi,
+    const double *DENS0, const double *MOMZ0, const double *MOMX0, const double *MOMY0, const double *RHOT0,
+    const double *DENS, const double *MOMZ, const double *MOMX, const double *MOMY, const double *RHOT,
+    const double *DENS_t, const double *MOMZ_t, const double *MOMX_t, const double *MOMY_t, const double *RHOT_t,
+    const double *DPRES0, const double *RT2P, const double *CORIOLI,
+    const double *num_diff, const double *wdamp_coef, double divdmp_coef, const double *DDIV,
+    const double *CDZ, const double *FDZ, const double *FDX, const double *FDY,
+    const double *RCDZ, const double *RCDX, const double *RCDY,
+    const double *RFDZ, const double *RFDX, const double *RFDY,
+    const double *PHI, const double *GSQRT, const double *J13G, const double *J23G, double J33G,
+    const double *MAPF, const double *REF_dens, const double *REF_rhot,
+    double dtrk);
+int og_heve_stage(
+    const og_dims *d, int scheme, og_stage_work *w,
+    double *DENS_RK, double *MOMZ_RK, double *MOMX_RK, double *MOMY_RK, double *RHOT_RK,
+    double *mflx_hi, double *tflx_hi,
+    const double *DENS0, const double *MOMZ0, const double *MOMX0, const double *MOMY0, const double *RHOT0,
+    const double *DENS, const double *MOMZ, const double *MOMX, const double *MOMY, const double *RHOT,
+    const double *DENS_t, const double *MOMZ_t, const double *MOMX_t, const double *MOMY_t, const double *RHOT_t,
+    const double *DPRES0, const double *RT2P, const double *CORIOLI,
+    const double *num_diff, const double *wdamp_coef, double divdmp_coef, const double *DDIV,
+    const double *CDZ, const double *FDZ, const double *FDX, const double *FDY,
+    const double *RCDZ, const double *RCDX, const double *RCDY,
+    const double *RFDZ, const double *RFDX, const double *RFDY,
+    const double *PHI, const double *GSQRT, const double *J13G, const double *J23G, double J33G,
+    const double *MAPF, const double *REF_dens, const double *REF_rhot,
+    double dtrk);
+
 /* ---- flux family (19 routines), one generic restatement per reference routine ---- */
 typedef struct {
     int IIS, IIE, JJS, JJE;

@@ -85,6 +85,39 @@ int og_tinteg_short_rk4(
     const double *MAPF, const double *REF_dens, const double *REF_rhot,
     double dt);
 
+/* ---- one HEVE stage (fully explicit; no momentum/theta FCT):
+ *      scale_atmos_dyn_tstep_short_fvm_heve.F90:109-1518 ---- */
+int og_tstep_short_fvm_heve(
+    const og_dims *d, int scheme,
+    double *DENS_RK, double *MOMZ_RK, double *MOMX_RK, double *MOMY_RK, double *RHOT_RK,
+    double *mflx_hi, double *tflx_hi,
+    const double *DENS0, const double *MOMZ0, const double *MOMX0, const double *MOMY0, const double *RHOT0,
+    const double *DENS, const double *MOMZ, const double *MOMX, const double *MOMY, const double *RHOT,
+    const double *DENS_t, const double *MOMZ_t, const double *MOMX_t, const double *MOMY_t, const double *RHOT_t,
+    const double *DPRES0, const double *RT2P, const double *CORIOLI,
+    const double *num_diff, const double *wdamp_coef, double divdmp_coef, const double *DDIV,
+    const double *CDZ, const double *FDZ, const double *FDX, const double *FDY,
+    const double *RCDZ, const double *RCDX, const double *RCDY,
+    const double *RFDZ, const double *RFDX, const double *RFDY,
+    const double *PHI, const double *GSQRT, const double *J13G, const double *J23G, double J33G,
+    const double *MAPF, const double *REF_dens, const double *REF_rhot,
+    double dtrk);
+
+/* ---- the RK4 short integrator with the HEVE stage ---- */
+int og_tinteg_short_rk4_heve(
+    const og_dims *d, int scheme,
+    double *DENS, double *MOMZ, double *MOMX, double *MOMY, double *RHOT,
+    double *mflx_hi, double *tflx_hi,
+    const double *DENS_t, const double *MOMZ_t, const double *MOMX_t, const double *MOMY_t, const double *RHOT_t,
+    const double *DPRES0, const double *RT2P, const double *CORIOLI,
+    const double *num_diff, const double *wdamp_coef, double divdmp_coef, const double *DDIV,
+    const double *CDZ, const double *FDZ, const double *FDX, const double *FDY,
+    const double *RCDZ, const double *RCDX, const double *RCDY,
+    const double *RFDZ, const double *RFDX, const double *RFDY,
+    const double *PHI, const double *GSQRT, const double *J13G, const double *J23G, double J33G,
+    const double *MAPF, const double *REF_dens, const double *REF_rhot,
+    double dt);
+
 /* ---- periodic 8-neighbour halo fill, scale_comm_cartesC.F90 (COMM_vars8 on a periodic 1x1 grid) ---- */
 void og_halo_periodic(const og_dims *d, double *var, int nfields);
 

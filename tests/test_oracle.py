@@ -304,3 +304,62 @@ def test_numfilter_higher_orders_damp_the_two_grid_wave_alike():
         nd = g.zeros(5, 3)
         oracle.numfilter(g, nd, st, c.ref, DT=1.0, ND_COEF=1e-2, ND_ORDER=order)
         assert np.max(np.abs(_interior(nd[..., 0, 1], g))) < 1e-14
+
+
+def _heve_steps(c, nsteps):
+    """nsteps RK4 short steps with the HEVE stage; c.state is advanced in place."""
+    g = c.g
+    a = helpers.short_inputs(c, full=False)
+    for k in ("DENS0", "MOMZ0", "MOMX0", "MOMY0", "RHOT0", "DENS", "MOMZ", "MOMX", "MOMY", "RHOT", "dtrk"):
+        a.pop(k)
+    x = {n: c.state[n] for n in STATE}
+    x["mflx_hi"], x["tflx_hi"] = g.zeros(3), g.zeros(3)
+    for _ in range(nsteps):
+        oracle.tinteg_short_rk4(g, c.scheme, x, dict(a, dt=c.dt), short="HEVE")
+        for n in STATE:  # the large step's halo fill after each short step
+            mkinit.periodic_fill(c.state[n], g)
+        mkinit.vertical_fill(c.state, g)
+    return x
+
+
+@pytest.mark.parametrize("scheme", ["UD3", "CD4", "UD5"])
+def test_heve_const(scheme):
+    """test_const (test_atmos_dyn.f90:382-454) with the HEVE short step: a
+    horizontally uniform state stays uniform."""
+    g = helpers.small_grid(8, 6, 12, halo=helpers.halo_of(scheme))
+    c = mkinit.make_case("const heve", g, scheme, scheme, dt=0.5)
+    st = c.state
+    st["DENS"][...] = c.ref["REF_dens"]
+    st["MOMX"][...] = 3.0
+    st["MOMY"][...] = 4.0
+    st["RHOT"][...] = c.ref["REF_dens"] * 300.0
+    st["MOMZ"][...] = 0.0
+    mkinit.vertical_fill(st, g)
+    _heve_steps(c, 3)
+    for n in STATE:
+        x = _interior(st[n], g)
+        assert np.array_equal(x, np.broadcast_to(x[:, :1, :1], x.shape)), n
+        assert np.isfinite(x).all(), n
+
+
+@pytest.mark.parametrize("scheme", ["UD3", "CD4", "UD5"])
+def test_heve_conserve(scheme):
+    """test_conserve (test_atmos_dyn.f90:456-592) with the HEVE short step:
+    the volume-weighted totals of DENS and RHOT are conserved to round-off."""
+    g = helpers.small_grid(10, 8, 14, stretched=True, halo=helpers.halo_of(scheme))
+    c = mkinit.make_case("conserve heve", g, scheme, scheme, dt=0.5)
+    k, i, j = np.meshgrid(np.arange(1, g.KA + 1), np.arange(1, g.IA + 1), np.arange(1, g.JA + 1), indexing="ij")
+    st = c.state
+    st["MOMZ"][...] = (k + i + j) * 0.01
+    st["MOMX"][...] = (k * 2 + i + j) * 0.01
+    st["MOMY"][...] = (k + i * 2 + j) * 0.01
+    st["DENS"][...] = c.ref["REF_dens"] + (k * 2 + i * 2 + j) * 1e-4
+    st["RHOT"][...] = st["DENS"] * (300.0 + (k + i + j * 2) * 0.01)
+    for n in STATE:
+        mkinit.periodic_fill(st[n], g)
+    mkinit.vertical_fill(st, g)
+    m0 = oracle.domain_sum(g, st["DENS"])
+    t0 = oracle.domain_sum(g, st["RHOT"])
+    _heve_steps(c, 3)
+    assert abs(oracle.domain_sum(g, st["DENS"]) - m0) / m0 < 1e-13
+    assert abs(oracle.domain_sum(g, st["RHOT"]) - t0) / t0 < 1e-13
