@@ -125,6 +125,23 @@ int ATMOS_DYN_Tstep_short_fvm_hevi_b200(SCALE_HEVI_TSTEP_SHORT_ARGS);
 int ATMOS_DYN_Tstep_short_fvm_hevi_b200_dev(SCALE_HEVI_TSTEP_SHORT_ARGS);
 
 /* ---------------------------------------------------------------------------
+ * One HEVE stage, the fully explicit short step. Replaces
+ * ATMOS_DYN_Tstep_short_fvm_heve (scale_atmos_dyn_tstep_short_fvm_heve.F90:109-1518),
+ * the other target of ATMOS_DYN_Tstep_short. Same arguments as the HEVI
+ * stage. FLAG_FCT_MOMENTUM and FLAG_FCT_T must be .false. (the momentum and
+ * theta FCT branches, :386-447, :716-1309, :1388-1515, are not provided);
+ * FP64 only.
+ * ------------------------------------------------------------------------- */
+int ATMOS_DYN_Tstep_short_fvm_heve_b200(SCALE_HEVI_TSTEP_SHORT_ARGS);
+int ATMOS_DYN_Tstep_short_fvm_heve_b200_dev(SCALE_HEVI_TSTEP_SHORT_ARGS);
+
+/* Registers the short step that the RK4 entries and the large step run, as
+ * ATMOS_DYN_Tstep_short_regist does for ATMOS_DYN_TSTEP_SHORT_TYPE
+ * (scale_atmos_dyn_tstep_short.F90:153-215): "HEVI" (the default after setup)
+ * or "HEVE". The mixed-precision and differentiated entries take HEVI only. */
+int scale_hevi_short_type(const char *type);
+
+/* ---------------------------------------------------------------------------
  * One short time step with the four-stage Runge-Kutta integrator. Replaces
  * ATMOS_DYN_tinteg_short_rk4 (scale_atmos_dyn_tinteg_short_rk4.F90:199-650),
  * target of ATMOS_DYN_Tinteg_short (scale_atmos_dyn_tinteg_short.F90:32-108).

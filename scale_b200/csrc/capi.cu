@@ -30,6 +30,7 @@ struct Ctx {
     scale_hevi_index idx{};
     Grid g{};
     int scheme = UD3, scheme_tracer = UD3;
+    int short_type = 0;  // the registered short step of the RK4 and large-step entries: 0 HEVI, 1 HEVE
     size_t N3 = 0;   // points of one 3-D field (all members)
     // ensemble members sharing the pooled arrays (one entry for a single domain)
     std::vector<MemberGeom> members;
@@ -482,11 +483,26 @@ int autotune_stage(const StageInT<F> &in, double dtrk)
 }
 
 template <typename F>
-int run_stage(const StageInT<F> &in, double *const out[5], F *mflx, F *tflx, double dtrk, int mode)
+// kind: 0 HEVI, 1 HEVE, -1 the registered short step (scale_hevi_short_type)
+int run_stage(const StageInT<F> &in, double *const out[5], F *mflx, F *tflx, double dtrk, int mode, int kind = -1)
 {
     if (in.divdmp != 0.0 && !in.DDIV) return fail(SCALE_HEVI_ERR_ARG, "divdmp_coef is nonzero but DDIV is NULL");
     if (in.divdmp != 0.0 && C.members.size() > 1)
         return fail(SCALE_HEVI_ERR_UNSUPPORTED, "divergence damping is not available for an ensemble");
+    if (kind < 0) kind = C.short_type;
+    if (kind == 1) {
+        if constexpr (sizeof(F) != sizeof(double)) {
+            return fail(SCALE_HEVI_ERR_UNSUPPORTED, "the mixed-precision path takes the HEVI short step only");
+        } else {
+            const StageArgsT<double> a = stage_args(in, out, mflx, tflx, dtrk, mode);
+            CK(timed("heve_stage", [&] {
+                CU(launch_heve_stage(C.g, mem(), a, C.scheme, C.stream));
+                return SCALE_HEVI_OK;
+            }));
+            ++C.launches;
+            return SCALE_HEVI_OK;
+        }
+    }
     const int p = sizeof(F) == sizeof(double) ? 0 : 1;
     if (C.autotune && !C.tuned[p] && !C.capturing) CK(autotune_stage(in, dtrk));
     const StageArgsT<F> a = stage_args(in, out, mflx, tflx, dtrk, mode);
@@ -733,6 +749,17 @@ int scale_hevi_ensemble_layout(long long *cell0, long long *col0, long long *z0,
     return SCALE_HEVI_OK;
 }
 
+int scale_hevi_short_type(const char *type)
+{
+    CK(need_setup());
+    if (!type) return fail(SCALE_HEVI_ERR_ARG, "short-step type is NULL");
+    std::string n(type);
+    while (!n.empty() && n.back() == ' ') n.pop_back(); // Fortran blank padding
+    if (n == "HEVI" || n == "FVM-HEVI") { C.short_type = 0; return SCALE_HEVI_OK; }
+    if (n == "HEVE" || n == "FVM-HEVE") { C.short_type = 1; return SCALE_HEVI_OK; }
+    return fail(SCALE_HEVI_ERR_UNSUPPORTED, "short-step type '%s' is not supported (HEVI, HEVE)", n.c_str());
+}
+
 int scale_hevi_stage_shape(int tile_x, int raster)
 {
     CK(need_setup());
@@ -793,6 +820,14 @@ int scale_hevi_check(void)
 }
 
 // ---- HEVI stage --------------------------------------------------------------
+#define SCALE_HEVI_TSTEP_SHORT_NAMES                                                                            \
+    DENS_RK, MOMZ_RK, MOMX_RK, MOMY_RK, RHOT_RK, PROG_RK, mflx_hi, tflx_hi, DENS0, MOMZ0, MOMX0, MOMY0, RHOT0, \
+        DENS, MOMZ, MOMX, MOMY, RHOT, DENS_t, MOMZ_t, MOMX_t, MOMY_t, RHOT_t, PROG0, PROG, DPRES0, RT2P,        \
+        CORIOLI, num_diff, wdamp_coef, divdmp_coef, DDIV, FLAG_FCT_MOMENTUM, FLAG_FCT_T, FLAG_FCT_ALONG_STREAM, \
+        CDZ, FDZ, FDX, FDY, RCDZ, RCDX, RCDY, RFDZ, RFDX, RFDY, PHI, GSQRT, J13G, J23G, J33G, MAPF, REF_dens,   \
+        REF_rhot, BND_W, BND_E, BND_S, BND_N, dtrk, last
+static int stage_host(SCALE_HEVI_TSTEP_SHORT_ARGS, int kind);
+
 int ATMOS_DYN_Tstep_short_fvm_hevi_b200_dev(SCALE_HEVI_TSTEP_SHORT_ARGS)
 {
     (void)PROG_RK; (void)PROG0; (void)PROG; (void)FLAG_FCT_MOMENTUM; (void)FLAG_FCT_T; (void)FLAG_FCT_ALONG_STREAM;
@@ -805,10 +840,45 @@ int ATMOS_DYN_Tstep_short_fvm_hevi_b200_dev(SCALE_HEVI_TSTEP_SHORT_ARGS)
                DENS_t, MOMZ_t, MOMX_t, MOMY_t, RHOT_t, DPRES0, RT2P, CORIOLI, num_diff, DDIV, REF_dens, REF_rhot,
                *divdmp_coef, *J33G};
     double *out[5] = {DENS_RK, MOMZ_RK, MOMX_RK, MOMY_RK, RHOT_RK};
-    return run_stage(in, out, mflx_hi, tflx_hi, *dtrk, RK_PLAIN);
+    return run_stage(in, out, mflx_hi, tflx_hi, *dtrk, RK_PLAIN, 0);
 }
 
 int ATMOS_DYN_Tstep_short_fvm_hevi_b200(SCALE_HEVI_TSTEP_SHORT_ARGS)
+{
+    return stage_host(SCALE_HEVI_TSTEP_SHORT_NAMES, 0);
+}
+
+// ---- HEVE stage (ATMOS_DYN_Tstep_short_fvm_heve, scale_atmos_dyn_tstep_short_fvm_heve.F90:109-1518) ----
+static int check_heve_fct(const int *FLAG_FCT_MOMENTUM, const int *FLAG_FCT_T)
+{
+    if ((FLAG_FCT_MOMENTUM && *FLAG_FCT_MOMENTUM) || (FLAG_FCT_T && *FLAG_FCT_T))
+        return fail(SCALE_HEVI_ERR_UNSUPPORTED, "the HEVE momentum/theta FCT is not supported");
+    return SCALE_HEVI_OK;
+}
+
+int ATMOS_DYN_Tstep_short_fvm_heve_b200_dev(SCALE_HEVI_TSTEP_SHORT_ARGS)
+{
+    (void)PROG_RK; (void)PROG0; (void)PROG; (void)FLAG_FCT_ALONG_STREAM; (void)last; (void)PHI;
+    CK(need_setup());
+    CK(check_heve_fct(FLAG_FCT_MOMENTUM, FLAG_FCT_T));
+    CK(check_bnd(BND_W, BND_E, BND_S, BND_N));
+    CK(check_flat(GSQRT, J13G, J23G, MAPF, true));
+    CK(prepare_tables(CDZ, FDZ, RCDZ, RFDZ, FDX, RCDX, RFDX, FDY, RCDY, RFDY, wdamp_coef, nullptr, nullptr));
+    StageIn in{DENS0, MOMZ0, MOMX0, MOMY0, RHOT0, DENS, MOMZ, MOMX, MOMY, RHOT,
+               DENS_t, MOMZ_t, MOMX_t, MOMY_t, RHOT_t, DPRES0, RT2P, CORIOLI, num_diff, DDIV, REF_dens, REF_rhot,
+               *divdmp_coef, *J33G};
+    double *out[5] = {DENS_RK, MOMZ_RK, MOMX_RK, MOMY_RK, RHOT_RK};
+    return run_stage(in, out, mflx_hi, tflx_hi, *dtrk, RK_PLAIN, 1);
+}
+
+int ATMOS_DYN_Tstep_short_fvm_heve_b200(SCALE_HEVI_TSTEP_SHORT_ARGS)
+{
+    CK(check_heve_fct(FLAG_FCT_MOMENTUM, FLAG_FCT_T));
+    return stage_host(SCALE_HEVI_TSTEP_SHORT_NAMES, 1);
+}
+
+// host-array form of one stage (kind 0 HEVI, 1 HEVE): copies in, runs, copies back
+static int stage_host(SCALE_HEVI_TSTEP_SHORT_ARGS, int kind)
 {
     CK(need_single("the host-array stage entry"));
     CK(check_bnd(BND_W, BND_E, BND_S, BND_N));
@@ -840,7 +910,7 @@ int ATMOS_DYN_Tstep_short_fvm_hevi_b200(SCALE_HEVI_TSTEP_SHORT_ARGS)
     CK(prepare_tables(CDZ, FDZ, RCDZ, RFDZ, FDX, RCDX, RFDX, FDY, RCDY, RFDY, wdamp_coef, nullptr, nullptr));
     StageIn in{i0[0], i0[1], i0[2], i0[3], i0[4], iv[0], iv[1], iv[2], iv[3], iv[4],
                it[0], it[1], it[2], it[3], it[4], dp0, rt, cor, nd, ddiv, rd, rr, *divdmp_coef, *J33G};
-    CK(run_stage(in, o, mf, tf, *dtrk, RK_PLAIN));
+    CK(run_stage(in, o, mf, tf, *dtrk, RK_PLAIN, kind));
     for (int v = 0; v < 5; ++v) CK(d2h(hout[v], o[v], N3));
     CK(d2h(mflx_hi, mf, 3 * N3));
     CK(d2h(tflx_hi, tf, 3 * N3));
@@ -852,8 +922,9 @@ int ATMOS_DYN_Tstep_short_fvm_hevi_b200(SCALE_HEVI_TSTEP_SHORT_ARGS)
 // ---- RK4 short step ------------------------------------------------------------
 int ATMOS_DYN_Tinteg_short_rk4_b200_dev(SCALE_HEVI_TINTEG_SHORT_ARGS)
 {
-    (void)PROG; (void)FLAG_FCT_MOMENTUM; (void)FLAG_FCT_T; (void)FLAG_FCT_ALONG_STREAM; (void)PHI;
+    (void)PROG; (void)FLAG_FCT_ALONG_STREAM; (void)PHI;
     CK(need_setup());
+    if (C.short_type == 1) CK(check_heve_fct(FLAG_FCT_MOMENTUM, FLAG_FCT_T));
     CK(check_bnd(BND_W, BND_E, BND_S, BND_N));
     CK(check_flat(GSQRT, J13G, J23G, MAPF, true));
     CK(prepare_tables(CDZ, FDZ, RCDZ, RFDZ, FDX, RCDX, RFDX, FDY, RCDY, RFDY, wdamp_coef, nullptr, nullptr));
@@ -867,6 +938,7 @@ int ATMOS_DYN_Tinteg_short_rk4_b200_dev(SCALE_HEVI_TINTEG_SHORT_ARGS)
 int ATMOS_DYN_Tinteg_short_rk4_b200(SCALE_HEVI_TINTEG_SHORT_ARGS)
 {
     CK(need_single("the host-array RK4 entry"));
+    if (C.short_type == 1) CK(check_heve_fct(FLAG_FCT_MOMENTUM, FLAG_FCT_T));
     CK(check_bnd(BND_W, BND_E, BND_S, BND_N));
     CK(check_flat(GSQRT, J13G, J23G, MAPF, false));
     const size_t N3 = n3(), N2 = (size_t)C.g.IA * C.g.JA;
@@ -902,8 +974,9 @@ int ATMOS_DYN_Tinteg_short_rk4_b200(SCALE_HEVI_TINTEG_SHORT_ARGS)
 // ---- mixed precision: FP32 flux arithmetic, FP64 state and solve -----------------
 int ATMOS_DYN_Tinteg_short_rk4_b200_mixed_dev(SCALE_HEVI_TINTEG_SHORT_MIXED_ARGS)
 {
-    (void)PROG; (void)FLAG_FCT_MOMENTUM; (void)FLAG_FCT_T; (void)FLAG_FCT_ALONG_STREAM; (void)PHI;
+    (void)PROG; (void)FLAG_FCT_ALONG_STREAM; (void)PHI;
     CK(need_setup());
+    if (C.short_type == 1) CK(check_heve_fct(FLAG_FCT_MOMENTUM, FLAG_FCT_T));
     CK(check_bnd(BND_W, BND_E, BND_S, BND_N));
     CK(check_flat(GSQRT, J13G, J23G, MAPF, true));
     CK(prepare_tables(CDZ, FDZ, RCDZ, RFDZ, FDX, RCDX, RFDX, FDY, RCDY, RFDY, wdamp_coef, nullptr, nullptr));
@@ -1311,6 +1384,7 @@ int scale_hevi_adjoint_setup(const double *DPRES0, const double *RT2P, const dou
     CK(need_single("the differentiated short step"));
     if (wide_scheme(C.scheme))
         return fail(SCALE_HEVI_ERR_UNSUPPORTED, "the differentiated short step supports UD3, CD4, UD3KOREN1993 and CD2");
+    if (C.short_type != 0) return fail(SCALE_HEVI_ERR_UNSUPPORTED, "the differentiated short step is the HEVI step");
     const double *v[12] = {CDZ, CDX, CDY, FDZ, FDX, FDY, RCDZ, RCDX, RCDY, RFDZ, RFDX, RFDY};
     const int len[12] = {C.g.KA, C.g.IA, C.g.JA, C.g.KA - 1, C.g.IA - 1, C.g.JA - 1,
                          C.g.KA, C.g.IA, C.g.JA, C.g.KA - 1, C.g.IA - 1, C.g.JA - 1};

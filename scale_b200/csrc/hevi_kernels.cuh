@@ -111,6 +111,9 @@ constexpr int STAGE_RASTER_DEFAULT = 16;
 template <typename R>
 cudaError_t launch_hevi_stage(const Grid &g, const Members &mem, const StageArgsT<R> &a, int scheme, StageShape shape,
                               cudaStream_t st);
+// one HEVE stage (FP64), same arguments; the RK4 combine modes apply as for HEVI
+cudaError_t launch_heve_stage(const Grid &g, const Members &mem, const StageArgsT<double> &a, int scheme,
+                              cudaStream_t st);
 
 // ---- utilities (misc.cu) ----
 template <typename T>

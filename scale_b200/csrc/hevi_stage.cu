@@ -178,7 +178,10 @@ __device__ __forceinline__ R adv_w_h(const Grid &g, const StageArgsT<R> &a, cons
 // one above the level of the previous lane, passed by a warp shuffle. The
 // advective and Coriolis terms are flux arithmetic (R); the pressure gradient
 // of the deviation from the base state and the update of the state are FP64.
-template <int S, int V, typename R>
+// HEVE = true takes the divergence-damping term as the HEVE module writes it,
+// divdmp_coef / dtrk * FDX(i) * (DDIV(i+1) - DDIV(i)) (tstep_short_fvm_heve.F90:907,
+// :1154), instead of the HEVI form (DDIV(i+1) - DDIV(i)) * ... * FDX(i).
+template <int S, int V, typename R, bool HEVE = false>
 __device__ __forceinline__ void update_mom(const Grid &g, const StageArgsT<R> &a, const Nd<R> &nd, size_t N3, int k, int i,
                                            int j, bool valid)
 {
@@ -252,7 +255,9 @@ __device__ __forceinline__ void update_mom(const Grid &g, const StageArgsT<R> &a
         const double DPe = AT(a.DPRES0, 0, 1, 0) + AT(a.RT2P, 0, 1, 0) * (AT(RT, 0, 1, 0) - AT(a.REF_rhot, 0, 1, 0));
         const double pg = (DPe - DP00) * rfdx;
         const R cf = cor_u * (AR(MY, 0, 1, 0) + AR(MY, 0, 0, 0) + AR(MY, 0, 1, -1) + AR(MY, 0, 0, -1));
-        const R div = use_div ? ddc * (AT(a.DDIV, 0, 1, 0) - AT(a.DDIV, 0, 0, 0)) * fdx : R(0.0);
+        const R div = !use_div ? R(0.0)
+                      : HEVE ? ddc * fdx * (AT(a.DDIV, 0, 1, 0) - AT(a.DDIV, 0, 0, 0))
+                             : ddc * (AT(a.DDIV, 0, 1, 0) - AT(a.DDIV, 0, 0, 0)) * fdx;
         const double val = lds(a.MOMX0 + c) + dt * (((((double)(advcv + advch)) - pg) + (double)cf) + (double)div + (double)lds(a.MOMX_t + c));
         put_state(a, N3, 2, a.MOMX_RK, a.MOMX0, c, val, true);
     }
@@ -283,7 +288,9 @@ __device__ __forceinline__ void update_mom(const Grid &g, const StageArgsT<R> &a
         const double DPn = AT(a.DPRES0, 0, 0, 1) + AT(a.RT2P, 0, 0, 1) * (AT(RT, 0, 0, 1) - AT(a.REF_rhot, 0, 0, 1));
         const double pg = (DPn - DP00) * rfdy;
         const R cf = cor_v * (AR(MX, 0, 0, 1) + AR(MX, 0, 0, 0) + AR(MX, 0, -1, 1) + AR(MX, 0, -1, 0));
-        const R div = use_div ? ddc * (AT(a.DDIV, 0, 0, 1) - AT(a.DDIV, 0, 0, 0)) * fdy : R(0.0);
+        const R div = !use_div ? R(0.0)
+                      : HEVE ? ddc * fdy * (AT(a.DDIV, 0, 0, 1) - AT(a.DDIV, 0, 0, 0))
+                             : ddc * (AT(a.DDIV, 0, 0, 1) - AT(a.DDIV, 0, 0, 0)) * fdy;
         const double val = lds(a.MOMY0 + c) + dt * (((((double)(advcv + advch)) - pg) + (double)cf) + (double)div + (double)lds(a.MOMY_t + c));
         put_state(a, N3, 3, a.MOMY_RK, a.MOMY0, c, val, true);
     }
@@ -566,6 +573,170 @@ __global__ void __launch_bounds__(32 * HEVI_COL_TC, HEVI_COL_MINB)
 #undef XS
 #undef XS_PUT
 }
+// =============================================================================
+// the HEVE stage (ATMOS_DYN_Tstep_short_fvm_heve, scale_atmos_dyn_tstep_short_fvm_heve.F90:109-1518,
+// without the momentum/theta FCT branches): every tendency is explicit, so each
+// warp updates one column, lanes along k, with no column solve. The rho*u and
+// rho*v updates are the HEVI ones (the two modules write them alike up to the
+// divergence-damping term); the vertical mass flux is the explicit
+// J33G * MOMZ + num_diff (:460-479), and the theta flux, the pressure gradient
+// and the buoyancy of rho*w follow :622-688 and :1328-1371. Line numbers refer
+// to the HEVE file. FP64, flat terrain as in the HEVI kernel.
+// =============================================================================
+constexpr int HEVE_WARPS = 4; // columns (warps) per CTA
+
+template <int S, int NM>
+__global__ void __launch_bounds__(32 * HEVE_WARPS)
+    k_heve_stage(const Grid gt, const StageArgsT<double> a, const BatchT<NM> B)
+{
+    using R = double;
+    __shared__ double spott[HEVE_WARPS][MAXKA]; // POTT of each warp's column
+    int b;
+    const Grid g = block_domain(gt, B, b);
+    const Block2 p = split_block(b, (g.IMAX + HEVE_WARPS - 1) / HEVE_WARPS);
+    const int lane = threadIdx.x, w = threadIdx.y;
+    const int i = g.IS + p.x * HEVE_WARPS + w, j = g.JS + p.y;
+    if (i > g.IE) return; // warp-uniform; the kernel has no block-wide barrier
+    const size_t N3 = n3(g);
+    const int sI = g.KA, sJ = g.KA * g.IA;
+    const int KS = g.KS, KE = g.KE;
+    const int col = (int)idx3(g, 1, i, j);
+    const Nd<R> nd(a, N3);
+    const double dt = a.dtrk, J33G = a.J33G;
+    const bool use_div = a.divdmp_coef != 0.0;
+    const R ddc = use_div ? R(a.divdmp_coef / dt) : R(0.0);
+    const R rcdx = ld(g.RCDX + i - 1), rcdy = ld(g.RCDY + j - 1);
+    constexpr bool W6 = wide_scheme(S);
+    const unsigned FULL = 0xffffffffu;
+    double *P = spott[w];
+
+    // potential temperature of the column, :375-382
+    for (int L = KS + lane; L <= KE; L += 32) P[L - 1] = ld(a.RHOT + col + L - 1) / ld(a.DENS + col + L - 1);
+    __syncwarp();
+    auto pott = [&](int l) { return P[l - 1]; };
+    // the explicit vertical mass flux at w-level m (zero at KS-1 and KE), :460-479 (flat terrain)
+    auto mflx_z = [&](int m) -> R {
+        if (m < KS || m > KE - 1) return R(0.0);
+        return J33G * ld(a.MOMZ + col + m - 1) + ld(nd.DZ() + col + m - 1);
+    };
+    // theta flux at w-level m, fluxZ_XYZ (ud3.F90:157-247)
+    auto tflx_z = [&](int m) -> R {
+        if (m < KS || m > KE - 1) return R(0.0);
+        const R vel = mflx_z(m);
+        return vel * zface<S>(vel, m, KS, KE, pott) + ld(nd.TZ() + col + m - 1);
+    };
+    // w-momentum flux at level m (between w-levels m-1 and m... as fluxZ_XYW writes flux(m)), zero outside KS..KE-2
+    auto qz_w = [&](int m) -> R {
+        if (m < KS || m > KE - 2) return R(0.0);
+        const R Mk = ld(a.MOMZ + col + m - 1), Mk1 = ld(a.MOMZ + col + m);
+        const R vel = (R(0.5) * (Mk + Mk1)) / R(ld(a.DENS + col + m));
+        const R q = zface<S>(vel, m, KS, KE, [&](int l) { return R(ld(a.MOMZ + col + l - 1)); });
+        return R(J33G) * vel * q + ld(nd.WZ() + col + m);
+    };
+    auto dpres = [&](int c) { return ld(a.DPRES0 + c) + ld(a.RT2P + c) * (ld(a.RHOT + c) - ld(a.REF_rhot + c)); };
+    // POTT of a horizontal neighbour column
+    auto pott_at = [&](int c) { return ld(a.RHOT + c) / ld(a.DENS + c); };
+
+    for (int L0 = KS; L0 <= KE; L0 += 32) {
+        const int L = L0 + lane;
+        const bool valid = L <= KE;
+        const int c = col + L - 1;
+        // z fluxes through the face above each level; the face below is the previous lane's
+        const R mz = valid ? mflx_z(L) : R(0.0), tz = valid ? tflx_z(L) : R(0.0), qz = valid ? qz_w(L) : R(0.0);
+        R mzm = __shfl_up_sync(FULL, mz, 1), tzm = __shfl_up_sync(FULL, tz, 1), qzm = __shfl_up_sync(FULL, qz, 1);
+        if (lane == 0) { mzm = mflx_z(L - 1); tzm = tflx_z(L - 1); qzm = qz_w(L - 1); }
+        if (valid) {
+            const R rcdz = ld(g.RCDZ + L - 1);
+            // ---- density, :460-532 ----
+            const MassFlux<R> m = mass_flux(a, nd, c, sI, sJ);
+            {
+                const R advcv = -(mz - mzm) * rcdz;
+                const R advch = -(m.Xe - m.Xw) * rcdx - (m.Yn - m.Ys) * rcdy;
+                put_state(a, N3, 0, a.DENS_RK, a.DENS0, c, ld(a.DENS0 + c) + dt * ((advcv + advch) + ld(a.DENS_t + c)), true);
+            }
+            put_flux(a, N3, 0, c, mz, true);
+            put_flux(a, N3, 1, c, m.Xe, true);
+            put_flux(a, N3, 2, c, m.Yn, true);
+            if (i == g.IS) put_flux(a, N3, 1, c - sI, m.Xw, false);
+            if (j == g.JS) put_flux(a, N3, 2, c - sJ, m.Ys, false);
+            // ---- rho*theta, :1328-1371 ----
+            {
+                const R P00 = P[L - 1];
+                auto px = [&](int d) { return d == 0 ? P00 : pott_at(c + d * sI); };
+                auto py = [&](int d) { return d == 0 ? P00 : pott_at(c + d * sJ); };
+                const R Pm3 = W6 ? px(-3) : R(0.0), Pp3 = W6 ? px(3) : R(0.0);
+                const R Qm3 = W6 ? py(-3) : R(0.0), Qp3 = W6 ? py(3) : R(0.0);
+                const R Pm2 = px(-2), Pm1 = px(-1), Pp1 = px(1), Pp2 = px(2);
+                const R Qm2 = py(-2), Qm1 = py(-1), Qp1 = py(1), Qp2 = py(2);
+                const R tXe = m.Xe * ip6<S>(m.Xe, Pm2, Pm1, P00, Pp1, Pp2, Pp3) + ld(nd.TX() + c);
+                const R tXw = m.Xw * ip6<S>(m.Xw, Pm3, Pm2, Pm1, P00, Pp1, Pp2) + ld(nd.TX() + c - sI);
+                const R tYn = m.Yn * ip6<S>(m.Yn, Qm2, Qm1, P00, Qp1, Qp2, Qp3) + ld(nd.TY() + c);
+                const R tYs = m.Ys * ip6<S>(m.Ys, Qm3, Qm2, Qm1, P00, Qp1, Qp2) + ld(nd.TY() + c - sJ);
+                const R advcv = -(tz - tzm) * rcdz;
+                const R advch = -(tXe - tXw) * rcdx - (tYn - tYs) * rcdy;
+                put_state(a, N3, 4, a.RHOT_RK, a.RHOT0, c, ld(a.RHOT0 + c) + dt * ((advcv + advch) + ld(a.RHOT_t + c)), true);
+                put_flux(a, N3, 3, c, tz, true);
+                put_flux(a, N3, 4, c, tXe, true);
+                put_flux(a, N3, 5, c, tYn, true);
+                if (i == g.IS) put_flux(a, N3, 4, c - sI, tXw, false);
+                if (j == g.JS) put_flux(a, N3, 5, c - sJ, tYs, false);
+            }
+            // ---- rho*w, :586-688 ----
+            if (L <= KE - 1) {
+                const R advcv = -(qz - qzm) * R(ld(g.RFDZ + L - 1));
+                const R advch = adv_w_h<S>(g, a, nd, c, L, sI, sJ, rcdx, rcdy);
+                const R pgf = J33G * (dpres(c + 1) - dpres(c)) * ld(g.RFDZ + L - 1);
+                const R buoy = GRAV * (ld(g.F2H1 + L - 1) * (ld(a.DENS + c + 1) - ld(a.REF_dens + c + 1))
+                                       + ld(g.F2H2 + L - 1) * (ld(a.DENS + c) - ld(a.REF_dens + c)));
+                const R wdamp = -ld(a.wdamp + g.z0 + L - 1) * ld(a.MOMZ0 + c);
+                const R div = use_div ? ddc * R(ld(g.FDZ + L - 1)) * (ld(a.DDIV + c + 1) - ld(a.DDIV + c)) : R(0.0);
+                const double val = ld(a.MOMZ0 + c) + dt * ((((advcv + advch) - pgf) - buoy) + wdamp + div + ld(a.MOMZ_t + c));
+                put_state(a, N3, 1, a.MOMZ_RK, a.MOMZ0, c, val, true);
+            } else {
+                put_state(a, N3, 1, a.MOMZ_RK, a.MOMZ0, c, 0.0, false);
+            }
+        }
+        // ---- rho*u and rho*v, :819-1170 (all 32 lanes take part: the updates shuffle) ----
+        update_mom<S, 0, R, true>(g, a, nd, N3, L, i, j, valid);
+        update_mom<S, 1, R, true>(g, a, nd, N3, L, i, j, valid);
+    }
+    if (lane == 0) {
+        // MOMZ_RK(KS-1) and the zero fluxes through the surface
+        put_state(a, N3, 1, a.MOMZ_RK, a.MOMZ0, col + KS - 2, 0.0, false);
+        put_flux(a, N3, 0, col + KS - 2, R(0.0), false);
+        put_flux(a, N3, 3, col + KS - 2, R(0.0), false);
+    }
+}
+
+template <int S, int NM>
+static cudaError_t launch_heve_one(const Grid &g, const StageArgsT<double> &a, const BatchT<NM> &B, int nblocks,
+                                   cudaStream_t st)
+{
+    k_heve_stage<S, NM><<<nblocks, dim3(32, HEVE_WARPS), 0, st>>>(g, a, B);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_heve_stage(const Grid &g, const Members &mem, const StageArgsT<double> &a, int scheme,
+                              cudaStream_t st)
+{
+    int maxKA = g.KA;
+    for (int q = 0; q < mem.n; ++q) maxKA = mem.m[q].KMAX + 4 > maxKA ? mem.m[q].KMAX + 4 : maxKA;
+    if (maxKA > MAXKA) return cudaErrorInvalidValue;
+    auto nblocks = [](const Grid &m) { return ((m.IMAX + HEVE_WARPS - 1) / HEVE_WARPS) * m.JMAX; };
+    return with_batch(g, mem, nblocks, [&](const auto &B, int nb) -> cudaError_t {
+        constexpr int NM = std::decay_t<decltype(B)>::NMAX;
+        switch (scheme) {
+        case UD3: return launch_heve_one<UD3, NM>(g, a, B, nb, st);
+        case CD4: return launch_heve_one<CD4, NM>(g, a, B, nb, st);
+        case KOREN: return launch_heve_one<KOREN, NM>(g, a, B, nb, st);
+        case CD2: return launch_heve_one<CD2, NM>(g, a, B, nb, st);
+        case UD5: return launch_heve_one<UD5, NM>(g, a, B, nb, st);
+        case CD6: return launch_heve_one<CD6, NM>(g, a, B, nb, st);
+        default: return cudaErrorInvalidValue;
+        }
+    });
+}
+
 #undef AT
 #undef AR
 

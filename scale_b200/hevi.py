@@ -94,6 +94,8 @@ def load(path: str | os.PathLike | None = None) -> C.CDLL:
             f.argtypes = [C.c_int, C.POINTER(Index), C.c_char_p, C.c_char_p, C.c_int]
         elif name == "scale_hevi_stage_shape":
             f.argtypes = [C.c_int, C.c_int]
+        elif name == "scale_hevi_short_type":
+            f.argtypes = [C.c_char_p]
         elif name == "scale_hevi_stage_autotune":
             f.argtypes = [C.c_int]
         elif name == "scale_hevi_stage_shape_get":
@@ -218,6 +220,12 @@ def unpool(pooled: np.ndarray, offsets: np.ndarray, shapes: list[tuple], ncomp: 
     return out
 
 
+def short_type(name: str = "HEVI") -> None:
+    """The short step the RK4 entries and the large step run: "HEVI" or "HEVE"
+    (ATMOS_DYN_Tstep_short_regist)."""
+    _check(load().scale_hevi_short_type(name.encode()))
+
+
 def stage_shape(tile_x: int = 0, raster: int = 0) -> None:
     """Tile width and raster height of the stage kernel (0: defaults)."""
     _check(load().scale_hevi_stage_shape(int(tile_x), int(raster)))
@@ -300,6 +308,10 @@ def ATMOS_DYN_Tstep_short_fvm_hevi(**kw):
     call("ATMOS_DYN_Tstep_short_fvm_hevi_b200", **kw)
 
 
+def ATMOS_DYN_Tstep_short_fvm_heve(**kw):
+    call("ATMOS_DYN_Tstep_short_fvm_heve_b200", **kw)
+
+
 def ATMOS_DYN_Tinteg_short_rk4(**kw):
     call("ATMOS_DYN_Tinteg_short_rk4_b200", **kw)
 
@@ -327,6 +339,10 @@ def ATMOS_DYN_divergence(**kw):
 # ---- device-array entries -----------------------------------------------------------
 def ATMOS_DYN_Tstep_short_fvm_hevi_dev(**kw):
     call("ATMOS_DYN_Tstep_short_fvm_hevi_b200_dev", **kw)
+
+
+def ATMOS_DYN_Tstep_short_fvm_heve_dev(**kw):
+    call("ATMOS_DYN_Tstep_short_fvm_heve_b200_dev", **kw)
 
 
 def ATMOS_DYN_Tinteg_short_rk4_dev(**kw):
