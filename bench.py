@@ -35,6 +35,7 @@ sys.path.insert(0, str(ROOT))
 METRIC = "HEVI short-step cell-updates/s on 1 B200, FP64 vs mixed at stated error; %HBM"
 UNIT = "cell-updates/s"
 L2_BYTES = 126 * 1024 * 1024
+HEVE_DT = 0.04  # s; below the vertical acoustic limit dz / c_s of the 50 m lowest layer
 # algorithmic bytes per interior cell: one HEVI stage reads 34
 # fields (DENS0..RHOT0, DENS..RHOT, *_t, DPRES0, RT2P, REF_dens, REF_rhot and the
 # 15 num_diff components; DDIV is not read because divdmp_coef = 0) and writes 11
@@ -180,7 +181,7 @@ def run_b200(args):
     for v, n in enumerate(("DENS", "MOMZ", "MOMX", "MOMY", "RHOT")):
         st[v].copy_(to_dev(c.state[n], torch))
     X = dict(DENS=st[0], MOMZ=st[1], MOMX=st[2], MOMY=st[3], RHOT=st[4])
-    st0 = st.clone() if not args.no_mixed else None
+    st0 = st.clone() if not (args.no_mixed and args.no_heve) else None
     z = lambda k=1: torch.zeros(k * N3, dtype=torch.float64, device="cuda")  # noqa: E731
     mflx, tflx, nd = z(3), z(3), z(15)
     tend = {n: z() for n in ("DENS_t", "MOMZ_t", "MOMX_t", "MOMY_t", "RHOT_t")}
@@ -195,7 +196,7 @@ def run_b200(args):
                 RFDX=g.RFDX, RFDY=g.RFDY)
     dts = c.dt
 
-    def step():
+    def step(dts=dts):
         # numerical filter (tstep_large:847-858) on the state at the start of the short step
         hevi.ATMOS_DYN_numfilter_coef_dev(num_diff=nd, CDZ=g.CDZ, CDX=g.CDX, CDY=g.CDY, FDZ=g.FDZ, FDX=g.FDX,
                                           FDY=g.FDY, DT=dts, REF_dens=ref["REF_dens"], REF_pott=ref["REF_pott"],
@@ -279,7 +280,6 @@ def run_b200(args):
         # the same workload from the same initial state on the mixed-precision path
         st_fp64 = st.clone()
         st.copy_(st0)
-        del st0
         f32 = lambda k=1: torch.zeros(k * N3, dtype=torch.float32, device="cuda")  # noqa: E731
         mflx32, tflx32, nd32 = f32(3), f32(3), f32(15)
         tend32 = {n: f32() for n in ("DENS_t", "MOMZ_t", "MOMX_t", "MOMY_t", "RHOT_t")}
@@ -343,6 +343,10 @@ def run_b200(args):
         }
         del st_fp64
 
+    if not args.no_heve:
+        out["heve"] = run_heve(args, hevi, torch, step, st, st0, X, g, cells, stream, t0, t1, dist, world, hbm)
+    del st0
+
     if rank == 0 and not args.no_e2e:
         out["e2e"] = run_e2e(args, c, hevi, torch)
     if rank == 0 and not args.no_cpu_baseline:
@@ -363,6 +367,49 @@ def run_b200(args):
         dist.destroy_process_group()
     if rank == 0:
         print(json.dumps(out), flush=True)
+
+
+def run_heve(args, hevi, torch, step, st, st0, X, g, cells, stream, t0, t1, dist, world, hbm):
+    """The same short steps with HEVE registered as the short step
+    (ATMOS_DYN_Tstep_short_fvm_heve, explicit in the vertical too), from the
+    same initial state. HEVE's step is bounded by the vertical acoustic limit
+    dz / c_s of the 50 m lowest layer, so it runs at dt = 0.04 s; the work
+    per step does not depend on dt."""
+    st.copy_(st0)
+    hevi.short_type("HEVE")
+    try:
+        for _ in range(args.warmup):
+            step(HEVE_DT)
+        hevi.check()
+        m0 = hevi.domain_sum_dev(X["DENS"], g.CDZ, g.CDX, g.CDY)
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        hevi.profile(True)
+        t0.record(stream)
+        for _ in range(args.steps):
+            step(HEVE_DT)
+        t1.record(stream)
+        torch.cuda.synchronize()
+        prof = hevi.profile_report()
+        hevi.profile(False)
+        hevi.check()
+        m1 = hevi.domain_sum_dev(X["DENS"], g.CDZ, g.CDX, g.CDY)
+    finally:
+        hevi.short_type("HEVI")
+    ms = max_over_ranks(t0.elapsed_time(t1), dist, "cuda") / args.steps
+    n, tot = prof.get("heve_stage", (0, 0.0))
+    stage_ms = tot / max(n, 1)
+    ach = STAGE_BYTES * cells / (stage_ms * 1e-3) / 1e9 if stage_ms > 0 else None
+    return {
+        "value": aggregate_rate(cells, world, 1, ms), "unit": UNIT, "ms_per_step": ms, "dt": HEVE_DT,
+        "step": "numfilter + RK4 of 4 HEVE stages + boundary/halo, FP64, same workload",
+        "mass_drift_rel": abs(m1 - m0) / m0,
+        "roofline": {"bound": "hbm", "kernel": "k_heve_stage (one HEVE stage)", "achieved": ach, "peak": hbm,
+                     "unit": "GB/s", "frac": (ach / hbm) if ach else None,
+                     "algorithmic_bytes_per_launch": STAGE_BYTES * cells, "stage_ms": stage_ms},
+        "sections_ms_per_step": {k: v[1] / args.steps for k, v in prof.items()},
+    }
 
 
 def run_mixed_large(args, hevi, torch):
@@ -723,6 +770,7 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision measurement")
+    ap.add_argument("--no-heve", action="store_true", help="skip the HEVE short-step measurement")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the 48-member ensemble measurement")
     ap.add_argument("--ensemble-steps", type=int, default=20)
     ap.add_argument("--ensemble-scale", type=float, default=1.0, help="horizontal scale of the ensemble members")

@@ -53,7 +53,7 @@ def _signatures() -> dict[str, str]:
 
 
 _RESTYPE = {"og_halo_periodic": None, "og_divergence": None, "og_hevi_max_residual": C.c_double,
-            "og_domain_sum": C.c_double}
+            "og_domain_sum": C.c_double, "og_short_type": None}
 
 
 def load() -> C.CDLL:
@@ -174,10 +174,21 @@ def tinteg_tracer_rk3(g, scheme, QTRC, QTRC0, RHOQ_t, DENS0, DENS, mflx_hi, num_
 
 
 def tstep_large(g, scheme, scheme_tracer, st, out, tp, ref, aq, GSQRT, J13G, J23G, MAPF, CORIOLI, wdamp, dtl, dts,
-                ND_COEF=1e-4, divdmp=0.0, fct=False, along=True, QA=0, ND_ORDER=1):
-    """Large step of the dynamics; st (DENS..RHOT, QTRC) is advanced in place."""
+                ND_COEF=1e-4, divdmp=0.0, fct=False, along=True, QA=0, ND_ORDER=1, short="HEVI"):
+    """Large step of the dynamics; st (DENS..RHOT, QTRC) is advanced in place.
+    short is the registered short step, "HEVI" or "HEVE"."""
     QTRC = st.get("QTRC") if QA else None
     R, CV, CP, M = aq if QA else (None, None, None, None)
+    load().og_short_type({"HEVI": 0, "HEVE": 1}[short])
+    try:
+        return _tstep_large(g, scheme, scheme_tracer, st, out, tp, ref, GSQRT, J13G, J23G, MAPF, CORIOLI, wdamp,
+                            dtl, dts, ND_COEF, divdmp, fct, along, QA, ND_ORDER, QTRC, R, CV, CP, M)
+    finally:
+        load().og_short_type(0)
+
+
+def _tstep_large(g, scheme, scheme_tracer, st, out, tp, ref, GSQRT, J13G, J23G, MAPF, CORIOLI, wdamp, dtl, dts,
+                 ND_COEF, divdmp, fct, along, QA, ND_ORDER, QTRC, R, CV, CP, M):
     return _call("og_tstep_large", g, SCHEMES[scheme], SCHEMES[scheme_tracer],
                  st["DENS"], st["MOMZ"], st["MOMX"], st["MOMY"], st["RHOT"], QTRC, int(QA),
                  out["mflx_hi"], out["tflx_hi"], out["num_diff"],

@@ -128,6 +128,10 @@ out:
 /* Large step, tstep_large_fvm_heve.F90:171-1130. Restated subset: periodic lateral
  * boundaries, DAMP_alpha = 0 (no nudging), ND_COEF_Q = 0, USE_AVERAGE off,
  * FLAG_TRACER_SPLIT_TEND off, EULER large-step integrator (Llast = .true., QTRC0 = QTRC). */
+/* the registered short step of the large step (ATMOS_DYN_Tstep_short_regist): 0 HEVI, 1 HEVE */
+static int og_short = 0;
+void og_short_type(int type) { og_short = type; }
+
 int og_tstep_large(
     const og_dims *d, int scheme, int scheme_tracer,
     double *DENS, double *MOMZ, double *MOMX, double *MOMY, double *RHOT, double *QTRC, int QA,
@@ -210,7 +214,8 @@ int og_tstep_large(
         else
             memset(DDIV, 0, N3 * sizeof(double));
         /* short step :880-894 */
-        if ((rc = og_tinteg_short_rk4(d, scheme, DENS, MOMZ, MOMX, MOMY, RHOT, mflx_hi, tflx_hi,
+        if ((rc = (og_short ? og_tinteg_short_rk4_heve : og_tinteg_short_rk4)(
+                 d, scheme, DENS, MOMZ, MOMX, MOMY, RHOT, mflx_hi, tflx_hi,
                                       tend, tend + N3, tend + 2 * N3, tend + 3 * N3, tend + 4 * N3,
                                       DPRES0, RT2P, CORIOLI, num_diff, wdamp_coef, divdmp_coef, DDIV,
                                       CDZ, FDZ, FDX, FDY, RCDZ, RCDX, RCDY, RFDZ, RFDX, RFDY,

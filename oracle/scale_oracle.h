@@ -118,6 +118,9 @@ int og_tinteg_short_rk4_heve(
     const double *MAPF, const double *REF_dens, const double *REF_rhot,
     double dt);
 
+/* ---- the short step og_tstep_large runs (ATMOS_DYN_Tstep_short_regist): 0 HEVI (default), 1 HEVE ---- */
+void og_short_type(int type);
+
 /* ---- periodic 8-neighbour halo fill, scale_comm_cartesC.F90 (COMM_vars8 on a periodic 1x1 grid) ---- */
 void og_halo_periodic(const og_dims *d, double *var, int nfields);
 

@@ -584,9 +584,12 @@ __global__ void __launch_bounds__(32 * HEVI_COL_TC, HEVI_COL_MINB)
 // to the HEVE file. FP64, flat terrain as in the HEVI kernel.
 // =============================================================================
 constexpr int HEVE_WARPS = 4; // columns (warps) per CTA
+#ifndef HEVE_MINB
+#define HEVE_MINB 8 // resident CTAs per SM the register allocator must allow (32 warps)
+#endif
 
 template <int S, int NM>
-__global__ void __launch_bounds__(32 * HEVE_WARPS)
+__global__ void __launch_bounds__(32 * HEVE_WARPS, HEVE_MINB)
     k_heve_stage(const Grid gt, const StageArgsT<double> a, const BatchT<NM> B)
 {
     using R = double;
