@@ -171,6 +171,26 @@ int ATMOS_DYN_Tinteg_short_rk4_b200(SCALE_HEVI_TINTEG_SHORT_ARGS);
 int ATMOS_DYN_Tinteg_short_rk4_b200_dev(SCALE_HEVI_TINTEG_SHORT_ARGS);
 
 /* ---------------------------------------------------------------------------
+ * One short time step with a three-stage Runge-Kutta integrator. Replaces
+ * ATMOS_DYN_tinteg_short_rk3 (scale_atmos_dyn_tinteg_short_rk3.F90:188-576),
+ * the other target of ATMOS_DYN_Tinteg_short. Same arguments as the RK4 step.
+ * The variant is the registered one (scale_hevi_tinteg_short_type), as the
+ * reference fixes it in ATMOS_DYN_Tinteg_short_rk3_setup (:89-184): "RK3",
+ * Heun's method, stages at dt/3, 2dt/3, dt and the state
+ * (r1*3 + r3*3 - phi_n*2)/4, fluxes (F1 + F3*3)/4; or "RK3WS2002" (Wicker and
+ * Skamarock 2002), stages at dt/3, dt/2, dt and the third stage kept. With RK4
+ * registered both entries return SCALE_HEVI_ERR_UNSUPPORTED.
+ * ------------------------------------------------------------------------- */
+int ATMOS_DYN_Tinteg_short_rk3_b200(SCALE_HEVI_TINTEG_SHORT_ARGS);
+int ATMOS_DYN_Tinteg_short_rk3_b200_dev(SCALE_HEVI_TINTEG_SHORT_ARGS);
+
+/* Registers the short integrator of the large step and the RK3 entries, as
+ * ATMOS_DYN_Tinteg_short_setup does for ATMOS_DYN_TINTEG_SHORT_TYPE
+ * (scale_atmos_dyn_tinteg_short.F90:146-159): "RK4" (the default after
+ * setup), "RK3" or "RK3WS2002". The differentiated entries take RK4 only. */
+int scale_hevi_tinteg_short_type(const char *type);
+
+/* ---------------------------------------------------------------------------
  * Mixed-precision RK4 short step (device arrays). No counterpart in the
  * reference, which is either all FP64 or, built with -DSINGLE, all FP32. Flux
  * and divergence arithmetic runs in FP32. The state (DENS..RHOT), DPRES0, RT2P,

@@ -53,7 +53,7 @@ def _signatures() -> dict[str, str]:
 
 
 _RESTYPE = {"og_halo_periodic": None, "og_divergence": None, "og_hevi_max_residual": C.c_double,
-            "og_domain_sum": C.c_double, "og_short_type": None}
+            "og_domain_sum": C.c_double, "og_short_type": None, "og_tinteg_short_type": None}
 
 
 def load() -> C.CDLL:
@@ -146,6 +146,22 @@ def tinteg_short_rk4(g, scheme, x, a, short="HEVI"):
                  float(a["dt"]))
 
 
+def tinteg_short_rk3(g, scheme, x, a, ws2002=True, short="HEVI"):
+    """RK3 short step (RK3WS2002 or, with ws2002=False, Heun's RK3) with the
+    short step `short`; x as for tinteg_short_rk4."""
+    load().og_short_type({"HEVI": 0, "HEVE": 1}[short])
+    try:
+        return _call("og_tinteg_short_rk3", g, SCHEMES[scheme], int(bool(ws2002)),
+                     x["DENS"], x["MOMZ"], x["MOMX"], x["MOMY"], x["RHOT"], x["mflx_hi"], x["tflx_hi"],
+                     a["DENS_t"], a["MOMZ_t"], a["MOMX_t"], a["MOMY_t"], a["RHOT_t"],
+                     a["DPRES0"], a["RT2P"], a["CORIOLI"], a["num_diff"], a["wdamp_coef"], float(a["divdmp_coef"]),
+                     a["DDIV"], a["CDZ"], a["FDZ"], a["FDX"], a["FDY"], a["RCDZ"], a["RCDX"], a["RCDY"], a["RFDZ"],
+                     a["RFDX"], a["RFDY"], a["PHI"], a["GSQRT"], a["J13G"], a["J23G"], float(a["J33G"]), a["MAPF"],
+                     a["REF_dens"], a["REF_rhot"], float(a["dt"]))
+    finally:
+        load().og_short_type(0)
+
+
 def halo(g, var, nfields=1):
     _call("og_halo_periodic", g, var, int(nfields))
 
@@ -174,17 +190,20 @@ def tinteg_tracer_rk3(g, scheme, QTRC, QTRC0, RHOQ_t, DENS0, DENS, mflx_hi, num_
 
 
 def tstep_large(g, scheme, scheme_tracer, st, out, tp, ref, aq, GSQRT, J13G, J23G, MAPF, CORIOLI, wdamp, dtl, dts,
-                ND_COEF=1e-4, divdmp=0.0, fct=False, along=True, QA=0, ND_ORDER=1, short="HEVI"):
+                ND_COEF=1e-4, divdmp=0.0, fct=False, along=True, QA=0, ND_ORDER=1, short="HEVI", tinteg="RK4"):
     """Large step of the dynamics; st (DENS..RHOT, QTRC) is advanced in place.
-    short is the registered short step, "HEVI" or "HEVE"."""
+    short is the registered short step ("HEVI" or "HEVE"), tinteg the short
+    integrator ("RK4", "RK3" or "RK3WS2002")."""
     QTRC = st.get("QTRC") if QA else None
     R, CV, CP, M = aq if QA else (None, None, None, None)
     load().og_short_type({"HEVI": 0, "HEVE": 1}[short])
+    load().og_tinteg_short_type({"RK4": 0, "RK3": 1, "RK3WS2002": 2}[tinteg])
     try:
         return _tstep_large(g, scheme, scheme_tracer, st, out, tp, ref, GSQRT, J13G, J23G, MAPF, CORIOLI, wdamp,
                             dtl, dts, ND_COEF, divdmp, fct, along, QA, ND_ORDER, QTRC, R, CV, CP, M)
     finally:
         load().og_short_type(0)
+        load().og_tinteg_short_type(0)
 
 
 def _tstep_large(g, scheme, scheme_tracer, st, out, tp, ref, GSQRT, J13G, J23G, MAPF, CORIOLI, wdamp, dtl, dts,

@@ -513,6 +513,110 @@ int og_tinteg_short_rk4(
                             REF_rhot, dt);
 }
 
+/* RK3 short integrator, tinteg_short_rk3.F90:188-576 (setup :89-184): the
+ * registered short step at dt*(1/3), dt*fact_dt2 and dt, each of the first two
+ * followed by the periodic halo of its output; fact_dt2 = 1/2 for RK3WS2002
+ * (the result is the third stage), 2/3 for RK3 (Heun: the state becomes
+ * (r1*3 + r3*3 - phi0*2)/4 and the fluxes (F1 + F3*3)/4 on the interior, :486-566) */
+static int tinteg_short_rk3(
+    og_stage_fn stage, int ws2002, const og_dims *d, int scheme,
+    double *DENS, double *MOMZ, double *MOMX, double *MOMY, double *RHOT,
+    double *mflx_hi, double *tflx_hi,
+    const double *DENS_t, const double *MOMZ_t, const double *MOMX_t, const double *MOMY_t, const double *RHOT_t,
+    const double *DPRES0, const double *RT2P, const double *CORIOLI,
+    const double *num_diff, const double *wdamp_coef, double divdmp_coef, const double *DDIV,
+    const double *CDZ, const double *FDZ, const double *FDX, const double *FDY,
+    const double *RCDZ, const double *RCDX, const double *RCDY,
+    const double *RFDZ, const double *RFDX, const double *RFDY,
+    const double *PHI, const double *GSQRT, const double *J13G, const double *J23G, double J33G,
+    const double *MAPF, const double *REF_dens, const double *REF_rhot,
+    double dt)
+{
+    OG_DIMS(d);
+    const double fact_dt1 = 1.0 / 3.0, fact_dt2 = ws2002 ? 1.0 / 2.0 : 2.0 / 3.0;
+    double *RK[2] = {og_alloc_undef(5 * N3), og_alloc_undef(5 * N3)};
+    double *S0 = og_alloc(5 * N3);
+    double *mRK = og_alloc_undef(2 * 3 * N3), *tRK = og_alloc_undef(2 * 3 * N3);
+    og_stage_work w;
+    int bad = og_stage_work_alloc(&w, N3) || !RK[0] || !RK[1] || !S0 || !mRK || !tRK;
+    if (bad) {
+        free(RK[0]); free(RK[1]); free(S0); free(mRK); free(tRK); og_stage_work_free(&w);
+        return -1;
+    }
+    double *X[5] = {DENS, MOMZ, MOMX, MOMY, RHOT};
+    for (int v = 0; v < 5; ++v) memcpy(S0 + v * N3, X[v], N3 * sizeof(double));
+    const double *X0[5] = {S0, S0 + N3, S0 + 2 * N3, S0 + 3 * N3, S0 + 4 * N3};
+    const double dts[3] = {dt * fact_dt1, dt * fact_dt2, dt};
+    for (int s = 0; s < 3; ++s) {
+        double *out[5], *mo, *to;
+        const double *in[5];
+        if (s < 2) {
+            for (int v = 0; v < 5; ++v) out[v] = RK[s] + v * N3;
+            mo = mRK + (size_t)s * 3 * N3;
+            to = tRK + (size_t)s * 3 * N3;
+        } else {
+            for (int v = 0; v < 5; ++v) out[v] = X[v];
+            mo = mflx_hi;
+            to = tflx_hi;
+        }
+        if (s == 0) for (int v = 0; v < 5; ++v) in[v] = X[v];
+        else for (int v = 0; v < 5; ++v) in[v] = RK[s - 1] + v * N3;
+        stage(d, scheme, &w, out[0], out[1], out[2], out[3], out[4], mo, to,
+              X0[0], X0[1], X0[2], X0[3], X0[4], in[0], in[1], in[2], in[3], in[4],
+              DENS_t, MOMZ_t, MOMX_t, MOMY_t, RHOT_t, DPRES0, RT2P, CORIOLI,
+              num_diff, wdamp_coef, divdmp_coef, DDIV, CDZ, FDZ, FDX, FDY, RCDZ, RCDX, RCDY,
+              RFDZ, RFDX, RFDY, PHI, GSQRT, J13G, J23G, J33G, MAPF, REF_dens, REF_rhot, dts[s]);
+        if (s < 2) og_halo_periodic(d, RK[s], 5);
+    }
+    if (!ws2002) {
+        for (int v = 0; v < 5; ++v) {
+            double *x = X[v];
+            const double *r1 = RK[0] + v * N3, *x0 = X0[v];
+            const int kend = (v == 1) ? KE - 1 : KE; /* MOMZ: KS..KE-1 */
+#pragma omp parallel for collapse(2)
+            for (int j = JS; j <= JE; ++j)
+                for (int i = IS; i <= IE; ++i)
+                    for (int k = KS; k <= kend; ++k) {
+                        size_t q = I3(k, i, j);
+                        x[q] = (r1[q] * 3.0 + x[q] * 3.0 - x0[q] * 2.0) / 4.0;
+                    }
+        }
+        for (int n = 0; n < 3; ++n) {
+#pragma omp parallel for collapse(2)
+            for (int j = JS; j <= JE; ++j)
+                for (int i = IS; i <= IE; ++i)
+                    for (int k = KS; k <= KE; ++k) {
+                        size_t q = I3(k, i, j) + (size_t)n * N3;
+                        mflx_hi[q] = (mRK[q] + mflx_hi[q] * 3.0) / 4.0;
+                        tflx_hi[q] = (tRK[q] + tflx_hi[q] * 3.0) / 4.0;
+                    }
+        }
+    }
+    free(RK[0]); free(RK[1]); free(S0); free(mRK); free(tRK);
+    og_stage_work_free(&w);
+    return 0;
+}
+
+int og_tinteg_short_rk3(
+    const og_dims *d, int scheme, int ws2002,
+    double *DENS, double *MOMZ, double *MOMX, double *MOMY, double *RHOT,
+    double *mflx_hi, double *tflx_hi,
+    const double *DENS_t, const double *MOMZ_t, const double *MOMX_t, const double *MOMY_t, const double *RHOT_t,
+    const double *DPRES0, const double *RT2P, const double *CORIOLI,
+    const double *num_diff, const double *wdamp_coef, double divdmp_coef, const double *DDIV,
+    const double *CDZ, const double *FDZ, const double *FDX, const double *FDY,
+    const double *RCDZ, const double *RCDX, const double *RCDY,
+    const double *RFDZ, const double *RFDX, const double *RFDY,
+    const double *PHI, const double *GSQRT, const double *J13G, const double *J23G, double J33G,
+    const double *MAPF, const double *REF_dens, const double *REF_rhot,
+    double dt)
+{
+    return tinteg_short_rk3(og_short_type_get() ? og_heve_stage : hevi_stage_fn, ws2002, d, scheme, DENS, MOMZ,
+                            MOMX, MOMY, RHOT, mflx_hi, tflx_hi, DENS_t, MOMZ_t, MOMX_t, MOMY_t, RHOT_t, DPRES0, RT2P,
+                            CORIOLI, num_diff, wdamp_coef, divdmp_coef, DDIV, CDZ, FDZ, FDX, FDY, RCDZ, RCDX, RCDY,
+                            RFDZ, RFDX, RFDY, PHI, GSQRT, J13G, J23G, J33G, MAPF, REF_dens, REF_rhot, dt);
+}
+
 /* the same RK4 with the HEVE short step registered (ATMOS_DYN_TSTEP_SHORT_TYPE = "HEVE") */
 int og_tinteg_short_rk4_heve(
     const og_dims *d, int scheme,

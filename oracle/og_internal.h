@@ -166,6 +166,8 @@ typedef struct {
     double *POTT, *DPRES, *qflx_hi, *qflx_J13, *qflx_J23, *Sr, *Sw, *St;
 } og_stage_work;
 int og_stage_work_alloc(og_stage_work *w, size_t N3);
+int og_short_type_get(void);        /* the registered short step: 0 HEVI, 1 HEVE */
+int og_tinteg_short_type_get(void); /* the registered short integrator: 0 RK4, 1 RK3, 2 RK3WS2002 */
 void og_stage_work_free(og_stage_work *w);
 typedef int (*og_stage_fn)(
     const og_dims *d, int scheme, og_stage_work *w,

@@ -131,6 +131,11 @@ out:
 /* the registered short step of the large step (ATMOS_DYN_Tstep_short_regist): 0 HEVI, 1 HEVE */
 static int og_short = 0;
 void og_short_type(int type) { og_short = type; }
+int og_short_type_get(void) { return og_short; }
+/* the registered short integrator (ATMOS_DYN_TINTEG_SHORT_TYPE): 0 RK4, 1 RK3, 2 RK3WS2002 */
+static int og_tinteg = 0;
+void og_tinteg_short_type(int type) { og_tinteg = type; }
+int og_tinteg_short_type_get(void) { return og_tinteg; }
 
 int og_tstep_large(
     const og_dims *d, int scheme, int scheme_tracer,
@@ -214,13 +219,21 @@ int og_tstep_large(
         else
             memset(DDIV, 0, N3 * sizeof(double));
         /* short step :880-894 */
-        if ((rc = (og_short ? og_tinteg_short_rk4_heve : og_tinteg_short_rk4)(
-                 d, scheme, DENS, MOMZ, MOMX, MOMY, RHOT, mflx_hi, tflx_hi,
-                                      tend, tend + N3, tend + 2 * N3, tend + 3 * N3, tend + 4 * N3,
-                                      DPRES0, RT2P, CORIOLI, num_diff, wdamp_coef, divdmp_coef, DDIV,
-                                      CDZ, FDZ, FDX, FDY, RCDZ, RCDX, RCDY, RFDZ, RFDX, RFDY,
-                                      PHI, GSQRT, J13G, J23G, J33G, MAPF, REF_dens, REF_rhot, dts)))
-            goto out;
+        /* ATMOS_DYN_tinteg_short: the registered integrator and short step */
+        if (og_tinteg)
+            rc = og_tinteg_short_rk3(d, scheme, og_tinteg == 2, DENS, MOMZ, MOMX, MOMY, RHOT, mflx_hi, tflx_hi,
+                                     tend, tend + N3, tend + 2 * N3, tend + 3 * N3, tend + 4 * N3,
+                                     DPRES0, RT2P, CORIOLI, num_diff, wdamp_coef, divdmp_coef, DDIV,
+                                     CDZ, FDZ, FDX, FDY, RCDZ, RCDX, RCDY, RFDZ, RFDX, RFDY,
+                                     PHI, GSQRT, J13G, J23G, J33G, MAPF, REF_dens, REF_rhot, dts);
+        else
+            rc = (og_short ? og_tinteg_short_rk4_heve : og_tinteg_short_rk4)(
+                d, scheme, DENS, MOMZ, MOMX, MOMY, RHOT, mflx_hi, tflx_hi,
+                tend, tend + N3, tend + 2 * N3, tend + 3 * N3, tend + 4 * N3,
+                DPRES0, RT2P, CORIOLI, num_diff, wdamp_coef, divdmp_coef, DDIV,
+                CDZ, FDZ, FDX, FDY, RCDZ, RCDX, RCDY, RFDZ, RFDX, RFDY,
+                PHI, GSQRT, J13G, J23G, J33G, MAPF, REF_dens, REF_rhot, dts);
+        if (rc) goto out;
         /* vertical boundary fill :910-926 */
 #pragma omp parallel for collapse(2)
         for (int j = JS; j <= JE; ++j)

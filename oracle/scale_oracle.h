@@ -118,8 +118,27 @@ int og_tinteg_short_rk4_heve(
     const double *MAPF, const double *REF_dens, const double *REF_rhot,
     double dt);
 
-/* ---- the short step og_tstep_large runs (ATMOS_DYN_Tstep_short_regist): 0 HEVI (default), 1 HEVE ---- */
+/* ---- RK3 short integrator: scale_atmos_dyn_tinteg_short_rk3.F90:188-576, with the
+ *      registered short step; ws2002 = 1 for RK3WS2002, 0 for RK3 (Heun) ---- */
+int og_tinteg_short_rk3(
+    const og_dims *d, int scheme, int ws2002,
+    double *DENS, double *MOMZ, double *MOMX, double *MOMY, double *RHOT,
+    double *mflx_hi, double *tflx_hi,
+    const double *DENS_t, const double *MOMZ_t, const double *MOMX_t, const double *MOMY_t, const double *RHOT_t,
+    const double *DPRES0, const double *RT2P, const double *CORIOLI,
+    const double *num_diff, const double *wdamp_coef, double divdmp_coef, const double *DDIV,
+    const double *CDZ, const double *FDZ, const double *FDX, const double *FDY,
+    const double *RCDZ, const double *RCDX, const double *RCDY,
+    const double *RFDZ, const double *RFDX, const double *RFDY,
+    const double *PHI, const double *GSQRT, const double *J13G, const double *J23G, double J33G,
+    const double *MAPF, const double *REF_dens, const double *REF_rhot,
+    double dt);
+
+/* ---- the short step and short integrator that og_tstep_large and og_tinteg_short_rk3 run
+ *      (ATMOS_DYN_Tstep_short_regist, ATMOS_DYN_TINTEG_SHORT_TYPE): short 0 HEVI (default),
+ *      1 HEVE; integrator 0 RK4 (default), 1 RK3, 2 RK3WS2002 ---- */
 void og_short_type(int type);
+void og_tinteg_short_type(int type);
 
 /* ---- periodic 8-neighbour halo fill, scale_comm_cartesC.F90 (COMM_vars8 on a periodic 1x1 grid) ---- */
 void og_halo_periodic(const og_dims *d, double *var, int nfields);

@@ -31,6 +31,7 @@ struct Ctx {
     Grid g{};
     int scheme = UD3, scheme_tracer = UD3;
     int short_type = 0;  // the registered short step of the RK4 and large-step entries: 0 HEVI, 1 HEVE
+    int tinteg_type = 0; // the short integrator of the large step: 0 RK4, 1 RK3 (Heun), 2 RK3WS2002
     size_t N3 = 0;   // points of one 3-D field (all members)
     // ensemble members sharing the pooled arrays (one entry for a single domain)
     std::vector<MemberGeom> members;
@@ -423,7 +424,8 @@ StageArgsT<F> stage_args(const StageInT<F> &in, double *const out[5], F *mflx, F
     a.DPRES0 = in.DPRES0; a.RT2P = in.RT2P; a.CORIOLI = in.CORIOLI; a.num_diff = in.num_diff;
     a.wdamp = C.d_wdamp; a.DDIV = in.DDIV; a.REF_dens = in.REF_dens; a.REF_rhot = in.REF_rhot;
     a.divdmp_coef = in.divdmp; a.J33G = in.J33G; a.dtrk = dtrk;
-    a.rk_mode = mode; a.acc = C.acc; a.facc = facc_buf<F>(); a.status = C.status; a.colscr = colscr_buf<F>();
+    a.rk_mode = mode; a.acc = mode == RK_HEUN3 ? C.rk[0] : C.acc; a.facc = facc_buf<F>(); a.status = C.status;
+    a.colscr = colscr_buf<F>();
     return a;
 }
 
@@ -540,6 +542,47 @@ int run_rk4(double *X[5], F *mflx, F *tflx, const StageInT<F> &base, double dt)
         }
     }
     return SCALE_HEVI_OK;
+}
+
+// RK3 short step on device arrays (tinteg_short_rk3.F90:188-576): stages at
+// dt/3, dt*fact_dt2 and dt; stage 1 writes C.rk[0], stage 2 C.rk[1] (each then
+// halo-filled, :391-406 and :444-459), stage 3 the state in place. Heun's RK3
+// (fact_dt2 = 2/3) combines RK1 and the third stage in the last epilogue
+// (:486-566); RK3WS2002 (fact_dt2 = 1/2) keeps the third stage. Stages 1-2 of
+// RK3WS2002 and stage 2 of Heun's write their fluxes to mflx/tflx, where stage 3
+// overwrites them at the same cells.
+template <typename F>
+int run_rk3(double *X[5], F *mflx, F *tflx, const StageInT<F> &base, double dt, bool ws2002)
+{
+    StageInT<F> in = base;
+    in.DENS0 = X[0]; in.MOMZ0 = X[1]; in.MOMX0 = X[2]; in.MOMY0 = X[3]; in.RHOT0 = X[4];
+    const double fact_dt1 = 1.0 / 3.0, fact_dt2 = ws2002 ? 1.0 / 2.0 : 2.0 / 3.0;
+    const double dts[3] = {dt * fact_dt1, dt * fact_dt2, dt};
+    const int modes[3] = {ws2002 ? RK_PLAIN : RK_HEUN1, RK_PLAIN, ws2002 ? RK_PLAIN : RK_HEUN3};
+    const double *src[5] = {X[0], X[1], X[2], X[3], X[4]};
+    for (int s = 0; s < 3; ++s) {
+        in.DENS = src[0]; in.MOMZ = src[1]; in.MOMX = src[2]; in.MOMY = src[3]; in.RHOT = src[4];
+        double *out[5];
+        if (s < 2) {
+            for (int v = 0; v < 5; ++v) out[v] = C.rk[s] + (size_t)v * C.N3;
+        } else {
+            for (int v = 0; v < 5; ++v) out[v] = X[v];
+        }
+        CK(run_stage(in, out, mflx, tflx, dts[s], modes[s]));
+        if (s < 2) {
+            CK(halo(out, 5));
+            for (int v = 0; v < 5; ++v) src[v] = out[v];
+        }
+    }
+    return SCALE_HEVI_OK;
+}
+
+// the registered short integrator (ATMOS_DYN_tinteg_short, scale_atmos_dyn_tinteg_short.F90)
+template <typename F>
+int run_short(double *X[5], F *mflx, F *tflx, const StageInT<F> &base, double dt)
+{
+    if (C.tinteg_type == 0) return run_rk4(X, mflx, tflx, base, dt);
+    return run_rk3(X, mflx, tflx, base, dt, C.tinteg_type == 2);
 }
 
 template <typename R>
@@ -760,6 +803,18 @@ int scale_hevi_short_type(const char *type)
     return fail(SCALE_HEVI_ERR_UNSUPPORTED, "short-step type '%s' is not supported (HEVI, HEVE)", n.c_str());
 }
 
+int scale_hevi_tinteg_short_type(const char *type)
+{
+    CK(need_setup());
+    if (!type) return fail(SCALE_HEVI_ERR_ARG, "short integrator type is NULL");
+    std::string n(type);
+    while (!n.empty() && n.back() == ' ') n.pop_back(); // Fortran blank padding
+    if (n == "RK4") { C.tinteg_type = 0; return SCALE_HEVI_OK; }
+    if (n == "RK3") { C.tinteg_type = 1; return SCALE_HEVI_OK; }
+    if (n == "RK3WS2002") { C.tinteg_type = 2; return SCALE_HEVI_OK; }
+    return fail(SCALE_HEVI_ERR_UNSUPPORTED, "short integrator '%s' is not supported (RK4, RK3, RK3WS2002)", n.c_str());
+}
+
 int scale_hevi_stage_shape(int tile_x, int raster)
 {
     CK(need_setup());
@@ -963,6 +1018,72 @@ int ATMOS_DYN_Tinteg_short_rk4_b200(SCALE_HEVI_TINTEG_SHORT_ARGS)
     StageIn base{nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
                  T[0], T[1], T[2], T[3], T[4], dp0, rt, cor, nd, ddiv, rd, rr, *divdmp_coef, *J33G};
     CK(run_rk4(X, mf, tf, base, *dt));
+    for (int v = 0; v < 5; ++v) CK(d2h(hx[v], X[v], N3));
+    CK(d2h(mflx_hi, mf, 3 * N3));
+    CK(d2h(tflx_hi, tf, 3 * N3));
+    CU(cudaStreamSynchronize(C.stream));
+    (void)PROG; (void)FLAG_FCT_MOMENTUM; (void)FLAG_FCT_T; (void)FLAG_FCT_ALONG_STREAM; (void)PHI;
+    return scale_hevi_check();
+}
+
+// ---- RK3 short step (Heun's RK3 or RK3WS2002) -----------------------------------
+// the RK3 variant chosen by ATMOS_DYN_Tinteg_short_rk3_setup (tinteg_short_rk3.F90:104-132),
+// here by scale_hevi_tinteg_short_type
+static int rk3_type(bool *ws2002)
+{
+    if (C.tinteg_type == 0)
+        return fail(SCALE_HEVI_ERR_UNSUPPORTED, "the registered short integrator is RK4; register RK3 or RK3WS2002 first");
+    *ws2002 = C.tinteg_type == 2;
+    return SCALE_HEVI_OK;
+}
+
+int ATMOS_DYN_Tinteg_short_rk3_b200_dev(SCALE_HEVI_TINTEG_SHORT_ARGS)
+{
+    (void)PROG; (void)FLAG_FCT_ALONG_STREAM; (void)PHI;
+    CK(need_setup());
+    bool ws2002;
+    CK(rk3_type(&ws2002));
+    if (C.short_type == 1) CK(check_heve_fct(FLAG_FCT_MOMENTUM, FLAG_FCT_T));
+    CK(check_bnd(BND_W, BND_E, BND_S, BND_N));
+    CK(check_flat(GSQRT, J13G, J23G, MAPF, true));
+    CK(prepare_tables(CDZ, FDZ, RCDZ, RFDZ, FDX, RCDX, RFDX, FDY, RCDY, RFDY, wdamp_coef, nullptr, nullptr));
+    double *X[5] = {DENS, MOMZ, MOMX, MOMY, RHOT};
+    StageIn base{nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
+                 DENS_t, MOMZ_t, MOMX_t, MOMY_t, RHOT_t, DPRES0, RT2P, CORIOLI, num_diff, DDIV, REF_dens, REF_rhot,
+                 *divdmp_coef, *J33G};
+    return run_rk3(X, mflx_hi, tflx_hi, base, *dt, ws2002);
+}
+
+int ATMOS_DYN_Tinteg_short_rk3_b200(SCALE_HEVI_TINTEG_SHORT_ARGS)
+{
+    CK(need_single("the host-array RK3 entry"));
+    bool ws2002;
+    CK(rk3_type(&ws2002));
+    if (C.short_type == 1) CK(check_heve_fct(FLAG_FCT_MOMENTUM, FLAG_FCT_T));
+    CK(check_bnd(BND_W, BND_E, BND_S, BND_N));
+    CK(check_flat(GSQRT, J13G, J23G, MAPF, false));
+    const size_t N3 = n3(), N2 = (size_t)C.g.IA * C.g.JA;
+    double *hx[5] = {DENS, MOMZ, MOMX, MOMY, RHOT};
+    const double *htt[5] = {DENS_t, MOMZ_t, MOMX_t, MOMY_t, RHOT_t};
+    static const char *n_x[5] = {"x0", "x1", "x2", "x3", "x4"}, *n_t[5] = {"t0", "t1", "t2", "t3", "t4"};
+    double *X[5], *T[5], *mf, *tf, *dp0, *rt, *cor, *nd, *ddiv = nullptr, *rd, *rr;
+    for (int v = 0; v < 5; ++v) {
+        CK(h2d(n_x[v], hx[v], N3, &X[v]));
+        CK(h2d(n_t[v], htt[v], N3, &T[v]));
+    }
+    CK(h2d("mflx", mflx_hi, 3 * N3, &mf));
+    CK(h2d("tflx", tflx_hi, 3 * N3, &tf));
+    CK(h2d("DPRES0", DPRES0, N3, &dp0));
+    CK(h2d("RT2P", RT2P, N3, &rt));
+    CK(h2d("CORIOLI", CORIOLI, N2, &cor));
+    CK(h2d("num_diff", num_diff, 15 * N3, &nd));
+    if (*divdmp_coef != 0.0) CK(h2d("DDIV", DDIV, N3, &ddiv));
+    CK(h2d("REF_dens", REF_dens, N3, &rd));
+    CK(h2d("REF_rhot", REF_rhot, N3, &rr));
+    CK(prepare_tables(CDZ, FDZ, RCDZ, RFDZ, FDX, RCDX, RFDX, FDY, RCDY, RFDY, wdamp_coef, nullptr, nullptr));
+    StageIn base{nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
+                 T[0], T[1], T[2], T[3], T[4], dp0, rt, cor, nd, ddiv, rd, rr, *divdmp_coef, *J33G};
+    CK(run_rk3(X, mf, tf, base, *dt, ws2002));
     for (int v = 0; v < 5; ++v) CK(d2h(hx[v], X[v], N3));
     CK(d2h(mflx_hi, mf, 3 * N3));
     CK(d2h(tflx_hi, tf, 3 * N3));
@@ -1258,7 +1379,7 @@ int ATMOS_DYN_Tstep_large_fvm_heve_b200_dev(SCALE_HEVI_LARGE_ARGS)
         // divergence for the damping term, :860-871
         if (use_div) CK(run_divergence(DDIV, MOMZ, MOMX, MOMY, C.g.RCDZ, C.g.RCDX, C.g.RCDY, *J33G));
         if (step == 1) CK(wait_in(2));
-        CK(run_rk4(X, mflx_hi, tflx_hi, base, dts));
+        CK(run_short(X, mflx_hi, tflx_hi, base, dts));
         CK(timed("boundary", [&] { vertical_bc(C.g, mem(), DENS, MOMZ, MOMX, MOMY, RHOT, C.stream); return SCALE_HEVI_OK; }));
         ++C.launches;
         CK(halo(X, 5));
@@ -1385,6 +1506,8 @@ int scale_hevi_adjoint_setup(const double *DPRES0, const double *RT2P, const dou
     if (wide_scheme(C.scheme))
         return fail(SCALE_HEVI_ERR_UNSUPPORTED, "the differentiated short step supports UD3, CD4, UD3KOREN1993 and CD2");
     if (C.short_type != 0) return fail(SCALE_HEVI_ERR_UNSUPPORTED, "the differentiated short step is the HEVI step");
+    if (C.tinteg_type != 0)
+        return fail(SCALE_HEVI_ERR_UNSUPPORTED, "the differentiated short step is integrated with RK4");
     const double *v[12] = {CDZ, CDX, CDY, FDZ, FDX, FDY, RCDZ, RCDX, RCDY, RFDZ, RFDX, RFDY};
     const int len[12] = {C.g.KA, C.g.IA, C.g.JA, C.g.KA - 1, C.g.IA - 1, C.g.JA - 1,
                          C.g.KA, C.g.IA, C.g.JA, C.g.KA - 1, C.g.IA - 1, C.g.JA - 1};

@@ -62,7 +62,7 @@ template <typename T> __device__ __forceinline__ T lds(const T *p) { return __ld
 template <typename T> __device__ __forceinline__ void sts(T *p, T v) { *p = v; }
 #endif
 
-// store one prognostic value of the stage, folding in the RK4 combine
+// store one prognostic value of the stage, folding in the RK4 or RK3 combine
 template <typename F>
 __device__ __forceinline__ void put_state(const StageArgsT<F> &a, size_t N3, int v, double *out, const double *x0,
                                           size_t c, double val, bool combine)
@@ -73,6 +73,13 @@ __device__ __forceinline__ void put_state(const StageArgsT<F> &a, size_t N3, int
     case RK_STAGE1: sts(out + c, val); if (combine) sts(acc, val * 2.0); break;
     case RK_STAGE2: sts(out + c, val); if (combine) sts(acc, lds(acc) + val * 4.0); break;
     case RK_STAGE3: sts(out + c, val); if (combine) sts(acc, lds(acc) + val * 2.0); break;
+    case RK_HEUN1: sts(out + c, val); break;
+    case RK_HEUN3: {
+        double r = combine ? ((lds(acc) * 3.0 + val * 3.0) - lds(x0 + c) * 2.0) / 4.0 : val;
+        sts(out + c, r);
+        flag_nonfinite(a.status, r);
+        break;
+    }
     default: {
         double r = combine ? ((lds(acc) + val) - lds(x0 + c) * 3.0) / 6.0 : val;
         sts(out + c, r);
@@ -82,7 +89,7 @@ __device__ __forceinline__ void put_state(const StageArgsT<F> &a, size_t N3, int
 }
 
 // store one flux value (f: 0..2 mflx Z,X,Y; 3..5 tflx Z,X,Y); 'interior' marks the
-// cells the RK4 combine averages (k in KS:KE, i in IS:IE, j in JS:JE)
+// cells the RK4 and RK3 combines average (k in KS:KE, i in IS:IE, j in JS:JE)
 template <typename F>
 __device__ __forceinline__ void put_flux(const StageArgsT<F> &a, size_t N3, int f, size_t c, F val, bool interior)
 {
@@ -93,6 +100,8 @@ __device__ __forceinline__ void put_flux(const StageArgsT<F> &a, size_t N3, int 
     case RK_STAGE1: if (interior) sts(acc, val); break;
     case RK_STAGE2:
     case RK_STAGE3: if (interior) sts(acc, lds(acc) + val * F(2.0)); break;
+    case RK_HEUN1: if (interior) sts(acc, val); break;
+    case RK_HEUN3: sts(out, interior ? (lds(acc) + val * F(3.0)) / F(4.0) : val); break;
     default: sts(out, interior ? (lds(acc) + val) / F(6.0) : val);
     }
 }
@@ -563,7 +572,7 @@ __global__ void __launch_bounds__(32 * HEVI_COL_TC, HEVI_COL_MINB)
     }
     // hevi_mflx_z :369-393 also fills the halo column i = IS-1 with the explicit
     // part of the vertical mass flux; the solver never updates it
-    if (ti == 0 && tx == 0 && col_ok && (a.rk_mode == RK_PLAIN || a.rk_mode == RK_FINAL)) {
+    if (ti == 0 && tx == 0 && col_ok && (a.rk_mode == RK_PLAIN || a.rk_mode == RK_FINAL || a.rk_mode == RK_HEUN3)) {
         const size_t ch = idx3(g, 1, g.IS - 1, j);
         for (int k = KS - 1 + lane; k <= KE; k += 32)
             a.mflx[ch + k - 1] = (k >= KS && k <= KE - 1) ? ld(nd.DZ() + ch + k - 1) : R(0.0);

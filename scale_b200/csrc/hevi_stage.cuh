@@ -17,6 +17,12 @@ enum RkMode : int {
     RK_STAGE2 = 2, // acc += X*4, facc += F*2
     RK_STAGE3 = 3, // acc += X*2, facc += F*2
     RK_FINAL = 4,  // X = ((acc + X) - X0*3)/6, F = (facc + F)/6 over the interior
+    // Heun's RK3 (scale_atmos_dyn_tinteg_short_rk3.F90:188-576): stage 1 writes
+    // RK1 to its buffer and F1 to facc; stage 2 is RK_PLAIN; stage 3 forms
+    //   X = ((RK1*3 + X3*3) - X0*2)/4, F = (F1 + F3*3)/4 over the interior
+    // with acc pointing at the stage-1 buffer.
+    RK_HEUN1 = 5,
+    RK_HEUN3 = 6,
 };
 
 // Per-level sources Sr, St and the vertical theta flux tZ of the implicit

@@ -94,7 +94,7 @@ def load(path: str | os.PathLike | None = None) -> C.CDLL:
             f.argtypes = [C.c_int, C.POINTER(Index), C.c_char_p, C.c_char_p, C.c_int]
         elif name == "scale_hevi_stage_shape":
             f.argtypes = [C.c_int, C.c_int]
-        elif name == "scale_hevi_short_type":
+        elif name in ("scale_hevi_short_type", "scale_hevi_tinteg_short_type"):
             f.argtypes = [C.c_char_p]
         elif name == "scale_hevi_stage_autotune":
             f.argtypes = [C.c_int]
@@ -226,6 +226,12 @@ def short_type(name: str = "HEVI") -> None:
     _check(load().scale_hevi_short_type(name.encode()))
 
 
+def tinteg_short_type(name: str = "RK4") -> None:
+    """The short integrator the large step and the RK3 entries run: "RK4",
+    "RK3" (Heun) or "RK3WS2002" (ATMOS_DYN_Tinteg_short_setup)."""
+    _check(load().scale_hevi_tinteg_short_type(name.encode()))
+
+
 def stage_shape(tile_x: int = 0, raster: int = 0) -> None:
     """Tile width and raster height of the stage kernel (0: defaults)."""
     _check(load().scale_hevi_stage_shape(int(tile_x), int(raster)))
@@ -316,6 +322,10 @@ def ATMOS_DYN_Tinteg_short_rk4(**kw):
     call("ATMOS_DYN_Tinteg_short_rk4_b200", **kw)
 
 
+def ATMOS_DYN_Tinteg_short_rk3(**kw):
+    call("ATMOS_DYN_Tinteg_short_rk3_b200", **kw)
+
+
 def ATMOS_DYN_numfilter_coef(**kw):
     call("ATMOS_DYN_numfilter_coef_b200", **kw)
 
@@ -347,6 +357,10 @@ def ATMOS_DYN_Tstep_short_fvm_heve_dev(**kw):
 
 def ATMOS_DYN_Tinteg_short_rk4_dev(**kw):
     call("ATMOS_DYN_Tinteg_short_rk4_b200_dev", **kw)
+
+
+def ATMOS_DYN_Tinteg_short_rk3_dev(**kw):
+    call("ATMOS_DYN_Tinteg_short_rk3_b200_dev", **kw)
 
 
 def ATMOS_DYN_numfilter_coef_dev(**kw):

@@ -184,7 +184,7 @@ def _large_inputs(c):
     return tp, GS, J13, J23, MAPF
 
 
-def _run_large_both(c, nlarge, lib, divdmp=0.0, nd_order=1, short="HEVI"):
+def _run_large_both(c, nlarge, lib, divdmp=0.0, nd_order=1, short="HEVI", tinteg="RK4"):
     g = c.g
     tp, GS, J13, J23, MAPF = _large_inputs(c)
     aq = mkinit.aq_props(c.QA) if c.QA else None
@@ -197,9 +197,10 @@ def _run_large_both(c, nlarge, lib, divdmp=0.0, nd_order=1, short="HEVI"):
     for _ in range(nlarge):
         oracle.tstep_large(g, c.scheme, c.scheme_tracer, st_ref, out_ref, tp, c.ref, aq, GS, J13, J23, MAPF, cor, wd,
                            c.dtl, c.dt, ND_COEF=c.nd_coef, divdmp=divdmp, fct=c.fct, QA=c.QA, ND_ORDER=nd_order,
-                           short=short)
+                           short=short, tinteg=tinteg)
     lib.setup(g.index_dict(), c.scheme, c.scheme_tracer)
     lib.short_type(short)
+    lib.tinteg_short_type(tinteg)
     R, CV, CP, M = aq if aq else (None, None, None, None)
     for _ in range(nlarge):
         lib.ATMOS_DYN_Tstep_large_fvm_heve(

@@ -223,6 +223,84 @@ def test_rk4_equals_four_stages():
         assert np.array_equal(got[sl], exp[sl])
 
 
+@pytest.mark.parametrize("ws2002", [True, False])
+def test_rk3_equals_three_stages(ws2002):
+    """ATMOS_DYN_tinteg_short_rk3 restated twice: the oracle's integrator against
+    an explicit sequence of three oracle stages, with Heun's combine for RK3
+    (scale_atmos_dyn_tinteg_short_rk3.F90:188-576)."""
+    g = helpers.small_grid(9, 8, 12)
+    c = helpers.small_case(g)
+    helpers.perturb_state(c)
+    a = helpers.short_inputs(c, full=True)
+    for kk in ("DENS0", "MOMZ0", "MOMX0", "MOMY0", "RHOT0", "DENS", "MOMZ", "MOMX", "MOMY", "RHOT", "dtrk"):
+        a.pop(kk)
+    x = {n: c.state[n].copy(order="F") for n in STATE}
+    x["mflx_hi"] = g.zeros(3) + 7.0
+    x["tflx_hi"] = g.zeros(3) + 7.0
+    x0 = {n: v.copy(order="F") for n, v in x.items()}
+    dt = 1.5
+    oracle.tinteg_short_rk3(g, "CD4", x, dict(a, dt=dt), ws2002=ws2002)
+    rk, fl = [], []
+    cur = {n: x0[n] for n in STATE}
+    for s, dtrk in enumerate((dt * (1.0 / 3.0), dt * (1.0 / 2.0 if ws2002 else 2.0 / 3.0), dt)):
+        o = helpers.stage_outputs(g, 0.0)
+        args = dict(a, dtrk=dtrk)
+        args.update({n + "0": x0[n] for n in STATE})
+        args.update(cur)
+        if s == 2:
+            o["mflx_hi"] = x0["mflx_hi"].copy(order="F")
+            o["tflx_hi"] = x0["tflx_hi"].copy(order="F")
+        oracle.tstep_short(g, "CD4", o, args)
+        st = {n: o[n + "_RK"] for n in STATE}
+        if s < 2:
+            for n in STATE:
+                oracle.halo(g, st[n])
+        rk.append(st)
+        fl.append((o["mflx_hi"], o["tflx_hi"]))
+        cur = st
+    sl = (slice(g.KS - 1, g.KE), slice(g.IS - 1, g.IE), slice(g.JS - 1, g.JE))
+    for n in STATE:
+        exp = rk[2][n] if ws2002 else (rk[0][n] * 3.0 + rk[2][n] * 3.0 - x0[n] * 2.0) / 4.0
+        ks = slice(g.KS - 1, g.KE - 1) if n == "MOMZ" else sl[0]
+        assert np.array_equal(x[n][ks, sl[1], sl[2]], exp[ks, sl[1], sl[2]]), n
+    for f in range(2):
+        got = x["mflx_hi" if f == 0 else "tflx_hi"]
+        exp = fl[2][f] if ws2002 else (fl[0][f] + fl[2][f] * 3.0) / 4.0
+        assert np.array_equal(got[sl], exp[sl])
+
+
+@pytest.mark.parametrize("tinteg", ["RK3", "RK3WS2002"])
+def test_rk3_conserve(tinteg):
+    """test_conserve (test_atmos_dyn.f90:456-592) with the RK3 short integrators:
+    the volume-weighted totals of DENS and RHOT are conserved to round-off."""
+    g = helpers.small_grid(10, 8, 14, stretched=True)
+    c = mkinit.make_case("conserve rk3", g, "CD4", "CD4", dt=0.5)
+    k, i, j = np.meshgrid(np.arange(1, g.KA + 1), np.arange(1, g.IA + 1), np.arange(1, g.JA + 1), indexing="ij")
+    st = c.state
+    st["MOMZ"][...] = (k + i + j) * 0.01
+    st["MOMX"][...] = (k * 2 + i + j) * 0.01
+    st["MOMY"][...] = (k + i * 2 + j) * 0.01
+    st["DENS"][...] = c.ref["REF_dens"] + (k * 2 + i * 2 + j) * 1e-4
+    st["RHOT"][...] = st["DENS"] * (300.0 + (k + i + j * 2) * 0.01)
+    for n in STATE:
+        mkinit.periodic_fill(st[n], g)
+    mkinit.vertical_fill(st, g)
+    m0 = oracle.domain_sum(g, st["DENS"])
+    t0 = oracle.domain_sum(g, st["RHOT"])
+    a = helpers.short_inputs(c, full=False)
+    for kk in ("DENS0", "MOMZ0", "MOMX0", "MOMY0", "RHOT0", "DENS", "MOMZ", "MOMX", "MOMY", "RHOT", "dtrk"):
+        a.pop(kk)
+    x = {n: st[n] for n in STATE}
+    x["mflx_hi"], x["tflx_hi"] = g.zeros(3), g.zeros(3)
+    for _ in range(3):
+        oracle.tinteg_short_rk3(g, c.scheme, x, dict(a, dt=c.dt), ws2002=(tinteg == "RK3WS2002"))
+        for n in STATE:
+            mkinit.periodic_fill(st[n], g)
+        mkinit.vertical_fill(st, g)
+    assert abs(oracle.domain_sum(g, st["DENS"]) - m0) / m0 < 1e-13
+    assert abs(oracle.domain_sum(g, st["RHOT"]) - t0) / t0 < 1e-13
+
+
 @pytest.mark.parametrize("fct", [False, True])
 def test_koren_tracer_keeps_uniform_tracer(fct):
     """test_cwc with the UD3KOREN1993 tracer flux (the reference's default
