@@ -5,11 +5,11 @@
 //
 // Two kernels. k_phi evaluates the five filtered quantities (density and
 // theta deviations, three velocities) once at every point into a scratch of
-// five fields, so no quotient is formed twice. k_numfilter then has one thread
-// per (k,i,j) of an interior column write all 15 components at its level,
-// including the zero and mirrored values of the vertical halo, reading the
-// quantities from the scratch. The lateral halo is filled afterwards by the
-// periodic halo kernel, as COMM_vars8 does in the reference.
+// five fields, so no quotient is formed twice. k_numfilter then has the lanes
+// of a warp take the levels KS..KE of one interior column and write all 15
+// components there, then the zero and mirrored values of the vertical halo,
+// reading the quantities from the scratch. The lateral halo is filled
+// afterwards by the periodic halo kernel, as COMM_vars8 does in the reference.
 //
 // R is the output and arithmetic type: double on the plain path, float on the
 // mixed-precision path (the deviations from the base state and the quotients
@@ -22,31 +22,38 @@ namespace hevi {
 #define CX3(n, i, s) (R)ld(c.CNX3 + ((n) - 1) + 3 * ((size_t)((i) - 1) + (size_t)g.IA * ((s) - 1)))
 #define CY3(n, j, s) (R)ld(c.CNY3 + ((n) - 1) + 3 * ((size_t)((j) - 1) + (size_t)g.JA * ((s) - 1)))
 
+constexpr int PHI_THREADS = 256;
+
 // The five filtered quantities at one point.
 // q: 0 DENS-REF_dens, 1 VELZ, 2 VELX, 3 VELY, 4 RHOT/DENS-REF_pott  (:538-547, 621-626, 715-720, 799-804, 876-883)
 // A velocity needs the density one point above (VELZ), east (VELX) or north
 // (VELY); at the last point of the array in that direction, which no stencil
-// reads, it is stored as zero.
+// reads, it is stored as zero. One thread per point of the (KA,IA,JA) array,
+// in memory order: one fully coalesced stream with no idle lanes at the
+// column ends.
 template <typename R, int NM>
-__global__ void __launch_bounds__(128) k_phi(const Grid gt, const NdArgsT<R> a, const BatchT<NM> B)
+__global__ void __launch_bounds__(PHI_THREADS) k_phi(const Grid gt, const NdArgsT<R> a, const BatchT<NM> B)
 {
     int b;
     const Grid g = block_domain(gt, B, b);
-    const Block2 p = split_block(b, (g.IA + 3) / 4);
-    const int i = 1 + p.x * blockDim.y + threadIdx.y;
-    const int j = 1 + p.y;
-    if (i > g.IA) return;
+    // 32-bit index arithmetic: a field has fewer than 2^31 points (checked at setup)
+    const unsigned npts = (unsigned)g.KA * g.IA * g.JA;
+    const unsigned pt = (unsigned)b * PHI_THREADS + threadIdx.x;
+    if (pt >= npts) return;
+    const unsigned KA = g.KA, IA = g.IA;
+    const unsigned r = pt / KA;
+    const int k = (int)(pt - r * KA) + 1;
+    const unsigned jj = r / IA;
+    const int i = (int)(r - jj * IA) + 1, j = (int)jj + 1;
     const size_t N3 = n3(g);
     const long sI = g.KA, sJ = (long)g.KA * g.IA;
-    for (int k = 1 + threadIdx.x; k <= g.KA; k += 32) {
-        const size_t c = idx3(g, k, i, j);
-        const double D = ld(a.DENS + c);
-        a.phi[c] = R(D - ld(a.REF_dens + c));
-        a.phi[c + N3] = R(k < g.KA ? 2.0 * ld(a.MOMZ + c) / (ld(a.DENS + c + 1) + D) : 0.0);
-        a.phi[c + 2 * N3] = R(i < g.IA ? 2.0 * ld(a.MOMX + c) / (ld(a.DENS + c + sI) + D) : 0.0);
-        a.phi[c + 3 * N3] = R(j < g.JA ? 2.0 * ld(a.MOMY + c) / (ld(a.DENS + c + sJ) + D) : 0.0);
-        a.phi[c + 4 * N3] = R(ld(a.RHOT + c) / D - ld(a.REF_pott + c));
-    }
+    const size_t c = (size_t)g.cell0 + (size_t)pt;
+    const double D = ld(a.DENS + c);
+    a.phi[c] = R(D - ld(a.REF_dens + c));
+    a.phi[c + N3] = R(k < g.KA ? 2.0 * ld(a.MOMZ + c) / (ld(a.DENS + c + 1) + D) : 0.0);
+    a.phi[c + 2 * N3] = R(i < g.IA ? 2.0 * ld(a.MOMX + c) / (ld(a.DENS + c + sI) + D) : 0.0);
+    a.phi[c + 3 * N3] = R(j < g.JA ? 2.0 * ld(a.MOMY + c) / (ld(a.DENS + c + sJ) + D) : 0.0);
+    a.phi[c + 4 * N3] = R(ld(a.RHOT + c) / D - ld(a.REF_pott + c));
 }
 
 // the quantities read back by the stencils
@@ -145,6 +152,10 @@ __device__ __forceinline__ R dy(const Grid &g, const NdCoef &c, const Phi<R> &ph
 
 // FW: the differences come from the calc_numdiff work buffer W (ND_ORDER > 1)
 // instead of being formed from phi here (ND_ORDER = 1)
+//
+// The lanes of a warp take the levels KS..KE of one column, so that every
+// pass over 32 levels but the last is full; the halo levels (zero, except the
+// mirrors at KS-1 of density and theta) are written by a short tail pass.
 template <typename R, int NM, bool FW = false>
 __global__ void __launch_bounds__(128, HEVI_ND_MINB)
     k_numfilter(const Grid gt, const NdCoef ct, const NdArgsT<R> a, const BatchT<NM> B, const double *W = nullptr)
@@ -169,60 +180,75 @@ __global__ void __launch_bounds__(128, HEVI_ND_MINB)
         if (k == KS + 1) return v * (R(1.0) + sfc) * R(0.5);
         return v;
     };
-    for (int k = 1 + threadIdx.x; k <= g.KA; k += 32) {
+    R *ND = a.num_diff;
+    for (int k = KS + threadIdx.x; k <= KE; k += 32) {
         const size_t o = idx3(g, k, i, j);
         // the difference of quantity q in a direction: formed here from phi, or
         // read from the work buffer (the expression is then not evaluated)
 #define DZ(q, expr) (FW ? R(ld(W + (size_t)(3 * (q) + 0) * N3 + o)) : (expr))
 #define DX(q, expr) (FW ? R(ld(W + (size_t)(3 * (q) + 1) * N3 + o)) : (expr))
 #define DY(q, expr) (FW ? R(ld(W + (size_t)(3 * (q) + 2) * N3 + o)) : (expr))
-        const R ncz = (k >= KS - 1 && k <= KE) ? R(ld(c.cdz + k - 1)) : R(0.0);
-        R *ND = a.num_diff;
-        const bool kin = (k >= KS && k <= KE);
-        // ---- density (:553-610) ----
-        ND[o + N3 * 0] = (k >= KS - 1 && k <= KE) ? DZ(0, dz0(g, c, phi, 0, k, i, j)) * ncz : R(0.0);
-        ND[o + N3 * 5] = kin ? sfct(k, DX(0, dx(g, c, phi, 0, 0, k, i, j)) * ncx) : R(0.0);
-        ND[o + N3 * 10] = kin ? sfct(k, DY(0, dy(g, c, phi, 0, 0, k, i, j)) * ncy) : R(0.0);
-        // ---- z momentum (:628-698), phi = VELZ on KS..KE-1 ----
-        {
-            const bool kz = (k >= KS && k <= KE - 1);
-            const R nfz = (k >= KS + 1 && k <= KE - 1) ? R(ld(c.fdz + k - 1)) : R(0.0);
-            ND[o + N3 * 1] = (k >= KS + 1 && k <= KE - 1) ? DZ(1, dz1(g, c, phi, 1, k, i, j)) * nfz * R(ld(DN + o)) : R(0.0);
-            ND[o + N3 * 6] = kz ? sfct(k, DX(1, dx(g, c, phi, 1, 0, k, i, j)) * ncx
-                                              * R(0.25) * (R(ld(DN + o + 1 + sI)) + R(ld(DN + o + 1)) + R(ld(DN + o + sI)) + R(ld(DN + o))))
-                                : R(0.0);
-            ND[o + N3 * 11] = kz ? sfct(k, DY(1, dy(g, c, phi, 1, 0, k, i, j)) * ncy
-                                               * R(0.25) * (R(ld(DN + o + 1 + sJ)) + R(ld(DN + o + 1)) + R(ld(DN + o + sJ)) + R(ld(DN + o))))
-                                 : R(0.0);
+        const R ncz = R(ld(c.cdz + k - 1));
+        const bool kz = k <= KE - 1;
+        // one quantity at a time (the loop is kept rolled, so that the loads of
+        // one quantity's three components are all that is in flight)
+#pragma unroll 1
+        for (int q = 0; q < 5; ++q) {
+            switch (q) {
+            case 0: // ---- density (:553-610) ----
+                ND[o + N3 * 0] = DZ(0, dz0(g, c, phi, 0, k, i, j)) * ncz;
+                ND[o + N3 * 5] = sfct(k, DX(0, dx(g, c, phi, 0, 0, k, i, j)) * ncx);
+                ND[o + N3 * 10] = sfct(k, DY(0, dy(g, c, phi, 0, 0, k, i, j)) * ncy);
+                break;
+            case 1: { // ---- z momentum (:628-698), phi = VELZ on KS..KE-1 ----
+                const bool kz1 = k >= KS + 1 && kz;
+                const R nfz = kz1 ? R(ld(c.fdz + k - 1)) : R(0.0);
+                ND[o + N3 * 1] = kz1 ? DZ(1, dz1(g, c, phi, 1, k, i, j)) * nfz * R(ld(DN + o)) : R(0.0);
+                ND[o + N3 * 6] = kz ? sfct(k, DX(1, dx(g, c, phi, 1, 0, k, i, j)) * ncx
+                                                  * R(0.25) * (R(ld(DN + o + 1 + sI)) + R(ld(DN + o + 1)) + R(ld(DN + o + sI)) + R(ld(DN + o))))
+                                    : R(0.0);
+                ND[o + N3 * 11] = kz ? sfct(k, DY(1, dy(g, c, phi, 1, 0, k, i, j)) * ncy
+                                                   * R(0.25) * (R(ld(DN + o + 1 + sJ)) + R(ld(DN + o + 1)) + R(ld(DN + o + sJ)) + R(ld(DN + o))))
+                                     : R(0.0);
+                break;
+            }
+            case 2: // ---- x momentum (:728-790), phi = VELX ----
+                ND[o + N3 * 2] = kz ? DZ(2, dz0(g, c, phi, 2, k, i, j)) * ncz
+                                          * R(0.25) * (R(ld(DN + o + 1 + sI)) + R(ld(DN + o + 1)) + R(ld(DN + o + sI)) + R(ld(DN + o)))
+                                    : R(0.0);
+                ND[o + N3 * 7] = sfct(k, DX(2, dx(g, c, phi, 2, 1, k, i, j)) * nfx * R(ld(DN + o)));
+                ND[o + N3 * 12] = sfct(k, DY(2, dy(g, c, phi, 2, 0, k, i, j)) * ncy
+                                              * R(0.25) * (R(ld(DN + o + sI + sJ)) + R(ld(DN + o + sI)) + R(ld(DN + o + sJ)) + R(ld(DN + o))));
+                break;
+            case 3: // ---- y momentum (:812-870), phi = VELY ----
+                ND[o + N3 * 3] = kz ? DZ(3, dz0(g, c, phi, 3, k, i, j)) * ncz
+                                          * R(0.25) * (R(ld(DN + o + 1 + sJ)) + R(ld(DN + o + 1)) + R(ld(DN + o + sJ)) + R(ld(DN + o)))
+                                    : R(0.0);
+                ND[o + N3 * 8] = sfct(k, DX(3, dx(g, c, phi, 3, 0, k, i, j)) * ncx
+                                             * R(0.25) * (R(ld(DN + o + sI + sJ)) + R(ld(DN + o + sJ)) + R(ld(DN + o + sI)) + R(ld(DN + o))));
+                ND[o + N3 * 13] = sfct(k, DY(3, dy(g, c, phi, 3, 1, k, i, j)) * nfy * R(ld(DN + o)));
+                break;
+            default: { // ---- rho*theta (:885-960) ----
+                const R v = DZ(4, dz0(g, c, phi, 4, k, i, j)) * ncz;
+                ND[o + N3 * 4] = kz ? v * R(0.5) * (R(ld(DN + o + 1)) + R(ld(DN + o))) : v * R(ld(DN + o));
+                ND[o + N3 * 9] = sfct(k, DX(4, dx(g, c, phi, 4, 0, k, i, j)) * ncx * R(0.5) * (R(ld(DN + o + sI)) + R(ld(DN + o))));
+                ND[o + N3 * 14] = sfct(k, DY(4, dy(g, c, phi, 4, 0, k, i, j)) * ncy * R(0.5) * (R(ld(DN + o + sJ)) + R(ld(DN + o))));
+            }
+            }
         }
-        // ---- x momentum (:728-790), phi = VELX ----
-        ND[o + N3 * 2] = (k >= KS && k <= KE - 1)
-                             ? DZ(2, dz0(g, c, phi, 2, k, i, j)) * ncz
-                                   * R(0.25) * (R(ld(DN + o + 1 + sI)) + R(ld(DN + o + 1)) + R(ld(DN + o + sI)) + R(ld(DN + o)))
-                             : R(0.0);
-        ND[o + N3 * 7] = kin ? sfct(k, DX(2, dx(g, c, phi, 2, 1, k, i, j)) * nfx * R(ld(DN + o))) : R(0.0);
-        ND[o + N3 * 12] = kin ? sfct(k, DY(2, dy(g, c, phi, 2, 0, k, i, j)) * ncy
-                                            * R(0.25) * (R(ld(DN + o + sI + sJ)) + R(ld(DN + o + sI)) + R(ld(DN + o + sJ)) + R(ld(DN + o))))
-                              : R(0.0);
-        // ---- y momentum (:812-870), phi = VELY ----
-        ND[o + N3 * 3] = (k >= KS && k <= KE - 1)
-                             ? DZ(3, dz0(g, c, phi, 3, k, i, j)) * ncz
-                                   * R(0.25) * (R(ld(DN + o + 1 + sJ)) + R(ld(DN + o + 1)) + R(ld(DN + o + sJ)) + R(ld(DN + o)))
-                             : R(0.0);
-        ND[o + N3 * 8] = kin ? sfct(k, DX(3, dx(g, c, phi, 3, 0, k, i, j)) * ncx
-                                           * R(0.25) * (R(ld(DN + o + sI + sJ)) + R(ld(DN + o + sJ)) + R(ld(DN + o + sI)) + R(ld(DN + o))))
-                             : R(0.0);
-        ND[o + N3 * 13] = kin ? sfct(k, DY(3, dy(g, c, phi, 3, 1, k, i, j)) * nfy * R(ld(DN + o))) : R(0.0);
-        // ---- rho*theta (:885-960) ----
-        {
-            R v = R(0.0);
-            if (k >= KS && k <= KE - 1) v = DZ(4, dz0(g, c, phi, 4, k, i, j)) * ncz * R(0.5) * (R(ld(DN + o + 1)) + R(ld(DN + o)));
-            else if (k == KS - 1) v = DZ(4, dz0(g, c, phi, 4, k, i, j)) * ncz * R(R(ld(DN + idx3(g, KS, i, j))));
-            else if (k == KE) v = DZ(4, dz0(g, c, phi, 4, k, i, j)) * ncz * R(ld(DN + o));
-            ND[o + N3 * 4] = v;
+    }
+    // halo levels 1..KS-1 and KE+1..KA: zero, except density and theta z at
+    // KS-1 (the mirror -atKS of level KS)
+    const int nlo = KS - 1, nh = nlo + (g.KA - KE);
+    for (int h = threadIdx.x; h < nh; h += 32) {
+        const int k = h < nlo ? h + 1 : KE + 1 + (h - nlo);
+        const size_t o = idx3(g, k, i, j);
+        for (int q = 0; q < 15; ++q) ND[o + N3 * q] = R(0.0);
+        if (k == KS - 1) {
+            const R ncz = R(ld(c.cdz + k - 1));
+            ND[o + N3 * 0] = DZ(0, dz0(g, c, phi, 0, k, i, j)) * ncz;
+            ND[o + N3 * 4] = DZ(4, dz0(g, c, phi, 4, k, i, j)) * ncz * R(R(ld(DN + idx3(g, KS, i, j))));
         }
-        ND[o + N3 * 9] = kin ? sfct(k, DX(4, dx(g, c, phi, 4, 0, k, i, j)) * ncx * R(0.5) * (R(ld(DN + o + sI)) + R(ld(DN + o)))) : R(0.0);
-        ND[o + N3 * 14] = kin ? sfct(k, DY(4, dy(g, c, phi, 4, 0, k, i, j)) * ncy * R(0.5) * (R(ld(DN + o + sJ)) + R(ld(DN + o)))) : R(0.0);
     }
 }
 
@@ -298,8 +324,9 @@ cudaError_t launch_numfilter_high(const Grid &g, const NdCoef &c, const NdArgs &
                                   cudaStream_t st)
 {
     dim3 b(32, 4), gr((g.IMAX + 3) / 4, g.JMAX);
-    const BatchT<1> one{1, {0, ((g.IA + 3) / 4) * g.JA}, {}};
-    k_phi<double, 1><<<one.first[1], b, 0, st>>>(g, a, one);
+    const int nphi = (int)(((long)g.KA * g.IA * g.JA + PHI_THREADS - 1) / PHI_THREADS);
+    const BatchT<1> one{1, {0, nphi}, {}};
+    k_phi<double, 1><<<nphi, PHI_THREADS, 0, st>>>(g, a, one);
     k_nd_diff3<<<gr, b, 0, st>>>(g, c, a, w1);
     double *in = w1, *out = w2;
     for (int no = 2; no <= c.order; ++no) {
@@ -319,10 +346,10 @@ cudaError_t launch_numfilter_high(const Grid &g, const NdCoef &c, const NdArgs &
 template <typename R>
 cudaError_t launch_numfilter(const Grid &g, const Members &mem, const NdCoef &c, const NdArgsT<R> &a, cudaStream_t st)
 {
-    auto nb_phi = [](const Grid &m) { return ((m.IA + 3) / 4) * m.JA; };
+    auto nb_phi = [](const Grid &m) { return (int)(((long)m.KA * m.IA * m.JA + PHI_THREADS - 1) / PHI_THREADS); };
     auto nb_nd = [](const Grid &m) { return ((m.IMAX + 3) / 4) * m.JMAX; };
     with_batch(g, mem, nb_phi, [&](const auto &B, int nb) {
-        k_phi<R, std::decay_t<decltype(B)>::NMAX><<<nb, dim3(32, 4), 0, st>>>(g, a, B);
+        k_phi<R, std::decay_t<decltype(B)>::NMAX><<<nb, PHI_THREADS, 0, st>>>(g, a, B);
         return cudaSuccess;
     });
     with_batch(g, mem, nb_nd, [&](const auto &B, int nb) {
