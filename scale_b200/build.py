@@ -62,7 +62,7 @@ def build_cuda(force: bool = False, verbose: bool = False) -> Path:
     objdir = PKG / "_build"
     objdir.mkdir(exist_ok=True)
     nvcc = _nvcc()
-    common = ["-O3", "-std=c++17", "--fmad=false", "-lineinfo", "-ccbin", _host_cxx(),
+    common = ["-O3", "-std=c++17", "--fmad=false", "--extended-lambda", "-lineinfo", "-ccbin", _host_cxx(),
               "-Xcompiler", "-fPIC,-ffp-contract=off", "-I", str(ROOT / "include")]
     objs, cmds = [], []
     for src in CU_SOURCES + CPP_SOURCES:

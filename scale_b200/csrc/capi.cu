@@ -67,6 +67,12 @@ struct Ctx {
     double *tr = nullptr;           // tracer: RK1, RK2, phi_lo, anti(3), rjp, rjm = 8*N3
     double *lg = nullptr;           // large step: DENS00, RT2P, DPRES0, REF_rhot, mflx_av(3), DDIV = 8*N3
     double *sum_part = nullptr, *sum_out = nullptr;
+    // terrain-following metrics of the current call (the general-metric stage runs when set)
+    bool terrain = false;
+    Metrics tm{};
+    TerrainWork tw{};
+    double *tw_buf = nullptr; // TERRAIN_WORK_FIELDS * N3 (allocated on first use)
+    std::vector<std::vector<const void *>> nonflat; // metric sets already seen to be non-flat
     unsigned *status = nullptr;
     unsigned long long *count = nullptr;
     // metric check cache (pointer tuples already verified flat)
@@ -182,7 +188,8 @@ int falloc(float **p, size_t n)
 
 void free_all()
 {
-    double *bufs[] = {C.phi, C.ndw, C.colscr, C.d_tab, C.d_nd, C.rk[0], C.rk[1], C.acc, C.facc, C.tr, C.lg, C.sum_part, C.sum_out};
+    double *bufs[] = {C.phi, C.ndw, C.colscr, C.d_tab, C.d_nd, C.rk[0], C.rk[1], C.acc, C.facc, C.tr, C.lg, C.sum_part, C.sum_out,
+                      C.tw_buf};
     for (double *b : bufs) if (b) cudaFree(b);
     for (auto &kv : C.stage) cudaFree(kv.second.first);
     for (float *b : {C.facc_f, C.colscr_f, C.phi_f}) if (b) cudaFree(b);
@@ -253,12 +260,14 @@ int check_bnd(const int *W, const int *E, const int *S, const int *N)
     return SCALE_HEVI_OK;
 }
 
-// The kernels assume flat terrain. Verify GSQRT == 1, J13G == J23G == 0 and
-// MAPF == 1 once per distinct set of metric arrays.
-int check_flat(const double *GSQRT, const double *J13G, const double *J23G, const double *MAPF, bool on_device)
+// Whether the metric arrays are those of flat terrain (GSQRT == 1, J13G ==
+// J23G == 0, MAPF == 1), counted once per distinct set of arrays.
+int metrics_flat(const double *GSQRT, const double *J13G, const double *J23G, const double *MAPF, bool on_device,
+                 bool *flat, unsigned long long *nbad = nullptr)
 {
     std::vector<const void *> key = {GSQRT, J13G, J23G, MAPF, (const void *)(size_t)on_device};
-    for (auto &k : C.flat_ok) if (k == key) return SCALE_HEVI_OK;
+    for (auto &k : C.flat_ok) if (k == key) { *flat = true; return SCALE_HEVI_OK; }
+    for (auto &k : C.nonflat) if (k == key) { *flat = false; return SCALE_HEVI_OK; }
     const size_t n7 = 7 * C.N3, nm = C.N2 * 2 * 4;
     unsigned long long bad = 0;
     if (on_device) {
@@ -275,10 +284,60 @@ int check_flat(const double *GSQRT, const double *J13G, const double *J23G, cons
         for (size_t q = 0; J23G && q < n7; ++q) bad += J23G[q] != 0.0;
         for (size_t q = 0; MAPF && q < nm; ++q) bad += MAPF[q] != 1.0;
     }
-    if (bad)
+    *flat = bad == 0;
+    if (nbad) *nbad = bad;
+    (*flat ? C.flat_ok : C.nonflat).push_back(key);
+    return SCALE_HEVI_OK;
+}
+
+// Entries without a general-metric path: flat terrain only.
+int check_flat(const double *GSQRT, const double *J13G, const double *J23G, const double *MAPF, bool on_device)
+{
+    C.terrain = false;
+    bool flat = false;
+    unsigned long long bad = 0;
+    CK(metrics_flat(GSQRT, J13G, J23G, MAPF, on_device, &flat, &bad));
+    if (!flat)
         return fail(SCALE_HEVI_ERR_UNSUPPORTED,
-                    "terrain-following metrics (%llu values of GSQRT/J13G/J23G/MAPF differ from flat terrain) are not supported", bad);
-    C.flat_ok.push_back(key);
+                    "terrain-following metrics (GSQRT/J13G/J23G/MAPF of non-flat terrain) are not supported by this entry");
+    return SCALE_HEVI_OK;
+}
+
+// Entries of the HEVI stage and the short integrators: flat metrics select the
+// fused kernels, any others the general-metric stage (FP64, one domain), which
+// also reads PHI. Host arrays are copied to the device first.
+int use_metrics(const double *GSQRT, const double *J13G, const double *J23G, const double *MAPF, const double *PHI,
+                bool on_device)
+{
+    C.terrain = false;
+    bool flat = false;
+    CK(metrics_flat(GSQRT, J13G, J23G, MAPF, on_device, &flat));
+    if (flat) return SCALE_HEVI_OK;
+    if (C.members.size() > 1)
+        return fail(SCALE_HEVI_ERR_UNSUPPORTED, "terrain-following metrics are supported for a single domain");
+    if (!GSQRT || !J13G || !J23G || !MAPF || !PHI)
+        return fail(SCALE_HEVI_ERR_ARG, "terrain-following metrics need GSQRT, J13G, J23G, MAPF and PHI");
+    if (on_device) {
+        C.tm = Metrics{GSQRT, J13G, J23G, MAPF, PHI};
+    } else {
+        double *g7, *j13, *j23, *mp, *ph;
+        CK(h2d("GSQRT", GSQRT, 7 * C.N3, &g7));
+        CK(h2d("J13G", J13G, 7 * C.N3, &j13));
+        CK(h2d("J23G", J23G, 7 * C.N3, &j23));
+        CK(h2d("MAPF", MAPF, C.N2 * 2 * 4, &mp));
+        CK(h2d("PHI", PHI, C.N3, &ph));
+        C.tm = Metrics{g7, j13, j23, mp, ph};
+    }
+    if (!C.tw_buf) {
+        CK(dalloc(&C.tw_buf, (size_t)TERRAIN_WORK_FIELDS * C.N3));
+        double *q = C.tw_buf;
+        double **f[TERRAIN_WORK_FIELDS] = {&C.tw.POTT, &C.tw.DPRES, &C.tw.qZ, &C.tw.qX, &C.tw.qY, &C.tw.qJ13, &C.tw.qJ23,
+                                           &C.tw.Sr, &C.tw.Sw, &C.tw.St, &C.tw.mZ, &C.tw.mX, &C.tw.mY, &C.tw.tZ,
+                                           &C.tw.tX, &C.tw.tY, &C.tw.A, &C.tw.PT, &C.tw.F1, &C.tw.F2, &C.tw.F3,
+                                           &C.tw.C, &C.tw.e, &C.tw.f};
+        for (int q2 = 0; q2 < TERRAIN_WORK_FIELDS; ++q2) *f[q2] = q + (size_t)q2 * C.N3;
+    }
+    C.terrain = true;
     return SCALE_HEVI_OK;
 }
 
@@ -492,6 +551,20 @@ int run_stage(const StageInT<F> &in, double *const out[5], F *mflx, F *tflx, dou
     if (in.divdmp != 0.0 && C.members.size() > 1)
         return fail(SCALE_HEVI_ERR_UNSUPPORTED, "divergence damping is not available for an ensemble");
     if (kind < 0) kind = C.short_type;
+    if (C.terrain) {
+        if (kind == 1) return fail(SCALE_HEVI_ERR_UNSUPPORTED, "the HEVE short step takes flat terrain only");
+        if constexpr (sizeof(F) != sizeof(double)) {
+            return fail(SCALE_HEVI_ERR_UNSUPPORTED, "the mixed-precision path takes flat terrain only");
+        } else {
+            const StageArgsT<double> a = stage_args(in, out, mflx, tflx, dtrk, mode);
+            CK(timed("hevi_stage_terrain", [&] {
+                CU(launch_terrain_stage(C.g, a, C.tm, C.tw, C.scheme, C.stream));
+                return SCALE_HEVI_OK;
+            }));
+            C.launches += TERRAIN_STAGE_LAUNCHES;
+            return SCALE_HEVI_OK;
+        }
+    }
     if (kind == 1) {
         if constexpr (sizeof(F) != sizeof(double)) {
             return fail(SCALE_HEVI_ERR_UNSUPPORTED, "the mixed-precision path takes the HEVI short step only");
@@ -889,7 +962,7 @@ int ATMOS_DYN_Tstep_short_fvm_hevi_b200_dev(SCALE_HEVI_TSTEP_SHORT_ARGS)
     (void)last; (void)PHI;
     CK(need_setup());
     CK(check_bnd(BND_W, BND_E, BND_S, BND_N));
-    CK(check_flat(GSQRT, J13G, J23G, MAPF, true));
+    CK(use_metrics(GSQRT, J13G, J23G, MAPF, PHI, true));
     CK(prepare_tables(CDZ, FDZ, RCDZ, RFDZ, FDX, RCDX, RFDX, FDY, RCDY, RFDY, wdamp_coef, nullptr, nullptr));
     StageIn in{DENS0, MOMZ0, MOMX0, MOMY0, RHOT0, DENS, MOMZ, MOMX, MOMY, RHOT,
                DENS_t, MOMZ_t, MOMX_t, MOMY_t, RHOT_t, DPRES0, RT2P, CORIOLI, num_diff, DDIV, REF_dens, REF_rhot,
@@ -937,7 +1010,7 @@ static int stage_host(SCALE_HEVI_TSTEP_SHORT_ARGS, int kind)
 {
     CK(need_single("the host-array stage entry"));
     CK(check_bnd(BND_W, BND_E, BND_S, BND_N));
-    CK(check_flat(GSQRT, J13G, J23G, MAPF, false));
+    CK(use_metrics(GSQRT, J13G, J23G, MAPF, PHI, false));
     const size_t N3 = n3(), N2 = (size_t)C.g.IA * C.g.JA;
     const bool use_div = *divdmp_coef != 0.0;
     double *o[5], *mf, *tf, *i0[5], *iv[5], *it[5], *dp0, *rt, *cor, *nd, *ddiv = nullptr, *rd, *rr;
@@ -981,7 +1054,7 @@ int ATMOS_DYN_Tinteg_short_rk4_b200_dev(SCALE_HEVI_TINTEG_SHORT_ARGS)
     CK(need_setup());
     if (C.short_type == 1) CK(check_heve_fct(FLAG_FCT_MOMENTUM, FLAG_FCT_T));
     CK(check_bnd(BND_W, BND_E, BND_S, BND_N));
-    CK(check_flat(GSQRT, J13G, J23G, MAPF, true));
+    CK(use_metrics(GSQRT, J13G, J23G, MAPF, PHI, true));
     CK(prepare_tables(CDZ, FDZ, RCDZ, RFDZ, FDX, RCDX, RFDX, FDY, RCDY, RFDY, wdamp_coef, nullptr, nullptr));
     double *X[5] = {DENS, MOMZ, MOMX, MOMY, RHOT};
     StageIn base{nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
@@ -995,7 +1068,7 @@ int ATMOS_DYN_Tinteg_short_rk4_b200(SCALE_HEVI_TINTEG_SHORT_ARGS)
     CK(need_single("the host-array RK4 entry"));
     if (C.short_type == 1) CK(check_heve_fct(FLAG_FCT_MOMENTUM, FLAG_FCT_T));
     CK(check_bnd(BND_W, BND_E, BND_S, BND_N));
-    CK(check_flat(GSQRT, J13G, J23G, MAPF, false));
+    CK(use_metrics(GSQRT, J13G, J23G, MAPF, PHI, false));
     const size_t N3 = n3(), N2 = (size_t)C.g.IA * C.g.JA;
     double *hx[5] = {DENS, MOMZ, MOMX, MOMY, RHOT};
     const double *htt[5] = {DENS_t, MOMZ_t, MOMX_t, MOMY_t, RHOT_t};
@@ -1045,7 +1118,7 @@ int ATMOS_DYN_Tinteg_short_rk3_b200_dev(SCALE_HEVI_TINTEG_SHORT_ARGS)
     CK(rk3_type(&ws2002));
     if (C.short_type == 1) CK(check_heve_fct(FLAG_FCT_MOMENTUM, FLAG_FCT_T));
     CK(check_bnd(BND_W, BND_E, BND_S, BND_N));
-    CK(check_flat(GSQRT, J13G, J23G, MAPF, true));
+    CK(use_metrics(GSQRT, J13G, J23G, MAPF, PHI, true));
     CK(prepare_tables(CDZ, FDZ, RCDZ, RFDZ, FDX, RCDX, RFDX, FDY, RCDY, RFDY, wdamp_coef, nullptr, nullptr));
     double *X[5] = {DENS, MOMZ, MOMX, MOMY, RHOT};
     StageIn base{nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
@@ -1061,7 +1134,7 @@ int ATMOS_DYN_Tinteg_short_rk3_b200(SCALE_HEVI_TINTEG_SHORT_ARGS)
     CK(rk3_type(&ws2002));
     if (C.short_type == 1) CK(check_heve_fct(FLAG_FCT_MOMENTUM, FLAG_FCT_T));
     CK(check_bnd(BND_W, BND_E, BND_S, BND_N));
-    CK(check_flat(GSQRT, J13G, J23G, MAPF, false));
+    CK(use_metrics(GSQRT, J13G, J23G, MAPF, PHI, false));
     const size_t N3 = n3(), N2 = (size_t)C.g.IA * C.g.JA;
     double *hx[5] = {DENS, MOMZ, MOMX, MOMY, RHOT};
     const double *htt[5] = {DENS_t, MOMZ_t, MOMX_t, MOMY_t, RHOT_t};
@@ -1548,6 +1621,7 @@ static int ad_prepare()
 {
     CK(need_single("the differentiated short step"));
     if (!C.ad_ready) return fail(SCALE_HEVI_ERR_NOT_SETUP, "scale_hevi_adjoint_setup() has not been called");
+    C.terrain = false; // the differentiated model is the flat-terrain step
     const auto &v = C.ad_vec;
     CK(prepare_tables(v[0].data(), v[3].data(), v[6].data(), v[9].data(), v[4].data(), v[7].data(), v[10].data(),
                       v[5].data(), v[8].data(), v[11].data(), C.ad_wdamp.data(), nullptr, nullptr));

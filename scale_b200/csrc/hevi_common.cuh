@@ -7,11 +7,12 @@
 //
 // Arithmetic: FP64, compiled with --fmad=false, and each expression keeps the
 // Fortran evaluation order, so the plain path reproduces the reference's
-// IEEE-754 results operation by operation. Flat terrain is assumed by these
-// kernels (GSQRT = 1, J13G = J23G = 0, MAPF = 1; checked by the host before any
-// launch): the metric factors then multiply or divide by exactly 1 and the
-// J13/J23 flux terms are exact zeros, so dropping them leaves every non-zero
-// value unchanged.
+// IEEE-754 results operation by operation. Flat terrain is assumed by the
+// fused kernels (GSQRT = 1, J13G = J23G = 0, MAPF = 1; classified by the host
+// before any launch): the metric factors then multiply or divide by exactly 1
+// and the J13/J23 flux terms are exact zeros, so dropping them leaves every
+// non-zero value unchanged. Other metrics go to the general-metric stage
+// (terrain_stage in hevi_stage.cu), which keeps every metric term.
 #pragma once
 #include <cstddef>
 #include <cstdint>

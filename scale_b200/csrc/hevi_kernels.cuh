@@ -47,6 +47,22 @@ cudaError_t with_batch(const Grid &g, const Members &mem, NB nblocks_of, L launc
 struct Block2 { int x, y; };
 __device__ __forceinline__ Block2 split_block(int b, int gx) { return {b % gx, b / gx}; }
 
+// ---- the HEVI stage with terrain-following metrics (hevi_stage.cu) ----
+// GSQRT, J13G, J23G (KA,IA,JA,7), MAPF (IA,JA,2,4), PHI (KA,IA,JA): device arrays
+struct Metrics {
+    const double *GSQRT, *J13G, *J23G, *MAPF, *PHI;
+};
+// work arrays of one field each (KA,IA,JA), device memory
+struct TerrainWork {
+    double *POTT, *DPRES, *qZ, *qX, *qY, *qJ13, *qJ23, *Sr, *Sw, *St;
+    double *mZ, *mX, *mY, *tZ, *tX, *tY;
+    double *A, *PT, *F1, *F2, *F3, *C, *e, *f;
+};
+constexpr int TERRAIN_WORK_FIELDS = 24;
+constexpr int TERRAIN_STAGE_LAUNCHES = 24; // kernels of one general-metric stage
+cudaError_t launch_terrain_stage(const Grid &g, const StageArgsT<double> &a, const Metrics &M, const TerrainWork &W,
+                                 int scheme, cudaStream_t st);
+
 // ---- numerical filter (numfilter.cu) ----
 // coefficient tables built on the host (grid_coef.cpp), 0-based storage of
 // CNZ3(3,KA,2), CNX3(3,IA,2), CNY3(3,JA,2) and the nd_coef_* vectors

@@ -25,7 +25,8 @@
 // side and the Thomas solve stay FP64. Every FP64 operand is converted with
 // R(...) at its use, which is the identity for R = double.
 //
-// Flat terrain only (see hevi_common.cuh). Line numbers below refer to the
+// k_hevi_stage takes flat terrain (see hevi_common.cuh); the general-metric
+// stage at the end of this file takes any GSQRT/J13G/J23G/MAPF. Line numbers below refer to the
 // reference HEVI file unless a flux file is named.
 #include "hevi_kernels.cuh"
 
@@ -820,5 +821,535 @@ template cudaError_t launch_hevi_stage<double>(const Grid &, const Members &, co
                                                StageShape, cudaStream_t);
 template cudaError_t launch_hevi_stage<float>(const Grid &, const Members &, const StageArgsT<float> &, int,
                                               StageShape, cudaStream_t);
+
+// =============================================================================
+// The HEVI stage with terrain-following metrics (GSQRT, J13G, J23G) and map
+// factors (MAPF): ATMOS_DYN_Tstep_short_fvm_hevi (:128-1089) with every metric
+// term, each loop nest of the reference one launch over its own (i,j) range,
+// lanes along k, the intermediate fields in device work arrays. The flux
+// routines are those of scale_atmos_dyn_fvm_flux_ud3.F90 (and the other
+// scheme files), restated with their metric arguments. The outputs go through
+// put_state/put_flux, so the RK4/RK3 folds of the fused kernel apply unchanged.
+// FP64, one domain.
+// =============================================================================
+template <class F>
+__global__ void __launch_bounds__(128) k_gcols(int i0, int ni, int j0, int ncol, F f)
+{
+    const int col = blockIdx.x * 4 + threadIdx.y;
+    if (col >= ncol) return;
+    f(i0 + col % ni, j0 + col / ni, (int)threadIdx.x);
+}
+// f(i, j, lane) for every column of i0..i1 x j0..j1, one warp per column
+template <class F>
+static void gcols(int i0, int i1, int j0, int j1, cudaStream_t st, F f)
+{
+    const int ni = i1 - i0 + 1, ncol = ni * (j1 - j0 + 1);
+    if (ni <= 0 || ncol <= 0) return;
+    k_gcols<<<(ncol + 3) / 4, dim3(32, 4), 0, st>>>(i0, ni, j0, ncol, f);
+}
+
+// face value between p[0] and p[s] along a horizontal direction of stride s
+template <int S>
+__device__ __forceinline__ double hface(double vel, const double *p, long s)
+{
+    if constexpr (wide_scheme(S)) return ip6<S>(vel, p[-2 * s], p[-s], p[0], p[s], p[2 * s], p[3 * s]);
+    else return ip4<S>(vel, p[-s], p[0], p[s], p[2 * s]);
+}
+
+// staggering ids (scale_atmos_grid_cartesC_index.F90:90-101), variable ids and directions
+enum : int { I_XYZ = 1, I_XYW, I_UYW, I_XVW, I_UYZ, I_XVZ, I_UVZ };
+enum : int { I_XY = 1, I_UY, I_XV, I_UV };
+enum : int { V_DENS = 1, V_MOMZ, V_MOMX, V_MOMY, V_RHOT };
+enum : int { DZIR = 1, DXIR, DYIR };
+
+template <int S>
+static void terrain_stage(const Grid &g, const StageArgsT<double> &a, const Metrics &M, const TerrainWork &W,
+                          cudaStream_t st)
+{
+    const int KS = g.KS, KE = g.KE, IS = g.IS, IE = g.IE, JS = g.JS, JE = g.JE;
+    const int IEH = g.IEH < IE ? g.IEH : IE, JEH = g.JEH < JE ? g.JEH : JE;
+    const size_t N3 = n3(g);
+    const long sI = g.KA, sJ = (long)g.KA * g.IA;
+    const double dt = a.dtrk, J33G = a.J33G;
+    const bool use_div = a.divdmp_coef != 0.0;
+#define X3(k, i, j) idx3(g, k, i, j)
+#define GSs(idx) (M.GSQRT + (size_t)((idx) - 1) * N3)
+#define J13s(idx) (M.J13G + (size_t)((idx) - 1) * N3)
+#define J23s(idx) (M.J23G + (size_t)((idx) - 1) * N3)
+#define GS(k, i, j, idx) GSs(idx)[X3(k, i, j)]
+#define J13(k, i, j, idx) J13s(idx)[X3(k, i, j)]
+#define J23(k, i, j, idx) J23s(idx)[X3(k, i, j)]
+#define MAPFv(i, j, aa, bb) \
+    M.MAPF[(size_t)((i) - 1) + (size_t)g.IA * ((size_t)((j) - 1) + (size_t)g.JA * ((size_t)((aa) - 1) + 2 * (size_t)((bb) - 1)))]
+#define NDp(v, dir) (a.num_diff + N3 * (size_t)(((v) - 1) + 5 * ((dir) - 1)))
+#define CDZv(k) ld(g.CDZ + (k) - 1)
+    // F2H(k,p) of a GSQRT slice Gs (ud3.F90:75, tstep_short_fvm_hevi.F90:62)
+#define F2Hg(Gs, k, p) (CDZv((k) + (p) - 1) * (Gs)[X3((k) + (p) - 1, i, j)] \
+                        / (CDZv(k) * (Gs)[X3(k, i, j)] + CDZv((k) + 1) * (Gs)[X3((k) + 1, i, j)]))
+    const double *DN = a.DENS, *MZ = a.MOMZ, *MX = a.MOMX, *MY = a.MOMY;
+
+    // ---- hevi_pres :343-361 ----
+    gcols(IS, IE + 1, JS, JE + 1, st, [=] __device__(int i, int j, int lane) {
+        for (int k = KS + lane; k <= KE; k += 32) {
+            const size_t c = X3(k, i, j);
+            W.DPRES[c] = a.DPRES0[c] + a.RT2P[c] * (a.RHOT[c] - a.REF_rhot[c]);
+        }
+        if (lane == 0) {
+            W.DPRES[X3(KS - 1, i, j)] = a.DPRES0[X3(KS - 1, i, j)] - DN[X3(KS, i, j)] * (M.PHI[X3(KS - 1, i, j)] - M.PHI[X3(KS + 1, i, j)]);
+            W.DPRES[X3(KE + 1, i, j)] = a.DPRES0[X3(KE + 1, i, j)] - DN[X3(KE, i, j)] * (M.PHI[X3(KE + 1, i, j)] - M.PHI[X3(KE - 1, i, j)]);
+        }
+    });
+    // ---- hevi_mflx_z :365-397 (the halo column IS-1 is an output too) ----
+    gcols(IS - 1, IE, JS, JE, st, [=] __device__(int i, int j, int lane) {
+        const bool in = i >= IS;
+        for (int k = KS + lane; k <= KE - 1; k += 32) {
+            const size_t c = X3(k, i, j);
+            const double v = J13(k, i, j, I_XYW) * 0.25 / MAPFv(i, j, 2, I_XY)
+                                 * (MX[X3(k + 1, i, j)] + MX[X3(k + 1, i - 1, j)] + MX[c] + MX[X3(k, i - 1, j)])
+                             + J23(k, i, j, I_XYW) * 0.25 / MAPFv(i, j, 1, I_XY)
+                                 * (MY[X3(k + 1, i, j)] + MY[X3(k + 1, i, j - 1)] + MY[c] + MY[X3(k, i, j - 1)])
+                             + GS(k, i, j, I_XYW) / (MAPFv(i, j, 1, I_XY) * MAPFv(i, j, 2, I_XY)) * NDp(V_DENS, DZIR)[c];
+            W.mZ[c] = v;
+            if (!in) put_flux(a, N3, 0, c, v, false);
+        }
+        if (lane == 0) {
+            W.mZ[X3(KS - 1, i, j)] = 0.0;
+            W.mZ[X3(KE, i, j)] = 0.0;
+            if (!in) {
+                put_flux(a, N3, 0, X3(KS - 1, i, j), 0.0, false);
+                put_flux(a, N3, 0, X3(KE, i, j), 0.0, false);
+            }
+        }
+    });
+    // ---- hevi_mflx_x :399-421, hevi_mflx_y :423-438 ----
+    gcols(IS - 1, IEH, JS, JE, st, [=] __device__(int i, int j, int lane) {
+        for (int k = KS + lane; k <= KE; k += 32) {
+            const size_t c = X3(k, i, j);
+            const double v = GS(k, i, j, I_UYZ) / MAPFv(i, j, 2, I_UY) * (MX[c] + NDp(V_DENS, DXIR)[c]);
+            W.mX[c] = v;
+            put_flux(a, N3, 1, c, v, i >= IS);
+        }
+    });
+    gcols(IS, IE, JS - 1, JEH, st, [=] __device__(int i, int j, int lane) {
+        for (int k = KS + lane; k <= KE; k += 32) {
+            const size_t c = X3(k, i, j);
+            const double v = GS(k, i, j, I_XVZ) / MAPFv(i, j, 1, I_XV) * (MY[c] + NDp(V_DENS, DYIR)[c]);
+            W.mY[c] = v;
+            put_flux(a, N3, 2, c, v, j >= JS);
+        }
+    });
+    // ---- hevi_sr :443-479 ----
+    gcols(IS, IE, JS, JE, st, [=] __device__(int i, int j, int lane) {
+        for (int k = KS + lane; k <= KE; k += 32) {
+            const size_t c = X3(k, i, j);
+            const double advcv = -(W.mZ[c] - W.mZ[c - 1]) * ld(g.RCDZ + k - 1);
+            const double advch = -((W.mX[c] - W.mX[c - sI]) * ld(g.RCDX + i - 1) + (W.mY[c] - W.mY[c - sJ]) * ld(g.RCDY + j - 1));
+            W.Sr[c] = (advcv + advch) * MAPFv(i, j, 1, I_XY) * MAPFv(i, j, 2, I_XY) / GS(k, i, j, I_XYZ) + a.DENS_t[c];
+        }
+    });
+    // ---- momentum (z) fluxes :485-525 ----
+    // fluxZ_XYW (ud3.F90:358-452): flux(k-1) for k = KS+1..KE-1
+    gcols(IS, IE, JS, JE, st, [=] __device__(int i, int j, int lane) {
+        const double *Gs = GSs(I_XYZ), *nd = NDp(V_MOMZ, DZIR), *col = MZ + X3(1, i, j);
+        for (int k = KS + 1 + lane; k <= KE - 1; k += 32) {
+            const size_t c = X3(k, i, j);
+            const double vel = (0.5 * (MZ[c - 1] + MZ[c])) / DN[c];
+            W.qZ[c - 1] = J33G * vel * zface<S>(vel, k - 1, KS, KE, [&](int l) { return col[l - 1]; }) + Gs[c] * nd[c];
+        }
+        if (lane == 0) {
+            W.qZ[X3(KS - 1, i, j)] = 0.0;
+            W.qZ[X3(KE - 1, i, j)] = 0.0;
+            W.qZ[X3(KE, i, j)] = 0.0;
+        }
+    });
+    // fluxJ13_XYW (ud3.F90:457-523) and fluxJ23_XYW (:527-593)
+    gcols(IS, IE, JS, JE, st, [=] __device__(int i, int j, int lane) {
+        constexpr bool wide = wide_scheme(S);
+        const int kend = wide ? KE - 2 : KE - 1;
+        const double *J1 = J13s(I_XYZ), *J2 = J23s(I_XYZ);
+        const double m2 = MAPFv(i, j, 2, I_XY), m1 = MAPFv(i, j, 1, I_XY);
+        auto V = [&](int k) { return MZ[X3(k, i, j)]; };
+        auto face = [&](double vel, int k) {
+            if constexpr (wide) return ip6<S>(vel, V(k - 3), V(k - 2), V(k - 1), V(k), V(k + 1), V(k + 2));
+            else return ip4<S>(vel, V(k - 2), V(k - 1), V(k), V(k + 1));
+        };
+        for (int k = KS + 2 + lane; k <= kend; k += 32) {
+            const size_t c = X3(k, i, j);
+            double vel = (0.5 * (MX[c] + MX[c - sI])) / DN[c];
+            vel = vel * J1[c];
+            W.qJ13[c - 1] = vel / m2 * face(vel, k);
+            double vel2 = (0.5 * (MY[c] + MY[c - sJ])) / DN[c];
+            vel2 = vel2 * J2[c];
+            W.qJ23[c - 1] = vel2 / m1 * face(vel2, k);
+        }
+        if (lane == 0) {
+            W.qJ13[X3(KS - 1, i, j)] = 0.0;
+            W.qJ23[X3(KS - 1, i, j)] = 0.0;
+            const size_t c0 = X3(KS, i, j), c1 = X3(KS + 1, i, j);
+            double vel = ((0.5 * (MX[c1] + MX[c1 - sI])) / DN[c1] + (0.5 * (MX[c0] + MX[c0 - sI])) / DN[c0]) * 0.5;
+            vel = vel * J1[c1];
+            W.qJ13[c0] = vel / m2 * ipL<S>(vel, V(KS), V(KS + 1), V(KS + 2));
+            double vel2 = ((0.5 * (MY[c1] + MY[c1 - sJ])) / DN[c1] + (0.5 * (MY[c0] + MY[c0 - sJ])) / DN[c0]) * 0.5;
+            vel2 = vel2 * J2[c1];
+            W.qJ23[c0] = vel2 / m1 * ipL<S>(vel2, V(KS), V(KS + 1), V(KS + 2));
+            if constexpr (wide) {
+                const size_t ce = X3(KE - 1, i, j);
+                double ve = (0.5 * (MX[ce] + MX[ce - sI])) / DN[ce];
+                ve = ve * J1[ce];
+                W.qJ13[X3(KE - 2, i, j)] = ve / m2 * ipH<S>(ve, V(KE - 1), V(KE - 2), V(KE - 3));
+                double ve2 = (0.5 * (MY[ce] + MY[ce - sJ])) / DN[ce];
+                ve2 = ve2 * J2[ce];
+                W.qJ23[X3(KE - 2, i, j)] = ve2 / m1 * ipH<S>(ve2, V(KE - 1), V(KE - 2), V(KE - 3));
+            }
+            W.qJ13[X3(KE - 1, i, j)] = 0.0;
+            W.qJ23[X3(KE - 1, i, j)] = 0.0;
+        }
+    });
+    // fluxX_XYW (ud3.F90:598-671)
+    gcols(IS - 1, IE, JS, JE, st, [=] __device__(int i, int j, int lane) {
+        const double *Gs = GSs(I_UYW), *nd = NDp(V_MOMZ, DXIR);
+        const double mp = MAPFv(i, j, 2, I_UY);
+        for (int k = KS + lane; k <= KE - 1; k += 32) {
+            const size_t c = X3(k, i, j);
+            const double vel = (F2Hg(Gs, k, 1) * MX[c + 1] + F2Hg(Gs, k, 2) * MX[c])
+                               / (F2Hg(Gs, k, 1) * 0.5 * (DN[c + 1] + DN[c + 1 + sI]) + F2Hg(Gs, k, 2) * 0.5 * (DN[c] + DN[c + sI]));
+            W.qX[c] = Gs[c] / mp * vel * hface<S>(vel, MZ + c, sI) + Gs[c] * nd[c];
+        }
+        if (lane == 0) W.qX[X3(KE, i, j)] = 0.0;
+    });
+    // fluxY_XYW (ud3.F90:675-748)
+    gcols(IS, IE, JS - 1, JE, st, [=] __device__(int i, int j, int lane) {
+        const double *Gs = GSs(I_XVW), *nd = NDp(V_MOMZ, DYIR);
+        const double mp = MAPFv(i, j, 1, I_XV);
+        for (int k = KS + lane; k <= KE - 1; k += 32) {
+            const size_t c = X3(k, i, j);
+            const double vel = (F2Hg(Gs, k, 1) * MY[c + 1] + F2Hg(Gs, k, 2) * MY[c])
+                               / (F2Hg(Gs, k, 1) * 0.5 * (DN[c + 1] + DN[c + 1 + sJ]) + F2Hg(Gs, k, 2) * 0.5 * (DN[c] + DN[c + sJ]));
+            W.qY[c] = Gs[c] / mp * vel * hface<S>(vel, MZ + c, sJ) + Gs[c] * nd[c];
+        }
+        if (lane == 0) W.qY[X3(KE, i, j)] = 0.0;
+    });
+    // ---- hevi_sw :528-578 ----
+    gcols(IS, IE, JS, JE, st, [=] __device__(int i, int j, int lane) {
+        for (int k = KS + lane; k <= KE - 1; k += 32) {
+            const size_t c = X3(k, i, j);
+            const double advcv = -(W.qZ[c] - W.qZ[c - 1] + W.qJ13[c] - W.qJ13[c - 1] + W.qJ23[c] - W.qJ23[c - 1]) * ld(g.RFDZ + k - 1);
+            const double advch = -((W.qX[c] - W.qX[c - sI]) * ld(g.RCDX + i - 1) + (W.qY[c] - W.qY[c - sJ]) * ld(g.RCDY + j - 1))
+                                 * MAPFv(i, j, 1, I_XY) * MAPFv(i, j, 2, I_XY);
+            const double wdmp = -ld(a.wdamp + g.z0 + k - 1) * a.MOMZ0[c];
+            const double div = use_div ? a.divdmp_coef / dt * (a.DDIV[c + 1] - a.DDIV[c]) * ld(g.FDZ + k - 1) : 0.0;
+            W.Sw[c] = (advcv + advch) / GS(k, i, j, I_XYW) + wdmp + div + a.MOMZ_t[c];
+        }
+    });
+    // ---- POTT :586-598, over the halo too ----
+    gcols(IS - g.IHALO, IE + g.IHALO, JS - g.JHALO, JE + g.JHALO, st, [=] __device__(int i, int j, int lane) {
+        for (int k = KS + lane; k <= KE; k += 32) {
+            const size_t c = X3(k, i, j);
+            W.POTT[c] = a.RHOT[c] / DN[c];
+        }
+    });
+    // ---- theta fluxes :603-622: fluxZ_XYZ (ud3.F90:157-247) ----
+    gcols(IS, IE, JS, JE, st, [=] __device__(int i, int j, int lane) {
+        const double *Gs = GSs(I_XYW), *nd = NDp(V_RHOT, DZIR), *col = W.POTT + X3(1, i, j);
+        for (int k = KS + lane; k <= KE - 1; k += 32) {
+            const size_t c = X3(k, i, j);
+            const double vel = W.mZ[c];
+            W.tZ[c] = vel * zface<S>(vel, k, KS, KE, [&](int l) { return col[l - 1]; }) + Gs[c] * nd[c];
+        }
+        if (lane == 0) {
+            W.tZ[X3(KS - 1, i, j)] = 0.0;
+            W.tZ[X3(KE, i, j)] = 0.0;
+        }
+    });
+    // fluxX_XYZ (:251-300), fluxY_XYZ (:304-353)
+    gcols(IS - 1, IE, JS, JE, st, [=] __device__(int i, int j, int lane) {
+        const double *Gs = GSs(I_UYZ), *nd = NDp(V_RHOT, DXIR);
+        for (int k = KS + lane; k <= KE; k += 32) {
+            const size_t c = X3(k, i, j);
+            const double vel = W.mX[c];
+            const double v = vel * hface<S>(vel, W.POTT + c, sI) + Gs[c] * nd[c];
+            W.tX[c] = v;
+            put_flux(a, N3, 4, c, v, i >= IS);
+        }
+    });
+    gcols(IS, IE, JS - 1, JE, st, [=] __device__(int i, int j, int lane) {
+        const double *Gs = GSs(I_XVZ), *nd = NDp(V_RHOT, DYIR);
+        for (int k = KS + lane; k <= KE; k += 32) {
+            const size_t c = X3(k, i, j);
+            const double vel = W.mY[c];
+            const double v = vel * hface<S>(vel, W.POTT + c, sJ) + Gs[c] * nd[c];
+            W.tY[c] = v;
+            put_flux(a, N3, 5, c, v, j >= JS);
+        }
+    });
+    // ---- hevi_st :625-661 ----
+    gcols(IS, IE, JS, JE, st, [=] __device__(int i, int j, int lane) {
+        for (int k = KS + lane; k <= KE; k += 32) {
+            const size_t c = X3(k, i, j);
+            const double advcv = -(W.tZ[c] - W.tZ[c - 1]) * ld(g.RCDZ + k - 1);
+            const double advch = -((W.tX[c] - W.tX[c - sI]) * ld(g.RCDX + i - 1) + (W.tY[c] - W.tY[c - sJ]) * ld(g.RCDY + j - 1));
+            W.St[c] = (advcv + advch) * MAPFv(i, j, 1, I_XY) * MAPFv(i, j, 2, I_XY) / GS(k, i, j, I_XYZ) + a.RHOT_t[c];
+        }
+    });
+    // ---- hevi_solver :665-809 (solve_direct :1092-1127), one warp per column ----
+    gcols(IS, IE, JS, JE, st, [=] __device__(int i, int j, int lane) {
+        const double *GW = GSs(I_XYW), *GZ = GSs(I_XYZ);
+        const double *col_mz = MZ + X3(1, i, j), *col_pt = W.POTT + X3(1, i, j);
+        const size_t c1 = X3(1, i, j);
+        double *A = W.A + c1 - 1, *PT = W.PT + c1 - 1, *F1 = W.F1 + c1 - 1, *F2 = W.F2 + c1 - 1, *F3 = W.F3 + c1 - 1;
+        double *C = W.C + c1 - 1, *e = W.e + c1 - 1, *f = W.f + c1 - 1; // 1-based level index
+        for (int k = KS + lane; k <= KE; k += 32) {
+            if (k <= KE - 1) PT[k] = zface<S>(col_mz[k - 1], k, KS, KE, [&](int l) { return col_pt[l - 1]; }); // valueW_Z
+            A[k] = dt * dt * J33G * ld(g.RCDZ + k - 1) * a.RT2P[c1 + k - 1] * J33G / GZ[c1 + k - 1];
+        }
+        __syncwarp();
+        for (int k = KS + lane; k <= KE - 1; k += 32) {
+            const double B = GRAV * (dt * dt) * J33G / (CDZv(k + 1) + CDZv(k));
+            const double rfdz = ld(g.RFDZ + k - 1), gw = GW[c1 + k - 1];
+            if (k <= KE - 2) F1[k] = -(PT[k + 1] * rfdz * A[k + 1] + B) / gw;
+            F2[k] = 1.0 + (PT[k] * rfdz * (A[k + 1] + A[k])) / gw;
+            if (k >= KS + 1) F3[k] = -(PT[k - 1] * rfdz * A[k] - B) / gw;
+            const size_t c = c1 + k - 1;
+            const double pg = -(W.DPRES[c + 1] + a.RT2P[c + 1] * dt * W.St[c + 1] - W.DPRES[c] - a.RT2P[c] * dt * W.St[c])
+                                  * rfdz * J33G / gw
+                              - GRAV * (F2Hg(GZ, k, 1) * (DN[c + 1] - a.REF_dens[c + 1] + W.Sr[c + 1] * dt)
+                                        + F2Hg(GZ, k, 2) * (DN[c] - a.REF_dens[c] + W.Sr[c] * dt));
+            C[k] = MZ[c] + dt * (pg + W.Sw[c]);
+        }
+        __syncwarp();
+        if (lane == 0) {
+            double rdenom = 1.0 / F2[KS];
+            e[KS] = -F1[KS] * rdenom;
+            f[KS] = C[KS] * rdenom;
+            for (int k = KS + 1; k <= KE - 2; ++k) {
+                rdenom = 1.0 / (F2[k] + F3[k] * e[k - 1]);
+                e[k] = -F1[k] * rdenom;
+                f[k] = (C[k] - F3[k] * f[k - 1]) * rdenom;
+            }
+            C[KE - 1] = (C[KE - 1] - F3[KE - 1] * f[KE - 2]) / (F2[KE - 1] + F3[KE - 1] * e[KE - 2]);
+            for (int k = KE - 2; k >= KS; --k) C[k] = e[k] * C[k + 1] + f[k];
+        }
+        __syncwarp();
+        const double mm = MAPFv(i, j, 1, I_XY) * MAPFv(i, j, 2, I_XY);
+        for (int k = KS + lane; k <= KE; k += 32) {
+            const size_t c = c1 + k - 1;
+            const double rcdz = ld(g.RCDZ + k - 1), gz = GZ[c];
+            double adr, adt;
+            if (k == KS) {
+                adr = -C[KS] * J33G * rcdz / gz;
+                adt = -C[KS] * PT[KS] * J33G * rcdz / gz;
+            } else if (k == KE) {
+                adr = C[KE - 1] * J33G * rcdz / gz;
+                adt = C[KE - 1] * PT[KE - 1] * J33G * rcdz / gz;
+            } else {
+                adr = -(C[k] - C[k - 1]) * J33G * rcdz / gz;
+                adt = -(C[k] * PT[k] - C[k - 1] * PT[k - 1]) * J33G * rcdz / gz;
+            }
+            put_state(a, N3, 0, a.DENS_RK, a.DENS0, c, a.DENS0[c] + dt * (adr + W.Sr[c]), true);
+            put_state(a, N3, 4, a.RHOT_RK, a.RHOT0, c, a.RHOT0[c] + dt * (adt + W.St[c]), true);
+            if (k <= KE - 1) {
+                put_flux(a, N3, 0, c, W.mZ[c] + J33G * C[k] / mm, true);
+                put_flux(a, N3, 3, c, W.tZ[c] + J33G * C[k] * PT[k] / mm, true);
+                put_state(a, N3, 1, a.MOMZ_RK, a.MOMZ0, c, a.MOMZ0[c] + (C[k] - MZ[c]), true);
+            } else {
+                put_flux(a, N3, 0, c, 0.0, true);
+                put_flux(a, N3, 3, c, 0.0, true);
+                put_state(a, N3, 1, a.MOMZ_RK, a.MOMZ0, c, 0.0, false);
+            }
+        }
+        if (lane == 0) {
+            put_state(a, N3, 1, a.MOMZ_RK, a.MOMZ0, c1 + KS - 2, 0.0, false);
+            put_flux(a, N3, 0, c1 + KS - 2, 0.0, false);
+            put_flux(a, N3, 3, c1 + KS - 2, 0.0, false);
+        }
+    });
+
+    // ---- hevi_momx :814-928 ----
+#define DEN_UYZ(Gs, k) (F2Hg(Gs, k, 1) * 0.5 * (DN[X3((k) + 1, i, j)] + DN[X3((k) + 1, i + 1, j)]) \
+                        + F2Hg(Gs, k, 2) * 0.5 * (DN[X3(k, i, j)] + DN[X3(k, i + 1, j)]))
+#define DEN_XVZ(Gs, k) (F2Hg(Gs, k, 1) * 0.5 * (DN[X3((k) + 1, i, j)] + DN[X3((k) + 1, i, j + 1)]) \
+                        + F2Hg(Gs, k, 2) * 0.5 * (DN[X3(k, i, j)] + DN[X3(k, i, j + 1)]))
+#define AVG4_UV(m, k) (0.25 * ((m)[X3(k, i, j)] + (m)[X3(k, i + 1, j)] + (m)[X3(k, i, j - 1)] + (m)[X3(k, i + 1, j - 1)]))
+#define AVG4_XV(m, k) (0.25 * ((m)[X3(k, i, j)] + (m)[X3(k, i - 1, j)] + (m)[X3(k, i, j + 1)] + (m)[X3(k, i - 1, j + 1)]))
+    // fluxZ_UYZ (ud3.F90:753-859), fluxJ13_UYZ (:863-954), fluxJ23_UYZ (:958-1049)
+    gcols(IS, IE, JS, JE, st, [=] __device__(int i, int j, int lane) {
+        const double *Gw = GSs(I_UYW), *Gz = GSs(I_UYZ), *J1 = J13s(I_UYW), *J2 = J23s(I_UYW), *nd = NDp(V_MOMX, DZIR);
+        const double *col = MX + X3(1, i, j);
+        auto V = [&](int l) { return col[l - 1]; };
+        const double m2 = MAPFv(i, j, 2, I_UY), m1 = MAPFv(i, j, 1, I_UY);
+        for (int k = KS + lane; k <= KE - 1; k += 32) {
+            const size_t c = X3(k, i, j);
+            const double vel = (0.5 * (MZ[c] + MZ[c + sI])) / DEN_UYZ(Gw, k);
+            W.qZ[c] = J33G * vel * zface<S>(vel, k, KS, KE, V) + Gw[c] * nd[c];
+            double v1 = (F2Hg(Gz, k, 1) * MX[c + 1] + F2Hg(Gz, k, 2) * MX[c]) / DEN_UYZ(Gz, k);
+            v1 = v1 * J1[c];
+            W.qJ13[c] = v1 / m2 * zface<S>(v1, k, KS, KE, V);
+            double v2 = (F2Hg(Gz, k, 1) * AVG4_UV(MY, k + 1) + F2Hg(Gz, k, 2) * AVG4_UV(MY, k)) / DEN_UYZ(Gz, k);
+            v2 = v2 * J2[c];
+            W.qJ23[c] = v2 / m1 * zface<S>(v2, k, KS, KE, V);
+        }
+        if (lane == 0) {
+            W.qZ[X3(KS - 1, i, j)] = 0.0; W.qZ[X3(KE, i, j)] = 0.0;
+            W.qJ13[X3(KS - 1, i, j)] = 0.0; W.qJ13[X3(KE, i, j)] = 0.0;
+            W.qJ23[X3(KS - 1, i, j)] = 0.0; W.qJ23[X3(KE, i, j)] = 0.0;
+        }
+    });
+    // fluxX_UYZ (ud3.F90:1053-1109): flux(k,i-1) for i = IS..IE+1
+    gcols(IS, IE + 1, JS, JE, st, [=] __device__(int i, int j, int lane) {
+        const double *Gs = GSs(I_XYZ), *nd = NDp(V_MOMX, DXIR);
+        const double mp = MAPFv(i, j, 2, I_XY);
+        for (int k = KS + lane; k <= KE; k += 32) {
+            const size_t c = X3(k, i, j);
+            const double vel = (0.5 * (MX[c] + MX[c - sI])) / (DN[c]);
+            W.qX[c - sI] = Gs[c] / mp * vel * hface<S>(vel, MX + c - sI, sI) + Gs[c] * nd[c];
+        }
+    });
+    // fluxY_UYZ (:1113-1167)
+    gcols(IS, IE, JS - 1, JE, st, [=] __device__(int i, int j, int lane) {
+        const double *Gs = GSs(I_UVZ), *nd = NDp(V_MOMX, DYIR);
+        const double mp = MAPFv(i, j, 1, I_UV);
+        for (int k = KS + lane; k <= KE; k += 32) {
+            const size_t c = X3(k, i, j);
+            const double vel = (0.5 * (MY[c] + MY[c + sI])) / (0.25 * (DN[c] + DN[c + sI] + DN[c + sJ] + DN[c + sI + sJ]));
+            W.qY[c] = Gs[c] / mp * vel * hface<S>(vel, MX + c, sJ) + Gs[c] * nd[c];
+        }
+    });
+    gcols(IS, IEH, JS, JE, st, [=] __device__(int i, int j, int lane) {
+        const double *GZ = GSs(I_XYZ), *GUZ = GSs(I_UYZ);
+        for (int k = KS + lane; k <= KE; k += 32) {
+            const size_t c = X3(k, i, j);
+            const double *DP = W.DPRES;
+            const double advcv = -(W.qZ[c] - W.qZ[c - 1] + W.qJ13[c] - W.qJ13[c - 1] + W.qJ23[c] - W.qJ23[c - 1]) * ld(g.RCDZ + k - 1);
+            const double advch = -((W.qX[c] - W.qX[c - sI]) * ld(g.RFDX + i - 1) + (W.qY[c] - W.qY[c - sJ]) * ld(g.RCDY + j - 1))
+                                 * MAPFv(i, j, 1, I_UY) * MAPFv(i, j, 2, I_UY);
+            const double *Gu = GUZ;
+            const double pg = ((GZ[c + sI] * DP[c + sI] - GZ[c] * DP[c]) * ld(g.RFDX + i - 1)
+                               + (J13(k, i, j, I_UYW)
+                                      * 0.5 * (F2Hg(Gu, k, 1) * (DP[c + 1 + sI] + DP[c + 1]) + F2Hg(Gu, k, 2) * (DP[c + sI] + DP[c]))
+                                  - J13(k - 1, i, j, I_UYW)
+                                      * 0.5 * (F2Hg(Gu, k, 1) * (DP[c + sI] + DP[c]) + F2Hg(Gu, k, 2) * (DP[c - 1 + sI] + DP[c - 1])))
+                                     * ld(g.RCDZ + k - 1))
+                              * MAPFv(i, j, 1, I_UY);
+            const double sumy = MY[c] + MY[c - sJ] + MY[c + sI] + MY[c + sI - sJ];
+            const double cf = 0.125 * (a.CORIOLI[g.c2 + (size_t)i + (size_t)g.IA * (j - 1)] + a.CORIOLI[g.c2 + (size_t)(i - 1) + (size_t)g.IA * (j - 1)])
+                                  * (MY[c + sI] + MY[c] + MY[c + sI - sJ] + MY[c - sJ])
+                              + 0.25 * MAPFv(i, j, 1, I_UY) * MAPFv(i, j, 2, I_UY) * sumy
+                                  * (sumy * 0.25 * (1.0 / MAPFv(i + 1, j, 2, I_XY) - 1.0 / MAPFv(i, j, 2, I_XY)) * ld(g.RFDX + i - 1)
+                                     - MX[c] * (1.0 / MAPFv(i, j, 1, I_UV) - 1.0 / MAPFv(i, j - 1, 1, I_UV)) * ld(g.RCDY + j - 1))
+                                  * 2.0 / (DN[c + sI] + DN[c]);
+            const double div = use_div ? a.divdmp_coef / dt * (a.DDIV[c + sI] / MAPFv(i + 1, j, 2, I_XY) - a.DDIV[c] / MAPFv(i, j, 1, I_XY))
+                                             * MAPFv(i, j, 1, I_UY) * MAPFv(i, j, 2, I_UY) * ld(g.FDX + i - 1)
+                                       : 0.0;
+            put_state(a, N3, 2, a.MOMX_RK, a.MOMX0, c,
+                      a.MOMX0[c] + dt * ((advcv + advch - pg) / GUZ[c] + cf + div + a.MOMX_t[c]), true);
+        }
+    });
+
+    // ---- hevi_momy :934-1048 ----
+    // fluxZ_XVZ (ud3.F90:1173-1279), fluxJ13_XVZ (:1283-1374), fluxJ23_XVZ (:1378-1469)
+    gcols(IS, IE, JS, JE, st, [=] __device__(int i, int j, int lane) {
+        const double *Gw = GSs(I_XVW), *Gz = GSs(I_XVZ), *J1 = J13s(I_XVW), *J2 = J23s(I_XVW), *nd = NDp(V_MOMY, DZIR);
+        const double *col = MY + X3(1, i, j);
+        auto V = [&](int l) { return col[l - 1]; };
+        const double m2 = MAPFv(i, j, 2, I_XV), m1 = MAPFv(i, j, 1, I_XV);
+        for (int k = KS + lane; k <= KE - 1; k += 32) {
+            const size_t c = X3(k, i, j);
+            const double vel = (0.5 * (MZ[c] + MZ[c + sJ])) / DEN_XVZ(Gw, k);
+            W.qZ[c] = J33G * vel * zface<S>(vel, k, KS, KE, V) + Gw[c] * nd[c];
+            double v1 = (F2Hg(Gz, k, 1) * AVG4_XV(MX, k + 1) + F2Hg(Gz, k, 2) * AVG4_XV(MX, k)) / DEN_XVZ(Gz, k);
+            v1 = v1 * J1[c];
+            W.qJ13[c] = v1 / m2 * zface<S>(v1, k, KS, KE, V);
+            double v2 = (F2Hg(Gz, k, 1) * MY[c + 1] + F2Hg(Gz, k, 2) * MY[c]) / DEN_XVZ(Gz, k);
+            v2 = v2 * J2[c];
+            W.qJ23[c] = v2 / m1 * zface<S>(v2, k, KS, KE, V);
+        }
+        if (lane == 0) {
+            W.qZ[X3(KS - 1, i, j)] = 0.0; W.qZ[X3(KE, i, j)] = 0.0;
+            W.qJ13[X3(KS - 1, i, j)] = 0.0; W.qJ13[X3(KE, i, j)] = 0.0;
+            W.qJ23[X3(KS - 1, i, j)] = 0.0; W.qJ23[X3(KE, i, j)] = 0.0;
+        }
+    });
+    // fluxX_XVZ (:1473-1527)
+    gcols(IS - 1, IE, JS, JE, st, [=] __device__(int i, int j, int lane) {
+        const double *Gs = GSs(I_UVZ), *nd = NDp(V_MOMY, DXIR);
+        const double mp = MAPFv(i, j, 2, I_UV);
+        for (int k = KS + lane; k <= KE; k += 32) {
+            const size_t c = X3(k, i, j);
+            const double vel = (0.5 * (MX[c] + MX[c + sJ])) / (0.25 * (DN[c] + DN[c + sI] + DN[c + sJ] + DN[c + sI + sJ]));
+            W.qX[c] = Gs[c] / mp * vel * hface<S>(vel, MY + c, sI) + Gs[c] * nd[c];
+        }
+    });
+    // fluxY_XVZ (:1531-1587): flux(k,i,j-1) for j = JS..JE+1
+    gcols(IS, IE, JS, JE + 1, st, [=] __device__(int i, int j, int lane) {
+        const double *Gs = GSs(I_XYZ), *nd = NDp(V_MOMY, DYIR);
+        const double mp = MAPFv(i, j, 1, I_XY);
+        for (int k = KS + lane; k <= KE; k += 32) {
+            const size_t c = X3(k, i, j);
+            const double vel = (0.5 * (MY[c] + MY[c - sJ])) / (DN[c]);
+            W.qY[c - sJ] = Gs[c] / mp * vel * hface<S>(vel, MY + c - sJ, sJ) + Gs[c] * nd[c];
+        }
+    });
+    gcols(IS, IE, JS, JEH, st, [=] __device__(int i, int j, int lane) {
+        const double *GZ = GSs(I_XYZ), *GVZ = GSs(I_XVZ);
+        for (int k = KS + lane; k <= KE; k += 32) {
+            const size_t c = X3(k, i, j);
+            const double *DP = W.DPRES;
+            const double advcv = -(W.qZ[c] - W.qZ[c - 1] + W.qJ13[c] - W.qJ13[c - 1] + W.qJ23[c] - W.qJ23[c - 1]) * ld(g.RCDZ + k - 1);
+            const double advch = -((W.qX[c] - W.qX[c - sI]) * ld(g.RCDX + i - 1) + (W.qY[c] - W.qY[c - sJ]) * ld(g.RFDY + j - 1))
+                                 * MAPFv(i, j, 1, I_XV) * MAPFv(i, j, 2, I_XV);
+            const double *Gv = GVZ;
+            const double pg = ((GZ[c + sJ] * DP[c + sJ] - GZ[c] * DP[c]) * ld(g.RFDY + j - 1)
+                               + (J23(k, i, j, I_XVW)
+                                      * 0.5 * (F2Hg(Gv, k, 1) * (DP[c + 1 + sJ] + DP[c + 1]) + F2Hg(Gv, k, 2) * (DP[c + sJ] + DP[c]))
+                                  - J23(k - 1, i, j, I_XVW)
+                                      * 0.5 * (F2Hg(Gv, k - 1, 1) * (DP[c + sJ] + DP[c]) + F2Hg(Gv, k - 1, 2) * (DP[c - 1 + sJ] + DP[c - 1])))
+                                     * ld(g.RCDZ + k - 1))
+                              * MAPFv(i, j, 2, I_XV);
+            const double sumx = MX[c] + MX[c - sI] + MX[c + sJ] + MX[c - sI + sJ];
+            const double cf = -0.125 * (a.CORIOLI[g.c2 + (size_t)(i - 1) + (size_t)g.IA * j] + a.CORIOLI[g.c2 + (size_t)(i - 1) + (size_t)g.IA * (j - 1)])
+                                  * (MX[c + sJ] + MX[c] + MX[c - sI + sJ] + MX[c - sI])
+                              - 0.25 * MAPFv(i, j, 1, I_XV) * MAPFv(i, j, 2, I_XV) * sumx
+                                  * (MY[c] * (1.0 / MAPFv(i, j, 2, I_UV) - 1.0 / MAPFv(i - 1, j, 2, I_UV)) * ld(g.RCDX + i - 1)
+                                     - 0.25 * (MX[c] + MX[c - sI] + MX[c + sJ] + MX[c - sI + sJ])
+                                           * (1.0 / MAPFv(i, j + 1, 1, I_XY) - 1.0 / MAPFv(i, j, 1, I_XY)) * ld(g.RFDY + j - 1))
+                                  * 2.0 / (DN[c + sJ] + DN[c]);
+            const double div = use_div ? a.divdmp_coef / dt * (a.DDIV[c + sJ] / MAPFv(i, j + 1, 1, I_XY) - a.DDIV[c] / MAPFv(i, j, 1, I_XY))
+                                             * MAPFv(i, j, 1, I_XV) * MAPFv(i, j, 2, I_XV) * ld(g.FDY + j - 1)
+                                       : 0.0;
+            put_state(a, N3, 3, a.MOMY_RK, a.MOMY0, c,
+                      a.MOMY0[c] + dt * ((advcv + advch - pg) / GVZ[c] + cf + div + a.MOMY_t[c]), true);
+        }
+    });
+#undef X3
+#undef GSs
+#undef J13s
+#undef J23s
+#undef GS
+#undef J13
+#undef J23
+#undef MAPFv
+#undef NDp
+#undef CDZv
+#undef F2Hg
+#undef DEN_UYZ
+#undef DEN_XVZ
+#undef AVG4_UV
+#undef AVG4_XV
+}
+
+cudaError_t launch_terrain_stage(const Grid &g, const StageArgsT<double> &a, const Metrics &M, const TerrainWork &W,
+                                 int scheme, cudaStream_t st)
+{
+    switch (scheme) {
+    case UD3: terrain_stage<UD3>(g, a, M, W, st); break;
+    case CD4: terrain_stage<CD4>(g, a, M, W, st); break;
+    case KOREN: terrain_stage<KOREN>(g, a, M, W, st); break;
+    case CD2: terrain_stage<CD2>(g, a, M, W, st); break;
+    case UD5: terrain_stage<UD5>(g, a, M, W, st); break;
+    case CD6: terrain_stage<CD6>(g, a, M, W, st); break;
+    default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
 
 }  // namespace hevi

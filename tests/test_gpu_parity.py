@@ -313,15 +313,23 @@ def test_mass_conserved_on_device(lib):
     assert abs(m1 - m0) / m0 < 1e-13, (m0, m1)
 
 
-def test_unsupported_terrain_is_rejected(lib):
+def test_single_terrain_point_takes_the_metric_stage(lib):
+    # one GSQRT value off 1 is terrain: the HEVI stage runs the general-metric
+    # kernels (bit-exact with the oracle), the HEVE stage refuses it
     g = helpers.small_grid()
     c = helpers.small_case(g)
     a = helpers.short_inputs(c, full=False)
     a["GSQRT"] = a["GSQRT"].copy(order="F")
     a["GSQRT"][3, 4, 5, 0] = 1.01
+    o_ref = helpers.stage_outputs(g)
+    oracle.tstep_short(g, "UD3", o_ref, a)
+    o_gpu = helpers.stage_outputs(g)
     lib.setup(g.index_dict(), "UD3", "UD3")
+    lib.ATMOS_DYN_Tstep_short_fvm_hevi(**_stage_call_args(a, o_gpu))
+    for n in o_ref:
+        assert helpers.same(o_gpu[n], o_ref[n]), n
     with pytest.raises(hevi.HeviError) as e:
-        lib.ATMOS_DYN_Tstep_short_fvm_hevi(**_stage_call_args(a, helpers.stage_outputs(g)))
+        lib.ATMOS_DYN_Tstep_short_fvm_heve(**_stage_call_args(a, helpers.stage_outputs(g)))
     assert e.value.code == 5
 
 

@@ -1,0 +1,135 @@
+"""The HEVI short step with terrain-following metrics: non-flat GSQRT, J13G,
+J23G and map factors MAPF (scale_atmos_dyn_tstep_short_fvm_hevi.F90:128-1089
+with every metric term, and the flux routines' GSQRT/J13G/J23G/MAPF
+arguments), against the oracle's restatement, bit for bit: one stage for
+every flux scheme, the RK4 and RK3 short steps, the device entry against the
+host entry; and the entries that take flat terrain only refuse it."""
+import numpy as np
+import pytest
+
+import helpers
+import oracle
+from scale_b200 import hevi
+
+pytestmark = pytest.mark.gpu
+
+STATE = ("DENS", "MOMZ", "MOMX", "MOMY", "RHOT")
+SCHEMES = ["UD3", "CD4", "UD3KOREN1993", "CD2", "UD5", "CD6"]
+SHORT_KW = dict(PROG=None, FLAG_FCT_MOMENTUM=False, FLAG_FCT_T=False, FLAG_FCT_ALONG_STREAM=True,
+                BND_W=False, BND_E=False, BND_S=False, BND_N=False)
+
+
+@pytest.fixture
+def lib(gpu):
+    yield hevi
+    hevi.finalize()
+
+
+def with_terrain(a, g, seed=17, amp=0.05):
+    """Seeded non-flat metrics: GSQRT and MAPF within amp of 1, J13G and J23G
+    within amp of 0, at every point and staggering."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    a = dict(a)
+    a["GSQRT"] = np.asfortranarray(1.0 + amp * rng.uniform(-1, 1, size=g.shape + (7,)))
+    a["J13G"] = np.asfortranarray(amp * rng.uniform(-1, 1, size=g.shape + (7,)))
+    a["J23G"] = np.asfortranarray(amp * rng.uniform(-1, 1, size=g.shape + (7,)))
+    a["MAPF"] = np.asfortranarray(1.0 + amp * rng.uniform(-1, 1, size=(g.IA, g.JA, 2, 4)))
+    return a
+
+
+def _stage_kw(a, o):
+    kw = dict(a)
+    kw.update(o)
+    kw.update(PROG_RK=None, PROG0=None, PROG=None, FLAG_FCT_MOMENTUM=False, FLAG_FCT_T=False,
+              FLAG_FCT_ALONG_STREAM=True, BND_W=False, BND_E=False, BND_S=False, BND_N=False, last=False)
+    return kw
+
+
+@pytest.mark.parametrize("scheme", SCHEMES)
+@pytest.mark.parametrize("stretched", [False, True])
+@pytest.mark.parametrize("full", [False, True])
+def test_terrain_stage_bit_exact(lib, scheme, stretched, full):
+    g = helpers.small_grid(IMAX=13, JMAX=9, KMAX=17, stretched=stretched, halo=helpers.halo_of(scheme))
+    c = helpers.small_case(g, scheme)
+    helpers.perturb_state(c)
+    a = with_terrain(helpers.short_inputs(c, dtrk=0.5, full=full), g)
+    o_ref = helpers.stage_outputs(g)
+    oracle.tstep_short(g, scheme, o_ref, a)
+    o_gpu = helpers.stage_outputs(g)
+    lib.setup(g.index_dict(), scheme, scheme)
+    lib.ATMOS_DYN_Tstep_short_fvm_hevi(**_stage_kw(a, o_gpu))
+    for n in o_ref:
+        assert helpers.same(o_gpu[n], o_ref[n]), f"{n}: max rel diff {helpers.max_rel(o_gpu[n], o_ref[n]):.3e}"
+
+
+def test_terrain_device_entry_matches_host_entry(lib):
+    import torch
+
+    g = helpers.small_grid(IMAX=16, JMAX=12, KMAX=20, stretched=True)
+    c = helpers.small_case(g, "CD4")
+    helpers.perturb_state(c)
+    a = with_terrain(helpers.short_inputs(c, full=True), g)
+    o_host = helpers.stage_outputs(g, 0.0)
+    lib.setup(g.index_dict(), "CD4", "CD4")
+    lib.ATMOS_DYN_Tstep_short_fvm_hevi(**_stage_kw(a, o_host))
+
+    def dev(x):
+        return torch.from_numpy(np.ravel(x, order="K").copy()).cuda() if isinstance(x, np.ndarray) and x.ndim >= 2 else x
+
+    ad = {k: dev(v) for k, v in a.items()}
+    od = {k: torch.zeros(v.size, dtype=torch.float64, device="cuda") for k, v in o_host.items()}
+    lib.ATMOS_DYN_Tstep_short_fvm_hevi_dev(**_stage_kw(ad, od))
+    lib.check()
+    for n, v in o_host.items():
+        got = od[n].cpu().numpy().reshape(v.shape, order="F")
+        assert np.array_equal(got, v), n
+
+
+def _short_inputs(g, scheme):
+    c = helpers.small_case(g, scheme)
+    helpers.perturb_state(c)
+    a = with_terrain(helpers.short_inputs(c, full=True), g)
+    for k in ("DENS0", "MOMZ0", "MOMX0", "MOMY0", "RHOT0", "DENS", "MOMZ", "MOMX", "MOMY", "RHOT", "dtrk"):
+        a.pop(k)
+    xs = {n: c.state[n].copy(order="F") for n in STATE}
+    xs["mflx_hi"] = np.full(g.shape + (3,), 7.0, order="F")
+    xs["tflx_hi"] = np.full(g.shape + (3,), 7.0, order="F")
+    return a, xs
+
+
+@pytest.mark.parametrize("scheme", ["UD3", "CD4", "UD5"])
+def test_terrain_rk4_bit_exact(lib, scheme):
+    g = helpers.small_grid(IMAX=14, JMAX=11, KMAX=18, stretched=True, halo=helpers.halo_of(scheme))
+    a, xs = _short_inputs(g, scheme)
+    xg = {n: v.copy(order="F") for n, v in xs.items()}
+    oracle.tinteg_short_rk4(g, scheme, xs, dict(a, dt=0.5))
+    lib.setup(g.index_dict(), scheme, scheme)
+    lib.ATMOS_DYN_Tinteg_short_rk4(**a, **xg, **SHORT_KW, dt=0.5)
+    for n in xs:
+        assert helpers.same(xg[n], xs[n]), f"{n}: max rel diff {helpers.max_rel(xg[n], xs[n]):.3e}"
+
+
+@pytest.mark.parametrize("tinteg", ["RK3", "RK3WS2002"])
+def test_terrain_rk3_bit_exact(lib, tinteg):
+    g = helpers.small_grid(IMAX=14, JMAX=11, KMAX=18, stretched=True)
+    a, xs = _short_inputs(g, "CD4")
+    xg = {n: v.copy(order="F") for n, v in xs.items()}
+    oracle.tinteg_short_rk3(g, "CD4", xs, dict(a, dt=0.5), ws2002=tinteg == "RK3WS2002")
+    lib.setup(g.index_dict(), "CD4", "CD4")
+    lib.tinteg_short_type(tinteg)
+    lib.ATMOS_DYN_Tinteg_short_rk3(**a, **xg, **SHORT_KW, dt=0.5)
+    for n in xs:
+        assert helpers.same(xg[n], xs[n]), f"{n}: max rel diff {helpers.max_rel(xg[n], xs[n]):.3e}"
+
+
+def test_flat_only_entries_refuse_terrain(lib):
+    g = helpers.small_grid()
+    c = helpers.small_case(g)
+    a = with_terrain(helpers.short_inputs(c, full=False), g)
+    lib.setup(g.index_dict(), "UD3", "UD3")
+    with pytest.raises(hevi.HeviError, match="flat terrain|not supported") as e:
+        lib.ATMOS_DYN_Tstep_short_fvm_heve(**_stage_kw(a, helpers.stage_outputs(g)))
+    assert e.value.code == 5
+    # the flat-terrain stage still runs after the refusal
+    a_flat = helpers.short_inputs(c, full=False)
+    lib.ATMOS_DYN_Tstep_short_fvm_hevi(**_stage_kw(a_flat, helpers.stage_outputs(g)))
