@@ -23,9 +23,9 @@
  * Supported configuration (checked, otherwise SCALE_HEVI_ERR_UNSUPPORTED):
  * periodic lateral boundaries (BND_* = .false.); terrain-following metrics
  * (GSQRT, J13G, J23G, MAPF not those of flat terrain, classified once per set
- * of metric arrays) in the FP64 HEVI stage, RK4 and RK3 entries of one domain,
- * where they select the general-metric stage and PHI is read; flat terrain
- * (GSQRT = 1, J13G = J23G = 0, MAPF = 1) in every other entry; the default
+ * of metric arrays) in the FP64 HEVI stage, RK4, RK3 and large-step entries of
+ * one domain, where they select the general-metric stage and PHI is read;
+ * flat terrain (GSQRT = 1, J13G = J23G = 0, MAPF = 1) in every other entry; the default
  * IBLOCK/JBLOCK (whole domain), flux schemes "UD3", "CD4", "CD2",
  * "UD3KOREN1993", "UD5" and "CD6", ND_ORDER >= 1 (above 1 on the FP64 path of
  * one domain with KMAX >= 6), 4 <= KMAX <= 256 (5 for UD5/CD6), KHALO = 2 and IHALO = JHALO

@@ -702,7 +702,8 @@ int run_divergence(double *DDIV, const double *MOMZ, const double *MOMX, const d
                    const double *RCDX, const double *RCDY, double J33G)
 {
     CK(timed("divergence", [&] {
-        divergence(C.g, DDIV, MOMZ, MOMX, MOMY, RCDZ, RCDX, RCDY, J33G, C.stream);
+        if (C.terrain) divergence_terrain(C.g, DDIV, MOMZ, MOMX, MOMY, C.tm, J33G, C.stream);
+        else divergence(C.g, DDIV, MOMZ, MOMX, MOMY, RCDZ, RCDX, RCDY, J33G, C.stream);
         CU(cudaGetLastError());
         return SCALE_HEVI_OK;
     }));
@@ -718,6 +719,9 @@ int run_tracer_rk3(double *QTRC, const double *QTRC0, const double *RHOQ_t, cons
     a.QTRC0 = QTRC0; a.RHOQ_t = RHOQ_t; a.DENS0 = DENS0; a.DENS = DENS; a.mflx = mflx; a.ndq = ndq;
     a.phi_lo = C.tr + 2 * C.N3; a.anti = C.tr + 3 * C.N3; a.rjp = C.tr + 6 * C.N3; a.rjm = C.tr + 7 * C.N3;
     a.along_stream = along ? 1 : 0;
+    // terrain-following metrics of the large step (the mass-point MAPF slice comes first)
+    a.GS = C.terrain ? C.tm.GSQRT : nullptr;
+    a.MAPF = C.terrain ? C.tm.MAPF : nullptr;
     double *rk1 = C.tr, *rk2 = C.tr + C.N3;
     // stage 1: dt/3 with DENS0 + (DENS-DENS0)/3
     a.QTRCo = rk1; a.QTRC = QTRC; a.dens_mode = 1; a.dtl = dtl / 3.0;
@@ -1404,7 +1408,9 @@ int ATMOS_DYN_Tstep_large_fvm_heve_b200_dev(SCALE_HEVI_LARGE_ARGS)
     if (*ND_COEF != 0.0 && (*ND_ORDER < 1 || *ND_ORDER > 8))
         return fail(SCALE_HEVI_ERR_UNSUPPORTED, "ND_ORDER=%d is not supported (1..8)", *ND_ORDER);
     if (*ND_COEF != 0.0 && !*ND_USE_RS) return fail(SCALE_HEVI_ERR_UNSUPPORTED, "ND_USE_RS=.false. is not supported");
-    CK(check_flat(GSQRT, J13G, J23G, MAPF, true));
+    CK(use_metrics(GSQRT, J13G, J23G, MAPF, PHI, true));
+    if (C.terrain && C.short_type != 0)
+        return fail(SCALE_HEVI_ERR_UNSUPPORTED, "the HEVE short step takes flat terrain only");
     const size_t N3 = C.N3;
     if (!C.lg) CK(dalloc(&C.lg, 8 * N3));
     if (!C.tr) CK(dalloc(&C.tr, 8 * N3));
@@ -1489,7 +1495,21 @@ int ATMOS_DYN_Tstep_large_fvm_heve_b200(SCALE_HEVI_LARGE_ARGS)
 {
     CK(need_single("the large step"));
     if (C.capturing) return fail(SCALE_HEVI_ERR_ARG, "the host-array large step cannot be captured");
-    CK(check_flat(GSQRT, J13G, J23G, MAPF, false));
+    bool flat = false;
+    CK(metrics_flat(GSQRT, J13G, J23G, MAPF, false, &flat));
+    // terrain-following metrics go to the device with PHI; flat terrain needs neither
+    const double *dGS = nullptr, *dJ13 = nullptr, *dJ23 = nullptr, *dMAPF = nullptr, *dPHI = PHI;
+    if (!flat) {
+        if (!GSQRT || !J13G || !J23G || !MAPF || !PHI)
+            return fail(SCALE_HEVI_ERR_ARG, "terrain-following metrics need GSQRT, J13G, J23G, MAPF and PHI");
+        double *g7, *j13, *j23, *mp, *ph;
+        CK(h2d("GSQRT", GSQRT, 7 * C.N3, &g7));
+        CK(h2d("J13G", J13G, 7 * C.N3, &j13));
+        CK(h2d("J23G", J23G, 7 * C.N3, &j23));
+        CK(h2d("MAPF", MAPF, C.N2 * 2 * 4, &mp));
+        CK(h2d("PHI", PHI, C.N3, &ph));
+        dGS = g7; dJ13 = j13; dJ23 = j23; dMAPF = mp; dPHI = ph;
+    }
     const size_t N3 = n3(), N2 = (size_t)C.g.IA * C.g.JA;
     const int qa = *QA;
     if (qa < 0 || qa > 8) return fail(SCALE_HEVI_ERR_UNSUPPORTED, "QA=%d (0..8 supported)", qa);
@@ -1546,7 +1566,7 @@ int ATMOS_DYN_Tstep_large_fvm_heve_b200(SCALE_HEVI_LARGE_ARGS)
     C.large_hooks = &hk;
     int rc = ATMOS_DYN_Tstep_large_fvm_heve_b200_dev(
         X[0], X[1], X[2], X[3], X[4], q, QA, mf, tf, nd, T[0], T[1], T[2], T[3], T[4], rq, cor,
-        CDZ, CDX, CDY, FDZ, FDX, FDY, RCDZ, RCDX, RCDY, RFDZ, RFDX, RFDY, PHI, nullptr, nullptr, nullptr, J33G, nullptr,
+        CDZ, CDX, CDY, FDZ, FDX, FDY, RCDZ, RCDX, RCDY, RFDZ, RFDX, RFDY, dPHI, dGS, dJ13, dJ23, J33G, dMAPF,
         AQ_R, AQ_CV, AQ_CP, AQ_MASS, rd, rp, rpres, ND_COEF, ND_ORDER, ND_SFC_FACT, ND_USE_RS, wdamp_coef, divdmp_coef,
         FLAG_FCT_TRACER, FLAG_FCT_ALONG_STREAM, DTLS, DTSS);
     C.large_hooks = nullptr;

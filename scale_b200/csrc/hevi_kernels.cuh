@@ -112,8 +112,14 @@ struct TracerArgs {
     double dtl;
     double *phi_lo, *anti, *rjp, *rjm; // limiter scratch (anti is 3 fields)
     int along_stream;
+    // terrain-following metrics, null on flat terrain: GSQRT (KA,IA,JA,7) and
+    // the MAPF slice (IA,JA,2) of the mass points
+    const double *GS, *MAPF;
 };
 cudaError_t launch_tracer_stage(const Grid &g, const TracerArgs &a, int scheme, bool fct, cudaStream_t st);
+// ATMOS_DYN_divergence with every metric term (misc.cu)
+void divergence_terrain(const Grid &g, double *DDIV, const double *MOMZ, const double *MOMX, const double *MOMY,
+                        const Metrics &M, double J33G, cudaStream_t st);
 
 // ---- HEVI stage (hevi_stage.cu) ----
 // tile width (columns along i; the CTA's HEVI_COL_TC columns make the tile)

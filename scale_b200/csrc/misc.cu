@@ -122,6 +122,60 @@ void divergence(const Grid &g, double *DDIV, const double *MOMZ, const double *M
     k_divergence<<<gr, b, 0, st>>>(g, DDIV, MOMZ, MOMX, MOMY, RCDZ, RCDX, RCDY, J33G);
 }
 
+// ATMOS_DYN_divergence with terrain-following metrics (scale_atmos_dyn_common.F90:1437-1515):
+// the general row for KS-1..KE+1, the rows at KS and KE written in place of it
+__global__ void k_divergence_terrain(const Grid g, double *DDIV, const double *MOMZ, const double *MOMX,
+                                     const double *MOMY, const Metrics M, double J33G)
+{
+    const int i = g.IS + blockIdx.x * blockDim.y + threadIdx.y;
+    const int j = g.JS + blockIdx.y;
+    if (i > g.IE + 1) return;
+    const size_t N3 = n3(g);
+    const long sI = g.KA, sJ = (long)g.KA * g.IA;
+    const int KS = g.KS, KE = g.KE;
+    const double rcdx = ld(g.RCDX + i - 1), rcdy = ld(g.RCDY + j - 1);
+    const double *GUZ = M.GSQRT + 4 * N3, *GVZ = M.GSQRT + 5 * N3; // I_UYZ, I_XVZ
+    const double *J13 = M.J13G + N3, *J23 = M.J23G + N3;            // I_XYW
+    const size_t NP = (size_t)g.IA * g.JA, p = (size_t)(i - 1) + (size_t)g.IA * (j - 1);
+    // MAPF(i,j,a,b), b = I_XY (1), I_UY (2), I_XV (3)
+#define MF(pp, aa, bb) ld(M.MAPF + (pp) + NP * ((size_t)((aa) - 1) + 2 * (size_t)((bb) - 1)))
+    const double mxy = MF(p, 1, 1) * MF(p, 2, 1);
+    for (int k = KS - 1 + threadIdx.x; k <= KE + 1; k += 32) {
+        const size_t c = idx3(g, k, i, j);
+        const double h = mxy * ((ld(MOMX + c) * ld(GUZ + c) / MF(p, 2, 2) - ld(MOMX + c - sI) * ld(GUZ + c - sI) / MF(p - 1, 2, 2)) * rcdx
+                                + (ld(MOMY + c) * ld(GVZ + c) / MF(p, 1, 3) - ld(MOMY + c - sJ) * ld(GVZ + c - sJ) / MF(p - g.IA, 1, 3)) * rcdy);
+        double v;
+        if (k == KS) {
+            v = J33G * (ld(MOMZ + c)) * ld(g.RCDZ + k - 1)
+                + ((ld(MOMX + c + 1) + ld(MOMX + c + 1 - sI)) * ld(J13 + c + 1) - (ld(MOMX + c - 1) + ld(MOMX + c - sI)) * ld(J13 + c)
+                   + (ld(MOMY + c + 1) + ld(MOMY + c + 1 - sJ)) * ld(J23 + c + 1) - (ld(MOMY + c) + ld(MOMY + c - sJ)) * ld(J23 + c))
+                      * ld(g.RFDZ + k - 1)
+                + h;
+        } else if (k == KE) {
+            v = J33G * (-ld(MOMZ + c - 1)) * ld(g.RCDZ + k - 1)
+                + ((ld(MOMX + c) + ld(MOMX + c - sI)) * ld(J13 + c) - (ld(MOMX + c - 1) + ld(MOMX + c - 1 - sI)) * ld(J13 + c - 1)
+                   + (ld(MOMY + c) + ld(MOMY + c - sJ)) * ld(J23 + c) - (ld(MOMY + c - 1) + ld(MOMY + c - 1 - sJ)) * ld(J23 + c - 1))
+                      * ld(g.RFDZ + k - 1)
+                + h;
+        } else {
+            v = J33G * (ld(MOMZ + c) - ld(MOMZ + c - 1)) * ld(g.RCDZ + k - 1)
+                + ((ld(MOMX + c + 1) + ld(MOMX + c + 1 - sI)) * ld(J13 + c + 1) - (ld(MOMX + c - 1) + ld(MOMX + c - 1 - sI)) * ld(J13 + c - 1)
+                   + (ld(MOMY + c + 1) + ld(MOMY + c + 1 - sJ)) * ld(J23 + c + 1) - (ld(MOMY + c - 1) + ld(MOMY + c - 1 - sJ)) * ld(J23 + c - 1))
+                      / (ld(g.FDZ + k - 1) + ld(g.FDZ + k - 2))
+                + h;
+        }
+        DDIV[c] = v;
+    }
+#undef MF
+}
+
+void divergence_terrain(const Grid &g, double *DDIV, const double *MOMZ, const double *MOMX, const double *MOMY,
+                        const Metrics &M, double J33G, cudaStream_t st)
+{
+    dim3 b(32, 4), gr((g.IMAX + 1 + 3) / 4, g.JMAX + 1);
+    k_divergence_terrain<<<gr, b, 0, st>>>(g, DDIV, MOMZ, MOMX, MOMY, M, J33G);
+}
+
 // ---- RT2P, DPRES0, REF_rhot once per large step (tstep_large_fvm_heve.F90:428-470, moist form) ----
 __global__ void k_large_prep(const Grid g, const PrepArgs a)
 {

@@ -11,7 +11,8 @@
 //               raw anti-diffusive fluxes of every face an interior cell owns
 //   k_fct_r     P+/P-, the along-stream (or 7-point) bounds Q+/Q-, R+/R-
 //   k_fct_apply limit the anti-diffusive fluxes and update the tracer
-// Flat terrain only (GSQRT = MAPF = 1).
+// Terrain-following metrics (TracerArgs::GS, MAPF) enter the num_diff terms and
+// the metric factor of every flux divergence; null pointers mean flat terrain.
 #include "hevi_kernels.cuh"
 
 namespace hevi {
@@ -25,9 +26,23 @@ __device__ __forceinline__ double dens_of(const TracerArgs &a, size_t c)
     return a.dens_mode == 1 ? d0 + (d - d0) / 3.0 : d0 + (d - d0) * 0.5;
 }
 
+// the num_diff term of a high-order flux; with terrain GSQRT times it, at the
+// staggering of the face (fluxZ/X/Y_XYZ: I_XYW, I_UYZ, I_XVZ)
 __device__ __forceinline__ double ndq_at(const TracerArgs &a, size_t N3, int dir, size_t c)
 {
-    return a.ndq ? ld(a.ndq + (size_t)dir * N3 + c) : 0.0;
+    const double nd = a.ndq ? ld(a.ndq + (size_t)dir * N3 + c) : 0.0;
+    if (!a.GS) return nd;
+    const int slice = dir == 0 ? 1 : dir == 1 ? 4 : 5; // I_XYW, I_UYZ, I_XVZ (0-based)
+    return ld(a.GS + (size_t)slice * N3 + c) * nd;
+}
+// x * MAPF(i,j,1) * MAPF(i,j,2) / GSQRT(k,i,j,I_XYZ) with terrain, x on flat terrain
+// (the metric factor of every flux divergence, tstep_tracer_fvm_heve.F90:188-236,
+// common.F90:2051-2120)
+__device__ __forceinline__ double mfac(const Grid &g, const TracerArgs &a, double x, int i, int j, size_t c)
+{
+    if (!a.GS) return x;
+    const size_t p = (size_t)(i - 1) + (size_t)g.IA * (size_t)(j - 1);
+    return x * ld(a.MAPF + p) * ld(a.MAPF + p + (size_t)g.IA * g.JA) / ld(a.GS + c);
 }
 
 // high-order z flux at the face above level m (fluxZ_XYZ, ud3.F90:157-247, ud5.F90:194-321)
@@ -75,7 +90,7 @@ __global__ void __launch_bounds__(128) k_tracer_plain(const Grid g, const Tracer
         const double hx = hflux_h<S>(a, N3, 1, c, sI), hxm = hflux_h<S>(a, N3, 1, c - sI, sI);
         const double hy = hflux_h<S>(a, N3, 2, c, sJ), hym = hflux_h<S>(a, N3, 2, c - sJ, sJ);
         const double div = (hz - hzm) * ld(g.RCDZ + k - 1) + (hx - hxm) * rcdx + (hy - hym) * rcdy;
-        a.QTRCo[c] = (ld(a.QTRC0 + c) * ld(a.DENS0 + c) + a.dtl * (-div + ld(a.RHOQ_t + c))) / dens_of(a, c);
+        a.QTRCo[c] = (ld(a.QTRC0 + c) * ld(a.DENS0 + c) + a.dtl * (mfac(g, a, -div, i, j, c) + ld(a.RHOQ_t + c))) / dens_of(a, c);
     }
 }
 
@@ -99,7 +114,7 @@ __global__ void __launch_bounds__(128) k_fct_lo(const Grid g, const TracerArgs a
         const double lx = lflux(a, N3, 1, c, sI), lxm = lflux(a, N3, 1, c - sI, sI);
         const double ly = lflux(a, N3, 2, c, sJ), lym = lflux(a, N3, 2, c - sJ, sJ);
         a.phi_lo[c] = (ld(a.QTRC0 + c) * ld(a.DENS0 + c)
-                       + a.dtl * (-((lz - lzm) * ld(g.RCDZ + k - 1) + (lx - lxm) * rcdx + (ly - lym) * rcdy)))
+                       + a.dtl * mfac(g, a, -((lz - lzm) * ld(g.RCDZ + k - 1) + (lx - lxm) * rcdx + (ly - lym) * rcdy), i, j, c))
                       / ld(a.DENS + c);
         if (inter) {
             double *aZ = a.anti, *aX = a.anti + N3, *aY = a.anti + 2 * N3;
@@ -176,11 +191,11 @@ __global__ void __launch_bounds__(128) k_fct_r(const Grid g, const TracerArgs a)
         const double pz = fmax2(0.0, ld(aZ + c - 1)) - fmin2(0.0, ld(aZ + c));
         const double px = fmax2(0.0, ld(aX + c - sI)) - fmin2(0.0, ld(aX + c));
         const double py = fmax2(0.0, ld(aY + c - sJ)) - fmin2(0.0, ld(aY + c));
-        const double pjpls = a.dtl * (pz * rdz + px * rdx + py * rdy);
+        const double pjpls = mfac(g, a, a.dtl * (pz * rdz + px * rdx + py * rdy), i, j, c);
         const double mz = fmax2(0.0, ld(aZ + c)) - fmin2(0.0, ld(aZ + c - 1));
         const double mx = fmax2(0.0, ld(aX + c)) - fmin2(0.0, ld(aX + c - sI));
         const double my = fmax2(0.0, ld(aY + c)) - fmin2(0.0, ld(aY + c - sJ));
-        const double pjmns = a.dtl * (mz * rdz + mx * rdx + my * rdy);
+        const double pjmns = mfac(g, a, a.dtl * (mz * rdz + mx * rdx + my * rdy), i, j, c);
 
         const double *PI = a.QTRC0 + c, *PL = a.phi_lo + c;
         double qmax, qmin;
@@ -267,7 +282,7 @@ __global__ void __launch_bounds__(128) k_fct_apply(const Grid g, const TracerArg
         const double hy = hflux_h<S>(a, N3, 2, c, sJ), hym = hflux_h<S>(a, N3, 2, c - sJ, sJ);
         const double div = (hz - az - hzm + azm) * ld(g.RCDZ + k - 1) + (hx - ax - hxm + axm) * rcdx
                            + (hy - ay - hym + aym) * rcdy;
-        a.QTRCo[c] = (ld(a.QTRC0 + c) * ld(a.DENS0 + c) + a.dtl * (-div + ld(a.RHOQ_t + c))) / ld(a.DENS + c);
+        a.QTRCo[c] = (ld(a.QTRC0 + c) * ld(a.DENS0 + c) + a.dtl * (mfac(g, a, -div, i, j, c) + ld(a.RHOQ_t + c))) / ld(a.DENS + c);
     }
 }
 

@@ -184,9 +184,11 @@ def _large_inputs(c):
     return tp, GS, J13, J23, MAPF
 
 
-def _run_large_both(c, nlarge, lib, divdmp=0.0, nd_order=1, short="HEVI", tinteg="RK4"):
+def _run_large_both(c, nlarge, lib, divdmp=0.0, nd_order=1, short="HEVI", tinteg="RK4", metrics=None):
     g = c.g
     tp, GS, J13, J23, MAPF = _large_inputs(c)
+    if metrics is not None:
+        GS, J13, J23, MAPF = metrics
     aq = mkinit.aq_props(c.QA) if c.QA else None
     cor = np.zeros((g.IA, g.JA), order="F")
     wd = np.zeros(g.KA)

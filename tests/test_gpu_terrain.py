@@ -9,7 +9,7 @@ import pytest
 
 import helpers
 import oracle
-from scale_b200 import hevi
+from scale_b200 import hevi, mkinit
 
 pytestmark = pytest.mark.gpu
 
@@ -133,3 +133,23 @@ def test_flat_only_entries_refuse_terrain(lib):
     # the flat-terrain stage still runs after the refusal
     a_flat = helpers.short_inputs(c, full=False)
     lib.ATMOS_DYN_Tstep_short_fvm_hevi(**_stage_kw(a_flat, helpers.stage_outputs(g)))
+
+
+@pytest.mark.parametrize("case,divdmp", [("dry", 0.0), ("dry", 0.05), ("moist_fct", 0.0)])
+def test_terrain_large_step_parity(lib, case, divdmp):
+    """The device-resident large step with terrain: the general-metric short
+    step, the metric divergence for divergence damping and the tracer step
+    with GSQRT/MAPF, against the oracle's large step (the tolerance of the
+    flat large-step tests: the moist RT2P goes through pow())."""
+    from test_gpu_parity import _field_err, _run_large_both
+
+    c = mkinit.config(1, scale=0.3) if case == "dry" else mkinit.config(2, scale=0.04)
+    m = with_terrain(dict(), c.g, seed=5, amp=0.02)
+    st_ref, st_gpu = _run_large_both(c, 2, lib, divdmp=divdmp, metrics=(m["GSQRT"], m["J13G"], m["J23G"], m["MAPF"]))
+    for n in STATE:
+        assert np.isfinite(st_gpu[n]).all(), n
+        err = _field_err(st_gpu[n], st_ref[n], c.g)
+        assert err <= 1e-10, f"{n}: {err:.3e}"
+    for iq in range(c.QA):
+        err = _field_err(st_gpu["QTRC"][..., iq], st_ref["QTRC"][..., iq], c.g)
+        assert err <= 1e-10, f"QTRC[{iq}]: {err:.3e}"
