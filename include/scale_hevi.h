@@ -23,8 +23,8 @@
  * Supported configuration (checked, otherwise SCALE_HEVI_ERR_UNSUPPORTED):
  * periodic lateral boundaries (BND_* = .false.); terrain-following metrics
  * (GSQRT, J13G, J23G, MAPF not those of flat terrain, classified once per set
- * of metric arrays) in the FP64 HEVI stage, RK4, RK3 and large-step entries of
- * one domain, where they select the general-metric stage and PHI is read;
+ * of metric arrays) in the FP64 HEVI and HEVE stage, RK4, RK3 and large-step
+ * entries of one domain, where they select the general-metric stage and PHI is read;
  * flat terrain (GSQRT = 1, J13G = J23G = 0, MAPF = 1) in every other entry; the default
  * IBLOCK/JBLOCK (whole domain), flux schemes "UD3", "CD4", "CD2",
  * "UD3KOREN1993", "UD5" and "CD6", ND_ORDER >= 1 (above 1 on the FP64 path of
@@ -133,7 +133,7 @@ int ATMOS_DYN_Tstep_short_fvm_hevi_b200_dev(SCALE_HEVI_TSTEP_SHORT_ARGS);
  * the other target of ATMOS_DYN_Tstep_short. Same arguments as the HEVI
  * stage. FLAG_FCT_MOMENTUM and FLAG_FCT_T must be .false. (the momentum and
  * theta FCT branches, :386-447, :716-1309, :1388-1515, are not provided);
- * FP64 only.
+ * FP64 only. Terrain-following metrics select the general-metric HEVE stage.
  * ------------------------------------------------------------------------- */
 int ATMOS_DYN_Tstep_short_fvm_heve_b200(SCALE_HEVI_TSTEP_SHORT_ARGS);
 int ATMOS_DYN_Tstep_short_fvm_heve_b200_dev(SCALE_HEVI_TSTEP_SHORT_ARGS);

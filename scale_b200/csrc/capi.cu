@@ -552,16 +552,17 @@ int run_stage(const StageInT<F> &in, double *const out[5], F *mflx, F *tflx, dou
         return fail(SCALE_HEVI_ERR_UNSUPPORTED, "divergence damping is not available for an ensemble");
     if (kind < 0) kind = C.short_type;
     if (C.terrain) {
-        if (kind == 1) return fail(SCALE_HEVI_ERR_UNSUPPORTED, "the HEVE short step takes flat terrain only");
         if constexpr (sizeof(F) != sizeof(double)) {
             return fail(SCALE_HEVI_ERR_UNSUPPORTED, "the mixed-precision path takes flat terrain only");
         } else {
             const StageArgsT<double> a = stage_args(in, out, mflx, tflx, dtrk, mode);
-            CK(timed("hevi_stage_terrain", [&] {
-                CU(launch_terrain_stage(C.g, a, C.tm, C.tw, C.scheme, C.stream));
+            const bool heve = kind == 1;
+            CK(timed(heve ? "heve_stage_terrain" : "hevi_stage_terrain", [&] {
+                CU(heve ? launch_terrain_heve_stage(C.g, a, C.tm, C.tw, C.scheme, C.stream)
+                        : launch_terrain_stage(C.g, a, C.tm, C.tw, C.scheme, C.stream));
                 return SCALE_HEVI_OK;
             }));
-            C.launches += TERRAIN_STAGE_LAUNCHES;
+            C.launches += heve ? TERRAIN_HEVE_LAUNCHES : TERRAIN_STAGE_LAUNCHES;
             return SCALE_HEVI_OK;
         }
     }
@@ -994,7 +995,7 @@ int ATMOS_DYN_Tstep_short_fvm_heve_b200_dev(SCALE_HEVI_TSTEP_SHORT_ARGS)
     CK(need_setup());
     CK(check_heve_fct(FLAG_FCT_MOMENTUM, FLAG_FCT_T));
     CK(check_bnd(BND_W, BND_E, BND_S, BND_N));
-    CK(check_flat(GSQRT, J13G, J23G, MAPF, true));
+    CK(use_metrics(GSQRT, J13G, J23G, MAPF, PHI, true));
     CK(prepare_tables(CDZ, FDZ, RCDZ, RFDZ, FDX, RCDX, RFDX, FDY, RCDY, RFDY, wdamp_coef, nullptr, nullptr));
     StageIn in{DENS0, MOMZ0, MOMX0, MOMY0, RHOT0, DENS, MOMZ, MOMX, MOMY, RHOT,
                DENS_t, MOMZ_t, MOMX_t, MOMY_t, RHOT_t, DPRES0, RT2P, CORIOLI, num_diff, DDIV, REF_dens, REF_rhot,
@@ -1409,8 +1410,6 @@ int ATMOS_DYN_Tstep_large_fvm_heve_b200_dev(SCALE_HEVI_LARGE_ARGS)
         return fail(SCALE_HEVI_ERR_UNSUPPORTED, "ND_ORDER=%d is not supported (1..8)", *ND_ORDER);
     if (*ND_COEF != 0.0 && !*ND_USE_RS) return fail(SCALE_HEVI_ERR_UNSUPPORTED, "ND_USE_RS=.false. is not supported");
     CK(use_metrics(GSQRT, J13G, J23G, MAPF, PHI, true));
-    if (C.terrain && C.short_type != 0)
-        return fail(SCALE_HEVI_ERR_UNSUPPORTED, "the HEVE short step takes flat terrain only");
     const size_t N3 = C.N3;
     if (!C.lg) CK(dalloc(&C.lg, 8 * N3));
     if (!C.tr) CK(dalloc(&C.tr, 8 * N3));

@@ -60,6 +60,9 @@ struct TerrainWork {
 };
 constexpr int TERRAIN_WORK_FIELDS = 24;
 constexpr int TERRAIN_STAGE_LAUNCHES = 24; // kernels of one general-metric stage
+constexpr int TERRAIN_HEVE_LAUNCHES = 23;  // kernels of one general-metric HEVE stage
+cudaError_t launch_terrain_heve_stage(const Grid &g, const StageArgsT<double> &a, const Metrics &M,
+                                      const TerrainWork &W, int scheme, cudaStream_t st);
 cudaError_t launch_terrain_stage(const Grid &g, const StageArgsT<double> &a, const Metrics &M, const TerrainWork &W,
                                  int scheme, cudaStream_t st);
 

@@ -1337,6 +1337,405 @@ static void terrain_stage(const Grid &g, const StageArgsT<double> &a, const Metr
 #undef AVG4_XV
 }
 
+// The HEVE stage with terrain-following metrics (ATMOS_DYN_Tstep_short_fvm_heve,
+// scale_atmos_dyn_tstep_short_fvm_heve.F90:109-1518 without the momentum/theta
+// FCT branches), in the same form as terrain_stage: one launch per loop nest,
+// the flux routines with their metric arguments, outputs through put_state/put_flux.
+template <int S>
+static void terrain_heve_stage(const Grid &g, const StageArgsT<double> &a, const Metrics &M, const TerrainWork &W,
+                               cudaStream_t st)
+{
+    const int KS = g.KS, KE = g.KE, IS = g.IS, IE = g.IE, JS = g.JS, JE = g.JE;
+    const int IEH = g.IEH < IE ? g.IEH : IE, JEH = g.JEH < JE ? g.JEH : JE;
+    const size_t N3 = n3(g);
+    const long sI = g.KA, sJ = (long)g.KA * g.IA;
+    const double dt = a.dtrk, J33G = a.J33G;
+    const bool use_div = a.divdmp_coef != 0.0;
+#define X3(k, i, j) idx3(g, k, i, j)
+#define GSs(idx) (M.GSQRT + (size_t)((idx) - 1) * N3)
+#define J13s(idx) (M.J13G + (size_t)((idx) - 1) * N3)
+#define J23s(idx) (M.J23G + (size_t)((idx) - 1) * N3)
+#define GS(k, i, j, idx) GSs(idx)[X3(k, i, j)]
+#define J13(k, i, j, idx) J13s(idx)[X3(k, i, j)]
+#define J23(k, i, j, idx) J23s(idx)[X3(k, i, j)]
+#define MAPFv(i, j, aa, bb) \
+    M.MAPF[(size_t)((i) - 1) + (size_t)g.IA * ((size_t)((j) - 1) + (size_t)g.JA * ((size_t)((aa) - 1) + 2 * (size_t)((bb) - 1)))]
+#define NDp(v, dir) (a.num_diff + N3 * (size_t)(((v) - 1) + 5 * ((dir) - 1)))
+#define CDZv(k) ld(g.CDZ + (k) - 1)
+#define F2Hg(Gs, k, p) (CDZv((k) + (p) - 1) * (Gs)[X3((k) + (p) - 1, i, j)] \
+                        / (CDZv(k) * (Gs)[X3(k, i, j)] + CDZv((k) + 1) * (Gs)[X3((k) + 1, i, j)]))
+#define DEN_UYZ(Gs, k) (F2Hg(Gs, k, 1) * 0.5 * (DN[X3((k) + 1, i, j)] + DN[X3((k) + 1, i + 1, j)]) \
+                        + F2Hg(Gs, k, 2) * 0.5 * (DN[X3(k, i, j)] + DN[X3(k, i + 1, j)]))
+#define DEN_XVZ(Gs, k) (F2Hg(Gs, k, 1) * 0.5 * (DN[X3((k) + 1, i, j)] + DN[X3((k) + 1, i, j + 1)]) \
+                        + F2Hg(Gs, k, 2) * 0.5 * (DN[X3(k, i, j)] + DN[X3(k, i, j + 1)]))
+#define AVG4_UV(m, k) (0.25 * ((m)[X3(k, i, j)] + (m)[X3(k, i + 1, j)] + (m)[X3(k, i, j - 1)] + (m)[X3(k, i + 1, j - 1)]))
+#define AVG4_XV(m, k) (0.25 * ((m)[X3(k, i, j)] + (m)[X3(k, i - 1, j)] + (m)[X3(k, i, j + 1)] + (m)[X3(k, i - 1, j + 1)]))
+    const double *DN = a.DENS, *MZ = a.MOMZ, *MX = a.MOMX, *MY = a.MOMY;
+
+    // ---- pressure :360-373, potential temperature :375-382 ----
+    gcols(IS - 2, IE + 2, JS - 2, JE + 2, st, [=] __device__(int i, int j, int lane) {
+        for (int k = KS + lane; k <= KE; k += 32) {
+            const size_t c = X3(k, i, j);
+            W.DPRES[c] = a.DPRES0[c] + a.RT2P[c] * (a.RHOT[c] - a.REF_rhot[c]);
+        }
+        if (lane == 0) {
+            W.DPRES[X3(KS - 1, i, j)] = a.DPRES0[X3(KS - 1, i, j)] - DN[X3(KS, i, j)] * (M.PHI[X3(KS - 1, i, j)] - M.PHI[X3(KS + 1, i, j)]);
+            W.DPRES[X3(KE + 1, i, j)] = a.DPRES0[X3(KE + 1, i, j)] - DN[X3(KE, i, j)] * (M.PHI[X3(KE + 1, i, j)] - M.PHI[X3(KE - 1, i, j)]);
+        }
+    });
+    gcols(IS - g.IHALO, IE + g.IHALO, JS - g.JHALO, JE + g.JHALO, st, [=] __device__(int i, int j, int lane) {
+        for (int k = KS + lane; k <= KE; k += 32) {
+            const size_t c = X3(k, i, j);
+            W.POTT[c] = a.RHOT[c] / DN[c];
+        }
+    });
+    // ---- mass fluxes :460-510 ----
+    gcols(IS, IE, JS, JE, st, [=] __device__(int i, int j, int lane) {
+        const double m1 = MAPFv(i, j, 1, I_XY), m2 = MAPFv(i, j, 2, I_XY);
+        for (int k = KS + lane; k <= KE - 1; k += 32) {
+            const size_t c = X3(k, i, j);
+            const double v = J33G * MZ[c] / (m1 * m2)
+                             + J13(k, i, j, I_XYW) * 0.25 * (MX[c + 1] + MX[c + 1 - sI] + MX[c] + MX[c - sI]) / m2
+                             + J23(k, i, j, I_XYW) * 0.25 * (MY[c + 1] + MY[c + 1 - sJ] + MY[c] + MY[c - sJ]) / m1
+                             + GS(k, i, j, I_XYW) * NDp(V_DENS, DZIR)[c] / (m1 * m2);
+            W.mZ[c] = v;
+            put_flux(a, N3, 0, c, v, true);
+        }
+        if (lane == 0) {
+            W.mZ[X3(KS - 1, i, j)] = 0.0;
+            W.mZ[X3(KE, i, j)] = 0.0;
+            put_flux(a, N3, 0, X3(KS - 1, i, j), 0.0, false);
+            put_flux(a, N3, 0, X3(KE, i, j), 0.0, true);
+        }
+    });
+    gcols(IS - 1, IEH, JS, JE, st, [=] __device__(int i, int j, int lane) {
+        for (int k = KS + lane; k <= KE; k += 32) {
+            const size_t c = X3(k, i, j);
+            const double v = GS(k, i, j, I_UYZ) / MAPFv(i, j, 2, I_UY) * (MX[c] + NDp(V_DENS, DXIR)[c]);
+            W.mX[c] = v;
+            put_flux(a, N3, 1, c, v, i >= IS);
+        }
+    });
+    gcols(IS, IE, JS - 1, JEH, st, [=] __device__(int i, int j, int lane) {
+        for (int k = KS + lane; k <= KE; k += 32) {
+            const size_t c = X3(k, i, j);
+            const double v = GS(k, i, j, I_XVZ) / MAPFv(i, j, 1, I_XV) * (MY[c] + NDp(V_DENS, DYIR)[c]);
+            W.mY[c] = v;
+            put_flux(a, N3, 2, c, v, j >= JS);
+        }
+    });
+    // ---- density :512-532 ----
+    gcols(IS, IE, JS, JE, st, [=] __device__(int i, int j, int lane) {
+        for (int k = KS + lane; k <= KE; k += 32) {
+            const size_t c = X3(k, i, j);
+            const double advcv = -(W.mZ[c] - W.mZ[c - 1]) * ld(g.RCDZ + k - 1);
+            const double advch = -(W.mX[c] - W.mX[c - sI]) * ld(g.RCDX + i - 1) - (W.mY[c] - W.mY[c - sJ]) * ld(g.RCDY + j - 1);
+            put_state(a, N3, 0, a.DENS_RK, a.DENS0, c,
+                      a.DENS0[c] + dt * ((advcv + advch) * MAPFv(i, j, 1, I_XY) * MAPFv(i, j, 2, I_XY) / GS(k, i, j, I_XYZ) + a.DENS_t[c]),
+                      true);
+        }
+    });
+    // ---- momentum (z): fluxes :586-620 (the HEVI routines) ----
+    gcols(IS, IE, JS, JE, st, [=] __device__(int i, int j, int lane) {
+        const double *Gs = GSs(I_XYZ), *nd = NDp(V_MOMZ, DZIR), *col = MZ + X3(1, i, j);
+        for (int k = KS + 1 + lane; k <= KE - 1; k += 32) {
+            const size_t c = X3(k, i, j);
+            const double vel = (0.5 * (MZ[c - 1] + MZ[c])) / DN[c];
+            W.qZ[c - 1] = J33G * vel * zface<S>(vel, k - 1, KS, KE, [&](int l) { return col[l - 1]; }) + Gs[c] * nd[c];
+        }
+        if (lane == 0) {
+            W.qZ[X3(KS - 1, i, j)] = 0.0;
+            W.qZ[X3(KE - 1, i, j)] = 0.0;
+            W.qZ[X3(KE, i, j)] = 0.0;
+        }
+    });
+    gcols(IS, IE, JS, JE, st, [=] __device__(int i, int j, int lane) {
+        constexpr bool wide = wide_scheme(S);
+        const int kend = wide ? KE - 2 : KE - 1;
+        const double *J1 = J13s(I_XYZ), *J2 = J23s(I_XYZ);
+        const double m2 = MAPFv(i, j, 2, I_XY), m1 = MAPFv(i, j, 1, I_XY);
+        auto V = [&](int k) { return MZ[X3(k, i, j)]; };
+        auto face = [&](double vel, int k) {
+            if constexpr (wide) return ip6<S>(vel, V(k - 3), V(k - 2), V(k - 1), V(k), V(k + 1), V(k + 2));
+            else return ip4<S>(vel, V(k - 2), V(k - 1), V(k), V(k + 1));
+        };
+        for (int k = KS + 2 + lane; k <= kend; k += 32) {
+            const size_t c = X3(k, i, j);
+            double vel = (0.5 * (MX[c] + MX[c - sI])) / DN[c];
+            vel = vel * J1[c];
+            W.qJ13[c - 1] = vel / m2 * face(vel, k);
+            double vel2 = (0.5 * (MY[c] + MY[c - sJ])) / DN[c];
+            vel2 = vel2 * J2[c];
+            W.qJ23[c - 1] = vel2 / m1 * face(vel2, k);
+        }
+        if (lane == 0) {
+            W.qJ13[X3(KS - 1, i, j)] = 0.0;
+            W.qJ23[X3(KS - 1, i, j)] = 0.0;
+            const size_t c0 = X3(KS, i, j), c1 = X3(KS + 1, i, j);
+            double vel = ((0.5 * (MX[c1] + MX[c1 - sI])) / DN[c1] + (0.5 * (MX[c0] + MX[c0 - sI])) / DN[c0]) * 0.5;
+            vel = vel * J1[c1];
+            W.qJ13[c0] = vel / m2 * ipL<S>(vel, V(KS), V(KS + 1), V(KS + 2));
+            double vel2 = ((0.5 * (MY[c1] + MY[c1 - sJ])) / DN[c1] + (0.5 * (MY[c0] + MY[c0 - sJ])) / DN[c0]) * 0.5;
+            vel2 = vel2 * J2[c1];
+            W.qJ23[c0] = vel2 / m1 * ipL<S>(vel2, V(KS), V(KS + 1), V(KS + 2));
+            if constexpr (wide) {
+                const size_t ce = X3(KE - 1, i, j);
+                double ve = (0.5 * (MX[ce] + MX[ce - sI])) / DN[ce];
+                ve = ve * J1[ce];
+                W.qJ13[X3(KE - 2, i, j)] = ve / m2 * ipH<S>(ve, V(KE - 1), V(KE - 2), V(KE - 3));
+                double ve2 = (0.5 * (MY[ce] + MY[ce - sJ])) / DN[ce];
+                ve2 = ve2 * J2[ce];
+                W.qJ23[X3(KE - 2, i, j)] = ve2 / m1 * ipH<S>(ve2, V(KE - 1), V(KE - 2), V(KE - 3));
+            }
+            W.qJ13[X3(KE - 1, i, j)] = 0.0;
+            W.qJ23[X3(KE - 1, i, j)] = 0.0;
+        }
+    });
+    gcols(IS - 1, IE, JS, JE, st, [=] __device__(int i, int j, int lane) {
+        const double *Gs = GSs(I_UYW), *nd = NDp(V_MOMZ, DXIR);
+        const double mp = MAPFv(i, j, 2, I_UY);
+        for (int k = KS + lane; k <= KE - 1; k += 32) {
+            const size_t c = X3(k, i, j);
+            const double vel = (F2Hg(Gs, k, 1) * MX[c + 1] + F2Hg(Gs, k, 2) * MX[c])
+                               / (F2Hg(Gs, k, 1) * 0.5 * (DN[c + 1] + DN[c + 1 + sI]) + F2Hg(Gs, k, 2) * 0.5 * (DN[c] + DN[c + sI]));
+            W.qX[c] = Gs[c] / mp * vel * hface<S>(vel, MZ + c, sI) + Gs[c] * nd[c];
+        }
+        if (lane == 0) W.qX[X3(KE, i, j)] = 0.0;
+    });
+    gcols(IS, IE, JS - 1, JE, st, [=] __device__(int i, int j, int lane) {
+        const double *Gs = GSs(I_XVW), *nd = NDp(V_MOMZ, DYIR);
+        const double mp = MAPFv(i, j, 1, I_XV);
+        for (int k = KS + lane; k <= KE - 1; k += 32) {
+            const size_t c = X3(k, i, j);
+            const double vel = (F2Hg(Gs, k, 1) * MY[c + 1] + F2Hg(Gs, k, 2) * MY[c])
+                               / (F2Hg(Gs, k, 1) * 0.5 * (DN[c + 1] + DN[c + 1 + sJ]) + F2Hg(Gs, k, 2) * 0.5 * (DN[c] + DN[c + sJ]));
+            W.qY[c] = Gs[c] / mp * vel * hface<S>(vel, MZ + c, sJ) + Gs[c] * nd[c];
+        }
+        if (lane == 0) W.qY[X3(KE, i, j)] = 0.0;
+    });
+    // pressure gradient :622-631, buoyancy :633-644, update :646-688
+    gcols(IS, IE, JS, JE, st, [=] __device__(int i, int j, int lane) {
+        const double *GZ = GSs(I_XYZ);
+        for (int k = KS + lane; k <= KE; k += 32) {
+            const size_t c = X3(k, i, j);
+            if (k == KE) { put_state(a, N3, 1, a.MOMZ_RK, a.MOMZ0, c, 0.0, false); continue; }
+            const double pgf = J33G * (W.DPRES[c + 1] - W.DPRES[c]) * ld(g.RFDZ + k - 1);
+            const double buoy = GRAV * GS(k, i, j, I_XYW)
+                                * (F2Hg(GZ, k, 1) * (DN[c + 1] - a.REF_dens[c + 1]) + F2Hg(GZ, k, 2) * (DN[c] - a.REF_dens[c]));
+            const double advcv = -(W.qZ[c] - W.qZ[c - 1] + W.qJ13[c] - W.qJ13[c - 1] + W.qJ23[c] - W.qJ23[c - 1]) * ld(g.RFDZ + k - 1);
+            const double advch = -((W.qX[c] - W.qX[c - sI]) * ld(g.RCDX + i - 1) + (W.qY[c] - W.qY[c - sJ]) * ld(g.RCDY + j - 1))
+                                 * MAPFv(i, j, 1, I_XY) * MAPFv(i, j, 2, I_XY);
+            const double wdamp = -ld(a.wdamp + g.z0 + k - 1) * a.MOMZ0[c];
+            const double div = use_div ? a.divdmp_coef / dt * ld(g.FDZ + k - 1) * (a.DDIV[c + 1] - a.DDIV[c]) : 0.0;
+            put_state(a, N3, 1, a.MOMZ_RK, a.MOMZ0, c,
+                      a.MOMZ0[c] + dt * ((advcv + advch - pgf - buoy) / GS(k, i, j, I_XYW) + wdamp + div + a.MOMZ_t[c]), true);
+        }
+        if (lane == 0) put_state(a, N3, 1, a.MOMZ_RK, a.MOMZ0, X3(KS - 1, i, j), 0.0, false);
+    });
+
+    // ---- momentum (x): fluxes :829-860, pressure gradient, Coriolis, update :862-922 ----
+    gcols(IS, IE, JS, JE, st, [=] __device__(int i, int j, int lane) {
+        const double *Gw = GSs(I_UYW), *Gz = GSs(I_UYZ), *J1 = J13s(I_UYW), *J2 = J23s(I_UYW), *nd = NDp(V_MOMX, DZIR);
+        const double *col = MX + X3(1, i, j);
+        auto V = [&](int l) { return col[l - 1]; };
+        const double m2 = MAPFv(i, j, 2, I_UY), m1 = MAPFv(i, j, 1, I_UY);
+        for (int k = KS + lane; k <= KE - 1; k += 32) {
+            const size_t c = X3(k, i, j);
+            const double vel = (0.5 * (MZ[c] + MZ[c + sI])) / DEN_UYZ(Gw, k);
+            W.qZ[c] = J33G * vel * zface<S>(vel, k, KS, KE, V) + Gw[c] * nd[c];
+            double v1 = (F2Hg(Gz, k, 1) * MX[c + 1] + F2Hg(Gz, k, 2) * MX[c]) / DEN_UYZ(Gz, k);
+            v1 = v1 * J1[c];
+            W.qJ13[c] = v1 / m2 * zface<S>(v1, k, KS, KE, V);
+            double v2 = (F2Hg(Gz, k, 1) * AVG4_UV(MY, k + 1) + F2Hg(Gz, k, 2) * AVG4_UV(MY, k)) / DEN_UYZ(Gz, k);
+            v2 = v2 * J2[c];
+            W.qJ23[c] = v2 / m1 * zface<S>(v2, k, KS, KE, V);
+        }
+        if (lane == 0) {
+            W.qZ[X3(KS - 1, i, j)] = 0.0; W.qZ[X3(KE, i, j)] = 0.0;
+            W.qJ13[X3(KS - 1, i, j)] = 0.0; W.qJ13[X3(KE, i, j)] = 0.0;
+            W.qJ23[X3(KS - 1, i, j)] = 0.0; W.qJ23[X3(KE, i, j)] = 0.0;
+        }
+    });
+    gcols(IS, IE + 1, JS, JE, st, [=] __device__(int i, int j, int lane) {
+        const double *Gs = GSs(I_XYZ), *nd = NDp(V_MOMX, DXIR);
+        const double mp = MAPFv(i, j, 2, I_XY);
+        for (int k = KS + lane; k <= KE; k += 32) {
+            const size_t c = X3(k, i, j);
+            const double vel = (0.5 * (MX[c] + MX[c - sI])) / (DN[c]);
+            W.qX[c - sI] = Gs[c] / mp * vel * hface<S>(vel, MX + c - sI, sI) + Gs[c] * nd[c];
+        }
+    });
+    gcols(IS, IE, JS - 1, JE, st, [=] __device__(int i, int j, int lane) {
+        const double *Gs = GSs(I_UVZ), *nd = NDp(V_MOMX, DYIR);
+        const double mp = MAPFv(i, j, 1, I_UV);
+        for (int k = KS + lane; k <= KE; k += 32) {
+            const size_t c = X3(k, i, j);
+            const double vel = (0.5 * (MY[c] + MY[c + sI])) / (0.25 * (DN[c] + DN[c + sI] + DN[c + sJ] + DN[c + sI + sJ]));
+            W.qY[c] = Gs[c] / mp * vel * hface<S>(vel, MX + c, sJ) + Gs[c] * nd[c];
+        }
+    });
+    gcols(IS, IEH, JS, JE, st, [=] __device__(int i, int j, int lane) {
+        const double *GZ = GSs(I_XYZ), *Gu = GSs(I_UYZ);
+        for (int k = KS + lane; k <= KE; k += 32) {
+            const size_t c = X3(k, i, j);
+            const double *DP = W.DPRES;
+            const double pgf = ((GZ[c + sI] * DP[c + sI] - GZ[c] * DP[c]) * ld(g.RFDX + i - 1)
+                                + (J13(k, i, j, I_UYW)
+                                       * 0.5 * (F2Hg(Gu, k, 1) * (DP[c + 1 + sI] + DP[c + 1]) + F2Hg(Gu, k, 2) * (DP[c + sI] + DP[c]))
+                                   - J13(k - 1, i, j, I_UYW)
+                                       * 0.5 * (F2Hg(Gu, k, 1) * (DP[c + sI] + DP[c]) + F2Hg(Gu, k, 2) * (DP[c - 1 + sI] + DP[c - 1])))
+                                      * ld(g.RCDZ + k - 1))
+                               * MAPFv(i, j, 1, I_UY);
+            const double sumy = MY[c] + MY[c - sJ] + MY[c + sI] + MY[c + sI - sJ];
+            const double cor = 0.125 * (a.CORIOLI[g.c2 + (size_t)i + (size_t)g.IA * (j - 1)] + a.CORIOLI[g.c2 + (size_t)(i - 1) + (size_t)g.IA * (j - 1)])
+                                   * (MY[c + sI] + MY[c] + MY[c + sI - sJ] + MY[c - sJ])
+                               + 0.25 * MAPFv(i, j, 1, I_UY) * MAPFv(i, j, 2, I_UY) * sumy
+                                   * (sumy * 0.25 * (1.0 / MAPFv(i + 1, j, 2, I_XY) - 1.0 / MAPFv(i, j, 2, I_XY)) * ld(g.RFDX + i - 1)
+                                      - MX[c] * (1.0 / MAPFv(i, j, 1, I_UV) - 1.0 / MAPFv(i, j - 1, 1, I_UV)) * ld(g.RCDY + j - 1))
+                                   * 2.0 / (DN[c + sI] + DN[c]);
+            const double advcv = -(W.qZ[c] - W.qZ[c - 1] + W.qJ13[c] - W.qJ13[c - 1] + W.qJ23[c] - W.qJ23[c - 1]) * ld(g.RCDZ + k - 1);
+            const double advch = -((W.qX[c] - W.qX[c - sI]) * ld(g.RFDX + i - 1) + (W.qY[c] - W.qY[c - sJ]) * ld(g.RCDY + j - 1))
+                                 * MAPFv(i, j, 1, I_UY) * MAPFv(i, j, 2, I_UY);
+            const double div = use_div ? a.divdmp_coef / dt * ld(g.FDX + i - 1) * (a.DDIV[c + sI] - a.DDIV[c]) : 0.0;
+            put_state(a, N3, 2, a.MOMX_RK, a.MOMX0, c,
+                      a.MOMX0[c] + dt * ((advcv + advch - pgf) / Gu[c] + cor + div + a.MOMX_t[c]), true);
+        }
+    });
+
+    // ---- momentum (y): fluxes :1076-1107, pressure gradient, Coriolis, update :1109-1170 ----
+    gcols(IS, IE, JS, JE, st, [=] __device__(int i, int j, int lane) {
+        const double *Gw = GSs(I_XVW), *Gz = GSs(I_XVZ), *J1 = J13s(I_XVW), *J2 = J23s(I_XVW), *nd = NDp(V_MOMY, DZIR);
+        const double *col = MY + X3(1, i, j);
+        auto V = [&](int l) { return col[l - 1]; };
+        const double m2 = MAPFv(i, j, 2, I_XV), m1 = MAPFv(i, j, 1, I_XV);
+        for (int k = KS + lane; k <= KE - 1; k += 32) {
+            const size_t c = X3(k, i, j);
+            const double vel = (0.5 * (MZ[c] + MZ[c + sJ])) / DEN_XVZ(Gw, k);
+            W.qZ[c] = J33G * vel * zface<S>(vel, k, KS, KE, V) + Gw[c] * nd[c];
+            double v1 = (F2Hg(Gz, k, 1) * AVG4_XV(MX, k + 1) + F2Hg(Gz, k, 2) * AVG4_XV(MX, k)) / DEN_XVZ(Gz, k);
+            v1 = v1 * J1[c];
+            W.qJ13[c] = v1 / m2 * zface<S>(v1, k, KS, KE, V);
+            double v2 = (F2Hg(Gz, k, 1) * MY[c + 1] + F2Hg(Gz, k, 2) * MY[c]) / DEN_XVZ(Gz, k);
+            v2 = v2 * J2[c];
+            W.qJ23[c] = v2 / m1 * zface<S>(v2, k, KS, KE, V);
+        }
+        if (lane == 0) {
+            W.qZ[X3(KS - 1, i, j)] = 0.0; W.qZ[X3(KE, i, j)] = 0.0;
+            W.qJ13[X3(KS - 1, i, j)] = 0.0; W.qJ13[X3(KE, i, j)] = 0.0;
+            W.qJ23[X3(KS - 1, i, j)] = 0.0; W.qJ23[X3(KE, i, j)] = 0.0;
+        }
+    });
+    gcols(IS - 1, IE, JS, JE, st, [=] __device__(int i, int j, int lane) {
+        const double *Gs = GSs(I_UVZ), *nd = NDp(V_MOMY, DXIR);
+        const double mp = MAPFv(i, j, 2, I_UV);
+        for (int k = KS + lane; k <= KE; k += 32) {
+            const size_t c = X3(k, i, j);
+            const double vel = (0.5 * (MX[c] + MX[c + sJ])) / (0.25 * (DN[c] + DN[c + sI] + DN[c + sJ] + DN[c + sI + sJ]));
+            W.qX[c] = Gs[c] / mp * vel * hface<S>(vel, MY + c, sI) + Gs[c] * nd[c];
+        }
+    });
+    gcols(IS, IE, JS, JE + 1, st, [=] __device__(int i, int j, int lane) {
+        const double *Gs = GSs(I_XYZ), *nd = NDp(V_MOMY, DYIR);
+        const double mp = MAPFv(i, j, 1, I_XY);
+        for (int k = KS + lane; k <= KE; k += 32) {
+            const size_t c = X3(k, i, j);
+            const double vel = (0.5 * (MY[c] + MY[c - sJ])) / (DN[c]);
+            W.qY[c - sJ] = Gs[c] / mp * vel * hface<S>(vel, MY + c - sJ, sJ) + Gs[c] * nd[c];
+        }
+    });
+    gcols(IS, IE, JS, JEH, st, [=] __device__(int i, int j, int lane) {
+        const double *GZ = GSs(I_XYZ), *Gv = GSs(I_XVZ);
+        for (int k = KS + lane; k <= KE; k += 32) {
+            const size_t c = X3(k, i, j);
+            const double *DP = W.DPRES;
+            const double pgf = ((GZ[c + sJ] * DP[c + sJ] - GZ[c] * DP[c]) * ld(g.RFDY + j - 1)
+                                + (J23(k, i, j, I_XVW)
+                                       * 0.5 * (F2Hg(Gv, k, 1) * (DP[c + 1 + sJ] + DP[c + 1]) + F2Hg(Gv, k, 2) * (DP[c + sJ] + DP[c]))
+                                   - J23(k - 1, i, j, I_XVW)
+                                       * 0.5 * (F2Hg(Gv, k - 1, 1) * (DP[c + sJ] + DP[c]) + F2Hg(Gv, k - 1, 2) * (DP[c - 1 + sJ] + DP[c - 1])))
+                                      * ld(g.RCDZ + k - 1))
+                               * MAPFv(i, j, 2, I_XV);
+            const double sumx = MX[c] + MX[c - sI] + MX[c + sJ] + MX[c - sI + sJ];
+            const double cor = -0.125 * (a.CORIOLI[g.c2 + (size_t)(i - 1) + (size_t)g.IA * j] + a.CORIOLI[g.c2 + (size_t)(i - 1) + (size_t)g.IA * (j - 1)])
+                                   * (MX[c + sJ] + MX[c] + MX[c - sI + sJ] + MX[c - sI])
+                               - 0.25 * MAPFv(i, j, 1, I_XV) * MAPFv(i, j, 2, I_XV) * sumx
+                                   * (MY[c] * (1.0 / MAPFv(i, j, 2, I_UV) - 1.0 / MAPFv(i - 1, j, 2, I_UV)) * ld(g.RCDX + i - 1)
+                                      - 0.25 * (MX[c] + MX[c - sI] + MX[c + sJ] + MX[c - sI + sJ])
+                                            * (1.0 / MAPFv(i, j + 1, 1, I_XY) - 1.0 / MAPFv(i, j, 1, I_XY)) * ld(g.RFDY + j - 1))
+                                   * 2.0 / (DN[c] + DN[c + sJ]);
+            const double advcv = -(W.qZ[c] - W.qZ[c - 1] + W.qJ13[c] - W.qJ13[c - 1] + W.qJ23[c] - W.qJ23[c - 1]) * ld(g.RCDZ + k - 1);
+            const double advch = -((W.qX[c] - W.qX[c - sI]) * ld(g.RCDX + i - 1) + (W.qY[c] - W.qY[c - sJ]) * ld(g.RFDY + j - 1))
+                                 * MAPFv(i, j, 1, I_XV) * MAPFv(i, j, 2, I_XV);
+            const double div = use_div ? a.divdmp_coef / dt * ld(g.FDY + j - 1) * (a.DDIV[c + sJ] - a.DDIV[c]) : 0.0;
+            put_state(a, N3, 3, a.MOMY_RK, a.MOMY0, c,
+                      a.MOMY0[c] + dt * ((advcv + advch - pgf) / Gv[c] + cor + div + a.MOMY_t[c]), true);
+        }
+    });
+
+    // ---- rho*theta: fluxes :1328-1348 (mass fluxes as they are), update :1350-1371 ----
+    gcols(IS, IE, JS, JE, st, [=] __device__(int i, int j, int lane) {
+        const double *Gs = GSs(I_XYW), *nd = NDp(V_RHOT, DZIR), *col = W.POTT + X3(1, i, j);
+        for (int k = KS + lane; k <= KE - 1; k += 32) {
+            const size_t c = X3(k, i, j);
+            const double vel = W.mZ[c];
+            const double v = vel * zface<S>(vel, k, KS, KE, [&](int l) { return col[l - 1]; }) + Gs[c] * nd[c];
+            W.tZ[c] = v;
+            put_flux(a, N3, 3, c, v, true);
+        }
+        if (lane == 0) {
+            W.tZ[X3(KS - 1, i, j)] = 0.0;
+            W.tZ[X3(KE, i, j)] = 0.0;
+            put_flux(a, N3, 3, X3(KS - 1, i, j), 0.0, false);
+            put_flux(a, N3, 3, X3(KE, i, j), 0.0, true);
+        }
+    });
+    gcols(IS - 1, IE, JS, JE, st, [=] __device__(int i, int j, int lane) {
+        const double *Gs = GSs(I_UYZ), *nd = NDp(V_RHOT, DXIR);
+        for (int k = KS + lane; k <= KE; k += 32) {
+            const size_t c = X3(k, i, j);
+            const double vel = W.mX[c];
+            const double v = vel * hface<S>(vel, W.POTT + c, sI) + Gs[c] * nd[c];
+            W.tX[c] = v;
+            put_flux(a, N3, 4, c, v, i >= IS);
+        }
+    });
+    gcols(IS, IE, JS - 1, JE, st, [=] __device__(int i, int j, int lane) {
+        const double *Gs = GSs(I_XVZ), *nd = NDp(V_RHOT, DYIR);
+        for (int k = KS + lane; k <= KE; k += 32) {
+            const size_t c = X3(k, i, j);
+            const double vel = W.mY[c];
+            const double v = vel * hface<S>(vel, W.POTT + c, sJ) + Gs[c] * nd[c];
+            W.tY[c] = v;
+            put_flux(a, N3, 5, c, v, j >= JS);
+        }
+    });
+    gcols(IS, IE, JS, JE, st, [=] __device__(int i, int j, int lane) {
+        for (int k = KS + lane; k <= KE; k += 32) {
+            const size_t c = X3(k, i, j);
+            const double advcv = -(W.tZ[c] - W.tZ[c - 1]) * ld(g.RCDZ + k - 1);
+            const double advch = -(W.tX[c] - W.tX[c - sI]) * ld(g.RCDX + i - 1) - (W.tY[c] - W.tY[c - sJ]) * ld(g.RCDY + j - 1);
+            put_state(a, N3, 4, a.RHOT_RK, a.RHOT0, c,
+                      a.RHOT0[c] + dt * ((advcv + advch) * MAPFv(i, j, 1, I_XY) * MAPFv(i, j, 2, I_XY) / GS(k, i, j, I_XYZ) + a.RHOT_t[c]),
+                      true);
+        }
+    });
+#undef X3
+#undef GSs
+#undef J13s
+#undef J23s
+#undef GS
+#undef J13
+#undef J23
+#undef MAPFv
+#undef NDp
+#undef CDZv
+#undef F2Hg
+#undef DEN_UYZ
+#undef DEN_XVZ
+#undef AVG4_UV
+#undef AVG4_XV
+}
+
 cudaError_t launch_terrain_stage(const Grid &g, const StageArgsT<double> &a, const Metrics &M, const TerrainWork &W,
                                  int scheme, cudaStream_t st)
 {
@@ -1347,6 +1746,21 @@ cudaError_t launch_terrain_stage(const Grid &g, const StageArgsT<double> &a, con
     case CD2: terrain_stage<CD2>(g, a, M, W, st); break;
     case UD5: terrain_stage<UD5>(g, a, M, W, st); break;
     case CD6: terrain_stage<CD6>(g, a, M, W, st); break;
+    default: return cudaErrorInvalidValue;
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_terrain_heve_stage(const Grid &g, const StageArgsT<double> &a, const Metrics &M,
+                                      const TerrainWork &W, int scheme, cudaStream_t st)
+{
+    switch (scheme) {
+    case UD3: terrain_heve_stage<UD3>(g, a, M, W, st); break;
+    case CD4: terrain_heve_stage<CD4>(g, a, M, W, st); break;
+    case KOREN: terrain_heve_stage<KOREN>(g, a, M, W, st); break;
+    case CD2: terrain_heve_stage<CD2>(g, a, M, W, st); break;
+    case UD5: terrain_heve_stage<UD5>(g, a, M, W, st); break;
+    case CD6: terrain_heve_stage<CD6>(g, a, M, W, st); break;
     default: return cudaErrorInvalidValue;
     }
     return cudaGetLastError();

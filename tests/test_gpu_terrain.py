@@ -122,13 +122,44 @@ def test_terrain_rk3_bit_exact(lib, tinteg):
         assert helpers.same(xg[n], xs[n]), f"{n}: max rel diff {helpers.max_rel(xg[n], xs[n]):.3e}"
 
 
+@pytest.mark.parametrize("scheme", SCHEMES)
+@pytest.mark.parametrize("full", [False, True])
+def test_terrain_heve_stage_bit_exact(lib, scheme, full):
+    g = helpers.small_grid(IMAX=13, JMAX=9, KMAX=17, stretched=True, halo=helpers.halo_of(scheme))
+    c = helpers.small_case(g, scheme)
+    helpers.perturb_state(c)
+    a = with_terrain(helpers.short_inputs(c, dtrk=0.5, full=full), g)
+    o_ref = helpers.stage_outputs(g)
+    oracle.tstep_short_heve(g, scheme, o_ref, a)
+    o_gpu = helpers.stage_outputs(g)
+    lib.setup(g.index_dict(), scheme, scheme)
+    lib.ATMOS_DYN_Tstep_short_fvm_heve(**_stage_kw(a, o_gpu))
+    for n in o_ref:
+        assert helpers.same(o_gpu[n], o_ref[n]), f"{n}: max rel diff {helpers.max_rel(o_gpu[n], o_ref[n]):.3e}"
+
+
+@pytest.mark.parametrize("scheme", ["CD4", "UD5"])
+def test_terrain_heve_rk4_bit_exact(lib, scheme):
+    g = helpers.small_grid(IMAX=14, JMAX=11, KMAX=18, stretched=True, halo=helpers.halo_of(scheme))
+    a, xs = _short_inputs(g, scheme)
+    xg = {n: v.copy(order="F") for n, v in xs.items()}
+    oracle.tinteg_short_rk4(g, scheme, xs, dict(a, dt=0.1), short="HEVE")
+    lib.setup(g.index_dict(), scheme, scheme)
+    lib.short_type("HEVE")
+    lib.ATMOS_DYN_Tinteg_short_rk4(**a, **xg, **SHORT_KW, dt=0.1)
+    for n in xs:
+        assert helpers.same(xg[n], xs[n]), f"{n}: max rel diff {helpers.max_rel(xg[n], xs[n]):.3e}"
+
+
 def test_flat_only_entries_refuse_terrain(lib):
     g = helpers.small_grid()
     c = helpers.small_case(g)
     a = with_terrain(helpers.short_inputs(c, full=False), g)
     lib.setup(g.index_dict(), "UD3", "UD3")
-    with pytest.raises(hevi.HeviError, match="flat terrain|not supported") as e:
-        lib.ATMOS_DYN_Tstep_short_fvm_heve(**_stage_kw(a, helpers.stage_outputs(g)))
+    with pytest.raises(hevi.HeviError, match="not supported") as e:
+        lib.ATMOS_DYN_divergence(DDIV=g.zeros(), MOMZ=c.state["MOMZ"], MOMX=c.state["MOMX"], MOMY=c.state["MOMY"],
+                                 GSQRT=a["GSQRT"], J13G=a["J13G"], J23G=a["J23G"], J33G=1.0, MAPF=a["MAPF"],
+                                 RCDZ=g.RCDZ, RCDX=g.RCDX, RCDY=g.RCDY, RFDZ=g.RFDZ, FDZ=g.FDZ)
     assert e.value.code == 5
     # the flat-terrain stage still runs after the refusal
     a_flat = helpers.short_inputs(c, full=False)
