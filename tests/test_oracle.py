@@ -301,6 +301,62 @@ def test_rk3_conserve(tinteg):
     assert abs(oracle.domain_sum(g, st["RHOT"]) - t0) / t0 < 1e-13
 
 
+def _periodic_metrics(g, seed, amp=0.05):
+    """Seeded terrain-following metrics, periodic across the lateral halo."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    GS = np.asfortranarray(1.0 + amp * rng.uniform(-1, 1, size=g.shape + (7,)))
+    J13 = np.asfortranarray(amp * rng.uniform(-1, 1, size=g.shape + (7,)))
+    J23 = np.asfortranarray(amp * rng.uniform(-1, 1, size=g.shape + (7,)))
+    for arr in (GS, J13, J23):
+        for q in range(7):
+            mkinit.periodic_fill(arr[..., q], g)
+    MAPF = np.asfortranarray(1.0 + amp * rng.uniform(-1, 1, size=(g.IA, g.JA, 2, 4)))
+    for a in range(2):
+        for b in range(4):
+            mkinit.periodic_fill(MAPF[None, :, :, a, b], g)
+    return GS, J13, J23, MAPF
+
+
+@pytest.mark.parametrize("short", ["HEVI", "HEVE"])
+def test_terrain_conserve(short):
+    """test_conserve (test_atmos_dyn.f90:456-592) with terrain-following
+    metrics: the total mass sum(DENS * GSQRT / (MAPF_1 * MAPF_2) * volume),
+    the quantity the flux form of Sr (tstep_short_fvm_hevi.F90:443-479)
+    telescopes, is conserved to round-off by the oracle's short steps."""
+    g = helpers.small_grid(10, 8, 14, stretched=True)
+    c = mkinit.make_case("conserve terrain", g, "CD4", "CD4", dt=0.2 if short == "HEVI" else 0.05)
+    k, i, j = np.meshgrid(np.arange(1, g.KA + 1), np.arange(1, g.IA + 1), np.arange(1, g.JA + 1), indexing="ij")
+    st = c.state
+    st["MOMZ"][...] = (k + i + j) * 0.01
+    st["MOMX"][...] = (k * 2 + i + j) * 0.01
+    st["MOMY"][...] = (k + i * 2 + j) * 0.01
+    st["DENS"][...] = c.ref["REF_dens"] + (k * 2 + i * 2 + j) * 1e-4
+    st["RHOT"][...] = st["DENS"] * (300.0 + (k + i + j * 2) * 0.01)
+    for n in STATE:
+        mkinit.periodic_fill(st[n], g)
+    mkinit.vertical_fill(st, g)
+    GS, J13, J23, MAPF = _periodic_metrics(g, 9)
+    w = GS[..., 0] / (MAPF[:, :, 0, 0] * MAPF[:, :, 1, 0])[None, :, :]
+
+    def total(x):
+        return oracle.domain_sum(g, np.asfortranarray(x * w))
+
+    m0, t0 = total(st["DENS"]), total(st["RHOT"])
+    a = helpers.short_inputs(c, full=False)
+    for kk in ("DENS0", "MOMZ0", "MOMX0", "MOMY0", "RHOT0", "DENS", "MOMZ", "MOMX", "MOMY", "RHOT", "dtrk"):
+        a.pop(kk)
+    a.update(GSQRT=GS, J13G=J13, J23G=J23, MAPF=MAPF)
+    x = {n: st[n] for n in STATE}
+    x["mflx_hi"], x["tflx_hi"] = g.zeros(3), g.zeros(3)
+    for _ in range(3):
+        oracle.tinteg_short_rk4(g, c.scheme, x, dict(a, dt=c.dt), short=short)
+        for n in STATE:
+            mkinit.periodic_fill(st[n], g)
+        mkinit.vertical_fill(st, g)
+    assert abs(total(st["DENS"]) - m0) / m0 < 1e-13
+    assert abs(total(st["RHOT"]) - t0) / t0 < 1e-13
+
+
 @pytest.mark.parametrize("fct", [False, True])
 def test_koren_tracer_keeps_uniform_tracer(fct):
     """test_cwc with the UD3KOREN1993 tracer flux (the reference's default
