@@ -187,6 +187,23 @@ int ATMOS_DYN_Tinteg_short_rk4_b200_dev(SCALE_HEVI_TINTEG_SHORT_ARGS);
 int ATMOS_DYN_Tinteg_short_rk3_b200(SCALE_HEVI_TINTEG_SHORT_ARGS);
 int ATMOS_DYN_Tinteg_short_rk3_b200_dev(SCALE_HEVI_TINTEG_SHORT_ARGS);
 
+/* ---------------------------------------------------------------------------
+ * Halo exchange hook for a domain decomposed over ranks. Replaces the
+ * periodic self-exchange of COMM_vars8/COMM_wait
+ * (scale_comm_cartesC.F90:1600-2043, 2787-3023) that the library does on one
+ * rank. When fn is set, every lateral halo fill of the short step and the
+ * large step (the RK stage buffers, the state, num_diff, mflx_hi and the
+ * tracers) calls fn instead: fn receives the device addresses of nfields
+ * (KA,IA,JA) fields with elements of elem_bytes (8 or 4) and must have filled
+ * their lateral halos (IHALO columns, JHALO rows, corners included) when it
+ * returns 0 (a nonzero return is reported as an error). The library's stream is idle during the call.
+ * NULL restores the periodic fill. One domain only; the filter at ND_ORDER > 1
+ * and the FCT tracer limiter, whose inner halo fills are not routed through
+ * the hook, return SCALE_HEVI_ERR_UNSUPPORTED while it is set.
+ * ------------------------------------------------------------------------- */
+typedef int (*scale_hevi_halo_fn)(void *const *fields, int nfields, int elem_bytes, void *user);
+int scale_hevi_set_halo_exchange(scale_hevi_halo_fn fn, void *user);
+
 /* Registers the short integrator of the large step and the RK3 entries, as
  * ATMOS_DYN_Tinteg_short_setup does for ATMOS_DYN_TINTEG_SHORT_TYPE
  * (scale_atmos_dyn_tinteg_short.F90:146-159): "RK4" (the default after

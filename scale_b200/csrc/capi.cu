@@ -32,6 +32,8 @@ struct Ctx {
     int scheme = UD3, scheme_tracer = UD3;
     int short_type = 0;  // the registered short step of the RK4 and large-step entries: 0 HEVI, 1 HEVE
     int tinteg_type = 0; // the short integrator of the large step: 0 RK4, 1 RK3 (Heun), 2 RK3WS2002
+    scale_hevi_halo_fn halo_fn = nullptr; // lateral halo exchange of a decomposed domain (null: periodic)
+    void *halo_user = nullptr;
     size_t N3 = 0;   // points of one 3-D field (all members)
     // ensemble members sharing the pooled arrays (one entry for a single domain)
     std::vector<MemberGeom> members;
@@ -442,6 +444,14 @@ int prepare_nd(const double *CDZ, const double *CDX, const double *CDY, const do
 template <typename T>
 int halo(T *const *f, int n)
 {
+    if (C.halo_fn) {
+        // the exchange of a decomposed domain, with the library's stream idle
+        CU(cudaStreamSynchronize(C.stream));
+        std::vector<void *> p(f, f + n);
+        const int rc = C.halo_fn(p.data(), n, (int)sizeof(T), C.halo_user);
+        if (rc) return fail(SCALE_HEVI_ERR_CUDA, "the halo exchange hook returned %d", rc);
+        return SCALE_HEVI_OK;
+    }
     C.launches += (n + 15) / 16;
     return timed("halo", [&] {
         periodic_halo(C.g, mem(), f, n, C.stream);
@@ -675,6 +685,7 @@ int run_numfilter(R *num_diff, const double *DENS, const double *MOMZ, const dou
         if (sizeof(R) != sizeof(double))
             return fail(SCALE_HEVI_ERR_UNSUPPORTED, "ND_ORDER > 1 is supported on the FP64 path only");
         if (C.members.size() > 1) return fail(SCALE_HEVI_ERR_UNSUPPORTED, "ND_ORDER > 1 is not available for an ensemble");
+        if (C.halo_fn) return fail(SCALE_HEVI_ERR_UNSUPPORTED, "ND_ORDER > 1 is not available with a halo exchange hook");
         if (!C.ndw) CK(dalloc(&C.ndw, 30 * C.N3));
         NdArgs ah{reinterpret_cast<double *>(num_diff), DENS, MOMZ, MOMX, MOMY, RHOT, REF_dens, REF_pott,
                   reinterpret_cast<double *>(phi)};
@@ -716,6 +727,8 @@ int run_divergence(double *DDIV, const double *MOMZ, const double *MOMX, const d
 int run_tracer_rk3(double *QTRC, const double *QTRC0, const double *RHOQ_t, const double *DENS0, const double *DENS,
                    const double *mflx, const double *ndq, double dtl, bool fct, bool along)
 {
+    if (fct && C.halo_fn)
+        return fail(SCALE_HEVI_ERR_UNSUPPORTED, "the FCT tracer limiter is not available with a halo exchange hook");
     TracerArgs a{};
     a.QTRC0 = QTRC0; a.RHOQ_t = RHOQ_t; a.DENS0 = DENS0; a.DENS = DENS; a.mflx = mflx; a.ndq = ndq;
     a.phi_lo = C.tr + 2 * C.N3; a.anti = C.tr + 3 * C.N3; a.rjp = C.tr + 6 * C.N3; a.rjm = C.tr + 7 * C.N3;
@@ -879,6 +892,15 @@ int scale_hevi_short_type(const char *type)
     if (n == "HEVI" || n == "FVM-HEVI") { C.short_type = 0; return SCALE_HEVI_OK; }
     if (n == "HEVE" || n == "FVM-HEVE") { C.short_type = 1; return SCALE_HEVI_OK; }
     return fail(SCALE_HEVI_ERR_UNSUPPORTED, "short-step type '%s' is not supported (HEVI, HEVE)", n.c_str());
+}
+
+int scale_hevi_set_halo_exchange(scale_hevi_halo_fn fn, void *user)
+{
+    CK(need_setup());
+    if (fn) CK(need_single("a halo exchange hook"));
+    C.halo_fn = fn;
+    C.halo_user = user;
+    return SCALE_HEVI_OK;
 }
 
 int scale_hevi_tinteg_short_type(const char *type)
@@ -1269,6 +1291,8 @@ int ATMOS_DYN_Tstep_tracer_fvm_heve_b200_dev(SCALE_HEVI_TSTEP_TRACER_ARGS)
     a.phi_lo = C.tr + 2 * C.N3; a.anti = C.tr + 3 * C.N3; a.rjp = C.tr + 6 * C.N3; a.rjm = C.tr + 7 * C.N3;
     a.along_stream = *FLAG_FCT_ALONG_STREAM ? 1 : 0;
     const bool fct = *FLAG_FCT_TRACER != 0;
+    if (fct && C.halo_fn)
+        return fail(SCALE_HEVI_ERR_UNSUPPORTED, "the FCT tracer limiter is not available with a halo exchange hook");
     CU(launch_tracer_stage(C.g, a, C.scheme_tracer, fct, C.stream));
     C.launches += fct ? 4 : 1;
     return SCALE_HEVI_OK;

@@ -66,6 +66,8 @@ def header_functions() -> dict[str, list[str]]:
 
 _lib = None
 _sig = None
+# int (*)(void *const *fields, int nfields, int elem_bytes, void *user)
+HALO_FN = C.CFUNCTYPE(C.c_int, C.POINTER(C.c_void_p), C.c_int, C.c_int, C.c_void_p)
 
 
 def load(path: str | os.PathLike | None = None) -> C.CDLL:
@@ -96,6 +98,8 @@ def load(path: str | os.PathLike | None = None) -> C.CDLL:
             f.argtypes = [C.c_int, C.c_int]
         elif name in ("scale_hevi_short_type", "scale_hevi_tinteg_short_type"):
             f.argtypes = [C.c_char_p]
+        elif name == "scale_hevi_set_halo_exchange":
+            f.argtypes = [HALO_FN, C.c_void_p]
         elif name == "scale_hevi_stage_autotune":
             f.argtypes = [C.c_int]
         elif name == "scale_hevi_stage_shape_get":
@@ -230,6 +234,34 @@ def tinteg_short_type(name: str = "RK4") -> None:
     """The short integrator the large step and the RK3 entries run: "RK4",
     "RK3" (Heun) or "RK3WS2002" (ATMOS_DYN_Tinteg_short_setup)."""
     _check(load().scale_hevi_tinteg_short_type(name.encode()))
+
+
+_halo_cb = None  # the registered callback object, kept alive while set
+
+
+def set_halo_exchange(fn) -> None:
+    """Register fn(ptrs, nfields, elem_bytes) -> None as the lateral halo
+    exchange of every halo fill (None restores the periodic fill); ptrs are
+    the device addresses of the (KA,IA,JA) fields (scale_hevi_set_halo_exchange)."""
+    global _halo_cb
+    if fn is None:
+        _check(load().scale_hevi_set_halo_exchange(HALO_FN(), None))
+        _halo_cb = None  # finalize() clears the library's hook as well
+        return
+
+    def tramp(fields, nfields, elem_bytes, user):
+        try:
+            fn([fields[q] for q in range(nfields)], nfields, elem_bytes)
+            return 0
+        except Exception:  # reported to the library as a failed exchange
+            import traceback
+
+            traceback.print_exc()
+            return 1
+
+    cb = HALO_FN(tramp)
+    _check(load().scale_hevi_set_halo_exchange(cb, None))
+    _halo_cb = cb
 
 
 def stage_shape(tile_x: int = 0, raster: int = 0) -> None:
