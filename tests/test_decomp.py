@@ -110,3 +110,122 @@ def test_layout_and_neighbours():
         Decomposition(15, 12, 4, 3, 0)
     with pytest.raises(ValueError):
         Decomposition(16, 12, 4, 3, 12)
+
+
+# ---- the dynamics on a decomposed domain: oracle RK4 stages per subdomain ----
+STATE = ("DENS", "MOMZ", "MOMX", "MOMY", "RHOT")
+
+
+def _local_inputs(dec, g_glob, a):
+    """This rank's block of every input array (3-D and 2-D by its lateral
+    block, 1-D lateral vectors by its slice, the rest as they are)."""
+    H = dec.halo
+    isl = slice(dec.i0, dec.i0 + dec.imax + 2 * H)
+    jsl = slice(dec.j0, dec.j0 + dec.jmax + 2 * H)
+    out = {}
+    for k, v in a.items():
+        if not isinstance(v, np.ndarray):
+            out[k] = v
+        elif v.ndim >= 3 and v.shape[:3] == g_glob.shape:
+            out[k] = np.asfortranarray(v[:, isl, jsl])
+        elif v.ndim >= 2 and v.shape[:2] == (g_glob.IA, g_glob.JA):
+            out[k] = np.asfortranarray(v[isl, jsl])
+        elif v.ndim == 1 and len(v) == g_glob.IA and k.endswith("X"):
+            out[k] = v[isl].copy()
+        elif v.ndim == 1 and len(v) == g_glob.JA and k.endswith("Y"):
+            out[k] = v[jsl].copy()
+        else:
+            out[k] = v
+    return out
+
+
+def _rk4_decomposed(dec, g_loc, x, a, dt):
+    """ATMOS_DYN_tinteg_short_rk4 (rk4.F90:376-650) with the oracle's stage on
+    this rank's subdomain and dec.exchange in place of COMM_vars8."""
+    import helpers
+    import oracle
+
+    x0 = {n: v.copy(order="F") for n, v in x.items()}
+    rk, fl, cur = [], [], {n: x0[n] for n in STATE}
+    for s, dtrk in enumerate((dt / 2.0, dt / 2.0, dt, dt)):
+        o = helpers.stage_outputs(g_loc, 0.0)
+        args = dict(a, dtrk=dtrk)
+        args.update({n + "0": x0[n] for n in STATE})
+        args.update(cur)
+        if s == 3:
+            o["mflx_hi"] = x0["mflx_hi"].copy(order="F")
+            o["tflx_hi"] = x0["tflx_hi"].copy(order="F")
+        oracle.tstep_short(g_loc, "CD4", o, args)
+        st = {n: o[n + "_RK"] for n in STATE}
+        if s < 3:
+            t = [torch.from_numpy(np.ravel(st[n], order="F").copy()) for n in STATE]
+            dec.exchange(t)
+            st = {n: t[q].numpy().reshape(g_loc.shape, order="F").copy(order="F") for q, n in enumerate(STATE)}
+        rk.append(st)
+        fl.append((o["mflx_hi"], o["tflx_hi"]))
+        cur = st
+    g = g_loc
+    sl = (slice(g.KS - 1, g.KE), slice(g.IS - 1, g.IE), slice(g.JS - 1, g.JE))
+    for n in STATE:
+        ks = slice(g.KS - 1, g.KE - 1) if n == "MOMZ" else sl[0]
+        comb = (rk[0][n] * 2.0 + rk[1][n] * 4.0 + rk[2][n] * 2.0 + rk[3][n] - x0[n] * 3.0) / 6.0
+        x[n][ks, sl[1], sl[2]] = comb[ks, sl[1], sl[2]]
+    for f, name in enumerate(("mflx_hi", "tflx_hi")):
+        comb = (fl[0][f] + fl[1][f] * 2.0 + fl[2][f] * 2.0 + fl[3][f]) / 6.0
+        x[name][sl] = comb[sl]
+    return x
+
+
+def _dyn_worker(rank, world, port, nx, ny, out):
+    import datetime
+
+    import torch.distributed as dist
+
+    sys.path.insert(0, str(ROOT / "tests"))
+    import helpers
+    import oracle
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=120))
+    try:
+        g = helpers.small_grid(IMAX=12, JMAX=10, KMAX=12)
+        c = helpers.small_case(g, "CD4")
+        helpers.perturb_state(c)
+        a = helpers.short_inputs(c, full=True)
+        for k in ("DENS0", "MOMZ0", "MOMX0", "MOMY0", "RHOT0", "DENS", "MOMZ", "MOMX", "MOMY", "RHOT", "dtrk"):
+            a.pop(k)
+        xg = {n: c.state[n].copy(order="F") for n in STATE}
+        xg["mflx_hi"], xg["tflx_hi"] = g.zeros(3), g.zeros(3)
+        dec = Decomposition(g.IMAX, g.JMAX, nx, ny, rank, g.halo)
+        g_loc = helpers.small_grid(IMAX=dec.imax, JMAX=dec.jmax, KMAX=12)
+        xl = {n: np.asfortranarray(v[:, dec.i0: dec.i0 + dec.imax + 4, dec.j0: dec.j0 + dec.jmax + 4])
+              for n, v in xg.items()}
+        al = _local_inputs(dec, g, a)
+        oracle.tinteg_short_rk4(g, "CD4", xg, dict(a, dt=1.0))  # the global run
+        _rk4_decomposed(dec, g_loc, xl, al, 1.0)
+        ok = True
+        for n in xl:
+            glob = xg[n][:, dec.i0 + 2: dec.i0 + 2 + dec.imax, dec.j0 + 2: dec.j0 + 2 + dec.jmax]
+            ok &= bool(np.array_equal(xl[n][:, 2:-2, 2:-2], glob))
+        out[rank] = ok
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+def test_decomposed_rk4_matches_global_run():
+    """The RK4 short step on a 2x1 decomposition, each rank running the
+    oracle's stage on its subdomain and exchanging the stage buffers, equals
+    the global run on every rank's interior, bit for bit."""
+    world, nx, ny = 2, 2, 1
+    ctx = mp.get_context("spawn")
+    with ctx.Manager() as m:
+        out = m.dict()
+        port = _free_port()
+        procs = [ctx.Process(target=_dyn_worker, args=(r, world, port, nx, ny, out)) for r in range(world)]
+        for p in procs:
+            p.start()
+        for p in procs:
+            p.join(300)
+            assert p.exitcode == 0
+        assert all(out[r] for r in range(world)), dict(out)
