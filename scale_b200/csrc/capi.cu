@@ -1249,16 +1249,25 @@ int ATMOS_DYN_numfilter_coef_b200(SCALE_HEVI_NUMFILTER_ARGS)
 }
 
 // ---- tracer ------------------------------------------------------------------
-static int tracer_common_checks(const double *GSQRT, const double *MAPF, bool on_device)
+// Metrics of the tracer entries: GSQRT (KA,IA,JA,7) and the (IA,JA,2) MAPF slice
+// at (x,y). Flat ones (GSQRT = 1, MAPF = 1) take the plain factors; others
+// enter the tracer kernels (TracerArgs::GS/MAPF), on the device. *dGS/*dMAPF
+// receive the device arrays of non-flat metrics (null on flat terrain); host
+// arrays are copied to the device first.
+static int tracer_metrics(const double *GSQRT, const double *MAPF, bool on_device, const double **dGS,
+                          const double **dMAPF)
 {
     CK(need_single("tracer advection"));
-    CK(check_flat(GSQRT, nullptr, nullptr, nullptr, on_device));
-    // MAPF here is the (IA,JA,2) slice at (x,y)
+    C.terrain = false;
+    *dGS = *dMAPF = nullptr;
+    bool flat_g = true, flat_m = true;
+    if (GSQRT) CK(metrics_flat(GSQRT, nullptr, nullptr, nullptr, on_device, &flat_g));
     if (MAPF) {
         std::vector<const void *> key = {MAPF, (const void *)(size_t)(on_device ? 3 : 2)};
-        bool ok = false;
-        for (auto &k : C.flat_ok) ok |= (k == key);
-        if (!ok) {
+        bool seen = false;
+        for (auto &k : C.flat_ok) if (k == key) { seen = true; flat_m = true; }
+        for (auto &k : C.nonflat) if (k == key) { seen = true; flat_m = false; }
+        if (!seen) {
             const size_t n = (size_t)C.g.IA * C.g.JA * 2;
             unsigned long long bad = 0;
             if (on_device) {
@@ -1270,17 +1279,30 @@ static int tracer_common_checks(const double *GSQRT, const double *MAPF, bool on
             } else {
                 for (size_t q = 0; q < n; ++q) bad += MAPF[q] != 1.0;
             }
-            if (bad) return fail(SCALE_HEVI_ERR_UNSUPPORTED, "map factors other than 1 are not supported");
-            C.flat_ok.push_back(key);
+            flat_m = bad == 0;
+            (flat_m ? C.flat_ok : C.nonflat).push_back(key);
         }
     }
     if (!C.tr) CK(dalloc(&C.tr, 8 * C.N3));
+    if (flat_g && flat_m) return SCALE_HEVI_OK;
+    if (!GSQRT || !MAPF) return fail(SCALE_HEVI_ERR_ARG, "terrain-following metrics need GSQRT and MAPF");
+    if (on_device) {
+        *dGS = GSQRT;
+        *dMAPF = MAPF;
+    } else {
+        double *g7, *mp;
+        CK(h2d("GSQRT", GSQRT, 7 * C.N3, &g7));
+        CK(h2d("MAPF_XY", MAPF, C.N2 * 2, &mp));
+        *dGS = g7;
+        *dMAPF = mp;
+    }
     return SCALE_HEVI_OK;
 }
 
 int ATMOS_DYN_Tstep_tracer_fvm_heve_b200_dev(SCALE_HEVI_TSTEP_TRACER_ARGS)
 {
-    CK(tracer_common_checks(GSQRT, MAPF, true));
+    const double *dGS, *dMAPF;
+    CK(tracer_metrics(GSQRT, MAPF, true, &dGS, &dMAPF));
     // the 1-D vectors this step needs; the others keep their last values
     std::vector<double> one(C.g.KA > C.g.IA ? (C.g.KA > C.g.JA ? C.g.KA : C.g.JA) : (C.g.IA > C.g.JA ? C.g.IA : C.g.JA), 1.0);
     CK(prepare_tables(CDZ, one.data(), RCDZ, one.data(), one.data(), RCDX, one.data(), one.data(), RCDY, one.data(),
@@ -1290,6 +1312,8 @@ int ATMOS_DYN_Tstep_tracer_fvm_heve_b200_dev(SCALE_HEVI_TSTEP_TRACER_ARGS)
     a.dens_mode = 0; a.mflx = mflx_hi; a.ndq = num_diff; a.dtl = *dtl;
     a.phi_lo = C.tr + 2 * C.N3; a.anti = C.tr + 3 * C.N3; a.rjp = C.tr + 6 * C.N3; a.rjm = C.tr + 7 * C.N3;
     a.along_stream = *FLAG_FCT_ALONG_STREAM ? 1 : 0;
+    a.GS = dGS;
+    a.MAPF = dMAPF;
     const bool fct = *FLAG_FCT_TRACER != 0;
     if (fct && C.halo_fn)
         return fail(SCALE_HEVI_ERR_UNSUPPORTED, "the FCT tracer limiter is not available with a halo exchange hook");
@@ -1300,7 +1324,8 @@ int ATMOS_DYN_Tstep_tracer_fvm_heve_b200_dev(SCALE_HEVI_TSTEP_TRACER_ARGS)
 
 int ATMOS_DYN_Tstep_tracer_fvm_heve_b200(SCALE_HEVI_TSTEP_TRACER_ARGS)
 {
-    CK(tracer_common_checks(GSQRT, MAPF, false));
+    const double *dGS, *dMAPF;
+    CK(tracer_metrics(GSQRT, MAPF, false, &dGS, &dMAPF));
     const size_t N3 = n3();
     double *qo, *q, *q0, *rq, *d0, *d, *mf, *nd = nullptr;
     CK(h2d("q_out", QTRCo, N3, &qo));
@@ -1311,7 +1336,7 @@ int ATMOS_DYN_Tstep_tracer_fvm_heve_b200(SCALE_HEVI_TSTEP_TRACER_ARGS)
     CK(h2d("DENS", DENS, N3, &d));
     CK(h2d("mflx", mflx_hi, 3 * N3, &mf));
     if (num_diff) CK(h2d("ndq", num_diff, 3 * N3, &nd));
-    int rc = ATMOS_DYN_Tstep_tracer_fvm_heve_b200_dev(qo, q, (QTRC0 == QTRCo) ? qo : q0, rq, d0, d, mf, nd, nullptr, nullptr,
+    int rc = ATMOS_DYN_Tstep_tracer_fvm_heve_b200_dev(qo, q, (QTRC0 == QTRCo) ? qo : q0, rq, d0, d, mf, nd, dGS, dMAPF,
                                                       CDZ, RCDZ, RCDX, RCDY, dtl, FLAG_FCT_TRACER, FLAG_FCT_ALONG_STREAM);
     if (rc) return rc;
     CK(d2h(QTRCo, qo, N3));
@@ -1322,7 +1347,13 @@ int ATMOS_DYN_Tstep_tracer_fvm_heve_b200(SCALE_HEVI_TSTEP_TRACER_ARGS)
 int ATMOS_DYN_Tinteg_tracer_rk3_b200_dev(SCALE_HEVI_TINTEG_TRACER_ARGS)
 {
     CK(check_bnd(BND_W, BND_E, BND_S, BND_N));
-    CK(tracer_common_checks(GSQRT, MAPF, true));
+    const double *dGS, *dMAPF;
+    CK(tracer_metrics(GSQRT, MAPF, true, &dGS, &dMAPF));
+    if (dGS) { // run_tracer_rk3 takes the metrics of the call from the library state
+        C.terrain = true;
+        C.tm.GSQRT = dGS;
+        C.tm.MAPF = dMAPF;
+    }
     std::vector<double> one(C.g.KA > C.g.IA ? (C.g.KA > C.g.JA ? C.g.KA : C.g.JA) : (C.g.IA > C.g.JA ? C.g.IA : C.g.JA), 1.0);
     CK(prepare_tables(CDZ, one.data(), RCDZ, one.data(), one.data(), RCDX, one.data(), one.data(), RCDY, one.data(),
                       nullptr, nullptr, nullptr));
@@ -1333,7 +1364,8 @@ int ATMOS_DYN_Tinteg_tracer_rk3_b200_dev(SCALE_HEVI_TINTEG_TRACER_ARGS)
 int ATMOS_DYN_Tinteg_tracer_rk3_b200(SCALE_HEVI_TINTEG_TRACER_ARGS)
 {
     CK(check_bnd(BND_W, BND_E, BND_S, BND_N));
-    CK(tracer_common_checks(GSQRT, MAPF, false));
+    const double *dGS, *dMAPF;
+    CK(tracer_metrics(GSQRT, MAPF, false, &dGS, &dMAPF));
     const size_t N3 = n3();
     double *q, *q0, *rq, *d0, *d, *mf, *nd = nullptr;
     CK(h2d("q_out", QTRC, N3, &q));
@@ -1343,7 +1375,7 @@ int ATMOS_DYN_Tinteg_tracer_rk3_b200(SCALE_HEVI_TINTEG_TRACER_ARGS)
     CK(h2d("DENS", DENS, N3, &d));
     CK(h2d("mflx", mflx_hi, 3 * N3, &mf));
     if (num_diff) CK(h2d("ndq", num_diff, 3 * N3, &nd));
-    int rc = ATMOS_DYN_Tinteg_tracer_rk3_b200_dev(q, (QTRC0 == QTRC) ? q : q0, rq, d0, d, mf, nd, nullptr, nullptr,
+    int rc = ATMOS_DYN_Tinteg_tracer_rk3_b200_dev(q, (QTRC0 == QTRC) ? q : q0, rq, d0, d, mf, nd, dGS, dMAPF,
                                                   CDZ, RCDZ, RCDX, RCDY, BND_W, BND_E, BND_S, BND_N, dtl,
                                                   FLAG_FCT_TRACER, FLAG_FCT_ALONG_STREAM);
     if (rc) return rc;

@@ -151,6 +151,53 @@ def test_terrain_heve_rk4_bit_exact(lib, scheme):
         assert helpers.same(xg[n], xs[n]), f"{n}: max rel diff {helpers.max_rel(xg[n], xs[n]):.3e}"
 
 
+@pytest.mark.parametrize("scheme", ["UD3", "UD3KOREN1993", "UD5"])
+@pytest.mark.parametrize("fct,along", [(False, True), (True, True), (True, False)])
+def test_terrain_tracer_step_bit_exact(lib, scheme, fct, along):
+    """ATMOS_DYN_Tstep_tracer_fvm_heve with GSQRT and the (IA,JA,2) MAPF slice
+    (tstep_tracer_fvm_heve.F90:72-240 and the limiter's metric factors,
+    common.F90:2051-2120), with a non-zero tracer num_diff."""
+    from test_gpu_parity import _tracer_inputs
+
+    g = helpers.small_grid(IMAX=12, JMAX=14, KMAX=16, halo=helpers.halo_of(scheme))
+    c = helpers.small_case(g)
+    helpers.perturb_state(c)
+    q0, q, d0, d, mflx, rhoq, _, _ = _tracer_inputs(g, c)
+    m = with_terrain(dict(), g, seed=23)
+    GS, MAPF = m["GSQRT"], np.asfortranarray(m["MAPF"][..., 0])
+    ndq = np.asfortranarray(1e-4 * np.random.Generator(np.random.PCG64(3)).standard_normal(g.shape + (3,)))
+    ref = np.full(g.shape, np.nan, order="F")
+    oracle.tstep_tracer(g, scheme, ref, q, q0, rhoq, d0, d, mflx, ndq, GS, MAPF, 2.5, fct, along)
+    got = np.full(g.shape, np.nan, order="F")
+    lib.setup(g.index_dict(), scheme, scheme)
+    lib.ATMOS_DYN_Tstep_tracer_fvm_heve(QTRCo=got, QTRC=q, QTRC0=q0, RHOQ_t=rhoq, DENS0=d0, DENS=d, mflx_hi=mflx,
+                                        num_diff=ndq, GSQRT=GS, MAPF=MAPF, CDZ=g.CDZ, RCDZ=g.RCDZ,
+                                        RCDX=g.RCDX, RCDY=g.RCDY, dtl=2.5, FLAG_FCT_TRACER=fct,
+                                        FLAG_FCT_ALONG_STREAM=along)
+    assert helpers.same(got, ref), f"max rel diff {helpers.max_rel(got, ref):.3e}"
+
+
+@pytest.mark.parametrize("fct", [False, True])
+def test_terrain_tracer_rk3_bit_exact(lib, fct):
+    from test_gpu_parity import _tracer_inputs
+
+    g = helpers.small_grid(IMAX=10, JMAX=12, KMAX=18, stretched=True)
+    c = helpers.small_case(g)
+    helpers.perturb_state(c)
+    q0, q, d0, d, mflx, rhoq, _, _ = _tracer_inputs(g, c)
+    m = with_terrain(dict(), g, seed=29)
+    GS, MAPF = m["GSQRT"], np.asfortranarray(m["MAPF"][..., 0])
+    ref = q0.copy(order="F")
+    oracle.tinteg_tracer_rk3(g, "UD3KOREN1993", ref, ref, rhoq, d0, d, mflx, g.zeros(3), GS, MAPF, 5.0, fct, True)
+    got = q0.copy(order="F")
+    lib.setup(g.index_dict(), "UD3", "UD3KOREN1993")
+    lib.ATMOS_DYN_Tinteg_tracer_rk3(QTRC=got, QTRC0=got, RHOQ_t=rhoq, DENS0=d0, DENS=d, mflx_hi=mflx,
+                                    num_diff=g.zeros(3), GSQRT=GS, MAPF=MAPF, CDZ=g.CDZ, RCDZ=g.RCDZ, RCDX=g.RCDX,
+                                    RCDY=g.RCDY, BND_W=False, BND_E=False, BND_S=False, BND_N=False, dtl=5.0,
+                                    FLAG_FCT_TRACER=fct, FLAG_FCT_ALONG_STREAM=True)
+    assert helpers.same(got, ref), f"max rel diff {helpers.max_rel(got, ref):.3e}"
+
+
 def test_flat_only_entries_refuse_terrain(lib):
     g = helpers.small_grid()
     c = helpers.small_case(g)
