@@ -23,9 +23,10 @@
  * Supported configuration (checked, otherwise SCALE_HEVI_ERR_UNSUPPORTED):
  * periodic lateral boundaries (BND_* = .false.); terrain-following metrics
  * (GSQRT, J13G, J23G, MAPF not those of flat terrain, classified once per set
- * of metric arrays) in the FP64 HEVI and HEVE stage, RK4, RK3, large-step and
- * tracer entries of one domain, where they select the general-metric stage
- * (PHI is read) or the tracer kernels' metric factors;
+ * of metric arrays) in the FP64 HEVI and HEVE stage, RK4, RK3, large-step,
+ * tracer and divergence entries of one domain, where they select the
+ * general-metric stage (PHI is read) or the metric forms of the tracer and
+ * divergence kernels;
  * flat terrain (GSQRT = 1, J13G = J23G = 0, MAPF = 1) in every other entry; the default
  * IBLOCK/JBLOCK (whole domain), flux schemes "UD3", "CD4", "CD2",
  * "UD3KOREN1993", "UD5" and "CD6", ND_ORDER >= 1 (above 1 on the FP64 path of

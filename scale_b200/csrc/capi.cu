@@ -1388,10 +1388,24 @@ int ATMOS_DYN_Tinteg_tracer_rk3_b200(SCALE_HEVI_TINTEG_TRACER_ARGS)
 // ---- divergence ------------------------------------------------------------------
 int ATMOS_DYN_divergence_b200_dev(SCALE_HEVI_DIVERGENCE_ARGS)
 {
-    (void)RFDZ;
     CK(need_single("the divergence"));
-    CK(check_flat(GSQRT, J13G, J23G, MAPF, true));
     if (!RCDZ || !RCDX || !RCDY || !FDZ) return fail(SCALE_HEVI_ERR_ARG, "a 1-D grid vector is NULL");
+    bool flat = false;
+    CK(metrics_flat(GSQRT, J13G, J23G, MAPF, true, &flat));
+    C.terrain = false;
+    if (!flat) {
+        // terrain: the metric divergence (k_divergence_terrain), which reads the
+        // library's 1-D tables; the vectors this entry does not take are ones there
+        if (!GSQRT || !J13G || !J23G || !MAPF || !RFDZ)
+            return fail(SCALE_HEVI_ERR_ARG, "terrain-following metrics need GSQRT, J13G, J23G, MAPF and RFDZ");
+        const int n = C.g.KA > C.g.IA ? (C.g.KA > C.g.JA ? C.g.KA : C.g.JA) : (C.g.IA > C.g.JA ? C.g.IA : C.g.JA);
+        std::vector<double> one(n, 1.0);
+        CK(prepare_tables(one.data(), FDZ, RCDZ, RFDZ, one.data(), RCDX, one.data(), one.data(), RCDY, one.data(),
+                          nullptr, nullptr, nullptr));
+        C.terrain = true;
+        C.tm = Metrics{GSQRT, J13G, J23G, MAPF, nullptr};
+        return run_divergence(DDIV, MOMZ, MOMX, MOMY, C.g.RCDZ, C.g.RCDX, C.g.RCDY, *J33G);
+    }
     const int KA = C.g.KA, IA = C.g.IA, JA = C.g.JA;
     double *t;
     CK(stage_buf("div_tab", (size_t)KA + IA + JA, &t));
@@ -1404,15 +1418,26 @@ int ATMOS_DYN_divergence_b200_dev(SCALE_HEVI_DIVERGENCE_ARGS)
 int ATMOS_DYN_divergence_b200(SCALE_HEVI_DIVERGENCE_ARGS)
 {
     CK(need_single("the divergence"));
-    CK(check_flat(GSQRT, J13G, J23G, MAPF, false));
+    bool flat = false;
+    CK(metrics_flat(GSQRT, J13G, J23G, MAPF, false, &flat));
+    const double *dGS = nullptr, *dJ13 = nullptr, *dJ23 = nullptr, *dMAPF = nullptr;
+    if (!flat) {
+        if (!GSQRT || !J13G || !J23G || !MAPF)
+            return fail(SCALE_HEVI_ERR_ARG, "terrain-following metrics need GSQRT, J13G, J23G and MAPF");
+        double *g7, *j13, *j23, *mp;
+        CK(h2d("GSQRT", GSQRT, 7 * C.N3, &g7));
+        CK(h2d("J13G", J13G, 7 * C.N3, &j13));
+        CK(h2d("J23G", J23G, 7 * C.N3, &j23));
+        CK(h2d("MAPF", MAPF, C.N2 * 2 * 4, &mp));
+        dGS = g7; dJ13 = j13; dJ23 = j23; dMAPF = mp;
+    }
     const size_t N3 = n3();
     double *dd, *mz, *mx, *my;
     CK(h2d("DDIV", DDIV, N3, &dd)); // cells the divergence does not write keep their contents
     CK(h2d("x1", MOMZ, N3, &mz));
     CK(h2d("x2", MOMX, N3, &mx));
     CK(h2d("x3", MOMY, N3, &my));
-    int rc = ATMOS_DYN_divergence_b200_dev(dd, mz, mx, my, nullptr, nullptr, nullptr, J33G, nullptr, RCDZ, RCDX, RCDY,
-                                           RFDZ, FDZ);
+    int rc = ATMOS_DYN_divergence_b200_dev(dd, mz, mx, my, dGS, dJ13, dJ23, J33G, dMAPF, RCDZ, RCDX, RCDY, RFDZ, FDZ);
     if (rc) return rc;
     CK(d2h(DDIV, dd, N3));
     CU(cudaStreamSynchronize(C.stream));

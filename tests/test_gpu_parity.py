@@ -317,7 +317,7 @@ def test_mass_conserved_on_device(lib):
 
 def test_single_terrain_point_takes_the_metric_stage(lib):
     # one GSQRT value off 1 is terrain: the HEVI stage runs the general-metric
-    # kernels (bit-exact with the oracle), the flat-only divergence entry refuses it
+    # kernels, bit-exact with the oracle
     g = helpers.small_grid()
     c = helpers.small_case(g)
     a = helpers.short_inputs(c, full=False)
@@ -330,11 +330,6 @@ def test_single_terrain_point_takes_the_metric_stage(lib):
     lib.ATMOS_DYN_Tstep_short_fvm_hevi(**_stage_call_args(a, o_gpu))
     for n in o_ref:
         assert helpers.same(o_gpu[n], o_ref[n]), n
-    with pytest.raises(hevi.HeviError) as e:
-        lib.ATMOS_DYN_divergence(DDIV=g.zeros(), MOMZ=c.state["MOMZ"], MOMX=c.state["MOMX"], MOMY=c.state["MOMY"],
-                                 GSQRT=a["GSQRT"], J13G=a["J13G"], J23G=a["J23G"], J33G=1.0, MAPF=a["MAPF"],
-                                 RCDZ=g.RCDZ, RCDX=g.RCDX, RCDY=g.RCDY, RFDZ=g.RFDZ, FDZ=g.FDZ)
-    assert e.value.code == 5
 
 
 def test_nonperiodic_boundary_is_rejected(lib):

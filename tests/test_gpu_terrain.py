@@ -198,15 +198,40 @@ def test_terrain_tracer_rk3_bit_exact(lib, fct):
     assert helpers.same(got, ref), f"max rel diff {helpers.max_rel(got, ref):.3e}"
 
 
+def test_terrain_divergence_bit_exact(lib):
+    """ATMOS_DYN_divergence (scale_atmos_dyn_common.F90:1437-1515) with its
+    J13G/J23G/GSQRT/MAPF terms."""
+    g = helpers.small_grid(IMAX=13, JMAX=11, KMAX=15, stretched=True)
+    c = helpers.small_case(g)
+    helpers.perturb_state(c)
+    m = with_terrain(dict(), g, seed=31)
+    ref = np.full(g.shape, np.nan, order="F")
+    oracle.divergence(g, ref, c.state, m["GSQRT"], m["J13G"], m["J23G"], 1.0, m["MAPF"])
+    got = np.full(g.shape, np.nan, order="F")
+    lib.setup(g.index_dict(), "UD3", "UD3")
+    lib.ATMOS_DYN_divergence(DDIV=got, MOMZ=c.state["MOMZ"], MOMX=c.state["MOMX"], MOMY=c.state["MOMY"],
+                             GSQRT=m["GSQRT"], J13G=m["J13G"], J23G=m["J23G"], J33G=1.0, MAPF=m["MAPF"],
+                             RCDZ=g.RCDZ, RCDX=g.RCDX, RCDY=g.RCDY, RFDZ=g.RFDZ, FDZ=g.FDZ)
+    assert helpers.same(got, ref), f"max rel diff {helpers.max_rel(got, ref):.3e}"
+
+
 def test_flat_only_entries_refuse_terrain(lib):
+    import torch
+
     g = helpers.small_grid()
     c = helpers.small_case(g)
     a = with_terrain(helpers.short_inputs(c, full=False), g)
     lib.setup(g.index_dict(), "UD3", "UD3")
+    dev = {k: (torch.from_numpy(np.ravel(v, order="K").copy()).cuda() if isinstance(v, np.ndarray) and v.ndim >= 2 else v)
+           for k, v in a.items()}
+    f32 = {k: dev[k].float() for k in ("num_diff", "DENS_t", "MOMZ_t", "MOMX_t", "MOMY_t", "RHOT_t", "DDIV")}
+    x = {n: dev[n].clone() for n in STATE}
+    flx = {n: torch.zeros(3 * g.shape[0] * g.shape[1] * g.shape[2], dtype=torch.float32, device="cuda")
+           for n in ("mflx_hi", "tflx_hi")}
+    kw = {k: v for k, v in dev.items() if k not in f32 and k not in STATE and k not in
+          ("DENS0", "MOMZ0", "MOMX0", "MOMY0", "RHOT0", "dtrk")}
     with pytest.raises(hevi.HeviError, match="not supported") as e:
-        lib.ATMOS_DYN_divergence(DDIV=g.zeros(), MOMZ=c.state["MOMZ"], MOMX=c.state["MOMX"], MOMY=c.state["MOMY"],
-                                 GSQRT=a["GSQRT"], J13G=a["J13G"], J23G=a["J23G"], J33G=1.0, MAPF=a["MAPF"],
-                                 RCDZ=g.RCDZ, RCDX=g.RCDX, RCDY=g.RCDY, RFDZ=g.RFDZ, FDZ=g.FDZ)
+        lib.ATMOS_DYN_Tinteg_short_rk4_mixed_dev(**kw, **f32, **x, **flx, **SHORT_KW, dt=0.5)
     assert e.value.code == 5
     # the flat-terrain stage still runs after the refusal
     a_flat = helpers.short_inputs(c, full=False)
