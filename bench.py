@@ -467,7 +467,7 @@ def run_terrain(args, hevi, torch, step, st, st0, g, cells, stream, t0, t1, dist
         "value": aggregate_rate(cells, world, 1, ms), "unit": UNIT, "ms_per_step": ms, "steps": TERRAIN_STEPS,
         "step": "numfilter + RK4 of 4 general-metric HEVI stages + boundary/halo, FP64, same workload, smooth "
                 "periodic metrics (GSQRT, MAPF within 2%/1% of 1; J13G, J23G within 0.01)",
-        "roofline": {"bound": "hbm", "kernel": "terrain_stage (24 launches, one HEVI stage)", "achieved": ach,
+        "roofline": {"bound": "hbm", "kernel": "terrain_stage (26 launches, one HEVI stage)", "achieved": ach,
                      "peak": hbm, "unit": "GB/s", "frac": (ach / hbm) if ach else None,
                      "algorithmic_bytes_per_launch": TERRAIN_BYTES * cells, "stage_ms": stage_ms},
         "sections_ms_per_step": {k: v[1] / TERRAIN_STEPS for k, v in prof.items()},

@@ -59,7 +59,7 @@ struct TerrainWork {
     double *A, *PT, *F1, *F2, *F3, *C, *e, *f;
 };
 constexpr int TERRAIN_WORK_FIELDS = 24;
-constexpr int TERRAIN_STAGE_LAUNCHES = 24; // kernels of one general-metric stage
+constexpr int TERRAIN_STAGE_LAUNCHES = 26; // kernels of one general-metric stage
 constexpr int TERRAIN_HEVE_LAUNCHES = 23;  // kernels of one general-metric HEVE stage
 cudaError_t launch_terrain_heve_stage(const Grid &g, const StageArgsT<double> &a, const Metrics &M,
                                       const TerrainWork &W, int scheme, cudaStream_t st);

@@ -848,6 +848,54 @@ static void gcols(int i0, int i1, int j0, int j1, cudaStream_t st, F f)
     k_gcols<<<(ncol + 3) / 4, dim3(32, 4), 0, st>>>(i0, ni, j0, ncol, f);
 }
 
+// solve_direct (tstep_short_fvm_hevi.F90:1092-1127) of the general-metric
+// stage: a warp per column stages F1, F2, F3 and C of its column in shared
+// memory (coalesced), lane 0 runs the recurrence there, the lanes store the
+// solution back. Shared memory: 4 columns x 6 arrays x KA doubles per block.
+__global__ void __launch_bounds__(128) k_terrain_solve(const Grid g, const TerrainWork W)
+{
+    extern __shared__ double sh[];
+    const int KA = g.KA, KS = g.KS, KE = g.KE, ni = g.IMAX, ncol = g.IMAX * g.JMAX;
+    const int w = threadIdx.y, lane = threadIdx.x;
+    const int col = blockIdx.x * 4 + w;
+    if (col >= ncol) return; // warp-uniform
+    const int i = g.IS + col % ni, j = g.JS + col / ni;
+    // level k at index k-1
+    double *F1 = sh + (size_t)w * 6 * KA, *F2 = F1 + KA, *F3 = F2 + KA, *C = F3 + KA, *e = C + KA, *f = e + KA;
+    const size_t c1 = idx3(g, 1, i, j);
+    for (int k = KS + lane; k <= KE - 1; k += 32) {
+        F1[k - 1] = W.F1[c1 + k - 1];
+        F2[k - 1] = W.F2[c1 + k - 1];
+        F3[k - 1] = W.F3[c1 + k - 1];
+        C[k - 1] = W.C[c1 + k - 1];
+    }
+    __syncwarp();
+    if (lane == 0) {
+        double rdenom = 1.0 / F2[KS - 1];
+        e[KS - 1] = -F1[KS - 1] * rdenom;
+        f[KS - 1] = C[KS - 1] * rdenom;
+        for (int k = KS + 1; k <= KE - 2; ++k) {
+            rdenom = 1.0 / (F2[k - 1] + F3[k - 1] * e[k - 2]);
+            e[k - 1] = -F1[k - 1] * rdenom;
+            f[k - 1] = (C[k - 1] - F3[k - 1] * f[k - 2]) * rdenom;
+        }
+        C[KE - 2] = (C[KE - 2] - F3[KE - 2] * f[KE - 3]) / (F2[KE - 2] + F3[KE - 2] * e[KE - 3]);
+        for (int k = KE - 2; k >= KS; --k) C[k - 1] = e[k - 1] * C[k] + f[k - 1];
+    }
+    __syncwarp();
+    for (int k = KS + lane; k <= KE - 1; k += 32) W.C[c1 + k - 1] = C[k - 1];
+}
+
+static void terrain_solve(const Grid &g, const TerrainWork &W, cudaStream_t st)
+{
+    const int ncol = g.IMAX * g.JMAX;
+    const size_t smem = (size_t)4 * 6 * g.KA * sizeof(double);
+    // above 48 KB (KA > 256) the opt-in size is needed; a failure shows in the
+    // launch error the caller returns
+    (void)allow_smem(k_terrain_solve);
+    k_terrain_solve<<<(ncol + 3) / 4, dim3(32, 4), smem, st>>>(g, W);
+}
+
 // face value between p[0] and p[s] along a horizontal direction of stride s
 template <int S>
 __device__ __forceinline__ double hface(double vel, const double *p, long s)
@@ -1091,13 +1139,14 @@ static void terrain_stage(const Grid &g, const StageArgsT<double> &a, const Metr
             W.St[c] = (advcv + advch) * MAPFv(i, j, 1, I_XY) * MAPFv(i, j, 2, I_XY) / GS(k, i, j, I_XYZ) + a.RHOT_t[c];
         }
     });
-    // ---- hevi_solver :665-809 (solve_direct :1092-1127), one warp per column ----
+    // ---- hevi_solver :665-809: the coefficients and right-hand side of each
+    // column (one warp per column, lanes along k), the solve, the back-update ----
     gcols(IS, IE, JS, JE, st, [=] __device__(int i, int j, int lane) {
         const double *GW = GSs(I_XYW), *GZ = GSs(I_XYZ);
         const double *col_mz = MZ + X3(1, i, j), *col_pt = W.POTT + X3(1, i, j);
         const size_t c1 = X3(1, i, j);
         double *A = W.A + c1 - 1, *PT = W.PT + c1 - 1, *F1 = W.F1 + c1 - 1, *F2 = W.F2 + c1 - 1, *F3 = W.F3 + c1 - 1;
-        double *C = W.C + c1 - 1, *e = W.e + c1 - 1, *f = W.f + c1 - 1; // 1-based level index
+        double *C = W.C + c1 - 1; // 1-based level index
         for (int k = KS + lane; k <= KE; k += 32) {
             if (k <= KE - 1) PT[k] = zface<S>(col_mz[k - 1], k, KS, KE, [&](int l) { return col_pt[l - 1]; }); // valueW_Z
             A[k] = dt * dt * J33G * ld(g.RCDZ + k - 1) * a.RT2P[c1 + k - 1] * J33G / GZ[c1 + k - 1];
@@ -1116,20 +1165,14 @@ static void terrain_stage(const Grid &g, const StageArgsT<double> &a, const Metr
                                         + F2Hg(GZ, k, 2) * (DN[c] - a.REF_dens[c] + W.Sr[c] * dt));
             C[k] = MZ[c] + dt * (pg + W.Sw[c]);
         }
-        __syncwarp();
-        if (lane == 0) {
-            double rdenom = 1.0 / F2[KS];
-            e[KS] = -F1[KS] * rdenom;
-            f[KS] = C[KS] * rdenom;
-            for (int k = KS + 1; k <= KE - 2; ++k) {
-                rdenom = 1.0 / (F2[k] + F3[k] * e[k - 1]);
-                e[k] = -F1[k] * rdenom;
-                f[k] = (C[k] - F3[k] * f[k - 1]) * rdenom;
-            }
-            C[KE - 1] = (C[KE - 1] - F3[KE - 1] * f[KE - 2]) / (F2[KE - 1] + F3[KE - 1] * e[KE - 2]);
-            for (int k = KE - 2; k >= KS; --k) C[k] = e[k] * C[k + 1] + f[k];
-        }
-        __syncwarp();
+    });
+    // solve_direct (:1092-1127), one warp per column with the column in shared memory
+    terrain_solve(g, W, st);
+    // back-update of the column (:728-790)
+    gcols(IS, IE, JS, JE, st, [=] __device__(int i, int j, int lane) {
+        const double *GZ = GSs(I_XYZ);
+        const size_t c1 = X3(1, i, j);
+        const double *PT = W.PT + c1 - 1, *C = W.C + c1 - 1;
         const double mm = MAPFv(i, j, 1, I_XY) * MAPFv(i, j, 2, I_XY);
         for (int k = KS + lane; k <= KE; k += 32) {
             const size_t c = c1 + k - 1;
