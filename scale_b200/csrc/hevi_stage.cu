@@ -924,16 +924,16 @@ static void terrain_stage(const Grid &g, const StageArgsT<double> &a, const Metr
 #define GSs(idx) (M.GSQRT + (size_t)((idx) - 1) * N3)
 #define J13s(idx) (M.J13G + (size_t)((idx) - 1) * N3)
 #define J23s(idx) (M.J23G + (size_t)((idx) - 1) * N3)
-#define GS(k, i, j, idx) GSs(idx)[X3(k, i, j)]
-#define J13(k, i, j, idx) J13s(idx)[X3(k, i, j)]
-#define J23(k, i, j, idx) J23s(idx)[X3(k, i, j)]
+#define GS(k, i, j, idx) ld(GSs(idx) + X3(k, i, j))
+#define J13(k, i, j, idx) ld(J13s(idx) + X3(k, i, j))
+#define J23(k, i, j, idx) ld(J23s(idx) + X3(k, i, j))
 #define MAPFv(i, j, aa, bb) \
-    M.MAPF[(size_t)((i) - 1) + (size_t)g.IA * ((size_t)((j) - 1) + (size_t)g.JA * ((size_t)((aa) - 1) + 2 * (size_t)((bb) - 1)))]
+    ld(M.MAPF + ((size_t)((i) - 1) + (size_t)g.IA * ((size_t)((j) - 1) + (size_t)g.JA * ((size_t)((aa) - 1) + 2 * (size_t)((bb) - 1)))))
 #define NDp(v, dir) (a.num_diff + N3 * (size_t)(((v) - 1) + 5 * ((dir) - 1)))
 #define CDZv(k) ld(g.CDZ + (k) - 1)
     // F2H(k,p) of a GSQRT slice Gs (ud3.F90:75, tstep_short_fvm_hevi.F90:62)
-#define F2Hg(Gs, k, p) (CDZv((k) + (p) - 1) * (Gs)[X3((k) + (p) - 1, i, j)] \
-                        / (CDZv(k) * (Gs)[X3(k, i, j)] + CDZv((k) + 1) * (Gs)[X3((k) + 1, i, j)]))
+#define F2Hg(Gs, k, p) (CDZv((k) + (p) - 1) * ld((Gs) + X3((k) + (p) - 1, i, j)) \
+                        / (CDZv(k) * ld((Gs) + X3(k, i, j)) + CDZv((k) + 1) * ld((Gs) + X3((k) + 1, i, j))))
     const double *DN = a.DENS, *MZ = a.MOMZ, *MX = a.MOMX, *MY = a.MOMY;
 
     // ---- hevi_pres :343-361 ----
@@ -1398,15 +1398,15 @@ static void terrain_heve_stage(const Grid &g, const StageArgsT<double> &a, const
 #define GSs(idx) (M.GSQRT + (size_t)((idx) - 1) * N3)
 #define J13s(idx) (M.J13G + (size_t)((idx) - 1) * N3)
 #define J23s(idx) (M.J23G + (size_t)((idx) - 1) * N3)
-#define GS(k, i, j, idx) GSs(idx)[X3(k, i, j)]
-#define J13(k, i, j, idx) J13s(idx)[X3(k, i, j)]
-#define J23(k, i, j, idx) J23s(idx)[X3(k, i, j)]
+#define GS(k, i, j, idx) ld(GSs(idx) + X3(k, i, j))
+#define J13(k, i, j, idx) ld(J13s(idx) + X3(k, i, j))
+#define J23(k, i, j, idx) ld(J23s(idx) + X3(k, i, j))
 #define MAPFv(i, j, aa, bb) \
-    M.MAPF[(size_t)((i) - 1) + (size_t)g.IA * ((size_t)((j) - 1) + (size_t)g.JA * ((size_t)((aa) - 1) + 2 * (size_t)((bb) - 1)))]
+    ld(M.MAPF + ((size_t)((i) - 1) + (size_t)g.IA * ((size_t)((j) - 1) + (size_t)g.JA * ((size_t)((aa) - 1) + 2 * (size_t)((bb) - 1)))))
 #define NDp(v, dir) (a.num_diff + N3 * (size_t)(((v) - 1) + 5 * ((dir) - 1)))
 #define CDZv(k) ld(g.CDZ + (k) - 1)
-#define F2Hg(Gs, k, p) (CDZv((k) + (p) - 1) * (Gs)[X3((k) + (p) - 1, i, j)] \
-                        / (CDZv(k) * (Gs)[X3(k, i, j)] + CDZv((k) + 1) * (Gs)[X3((k) + 1, i, j)]))
+#define F2Hg(Gs, k, p) (CDZv((k) + (p) - 1) * ld((Gs) + X3((k) + (p) - 1, i, j)) \
+                        / (CDZv(k) * ld((Gs) + X3(k, i, j)) + CDZv((k) + 1) * ld((Gs) + X3((k) + 1, i, j))))
 #define DEN_UYZ(Gs, k) (F2Hg(Gs, k, 1) * 0.5 * (DN[X3((k) + 1, i, j)] + DN[X3((k) + 1, i + 1, j)]) \
                         + F2Hg(Gs, k, 2) * 0.5 * (DN[X3(k, i, j)] + DN[X3(k, i + 1, j)]))
 #define DEN_XVZ(Gs, k) (F2Hg(Gs, k, 1) * 0.5 * (DN[X3((k) + 1, i, j)] + DN[X3((k) + 1, i, j + 1)]) \
