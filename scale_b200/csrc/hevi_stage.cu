@@ -896,6 +896,15 @@ static void terrain_solve(const Grid &g, const TerrainWork &W, cudaStream_t st)
     k_terrain_solve<<<(ncol + 3) / 4, dim3(32, 4), smem, st>>>(g, W);
 }
 
+// a field that no kernel of the stage writes: elements through the read-only
+// cache (so loads shared by several expressions are formed once), pointer
+// arithmetic as for the plain pointer
+struct RoField {
+    const double *p;
+    __device__ double operator[](size_t q) const { return __ldg(p + q); }
+    __device__ const double *operator+(size_t q) const { return p + q; }
+};
+
 // face value between p[0] and p[s] along a horizontal direction of stride s
 template <int S>
 __device__ __forceinline__ double hface(double vel, const double *p, long s)
@@ -934,7 +943,7 @@ static void terrain_stage(const Grid &g, const StageArgsT<double> &a, const Metr
     // F2H(k,p) of a GSQRT slice Gs (ud3.F90:75, tstep_short_fvm_hevi.F90:62)
 #define F2Hg(Gs, k, p) (CDZv((k) + (p) - 1) * ld((Gs) + X3((k) + (p) - 1, i, j)) \
                         / (CDZv(k) * ld((Gs) + X3(k, i, j)) + CDZv((k) + 1) * ld((Gs) + X3((k) + 1, i, j))))
-    const double *DN = a.DENS, *MZ = a.MOMZ, *MX = a.MOMX, *MY = a.MOMY;
+    const RoField DN{a.DENS}, MZ{a.MOMZ}, MX{a.MOMX}, MY{a.MOMY}; // the stage input, read-only here
 
     // ---- hevi_pres :343-361 ----
     gcols(IS, IE + 1, JS, JE + 1, st, [=] __device__(int i, int j, int lane) {
@@ -1413,7 +1422,7 @@ static void terrain_heve_stage(const Grid &g, const StageArgsT<double> &a, const
                         + F2Hg(Gs, k, 2) * 0.5 * (DN[X3(k, i, j)] + DN[X3(k, i, j + 1)]))
 #define AVG4_UV(m, k) (0.25 * ((m)[X3(k, i, j)] + (m)[X3(k, i + 1, j)] + (m)[X3(k, i, j - 1)] + (m)[X3(k, i + 1, j - 1)]))
 #define AVG4_XV(m, k) (0.25 * ((m)[X3(k, i, j)] + (m)[X3(k, i - 1, j)] + (m)[X3(k, i, j + 1)] + (m)[X3(k, i - 1, j + 1)]))
-    const double *DN = a.DENS, *MZ = a.MOMZ, *MX = a.MOMX, *MY = a.MOMY;
+    const RoField DN{a.DENS}, MZ{a.MOMZ}, MX{a.MOMX}, MY{a.MOMY}; // the stage input, read-only here
 
     // ---- pressure :360-373, potential temperature :375-382 ----
     gcols(IS - 2, IE + 2, JS - 2, JE + 2, st, [=] __device__(int i, int j, int lane) {
