@@ -308,7 +308,8 @@ int COMM_vars8_b200_dev(double *var, const int *nfields);
  * 3-D divergence of the momentum for divergence damping. Replaces
  * ATMOS_DYN_divergence (scale_atmos_dyn_common.F90:1437-1515), same arguments in
  * the same order. DDIV is written on k = KS-1..KE+1, i = IS..IE+1, j = JS..JE+1;
- * other cells keep their contents. Flat terrain only (checked).
+ * other cells keep their contents. Terrain-following metrics select the
+ * metric form of the divergence (its J13G/J23G/GSQRT/MAPF terms).
  * ------------------------------------------------------------------------- */
 #define SCALE_HEVI_DIVERGENCE_ARGS                                                                             \
     double *DDIV, const double *MOMZ, const double *MOMX, const double *MOMY,                                  \
@@ -511,7 +512,8 @@ int scale_hevi_domain_sum_dev(const double *var, const double *CDZ, const double
  * the cudaStream_t to run on (as void*), then the argument list of
  * ATMOS_DYN_Tstep_short_fvm_hevi_b200_dev (device pointers for the 2-D/3-D
  * arrays, host pointers for the 1-D vectors and scalars). It computes what
- * that entry computes.
+ * that entry computes on flat terrain. Terrain-following metrics are refused
+ * with SCALE_HEVI_ERR_UNSUPPORTED: the general-metric stage needs work arrays.
  *
  * Scratch: one fixed device array of SCALE_HEVI_NOALLOC_SCRATCH_BYTES inside
  * the library holds the status words, three per-level fields of the column

@@ -135,7 +135,8 @@ extern "C" int ATMOS_DYN_Tstep_short_fvm_hevi_b200_noalloc(const scale_hevi_inde
     double *colscr = reinterpret_cast<double *>(scr + kHeader);
     double *tab = colscr + ncol;
 
-    // flat terrain only, as the other entries (GSQRT = 1, J13G = J23G = 0, MAPF = 1)
+    // flat terrain only (GSQRT = 1, J13G = J23G = 0, MAPF = 1): the general-metric
+    // stage of the other entries keeps 24 work fields, which this entry does not have
     NA_CU(cudaMemsetAsync(scr, 0, kHeader, st)); // status and counter start at zero
     const size_t n7 = 7 * N3, nm = (size_t)IA * JA * 2 * 4;
     if (GSQRT) count_not_equal(GSQRT, n7, 1.0, count, st);
