@@ -97,3 +97,15 @@ def test_hook_refuses_unrouted_halo_fills(lib):
                                      REF_dens=c.ref["REF_dens"], REF_pott=c.ref["REF_pott"], ND_COEF=1e-3,
                                      ND_ORDER=2, ND_SFC_FACT=0.7, ND_USE_RS=True)
     assert e.value.code == 5
+
+
+def test_hook_mixed_precision_matches_periodic_halo(lib):
+    """The mixed path's FP32 fields (num_diff) reach the hook with 4-byte
+    elements; the result equals the library's own halo bit for bit."""
+    from test_gpu_mixed import run_short_steps
+
+    c = mkinit.config(1, scale=0.3)
+    plain = run_short_steps(c, 3, mixed=True)
+    hooked = run_short_steps(c, 3, mixed=True, hook=True)
+    for n in STATE:
+        assert np.array_equal(plain[n], hooked[n]), n

@@ -14,9 +14,10 @@ pytestmark = pytest.mark.gpu
 STATE = ("DENS", "MOMZ", "MOMX", "MOMY", "RHOT")
 
 
-def run_short_steps(c, nsteps, mixed):
+def run_short_steps(c, nsteps, mixed, hook=False):
     """nsteps short steps (numfilter + RK4 + boundary values and halo) on the
-    device, FP64 or mixed; returns the final state on the host."""
+    device, FP64 or mixed; returns the final state on the host. hook: the
+    halo fills go through a 1x1 decomposition's exchange (scale_b200.decomp)."""
     import torch
 
     g = c.g
@@ -39,6 +40,10 @@ def run_short_steps(c, nsteps, mixed):
     nf = hevi.ATMOS_DYN_numfilter_coef_mixed_dev if mixed else hevi.ATMOS_DYN_numfilter_coef_dev
     rk = hevi.ATMOS_DYN_Tinteg_short_rk4_mixed_dev if mixed else hevi.ATMOS_DYN_Tinteg_short_rk4_dev
     hevi.setup(g.index_dict(), c.scheme, c.scheme_tracer)
+    if hook:
+        from scale_b200 import decomp
+
+        decomp.attach(hevi, decomp.Decomposition(g.IMAX, g.JMAX, 1, 1, 0, g.halo), g.KA)
     try:
         for _ in range(nsteps):
             nf(num_diff=nd, CDZ=g.CDZ, CDX=g.CDX, CDY=g.CDY, FDZ=g.FDZ, FDX=g.FDX, FDY=g.FDY, DT=c.dt,
