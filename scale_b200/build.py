@@ -29,9 +29,11 @@ LIB = LIBDIR / "libscale_hevi.so"
 ORACLE_DIR = ROOT / "oracle"
 ORACLE_LIB = ORACLE_DIR / "build" / "liboracle.so"
 
-CU_SOURCES = ["capi.cu", "hevi_stage.cu", "numfilter.cu", "tracer.cu", "misc.cu", "noalloc.cu", "adjoint.cu"]
+CU_SOURCES = ["capi.cu", "hevi_stage.cu", "hevi_tma.cu", "numfilter.cu", "tracer.cu", "misc.cu", "noalloc.cu",
+              "adjoint.cu"]
 CPP_SOURCES = ["grid_coef.cpp"]
-HEADERS = ["hevi_common.cuh", "hevi_stage.cuh", "hevi_kernels.cuh", "adjoint.cuh", "grid_coef.h"]
+HEADERS = ["hevi_common.cuh", "hevi_stage.cuh", "hevi_kernels.cuh", "hevi_epilogue.cuh", "adjoint.cuh",
+           "grid_coef.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -60,7 +60,8 @@ struct Ctx {
     double *rk[2] = {nullptr, nullptr}; // 5*N3 each
     double *acc = nullptr;          // 5*N3
     double *facc = nullptr;         // 6*N3
-    double *colscr = nullptr;       // 3*N3 when HEVI_COL_SCRATCH
+    double *colscr = nullptr;       // 4*N3: Sr, St, tZ (fused and tiled stage), PT (tiled stage)
+    double *colC = nullptr;         // N3: the column problem's right-hand side (tiled stage, both paths)
     double *phi = nullptr;          // numerical filter: 5*N3 (allocated on first use)
     double *ndw = nullptr;          // numerical filter at ND_ORDER > 1: 2 x 15*N3 work (on first use)
     // mixed-precision path (allocated on first use): flux RK sums, column-solve
@@ -190,7 +191,7 @@ int falloc(float **p, size_t n)
 
 void free_all()
 {
-    double *bufs[] = {C.phi, C.ndw, C.colscr, C.d_tab, C.d_nd, C.rk[0], C.rk[1], C.acc, C.facc, C.tr, C.lg, C.sum_part, C.sum_out,
+    double *bufs[] = {C.phi, C.ndw, C.colscr, C.colC, C.d_tab, C.d_nd, C.rk[0], C.rk[1], C.acc, C.facc, C.tr, C.lg, C.sum_part, C.sum_out,
                       C.tw_buf};
     for (double *b : bufs) if (b) cudaFree(b);
     for (auto &kv : C.stage) cudaFree(kv.second.first);
@@ -495,13 +496,15 @@ StageArgsT<F> stage_args(const StageInT<F> &in, double *const out[5], F *mflx, F
     a.divdmp_coef = in.divdmp; a.J33G = in.J33G; a.dtrk = dtrk;
     a.rk_mode = mode; a.acc = mode == RK_HEUN3 ? C.rk[0] : C.acc; a.facc = facc_buf<F>(); a.status = C.status;
     a.colscr = colscr_buf<F>();
+    a.colC = C.colC;
     return a;
 }
 
-// Stage-shape autotuner: times every compiled tile width at three raster
-// heights on the caller's own inputs (one plain stage whose outputs go to
-// the library's scratch: the RK buffer, the flux RK sums, the column scratch;
-// nothing the caller holds is written) and keeps the fastest for this path.
+// Stage-shape autotuner: times the tiled stage (where it applies) and every
+// compiled tile width of the fused kernel, each at three raster heights, on
+// the caller's own inputs (one plain stage whose outputs go to the library's
+// scratch: the RK buffer, the flux RK sums, the column scratch; nothing the
+// caller holds is written) and keeps the fastest for this path.
 template <typename F>
 int autotune_stage(const StageInT<F> &in, double dtrk)
 {
@@ -518,10 +521,13 @@ int autotune_stage(const StageInT<F> &in, double dtrk)
     float best_ms = 1e30f;
     std::string rows;
     int rc = SCALE_HEVI_OK;
-    for (int tx : STAGE_TILE_XS) {
+    constexpr int FORMS[4] = {0, STAGE_TILE_XS[0], STAGE_TILE_XS[1], STAGE_TILE_XS[2]};
+    for (int tx : FORMS) {
         for (int r : RASTERS) {
             const StageShape sh{tx, r};
-            cudaError_t e = launch_hevi_stage(C.g, mem(), a, C.scheme, sh, C.stream); // warm-up
+            int nl = 1;
+            cudaError_t e = launch_hevi_stage(C.g, mem(), a, C.scheme, sh, C.stream, &nl); // warm-up
+            if (e == cudaSuccess && tx == 0 && nl == 1) break; // the tiled stage does not apply here
             cudaEventRecord(e0, C.stream);
             for (int q = 0; q < REPS && e == cudaSuccess; ++q) e = launch_hevi_stage(C.g, mem(), a, C.scheme, sh, C.stream);
             cudaEventRecord(e1, C.stream);
@@ -533,7 +539,7 @@ int autotune_stage(const StageInT<F> &in, double dtrk)
                 break;
             }
             ms /= REPS;
-            C.launches += 1 + REPS;
+            C.launches += (long long)nl * (1 + REPS);
             char buf[96];
             snprintf(buf, sizeof buf, "%s[%d, %d, %.4f]", rows.empty() ? "" : ", ", tx, r, ms);
             rows += buf;
@@ -592,11 +598,12 @@ int run_stage(const StageInT<F> &in, double *const out[5], F *mflx, F *tflx, dou
     const int p = sizeof(F) == sizeof(double) ? 0 : 1;
     if (C.autotune && !C.tuned[p] && !C.capturing) CK(autotune_stage(in, dtrk));
     const StageArgsT<F> a = stage_args(in, out, mflx, tflx, dtrk, mode);
+    int nl = 1;
     CK(timed(sizeof(F) == sizeof(double) ? "hevi_stage" : "hevi_stage_mixed", [&] {
-        CU(launch_hevi_stage(C.g, mem(), a, C.scheme, C.shape[p], C.stream));
+        CU(launch_hevi_stage(C.g, mem(), a, C.scheme, C.shape[p], C.stream, &nl));
         return SCALE_HEVI_OK;
     }));
-    ++C.launches;
+    C.launches += nl;
     return SCALE_HEVI_OK;
 }
 
@@ -847,7 +854,7 @@ int scale_hevi_ensemble_setup(int n, const scale_hevi_index *idx, const char *fl
         (rc = dalloc(&C.d_nd, 18 * (size_t)ZT + 18 * (size_t)XT + 18 * (size_t)YT)) ||
         (rc = dalloc(&C.rk[0], 5 * N3)) || (rc = dalloc(&C.rk[1], 5 * N3)) ||
         (rc = dalloc(&C.acc, 5 * N3)) || (rc = dalloc(&C.facc, 6 * N3)) ||
-        (HEVI_COL_SCRATCH && (rc = dalloc(&C.colscr, 3 * N3))) ||
+        (rc = dalloc(&C.colscr, 4 * N3)) || (rc = dalloc(&C.colC, N3)) ||
         (rc = dalloc(&C.sum_part, (size_t)x.IMAX * x.JMAX)) || (rc = dalloc(&C.sum_out, 1))) {
         free_all();
         return rc;
@@ -939,7 +946,7 @@ int scale_hevi_stage_shape_get(int *tile_x, int *raster, int mixed)
 {
     CK(need_setup());
     const StageShape &s = C.shape[mixed ? 1 : 0];
-    if (tile_x) *tile_x = s.tile_x > 0 ? s.tile_x : STAGE_TILE_X_DEFAULT;
+    if (tile_x) *tile_x = s.tile_x; // 0: the tiled stage where it applies
     if (raster) *raster = s.raster > 0 ? s.raster : STAGE_RASTER_DEFAULT;
     return SCALE_HEVI_OK;
 }
@@ -1202,7 +1209,7 @@ int ATMOS_DYN_Tinteg_short_rk4_b200_mixed_dev(SCALE_HEVI_TINTEG_SHORT_MIXED_ARGS
     CK(check_flat(GSQRT, J13G, J23G, MAPF, true));
     CK(prepare_tables(CDZ, FDZ, RCDZ, RFDZ, FDX, RCDX, RFDX, FDY, RCDY, RFDY, wdamp_coef, nullptr, nullptr));
     if (!C.facc_f) CK(falloc(&C.facc_f, 6 * C.N3));
-    if (HEVI_COL_SCRATCH && !C.colscr_f) CK(falloc(&C.colscr_f, 3 * C.N3));
+    if (!C.colscr_f) CK(falloc(&C.colscr_f, 4 * C.N3));
     double *X[5] = {DENS, MOMZ, MOMX, MOMY, RHOT};
     StageInT<float> base{nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr,
                          DENS_t, MOMZ_t, MOMX_t, MOMY_t, RHOT_t, DPRES0, RT2P, CORIOLI, num_diff, DDIV, REF_dens, REF_rhot,

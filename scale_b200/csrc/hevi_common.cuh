@@ -263,6 +263,7 @@ __device__ __forceinline__ T ld(const T *p) { return __ldg(p); }
 // device status word bits, read by the host after each call
 enum StatusBits : unsigned {
     ST_NONFINITE = 1u << 0,   // a prognostic output is NaN/Inf
+    ST_TMA_TIMEOUT = 1u << 1, // a bulk tensor copy did not complete within its wait limit
 };
 
 }  // namespace hevi

@@ -125,17 +125,26 @@ void divergence_terrain(const Grid &g, double *DDIV, const double *MOMZ, const d
                         const Metrics &M, double J33G, cudaStream_t st);
 
 // ---- HEVI stage (hevi_stage.cu) ----
-// tile width (columns along i; the CTA's HEVI_COL_TC columns make the tile)
-// and raster height of the stage launch; 0 selects the defaults
+// Form and launch shape of the stage. tile_x = 0: the tiled two-kernel stage
+// (hevi_tma.cu: 4 x 4 column tiles staged by bulk tensor copies, then the
+// column solve) where it applies, else the fused kernel with its default tile;
+// tile_x = 16, 8 or 4: the fused kernel k_hevi_stage with a tile of tile_x x
+// (16/tile_x) columns. raster: rows of tiles per raster group; 0 selects the default.
 struct StageShape {
     int tile_x = 0, raster = 0;
 };
 constexpr int STAGE_TILE_XS[3] = {16, 8, 4};
 constexpr int STAGE_TILE_X_DEFAULT = 16;
 constexpr int STAGE_RASTER_DEFAULT = 16;
+// *launches (optional) receives the number of kernels launched (2 tiled, 1 fused)
 template <typename R>
 cudaError_t launch_hevi_stage(const Grid &g, const Members &mem, const StageArgsT<R> &a, int scheme, StageShape shape,
-                              cudaStream_t st);
+                              cudaStream_t st, int *launches = nullptr);
+// the tiled stage alone; cudaErrorNotSupported where it does not apply (an
+// ensemble, odd KA, a field off a 16-byte boundary, no tiled column scratch)
+template <typename R>
+cudaError_t launch_hevi_stage_tiled(const Grid &g, const Members &mem, const StageArgsT<R> &a, int scheme, int raster,
+                                    cudaStream_t st);
 // one HEVE stage (FP64), same arguments; the RK4 combine modes apply as for HEVI
 cudaError_t launch_heve_stage(const Grid &g, const Members &mem, const StageArgsT<double> &a, int scheme,
                               cudaStream_t st);

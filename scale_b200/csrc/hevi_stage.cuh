@@ -56,7 +56,8 @@ struct StageArgsT {
     double *acc; // 5*N3: DENS, MOMZ, MOMX, MOMY, RHOT
     F *facc;     // 6*N3: mflx Z,X,Y then tflx Z,X,Y
     unsigned *status;
-    F *colscr; // 3*N3 (HEVI_COL_SCRATCH): Sr, St, tZ
+    F *colscr; // Sr, St, tZ (3*N3, the fused kernel) and PT (4*N3, the tiled kernels)
+    double *colC; // N3: right-hand side C of the column problem (tiled kernels; null: fused kernel only)
     int raster; // rows of tiles per raster group (set by the launcher)
 };
 using StageArgs = StageArgsT<double>;

@@ -1,0 +1,686 @@
+// The HEVI stage (ATMOS_DYN_Tstep_short_fvm_hevi,
+// scalelib/src/atmos-rm/dynamics/scale_atmos_dyn_tstep_short_fvm_hevi.F90:128-1089)
+// as two kernels that stage their tiles in shared memory with the tensor memory
+// accelerator (TMA). Line numbers refer to that file unless a flux file is named.
+//
+// k_hevi_explicit: everything explicit in the stage. A CTA owns a 4 x 4 tile of
+//   columns, one warp per column with its lanes along k, and marches up the
+//   column in chunks of 32 levels. For each chunk one thread issues
+//   cp.async.bulk.tensor copies of the five state fields (DENS, MOMZ, MOMX, MOMY,
+//   RHOT) over the tile, its lateral halo (2 points; 3 for the 6-point schemes)
+//   and the levels from 4 below to 2-3 above the chunk into shared memory,
+//   completing on an mbarrier; the tensor maps cover this GPU's own memory and
+//   the copies have no cluster multicast. Every stencil then reads shared
+//   memory at compile-time offsets. Per chunk:
+//     a. the pressure deviation DPRES (hevi_pres :343-361) of the tile and of
+//        its +x/+y neighbour columns; RHOT -> POTT in place (:586-600)
+//     b. x/y mass fluxes (:399-438), Sr (:443-479), PT and the vertical theta
+//        flux (valueW_Z, fluxZ_XYZ), the x/y theta fluxes and St (:603-661)
+//     c. one level lower: Sw (:528-578) and the right-hand side C (:698-722)
+//     d. rho*u and rho*v (hevi_momx :814-928, hevi_momy :934-1048)
+//   The fluxes and momenta leave through the RK folds of put_flux/put_state;
+//   Sr, St, tZ, PT and C go to the column scratch.
+// k_hevi_column: the implicit column problem. A CTA loads C, PT and A(k) of 16
+//   columns into shared memory, warp 0 runs the Thomas solve (solve_direct
+//   :1092-1127) one lane per column, and all warps back-update rho, rho*w and
+//   rho*theta and the vertical fluxes (:728-790).
+//
+// Every value keeps the operation order of the fused kernel k_hevi_stage
+// (hevi_stage.cu) and of the reference, so the two forms give identical bits.
+// Flat terrain, one domain, even KA (the tensor maps need 16-byte strides);
+// the launcher returns cudaErrorNotSupported otherwise and the fused kernel runs.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include "hevi_epilogue.cuh"
+#include "hevi_kernels.cuh"
+
+namespace hevi {
+namespace tma {
+
+constexpr int TX = 4, TY = 4, NCOL = TX * TY; // tile columns; one warp each
+constexpr int KC = 32;                        // levels per chunk (one per lane)
+constexpr int KLO = 4;                        // box levels below the chunk's first level
+template <int S> __host__ __device__ constexpr int reach() { return wide_scheme(S) ? 3 : 2; }
+// box levels: L0-4 .. L0+33 (4-point schemes) or L0-4 .. L0+35 (6-point), L0
+// the chunk's first level; 38 and 40 keep the inner box a multiple of 16 bytes
+template <int S> __host__ __device__ constexpr int box_k() { return wide_scheme(S) ? 40 : 38; }
+template <int S> __host__ __device__ constexpr int box_w() { return TX + 2 * reach<S>(); }
+template <int S> __host__ __device__ constexpr int box_h() { return TY + 2 * reach<S>(); }
+template <int S> __host__ __device__ constexpr int plane() { return box_k<S>() * box_w<S>() * box_h<S>(); }
+constexpr int NF = 5;                         // staged fields
+enum StagedField : int { F_DN = 0, F_MZ = 1, F_MX = 2, F_MY = 3, F_RT = 4 };
+constexpr int NDP = 33;                       // DPRES levels per column: L0-1 .. L0+31
+constexpr int DP_COLS = (TX + 1) * (TY + 1);  // tile columns and their +x/+y neighbours
+constexpr long long WAIT_CYCLES = 4000000000LL; // ~2 s: bound of every mbarrier wait
+
+template <int S> constexpr size_t smem_bytes()
+{
+    return (size_t)NF * plane<S>() * sizeof(double) + (size_t)DP_COLS * NDP * sizeof(double) + 16;
+}
+
+struct StateMaps {
+    CUtensorMap m[NF]; // DENS, MOMZ, MOMX, MOMY, RHOT as (KA, IA, JA) FP64 tensors
+};
+
+// ---- mbarrier and bulk tensor copies (PTX) ----
+__device__ __forceinline__ unsigned smem_u32(const void *p) { return (unsigned)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, unsigned bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+// one test of the phase with the given parity; true once it has completed
+__device__ __forceinline__ bool mbar_try(uint64_t *bar, unsigned parity)
+{
+    unsigned done;
+    asm volatile("{\n\t.reg .pred p;\n\t"
+                 "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                 "selp.u32 %0, 1, 0, p;\n\t}"
+                 : "=r"(done)
+                 : "r"(smem_u32(bar)), "r"(parity)
+                 : "memory");
+    return done != 0;
+}
+// bounded wait: gives up after about WAIT_CYCLES clocks
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned parity)
+{
+    const long long t0 = clock64();
+    while (!mbar_try(bar, parity))
+        if (clock64() - t0 > WAIT_CYCLES) return false;
+    return true;
+}
+__device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, int x, int y, int z, uint64_t *bar)
+{
+    asm volatile("cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+                 " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_u32(dst)),
+                 "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+                 : "memory");
+}
+
+// =============================================================================
+// k_hevi_explicit
+// =============================================================================
+template <int S, typename R, int NM>
+__global__ void __launch_bounds__(32 * NCOL, 2)
+    k_hevi_explicit(const Grid gt, const StageArgsT<R> a, const BatchT<NM> B, const __grid_constant__ StateMaps maps)
+{
+    constexpr int H = reach<S>(), BW = box_w<S>(), BK = box_k<S>(), PL = plane<S>();
+    constexpr int KX = BK, KY = BW * BK; // shared-memory strides of one column step in i and in j
+    constexpr bool W6 = wide_scheme(S);
+    extern __shared__ __align__(1024) double sm[];
+    double *stg = sm;                    // NF staged fields, [j][i][k] each
+    double *sdp = sm + NF * PL;          // DPRES, [DP_COLS][NDP]
+    uint64_t *bar = reinterpret_cast<uint64_t *>(sdp + DP_COLS * NDP);
+    __shared__ int s_ok;
+
+    int b;
+    const Grid g = block_domain(gt, B, b);
+    const int lane = threadIdx.x, w = threadIdx.y, tid = w * 32 + lane;
+    const int tx = w % TX, ty = w / TX;
+    int ti, tj;
+    {
+        // raster: consecutive CTAs walk down a.raster rows of tiles, then step in i
+        const int nti = (g.IMAX + TX - 1) / TX, ntj = (g.JMAX + TY - 1) / TY, RJ = a.raster;
+        const int grp = b / (nti * RJ), rem = b - grp * (nti * RJ);
+        const int rows = min(RJ, ntj - grp * RJ);
+        tj = grp * RJ + rem % rows;
+        ti = rem / rows;
+    }
+    const int i0 = g.IS + ti * TX, j0 = g.JS + tj * TY;
+    const int i = i0 + tx, j = j0 + ty;
+    const bool col_ok = i <= g.IE && j <= g.JE;
+    const size_t N3 = n3(g);
+    const int sI = g.KA, sJ = g.KA * g.IA;
+    const int KS = g.KS, KE = g.KE;
+    const int col = (int)idx3(g, 1, i, j); // offset of level 1 of this warp's column
+    const Nd<R> nd(a, N3);
+    const double dt = a.dtrk, J33G = a.J33G;
+    const bool use_div = a.divdmp_coef != 0.0;
+    const R ddc = use_div ? R(a.divdmp_coef / dt) : R(0.0);
+    const R rcdx = col_ok ? R(ld(g.RCDX + i - 1)) : R(0.0), rcdy = col_ok ? R(ld(g.RCDY + j - 1)) : R(0.0);
+    const R h = R(0.5), qr = R(0.25), J33R = R(J33G);
+    const unsigned FULL = 0xffffffffu;
+    const int NC = (g.KMAX + KC - 1) / KC;
+    R *const sSr = a.colscr, *const sSt = a.colscr + N3, *const stZ = a.colscr + 2 * N3, *const sPT = a.colscr + 3 * N3;
+
+    auto issue = [&](int ch) {
+        // box origin (0-based): level L0-4 = 32*ch - 2 (even, so its byte offset is a
+        // multiple of 16), column i0-H, row j0-H
+        const int x = KC * ch + (KS - 1) - KLO, y = i0 - H - 1, z = j0 - H - 1;
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        mbar_expect_tx(bar, (unsigned)(NF * PL * sizeof(double)));
+        for (int f = 0; f < NF; ++f) tma_load_3d(stg + f * PL, &maps.m[f], x, y, z, bar);
+    };
+    if (tid == 0) {
+        mbar_init(bar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        issue(0);
+    }
+    __syncthreads();
+
+    // this warp's column in the staged box, at the lane's level of the chunk
+    const int cbox = ((ty + H) * BW + (tx + H)) * BK + KLO + lane;
+    const double *sDN = stg + F_DN * PL + cbox, *sMZ = stg + F_MZ * PL + cbox;
+    const double *sMX = stg + F_MX * PL + cbox, *sMY = stg + F_MY * PL + cbox;
+    double *sPO = stg + F_RT * PL + cbox; // RHOT, then POTT
+    R Sr_prev = R(0.0), St_prev = R(0.0); // Sr, St of the previous chunk (lane 31's are carried)
+
+    for (int ch = 0; ch < NC; ++ch) {
+        const int L0 = KS + KC * ch, L = L0 + lane;
+        // ---- the chunk's copies: thread 0 waits (bounded), the block learns the outcome ----
+        if (tid == 0) {
+            const bool ok = mbar_wait(bar, ch & 1);
+            // on a timeout, wait once more (bounded) for the copies still in flight
+            // into this block's shared memory before the block leaves
+            if (!ok) (void)mbar_wait(bar, ch & 1);
+            s_ok = ok ? 1 : 0;
+        }
+        __syncthreads();
+        if (!s_ok) {
+            if (tid == 0) atomicOr(a.status, ST_TMA_TIMEOUT);
+            return; // block-uniform
+        }
+        (void)mbar_try(bar, ch & 1); // completed phase: makes the copied data visible to this thread
+
+        // ---- a. DPRES of the tile and its +x/+y neighbours, levels L0-1..L0+31 (:355) ----
+        for (int q = w; q < DP_COLS; q += NCOL) {
+            const int qx = q % (TX + 1), qy = q / (TX + 1);
+            const int ii = i0 + qx, jj = j0 + qy;
+            if (ii > g.IE + 1 || jj > g.JE + 1) continue;
+            const int cq = (int)idx3(g, 1, ii, jj);
+            const double *rt = stg + F_RT * PL + ((qy + H) * BW + (qx + H)) * BK + KLO - 1;
+            for (int lv = lane; lv < NDP; lv += 32) {
+                const int Lq = L0 - 1 + lv;
+                if (Lq > KE) break;
+                const int cc = cq + Lq - 1;
+                sdp[q * NDP + lv] = ld(a.DPRES0 + cc) + ld(a.RT2P + cc) * (rt[lv] - ld(a.REF_rhot + cc));
+            }
+        }
+        __syncthreads();
+        // RHOT -> POTT = RHOT/DENS (:586-600): the tile's own columns over the whole
+        // box height (the vertical stencils), the x/y arms of the halo at the chunk's
+        // levels (the horizontal theta fluxes)
+        for (int lv = lane; lv < BK; lv += 32) {
+            double *p = sPO - lane - KLO + lv; // box level lv of this warp's column
+            p[0] = (double)(R(p[0]) / R(p[(F_DN - F_RT) * PL]));
+        }
+        for (int q = w; q < 2 * H * (TX + TY); q += NCOL) {
+            int bx, by;
+            if (q < 2 * H * TY) {
+                const int s = q % (2 * H);
+                by = q / (2 * H) + H;
+                bx = s < H ? s : s + TX;
+            } else {
+                const int q2 = q - 2 * H * TY, s = q2 % (2 * H);
+                bx = q2 / (2 * H) + H;
+                by = s < H ? s : s + TY;
+            }
+            double *p = stg + F_RT * PL + (by * BW + bx) * BK + KLO + lane;
+            p[0] = (double)(R(p[0]) / R(p[(F_DN - F_RT) * PL]));
+        }
+        __syncthreads();
+
+        // ---- b. level L: mass and theta fluxes, Sr, St, PT, tZ ----
+        const bool vb = col_ok && L <= KE;
+        const int c = col + L - 1;
+        R Sr = R(0.0), St = R(0.0);
+        {
+            // the vertical mass flux through the faces above and below L (hevi_mflx_z :383-391)
+            const R mZ = (vb && L <= KE - 1) ? ld(nd.DZ() + c) : R(0.0);
+            R mZm1 = __shfl_up_sync(FULL, mZ, 1);
+            if (lane == 0) mZm1 = (vb && L - 1 >= KS) ? ld(nd.DZ() + c - 1) : R(0.0);
+            auto P = [&](int l) { return R(sPO[l - L]); };
+            auto pt_tz = [&](int Lq, R &pt, R &tz) {
+                if (Lq < KS || Lq > KE - 1) { pt = R(0.0); tz = R(0.0); return; }
+                const R m = ld(nd.DZ() + col + Lq - 1);
+                const R M0 = R(sMZ[Lq - L]);
+                pt = zface<S>(M0, Lq, KS, KE, P);
+                tz = m * zface<S>(m, Lq, KS, KE, P) + lds(nd.TZ() + col + Lq - 1);
+            };
+            R PT = R(0.0), tZ = R(0.0);
+            if (vb) pt_tz(L, PT, tZ);
+            R tZm = __shfl_up_sync(FULL, tZ, 1);
+            if (lane == 0 && vb) { R ptm; pt_tz(L - 1, ptm, tZm); }
+            if (vb) {
+                const R Xe = R(sMX[0]) + ld(nd.DX() + c), Xw = R(sMX[-KX]) + ld(nd.DX() + c - sI);
+                const R Yn = R(sMY[0]) + ld(nd.DY() + c), Ys = R(sMY[-KY]) + ld(nd.DY() + c - sJ);
+                const R adv_r = -((Xe - Xw) * rcdx + (Yn - Ys) * rcdy);
+                put_flux(a, N3, 1, c, Xe, true);
+                put_flux(a, N3, 2, c, Yn, true);
+                if (i == g.IS) put_flux(a, N3, 1, c - sI, Xw, false);
+                if (j == g.JS) put_flux(a, N3, 2, c - sJ, Ys, false);
+                const R rcdz = R(ld(g.RCDZ + L - 1));
+                Sr = (-(mZ - mZm1) * rcdz + adv_r) + lds(a.DENS_t + c);
+                // fluxX/Y_XYZ (ud3.F90:251-353)
+                const R P00 = R(sPO[0]);
+                const R Pm2 = R(sPO[-2 * KX]), Pm1 = R(sPO[-KX]), Pp1 = R(sPO[KX]), Pp2 = R(sPO[2 * KX]);
+                const R Qm2 = R(sPO[-2 * KY]), Qm1 = R(sPO[-KY]), Qp1 = R(sPO[KY]), Qp2 = R(sPO[2 * KY]);
+                const R Pm3 = W6 ? R(sPO[-3 * KX]) : R(0.0), Pp3 = W6 ? R(sPO[3 * KX]) : R(0.0);
+                const R Qm3 = W6 ? R(sPO[-3 * KY]) : R(0.0), Qp3 = W6 ? R(sPO[3 * KY]) : R(0.0);
+                const R tXe = Xe * ip6<S>(Xe, Pm2, Pm1, P00, Pp1, Pp2, Pp3) + ld(nd.TX() + c);
+                const R tXw = Xw * ip6<S>(Xw, Pm3, Pm2, Pm1, P00, Pp1, Pp2) + ld(nd.TX() + c - sI);
+                const R tYn = Yn * ip6<S>(Yn, Qm2, Qm1, P00, Qp1, Qp2, Qp3) + ld(nd.TY() + c);
+                const R tYs = Ys * ip6<S>(Ys, Qm3, Qm2, Qm1, P00, Qp1, Qp2) + ld(nd.TY() + c - sJ);
+                const R adv_t = -((tXe - tXw) * rcdx + (tYn - tYs) * rcdy); // hevi_st :646-648
+                put_flux(a, N3, 4, c, tXe, true);
+                put_flux(a, N3, 5, c, tYn, true);
+                if (i == g.IS) put_flux(a, N3, 4, c - sI, tXw, false);
+                if (j == g.JS) put_flux(a, N3, 5, c - sJ, tYs, false);
+                St = (-(tZ - tZm) * rcdz + adv_t) + lds(a.RHOT_t + c); // hevi_st :646-649
+                sSr[c] = Sr;
+                sSt[c] = St;
+                stZ[c] = tZ;
+                sPT[c] = PT;
+            }
+        }
+
+        // ---- c. level k = L-1: Sw (hevi_sw :528-578) and C(k) (:698-722) ----
+        {
+            R Sr_k = __shfl_up_sync(FULL, Sr, 1), St_k = __shfl_up_sync(FULL, St, 1);
+            const R Sr_c = __shfl_sync(FULL, Sr_prev, 31), St_c = __shfl_sync(FULL, St_prev, 31);
+            if (lane == 0) { Sr_k = Sr_c; St_k = St_c; }
+            Sr_prev = Sr;
+            St_prev = St;
+            const int k = L - 1;
+            const bool vc = col_ok && k >= KS && k <= KE - 1;
+            const double *cMZ = sMZ - 1, *cDN = sDN - 1, *cMX = sMX - 1, *cMY = sMY - 1; // level k
+            const int ck = c - 1;
+            auto vMZ = [&](int l) { return R(cMZ[l - k]); };
+            // vertical w-momentum flux above level kq, fluxZ_XYW (ud3.F90:358-452), zero outside KS..KE-2
+            auto qZ_at = [&](int kq) -> R {
+                if (kq < KS || kq > KE - 2) return R(0.0);
+                const R vel = (R(0.5) * (vMZ(kq) + vMZ(kq + 1))) / R(cDN[kq + 1 - k]);
+                const R q = zface<S>(vel, kq, KS, KE, vMZ);
+                return J33R * vel * q + lds(nd.WZ() + col + kq);
+            };
+            const R q_k = vc ? qZ_at(k) : R(0.0);
+            R q_km = __shfl_up_sync(FULL, q_k, 1);
+            if (lane == 0 && vc) q_km = qZ_at(k - 1);
+            if (vc) {
+                // horizontal w-momentum flux divergence, fluxX/Y_XYW (ud3.F90:598-748)
+                R adv_w;
+                {
+                    const R f1 = R(ld(g.F2H1 + k - 1)), f2 = R(ld(g.F2H2 + k - 1));
+                    const R vXe = (f1 * R(cMX[1]) + f2 * R(cMX[0]))
+                                  / (f1 * h * (R(cDN[1]) + R(cDN[1 + KX])) + f2 * h * (R(cDN[0]) + R(cDN[KX])));
+                    const R vXw = (f1 * R(cMX[1 - KX]) + f2 * R(cMX[-KX]))
+                                  / (f1 * h * (R(cDN[1 - KX]) + R(cDN[1])) + f2 * h * (R(cDN[-KX]) + R(cDN[0])));
+                    const R vYn = (f1 * R(cMY[1]) + f2 * R(cMY[0]))
+                                  / (f1 * h * (R(cDN[1]) + R(cDN[1 + KY])) + f2 * h * (R(cDN[0]) + R(cDN[KY])));
+                    const R vYs = (f1 * R(cMY[1 - KY]) + f2 * R(cMY[-KY]))
+                                  / (f1 * h * (R(cDN[1 - KY]) + R(cDN[1])) + f2 * h * (R(cDN[-KY]) + R(cDN[0])));
+                    const R W_m2 = R(cMZ[-2 * KX]), W_m1 = R(cMZ[-KX]), W_00 = R(cMZ[0]);
+                    const R W_p1 = R(cMZ[KX]), W_p2 = R(cMZ[2 * KX]);
+                    const R V_m2 = R(cMZ[-2 * KY]), V_m1 = R(cMZ[-KY]), V_p1 = R(cMZ[KY]), V_p2 = R(cMZ[2 * KY]);
+                    const R W_m3 = W6 ? R(cMZ[-3 * KX]) : R(0.0), W_p3 = W6 ? R(cMZ[3 * KX]) : R(0.0);
+                    const R V_m3 = W6 ? R(cMZ[-3 * KY]) : R(0.0), V_p3 = W6 ? R(cMZ[3 * KY]) : R(0.0);
+                    const R qXe = vXe * ip6<S>(vXe, W_m2, W_m1, W_00, W_p1, W_p2, W_p3) + ld(nd.WX() + ck);
+                    const R qXw = vXw * ip6<S>(vXw, W_m3, W_m2, W_m1, W_00, W_p1, W_p2) + ld(nd.WX() + ck - sI);
+                    const R qYn = vYn * ip6<S>(vYn, V_m2, V_m1, W_00, V_p1, V_p2, V_p3) + ld(nd.WY() + ck);
+                    const R qYs = vYs * ip6<S>(vYs, V_m3, V_m2, V_m1, W_00, V_p1, V_p2) + ld(nd.WY() + ck - sJ);
+                    adv_w = -((qXe - qXw) * rcdx + (qYn - qYs) * rcdy);
+                }
+                const R advcv = -(q_k - q_km) * R(ld(g.RFDZ + k - 1));
+                const R wdmp = -R(ld(a.wdamp + g.z0 + k - 1)) * R(ld(a.MOMZ0 + ck));
+                const R div = use_div ? ddc * (ld(a.DDIV + ck + 1) - ld(a.DDIV + ck)) * R(ld(g.FDZ + k - 1)) : R(0.0);
+                const R Sw = (advcv + adv_w) + wdmp + div + lds(a.MOMZ_t + ck);
+                const double rfdz = ld(g.RFDZ + k - 1);
+                const double RTL1 = ld(a.RT2P + ck + 1), RTL0 = ld(a.RT2P + ck);
+                const double *dp = sdp + (ty * (TX + 1) + tx) * NDP + lane; // DPRES at level k (slot k-L0+1 = lane)
+                const double pg = -(dp[1] + RTL1 * dt * (double)St - dp[0] - RTL0 * dt * (double)St_k) * rfdz * J33G
+                                  - GRAV * (ld(g.F2H1 + k - 1) * (cDN[1] - lds(a.REF_dens + ck + 1) + (double)Sr * dt)
+                                            + ld(g.F2H2 + k - 1) * (cDN[0] - lds(a.REF_dens + ck) + (double)Sr_k * dt));
+                a.colC[ck] = cMZ[0] + dt * (pg + (double)Sw);
+            }
+        }
+
+        // ---- d. rho*u (hevi_momx :814-928) and rho*v (hevi_momy :934-1048) at level L ----
+        {
+            const double rcdz_d = vb ? ld(g.RCDZ + L - 1) : 0.0;
+            const double *dp = sdp + (ty * (TX + 1) + tx) * NDP + lane + 1; // DPRES at level L, this column
+            auto vMX = [&](int l) { return R(sMX[l - L]); };
+            auto vMY = [&](int l) { return R(sMY[l - L]); };
+            // z flux at (u,y,w), fluxZ_UYZ (ud3.F90:753-859); m is the lower level of the face
+            auto qZu = [&](int m) -> R {
+                if (m < KS || m > KE - 1) return R(0.0);
+                const int dm = m - L;
+                const R den = R(ld(g.F2H1 + m - 1)) * h * (R(sDN[dm + 1]) + R(sDN[dm + 1 + KX]))
+                              + R(ld(g.F2H2 + m - 1)) * h * (R(sDN[dm]) + R(sDN[dm + KX]));
+                const R vel = (h * (R(sMZ[dm]) + R(sMZ[dm + KX]))) / den;
+                const R q = zface<S>(vel, m, KS, KE, vMX);
+                return J33R * vel * q + lds(nd.UZ() + c + dm);
+            };
+            // z flux at (x,v,w), fluxZ_XVZ (ud3.F90:1173-1279)
+            auto qZv = [&](int m) -> R {
+                if (m < KS || m > KE - 1) return R(0.0);
+                const int dm = m - L;
+                const R den = R(ld(g.F2H1 + m - 1)) * h * (R(sDN[dm + 1]) + R(sDN[dm + 1 + KY]))
+                              + R(ld(g.F2H2 + m - 1)) * h * (R(sDN[dm]) + R(sDN[dm + KY]));
+                const R vel = (h * (R(sMZ[dm]) + R(sMZ[dm + KY]))) / den;
+                const R q = zface<S>(vel, m, KS, KE, vMY);
+                return J33R * vel * q + lds(nd.VZ() + c + dm);
+            };
+            const bool do_u = vb && i <= g.IEH, do_v = vb && j <= g.JEH;
+            // u: the z flux above L; the one below comes from the previous lane
+            {
+                const R q_k = do_u ? qZu(L) : R(0.0);
+                R q_km = __shfl_up_sync(FULL, q_k, 1);
+                if (lane == 0 && do_u) q_km = qZu(L - 1);
+                if (do_u) {
+                    const R fdx = R(ld(g.FDX + i - 1));
+                    const double rfdx = ld(g.RFDX + i - 1);
+                    const R cor_u = R(0.125) * (R(ld(a.CORIOLI + g.c2 + (i) + (size_t)g.IA * (j - 1)))
+                                                + R(ld(a.CORIOLI + g.c2 + (i - 1) + (size_t)g.IA * (j - 1))));
+                    const R U_m2 = R(sMX[-2 * KX]), U_m1 = R(sMX[-KX]), U_00 = R(sMX[0]);
+                    const R U_p1 = R(sMX[KX]), U_p2 = R(sMX[2 * KX]);
+                    // x flux at (x,y,z) with the index shift of fluxX_UYZ (ud3.F90:1053-1109)
+                    const R vE = (h * (U_p1 + U_00)) / (R(sDN[KX]));
+                    const R U_m3 = W6 ? R(sMX[-3 * KX]) : R(0.0), U_p3 = W6 ? R(sMX[3 * KX]) : R(0.0);
+                    const R qXe = vE * ip6<S>(vE, U_m2, U_m1, U_00, U_p1, U_p2, U_p3) + ld(nd.UX() + c + sI);
+                    const R vW = (h * (U_00 + U_m1)) / (R(sDN[0]));
+                    const R qXw = vW * ip6<S>(vW, U_m3, U_m2, U_m1, U_00, U_p1, U_p2) + ld(nd.UX() + c);
+                    // y flux at (u,v,z), fluxY_UYZ (ud3.F90:1113-1167)
+                    const R vN = (h * (R(sMY[0]) + R(sMY[KX])))
+                                 / (qr * (R(sDN[0]) + R(sDN[KX]) + R(sDN[KY]) + R(sDN[KX + KY])));
+                    const R qYn = vN * ip6<S>(vN, W6 ? R(sMX[-2 * KY]) : R(0.0), R(sMX[-KY]), U_00, R(sMX[KY]),
+                                              R(sMX[2 * KY]), W6 ? R(sMX[3 * KY]) : R(0.0)) + ld(nd.UY() + c);
+                    const R vS = (h * (R(sMY[-KY]) + R(sMY[KX - KY])))
+                                 / (qr * (R(sDN[-KY]) + R(sDN[KX - KY]) + R(sDN[0]) + R(sDN[KX])));
+                    const R qYs = vS * ip6<S>(vS, W6 ? R(sMX[-3 * KY]) : R(0.0), R(sMX[-2 * KY]), R(sMX[-KY]), U_00,
+                                              R(sMX[KY]), W6 ? R(sMX[2 * KY]) : R(0.0)) + ld(nd.UY() + c - sJ);
+                    const R advcv = -(q_k - q_km) * R(rcdz_d);
+                    const R advch = -((qXe - qXw) * R(rfdx) + (qYn - qYs) * rcdy);
+                    const double DPe = dp[NDP]; // DPRES at (i+1, j)
+                    const double pg = (DPe - dp[0]) * rfdx;
+                    const R cf = cor_u * (R(sMY[KX]) + R(sMY[0]) + R(sMY[KX - KY]) + R(sMY[-KY]));
+                    const R div = !use_div ? R(0.0) : ddc * (ld(a.DDIV + c + sI) - ld(a.DDIV + c)) * fdx;
+                    const double val = lds(a.MOMX0 + c)
+                                       + dt * (((((double)(advcv + advch)) - pg) + (double)cf) + (double)div
+                                               + (double)lds(a.MOMX_t + c));
+                    put_state(a, N3, 2, a.MOMX_RK, a.MOMX0, c, val, true);
+                }
+            }
+            // v
+            {
+                const R q_k = do_v ? qZv(L) : R(0.0);
+                R q_km = __shfl_up_sync(FULL, q_k, 1);
+                if (lane == 0 && do_v) q_km = qZv(L - 1);
+                if (do_v) {
+                    const R fdy = R(ld(g.FDY + j - 1));
+                    const double rfdy = ld(g.RFDY + j - 1);
+                    const R cor_v = R(-0.125) * (R(ld(a.CORIOLI + g.c2 + (i - 1) + (size_t)g.IA * (j)))
+                                                 + R(ld(a.CORIOLI + g.c2 + (i - 1) + (size_t)g.IA * (j - 1))));
+                    const R Y_m2 = R(sMY[-2 * KY]), Y_m1 = R(sMY[-KY]), Y_00 = R(sMY[0]);
+                    const R Y_p1 = R(sMY[KY]), Y_p2 = R(sMY[2 * KY]);
+                    // x flux at (u,v,z), fluxX_XVZ (ud3.F90:1473-1527)
+                    const R vE = (h * (R(sMX[0]) + R(sMX[KY])))
+                                 / (qr * (R(sDN[0]) + R(sDN[KX]) + R(sDN[KY]) + R(sDN[KX + KY])));
+                    const R qXe = vE * ip6<S>(vE, W6 ? R(sMY[-2 * KX]) : R(0.0), R(sMY[-KX]), Y_00, R(sMY[KX]),
+                                              R(sMY[2 * KX]), W6 ? R(sMY[3 * KX]) : R(0.0)) + ld(nd.VX() + c);
+                    const R vW = (h * (R(sMX[-KX]) + R(sMX[KY - KX])))
+                                 / (qr * (R(sDN[-KX]) + R(sDN[0]) + R(sDN[KY - KX]) + R(sDN[KY])));
+                    const R qXw = vW * ip6<S>(vW, W6 ? R(sMY[-3 * KX]) : R(0.0), R(sMY[-2 * KX]), R(sMY[-KX]), Y_00,
+                                              R(sMY[KX]), W6 ? R(sMY[2 * KX]) : R(0.0)) + ld(nd.VX() + c - sI);
+                    // y flux with the index shift of fluxY_XVZ (ud3.F90:1531-1587)
+                    const R vN = (h * (Y_p1 + Y_00)) / (R(sDN[KY]));
+                    const R Y_m3 = W6 ? R(sMY[-3 * KY]) : R(0.0), Y_p3 = W6 ? R(sMY[3 * KY]) : R(0.0);
+                    const R qYn = vN * ip6<S>(vN, Y_m2, Y_m1, Y_00, Y_p1, Y_p2, Y_p3) + ld(nd.VY() + c + sJ);
+                    const R vS = (h * (Y_00 + Y_m1)) / (R(sDN[0]));
+                    const R qYs = vS * ip6<S>(vS, Y_m3, Y_m2, Y_m1, Y_00, Y_p1, Y_p2) + ld(nd.VY() + c);
+                    const R advcv = -(q_k - q_km) * R(rcdz_d);
+                    const R advch = -((qXe - qXw) * rcdx + (qYn - qYs) * R(rfdy));
+                    const double DPn = dp[(TX + 1) * NDP]; // DPRES at (i, j+1)
+                    const double pg = (DPn - dp[0]) * rfdy;
+                    const R cf = cor_v * (R(sMX[KY]) + R(sMX[0]) + R(sMX[KY - KX]) + R(sMX[-KX]));
+                    const R div = !use_div ? R(0.0) : ddc * (ld(a.DDIV + c + sJ) - ld(a.DDIV + c)) * fdy;
+                    const double val = lds(a.MOMY0 + c)
+                                       + dt * (((((double)(advcv + advch)) - pg) + (double)cf) + (double)div
+                                               + (double)lds(a.MOMY_t + c));
+                    put_state(a, N3, 3, a.MOMY_RK, a.MOMY0, c, val, true);
+                }
+            }
+        }
+        __syncthreads(); // every read of the staged box and of DPRES is done
+        if (tid == 0 && ch + 1 < NC) issue(ch + 1);
+    }
+}
+
+// =============================================================================
+// k_hevi_column
+// =============================================================================
+constexpr int CCOLS = 16;  // columns per CTA (consecutive in i)
+constexpr int CWARPS = 8;
+__host__ __device__ inline int col_pitch_c(int KA) { return KA | 1; }
+
+template <typename R, int NM>
+__global__ void __launch_bounds__(32 * CWARPS, 4) k_hevi_column(const Grid gt, const StageArgsT<R> a, const BatchT<NM> B)
+{
+    extern __shared__ double csm[];
+    int b;
+    const Grid g = block_domain(gt, B, b);
+    const int nbx = (g.IMAX + CCOLS - 1) / CCOLS;
+    const int i0 = g.IS + (b % nbx) * CCOLS, j = g.JS + b / nbx;
+    const int lane = threadIdx.x, w = threadIdx.y;
+    const size_t N3 = n3(g);
+    const int KS = g.KS, KE = g.KE, KP = col_pitch_c(g.KA);
+    const double dt = a.dtrk, J33G = a.J33G, dt2 = dt * dt;
+    const Nd<R> nd(a, N3);
+    const R *sSr = a.colscr, *sSt = a.colscr + N3, *stZ = a.colscr + 2 * N3, *sPT = a.colscr + 3 * N3;
+    // per-level arrays of the tile's columns: [array][column][level], odd pitch
+    double *sC = csm, *sP = csm + (size_t)CCOLS * KP, *sA = csm + (size_t)2 * CCOLS * KP;
+#define CA(arr, cc, L) arr[(size_t)(cc) * KP + (L) - 1]
+
+    // ---- load C, PT and A(k) = dt^2 J33G^2 RCDZ RT2P (:696) ----
+    for (int cc = w; cc < CCOLS; cc += CWARPS) {
+        const int i = i0 + cc;
+        if (i > g.IE) break;
+        const int col = (int)idx3(g, 1, i, j);
+        for (int L = KS + lane; L <= KE; L += 32) {
+            const int c = col + L - 1;
+            if (L <= KE - 1) {
+                CA(sC, cc, L) = __ldcg(a.colC + c);
+                CA(sP, cc, L) = (double)__ldcg(sPT + c);
+            }
+            CA(sA, cc, L) = dt2 * J33G * ld(g.RCDZ + L - 1) * ld(a.RT2P + c) * J33G;
+        }
+    }
+    __syncthreads();
+
+    // ---- Thomas solve, one lane per column (solve_direct :1092-1127 with F1..F3 of :699-709) ----
+    if (w == 0 && lane < CCOLS && i0 + lane <= g.IE) {
+        const int cc = lane;
+        double e_prev = 0.0, f_prev = 0.0;
+        for (int k = KS; k <= KE - 1; ++k) {
+            const double rfdz = ld(g.RFDZ + k - 1);
+            const double Bk = GRAV * dt2 * J33G / (ld(g.CDZ + k) + ld(g.CDZ + k - 1));
+            const double Ak = CA(sA, cc, k), Ak1 = CA(sA, cc, k + 1);
+            const double F2 = 1.0 + (CA(sP, cc, k) * rfdz * (Ak1 + Ak));
+            const double Ck = CA(sC, cc, k);
+            if (k == KS) {
+                const double F1 = -(CA(sP, cc, k + 1) * rfdz * Ak1 + Bk);
+                const double rdenom = 1.0 / F2;
+                e_prev = -F1 * rdenom;
+                f_prev = Ck * rdenom;
+            } else if (k <= KE - 2) {
+                const double F1 = -(CA(sP, cc, k + 1) * rfdz * Ak1 + Bk);
+                const double F3 = -(CA(sP, cc, k - 1) * rfdz * Ak - Bk);
+                const double rdenom = 1.0 / (F2 + F3 * e_prev);
+                e_prev = -F1 * rdenom;
+                f_prev = (Ck - F3 * f_prev) * rdenom;
+            } else {
+                const double F3 = -(CA(sP, cc, k - 1) * rfdz * Ak - Bk);
+                f_prev = (Ck - F3 * f_prev) / (F2 + F3 * e_prev); // the solution at KE-1
+            }
+            CA(sA, cc, k) = e_prev;
+            CA(sC, cc, k) = f_prev;
+        }
+        // back substitution, C(k) = e(k) C(k+1) + f(k)
+        double Cnext = f_prev;
+        for (int k = KE - 2; k >= KS; --k) {
+            Cnext = CA(sA, cc, k) * Cnext + CA(sC, cc, k);
+            CA(sC, cc, k) = Cnext;
+        }
+    }
+    __syncthreads();
+
+    // ---- back-update (:728-790) ----
+    for (int cc = w; cc < CCOLS; cc += CWARPS) {
+        const int i = i0 + cc;
+        if (i > g.IE) break;
+        const int col = (int)idx3(g, 1, i, j);
+        for (int m = KS + lane; m <= KE; m += 32) {
+            const int c = col + m - 1;
+            const double rcdz = ld(g.RCDZ + m - 1);
+            double adr, adt;
+            if (m == KE) {
+                const double Cm1 = CA(sC, cc, m - 1);
+                adr = Cm1 * J33G * rcdz;
+                adt = Cm1 * CA(sP, cc, KE - 1) * J33G * rcdz;
+            } else if (m == KS) {
+                const double Cm = CA(sC, cc, m);
+                adr = -Cm * J33G * rcdz;
+                adt = -Cm * CA(sP, cc, KS) * J33G * rcdz;
+            } else {
+                const double Cm = CA(sC, cc, m), Cm1 = CA(sC, cc, m - 1);
+                adr = -(Cm - Cm1) * J33G * rcdz;
+                adt = -(Cm * CA(sP, cc, m) - Cm1 * CA(sP, cc, m - 1)) * J33G * rcdz;
+            }
+            put_state(a, N3, 0, a.DENS_RK, a.DENS0, c, lds(a.DENS0 + c) + dt * (adr + (double)__ldcg(sSr + c)), true);
+            put_state(a, N3, 4, a.RHOT_RK, a.RHOT0, c, lds(a.RHOT0 + c) + dt * (adt + (double)__ldcg(sSt + c)), true);
+            if (m <= KE - 1) {
+                const double Cm = CA(sC, cc, m);
+                put_state(a, N3, 1, a.MOMZ_RK, a.MOMZ0, c, ld(a.MOMZ0 + c) + (Cm - ld(a.MOMZ + c)), true);
+                put_flux(a, N3, 0, c, R((double)ld(nd.DZ() + c) + J33G * Cm), true);
+                put_flux(a, N3, 3, c, R((double)__ldcg(stZ + c) + J33G * Cm * CA(sP, cc, m)), true);
+            } else {
+                put_state(a, N3, 1, a.MOMZ_RK, a.MOMZ0, c, 0.0, false);
+                put_flux(a, N3, 0, c, R(0.0), true);
+                put_flux(a, N3, 3, c, R(0.0), true);
+            }
+        }
+        if (lane == 0) {
+            // rigid-lid and surface values (:753-754) and the zero fluxes at KS-1 (:371, ud3.F90:222)
+            put_state(a, N3, 1, a.MOMZ_RK, a.MOMZ0, col + KS - 2, 0.0, false);
+            put_flux(a, N3, 0, col + KS - 2, R(0.0), false);
+            put_flux(a, N3, 3, col + KS - 2, R(0.0), false);
+        }
+        // hevi_mflx_z :369-393 also fills the halo column i = IS-1 with the explicit
+        // part of the vertical mass flux; the solver never updates it
+        if (i == g.IS && (a.rk_mode == RK_PLAIN || a.rk_mode == RK_FINAL || a.rk_mode == RK_HEUN3)) {
+            const size_t ch = idx3(g, 1, g.IS - 1, j);
+            for (int k = KS - 1 + lane; k <= KE; k += 32)
+                a.mflx[ch + k - 1] = (k >= KS && k <= KE - 1) ? ld(nd.DZ() + ch + k - 1) : R(0.0);
+        }
+    }
+#undef CA
+}
+
+// =============================================================================
+// host side
+// =============================================================================
+PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
+{
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q{};
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    }
+    return fn;
+}
+
+// FP64 (KA, IA, JA) tensor with a box of bk x bw x bh elements
+bool encode(CUtensorMap *m, const double *base, const Grid &g, int bk, int bw, int bh)
+{
+    auto fn = encode_fn();
+    if (!fn || ((uintptr_t)base & 15u)) return false;
+    const cuuint64_t dims[3] = {(cuuint64_t)g.KA, (cuuint64_t)g.IA, (cuuint64_t)g.JA};
+    const cuuint64_t strides[2] = {(cuuint64_t)g.KA * sizeof(double), (cuuint64_t)g.KA * g.IA * sizeof(double)};
+    const cuuint32_t box[3] = {(cuuint32_t)bk, (cuuint32_t)bw, (cuuint32_t)bh};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    return fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<double *>(base), dims, strides, box, estr,
+              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+              CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// opens the dynamic shared memory of a kernel instantiation, once per device
+template <class K>
+cudaError_t open_smem(K kern, size_t bytes)
+{
+    static std::pair<const void *, int> done[64];
+    static int ndone = 0;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    for (int q = 0; q < ndone; ++q)
+        if (done[q].first == (const void *)kern && done[q].second == dev) return cudaSuccess;
+    e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+    if (e == cudaSuccess && ndone < 64) done[ndone++] = {(const void *)kern, dev};
+    return e;
+}
+
+template <int S, typename R>
+cudaError_t launch_s(const Grid &g, StageArgsT<R> a, int raster, cudaStream_t st)
+{
+    StateMaps maps;
+    const double *f[NF] = {a.DENS, a.MOMZ, a.MOMX, a.MOMY, a.RHOT};
+    for (int q = 0; q < NF; ++q)
+        if (!encode(&maps.m[q], f[q], g, box_k<S>(), box_w<S>(), box_h<S>())) return cudaErrorNotSupported;
+    BatchT<1> B{};
+    B.n = 1;
+    a.raster = raster > 0 ? raster : STAGE_RASTER_DEFAULT;
+    const int ntiles = ((g.IMAX + TX - 1) / TX) * ((g.JMAX + TY - 1) / TY);
+    B.first[0] = 0;
+    B.first[1] = ntiles;
+    auto kx = k_hevi_explicit<S, R, 1>;
+    cudaError_t e = open_smem(kx, smem_bytes<S>());
+    if (e != cudaSuccess) return e;
+    kx<<<ntiles, dim3(32, NCOL), smem_bytes<S>(), st>>>(g, a, B, maps);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    auto kc = k_hevi_column<R, 1>;
+    // the attribute is set once per device, so it opens the largest size (KA = 260)
+    const size_t csmem = (size_t)3 * CCOLS * col_pitch_c(g.KA) * sizeof(double);
+    if ((e = open_smem(kc, (size_t)3 * CCOLS * col_pitch_c(260) * sizeof(double))) != cudaSuccess) return e;
+    const int ncb = ((g.IMAX + CCOLS - 1) / CCOLS) * g.JMAX;
+    B.first[1] = ncb;
+    kc<<<ncb, dim3(32, CWARPS), csmem, st>>>(g, a, B);
+    return cudaGetLastError();
+}
+
+}  // namespace tma
+
+// The tiled stage where it applies: one domain, even KA, KA <= MAXKA_TILED,
+// the column scratch of the tiled kernels present and every staged field on a
+// 16-byte boundary. cudaErrorNotSupported otherwise (the caller then runs the
+// fused kernel).
+template <typename R>
+cudaError_t launch_hevi_stage_tiled(const Grid &g, const Members &mem, const StageArgsT<R> &a, int scheme, int raster,
+                                    cudaStream_t st)
+{
+    if (mem.n > 1 || (g.KA & 1) || g.KA > 260 || !a.colC) return cudaErrorNotSupported;
+    switch (scheme) {
+    case UD3: return tma::launch_s<UD3, R>(g, a, raster, st);
+    case CD4: return tma::launch_s<CD4, R>(g, a, raster, st);
+    case KOREN: return tma::launch_s<KOREN, R>(g, a, raster, st);
+    case CD2: return tma::launch_s<CD2, R>(g, a, raster, st);
+    case UD5: return tma::launch_s<UD5, R>(g, a, raster, st);
+    case CD6: return tma::launch_s<CD6, R>(g, a, raster, st);
+    default: return cudaErrorInvalidValue;
+    }
+}
+template cudaError_t launch_hevi_stage_tiled<double>(const Grid &, const Members &, const StageArgsT<double> &, int,
+                                                     int, cudaStream_t);
+template cudaError_t launch_hevi_stage_tiled<float>(const Grid &, const Members &, const StageArgsT<float> &, int, int,
+                                                    cudaStream_t);
+
+}  // namespace hevi

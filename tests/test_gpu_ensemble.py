@@ -78,9 +78,11 @@ def test_ensemble_graph_replay(cases, alone):
 
 
 def test_ensemble_one_launch_per_kernel(cases):
-    # the launch count of a step does not depend on the number of members
-    _, l4 = _together(cases, 2)
-    _, l1 = _together(cases[:1], 2)
+    # the launch count of a step does not depend on the number of members; the
+    # fused stage form on both sides (a single domain would otherwise take the
+    # tiled stage, two kernels per stage)
+    _, l4 = _together(cases, 2, tile_x=16)
+    _, l1 = _together(cases[:1], 2, tile_x=16)
     assert l4 == l1
 
 
