@@ -174,7 +174,10 @@ def run_b200(args):
     N3 = int(np.prod(g.shape))
     cells = g.cells
     hevi.setup(g.index_dict(), c.scheme, c.scheme_tracer, device=local)
-    hevi.stage_autotune(True)  # the first warm-up step picks the stage tile shape
+    if args.stage_shape:
+        hevi.stage_shape(*[int(v) for v in args.stage_shape.split(",")])
+    else:
+        hevi.stage_autotune(True)  # the first warm-up step picks the stage tile shape
 
     # device-resident state and inputs (Fortran layout, one flat buffer each)
     st = torch.empty((5, N3), dtype=torch.float64, device="cuda")
@@ -829,6 +832,7 @@ def main():
     ap.add_argument("--cpu-scale", type=float, default=0.25, help="horizontal scale of the CPU sample")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="minimum CPU work of the baseline sample")
     ap.add_argument("--e2e-calls", type=int, default=2)
+    ap.add_argument("--stage-shape", default="", help="fixed stage form 'tile_x,raster' (0 = tiled) instead of the autotuner")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision measurement")

@@ -508,21 +508,26 @@ int scale_hevi_domain_sum_dev(const double *var, const double *CDZ, const double
  * run could fail or break its accounting, or a caller that cannot call
  * scale_hevi_setup.
  *
- * Arguments: the index set and flux scheme that scale_hevi_setup would take,
- * the cudaStream_t to run on (as void*), then the argument list of
+ * Arguments: the index set (halo 2) and the flux scheme, the cudaStream_t to
+ * run on (as void*), then the argument list of
  * ATMOS_DYN_Tstep_short_fvm_hevi_b200_dev (device pointers for the 2-D/3-D
  * arrays, host pointers for the 1-D vectors and scalars). It computes what
- * that entry computes on flat terrain. Terrain-following metrics are refused
- * with SCALE_HEVI_ERR_UNSUPPORTED: the general-metric stage needs work arrays.
+ * that entry computes, bit for bit, for the 4-point schemes (UD3, CD4,
+ * UD3KOREN1993, CD2; the 6-point schemes need a halo of 3) on flat terrain.
+ * Terrain-following metrics are refused with SCALE_HEVI_ERR_UNSUPPORTED: the
+ * general-metric stage needs work arrays. A metric set (device and the four
+ * pointers) found flat once is remembered in host memory and not checked
+ * again, which assumes its contents do not change.
  *
  * Scratch: one fixed device array of SCALE_HEVI_NOALLOC_SCRATCH_BYTES inside
  * the library holds the status words, three per-level fields of the column
  * solve and the 1-D grid tables: 256 + 8*(3*KA*IA*JA + 7*KA + 4*IA + 4*JA)
- * bytes. A larger domain is rejected with SCALE_HEVI_ERR_ARG. The first call
- * on a device looks up the array with that device current. Make that first
- * call before any stream capture. All calls on a device share the array, so
- * calls that overlap in time race. The entry synchronises the stream before
- * it returns.
+ * bytes. A larger domain is rejected with SCALE_HEVI_ERR_ARG. Every call looks
+ * the array up with the caller's device current; the first lookup on a device
+ * can load the module, so make the first call before any stream capture. The
+ * entry synchronises the stream before it returns, so it cannot itself be
+ * captured. All calls on a device share the array, so calls that overlap in
+ * time race.
  * ------------------------------------------------------------------------- */
 #define SCALE_HEVI_NOALLOC_SCRATCH_BYTES (32UL * 1024UL * 1024UL)
 int ATMOS_DYN_Tstep_short_fvm_hevi_b200_noalloc(const scale_hevi_index *idx, const char *flux_type, void *stream,

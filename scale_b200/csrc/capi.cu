@@ -61,7 +61,7 @@ struct Ctx {
     double *acc = nullptr;          // 5*N3
     double *facc = nullptr;         // 6*N3
     double *colscr = nullptr;       // 4*N3: Sr, St, tZ (fused and tiled stage), PT (tiled stage)
-    double *colC = nullptr;         // N3: the column problem's right-hand side (tiled stage, both paths)
+    double *colC = nullptr;         // 2*N3: the column problem's right-hand side, then f, and e (tiled stage)
     double *phi = nullptr;          // numerical filter: 5*N3 (allocated on first use)
     double *ndw = nullptr;          // numerical filter at ND_ORDER > 1: 2 x 15*N3 work (on first use)
     // mixed-precision path (allocated on first use): flux RK sums, column-solve
@@ -526,8 +526,9 @@ int autotune_stage(const StageInT<F> &in, double dtrk)
         for (int r : RASTERS) {
             const StageShape sh{tx, r};
             int nl = 1;
-            cudaError_t e = launch_hevi_stage(C.g, mem(), a, C.scheme, sh, C.stream, &nl); // warm-up
-            if (e == cudaSuccess && tx == 0 && nl == 1) break; // the tiled stage does not apply here
+            bool tiled = false;
+            cudaError_t e = launch_hevi_stage(C.g, mem(), a, C.scheme, sh, C.stream, &nl, &tiled); // warm-up
+            if (e == cudaSuccess && tx == 0 && !tiled) break; // the tiled stage does not apply here
             cudaEventRecord(e0, C.stream);
             for (int q = 0; q < REPS && e == cudaSuccess; ++q) e = launch_hevi_stage(C.g, mem(), a, C.scheme, sh, C.stream);
             cudaEventRecord(e1, C.stream);
@@ -854,7 +855,7 @@ int scale_hevi_ensemble_setup(int n, const scale_hevi_index *idx, const char *fl
         (rc = dalloc(&C.d_nd, 18 * (size_t)ZT + 18 * (size_t)XT + 18 * (size_t)YT)) ||
         (rc = dalloc(&C.rk[0], 5 * N3)) || (rc = dalloc(&C.rk[1], 5 * N3)) ||
         (rc = dalloc(&C.acc, 5 * N3)) || (rc = dalloc(&C.facc, 6 * N3)) ||
-        (rc = dalloc(&C.colscr, 4 * N3)) || (rc = dalloc(&C.colC, N3)) ||
+        (rc = dalloc(&C.colscr, 4 * N3)) || (rc = dalloc(&C.colC, 2 * N3)) ||
         (rc = dalloc(&C.sum_part, (size_t)x.IMAX * x.JMAX)) || (rc = dalloc(&C.sum_out, 1))) {
         free_all();
         return rc;

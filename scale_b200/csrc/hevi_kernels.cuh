@@ -125,9 +125,9 @@ void divergence_terrain(const Grid &g, double *DDIV, const double *MOMZ, const d
                         const Metrics &M, double J33G, cudaStream_t st);
 
 // ---- HEVI stage (hevi_stage.cu) ----
-// Form and launch shape of the stage. tile_x = 0: the tiled two-kernel stage
-// (hevi_tma.cu: 4 x 4 column tiles staged by bulk tensor copies, then the
-// column solve) where it applies, else the fused kernel with its default tile;
+// Form and launch shape of the stage. tile_x = 0: the tiled stage (hevi_tma.cu:
+// 4 x 4 column tiles staged by bulk tensor copies) where it applies, else the
+// fused kernel with its default tile;
 // tile_x = 16, 8 or 4: the fused kernel k_hevi_stage with a tile of tile_x x
 // (16/tile_x) columns. raster: rows of tiles per raster group; 0 selects the default.
 struct StageShape {
@@ -136,10 +136,11 @@ struct StageShape {
 constexpr int STAGE_TILE_XS[3] = {16, 8, 4};
 constexpr int STAGE_TILE_X_DEFAULT = 16;
 constexpr int STAGE_RASTER_DEFAULT = 16;
-// *launches (optional) receives the number of kernels launched (2 tiled, 1 fused)
+// *launches (optional) receives the number of kernels launched, *tiled
+// (optional) whether the tiled form ran
 template <typename R>
 cudaError_t launch_hevi_stage(const Grid &g, const Members &mem, const StageArgsT<R> &a, int scheme, StageShape shape,
-                              cudaStream_t st, int *launches = nullptr);
+                              cudaStream_t st, int *launches = nullptr, bool *tiled = nullptr);
 // the tiled stage alone; cudaErrorNotSupported where it does not apply (an
 // ensemble, odd KA, a field off a 16-byte boundary, no tiled column scratch)
 template <typename R>

@@ -695,13 +695,14 @@ static cudaError_t launch_one(const Grid &g, StageArgsT<R> a, const BatchT<NM> &
 
 template <typename R>
 cudaError_t launch_hevi_stage(const Grid &g, const Members &mem, const StageArgsT<R> &a, int scheme,
-                              StageShape shape, cudaStream_t st, int *launches)
+                              StageShape shape, cudaStream_t st, int *launches, bool *tiled)
 {
     if (launches) *launches = 1;
+    if (tiled) *tiled = false;
     if (shape.tile_x == 0) {
         const cudaError_t e = launch_hevi_stage_tiled(g, mem, a, scheme, shape.raster, st);
         if (e != cudaErrorNotSupported) {
-            if (launches) *launches = 2;
+            if (tiled) *tiled = true;
             return e;
         }
     }
@@ -735,9 +736,9 @@ cudaError_t launch_hevi_stage(const Grid &g, const Members &mem, const StageArgs
     }
 }
 template cudaError_t launch_hevi_stage<double>(const Grid &, const Members &, const StageArgsT<double> &, int,
-                                               StageShape, cudaStream_t, int *);
+                                               StageShape, cudaStream_t, int *, bool *);
 template cudaError_t launch_hevi_stage<float>(const Grid &, const Members &, const StageArgsT<float> &, int,
-                                              StageShape, cudaStream_t, int *);
+                                              StageShape, cudaStream_t, int *, bool *);
 
 // =============================================================================
 // The HEVI stage with terrain-following metrics (GSQRT, J13G, J23G) and map

@@ -57,7 +57,7 @@ struct StageArgsT {
     F *facc;     // 6*N3: mflx Z,X,Y then tflx Z,X,Y
     unsigned *status;
     F *colscr; // Sr, St, tZ (3*N3, the fused kernel) and PT (4*N3, the tiled kernels)
-    double *colC; // N3: right-hand side C of the column problem (tiled kernels; null: fused kernel only)
+    double *colC; // 2*N3: right-hand side C of the column problem, then f; e (tiled kernels; null: fused only)
     int raster; // rows of tiles per raster group (set by the launcher)
 };
 using StageArgs = StageArgsT<double>;

@@ -1,29 +1,33 @@
 // The HEVI stage (ATMOS_DYN_Tstep_short_fvm_hevi,
 // scalelib/src/atmos-rm/dynamics/scale_atmos_dyn_tstep_short_fvm_hevi.F90:128-1089)
-// as two kernels that stage their tiles in shared memory with the tensor memory
-// accelerator (TMA). Line numbers refer to that file unless a flux file is named.
+// as one kernel, k_hevi_tiled, that stages its tiles in shared memory with the
+// tensor memory accelerator (TMA). Line numbers refer to that file unless a
+// flux file is named.
 //
-// k_hevi_explicit: everything explicit in the stage. A CTA owns a 4 x 4 tile of
-//   columns, one warp per column with its lanes along k, and marches up the
-//   column in chunks of 32 levels. For each chunk one thread issues
-//   cp.async.bulk.tensor copies of the five state fields (DENS, MOMZ, MOMX, MOMY,
-//   RHOT) over the tile, its lateral halo (2 points; 3 for the 6-point schemes)
-//   and the levels from 4 below to 2-3 above the chunk into shared memory,
-//   completing on an mbarrier; the tensor maps cover this GPU's own memory and
-//   the copies have no cluster multicast. Every stencil then reads shared
-//   memory at compile-time offsets. Per chunk:
-//     a. the pressure deviation DPRES (hevi_pres :343-361) of the tile and of
-//        its +x/+y neighbour columns; RHOT -> POTT in place (:586-600)
-//     b. x/y mass fluxes (:399-438), Sr (:443-479), PT and the vertical theta
-//        flux (valueW_Z, fluxZ_XYZ), the x/y theta fluxes and St (:603-661)
-//     c. one level lower: Sw (:528-578) and the right-hand side C (:698-722)
-//     d. rho*u and rho*v (hevi_momx :814-928, hevi_momy :934-1048)
-//   The fluxes and momenta leave through the RK folds of put_flux/put_state;
-//   Sr, St, tZ, PT and C go to the column scratch.
-// k_hevi_column: the implicit column problem. A CTA loads C, PT and A(k) of 16
-//   columns into shared memory, warp 0 runs the Thomas solve (solve_direct
-//   :1092-1127) one lane per column, and all warps back-update rho, rho*w and
-//   rho*theta and the vertical fluxes (:728-790).
+// A CTA owns a 4 x 4 tile of columns, one warp per column with its lanes along
+// k. It marches up the columns in chunks of 32 levels. For each chunk one
+// thread issues cp.async.bulk.tensor copies of the five state fields (DENS,
+// MOMZ, MOMX, MOMY, RHOT) over the tile, its lateral halo (2 points; 3 for the
+// 6-point schemes) and the levels from 4 below to 2-3 above the chunk into
+// shared memory, completing on an mbarrier; the tensor maps cover this GPU's
+// own memory and the copies have no cluster multicast. Every stencil then
+// reads shared memory at compile-time offsets. Per chunk:
+//   a. the pressure deviation DPRES (hevi_pres :343-361) of the tile and of its
+//      +x/+y neighbour columns; RHOT -> POTT in place (:586-600)
+//   b. x/y mass fluxes (:399-438), Sr (:443-479), PT and the vertical theta
+//      flux (valueW_Z, fluxZ_XYZ), the x/y theta fluxes and St (:603-661)
+//   c. one level lower: Sw (:528-578) and the right-hand side C (:698-722)
+//   d. rho*u and rho*v (hevi_momx :814-928, hevi_momy :934-1048)
+// The z flux through the face below a level is the previous lane's flux
+// above it, by a warp shuffle; lane 0 takes the previous chunk's lane 31's.
+// Chunks clear of the near-wall face forms run without level dispatch.
+// The fluxes and momenta leave through the RK folds of put_flux/put_state;
+// Sr, St, tZ, PT and C go to the column scratch. After the march the staged
+// box holds the tile's column arrays: C, PT and A(k) come back from the
+// scratch (L2-resident), warp 0 runs the Thomas solve (solve_direct
+// :1092-1127) one lane per column, and the warps back-update rho, rho*w,
+// rho*theta and the vertical fluxes (:728-790). While one CTA of an SM solves,
+// the other keeps the SM's issue slots busy with its march.
 //
 // Every value keeps the operation order of the fused kernel k_hevi_stage
 // (hevi_stage.cu) and of the reference, so the two forms give identical bits.
@@ -52,11 +56,12 @@ constexpr int NF = 5;                         // staged fields
 enum StagedField : int { F_DN = 0, F_MZ = 1, F_MX = 2, F_MY = 3, F_RT = 4 };
 constexpr int NDP = 33;                       // DPRES levels per column: L0-1 .. L0+31
 constexpr int DP_COLS = (TX + 1) * (TY + 1);  // tile columns and their +x/+y neighbours
+constexpr int NLT = 6;                        // level tables per chunk: RCDZ, RFDZ, F2H1, F2H2, FDZ, wdamp
 constexpr long long WAIT_CYCLES = 4000000000LL; // ~2 s: bound of every mbarrier wait
 
 template <int S> constexpr size_t smem_bytes()
 {
-    return (size_t)NF * plane<S>() * sizeof(double) + (size_t)DP_COLS * NDP * sizeof(double) + 16;
+    return (size_t)NF * plane<S>() * sizeof(double) + (size_t)(DP_COLS + NCOL + NLT) * NDP * sizeof(double) + 16;
 }
 
 struct StateMaps {
@@ -106,6 +111,15 @@ __device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, i
 // =============================================================================
 // k_hevi_explicit
 // =============================================================================
+// the face value at w-level m in a chunk that lies clear of the near-wall
+// forms: zface<S> without its level dispatch
+template <int S, typename R, typename V>
+__device__ __forceinline__ R zface_in(R vel, int m, const V &v)
+{
+    if constexpr (wide_scheme(S)) return ip6<S>(vel, v(m - 2), v(m - 1), v(m), v(m + 1), v(m + 2), v(m + 3));
+    else return ip4<S>(vel, v(m - 1), v(m), v(m + 1), v(m + 2));
+}
+
 template <int S, typename R, int NM>
 __global__ void __launch_bounds__(32 * NCOL, 2)
     k_hevi_explicit(const Grid gt, const StageArgsT<R> a, const BatchT<NM> B, const __grid_constant__ StateMaps maps)
@@ -116,7 +130,9 @@ __global__ void __launch_bounds__(32 * NCOL, 2)
     extern __shared__ __align__(1024) double sm[];
     double *stg = sm;                    // NF staged fields, [j][i][k] each
     double *sdp = sm + NF * PL;          // DPRES, [DP_COLS][NDP]
-    uint64_t *bar = reinterpret_cast<uint64_t *>(sdp + DP_COLS * NDP);
+    double *srp = sdp + DP_COLS * NDP;   // RT2P of the tile's own columns, [NCOL][NDP]
+    double *slt = srp + NCOL * NDP;      // the chunk's level tables, [NLT][NDP]
+    uint64_t *bar = reinterpret_cast<uint64_t *>(slt + NLT * NDP);
     __shared__ int s_ok;
 
     int b;
@@ -169,7 +185,14 @@ __global__ void __launch_bounds__(32 * NCOL, 2)
     const double *sDN = stg + F_DN * PL + cbox, *sMZ = stg + F_MZ * PL + cbox;
     const double *sMX = stg + F_MX * PL + cbox, *sMY = stg + F_MY * PL + cbox;
     double *sPO = stg + F_RT * PL + cbox; // RHOT, then POTT
-    R Sr_prev = R(0.0), St_prev = R(0.0); // Sr, St of the previous chunk (lane 31's are carried)
+    // Values of the previous chunk's lane 31 that lane 0 of the next chunk
+    // needs: the fluxes through the face below its level (mass, theta, w, u, v)
+    // and Sr, St one level down. Zero below KS, where every one of them is zero.
+    R Sr_prev = R(0.0), St_prev = R(0.0);
+    R cy_mZ = R(0.0), cy_tZ = R(0.0), cy_qw = R(0.0), cy_qu = R(0.0), cy_qv = R(0.0);
+    double cy_rd = 0.0; // REF_dens one level down
+    // broadcast of lane 31's value (the carry into the next chunk)
+    auto from31 = [&](R v) { return __shfl_sync(FULL, v, 31); };
 
     for (int ch = 0; ch < NC; ++ch) {
         const int L0 = KS + KC * ch, L = L0 + lane;
@@ -188,7 +211,19 @@ __global__ void __launch_bounds__(32 * NCOL, 2)
         }
         (void)mbar_try(bar, ch & 1); // completed phase: makes the copied data visible to this thread
 
-        // ---- a. DPRES of the tile and its +x/+y neighbours, levels L0-1..L0+31 (:355) ----
+        // ---- a. the chunk's level tables (levels L0-1..L0+31, clamped to KE), DPRES
+        // of the tile and its +x/+y neighbours (:355) ----
+        if (w == NCOL - 1) {
+            for (int lv = lane; lv < NDP; lv += 32) {
+                const int Lq = min(L0 - 1 + lv, KE);
+                slt[0 * NDP + lv] = ld(g.RCDZ + Lq - 1);
+                slt[1 * NDP + lv] = ld(g.RFDZ + Lq - 1);
+                slt[2 * NDP + lv] = ld(g.F2H1 + Lq - 1);
+                slt[3 * NDP + lv] = ld(g.F2H2 + Lq - 1);
+                slt[4 * NDP + lv] = ld(g.FDZ + Lq - 1);
+                slt[5 * NDP + lv] = ld(a.wdamp + g.z0 + Lq - 1);
+            }
+        }
         for (int q = w; q < DP_COLS; q += NCOL) {
             const int qx = q % (TX + 1), qy = q / (TX + 1);
             const int ii = i0 + qx, jj = j0 + qy;
@@ -199,7 +234,9 @@ __global__ void __launch_bounds__(32 * NCOL, 2)
                 const int Lq = L0 - 1 + lv;
                 if (Lq > KE) break;
                 const int cc = cq + Lq - 1;
-                sdp[q * NDP + lv] = ld(a.DPRES0 + cc) + ld(a.RT2P + cc) * (rt[lv] - ld(a.REF_rhot + cc));
+                const double rt2p = ld(a.RT2P + cc);
+                sdp[q * NDP + lv] = ld(a.DPRES0 + cc) + rt2p * (rt[lv] - ld(a.REF_rhot + cc));
+                if (qx < TX && qy < TY) srp[(qy * TX + qx) * NDP + lv] = rt2p;
             }
         }
         __syncthreads();
@@ -226,237 +263,276 @@ __global__ void __launch_bounds__(32 * NCOL, 2)
         }
         __syncthreads();
 
-        // ---- b. level L: mass and theta fluxes, Sr, St, PT, tZ ----
-        const bool vb = col_ok && L <= KE;
-        const int c = col + L - 1;
-        R Sr = R(0.0), St = R(0.0);
-        {
-            // the vertical mass flux through the faces above and below L (hevi_mflx_z :383-391)
-            const R mZ = (vb && L <= KE - 1) ? ld(nd.DZ() + c) : R(0.0);
-            R mZm1 = __shfl_up_sync(FULL, mZ, 1);
-            if (lane == 0) mZm1 = (vb && L - 1 >= KS) ? ld(nd.DZ() + c - 1) : R(0.0);
-            auto P = [&](int l) { return R(sPO[l - L]); };
-            auto pt_tz = [&](int Lq, R &pt, R &tz) {
-                if (Lq < KS || Lq > KE - 1) { pt = R(0.0); tz = R(0.0); return; }
-                const R m = ld(nd.DZ() + col + Lq - 1);
-                const R M0 = R(sMZ[Lq - L]);
-                pt = zface<S>(M0, Lq, KS, KE, P);
-                tz = m * zface<S>(m, Lq, KS, KE, P) + lds(nd.TZ() + col + Lq - 1);
+        // Chunks clear of the near-wall face forms (every face of the chunk, from
+        // the one below L0-1 to the one above L0+31, in the interior range, and
+        // every level of the chunk at or below KE) run without level dispatch or
+        // range checks: EDGE = false.
+        const bool interior = L0 - 1 >= KS + (W6 ? 2 : 1) && L0 + 31 <= KE - (W6 ? 3 : 2);
+        // the level tables at this lane's level L (slot lane+1) and at k = L-1 (slot lane)
+        const double *lt = slt + lane;
+#define rcdz_L lt[0 * NDP + 1]
+#define rfdz_k lt[1 * NDP]
+#define f1_L lt[2 * NDP + 1]
+#define f1_k lt[2 * NDP]
+#define f2_L lt[3 * NDP + 1]
+#define f2_k lt[3 * NDP]
+#define fdz_k lt[4 * NDP]
+#define wd_k lt[5 * NDP]
+        auto chunk = [&](auto edge) {
+            constexpr bool EDGE = decltype(edge)::value;
+            auto zf = [&](R vel, int m, const auto &v) -> R {
+                if constexpr (EDGE) return zface<S>(vel, m, KS, KE, v);
+                else return zface_in<S>(vel, m, v);
             };
-            R PT = R(0.0), tZ = R(0.0);
-            if (vb) pt_tz(L, PT, tZ);
-            R tZm = __shfl_up_sync(FULL, tZ, 1);
-            if (lane == 0 && vb) { R ptm; pt_tz(L - 1, ptm, tZm); }
-            if (vb) {
-                const R Xe = R(sMX[0]) + ld(nd.DX() + c), Xw = R(sMX[-KX]) + ld(nd.DX() + c - sI);
-                const R Yn = R(sMY[0]) + ld(nd.DY() + c), Ys = R(sMY[-KY]) + ld(nd.DY() + c - sJ);
-                const R adv_r = -((Xe - Xw) * rcdx + (Yn - Ys) * rcdy);
-                put_flux(a, N3, 1, c, Xe, true);
-                put_flux(a, N3, 2, c, Yn, true);
-                if (i == g.IS) put_flux(a, N3, 1, c - sI, Xw, false);
-                if (j == g.JS) put_flux(a, N3, 2, c - sJ, Ys, false);
-                const R rcdz = R(ld(g.RCDZ + L - 1));
-                Sr = (-(mZ - mZm1) * rcdz + adv_r) + lds(a.DENS_t + c);
-                // fluxX/Y_XYZ (ud3.F90:251-353)
-                const R P00 = R(sPO[0]);
-                const R Pm2 = R(sPO[-2 * KX]), Pm1 = R(sPO[-KX]), Pp1 = R(sPO[KX]), Pp2 = R(sPO[2 * KX]);
-                const R Qm2 = R(sPO[-2 * KY]), Qm1 = R(sPO[-KY]), Qp1 = R(sPO[KY]), Qp2 = R(sPO[2 * KY]);
-                const R Pm3 = W6 ? R(sPO[-3 * KX]) : R(0.0), Pp3 = W6 ? R(sPO[3 * KX]) : R(0.0);
-                const R Qm3 = W6 ? R(sPO[-3 * KY]) : R(0.0), Qp3 = W6 ? R(sPO[3 * KY]) : R(0.0);
-                const R tXe = Xe * ip6<S>(Xe, Pm2, Pm1, P00, Pp1, Pp2, Pp3) + ld(nd.TX() + c);
-                const R tXw = Xw * ip6<S>(Xw, Pm3, Pm2, Pm1, P00, Pp1, Pp2) + ld(nd.TX() + c - sI);
-                const R tYn = Yn * ip6<S>(Yn, Qm2, Qm1, P00, Qp1, Qp2, Qp3) + ld(nd.TY() + c);
-                const R tYs = Ys * ip6<S>(Ys, Qm3, Qm2, Qm1, P00, Qp1, Qp2) + ld(nd.TY() + c - sJ);
-                const R adv_t = -((tXe - tXw) * rcdx + (tYn - tYs) * rcdy); // hevi_st :646-648
-                put_flux(a, N3, 4, c, tXe, true);
-                put_flux(a, N3, 5, c, tYn, true);
-                if (i == g.IS) put_flux(a, N3, 4, c - sI, tXw, false);
-                if (j == g.JS) put_flux(a, N3, 5, c - sJ, tYs, false);
-                St = (-(tZ - tZm) * rcdz + adv_t) + lds(a.RHOT_t + c); // hevi_st :646-649
-                sSr[c] = Sr;
-                sSt[c] = St;
-                stZ[c] = tZ;
-                sPT[c] = PT;
+            // ---- b. level L: mass and theta fluxes, Sr, St, PT, tZ ----
+            const bool vb = col_ok && (!EDGE || L <= KE);
+            const int c = col + L - 1;
+            R Sr = R(0.0), St = R(0.0);
+            {
+                // the vertical mass flux through the face above L (hevi_mflx_z :383-391);
+                // the face below is the previous lane's (lane 0: the previous chunk's lane 31)
+                const R mZ = (vb && (!EDGE || L <= KE - 1)) ? ld(nd.DZ() + c) : R(0.0);
+                R mZm1 = __shfl_up_sync(FULL, mZ, 1);
+                if (lane == 0) mZm1 = cy_mZ;
+                cy_mZ = from31(mZ);
+                auto P = [&](int l) { return R(sPO[l - L]); };
+                R PT = R(0.0), tZ = R(0.0);
+                if (vb && (!EDGE || L <= KE - 1)) {
+                    // PT: valueW_Z (ud3.F90:98-153); tZ: fluxZ_XYZ (ud3.F90:157-247)
+                    PT = zf(R(sMZ[0]), L, P);
+                    tZ = mZ * zf(mZ, L, P) + lds(nd.TZ() + c);
+                }
+                R tZm = __shfl_up_sync(FULL, tZ, 1);
+                if (lane == 0) tZm = cy_tZ;
+                cy_tZ = from31(tZ);
+                if (vb) {
+                    const R Xe = R(sMX[0]) + ld(nd.DX() + c), Xw = R(sMX[-KX]) + ld(nd.DX() + c - sI);
+                    const R Yn = R(sMY[0]) + ld(nd.DY() + c), Ys = R(sMY[-KY]) + ld(nd.DY() + c - sJ);
+                    const R adv_r = -((Xe - Xw) * rcdx + (Yn - Ys) * rcdy);
+                    put_flux(a, N3, 1, c, Xe, true);
+                    put_flux(a, N3, 2, c, Yn, true);
+                    if (i == g.IS) put_flux(a, N3, 1, c - sI, Xw, false);
+                    if (j == g.JS) put_flux(a, N3, 2, c - sJ, Ys, false);
+                    const R rcdz = R(rcdz_L);
+                    Sr = (-(mZ - mZm1) * rcdz + adv_r) + lds(a.DENS_t + c);
+                    // fluxX/Y_XYZ (ud3.F90:251-353)
+                    const R P00 = R(sPO[0]);
+                    const R Pm2 = R(sPO[-2 * KX]), Pm1 = R(sPO[-KX]), Pp1 = R(sPO[KX]), Pp2 = R(sPO[2 * KX]);
+                    const R Qm2 = R(sPO[-2 * KY]), Qm1 = R(sPO[-KY]), Qp1 = R(sPO[KY]), Qp2 = R(sPO[2 * KY]);
+                    const R Pm3 = W6 ? R(sPO[-3 * KX]) : R(0.0), Pp3 = W6 ? R(sPO[3 * KX]) : R(0.0);
+                    const R Qm3 = W6 ? R(sPO[-3 * KY]) : R(0.0), Qp3 = W6 ? R(sPO[3 * KY]) : R(0.0);
+                    const R tXe = Xe * ip6<S>(Xe, Pm2, Pm1, P00, Pp1, Pp2, Pp3) + ld(nd.TX() + c);
+                    const R tXw = Xw * ip6<S>(Xw, Pm3, Pm2, Pm1, P00, Pp1, Pp2) + ld(nd.TX() + c - sI);
+                    const R tYn = Yn * ip6<S>(Yn, Qm2, Qm1, P00, Qp1, Qp2, Qp3) + ld(nd.TY() + c);
+                    const R tYs = Ys * ip6<S>(Ys, Qm3, Qm2, Qm1, P00, Qp1, Qp2) + ld(nd.TY() + c - sJ);
+                    const R adv_t = -((tXe - tXw) * rcdx + (tYn - tYs) * rcdy); // hevi_st :646-648
+                    put_flux(a, N3, 4, c, tXe, true);
+                    put_flux(a, N3, 5, c, tYn, true);
+                    if (i == g.IS) put_flux(a, N3, 4, c - sI, tXw, false);
+                    if (j == g.JS) put_flux(a, N3, 5, c - sJ, tYs, false);
+                    St = (-(tZ - tZm) * rcdz + adv_t) + lds(a.RHOT_t + c); // hevi_st :646-649
+                    sSr[c] = Sr;
+                    sSt[c] = St;
+                    stZ[c] = tZ;
+                    sPT[c] = PT;
+                }
             }
-        }
 
-        // ---- c. level k = L-1: Sw (hevi_sw :528-578) and C(k) (:698-722) ----
-        {
-            R Sr_k = __shfl_up_sync(FULL, Sr, 1), St_k = __shfl_up_sync(FULL, St, 1);
-            const R Sr_c = __shfl_sync(FULL, Sr_prev, 31), St_c = __shfl_sync(FULL, St_prev, 31);
-            if (lane == 0) { Sr_k = Sr_c; St_k = St_c; }
-            Sr_prev = Sr;
-            St_prev = St;
-            const int k = L - 1;
-            const bool vc = col_ok && k >= KS && k <= KE - 1;
-            const double *cMZ = sMZ - 1, *cDN = sDN - 1, *cMX = sMX - 1, *cMY = sMY - 1; // level k
-            const int ck = c - 1;
-            auto vMZ = [&](int l) { return R(cMZ[l - k]); };
-            // vertical w-momentum flux above level kq, fluxZ_XYW (ud3.F90:358-452), zero outside KS..KE-2
-            auto qZ_at = [&](int kq) -> R {
-                if (kq < KS || kq > KE - 2) return R(0.0);
-                const R vel = (R(0.5) * (vMZ(kq) + vMZ(kq + 1))) / R(cDN[kq + 1 - k]);
-                const R q = zface<S>(vel, kq, KS, KE, vMZ);
-                return J33R * vel * q + lds(nd.WZ() + col + kq);
-            };
-            const R q_k = vc ? qZ_at(k) : R(0.0);
-            R q_km = __shfl_up_sync(FULL, q_k, 1);
-            if (lane == 0 && vc) q_km = qZ_at(k - 1);
-            if (vc) {
-                // horizontal w-momentum flux divergence, fluxX/Y_XYW (ud3.F90:598-748)
-                R adv_w;
+            // ---- c. level k = L-1: Sw (hevi_sw :528-578) and C(k) (:698-722) ----
+            {
+                R Sr_k = __shfl_up_sync(FULL, Sr, 1), St_k = __shfl_up_sync(FULL, St, 1);
+                if (lane == 0) { Sr_k = Sr_prev; St_k = St_prev; }
+                Sr_prev = from31(Sr);
+                St_prev = from31(St);
+                const int k = L - 1;
+                const bool vc = col_ok && (!EDGE || (k >= KS && k <= KE - 1));
+                const double *cMZ = sMZ - 1, *cDN = sDN - 1, *cMX = sMX - 1, *cMY = sMY - 1; // level k
+                const int ck = c - 1;
+                auto vMZ = [&](int l) { return R(cMZ[l - k]); };
+                // vertical w-momentum flux above level k, fluxZ_XYW (ud3.F90:358-452),
+                // zero outside KS..KE-2; the one below is the previous lane's
+                R q_k = R(0.0);
+                if (vc && (!EDGE || k <= KE - 2)) {
+                    const R vel = (R(0.5) * (vMZ(k) + vMZ(k + 1))) / R(cDN[1]);
+                    q_k = J33R * vel * zf(vel, k, vMZ) + lds(nd.WZ() + col + k);
+                }
+                R q_km = __shfl_up_sync(FULL, q_k, 1);
+                if (lane == 0) q_km = cy_qw;
+                cy_qw = from31(q_k);
+                const double rd1 = vb ? lds(a.REF_dens + c) : 0.0; // REF_dens(k+1)
+                double rd0 = __shfl_up_sync(FULL, rd1, 1);         // REF_dens(k)
+                if (lane == 0) rd0 = cy_rd;
+                cy_rd = __shfl_sync(FULL, rd1, 31);
+                if (vc) {
+                    // horizontal w-momentum flux divergence, fluxX/Y_XYW (ud3.F90:598-748)
+                    R adv_w;
+                    {
+                        const R f1 = R(f1_k), f2 = R(f2_k);
+                        const R vXe = (f1 * R(cMX[1]) + f2 * R(cMX[0]))
+                                      / (f1 * h * (R(cDN[1]) + R(cDN[1 + KX])) + f2 * h * (R(cDN[0]) + R(cDN[KX])));
+                        const R vXw = (f1 * R(cMX[1 - KX]) + f2 * R(cMX[-KX]))
+                                      / (f1 * h * (R(cDN[1 - KX]) + R(cDN[1])) + f2 * h * (R(cDN[-KX]) + R(cDN[0])));
+                        const R vYn = (f1 * R(cMY[1]) + f2 * R(cMY[0]))
+                                      / (f1 * h * (R(cDN[1]) + R(cDN[1 + KY])) + f2 * h * (R(cDN[0]) + R(cDN[KY])));
+                        const R vYs = (f1 * R(cMY[1 - KY]) + f2 * R(cMY[-KY]))
+                                      / (f1 * h * (R(cDN[1 - KY]) + R(cDN[1])) + f2 * h * (R(cDN[-KY]) + R(cDN[0])));
+                        const R W_m2 = R(cMZ[-2 * KX]), W_m1 = R(cMZ[-KX]), W_00 = R(cMZ[0]);
+                        const R W_p1 = R(cMZ[KX]), W_p2 = R(cMZ[2 * KX]);
+                        const R V_m2 = R(cMZ[-2 * KY]), V_m1 = R(cMZ[-KY]), V_p1 = R(cMZ[KY]), V_p2 = R(cMZ[2 * KY]);
+                        const R W_m3 = W6 ? R(cMZ[-3 * KX]) : R(0.0), W_p3 = W6 ? R(cMZ[3 * KX]) : R(0.0);
+                        const R V_m3 = W6 ? R(cMZ[-3 * KY]) : R(0.0), V_p3 = W6 ? R(cMZ[3 * KY]) : R(0.0);
+                        const R qXe = vXe * ip6<S>(vXe, W_m2, W_m1, W_00, W_p1, W_p2, W_p3) + ld(nd.WX() + ck);
+                        const R qXw = vXw * ip6<S>(vXw, W_m3, W_m2, W_m1, W_00, W_p1, W_p2) + ld(nd.WX() + ck - sI);
+                        const R qYn = vYn * ip6<S>(vYn, V_m2, V_m1, W_00, V_p1, V_p2, V_p3) + ld(nd.WY() + ck);
+                        const R qYs = vYs * ip6<S>(vYs, V_m3, V_m2, V_m1, W_00, V_p1, V_p2) + ld(nd.WY() + ck - sJ);
+                        adv_w = -((qXe - qXw) * rcdx + (qYn - qYs) * rcdy);
+                    }
+                    const R advcv = -(q_k - q_km) * R(rfdz_k);
+                    const R wdmp = -R(wd_k) * R(ld(a.MOMZ0 + ck));
+                    const R div = use_div ? ddc * (ld(a.DDIV + ck + 1) - ld(a.DDIV + ck)) * R(fdz_k) : R(0.0);
+                    const R Sw = (advcv + adv_w) + wdmp + div + lds(a.MOMZ_t + ck);
+                    const double rfdz = rfdz_k;
+                    const double *rp = srp + w * NDP + lane; // RT2P at level k
+                    const double RTL1 = rp[1], RTL0 = rp[0];
+                    const double *dp = sdp + (ty * (TX + 1) + tx) * NDP + lane; // DPRES at level k (slot k-L0+1 = lane)
+                    const double pg = -(dp[1] + RTL1 * dt * (double)St - dp[0] - RTL0 * dt * (double)St_k) * rfdz * J33G
+                                      - GRAV * (f1_k * (cDN[1] - rd1 + (double)Sr * dt)
+                                                + f2_k * (cDN[0] - rd0 + (double)Sr_k * dt));
+                    a.colC[ck] = cMZ[0] + dt * (pg + (double)Sw);
+                }
+            }
+
+            // ---- d. rho*u (hevi_momx :814-928) and rho*v (hevi_momy :934-1048) at level L ----
+            {
+                const double *dp = sdp + (ty * (TX + 1) + tx) * NDP + lane + 1; // DPRES at level L, this column
+                auto vMX = [&](int l) { return R(sMX[l - L]); };
+                auto vMY = [&](int l) { return R(sMY[l - L]); };
+                const bool do_u = vb && i <= g.IEH, do_v = vb && j <= g.JEH;
+                const bool zok = !EDGE || L <= KE - 1; // the face above L carries a flux
+                // u: the z flux at (u,y,w) above L, fluxZ_UYZ (ud3.F90:753-859); the one
+                // below is the previous lane's
                 {
-                    const R f1 = R(ld(g.F2H1 + k - 1)), f2 = R(ld(g.F2H2 + k - 1));
-                    const R vXe = (f1 * R(cMX[1]) + f2 * R(cMX[0]))
-                                  / (f1 * h * (R(cDN[1]) + R(cDN[1 + KX])) + f2 * h * (R(cDN[0]) + R(cDN[KX])));
-                    const R vXw = (f1 * R(cMX[1 - KX]) + f2 * R(cMX[-KX]))
-                                  / (f1 * h * (R(cDN[1 - KX]) + R(cDN[1])) + f2 * h * (R(cDN[-KX]) + R(cDN[0])));
-                    const R vYn = (f1 * R(cMY[1]) + f2 * R(cMY[0]))
-                                  / (f1 * h * (R(cDN[1]) + R(cDN[1 + KY])) + f2 * h * (R(cDN[0]) + R(cDN[KY])));
-                    const R vYs = (f1 * R(cMY[1 - KY]) + f2 * R(cMY[-KY]))
-                                  / (f1 * h * (R(cDN[1 - KY]) + R(cDN[1])) + f2 * h * (R(cDN[-KY]) + R(cDN[0])));
-                    const R W_m2 = R(cMZ[-2 * KX]), W_m1 = R(cMZ[-KX]), W_00 = R(cMZ[0]);
-                    const R W_p1 = R(cMZ[KX]), W_p2 = R(cMZ[2 * KX]);
-                    const R V_m2 = R(cMZ[-2 * KY]), V_m1 = R(cMZ[-KY]), V_p1 = R(cMZ[KY]), V_p2 = R(cMZ[2 * KY]);
-                    const R W_m3 = W6 ? R(cMZ[-3 * KX]) : R(0.0), W_p3 = W6 ? R(cMZ[3 * KX]) : R(0.0);
-                    const R V_m3 = W6 ? R(cMZ[-3 * KY]) : R(0.0), V_p3 = W6 ? R(cMZ[3 * KY]) : R(0.0);
-                    const R qXe = vXe * ip6<S>(vXe, W_m2, W_m1, W_00, W_p1, W_p2, W_p3) + ld(nd.WX() + ck);
-                    const R qXw = vXw * ip6<S>(vXw, W_m3, W_m2, W_m1, W_00, W_p1, W_p2) + ld(nd.WX() + ck - sI);
-                    const R qYn = vYn * ip6<S>(vYn, V_m2, V_m1, W_00, V_p1, V_p2, V_p3) + ld(nd.WY() + ck);
-                    const R qYs = vYs * ip6<S>(vYs, V_m3, V_m2, V_m1, W_00, V_p1, V_p2) + ld(nd.WY() + ck - sJ);
-                    adv_w = -((qXe - qXw) * rcdx + (qYn - qYs) * rcdy);
+                    R q_k = R(0.0);
+                    if (do_u && zok) {
+                        const R den = R(f1_L) * h * (R(sDN[1]) + R(sDN[1 + KX]))
+                                      + R(f2_L) * h * (R(sDN[0]) + R(sDN[KX]));
+                        const R vel = (h * (R(sMZ[0]) + R(sMZ[KX]))) / den;
+                        q_k = J33R * vel * zf(vel, L, vMX) + lds(nd.UZ() + c);
+                    }
+                    R q_km = __shfl_up_sync(FULL, q_k, 1);
+                    if (lane == 0) q_km = cy_qu;
+                    cy_qu = from31(q_k);
+                    if (do_u) {
+                        const R fdx = R(ld(g.FDX + i - 1));
+                        const double rfdx = ld(g.RFDX + i - 1);
+                        const R cor_u = R(0.125) * (R(ld(a.CORIOLI + g.c2 + (i) + (size_t)g.IA * (j - 1)))
+                                                    + R(ld(a.CORIOLI + g.c2 + (i - 1) + (size_t)g.IA * (j - 1))));
+                        const R U_m2 = R(sMX[-2 * KX]), U_m1 = R(sMX[-KX]), U_00 = R(sMX[0]);
+                        const R U_p1 = R(sMX[KX]), U_p2 = R(sMX[2 * KX]);
+                        // x flux at (x,y,z) with the index shift of fluxX_UYZ (ud3.F90:1053-1109)
+                        const R vE = (h * (U_p1 + U_00)) / (R(sDN[KX]));
+                        const R U_m3 = W6 ? R(sMX[-3 * KX]) : R(0.0), U_p3 = W6 ? R(sMX[3 * KX]) : R(0.0);
+                        const R qXe = vE * ip6<S>(vE, U_m2, U_m1, U_00, U_p1, U_p2, U_p3) + ld(nd.UX() + c + sI);
+                        const R vW = (h * (U_00 + U_m1)) / (R(sDN[0]));
+                        const R qXw = vW * ip6<S>(vW, U_m3, U_m2, U_m1, U_00, U_p1, U_p2) + ld(nd.UX() + c);
+                        // y flux at (u,v,z), fluxY_UYZ (ud3.F90:1113-1167)
+                        const R vN = (h * (R(sMY[0]) + R(sMY[KX])))
+                                     / (qr * (R(sDN[0]) + R(sDN[KX]) + R(sDN[KY]) + R(sDN[KX + KY])));
+                        const R qYn = vN * ip6<S>(vN, W6 ? R(sMX[-2 * KY]) : R(0.0), R(sMX[-KY]), U_00, R(sMX[KY]),
+                                                  R(sMX[2 * KY]), W6 ? R(sMX[3 * KY]) : R(0.0)) + ld(nd.UY() + c);
+                        const R vS = (h * (R(sMY[-KY]) + R(sMY[KX - KY])))
+                                     / (qr * (R(sDN[-KY]) + R(sDN[KX - KY]) + R(sDN[0]) + R(sDN[KX])));
+                        const R qYs = vS * ip6<S>(vS, W6 ? R(sMX[-3 * KY]) : R(0.0), R(sMX[-2 * KY]), R(sMX[-KY]), U_00,
+                                                  R(sMX[KY]), W6 ? R(sMX[2 * KY]) : R(0.0)) + ld(nd.UY() + c - sJ);
+                        const R advcv = -(q_k - q_km) * R(rcdz_L);
+                        const R advch = -((qXe - qXw) * R(rfdx) + (qYn - qYs) * rcdy);
+                        const double DPe = dp[NDP]; // DPRES at (i+1, j)
+                        const double pg = (DPe - dp[0]) * rfdx;
+                        const R cf = cor_u * (R(sMY[KX]) + R(sMY[0]) + R(sMY[KX - KY]) + R(sMY[-KY]));
+                        const R div = !use_div ? R(0.0) : ddc * (ld(a.DDIV + c + sI) - ld(a.DDIV + c)) * fdx;
+                        const double val = lds(a.MOMX0 + c)
+                                           + dt * (((((double)(advcv + advch)) - pg) + (double)cf) + (double)div
+                                                   + (double)lds(a.MOMX_t + c));
+                        put_state(a, N3, 2, a.MOMX_RK, a.MOMX0, c, val, true);
+                    }
                 }
-                const R advcv = -(q_k - q_km) * R(ld(g.RFDZ + k - 1));
-                const R wdmp = -R(ld(a.wdamp + g.z0 + k - 1)) * R(ld(a.MOMZ0 + ck));
-                const R div = use_div ? ddc * (ld(a.DDIV + ck + 1) - ld(a.DDIV + ck)) * R(ld(g.FDZ + k - 1)) : R(0.0);
-                const R Sw = (advcv + adv_w) + wdmp + div + lds(a.MOMZ_t + ck);
-                const double rfdz = ld(g.RFDZ + k - 1);
-                const double RTL1 = ld(a.RT2P + ck + 1), RTL0 = ld(a.RT2P + ck);
-                const double *dp = sdp + (ty * (TX + 1) + tx) * NDP + lane; // DPRES at level k (slot k-L0+1 = lane)
-                const double pg = -(dp[1] + RTL1 * dt * (double)St - dp[0] - RTL0 * dt * (double)St_k) * rfdz * J33G
-                                  - GRAV * (ld(g.F2H1 + k - 1) * (cDN[1] - lds(a.REF_dens + ck + 1) + (double)Sr * dt)
-                                            + ld(g.F2H2 + k - 1) * (cDN[0] - lds(a.REF_dens + ck) + (double)Sr_k * dt));
-                a.colC[ck] = cMZ[0] + dt * (pg + (double)Sw);
-            }
-        }
-
-        // ---- d. rho*u (hevi_momx :814-928) and rho*v (hevi_momy :934-1048) at level L ----
-        {
-            const double rcdz_d = vb ? ld(g.RCDZ + L - 1) : 0.0;
-            const double *dp = sdp + (ty * (TX + 1) + tx) * NDP + lane + 1; // DPRES at level L, this column
-            auto vMX = [&](int l) { return R(sMX[l - L]); };
-            auto vMY = [&](int l) { return R(sMY[l - L]); };
-            // z flux at (u,y,w), fluxZ_UYZ (ud3.F90:753-859); m is the lower level of the face
-            auto qZu = [&](int m) -> R {
-                if (m < KS || m > KE - 1) return R(0.0);
-                const int dm = m - L;
-                const R den = R(ld(g.F2H1 + m - 1)) * h * (R(sDN[dm + 1]) + R(sDN[dm + 1 + KX]))
-                              + R(ld(g.F2H2 + m - 1)) * h * (R(sDN[dm]) + R(sDN[dm + KX]));
-                const R vel = (h * (R(sMZ[dm]) + R(sMZ[dm + KX]))) / den;
-                const R q = zface<S>(vel, m, KS, KE, vMX);
-                return J33R * vel * q + lds(nd.UZ() + c + dm);
-            };
-            // z flux at (x,v,w), fluxZ_XVZ (ud3.F90:1173-1279)
-            auto qZv = [&](int m) -> R {
-                if (m < KS || m > KE - 1) return R(0.0);
-                const int dm = m - L;
-                const R den = R(ld(g.F2H1 + m - 1)) * h * (R(sDN[dm + 1]) + R(sDN[dm + 1 + KY]))
-                              + R(ld(g.F2H2 + m - 1)) * h * (R(sDN[dm]) + R(sDN[dm + KY]));
-                const R vel = (h * (R(sMZ[dm]) + R(sMZ[dm + KY]))) / den;
-                const R q = zface<S>(vel, m, KS, KE, vMY);
-                return J33R * vel * q + lds(nd.VZ() + c + dm);
-            };
-            const bool do_u = vb && i <= g.IEH, do_v = vb && j <= g.JEH;
-            // u: the z flux above L; the one below comes from the previous lane
-            {
-                const R q_k = do_u ? qZu(L) : R(0.0);
-                R q_km = __shfl_up_sync(FULL, q_k, 1);
-                if (lane == 0 && do_u) q_km = qZu(L - 1);
-                if (do_u) {
-                    const R fdx = R(ld(g.FDX + i - 1));
-                    const double rfdx = ld(g.RFDX + i - 1);
-                    const R cor_u = R(0.125) * (R(ld(a.CORIOLI + g.c2 + (i) + (size_t)g.IA * (j - 1)))
-                                                + R(ld(a.CORIOLI + g.c2 + (i - 1) + (size_t)g.IA * (j - 1))));
-                    const R U_m2 = R(sMX[-2 * KX]), U_m1 = R(sMX[-KX]), U_00 = R(sMX[0]);
-                    const R U_p1 = R(sMX[KX]), U_p2 = R(sMX[2 * KX]);
-                    // x flux at (x,y,z) with the index shift of fluxX_UYZ (ud3.F90:1053-1109)
-                    const R vE = (h * (U_p1 + U_00)) / (R(sDN[KX]));
-                    const R U_m3 = W6 ? R(sMX[-3 * KX]) : R(0.0), U_p3 = W6 ? R(sMX[3 * KX]) : R(0.0);
-                    const R qXe = vE * ip6<S>(vE, U_m2, U_m1, U_00, U_p1, U_p2, U_p3) + ld(nd.UX() + c + sI);
-                    const R vW = (h * (U_00 + U_m1)) / (R(sDN[0]));
-                    const R qXw = vW * ip6<S>(vW, U_m3, U_m2, U_m1, U_00, U_p1, U_p2) + ld(nd.UX() + c);
-                    // y flux at (u,v,z), fluxY_UYZ (ud3.F90:1113-1167)
-                    const R vN = (h * (R(sMY[0]) + R(sMY[KX])))
-                                 / (qr * (R(sDN[0]) + R(sDN[KX]) + R(sDN[KY]) + R(sDN[KX + KY])));
-                    const R qYn = vN * ip6<S>(vN, W6 ? R(sMX[-2 * KY]) : R(0.0), R(sMX[-KY]), U_00, R(sMX[KY]),
-                                              R(sMX[2 * KY]), W6 ? R(sMX[3 * KY]) : R(0.0)) + ld(nd.UY() + c);
-                    const R vS = (h * (R(sMY[-KY]) + R(sMY[KX - KY])))
-                                 / (qr * (R(sDN[-KY]) + R(sDN[KX - KY]) + R(sDN[0]) + R(sDN[KX])));
-                    const R qYs = vS * ip6<S>(vS, W6 ? R(sMX[-3 * KY]) : R(0.0), R(sMX[-2 * KY]), R(sMX[-KY]), U_00,
-                                              R(sMX[KY]), W6 ? R(sMX[2 * KY]) : R(0.0)) + ld(nd.UY() + c - sJ);
-                    const R advcv = -(q_k - q_km) * R(rcdz_d);
-                    const R advch = -((qXe - qXw) * R(rfdx) + (qYn - qYs) * rcdy);
-                    const double DPe = dp[NDP]; // DPRES at (i+1, j)
-                    const double pg = (DPe - dp[0]) * rfdx;
-                    const R cf = cor_u * (R(sMY[KX]) + R(sMY[0]) + R(sMY[KX - KY]) + R(sMY[-KY]));
-                    const R div = !use_div ? R(0.0) : ddc * (ld(a.DDIV + c + sI) - ld(a.DDIV + c)) * fdx;
-                    const double val = lds(a.MOMX0 + c)
-                                       + dt * (((((double)(advcv + advch)) - pg) + (double)cf) + (double)div
-                                               + (double)lds(a.MOMX_t + c));
-                    put_state(a, N3, 2, a.MOMX_RK, a.MOMX0, c, val, true);
+                // v: the z flux at (x,v,w), fluxZ_XVZ (ud3.F90:1173-1279)
+                {
+                    R q_k = R(0.0);
+                    if (do_v && zok) {
+                        const R den = R(f1_L) * h * (R(sDN[1]) + R(sDN[1 + KY]))
+                                      + R(f2_L) * h * (R(sDN[0]) + R(sDN[KY]));
+                        const R vel = (h * (R(sMZ[0]) + R(sMZ[KY]))) / den;
+                        q_k = J33R * vel * zf(vel, L, vMY) + lds(nd.VZ() + c);
+                    }
+                    R q_km = __shfl_up_sync(FULL, q_k, 1);
+                    if (lane == 0) q_km = cy_qv;
+                    cy_qv = from31(q_k);
+                    if (do_v) {
+                        const R fdy = R(ld(g.FDY + j - 1));
+                        const double rfdy = ld(g.RFDY + j - 1);
+                        const R cor_v = R(-0.125) * (R(ld(a.CORIOLI + g.c2 + (i - 1) + (size_t)g.IA * (j)))
+                                                     + R(ld(a.CORIOLI + g.c2 + (i - 1) + (size_t)g.IA * (j - 1))));
+                        const R Y_m2 = R(sMY[-2 * KY]), Y_m1 = R(sMY[-KY]), Y_00 = R(sMY[0]);
+                        const R Y_p1 = R(sMY[KY]), Y_p2 = R(sMY[2 * KY]);
+                        // x flux at (u,v,z), fluxX_XVZ (ud3.F90:1473-1527)
+                        const R vE = (h * (R(sMX[0]) + R(sMX[KY])))
+                                     / (qr * (R(sDN[0]) + R(sDN[KX]) + R(sDN[KY]) + R(sDN[KX + KY])));
+                        const R qXe = vE * ip6<S>(vE, W6 ? R(sMY[-2 * KX]) : R(0.0), R(sMY[-KX]), Y_00, R(sMY[KX]),
+                                                  R(sMY[2 * KX]), W6 ? R(sMY[3 * KX]) : R(0.0)) + ld(nd.VX() + c);
+                        const R vW = (h * (R(sMX[-KX]) + R(sMX[KY - KX])))
+                                     / (qr * (R(sDN[-KX]) + R(sDN[0]) + R(sDN[KY - KX]) + R(sDN[KY])));
+                        const R qXw = vW * ip6<S>(vW, W6 ? R(sMY[-3 * KX]) : R(0.0), R(sMY[-2 * KX]), R(sMY[-KX]), Y_00,
+                                                  R(sMY[KX]), W6 ? R(sMY[2 * KX]) : R(0.0)) + ld(nd.VX() + c - sI);
+                        // y flux with the index shift of fluxY_XVZ (ud3.F90:1531-1587)
+                        const R vN = (h * (Y_p1 + Y_00)) / (R(sDN[KY]));
+                        const R Y_m3 = W6 ? R(sMY[-3 * KY]) : R(0.0), Y_p3 = W6 ? R(sMY[3 * KY]) : R(0.0);
+                        const R qYn = vN * ip6<S>(vN, Y_m2, Y_m1, Y_00, Y_p1, Y_p2, Y_p3) + ld(nd.VY() + c + sJ);
+                        const R vS = (h * (Y_00 + Y_m1)) / (R(sDN[0]));
+                        const R qYs = vS * ip6<S>(vS, Y_m3, Y_m2, Y_m1, Y_00, Y_p1, Y_p2) + ld(nd.VY() + c);
+                        const R advcv = -(q_k - q_km) * R(rcdz_L);
+                        const R advch = -((qXe - qXw) * rcdx + (qYn - qYs) * R(rfdy));
+                        const double DPn = dp[(TX + 1) * NDP]; // DPRES at (i, j+1)
+                        const double pg = (DPn - dp[0]) * rfdy;
+                        const R cf = cor_v * (R(sMX[KY]) + R(sMX[0]) + R(sMX[KY - KX]) + R(sMX[-KX]));
+                        const R div = !use_div ? R(0.0) : ddc * (ld(a.DDIV + c + sJ) - ld(a.DDIV + c)) * fdy;
+                        const double val = lds(a.MOMY0 + c)
+                                           + dt * (((((double)(advcv + advch)) - pg) + (double)cf) + (double)div
+                                                   + (double)lds(a.MOMY_t + c));
+                        put_state(a, N3, 3, a.MOMY_RK, a.MOMY0, c, val, true);
+                    }
                 }
             }
-            // v
-            {
-                const R q_k = do_v ? qZv(L) : R(0.0);
-                R q_km = __shfl_up_sync(FULL, q_k, 1);
-                if (lane == 0 && do_v) q_km = qZv(L - 1);
-                if (do_v) {
-                    const R fdy = R(ld(g.FDY + j - 1));
-                    const double rfdy = ld(g.RFDY + j - 1);
-                    const R cor_v = R(-0.125) * (R(ld(a.CORIOLI + g.c2 + (i - 1) + (size_t)g.IA * (j)))
-                                                 + R(ld(a.CORIOLI + g.c2 + (i - 1) + (size_t)g.IA * (j - 1))));
-                    const R Y_m2 = R(sMY[-2 * KY]), Y_m1 = R(sMY[-KY]), Y_00 = R(sMY[0]);
-                    const R Y_p1 = R(sMY[KY]), Y_p2 = R(sMY[2 * KY]);
-                    // x flux at (u,v,z), fluxX_XVZ (ud3.F90:1473-1527)
-                    const R vE = (h * (R(sMX[0]) + R(sMX[KY])))
-                                 / (qr * (R(sDN[0]) + R(sDN[KX]) + R(sDN[KY]) + R(sDN[KX + KY])));
-                    const R qXe = vE * ip6<S>(vE, W6 ? R(sMY[-2 * KX]) : R(0.0), R(sMY[-KX]), Y_00, R(sMY[KX]),
-                                              R(sMY[2 * KX]), W6 ? R(sMY[3 * KX]) : R(0.0)) + ld(nd.VX() + c);
-                    const R vW = (h * (R(sMX[-KX]) + R(sMX[KY - KX])))
-                                 / (qr * (R(sDN[-KX]) + R(sDN[0]) + R(sDN[KY - KX]) + R(sDN[KY])));
-                    const R qXw = vW * ip6<S>(vW, W6 ? R(sMY[-3 * KX]) : R(0.0), R(sMY[-2 * KX]), R(sMY[-KX]), Y_00,
-                                              R(sMY[KX]), W6 ? R(sMY[2 * KX]) : R(0.0)) + ld(nd.VX() + c - sI);
-                    // y flux with the index shift of fluxY_XVZ (ud3.F90:1531-1587)
-                    const R vN = (h * (Y_p1 + Y_00)) / (R(sDN[KY]));
-                    const R Y_m3 = W6 ? R(sMY[-3 * KY]) : R(0.0), Y_p3 = W6 ? R(sMY[3 * KY]) : R(0.0);
-                    const R qYn = vN * ip6<S>(vN, Y_m2, Y_m1, Y_00, Y_p1, Y_p2, Y_p3) + ld(nd.VY() + c + sJ);
-                    const R vS = (h * (Y_00 + Y_m1)) / (R(sDN[0]));
-                    const R qYs = vS * ip6<S>(vS, Y_m3, Y_m2, Y_m1, Y_00, Y_p1, Y_p2) + ld(nd.VY() + c);
-                    const R advcv = -(q_k - q_km) * R(rcdz_d);
-                    const R advch = -((qXe - qXw) * rcdx + (qYn - qYs) * R(rfdy));
-                    const double DPn = dp[(TX + 1) * NDP]; // DPRES at (i, j+1)
-                    const double pg = (DPn - dp[0]) * rfdy;
-                    const R cf = cor_v * (R(sMX[KY]) + R(sMX[0]) + R(sMX[KY - KX]) + R(sMX[-KX]));
-                    const R div = !use_div ? R(0.0) : ddc * (ld(a.DDIV + c + sJ) - ld(a.DDIV + c)) * fdy;
-                    const double val = lds(a.MOMY0 + c)
-                                       + dt * (((((double)(advcv + advch)) - pg) + (double)cf) + (double)div
-                                               + (double)lds(a.MOMY_t + c));
-                    put_state(a, N3, 3, a.MOMY_RK, a.MOMY0, c, val, true);
-                }
-            }
-        }
+        };
+        if (interior) chunk(std::false_type{});
+        else chunk(std::true_type{});
+#undef rcdz_L
+#undef rfdz_k
+#undef f1_L
+#undef f1_k
+#undef f2_L
+#undef f2_k
+#undef fdz_k
+#undef wd_k
         __syncthreads(); // every read of the staged box and of DPRES is done
         if (tid == 0 && ch + 1 < NC) issue(ch + 1);
     }
+
 }
 
 // =============================================================================
-// k_hevi_column
+// k_hevi_column: the column problem of CCOLS columns per CTA
 // =============================================================================
+// The CTA loads C, PT and A(k) of its columns into shared memory, and the
+// per-level factors B(k) and RFDZ(k) of the coefficients once for all of
+// them. Warp 0 runs the Thomas solve (solve_direct :1092-1127) one lane per
+// column: the coefficients of level k+1 are formed while the division of
+// level k runs, so that only e(k-1) and f(k-1) chain the levels. Then all warps
+// back-update rho, rho*w, rho*theta and the vertical fluxes (:728-790).
 constexpr int CCOLS = 16;  // columns per CTA (consecutive in i)
 constexpr int CWARPS = 8;
 __host__ __device__ inline int col_pitch_c(int KA) { return KA | 1; }
+__host__ __device__ inline size_t column_smem(int KA) { return ((size_t)3 * CCOLS * col_pitch_c(KA) + 2 * (size_t)KA) * sizeof(double); }
 
 template <typename R, int NM>
 __global__ void __launch_bounds__(32 * CWARPS, 4) k_hevi_column(const Grid gt, const StageArgsT<R> a, const BatchT<NM> B)
@@ -472,11 +548,13 @@ __global__ void __launch_bounds__(32 * CWARPS, 4) k_hevi_column(const Grid gt, c
     const double dt = a.dtrk, J33G = a.J33G, dt2 = dt * dt;
     const Nd<R> nd(a, N3);
     const R *sSr = a.colscr, *sSt = a.colscr + N3, *stZ = a.colscr + 2 * N3, *sPT = a.colscr + 3 * N3;
-    // per-level arrays of the tile's columns: [array][column][level], odd pitch
+    // per-level arrays of the tile's columns: [array][column][level], odd pitch;
+    // then B(k) and RFDZ(k) by level
     double *sC = csm, *sP = csm + (size_t)CCOLS * KP, *sA = csm + (size_t)2 * CCOLS * KP;
+    double *sB = csm + (size_t)3 * CCOLS * KP, *sR = sB + g.KA;
 #define CA(arr, cc, L) arr[(size_t)(cc) * KP + (L) - 1]
 
-    // ---- load C, PT and A(k) = dt^2 J33G^2 RCDZ RT2P (:696) ----
+    // ---- load C, PT and A(k) = dt^2 J33G^2 RCDZ RT2P (:696); B(k) (:697) and RFDZ(k) ----
     for (int cc = w; cc < CCOLS; cc += CWARPS) {
         const int i = i0 + cc;
         if (i > g.IE) break;
@@ -490,36 +568,50 @@ __global__ void __launch_bounds__(32 * CWARPS, 4) k_hevi_column(const Grid gt, c
             CA(sA, cc, L) = dt2 * J33G * ld(g.RCDZ + L - 1) * ld(a.RT2P + c) * J33G;
         }
     }
+    for (int k = KS + w * 32 + lane; k <= KE - 1; k += 32 * CWARPS) {
+        sB[k - 1] = GRAV * dt2 * J33G / (ld(g.CDZ + k) + ld(g.CDZ + k - 1));
+        sR[k - 1] = ld(g.RFDZ + k - 1);
+    }
     __syncthreads();
 
-    // ---- Thomas solve, one lane per column (solve_direct :1092-1127 with F1..F3 of :699-709) ----
+    // ---- Thomas solve, one lane per column (F1..F3 of :699-709) ----
     if (w == 0 && lane < CCOLS && i0 + lane <= g.IE) {
         const int cc = lane;
-        double e_prev = 0.0, f_prev = 0.0;
-        for (int k = KS; k <= KE - 1; ++k) {
-            const double rfdz = ld(g.RFDZ + k - 1);
-            const double Bk = GRAV * dt2 * J33G / (ld(g.CDZ + k) + ld(g.CDZ + k - 1));
+        // F1, F2, F3 and C of level k (F1 is not used at KE-1, F3 not at KS)
+        auto coef = [&](int k, double &F1, double &F2, double &F3, double &Ck) {
+            const double rfdz = sR[k - 1], Bk = sB[k - 1];
             const double Ak = CA(sA, cc, k), Ak1 = CA(sA, cc, k + 1);
-            const double F2 = 1.0 + (CA(sP, cc, k) * rfdz * (Ak1 + Ak));
-            const double Ck = CA(sC, cc, k);
-            if (k == KS) {
-                const double F1 = -(CA(sP, cc, k + 1) * rfdz * Ak1 + Bk);
-                const double rdenom = 1.0 / F2;
-                e_prev = -F1 * rdenom;
-                f_prev = Ck * rdenom;
-            } else if (k <= KE - 2) {
-                const double F1 = -(CA(sP, cc, k + 1) * rfdz * Ak1 + Bk);
-                const double F3 = -(CA(sP, cc, k - 1) * rfdz * Ak - Bk);
-                const double rdenom = 1.0 / (F2 + F3 * e_prev);
-                e_prev = -F1 * rdenom;
-                f_prev = (Ck - F3 * f_prev) * rdenom;
-            } else {
-                const double F3 = -(CA(sP, cc, k - 1) * rfdz * Ak - Bk);
-                f_prev = (Ck - F3 * f_prev) / (F2 + F3 * e_prev); // the solution at KE-1
-            }
-            CA(sA, cc, k) = e_prev;
-            CA(sC, cc, k) = f_prev;
+            F2 = 1.0 + (CA(sP, cc, k) * rfdz * (Ak1 + Ak));
+            F1 = k <= KE - 2 ? -(CA(sP, cc, k + 1) * rfdz * Ak1 + Bk) : 0.0;
+            F3 = k >= KS + 1 ? -(CA(sP, cc, k - 1) * rfdz * Ak - Bk) : 0.0;
+            Ck = CA(sC, cc, k);
+        };
+        double F1, F2, F3, Ck;
+        coef(KS, F1, F2, F3, Ck);
+        double e_prev, f_prev;
+        {
+            const double rdenom = 1.0 / F2;
+            e_prev = -F1 * rdenom;
+            f_prev = Ck * rdenom;
         }
+        double nF1, nF2, nF3, nC; // the next level's coefficients
+        coef(KS + 1, nF1, nF2, nF3, nC);
+        // levels KS+1..KE-2: one straight block per level, in which the next
+        // level's coefficients fill the latency of this level's division
+        for (int k = KS + 1; k <= KE - 2; ++k) {
+            F1 = nF1; F2 = nF2; F3 = nF3; Ck = nC;
+            CA(sA, cc, k - 1) = e_prev;
+            CA(sC, cc, k - 1) = f_prev;
+            coef(k + 1, nF1, nF2, nF3, nC); // reads A(k+1), A(k+2): not yet overwritten
+            const double rdenom = 1.0 / (F2 + F3 * e_prev);
+            e_prev = -F1 * rdenom;
+            f_prev = (Ck - F3 * f_prev) * rdenom;
+        }
+        CA(sA, cc, KE - 2) = e_prev;
+        CA(sC, cc, KE - 2) = f_prev;
+        f_prev = (nC - nF3 * f_prev) / (nF2 + nF3 * e_prev); // the solution at KE-1
+        CA(sA, cc, KE - 1) = e_prev;
+        CA(sC, cc, KE - 1) = f_prev;
         // back substitution, C(k) = e(k) C(k+1) + f(k)
         double Cnext = f_prev;
         for (int k = KE - 2; k >= KS; --k) {
@@ -573,9 +665,9 @@ __global__ void __launch_bounds__(32 * CWARPS, 4) k_hevi_column(const Grid gt, c
         // hevi_mflx_z :369-393 also fills the halo column i = IS-1 with the explicit
         // part of the vertical mass flux; the solver never updates it
         if (i == g.IS && (a.rk_mode == RK_PLAIN || a.rk_mode == RK_FINAL || a.rk_mode == RK_HEUN3)) {
-            const size_t ch = idx3(g, 1, g.IS - 1, j);
+            const size_t chl = idx3(g, 1, g.IS - 1, j);
             for (int k = KS - 1 + lane; k <= KE; k += 32)
-                a.mflx[ch + k - 1] = (k >= KS && k <= KE - 1) ? ld(nd.DZ() + ch + k - 1) : R(0.0);
+                a.mflx[chl + k - 1] = (k >= KS && k <= KE - 1) ? ld(nd.DZ() + chl + k - 1) : R(0.0);
         }
     }
 #undef CA
@@ -649,11 +741,10 @@ cudaError_t launch_s(const Grid &g, StageArgsT<R> a, int raster, cudaStream_t st
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
     auto kc = k_hevi_column<R, 1>;
     // the attribute is set once per device, so it opens the largest size (KA = 260)
-    const size_t csmem = (size_t)3 * CCOLS * col_pitch_c(g.KA) * sizeof(double);
-    if ((e = open_smem(kc, (size_t)3 * CCOLS * col_pitch_c(260) * sizeof(double))) != cudaSuccess) return e;
+    if ((e = open_smem(kc, column_smem(260))) != cudaSuccess) return e;
     const int ncb = ((g.IMAX + CCOLS - 1) / CCOLS) * g.JMAX;
     B.first[1] = ncb;
-    kc<<<ncb, dim3(32, CWARPS), csmem, st>>>(g, a, B);
+    kc<<<ncb, dim3(32, CWARPS), column_smem(g.KA), st>>>(g, a, B);
     return cudaGetLastError();
 }
 
@@ -667,6 +758,7 @@ template <typename R>
 cudaError_t launch_hevi_stage_tiled(const Grid &g, const Members &mem, const StageArgsT<R> &a, int scheme, int raster,
                                     cudaStream_t st)
 {
+    // even KA: 16-byte strides for the tensor maps
     if (mem.n > 1 || (g.KA & 1) || g.KA > 260 || !a.colC) return cudaErrorNotSupported;
     switch (scheme) {
     case UD3: return tma::launch_s<UD3, R>(g, a, raster, st);

@@ -11,12 +11,20 @@
 // image, so the CUDA runtime creates it when it loads the module, not this code.
 //
 // Usage notes:
-//   - The first call on each device looks up the array's device address with
-//     cudaGetSymbolAddress, with that device current. That lookup can make the
-//     runtime load the module, so make the first call before any stream capture.
+//   - Every call looks up the array's device address with cudaGetSymbolAddress,
+//     with the caller's device current (a recreated context gets its own copy
+//     of the array, so no address is kept between calls). The first lookup on a
+//     device can make the runtime load the module, so make the first call
+//     before any stream capture. The entry synchronises its stream before it
+//     returns, so it cannot itself be captured into a graph.
 //   - The scratch is shared by every call on a device, so calls that overlap in
 //     time (two host threads, or two streams in flight) race on it.
-//   - The entry synchronises its stream before it returns.
+//   - Flat terrain only. The first call with a given set of metric arrays
+//     (device, GSQRT, J13G, J23G, MAPF pointers) counts their non-flat values
+//     on the device; a set found flat is remembered in host memory and later
+//     calls with the same pointers skip the check. The cache assumes that the
+//     contents of those arrays do not change between calls.
+//   - The 4-point flux schemes (UD3, CD4, UD3KOREN1993, CD2) on a halo of 2.
 //   - The scratch holds a 256-byte header (status word, terrain-check counter),
 //     three per-level fields of the column solve (3*KA*IA*JA doubles) and the
 //     1-D grid tables (7*KA + 4*IA + 4*JA doubles); at most
@@ -36,11 +44,16 @@ using namespace hevi;
 
 constexpr size_t kScratchBytes = SCALE_HEVI_NOALLOC_SCRATCH_BYTES;
 constexpr size_t kHeader = 256; // status word (offset 0) and terrain-check counter (offset 8)
-constexpr int kMaxDevices = 64;
-
 __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
 
-unsigned char *g_scratch_ptr[kMaxDevices] = {};
+// metric sets (device, GSQRT, J13G, J23G, MAPF) already found flat; host memory
+struct FlatKey {
+    int dev;
+    const void *p[4];
+};
+constexpr int kFlatSets = 64;
+FlatKey g_flat[kFlatSets];
+int g_nflat = 0;
 
 int err(int code, const char *fmt, ...)
 {
@@ -61,16 +74,24 @@ int err(int code, const char *fmt, ...)
 
 int scratch_for_current_device(unsigned char **out)
 {
-    int dev = 0;
-    NA_CU(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= kMaxDevices) return err(SCALE_HEVI_ERR_ARG, "device %d beyond the %d the no-alloc entry tracks", dev, kMaxDevices);
-    if (!g_scratch_ptr[dev]) {
-        void *p = nullptr;
-        NA_CU(cudaGetSymbolAddress(&p, g_noalloc_scratch));
-        g_scratch_ptr[dev] = static_cast<unsigned char *>(p);
-    }
-    *out = g_scratch_ptr[dev];
+    void *p = nullptr;
+    NA_CU(cudaGetSymbolAddress(&p, g_noalloc_scratch));
+    *out = static_cast<unsigned char *>(p);
     return SCALE_HEVI_OK;
+}
+
+bool known_flat(int dev, const void *const p[4])
+{
+    for (int q = 0; q < g_nflat; ++q)
+        if (g_flat[q].dev == dev && !memcmp(g_flat[q].p, p, sizeof g_flat[q].p)) return true;
+    return false;
+}
+
+void remember_flat(int dev, const void *const p[4])
+{
+    FlatKey &k = g_flat[g_nflat < kFlatSets ? g_nflat++ : (g_nflat - 1)]; // a full cache replaces its last entry
+    k.dev = dev;
+    memcpy(k.p, p, sizeof k.p);
 }
 
 int parse_scheme(const char *s, int *out)
@@ -78,9 +99,12 @@ int parse_scheme(const char *s, int *out)
     if (!s) return err(SCALE_HEVI_ERR_ARG, "flux scheme name is NULL");
     size_t n = strlen(s);
     while (n > 0 && s[n - 1] == ' ') --n; // Fortran blank padding
-    if (n == 3 && strncmp(s, "UD3", 3) == 0) { *out = UD3; return SCALE_HEVI_OK; }
-    if (n == 3 && strncmp(s, "CD4", 3) == 0) { *out = CD4; return SCALE_HEVI_OK; }
-    return err(SCALE_HEVI_ERR_UNSUPPORTED, "flux scheme '%.*s' is not supported (UD3, CD4)", (int)n, s);
+    const struct { const char *name; int id; } known[] = {{"UD3", UD3}, {"CD4", CD4}, {"UD3KOREN1993", KOREN}, {"CD2", CD2}};
+    for (const auto &k : known)
+        if (n == strlen(k.name) && strncmp(s, k.name, n) == 0) { *out = k.id; return SCALE_HEVI_OK; }
+    return err(SCALE_HEVI_ERR_UNSUPPORTED,
+               "flux scheme '%.*s' is not supported by the no-alloc entry (UD3, CD4, UD3KOREN1993, CD2 on a halo of 2)",
+               (int)n, s);
 }
 
 // copy n doubles of a host vector into the device table (n may be 0)
@@ -138,21 +162,30 @@ extern "C" int ATMOS_DYN_Tstep_short_fvm_hevi_b200_noalloc(const scale_hevi_inde
     // flat terrain only (GSQRT = 1, J13G = J23G = 0, MAPF = 1): the general-metric
     // stage of the other entries keeps 24 work fields, which this entry does not have
     NA_CU(cudaMemsetAsync(scr, 0, kHeader, st)); // status and counter start at zero
-    const size_t n7 = 7 * N3, nm = (size_t)IA * JA * 2 * 4;
-    if (GSQRT) count_not_equal(GSQRT, n7, 1.0, count, st);
-    if (J13G) count_not_equal(J13G, n7, 0.0, count, st);
-    if (J23G) count_not_equal(J23G, n7, 0.0, count, st);
-    if (MAPF) count_not_equal(MAPF, nm, 1.0, count, st);
-    NA_CU(cudaGetLastError());
-    unsigned long long bad = 0;
-    NA_CU(cudaMemcpyAsync(&bad, count, sizeof bad, cudaMemcpyDeviceToHost, st));
-    NA_CU(cudaStreamSynchronize(st));
-    if (bad)
-        return err(SCALE_HEVI_ERR_UNSUPPORTED,
-                   "terrain-following metrics (%llu values of GSQRT/J13G/J23G/MAPF differ from flat terrain) are not supported", bad);
+    int dev = 0;
+    NA_CU(cudaGetDevice(&dev));
+    const void *metrics[4] = {GSQRT, J13G, J23G, MAPF};
+    if (!known_flat(dev, metrics)) {
+        const size_t n7 = 7 * N3, nm = (size_t)IA * JA * 2 * 4;
+        if (GSQRT) count_not_equal(GSQRT, n7, 1.0, count, st);
+        if (J13G) count_not_equal(J13G, n7, 0.0, count, st);
+        if (J23G) count_not_equal(J23G, n7, 0.0, count, st);
+        if (MAPF) count_not_equal(MAPF, nm, 1.0, count, st);
+        NA_CU(cudaGetLastError());
+        unsigned long long bad = 0;
+        NA_CU(cudaMemcpyAsync(&bad, count, sizeof bad, cudaMemcpyDeviceToHost, st));
+        NA_CU(cudaStreamSynchronize(st));
+        if (bad)
+            return err(SCALE_HEVI_ERR_UNSUPPORTED,
+                       "terrain-following metrics (%llu values of GSQRT/J13G/J23G/MAPF differ from flat terrain) are not supported",
+                       bad);
+        remember_flat(dev, metrics);
+    }
 
-    // 1-D tables: CDZ FDZ RCDZ RFDZ F2H1 F2H2 wdamp (KA each) | FDX RCDX RFDX (IA) | FDY RCDY RFDY (JA)
-    static double f2h[2 * 260];
+    // 1-D tables: CDZ FDZ RCDZ RFDZ F2H1 F2H2 wdamp (KA each) | FDX RCDX RFDX (IA) | FDY RCDY RFDY (JA);
+    // the face weights are built on this call's stack: a copy from pageable host
+    // memory has read its source by the time cudaMemcpyAsync returns
+    double f2h[2 * 260];
     build_f2h(KA, CDZ, f2h, f2h + KA);
     NA_CU(cudaMemsetAsync(tab, 0, ntab * sizeof(double), st)); // the unused last entries of FDZ/RFDZ/FDX/... stay 0
     double *z = tab, *xs = tab + 7 * (size_t)KA, *ys = xs + 4 * (size_t)IA;
