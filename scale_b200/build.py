@@ -9,7 +9,9 @@ shared object travels with the repository snapshot to the GPU machine:
 FP64 code is compiled with --fmad=false and the host code with
 -ffp-contract=off: the kernels keep the reference's evaluation order without
 fused multiply-adds so their results can be compared bit for bit with the
-oracle, which the reference's GNU build flags also do not contract.
+oracle, which the reference's GNU build flags also do not contract. The FP32
+instantiations of the mixed-precision path (FLOAT_SOURCES, -DHEVI_FLOAT_TU)
+compile with FMA contraction.
 """
 from __future__ import annotations
 
@@ -32,6 +34,10 @@ ORACLE_LIB = ORACLE_DIR / "build" / "liboracle.so"
 CU_SOURCES = ["capi.cu", "hevi_stage.cu", "hevi_tma.cu", "numfilter.cu", "tracer.cu", "misc.cu", "noalloc.cu",
               "adjoint.cu"]
 CPP_SOURCES = ["grid_coef.cpp"]
+# The FP32 instantiations of the mixed-precision path compile a second time from
+# these sources, with -DHEVI_FLOAT_TU and FMA contraction on: their results are
+# held to a tolerance against the FP64 path, not bit for bit, so a*b+c may fuse.
+FLOAT_SOURCES = ["hevi_stage.cu", "hevi_tma.cu", "numfilter.cu"]
 HEADERS = ["hevi_common.cuh", "hevi_stage.cuh", "hevi_kernels.cuh", "hevi_epilogue.cuh", "adjoint.cuh",
            "grid_coef.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -75,6 +81,11 @@ def build_cuda(force: bool = False, verbose: bool = False) -> Path:
         if src.endswith(".cpp"):
             cmd = [nvcc, *common, *ARCH, "-x", "c++", "-c", str(CSRC / src), "-o", str(obj)]
         cmds.append(cmd)
+        objs.append(str(obj))
+    f32 = [a for a in common if a != "--fmad=false"] + ["--fmad=true", "-DHEVI_FLOAT_TU"]
+    for src in FLOAT_SOURCES:
+        obj = objdir / (Path(src).stem + "_f32.o")
+        cmds.append([nvcc, *f32, *ARCH, "-c", str(CSRC / src), "-o", str(obj)] + (["-Xptxas", "-v"] if verbose else []))
         objs.append(str(obj))
     # the translation units compile independently; the kernel templates make
     # some of them long, so they run side by side

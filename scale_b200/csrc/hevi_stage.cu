@@ -492,6 +492,7 @@ __global__ void __launch_bounds__(32 * HEVI_COL_TC, HEVI_COL_MINB)
 #undef XS
 #undef XS_PUT
 }
+#ifndef HEVI_FLOAT_TU // the FP64-only kernels live in the FP64 translation unit
 // =============================================================================
 // the HEVE stage (ATMOS_DYN_Tstep_short_fvm_heve, scale_atmos_dyn_tstep_short_fvm_heve.F90:109-1518,
 // without the momentum/theta FCT branches): every tendency is explicit, so each
@@ -658,6 +659,7 @@ cudaError_t launch_heve_stage(const Grid &g, const Members &mem, const StageArgs
         }
     });
 }
+#endif // HEVI_FLOAT_TU
 
 #undef AT
 #undef AR
@@ -735,10 +737,12 @@ cudaError_t launch_hevi_stage(const Grid &g, const Members &mem, const StageArgs
     default: return cudaErrorInvalidValue;
     }
 }
-template cudaError_t launch_hevi_stage<double>(const Grid &, const Members &, const StageArgsT<double> &, int,
-                                               StageShape, cudaStream_t, int *, bool *);
+#ifdef HEVI_FLOAT_TU
 template cudaError_t launch_hevi_stage<float>(const Grid &, const Members &, const StageArgsT<float> &, int,
                                               StageShape, cudaStream_t, int *, bool *);
+#else
+template cudaError_t launch_hevi_stage<double>(const Grid &, const Members &, const StageArgsT<double> &, int,
+                                               StageShape, cudaStream_t, int *, bool *);
 
 // =============================================================================
 // The HEVI stage with terrain-following metrics (GSQRT, J13G, J23G) and map
@@ -1735,5 +1739,7 @@ cudaError_t launch_terrain_heve_stage(const Grid &g, const StageArgsT<double> &a
     }
     return cudaGetLastError();
 }
+
+#endif // HEVI_FLOAT_TU
 
 }  // namespace hevi

@@ -676,7 +676,7 @@ __global__ void __launch_bounds__(32 * CWARPS, 4) k_hevi_column(const Grid gt, c
 // =============================================================================
 // host side
 // =============================================================================
-PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
+static PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
 {
     static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
     static bool tried = false;
@@ -692,7 +692,7 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
 }
 
 // FP64 (KA, IA, JA) tensor with a box of bk x bw x bh elements
-bool encode(CUtensorMap *m, const double *base, const Grid &g, int bk, int bw, int bh)
+static bool encode(CUtensorMap *m, const double *base, const Grid &g, int bk, int bw, int bh)
 {
     auto fn = encode_fn();
     if (!fn || ((uintptr_t)base & 15u)) return false;
@@ -770,9 +770,13 @@ cudaError_t launch_hevi_stage_tiled(const Grid &g, const Members &mem, const Sta
     default: return cudaErrorInvalidValue;
     }
 }
+#ifndef HEVI_FLOAT_TU
 template cudaError_t launch_hevi_stage_tiled<double>(const Grid &, const Members &, const StageArgsT<double> &, int,
                                                      int, cudaStream_t);
+#else
 template cudaError_t launch_hevi_stage_tiled<float>(const Grid &, const Members &, const StageArgsT<float> &, int, int,
                                                     cudaStream_t);
+
+#endif
 
 }  // namespace hevi

@@ -256,6 +256,7 @@ __global__ void __launch_bounds__(128, HEVI_ND_MINB)
 #undef DX
 #undef DY
 
+#ifndef HEVI_FLOAT_TU // the ND_ORDER > 1 path is FP64 only
 // ---- ND_ORDER > 1: calc_numdiff (scale_atmos_dyn_common.F90:1518-1573) -----------
 // calc_diff3 of the five quantities (q: 0 density, 1 VELZ, 2 VELX, 3 VELY, 4
 // theta) into the work buffer, at every level of the interior columns; the
@@ -342,6 +343,7 @@ cudaError_t launch_numfilter_high(const Grid &g, const NdCoef &c, const NdArgs &
     k_numfilter<double, 1, true><<<oneN.first[1], b, 0, st>>>(g, c, a, oneN, in);
     return cudaGetLastError();
 }
+#endif
 
 template <typename R>
 cudaError_t launch_numfilter(const Grid &g, const Members &mem, const NdCoef &c, const NdArgsT<R> &a, cudaStream_t st)
@@ -358,9 +360,12 @@ cudaError_t launch_numfilter(const Grid &g, const Members &mem, const NdCoef &c,
     });
     return cudaGetLastError();
 }
-template cudaError_t launch_numfilter<double>(const Grid &, const Members &, const NdCoef &, const NdArgsT<double> &,
-                                              cudaStream_t);
+#ifdef HEVI_FLOAT_TU
 template cudaError_t launch_numfilter<float>(const Grid &, const Members &, const NdCoef &, const NdArgsT<float> &,
                                              cudaStream_t);
+#else
+template cudaError_t launch_numfilter<double>(const Grid &, const Members &, const NdCoef &, const NdArgsT<double> &,
+                                              cudaStream_t);
+#endif
 
 }  // namespace hevi
