@@ -36,7 +36,7 @@ METRIC = "HEVI short-step cell-updates/s on 1 B200, FP64 vs mixed at stated erro
 UNIT = "cell-updates/s"
 L2_BYTES = 126 * 1024 * 1024
 HEVE_DT = 0.04  # s; below the vertical acoustic limit dz / c_s of the 50 m lowest layer
-# algorithmic bytes per interior cell (see DESIGN.md): one HEVI stage reads 34
+# algorithmic bytes per interior cell: one HEVI stage reads 34
 # fields (DENS0..RHOT0, DENS..RHOT, *_t, DPRES0, RT2P, REF_dens, REF_rhot and the
 # 15 num_diff components; DDIV is not read because divdmp_coef = 0) and writes 11
 # (DENS_RK..RHOT_RK, mflx_hi(3), tflx_hi(3)); the filter reads 7 and writes 15.
@@ -47,6 +47,10 @@ STEP_BYTES = 4 * STAGE_BYTES + NUMFILTER_BYTES
 # fields (num_diff 15, tendencies 5, mflx_hi 3, tflx_hi 3) are FP32
 MIXED_STAGE_BYTES = (5 + 5 + 4) * 8 + 5 * 8 + (15 + 5 + 3 + 3) * 4
 MIXED_NUMFILTER_BYTES = 7 * 8 + 15 * 4
+# tracer advection, per tracer and large step: 3 RK stages, each reading QTRC,
+# QTRC0, RHOQ_t, DENS0, DENS, mflx_hi (3) and the tracer num_diff (3) and
+# writing QTRCo
+TRACER_BYTES = 3 * 12 * 8
 
 
 def rank_info():
@@ -223,6 +227,7 @@ def run_b200(args):
             step()
         hevi.check()
         m0 = hevi.domain_sum_dev(X["DENS"], g.CDZ, g.CDX, g.CDY)
+        e0 = hevi.energy_sum_dev(**X, CZ=g.CZ, CDZ=g.CDZ, CDX=g.CDX, CDY=g.CDY)
 
         # ---- timed region ----
         if dist:
@@ -243,6 +248,7 @@ def run_b200(args):
     elapsed_ms = max_over_ranks(t0.elapsed_time(t1), dist, "cuda")
     hevi.check()
     m1 = hevi.domain_sum_dev(X["DENS"], g.CDZ, g.CDX, g.CDY)
+    e1 = hevi.energy_sum_dev(**X, CZ=g.CZ, CDZ=g.CDZ, CDX=g.CDX, CDY=g.CDY)
     clocks = clk.summary()
     ms_step = elapsed_ms / args.steps
     value = aggregate_rate(cells, world, args.steps, elapsed_ms)
@@ -276,6 +282,9 @@ def run_b200(args):
         "roofline": roofline,
         "sections_ms_per_step": {k: v[1] / args.steps for k, v in prof.items()},
         "mass_drift_rel": abs(m1 - m0) / m0,
+        "energy_budget": {"unit": "J", "before": e0, "after": e1,
+                          "ENGT_change_rel": (e1["ENGT"] - e0["ENGT"]) / e0["ENGT"],
+                          "sum": "FP64, on the device, fixed order (scale_hevi_energy_sum_dev)"},
         "gpu_launches": launches,
         "clocks": clocks,
         "autotune": hevi.autotune_report(),
@@ -319,6 +328,7 @@ def run_b200(args):
         hevi.profile(False)
         hevi.check()
         m1x = hevi.domain_sum_dev(X["DENS"], g.CDZ, g.CDX, g.CDY)
+        e_mixed = hevi.energy_sum_dev(**X, CZ=g.CZ, CDZ=g.CDZ, CDX=g.CDX, CDY=g.CDY)
         ms_mixed = max_over_ranks(t0.elapsed_time(t1), dist, "cuda") / args.steps
         nsm, tsm = profm.get("hevi_stage_mixed", (0, 0.0))
         sm_ms = tsm / max(nsm, 1)
@@ -340,6 +350,7 @@ def run_b200(args):
                          "base-state deviations, right-hand side and tridiagonal solve",
             "error_vs_fp64": {"steps": args.warmup + args.steps, "fields": errs},
             "mass_drift_rel": abs(m1x - m0x) / m0x,
+            "energy_ENGT_vs_fp64_rel": (e_mixed["ENGT"] - e1["ENGT"]) / e1["ENGT"],
             "roofline": {"bound": "hbm", "kernel": "k_hevi_stage<float> (one HEVI stage)", "achieved": ach,
                          "peak": hbm, "unit": "GB/s", "frac": (ach / hbm) if ach else None,
                          "algorithmic_bytes_per_launch": MIXED_STAGE_BYTES * cells, "stage_ms": sm_ms,
@@ -348,6 +359,8 @@ def run_b200(args):
         }
         del st_fp64
 
+    if not args.no_tracer:
+        out["tracer"] = run_tracer(args, c, hevi, torch, X, mflx, g, cells, stream, t0, t1, dist, world, hbm)
     if not args.no_heve:
         out["heve"] = run_heve(args, hevi, torch, step, st, st0, X, g, cells, stream, t0, t1, dist, world, hbm)
     if not args.no_terrain:
@@ -389,6 +402,7 @@ def run_heve(args, hevi, torch, step, st, st0, X, g, cells, stream, t0, t1, dist
             step(HEVE_DT)
         hevi.check()
         m0 = hevi.domain_sum_dev(X["DENS"], g.CDZ, g.CDX, g.CDY)
+        e0 = hevi.energy_sum_dev(**X, CZ=g.CZ, CDZ=g.CDZ, CDX=g.CDX, CDY=g.CDY)
         if dist:
             dist.barrier()
         torch.cuda.synchronize()
@@ -477,12 +491,75 @@ def run_terrain(args, hevi, torch, step, st, st0, g, cells, stream, t0, t1, dist
     }
 
 
+def run_tracer(args, c, hevi, torch, X, mflx, g, cells, stream, t0, t1, dist, world, hbm):
+    """Tracer advection of the workload's three moist tracers (QV at 80 % RH,
+    QC = QR = 0) over one large step each: ATMOS_DYN_Tinteg_tracer_rk3_b200_dev
+    (RK3WS2002, UD3 fluxes, FCT along-stream in the last stage), FP64, with the
+    mass fluxes of the last short step and a tracer num_diff array, timed on
+    the library stream. Algorithmic bytes: 11 fields read and 1 written per
+    cell and RK stage, 3 stages: 288 B per cell per tracer and large step."""
+    N3 = int(np.prod(g.shape))
+    q0 = torch.from_numpy(np.ravel(c.state["QTRC"], order="K").copy()).cuda()  # (KA,IA,JA,3)
+    qt = q0.clone()
+    q_start = [q0[n * N3:(n + 1) * N3].clone() for n in range(c.QA)]
+    zero = torch.zeros(N3, dtype=torch.float64, device="cuda")
+    ndq = torch.zeros(3 * N3, dtype=torch.float64, device="cuda")
+    dens0 = X["DENS"].clone()
+    kw = dict(RHOQ_t=zero, DENS0=dens0, DENS=X["DENS"], mflx_hi=mflx, num_diff=ndq, GSQRT=None, MAPF=None,
+              CDZ=g.CDZ, RCDZ=g.RCDZ, RCDX=g.RCDX, RCDY=g.RCDY, BND_W=False, BND_E=False, BND_S=False, BND_N=False,
+              dtl=c.dtl, FLAG_FCT_TRACER=True, FLAG_FCT_ALONG_STREAM=True)
+
+    def large_step():
+        for n in range(c.QA):
+            qn = qt[n * N3:(n + 1) * N3]
+            hevi.ATMOS_DYN_Tinteg_tracer_rk3_dev(QTRC=qn, QTRC0=qn, **kw)
+
+    k = max(1, args.tracer_steps)
+    for _ in range(max(3, args.warmup)):
+        large_step()
+    hevi.check()
+    qt.copy_(q0)
+    torch.cuda.synchronize()
+    hevi.profile(True)
+    l0 = hevi.kernel_launches()
+    t0.record(stream)
+    for _ in range(k):
+        large_step()
+    t1.record(stream)
+    torch.cuda.synchronize()
+    prof = hevi.profile_report()
+    hevi.profile(False)
+    hevi.check()
+    launches = hevi.kernel_launches() - l0
+    ms = max_over_ranks(t0.elapsed_time(t1), dist, "cuda") / k
+    ms_tracer = ms / c.QA
+    ach = TRACER_BYTES * cells / (ms_tracer * 1e-3) / 1e9
+    qmin = min(float(qt[n * N3:(n + 1) * N3].min()) for n in range(c.QA))
+    # tracer mass (rho*q) after the steps against the start, FP64 device sums
+    rq = [hevi.domain_sum_dev(X["DENS"] * qt[n * N3:(n + 1) * N3], g.CDZ, g.CDX, g.CDY) for n in range(c.QA)]
+    rq0 = [hevi.domain_sum_dev(dens0 * q_start[n], g.CDZ, g.CDX, g.CDY) for n in range(c.QA)]
+    return {
+        "value": aggregate_rate(cells, world, 1, ms_tracer), "unit": "cell-updates/s per tracer",
+        "ms_per_tracer_large_step": ms_tracer, "ms_per_large_step": ms, "tracers": c.QA, "large_steps": k,
+        "step": "ATMOS_DYN_Tinteg_tracer_rk3 (3 RK stages, UD3 fluxes, FCT along-stream), dtl = 2.5 s, FP64",
+        "roofline": {"bound": "hbm", "kernel": "tracer RK3 with FCT (k_tracer_plain x2, k_fct_lo, k_fct_r, "
+                     "k_fct_apply, halos)", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
+                     "algorithmic_bytes_per_cell": TRACER_BYTES},
+        "kernel_launches_per_tracer_step": launches / (k * c.QA),
+        "min_tracer_after": qmin, "tracer_mass_change_rel": [(a - b) / b if b else 0.0 for a, b in zip(rq, rq0)],
+        "sections_ms_per_large_step": {kk: v[1] / k for kk, v in prof.items()},
+    }
+
+
 def run_mixed_large(args, hevi, torch):
     """The multi-bubble configuration at its full 1024x1024x96 size: the same
     short steps (numfilter + RK4 + boundary/halo) from the same initial state
-    in FP64 and in mixed precision, timed on the library stream; errors of the
-    mixed state against the FP64 state after the same steps, relative to each
-    field's largest magnitude over the interior."""
+    in FP64 and in mixed precision, timed on the library stream over
+    args.mixed_large_steps steps after the warm-up; both paths then run on,
+    untimed, to args.mixed_error_steps steps in all, after which the errors of
+    the mixed state against the FP64 state are taken, relative to each field's
+    largest magnitude over the interior, with the FP64 mass and energy totals
+    of both states."""
     from scale_b200 import mkinit
 
     w0 = time.time()
@@ -511,6 +588,7 @@ def run_mixed_large(args, hevi, torch):
         stream = torch.cuda.ExternalStream(hevi.stream_handle())
         t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         k, warm = args.mixed_large_steps, max(3, args.warmup)
+        total = max(warm + k, args.mixed_error_steps)
 
         def run(mixed):
             ft = torch.float32 if mixed else torch.float64
@@ -546,11 +624,21 @@ def run_mixed_large(args, hevi, torch):
             prof = hevi.profile_report()
             hevi.profile(False)
             hevi.check()
+            ms = t0.elapsed_time(t1) / k
+            for _ in range(total - warm - k):  # on to the step of the error comparison, untimed
+                step()
+            hevi.check()
+            torch.cuda.synchronize()
+            mass = hevi.domain_sum_dev(X["DENS"], g.CDZ, g.CDX, g.CDY)
+            eng = hevi.energy_sum_dev(**X, CZ=g.CZ, CDZ=g.CDZ, CDX=g.CDX, CDY=g.CDY)
             del mflx, tflx, nd, tend
-            return st, t0.elapsed_time(t1) / k, prof
+            return st, ms, prof, mass, eng
 
-        st64, ms64, prof64 = run(False)
-        st32, ms32, prof32 = run(True)
+        X0 = dict(DENS=st0[0], MOMZ=st0[1], MOMX=st0[2], MOMY=st0[3], RHOT=st0[4])
+        mass0 = hevi.domain_sum_dev(X0["DENS"], g.CDZ, g.CDX, g.CDY)
+        eng0 = hevi.energy_sum_dev(**X0, CZ=g.CZ, CDZ=g.CDZ, CDX=g.CDX, CDY=g.CDY)
+        st64, ms64, prof64, mass64, eng64 = run(False)
+        st32, ms32, prof32, mass32, eng32 = run(True)
         sl = (slice(g.KS - 1, g.KE), slice(g.IS - 1, g.IE), slice(g.JS - 1, g.JE))
         errs = {}
         for v, n in enumerate(("DENS", "MOMZ", "MOMX", "MOMY", "RHOT")):
@@ -574,7 +662,13 @@ def run_mixed_large(args, hevi, torch):
                       "step_frac_of_measured_hbm": (4 * MIXED_STAGE_BYTES + MIXED_NUMFILTER_BYTES) * cells
                       / (ms32 * 1e-3) / 1e9 / hbm},
             "speedup_mixed_vs_fp64": ms64 / ms32,
-            "error_vs_fp64": {"steps": warm + k, "fields": errs},
+            "error_vs_fp64": {"steps": total, "fields": errs,
+                              "max_over_fields": max(e["max"] for e in errs.values()), "target": 1e-5},
+            "budgets_after_error_steps": {
+                "mass_drift_rel": {"fp64": (mass64 - mass0) / mass0, "mixed": (mass32 - mass0) / mass0},
+                "ENGT_change_rel": {"fp64": (eng64["ENGT"] - eng0["ENGT"]) / eng0["ENGT"],
+                                    "mixed": (eng32["ENGT"] - eng0["ENGT"]) / eng0["ENGT"]},
+                "ENGT_mixed_vs_fp64_rel": (eng32["ENGT"] - eng64["ENGT"]) / eng64["ENGT"]},
             "autotune": hevi.autotune_report(),
         }
     finally:
@@ -837,6 +931,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-precision measurement")
     ap.add_argument("--no-heve", action="store_true", help="skip the HEVE short-step measurement")
+    ap.add_argument("--no-tracer", action="store_true", help="skip the tracer advection measurement")
+    ap.add_argument("--tracer-steps", type=int, default=10, help="timed large steps of the tracer leg")
     ap.add_argument("--no-terrain", action="store_true", help="skip the terrain-following short-step measurement")
     ap.add_argument("--no-ensemble", action="store_true", help="skip the 48-member ensemble measurement")
     ap.add_argument("--ensemble-steps", type=int, default=20)
@@ -844,6 +940,7 @@ def main():
     ap.add_argument("--no-adjoint", action="store_true", help="skip the adjoint gradient measurement")
     ap.add_argument("--no-mixed-large", action="store_true", help="skip FP64 vs mixed on 1024x1024x96")
     ap.add_argument("--mixed-large-steps", type=int, default=20)
+    ap.add_argument("--mixed-error-steps", type=int, default=600, help="steps before the mixed-vs-FP64 error is taken")
     ap.add_argument("--mixed-scale", type=float, default=1.0, help="horizontal scale of the 1024x1024x96 leg")
     ap.add_argument("--adjoint-steps", type=int, default=120)
     args = ap.parse_args()

@@ -4,8 +4,8 @@
  *
  * Every entry point replaces one procedure of the reference dynamical core
  * (hisashiyashiro/scale, SCALE 5.3.6) and keeps its argument list and order so
- * that scale-rm's Fortran driver can bind it with ISO_C_BINDING (see
- * INTEGRATION.md). Conventions follow what gfortran passes for those dummies:
+ * that scale-rm's Fortran driver can bind it with ISO_C_BINDING.
+ * Conventions follow what gfortran passes for those dummies:
  *   - arrays are double* in Fortran column-major order with k fastest:
  *     a (KA,IA,JA) field is element (k,i,j) at (k-1) + KA*((i-1) + IA*(j-1));
  *   - intent(in) scalars are passed by reference (const double*, const int*);
@@ -499,6 +499,22 @@ int scale_hevi_replay(const int *n);
  * pointer, CDZ/CDX/CDY host arrays, total a host pointer. Synchronises.
  * ------------------------------------------------------------------------- */
 int scale_hevi_domain_sum_dev(const double *var, const double *CDZ, const double *CDX, const double *CDY, double *total);
+
+/* ---------------------------------------------------------------------------
+ * FP64 energy budget of dry air: totals[0..3] = the domain totals of ENGT,
+ * ENGP, ENGK and ENGI [J], the energies that scale-rm's monitor reports
+ * (scale-rm/src/atmos/mod_atmos_vars.F90:768-778 registration, :2097-2171 the
+ * per-cell values): ENGP = DENS*GRAV*CZ, ENGK = 0.5*DENS*(W^2+U^2+V^2) with the
+ * cell-centre velocities of ATMOS_DIAGNOSTIC_CARTESC_get_vel (flat terrain),
+ * ENGI = DENS*TEMP*CVdry with TEMP from rho*theta
+ * (ATMOS_THERMODYN_rhot2temp_pres), ENGT = ENGP+ENGK+ENGI, each cell weighted
+ * by CDZ*CDX*CDY and summed on the device in a fixed order. The state arrays
+ * are device pointers, CZ/CDZ/CDX/CDY host arrays (KA, KA, IA, JA), totals a
+ * host array of 4. One domain. Synchronises.
+ * ------------------------------------------------------------------------- */
+int scale_hevi_energy_sum_dev(const double *DENS, const double *MOMZ, const double *MOMX, const double *MOMY,
+                              const double *RHOT, const double *CZ, const double *CDZ, const double *CDX,
+                              const double *CDY, double *totals);
 
 /* ---------------------------------------------------------------------------
  * One HEVI stage that allocates no device memory. This entry has no

@@ -53,7 +53,8 @@ def _signatures() -> dict[str, str]:
 
 
 _RESTYPE = {"og_halo_periodic": None, "og_divergence": None, "og_hevi_max_residual": C.c_double,
-            "og_domain_sum": C.c_double, "og_short_type": None, "og_tinteg_short_type": None}
+            "og_domain_sum": C.c_double, "og_short_type": None, "og_tinteg_short_type": None,
+            "og_energy_sum": None}
 
 
 def load() -> C.CDLL:
@@ -229,3 +230,12 @@ def max_residual(g, scheme, st, DPRES0, RT2P, num_diff, ref, REF_rhot, dtrk):
 
 def domain_sum(g, var):
     return load().og_domain_sum(C.byref(dims(g)), _p(var), _p(g.CDZ), _p(g.CDX), _p(g.CDY))
+
+
+def energy_sum(g, st, CZ):
+    """Dry-air energy totals ENGT, ENGP, ENGK, ENGI [J] of a state dict."""
+    out = np.zeros(4)
+    load().og_energy_sum(C.byref(dims(g)), _p(st["DENS"]), _p(st["MOMZ"]), _p(st["MOMX"]), _p(st["MOMY"]),
+                         _p(st["RHOT"]), _p(np.ascontiguousarray(CZ, dtype=np.float64)), _p(g.CDZ), _p(g.CDX),
+                         _p(g.CDY), _p(out))
+    return dict(zip(("ENGT", "ENGP", "ENGK", "ENGI"), (float(v) for v in out)))

@@ -299,3 +299,45 @@ double og_domain_sum(const og_dims *d, const double *var, const double *CDZ, con
             for (int k = KS; k <= KE; ++k) total += var[I3(k, i, j)] * CDZ[k - 1] * CDX[i - 1] * CDY[j - 1];
     return total;
 }
+
+/* Dry-air energy totals [J]: totals[0..3] = ENGT, ENGP, ENGK, ENGI over the
+ * interior, each cell weighted by CDZ*CDX*CDY; per-cell values as
+ * scale-rm/src/atmos/mod_atmos_vars.F90:2097-2171 (ENGP = DENS*GRAV*CZ,
+ * ENGK = 0.5*DENS*(W**2+U**2+V**2), ENGI = DENS*QDRY*TEMP*CVdry with QDRY = 1,
+ * ENGT = ENGP+ENGK+ENGI), the cell-centre velocities of
+ * ATMOS_DIAGNOSTIC_CARTESC_get_vel on flat terrain
+ * (scalelib/src/atmosphere/common/scale_atmos_diagnostic_cartesC.F90:88-135:
+ * W(KS) = momws*0.5 with momws = MOMZ(KS), W(KE) = 0.5*MOMZ(KE-1)/DENS) and the
+ * temperature of ATMOS_THERMODYN_rhot2temp_pres (scale_atmos_thermodyn.F90:791-792). */
+void og_energy_sum(const og_dims *d, const double *DENS, const double *MOMZ, const double *MOMX, const double *MOMY,
+                   const double *RHOT, const double *CZ, const double *CDZ, const double *CDX, const double *CDY,
+                   double *totals)
+{
+    OG_DIMS(d);
+    const double CVdry = OG_CPDRY - OG_RDRY;
+    double tot[4] = {0.0, 0.0, 0.0, 0.0};
+    for (int j = JS; j <= JE; ++j)
+        for (int i = IS; i <= IE; ++i) {
+            double col[4] = {0.0, 0.0, 0.0, 0.0};
+            for (int k = KS; k <= KE; ++k) {
+                const double dn = DENS[I3(k, i, j)];
+                double w;
+                if (k == KS) w = MOMZ[I3(KS, i, j)] * 0.5;
+                else if (k == KE) w = 0.5 * (MOMZ[I3(KE - 1, i, j)]) / dn;
+                else w = 0.5 * (MOMZ[I3(k - 1, i, j)] + MOMZ[I3(k, i, j)]) / dn;
+                const double u = 0.5 * (MOMX[I3(k, i - 1, j)] + MOMX[I3(k, i, j)]) / dn;
+                const double v = 0.5 * (MOMY[I3(k, i, j - 1)] + MOMY[I3(k, i, j)]) / dn;
+                const double pres = OG_PRE00 * pow(RHOT[I3(k, i, j)] * OG_RDRY / OG_PRE00, OG_CPDRY / CVdry);
+                const double temp = pres / (dn * OG_RDRY);
+                const double engp = dn * OG_GRAV * CZ[k - 1];
+                const double engk = 0.5 * dn * (w * w + u * u + v * v);
+                const double engi = dn * 1.0 * temp * CVdry;
+                const double engt = engp + engk + engi;
+                const double e[4] = {engt, engp, engk, engi};
+                for (int q = 0; q < 4; ++q) col[q] += e[q] * CDZ[k - 1] * CDX[i - 1] * CDY[j - 1];
+            }
+            for (int q = 0; q < 4; ++q) tot[q] += col[q];
+        }
+    for (int q = 0; q < 4; ++q) totals[q] = tot[q];
+}
+

@@ -210,6 +210,10 @@ double og_hevi_max_residual(
 
 /* ---- FP64 domain budget: sum over the interior of field*CDZ*CDX*CDY (check_mass, scale_atmos_dyn.F90:530-688) ---- */
 double og_domain_sum(const og_dims *d, const double *var, const double *CDZ, const double *CDX, const double *CDY);
+/* ---- FP64 energy budget of dry air: totals ENGT, ENGP, ENGK, ENGI (mod_atmos_vars.F90:2097-2171) ---- */
+void og_energy_sum(const og_dims *d, const double *DENS, const double *MOMZ, const double *MOMX, const double *MOMY,
+                   const double *RHOT, const double *CZ, const double *CDZ, const double *CDX, const double *CDY,
+                   double *totals);
 
 int og_num_threads(void);
 

@@ -70,6 +70,7 @@ struct Ctx {
     double *tr = nullptr;           // tracer: RK1, RK2, phi_lo, anti(3), rjp, rjm = 8*N3
     double *lg = nullptr;           // large step: DENS00, RT2P, DPRES0, REF_rhot, mflx_av(3), DDIV = 8*N3
     double *sum_part = nullptr, *sum_out = nullptr;
+    double *eng_part = nullptr;     // energy budget: 4*IMAX*JMAX column sums + 4 totals (on first use)
     // terrain-following metrics of the current call (the general-metric stage runs when set)
     bool terrain = false;
     Metrics tm{};
@@ -191,7 +192,7 @@ int falloc(float **p, size_t n)
 
 void free_all()
 {
-    double *bufs[] = {C.phi, C.ndw, C.colscr, C.colC, C.d_tab, C.d_nd, C.rk[0], C.rk[1], C.acc, C.facc, C.tr, C.lg, C.sum_part, C.sum_out,
+    double *bufs[] = {C.eng_part, C.phi, C.ndw, C.colscr, C.colC, C.d_tab, C.d_nd, C.rk[0], C.rk[1], C.acc, C.facc, C.tr, C.lg, C.sum_part, C.sum_out,
                       C.tw_buf};
     for (double *b : bufs) if (b) cudaFree(b);
     for (auto &kv : C.stage) cudaFree(kv.second.first);
@@ -1868,6 +1869,33 @@ const char *scale_hevi_profile_report(void)
     }
     C.prof_text += "}";
     return C.prof_text.c_str();
+}
+
+int scale_hevi_energy_sum_dev(const double *DENS, const double *MOMZ, const double *MOMX, const double *MOMY,
+                              const double *RHOT, const double *CZ, const double *CDZ, const double *CDX,
+                              const double *CDY, double *totals)
+{
+    CK(need_single("the energy budget"));
+    if (!DENS || !MOMZ || !MOMX || !MOMY || !RHOT || !CZ || !CDZ || !CDX || !CDY || !totals)
+        return fail(SCALE_HEVI_ERR_ARG, "scale_hevi_energy_sum_dev: a NULL argument");
+    const int KA = C.g.KA, IA = C.g.IA, JA = C.g.JA;
+    const size_t ncol = (size_t)C.g.IMAX * C.g.JMAX;
+    if (!C.eng_part) CK(dalloc(&C.eng_part, 4 * ncol + 4));
+    std::vector<double> h(2 * (size_t)KA + IA + JA);
+    std::memcpy(h.data(), CDZ, KA * sizeof(double));
+    std::memcpy(h.data() + KA, CDX, IA * sizeof(double));
+    std::memcpy(h.data() + KA + IA, CDY, JA * sizeof(double));
+    std::memcpy(h.data() + KA + IA + JA, CZ, KA * sizeof(double));
+    double *d;
+    CK(stage_buf("energy_grid", h.size(), &d));
+    CU(cudaMemcpyAsync(d, h.data(), h.size() * sizeof(double), cudaMemcpyHostToDevice, C.stream));
+    energy_sum(C.g, DENS, MOMZ, MOMX, MOMY, RHOT, d + KA + IA + JA, d + KA, d + KA + IA, d, C.eng_part,
+               C.eng_part + 4 * ncol, C.stream);
+    C.launches += 5;
+    CU(cudaGetLastError());
+    CU(cudaMemcpyAsync(totals, C.eng_part + 4 * ncol, 4 * sizeof(double), cudaMemcpyDeviceToHost, C.stream));
+    CU(cudaStreamSynchronize(C.stream));
+    return SCALE_HEVI_OK;
 }
 
 int scale_hevi_domain_sum_dev(const double *var, const double *CDZ, const double *CDX, const double *CDY, double *total)

@@ -167,6 +167,10 @@ void large_prep(const Grid &g, const PrepArgs &a, cudaStream_t st);
 void count_not_equal(const double *p, size_t n, double want, unsigned long long *count, cudaStream_t st);
 void domain_sum(const Grid &g, const double *var, const double *CDX, const double *CDY, const double *CDZ,
                 double *part, double *out, cudaStream_t st);
+// FP64 totals of ENGT, ENGP, ENGK, ENGI (dry air) into out[0..3]; part: 4*IMAX*JMAX
+void energy_sum(const Grid &g, const double *DENS, const double *MOMZ, const double *MOMX, const double *MOMY,
+                const double *RHOT, const double *CZ, const double *CDX, const double *CDY, const double *CDZ,
+                double *part, double *out, cudaStream_t st);
 void mflx_accumulate(const Grid &g, double *av, const double *mflx, cudaStream_t st);
 void mflx_average(const Grid &g, double *mflx, const double *av, int nstep, cudaStream_t st);
 

@@ -272,6 +272,63 @@ void domain_sum(const Grid &g, const double *var, const double *CDX, const doubl
     k_tree_sum<<<1, 1024, 0, st>>>(part, (size_t)g.IMAX * g.JMAX, out);
 }
 
+// ---- FP64 energy budget of dry air: the totals of ENGP, ENGK, ENGI and ENGT,
+// scale-rm/src/atmos/mod_atmos_vars.F90:2097-2171, over the interior, each
+// cell weighted by CDZ*CDX*CDY and summed in the order of k_col_sum.
+// Cell-centre velocities as ATMOS_DIAGNOSTIC_CARTESC_get_vel
+// (scalelib/src/atmosphere/common/scale_atmos_diagnostic_cartesC.F90:88-135) on
+// flat terrain: W(KS) = MOMZ(KS)*0.5 (its flat-terrain value as written there),
+// W(KE) = 0.5*MOMZ(KE-1)/DENS, U and V averaged from the faces.
+// Temperature as ATMOS_THERMODYN_rhot2temp_pres (scale_atmos_thermodyn.F90:791-792)
+// with Rtot = Rdry, CPtot/CVtot = CPdry/CVdry; QDRY = 1.
+__global__ void k_energy_col(const Grid g, const double *DN, const double *MZ, const double *MX, const double *MY,
+                             const double *RT, const double *CZ, const double *CDX, const double *CDY,
+                             const double *CDZ, double *part)
+{
+    constexpr double Rdry = 287.04, CPdry = 1004.64, CVdry = CPdry - Rdry, PRE00 = 100000.0;
+    const int i = g.IS + blockIdx.x * blockDim.x + threadIdx.x;
+    const int j = g.JS + blockIdx.y;
+    if (i > g.IE) return;
+    const size_t col = idx3(g, 1, i, j), ncol = (size_t)g.IMAX * g.JMAX;
+    const size_t sI = g.KA, sJ = (size_t)g.KA * g.IA;
+    double sp = 0.0, sk = 0.0, si = 0.0, st = 0.0;
+    for (int k = g.KS; k <= g.KE; ++k) {
+        const size_t c = col + k - 1;
+        const double dn = DN[c];
+        double w;
+        if (k == g.KS) w = MZ[c] * 0.5;
+        else if (k == g.KE) w = 0.5 * (MZ[c - 1]) / dn;
+        else w = 0.5 * (MZ[c - 1] + MZ[c]) / dn;
+        const double u = 0.5 * (MX[c - sI] + MX[c]) / dn;
+        const double v = 0.5 * (MY[c - sJ] + MY[c]) / dn;
+        const double pres = PRE00 * pow(RT[c] * Rdry / PRE00, CPdry / CVdry);
+        const double temp = pres / (dn * Rdry);
+        const double engp = dn * GRAV * ld(CZ + k - 1);
+        const double engk = 0.5 * dn * (w * w + u * u + v * v);
+        const double engi = dn * 1.0 * temp * CVdry;
+        const double engt = engp + engk + engi;
+        sp += engp * ld(CDZ + k - 1) * ld(CDX + i - 1) * ld(CDY + j - 1);
+        sk += engk * ld(CDZ + k - 1) * ld(CDX + i - 1) * ld(CDY + j - 1);
+        si += engi * ld(CDZ + k - 1) * ld(CDX + i - 1) * ld(CDY + j - 1);
+        st += engt * ld(CDZ + k - 1) * ld(CDX + i - 1) * ld(CDY + j - 1);
+    }
+    const size_t q = (size_t)(i - g.IS) + (size_t)g.IMAX * (j - g.JS);
+    part[q] = st;
+    part[q + ncol] = sp;
+    part[q + 2 * ncol] = sk;
+    part[q + 3 * ncol] = si;
+}
+
+void energy_sum(const Grid &g, const double *DENS, const double *MOMZ, const double *MOMX, const double *MOMY,
+                const double *RHOT, const double *CZ, const double *CDX, const double *CDY, const double *CDZ,
+                double *part, double *out, cudaStream_t st)
+{
+    const size_t ncol = (size_t)g.IMAX * g.JMAX;
+    dim3 b(128), gr((g.IMAX + 127) / 128, g.JMAX);
+    k_energy_col<<<gr, b, 0, st>>>(g, DENS, MOMZ, MOMX, MOMY, RHOT, CZ, CDX, CDY, CDZ, part);
+    for (int n = 0; n < 4; ++n) k_tree_sum<<<1, 1024, 0, st>>>(part + n * ncol, ncol, out + n);
+}
+
 // ---- short-step average of the mass flux for tracer advection
 // (tstep_large_fvm_heve.F90:960-967 and :1012-1019), interior cells ----
 __global__ void k_mflx_acc(const Grid g, double *av, const double *mflx, int nstep, int mode)

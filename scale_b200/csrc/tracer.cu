@@ -84,9 +84,18 @@ __global__ void __launch_bounds__(128) k_tracer_plain(const Grid g, const Tracer
     const long sI = g.KA, sJ = (long)g.KA * g.IA;
     const size_t col = idx3(g, 1, i, j);
     const double rcdx = ld(g.RCDX + i - 1), rcdy = ld(g.RCDY + j - 1);
-    for (int k = g.KS + threadIdx.x; k <= g.KE; k += 32) {
+    // the z flux through the face above a level; the face below is the previous
+    // lane's (lane 0: the previous pass's lane 31; zero below KS)
+    double carry = 0.0;
+    for (int k0 = g.KS; k0 <= g.KE; k0 += 32) {
+        const int k = k0 + threadIdx.x;
+        const bool ok = k <= g.KE;
         const size_t c = col + k - 1;
-        const double hz = hflux_z<S>(g, a, N3, col, k), hzm = hflux_z<S>(g, a, N3, col, k - 1);
+        const double hz = ok ? hflux_z<S>(g, a, N3, col, k) : 0.0;
+        double hzm = __shfl_up_sync(0xffffffffu, hz, 1);
+        if (threadIdx.x == 0) hzm = carry;
+        carry = __shfl_sync(0xffffffffu, hz, 31);
+        if (!ok) continue;
         const double hx = hflux_h<S>(a, N3, 1, c, sI), hxm = hflux_h<S>(a, N3, 1, c - sI, sI);
         const double hy = hflux_h<S>(a, N3, 2, c, sJ), hym = hflux_h<S>(a, N3, 2, c - sJ, sJ);
         const double div = (hz - hzm) * ld(g.RCDZ + k - 1) + (hx - hxm) * rcdx + (hy - hym) * rcdy;

@@ -441,3 +441,11 @@ def domain_sum_dev(var, CDZ, CDX, CDY) -> float:
     out = np.zeros(1)
     call("scale_hevi_domain_sum_dev", var=var, CDZ=CDZ, CDX=CDX, CDY=CDY, total=out)
     return float(out[0])
+
+
+def energy_sum_dev(DENS, MOMZ, MOMX, MOMY, RHOT, CZ, CDZ, CDX, CDY) -> dict:
+    """FP64 domain totals of the dry-air energies [J]: ENGT, ENGP, ENGK, ENGI."""
+    out = np.zeros(4)
+    call("scale_hevi_energy_sum_dev", DENS=DENS, MOMZ=MOMZ, MOMX=MOMX, MOMY=MOMY, RHOT=RHOT, CZ=CZ, CDZ=CDZ,
+         CDX=CDX, CDY=CDY, totals=out)
+    return dict(zip(("ENGT", "ENGP", "ENGK", "ENGI"), (float(v) for v in out)))

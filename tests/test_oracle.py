@@ -497,3 +497,50 @@ def test_heve_conserve(scheme):
     _heve_steps(c, 3)
     assert abs(oracle.domain_sum(g, st["DENS"]) - m0) / m0 < 1e-13
     assert abs(oracle.domain_sum(g, st["RHOT"]) - t0) / t0 < 1e-13
+
+
+def _energy_numpy(g, st, CZ):
+    """Dry-air energies per cell restated with numpy (the cell-centre velocities of
+    ATMOS_DIAGNOSTIC_CARTESC_get_vel on flat terrain, TEMP of rhot2temp_pres)."""
+    ks, ke, is_, ie, js, je = g.KS - 1, g.KE, g.IS - 1, g.IE, g.JS - 1, g.JE
+    D, MZ, MX, MY, RT = (st[n] for n in ("DENS", "MOMZ", "MOMX", "MOMY", "RHOT"))
+    d = D[ks:ke, is_:ie, js:je]
+    w = np.empty_like(d)
+    w[0] = MZ[ks, is_:ie, js:je] * 0.5
+    w[1:-1] = 0.5 * (MZ[ks:ke - 2, is_:ie, js:je] + MZ[ks + 1:ke - 1, is_:ie, js:je]) / d[1:-1]
+    w[-1] = 0.5 * MZ[ke - 2, is_:ie, js:je] / d[-1]
+    u = 0.5 * (MX[ks:ke, is_ - 1:ie - 1, js:je] + MX[ks:ke, is_:ie, js:je]) / d
+    v = 0.5 * (MY[ks:ke, is_:ie, js - 1:je - 1] + MY[ks:ke, is_:ie, js:je]) / d
+    Rd, Cp = 287.04, 1004.64
+    Cv = Cp - Rd
+    pres = 100000.0 * (RT[ks:ke, is_:ie, js:je] * Rd / 100000.0) ** (Cp / Cv)
+    temp = pres / (d * Rd)
+    vol = g.CDZ[ks:ke, None, None] * g.CDX[None, is_:ie, None] * g.CDY[None, None, js:je]
+    engp = d * 9.80665 * CZ[ks:ke, None, None]
+    engk = 0.5 * d * (w * w + u * u + v * v)
+    engi = d * temp * Cv
+    return {n: float(np.sum(e * vol)) for n, e in
+            (("ENGT", engp + engk + engi), ("ENGP", engp), ("ENGK", engk), ("ENGI", engi))}
+
+
+def test_energy_budget_matches_a_direct_restatement():
+    g = helpers.small_grid(IMAX=10, JMAX=8, KMAX=12, stretched=True)
+    c = helpers.small_case(g, "CD4")
+    helpers.perturb_state(c)
+    got = oracle.energy_sum(g, c.state, g.CZ)
+    want = _energy_numpy(g, c.state, g.CZ)
+    for n in want:
+        assert abs(got[n] - want[n]) <= 1e-12 * abs(want["ENGT"]), (n, got[n], want[n])
+    assert abs(got["ENGT"] - (got["ENGP"] + got["ENGK"] + got["ENGI"])) <= 1e-12 * got["ENGT"]
+    assert got["ENGK"] > 0.0 and got["ENGP"] > 0.0 and got["ENGI"] > 0.0
+
+
+def test_energy_budget_of_a_state_at_rest_has_no_kinetic_part():
+    g = helpers.small_grid(IMAX=6, JMAX=5, KMAX=10)
+    c = helpers.small_case(g, "UD3", wind=0.0)
+    st = {n: v.copy(order="F") for n, v in c.state.items()}
+    for n in ("MOMZ", "MOMX", "MOMY"):
+        st[n][...] = 0.0
+    e = oracle.energy_sum(g, st, g.CZ)
+    assert e["ENGK"] == 0.0
+    assert e["ENGT"] == e["ENGP"] + e["ENGI"] or abs(e["ENGT"] - e["ENGP"] - e["ENGI"]) <= 1e-13 * e["ENGT"]
