@@ -253,7 +253,7 @@ def run_b200(args):
     ms_step = elapsed_ms / args.steps
     value = aggregate_rate(cells, world, args.steps, elapsed_ms)
 
-    # ---- roofline of the HEVI stage (k_hevi_horiz + k_hevi_column) ----
+    # ---- roofline of the HEVI stage (tiled: k_hevi_explicit + k_hevi_column) ----
     peaks = {}
     pk = ROOT / "MEASURED_PEAKS.json"
     if pk.exists():
@@ -264,7 +264,7 @@ def run_b200(args):
     stage_ms = stage_total / max(nst, 1)
     achieved = STAGE_BYTES * cells / (stage_ms * 1e-3) / 1e9 if stage_ms > 0 else None
     traffic = read_traffic()
-    roofline = {"bound": "hbm", "kernel": "k_hevi_stage (one HEVI stage)",
+    roofline = {"bound": "hbm", "kernel": stage_form_name(hevi),
                 "achieved": achieved, "peak": hbm, "peak_source": peak_src, "unit": "GB/s",
                 "frac": (achieved / hbm) if achieved else None, "algorithmic_bytes_per_launch": STAGE_BYTES * cells,
                 "stage_ms": stage_ms, "traffic": traffic,
@@ -351,7 +351,7 @@ def run_b200(args):
             "error_vs_fp64": {"steps": args.warmup + args.steps, "fields": errs},
             "mass_drift_rel": abs(m1x - m0x) / m0x,
             "energy_ENGT_vs_fp64_rel": (e_mixed["ENGT"] - e1["ENGT"]) / e1["ENGT"],
-            "roofline": {"bound": "hbm", "kernel": "k_hevi_stage<float> (one HEVI stage)", "achieved": ach,
+            "roofline": {"bound": "hbm", "kernel": stage_form_name(hevi, "float"), "achieved": ach,
                          "peak": hbm, "unit": "GB/s", "frac": (ach / hbm) if ach else None,
                          "algorithmic_bytes_per_launch": MIXED_STAGE_BYTES * cells, "stage_ms": sm_ms,
                          "step_frac": (4 * MIXED_STAGE_BYTES + MIXED_NUMFILTER_BYTES) * cells / (ms_mixed * 1e-3) / 1e9 / hbm},
@@ -538,6 +538,34 @@ def run_tracer(args, c, hevi, torch, X, mflx, g, cells, stream, t0, t1, dist, wo
     # tracer mass (rho*q) after the steps against the start, FP64 device sums
     rq = [hevi.domain_sum_dev(X["DENS"] * qt[n * N3:(n + 1) * N3], g.CDZ, g.CDX, g.CDY) for n in range(c.QA)]
     rq0 = [hevi.domain_sum_dev(dens0 * q_start[n], g.CDZ, g.CDX, g.CDY) for n in range(c.QA)]
+
+    # the same large steps with FP32 flux and limiter arithmetic, from the same start
+    q64 = qt.clone()
+    kw32 = dict(kw, RHOQ_t=zero.float(), mflx_hi=mflx.float(), num_diff=ndq.float())
+
+    def large_step_mixed():
+        for n in range(c.QA):
+            qn = qt[n * N3:(n + 1) * N3]
+            hevi.ATMOS_DYN_Tinteg_tracer_rk3_mixed_dev(QTRC=qn, QTRC0=qn, **kw32)
+
+    for _ in range(max(3, args.warmup)):
+        large_step_mixed()
+    hevi.check()
+    qt.copy_(q0)
+    torch.cuda.synchronize()
+    t0.record(stream)
+    for _ in range(k):
+        large_step_mixed()
+    t1.record(stream)
+    torch.cuda.synchronize()
+    hevi.check()
+    ms32 = max_over_ranks(t0.elapsed_time(t1), dist, "cuda") / k / c.QA
+    err32 = float((qt - q64).abs().max()) / float(q64.abs().max())
+    mixed = {"ms_per_tracer_large_step": ms32, "speedup_vs_fp64": ms_tracer / ms32,
+             "precision": "FP32 flux and FCT limiter arithmetic, FP32 mass fluxes, num_diff and tendency; FP64 tracer, "
+                          "densities and update",
+             "max_rel_error_vs_fp64": err32, "large_steps": k,
+             "min_tracer_after": min(float(qt[n * N3:(n + 1) * N3].min()) for n in range(c.QA))}
     return {
         "value": aggregate_rate(cells, world, 1, ms_tracer), "unit": "cell-updates/s per tracer",
         "ms_per_tracer_large_step": ms_tracer, "ms_per_large_step": ms, "tracers": c.QA, "large_steps": k,
@@ -548,6 +576,7 @@ def run_tracer(args, c, hevi, torch, X, mflx, g, cells, stream, t0, t1, dist, wo
         "kernel_launches_per_tracer_step": launches / (k * c.QA),
         "min_tracer_after": qmin, "tracer_mass_change_rel": [(a - b) / b if b else 0.0 for a, b in zip(rq, rq0)],
         "sections_ms_per_large_step": {kk: v[1] / k for kk, v in prof.items()},
+        "mixed": mixed,
     }
 
 
@@ -777,6 +806,14 @@ def run_adjoint(args, hevi, torch):
             hevi.finalize()
     out["workload"] = "warm bubble 128x128x64, dx=500 m, dt=1 s; J over x,y in [20,44] km, z in [2,6] km"
     return out
+
+
+def stage_form_name(hevi, r="double"):
+    """The kernels of one HEVI stage in the stage form the library runs now."""
+    tx, raster = hevi.stage_shape_get(r == "float")
+    if tx == 0:
+        return f"one HEVI stage: k_hevi_explicit<{r}> + k_hevi_column<{r}> (tiled form)"
+    return f"one HEVI stage: k_hevi_stage<{r}> (fused form, tile width {tx}, raster {raster})"
 
 
 def read_traffic():

@@ -297,6 +297,21 @@ int ATMOS_DYN_Tstep_tracer_fvm_heve_b200_dev(SCALE_HEVI_TSTEP_TRACER_ARGS);
 int ATMOS_DYN_Tinteg_tracer_rk3_b200(SCALE_HEVI_TINTEG_TRACER_ARGS);
 int ATMOS_DYN_Tinteg_tracer_rk3_b200_dev(SCALE_HEVI_TINTEG_TRACER_ARGS);
 
+/* The same tracer RK3 (scale_atmos_dyn_tinteg_tracer_rk3.F90:92-210) on the
+ * mixed-precision path: the high- and low-order fluxes and the FCT limiter
+ * (scale_atmos_dyn_common.F90:1922-2734) in FP32, with FP32 mass fluxes,
+ * tracer num_diff and tendency (the arrays of the mixed short step); the
+ * tracer, its RK stage values, the densities and the update stay FP64. The
+ * limiter's zero tests use the FP32 epsilon. Flat terrain; device pointers. */
+#define SCALE_HEVI_TINTEG_TRACER_MIXED_ARGS                                                                    \
+    double *QTRC, const double *QTRC0, const float *RHOQ_t,                                                    \
+    const double *DENS0, const double *DENS, const float *mflx_hi, const float *num_diff,                      \
+    const double *GSQRT, const double *MAPF,                                                                   \
+    const double *CDZ, const double *RCDZ, const double *RCDX, const double *RCDY,                             \
+    const int *BND_W, const int *BND_E, const int *BND_S, const int *BND_N,                                    \
+    const double *dtl, const int *FLAG_FCT_TRACER, const int *FLAG_FCT_ALONG_STREAM
+int ATMOS_DYN_Tinteg_tracer_rk3_b200_mixed_dev(SCALE_HEVI_TINTEG_TRACER_MIXED_ARGS);
+
 /* ---------------------------------------------------------------------------
  * Periodic halo exchange of nfields consecutive (KA,IA,JA) device fields on
  * one GPU. Replaces COMM_vars8 + COMM_wait of a periodic single-rank domain

@@ -67,6 +67,7 @@ struct Ctx {
     // mixed-precision path (allocated on first use): flux RK sums, column-solve
     // sources and the filtered quantities in FP32
     float *facc_f = nullptr, *colscr_f = nullptr, *phi_f = nullptr;
+    float *tr_f = nullptr;          // mixed tracer limiter: phi_lo, anti(3), rjp, rjm = 6*N3 (on first use)
     double *tr = nullptr;           // tracer: RK1, RK2, phi_lo, anti(3), rjp, rjm = 8*N3
     double *lg = nullptr;           // large step: DENS00, RT2P, DPRES0, REF_rhot, mflx_av(3), DDIV = 8*N3
     double *sum_part = nullptr, *sum_out = nullptr;
@@ -196,7 +197,7 @@ void free_all()
                       C.tw_buf};
     for (double *b : bufs) if (b) cudaFree(b);
     for (auto &kv : C.stage) cudaFree(kv.second.first);
-    for (float *b : {C.facc_f, C.colscr_f, C.phi_f}) if (b) cudaFree(b);
+    for (float *b : {C.facc_f, C.colscr_f, C.phi_f, C.tr_f}) if (b) cudaFree(b);
     for (double *b : {C.ad_scratch, C.ad_zero, C.ad_nd, C.ad_flx}) if (b) cudaFree(b);
     if (C.status) cudaFree(C.status);
     if (C.count) cudaFree(C.count);
@@ -733,32 +734,46 @@ int run_divergence(double *DDIV, const double *MOMZ, const double *MOMX, const d
 }
 
 // RK3 tracer integrator (tinteg_tracer_rk3.F90:92-210) on device arrays
-int run_tracer_rk3(double *QTRC, const double *QTRC0, const double *RHOQ_t, const double *DENS0, const double *DENS,
-                   const double *mflx, const double *ndq, double dtl, bool fct, bool along)
+// the limiter scratch of each precision: phi_lo, anti (3), rjp, rjm
+template <typename R> void limiter_scratch(TracerArgsT<R> &a);
+template <> void limiter_scratch<double>(TracerArgsT<double> &a)
+{
+    a.phi_lo = C.tr + 2 * C.N3; a.anti = C.tr + 3 * C.N3; a.rjp = C.tr + 6 * C.N3; a.rjm = C.tr + 7 * C.N3;
+}
+template <> void limiter_scratch<float>(TracerArgsT<float> &a)
+{
+    a.phi_lo = C.tr_f; a.anti = C.tr_f + C.N3; a.rjp = C.tr_f + 4 * C.N3; a.rjm = C.tr_f + 5 * C.N3;
+}
+
+template <typename R>
+int run_tracer_rk3(double *QTRC, const double *QTRC0, const R *RHOQ_t, const double *DENS0, const double *DENS,
+                   const R *mflx, const R *ndq, double dtl, bool fct, bool along)
 {
     if (fct && C.halo_fn)
         return fail(SCALE_HEVI_ERR_UNSUPPORTED, "the FCT tracer limiter is not available with a halo exchange hook");
-    TracerArgs a{};
+    TracerArgsT<R> a{};
     a.QTRC0 = QTRC0; a.RHOQ_t = RHOQ_t; a.DENS0 = DENS0; a.DENS = DENS; a.mflx = mflx; a.ndq = ndq;
-    a.phi_lo = C.tr + 2 * C.N3; a.anti = C.tr + 3 * C.N3; a.rjp = C.tr + 6 * C.N3; a.rjm = C.tr + 7 * C.N3;
+    limiter_scratch(a);
     a.along_stream = along ? 1 : 0;
     // terrain-following metrics of the large step (the mass-point MAPF slice comes first)
     a.GS = C.terrain ? C.tm.GSQRT : nullptr;
     a.MAPF = C.terrain ? C.tm.MAPF : nullptr;
-    double *rk1 = C.tr, *rk2 = C.tr + C.N3;
+    double *rk1 = C.tr, *rk2 = C.tr + C.N3; // the tracer's RK stage values stay FP64
+    const char *sec = sizeof(R) == sizeof(double) ? "tracer" : "tracer_mixed";
+    const char *sec_fct = sizeof(R) == sizeof(double) ? "tracer_fct" : "tracer_fct_mixed";
     // stage 1: dt/3 with DENS0 + (DENS-DENS0)/3
     a.QTRCo = rk1; a.QTRC = QTRC; a.dens_mode = 1; a.dtl = dtl / 3.0;
-    CK(timed("tracer", [&] { CU(launch_tracer_stage(C.g, a, C.scheme_tracer, false, C.stream)); return SCALE_HEVI_OK; }));
+    CK(timed(sec, [&] { CU(launch_tracer_stage(C.g, a, C.scheme_tracer, false, C.stream)); return SCALE_HEVI_OK; }));
     ++C.launches;
     CK(halo(&rk1, 1));
     // stage 2: dt/2 with DENS0 + (DENS-DENS0)*0.5
     a.QTRCo = rk2; a.QTRC = rk1; a.dens_mode = 2; a.dtl = dtl / 2.0;
-    CK(timed("tracer", [&] { CU(launch_tracer_stage(C.g, a, C.scheme_tracer, false, C.stream)); return SCALE_HEVI_OK; }));
+    CK(timed(sec, [&] { CU(launch_tracer_stage(C.g, a, C.scheme_tracer, false, C.stream)); return SCALE_HEVI_OK; }));
     ++C.launches;
     CK(halo(&rk2, 1));
     // stage 3: dt with DENS, FCT when requested
     a.QTRCo = QTRC; a.QTRC = rk2; a.dens_mode = 0; a.dtl = dtl;
-    CK(timed(fct ? "tracer_fct" : "tracer", [&] { CU(launch_tracer_stage(C.g, a, C.scheme_tracer, fct, C.stream)); return SCALE_HEVI_OK; }));
+    CK(timed(fct ? sec_fct : sec, [&] { CU(launch_tracer_stage(C.g, a, C.scheme_tracer, fct, C.stream)); return SCALE_HEVI_OK; }));
     C.launches += fct ? 4 : 1;
     return SCALE_HEVI_OK;
 }
@@ -1370,6 +1385,22 @@ int ATMOS_DYN_Tinteg_tracer_rk3_b200_dev(SCALE_HEVI_TINTEG_TRACER_ARGS)
                           *FLAG_FCT_ALONG_STREAM != 0);
 }
 
+// the tracer RK3 with FP32 flux and limiter arithmetic (the tracer and the
+// densities stay FP64); flat terrain
+int ATMOS_DYN_Tinteg_tracer_rk3_b200_mixed_dev(SCALE_HEVI_TINTEG_TRACER_MIXED_ARGS)
+{
+    CK(check_bnd(BND_W, BND_E, BND_S, BND_N));
+    const double *dGS, *dMAPF;
+    CK(tracer_metrics(GSQRT, MAPF, true, &dGS, &dMAPF));
+    if (dGS) return fail(SCALE_HEVI_ERR_UNSUPPORTED, "the mixed-precision tracer advection takes flat terrain only");
+    if (!C.tr_f) CK(falloc(&C.tr_f, 6 * C.N3));
+    std::vector<double> one(C.g.KA > C.g.IA ? (C.g.KA > C.g.JA ? C.g.KA : C.g.JA) : (C.g.IA > C.g.JA ? C.g.IA : C.g.JA), 1.0);
+    CK(prepare_tables(CDZ, one.data(), RCDZ, one.data(), one.data(), RCDX, one.data(), one.data(), RCDY, one.data(),
+                      nullptr, nullptr, nullptr));
+    return run_tracer_rk3(QTRC, QTRC0, RHOQ_t, DENS0, DENS, mflx_hi, num_diff, *dtl, *FLAG_FCT_TRACER != 0,
+                          *FLAG_FCT_ALONG_STREAM != 0);
+}
+
 int ATMOS_DYN_Tinteg_tracer_rk3_b200(SCALE_HEVI_TINTEG_TRACER_ARGS)
 {
     CK(check_bnd(BND_W, BND_E, BND_S, BND_N));
@@ -1565,7 +1596,7 @@ int ATMOS_DYN_Tstep_large_fvm_heve_b200_dev(SCALE_HEVI_LARGE_ARGS)
         CK(wait_in(3));
         for (int q = 0; q < qa; ++q) {
             double *qt = QTRC + (size_t)q * N3;
-            CK(run_tracer_rk3(qt, qt, RHOQ_tp + (size_t)q * N3, DENS00, DENS, mflx_hi, nullptr, dtl,
+            CK(run_tracer_rk3<double>(qt, qt, RHOQ_tp + (size_t)q * N3, DENS00, DENS, mflx_hi, nullptr, dtl,
                               *FLAG_FCT_TRACER != 0, *FLAG_FCT_ALONG_STREAM != 0));
             CK(halo(&qt, 1));
             CK(done(3, q));

@@ -103,23 +103,30 @@ __host__ __device__ __forceinline__ NdCoef member_nd(const NdCoef &c, const Grid
 }
 
 // ---- tracer advection (tracer.cu) ----
-struct TracerArgs {
+// R: the type of the flux and limiter arithmetic and of the flux-like arrays
+// (mass fluxes, num_diff, the tendency, the limiter scratch): double on the
+// plain path, float on the mixed-precision path. The tracer itself (the stage
+// values and QTRC0), the densities and the update stay FP64.
+template <typename R>
+struct TracerArgsT {
     double *QTRCo;
     const double *QTRC;   // stage input (high-order flux values)
     const double *QTRC0;  // value at the start of the large step (phi_in of the limiter)
-    const double *RHOQ_t;
+    const R *RHOQ_t;
     const double *DENS0, *DENS;
     int dens_mode;        // density of the stage: 0 DENS, 1 DENS0+(DENS-DENS0)/3, 2 DENS0+(DENS-DENS0)*0.5
-    const double *mflx;   // (KA,IA,JA,3)
-    const double *ndq;    // (KA,IA,JA,3) or null for ND_COEF_Q = 0
+    const R *mflx;        // (KA,IA,JA,3)
+    const R *ndq;         // (KA,IA,JA,3) or null for ND_COEF_Q = 0
     double dtl;
-    double *phi_lo, *anti, *rjp, *rjm; // limiter scratch (anti is 3 fields)
+    R *phi_lo, *anti, *rjp, *rjm; // limiter scratch (anti is 3 fields)
     int along_stream;
     // terrain-following metrics, null on flat terrain: GSQRT (KA,IA,JA,7) and
-    // the MAPF slice (IA,JA,2) of the mass points
+    // the MAPF slice (IA,JA,2) of the mass points (FP64 path only)
     const double *GS, *MAPF;
 };
-cudaError_t launch_tracer_stage(const Grid &g, const TracerArgs &a, int scheme, bool fct, cudaStream_t st);
+using TracerArgs = TracerArgsT<double>;
+template <typename R>
+cudaError_t launch_tracer_stage(const Grid &g, const TracerArgsT<R> &a, int scheme, bool fct, cudaStream_t st);
 // ATMOS_DYN_divergence with every metric term (misc.cu)
 void divergence_terrain(const Grid &g, double *DDIV, const double *MOMZ, const double *MOMX, const double *MOMY,
                         const Metrics &M, double J33G, cudaStream_t st);

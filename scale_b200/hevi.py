@@ -407,6 +407,12 @@ def ATMOS_DYN_Tinteg_tracer_rk3_dev(**kw):
     call("ATMOS_DYN_Tinteg_tracer_rk3_b200_dev", **kw)
 
 
+def ATMOS_DYN_Tinteg_tracer_rk3_mixed_dev(**kw):
+    """Tracer RK3 with FP32 flux and limiter arithmetic: float32 mflx_hi,
+    num_diff and RHOQ_t; float64 tracer and densities (device arrays)."""
+    call("ATMOS_DYN_Tinteg_tracer_rk3_b200_mixed_dev", **kw)
+
+
 def ATMOS_DYN_Tstep_large_fvm_heve_dev(**kw):
     call("ATMOS_DYN_Tstep_large_fvm_heve_b200_dev", **kw)
 

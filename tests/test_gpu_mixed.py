@@ -105,3 +105,47 @@ def test_mixed_precision_six_point_schemes(scheme):
     for n in STATE:
         emax, erms = field_errors(st32[n], st64[n], c.g)
         assert emax <= 1e-5, f"{n}: max {emax:.3e} rms {erms:.3e}"
+
+
+@pytest.mark.parametrize("fct,along", [(False, True), (True, True), (True, False)])
+def test_mixed_tracer_rk3_matches_fp64(fct, along):
+    """The tracer RK3 with FP32 flux and limiter arithmetic against the FP64
+    entry on the same inputs (the FP32 mass fluxes, num_diff and tendency are
+    the FP64 ones rounded): the tracer agrees to 1e-5 of its largest value and
+    the limiter keeps it as bounded as the FP64 limiter does."""
+    import torch
+
+    import helpers
+    from test_gpu_parity import _tracer_inputs
+
+    g = helpers.small_grid(IMAX=20, JMAX=16, KMAX=24, stretched=True)
+    c = helpers.small_case(g)
+    helpers.perturb_state(c)
+    q0, _, d0, d, mflx, rhoq, GS, MAPF = _tracer_inputs(g, c)
+    ndq = np.asfortranarray(1e-6 * np.random.default_rng(9).normal(size=g.shape + (3,)))
+    dev = lambda x, t=torch.float64: torch.from_numpy(np.ravel(x, order="K").copy()).to("cuda", t)  # noqa: E731
+    out = {}
+    hevi.setup(g.index_dict(), "UD3", "UD3")
+    try:
+        for mixed in (False, True):
+            ft = torch.float32 if mixed else torch.float64
+            q = dev(q0)
+            kw = dict(QTRC=q, QTRC0=q, RHOQ_t=dev(rhoq, ft), DENS0=dev(d0), DENS=dev(d), mflx_hi=dev(mflx, ft),
+                      num_diff=dev(ndq, ft), GSQRT=dev(GS), MAPF=dev(MAPF), CDZ=g.CDZ, RCDZ=g.RCDZ, RCDX=g.RCDX,
+                      RCDY=g.RCDY, BND_W=False, BND_E=False, BND_S=False, BND_N=False, dtl=5.0,
+                      FLAG_FCT_TRACER=fct, FLAG_FCT_ALONG_STREAM=along)
+            for _ in range(3):
+                (hevi.ATMOS_DYN_Tinteg_tracer_rk3_mixed_dev if mixed else hevi.ATMOS_DYN_Tinteg_tracer_rk3_dev)(**kw)
+                hevi.COMM_vars8_dev(q, 1)
+            hevi.check()
+            out[mixed] = q.cpu().numpy().reshape(g.shape, order="F")
+    finally:
+        hevi.finalize()
+    sl = (slice(g.KS - 1, g.KE), slice(g.IS - 1, g.IE), slice(g.JS - 1, g.JE))
+    a64, a32 = out[False][sl], out[True][sl]
+    assert np.isfinite(a32).all()
+    err = np.max(np.abs(a32 - a64)) / np.max(np.abs(a64))
+    assert err <= 1e-5, f"max relative error {err:.3e}"
+    if fct:
+        # no new minimum beyond FP32 rounding of the FP64 run's own
+        assert a32.min() >= a64.min() - 1e-6 * np.max(np.abs(a64))
