@@ -681,15 +681,28 @@ def run_mixed_large(args, hevi, torch):
         n64, t64 = prof64.get("hevi_stage", (0, 0.0))
         n32, t32 = prof32.get("hevi_stage_mixed", (0, 0.0))
         s64, s32 = t64 / max(n64, 1), t32 / max(n32, 1)
+
+        def leg_roofline(stage_bytes, step_bytes, stage_ms, step_ms, r):
+            ach = stage_bytes * cells / (stage_ms * 1e-3) / 1e9 if stage_ms else None
+            return {"bound": "hbm", "kernel": stage_form_name(hevi, r), "achieved": ach, "peak": hbm,
+                    "peak_source": "measured" if "hbm_gbs" in peaks else "fallback", "unit": "GB/s",
+                    "frac": ach / hbm if ach else None, "algorithmic_bytes_per_launch": stage_bytes * cells,
+                    "algorithmic_bytes_per_cell": stage_bytes, "stage_ms": stage_ms,
+                    "step_frac": step_bytes * cells / (step_ms * 1e-3) / 1e9 / hbm}
         return {
             "workload": f"{g.IMAX}x{g.JMAX}x{g.KMAX} multi-bubble (32 seeded bubbles +1..3 K), dx=dz=200 m, UD3, dt=0.4 s",
             "cells": cells, "steps": k, "input_prep_s": prep_s,
             "fp64": {"value": cells / (ms64 * 1e-3), "ms_per_step": ms64, "stage_ms": s64,
-                     "stage_frac_of_measured_hbm": STAGE_BYTES * cells / (s64 * 1e-3) / 1e9 / hbm if s64 else None},
+                     "stage_frac_of_measured_hbm": STAGE_BYTES * cells / (s64 * 1e-3) / 1e9 / hbm if s64 else None,
+                     "roofline": leg_roofline(STAGE_BYTES, STEP_BYTES, s64, ms64, "double"),
+                     "sections_ms_per_step": {q: v[1] / k for q, v in prof64.items()}},
             "mixed": {"value": cells / (ms32 * 1e-3), "ms_per_step": ms32, "stage_ms": s32,
                       "stage_frac_of_measured_hbm": MIXED_STAGE_BYTES * cells / (s32 * 1e-3) / 1e9 / hbm if s32 else None,
                       "step_frac_of_measured_hbm": (4 * MIXED_STAGE_BYTES + MIXED_NUMFILTER_BYTES) * cells
-                      / (ms32 * 1e-3) / 1e9 / hbm},
+                      / (ms32 * 1e-3) / 1e9 / hbm,
+                      "roofline": leg_roofline(MIXED_STAGE_BYTES, 4 * MIXED_STAGE_BYTES + MIXED_NUMFILTER_BYTES, s32,
+                                               ms32, "float"),
+                      "sections_ms_per_step": {q: v[1] / k for q, v in prof32.items()}},
             "speedup_mixed_vs_fp64": ms64 / ms32,
             "error_vs_fp64": {"steps": total, "fields": errs,
                               "max_over_fields": max(e["max"] for e in errs.values()), "target": 1e-5},
@@ -706,8 +719,10 @@ def run_mixed_large(args, hevi, torch):
 
 def run_ensemble(args, hevi, torch):
     """The 48-member uneven ensemble (16 each of 64x64x64, 128x128x96 and
-    256x256x96): every kernel of a short step launched once over all members,
-    the step replayed as a CUDA graph, the stage shape autotuned."""
+    256x256x96), advanced two ways on the same inputs: every kernel of a short
+    step launched once over all members with the step replayed as a CUDA graph
+    and the stage shape autotuned, and the whole short step as ONE persistent
+    cooperative launch (also replayed as a graph)."""
     from scale_b200 import mkinit
     from scale_b200.ensemble import Ensemble
 
@@ -719,16 +734,14 @@ def run_ensemble(args, hevi, torch):
     for c in cases:
         k = f"{c.g.IMAX}x{c.g.JMAX}x{c.g.KMAX}"
         sizes[k] = sizes.get(k, 0) + 1
-    e = Ensemble(cases)
-    del cases
-    try:
-        hevi.stage_autotune(True)
-        e.capture(1)  # one eager step (tunes the stage shape), then one recorded step
+    k = args.ensemble_steps
+
+    def timed(e):
+        e.capture(1)  # one eager step (tunes the stage shape / builds the block maps), then one recorded step
         e.run(max(3, args.warmup))
         hevi.check()
         stream = torch.cuda.ExternalStream(hevi.stream_handle())
         t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        k = args.ensemble_steps
         torch.cuda.synchronize()
         l0 = hevi.kernel_launches()
         t0.record(stream)
@@ -738,14 +751,33 @@ def run_ensemble(args, hevi, torch):
         ms = t0.elapsed_time(t1)
         launches = hevi.kernel_launches() - l0
         hevi.check()
+        return ms, launches
+
+    e = Ensemble(cases)
+    try:
+        hevi.stage_autotune(True)
+        ms, launches = timed(e)
         shape = hevi.stage_shape_get()
-        return {"value": cells * k / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms / k, "steps": k,
-                "members": len(e.shapes), "sizes": sizes, "cells": cells,
-                "kernel_launches_per_step": launches / k, "cuda_graph": True,
-                "stage_shape": {"tile_x": shape[0], "raster": shape[1]}, "autotune": hevi.autotune_report(),
-                "input_prep_s": prep_s, "l2": "inputs larger than L2"}
+        out = {"value": cells * k / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms / k, "steps": k,
+               "members": len(e.shapes), "sizes": sizes, "cells": cells,
+               "kernel_launches_per_step": launches / k, "cuda_graph": True,
+               "stage_shape": {"tile_x": shape[0], "raster": shape[1]}, "autotune": hevi.autotune_report(),
+               "input_prep_s": prep_s, "l2": "inputs larger than L2"}
     finally:
         e.close()
+    e = Ensemble(cases, persistent=True)
+    del cases
+    try:
+        ms, launches = timed(e)
+        out["persistent"] = {
+            "value": cells * k / (ms * 1e-3), "unit": UNIT, "ms_per_step": ms / k, "steps": k,
+            "kernel_launches_per_step": launches / k, "ctas": hevi.persistent_grid(), "cuda_graph": True,
+            "step": "numerical filter + RK4 of 4 HEVI stages + boundary values and halos as one cooperative launch "
+                    "(scale_hevi_short_step_persistent_dev), fused stage form, tile width 16",
+        }
+    finally:
+        e.close()
+    return out
 
 
 def run_adjoint(args, hevi, torch):

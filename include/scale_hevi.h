@@ -437,6 +437,60 @@ int scale_hevi_ensemble_setup(int n, const scale_hevi_index *idx, const char *fl
 int scale_hevi_ensemble_layout(long long *cell0, long long *col0, long long *z0, long long *x0, long long *y0);
 
 /* ---------------------------------------------------------------------------
+ * One short step of the large step's loop as ONE persistent launch; no
+ * counterpart in the reference. The numerical filter of the state
+ * (ATMOS_DYN_numfilter_coef, scale_atmos_dyn_common.F90:385-985, ND_ORDER 1,
+ * ND_USE_RS, DT = dt), the RK4 short step of HEVI stages
+ * (ATMOS_DYN_tinteg_short_rk4, scale_atmos_dyn_tinteg_short_rk4.F90:199-666),
+ * the vertical boundary values and the lateral halo of the state
+ * (scale_atmos_dyn_tstep_large_fvm_heve.F90:847-944): the same results, bit
+ * for bit, as ATMOS_DYN_numfilter_coef_b200_dev,
+ * ATMOS_DYN_Tinteg_short_rk4_b200_dev (tile width 16) and
+ * scale_hevi_boundary_dev called in turn, for one domain or every member of
+ * an ensemble (pooled arrays as above). Flat terrain (J33G = 1), no
+ * divergence damping, no halo exchange hook; SCALE_HEVI_ERR_UNSUPPORTED when
+ * the registered short step is not RK4 of HEVI stages.
+ *
+ * The launch is cooperative: as many CTAs as the GPU holds at once, which take
+ * the blocks of each phase in turn and meet at a grid barrier between phases.
+ * Every barrier waits at most a time limit (2 s unless
+ * scale_hevi_persistent_wait says otherwise); on expiry the launch ends and
+ * the next scale_hevi_check reports SCALE_HEVI_ERR_CUDA. The call can be
+ * captured in a CUDA graph (scale_hevi_capture_begin). The _mixed form takes
+ * the FP32 flux-like arrays of the mixed-precision path.
+ *
+ * scale_hevi_persistent_wait sets the barrier time limit (0 < seconds <= 60)
+ * and, for a test of that limit, extra_arrivals = 1 makes every barrier wait
+ * for one CTA more than the grid has, so that it expires. scale_hevi_persistent_grid
+ * gives the CTA count of the last launch.
+ * ------------------------------------------------------------------------- */
+#define SCALE_HEVI_SHORT_STEP_ARGS                                                                             \
+    double *DENS, double *MOMZ, double *MOMX, double *MOMY, double *RHOT,                                      \
+    double *mflx_hi, double *tflx_hi, double *num_diff,                                                        \
+    const double *DENS_t, const double *MOMZ_t, const double *MOMX_t, const double *MOMY_t, const double *RHOT_t, \
+    const double *DPRES0, const double *RT2P, const double *CORIOLI, const double *wdamp_coef,                 \
+    const double *CDZ, const double *CDX, const double *CDY, const double *FDZ, const double *FDX,             \
+    const double *FDY, const double *RCDZ, const double *RCDX, const double *RCDY,                             \
+    const double *RFDZ, const double *RFDX, const double *RFDY,                                                \
+    const double *REF_dens, const double *REF_pott, const double *REF_rhot,                                    \
+    const double *ND_COEF, const double *ND_SFC_FACT, const double *dt
+#define SCALE_HEVI_SHORT_STEP_MIXED_ARGS                                                                       \
+    double *DENS, double *MOMZ, double *MOMX, double *MOMY, double *RHOT,                                      \
+    float *mflx_hi, float *tflx_hi, float *num_diff,                                                           \
+    const float *DENS_t, const float *MOMZ_t, const float *MOMX_t, const float *MOMY_t, const float *RHOT_t,   \
+    const double *DPRES0, const double *RT2P, const double *CORIOLI, const double *wdamp_coef,                 \
+    const double *CDZ, const double *CDX, const double *CDY, const double *FDZ, const double *FDX,             \
+    const double *FDY, const double *RCDZ, const double *RCDX, const double *RCDY,                             \
+    const double *RFDZ, const double *RFDX, const double *RFDY,                                                \
+    const double *REF_dens, const double *REF_pott, const double *REF_rhot,                                    \
+    const double *ND_COEF, const double *ND_SFC_FACT, const double *dt
+
+int scale_hevi_short_step_persistent_dev(SCALE_HEVI_SHORT_STEP_ARGS);
+int scale_hevi_short_step_persistent_mixed_dev(SCALE_HEVI_SHORT_STEP_MIXED_ARGS);
+int scale_hevi_persistent_wait(const double *seconds, const int *extra_arrivals);
+int scale_hevi_persistent_grid(int *ctas);
+
+/* ---------------------------------------------------------------------------
  * Launch shape of the stage kernel; no counterpart in the reference. A CTA
  * owns 16 columns as a tile of tile_x x (16/tile_x) columns (tile_x one of
  * 16, 8, 4) and CTAs are issued in raster groups of `raster` tile rows.

@@ -32,14 +32,14 @@ ORACLE_DIR = ROOT / "oracle"
 ORACLE_LIB = ORACLE_DIR / "build" / "liboracle.so"
 
 CU_SOURCES = ["capi.cu", "hevi_stage.cu", "hevi_tma.cu", "numfilter.cu", "tracer.cu", "misc.cu", "noalloc.cu",
-              "adjoint.cu"]
+              "persist.cu", "adjoint.cu"]
 CPP_SOURCES = ["grid_coef.cpp"]
 # The FP32 instantiations of the mixed-precision path compile a second time from
 # these sources, with -DHEVI_FLOAT_TU and FMA contraction on: their results are
 # held to a tolerance against the FP64 path, not bit for bit, so a*b+c may fuse.
-FLOAT_SOURCES = ["hevi_stage.cu", "hevi_tma.cu", "numfilter.cu", "tracer.cu"]
+FLOAT_SOURCES = ["hevi_stage.cu", "hevi_tma.cu", "numfilter.cu", "tracer.cu", "persist.cu"]
 HEADERS = ["hevi_common.cuh", "hevi_stage.cuh", "hevi_kernels.cuh", "hevi_epilogue.cuh", "adjoint.cuh",
-           "grid_coef.h"]
+           "numfilter_body.cuh", "fill_body.cuh", "hevi_stage_body.cuh", "grid_coef.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

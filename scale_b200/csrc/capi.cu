@@ -106,6 +106,12 @@ struct Ctx {
     std::vector<double> ad_vec[12]; // CDZ CDX CDY FDZ FDX FDY RCDZ RCDX RCDY RFDZ RFDX RFDY
     std::vector<double> ad_wdamp;
     double ad_ndcoef = 0.0, ad_sfc = 1.0;
+    // persistent short step: the barrier and work counters, the barrier time
+    // limit and the extra arrivals a test of that limit asks for
+    unsigned *pbar = nullptr;
+    double pwait_s = 2.0;
+    unsigned pextra = 0;
+    int pgrid = 0; // CTAs of the last persistent launch
 };
 
 Ctx C;
@@ -201,6 +207,7 @@ void free_all()
     for (double *b : {C.ad_scratch, C.ad_zero, C.ad_nd, C.ad_flx}) if (b) cudaFree(b);
     if (C.status) cudaFree(C.status);
     if (C.count) cudaFree(C.count);
+    if (C.pbar) cudaFree(C.pbar);
     for (cudaEvent_t e : C.ev_pool) cudaEventDestroy(e);
     for (cudaEvent_t e : C.copy_ev) if (e) cudaEventDestroy(e);
     if (C.copy_stream) cudaStreamDestroy(C.copy_stream);
@@ -993,6 +1000,10 @@ int scale_hevi_check(void)
     CU(cudaMemcpyAsync(&st, C.status, sizeof st, cudaMemcpyDeviceToHost, C.stream));
     CU(cudaStreamSynchronize(C.stream));
     CU(cudaMemsetAsync(C.status, 0, sizeof(unsigned), C.stream));
+    if (st & ST_TMA_TIMEOUT)
+        return fail(SCALE_HEVI_ERR_CUDA, "a bulk tensor copy of the tiled stage did not complete within its wait limit");
+    if (st & ST_BARRIER_TIMEOUT)
+        return fail(SCALE_HEVI_ERR_CUDA, "a grid barrier of the persistent short step did not complete within its wait limit");
     if (st & ST_NONFINITE) return fail(SCALE_HEVI_ERR_NONFINITE, "a prognostic output became NaN or Inf");
     if (st & (1u << 4)) return fail(SCALE_HEVI_ERR_CUDA, "an adjoint pass loaded more inputs than its derivative slots");
     return SCALE_HEVI_OK;
@@ -1241,6 +1252,106 @@ int ATMOS_DYN_numfilter_coef_b200_mixed_dev(SCALE_HEVI_NUMFILTER_MIXED_ARGS)
     if (!*ND_USE_RS) return fail(SCALE_HEVI_ERR_UNSUPPORTED, "ND_USE_RS=.false. is not supported");
     CK(prepare_nd(CDZ, CDX, CDY, FDZ, FDX, FDY, *DT, *ND_COEF, *ND_ORDER, *ND_SFC_FACT));
     return run_numfilter(num_diff, DENS, MOMZ, MOMX, MOMY, RHOT, REF_dens, REF_pott);
+}
+
+// ---- the persistent short step ------------------------------------------------
+// numerical filter + RK4 HEVI + vertical boundary values + halo as one
+// cooperative launch over all members (persist.cu)
+extern "C++" {
+template <typename R>
+int short_step_persistent(double *X[5], R *mflx, R *tflx, R *num_diff, const R *const tend[5],
+                          const double *DPRES0, const double *RT2P, const double *CORIOLI, const double *wdamp_coef,
+                          const double *CDZ, const double *CDX, const double *CDY, const double *FDZ,
+                          const double *FDX, const double *FDY, const double *RCDZ, const double *RCDX,
+                          const double *RCDY, const double *RFDZ, const double *RFDX, const double *RFDY,
+                          const double *REF_dens, const double *REF_pott, const double *REF_rhot, double nd_coef,
+                          double sfc, double dt)
+{
+    CK(need_setup());
+    if (C.short_type != 0 || C.tinteg_type != 0)
+        return fail(SCALE_HEVI_ERR_UNSUPPORTED, "the persistent short step runs RK4 of HEVI stages only");
+    if (C.halo_fn) return fail(SCALE_HEVI_ERR_UNSUPPORTED, "the persistent short step does not take a halo exchange hook");
+    CK(prepare_nd(CDZ, CDX, CDY, FDZ, FDX, FDY, dt, nd_coef, 1, sfc));
+    CK(prepare_tables(CDZ, FDZ, RCDZ, RFDZ, FDX, RCDX, RFDX, FDY, RCDY, RFDY, wdamp_coef, nullptr, nullptr));
+    R *phi;
+    if constexpr (sizeof(R) == sizeof(double)) {
+        if (!C.phi) CK(dalloc(&C.phi, 5 * C.N3));
+        phi = C.phi;
+    } else {
+        if (!C.phi_f) CK(falloc(&C.phi_f, 5 * C.N3));
+        if (!C.facc_f) CK(falloc(&C.facc_f, 6 * C.N3));
+        if (!C.colscr_f) CK(falloc(&C.colscr_f, 4 * C.N3));
+        phi = C.phi_f;
+    }
+    if (!C.pbar && cudaMalloc((void **)&C.pbar, PERSIST_WORDS * sizeof(unsigned)) != cudaSuccess) {
+        C.pbar = nullptr;
+        cudaGetLastError();
+        return fail(SCALE_HEVI_ERR_ALLOC, "cudaMalloc of the persistent step's counters failed");
+    }
+    PersistStepT<R> p{};
+    p.ndc = C.ndc;
+    p.nd = NdArgsT<R>{num_diff, X[0], X[1], X[2], X[3], X[4], REF_dens, REF_pott, phi};
+    StageInT<R> in{X[0], X[1], X[2], X[3], X[4], nullptr, nullptr, nullptr, nullptr, nullptr,
+                   tend[0], tend[1], tend[2], tend[3], tend[4], DPRES0, RT2P, CORIOLI, num_diff, nullptr, REF_dens,
+                   REF_rhot, 0.0, 1.0};
+    const double dts[4] = {dt / 2.0, dt / 2.0, dt, dt};
+    const double *src[5] = {X[0], X[1], X[2], X[3], X[4]};
+    for (int s = 0; s < 4; ++s) {
+        in.DENS = src[0]; in.MOMZ = src[1]; in.MOMX = src[2]; in.MOMY = src[3]; in.RHOT = src[4];
+        double *out[5];
+        for (int v = 0; v < 5; ++v) out[v] = s < 3 ? C.rk[s % 2] + (size_t)v * C.N3 : X[v];
+        p.st[s] = stage_args(in, out, mflx, tflx, dts[s], RK_STAGE1 + s);
+        if (s < 3)
+            for (int v = 0; v < 5; ++v) { p.rk[s][v] = out[v]; src[v] = out[v]; }
+    }
+    for (int v = 0; v < 5; ++v) p.X[v] = X[v];
+    p.bar = C.pbar;
+    p.status = C.status;
+    p.raster = C.shape[sizeof(R) == sizeof(double) ? 0 : 1].raster;
+    p.wait_s = C.pwait_s;
+    p.extra = C.pextra;
+    CK(timed(sizeof(R) == sizeof(double) ? "short_step_persistent" : "short_step_persistent_mixed", [&] {
+        CU(launch_short_step_persistent(C.g, mem(), p, C.scheme, C.stream, &C.pgrid));
+        return SCALE_HEVI_OK;
+    }));
+    ++C.launches;
+    return SCALE_HEVI_OK;
+}
+} // extern "C++"
+
+#define SCALE_HEVI_SHORT_STEP_CALL                                                                              \
+    DPRES0, RT2P, CORIOLI, wdamp_coef, CDZ, CDX, CDY, FDZ, FDX, FDY, RCDZ, RCDX, RCDY, RFDZ, RFDX, RFDY,       \
+        REF_dens, REF_pott, REF_rhot, *ND_COEF, *ND_SFC_FACT, *dt
+
+int scale_hevi_short_step_persistent_dev(SCALE_HEVI_SHORT_STEP_ARGS)
+{
+    double *X[5] = {DENS, MOMZ, MOMX, MOMY, RHOT};
+    const double *tend[5] = {DENS_t, MOMZ_t, MOMX_t, MOMY_t, RHOT_t};
+    return short_step_persistent<double>(X, mflx_hi, tflx_hi, num_diff, tend, SCALE_HEVI_SHORT_STEP_CALL);
+}
+
+int scale_hevi_short_step_persistent_mixed_dev(SCALE_HEVI_SHORT_STEP_MIXED_ARGS)
+{
+    double *X[5] = {DENS, MOMZ, MOMX, MOMY, RHOT};
+    const float *tend[5] = {DENS_t, MOMZ_t, MOMX_t, MOMY_t, RHOT_t};
+    return short_step_persistent<float>(X, mflx_hi, tflx_hi, num_diff, tend, SCALE_HEVI_SHORT_STEP_CALL);
+}
+
+int scale_hevi_persistent_wait(const double *seconds, const int *extra_arrivals)
+{
+    CK(need_setup());
+    if (!(*seconds > 0.0) || *seconds > 60.0) return fail(SCALE_HEVI_ERR_ARG, "the wait limit must lie in (0, 60] s");
+    if (*extra_arrivals < 0 || *extra_arrivals > 1) return fail(SCALE_HEVI_ERR_ARG, "extra_arrivals must be 0 or 1");
+    C.pwait_s = *seconds;
+    C.pextra = (unsigned)*extra_arrivals;
+    return SCALE_HEVI_OK;
+}
+
+int scale_hevi_persistent_grid(int *ctas)
+{
+    CK(need_setup());
+    *ctas = C.pgrid;
+    return SCALE_HEVI_OK;
 }
 
 // ---- numerical filter --------------------------------------------------------

@@ -92,18 +92,18 @@ __host__ __device__ __forceinline__ Grid member_grid(const Grid &t, const Member
     return g;
 }
 
-// This block's domain and its block index b within that domain.
+// The domain of block x of a launch over all members, and its block index b
+// within that domain.
 template <int NM>
-__device__ __forceinline__ Grid block_domain(const Grid &t, const BatchT<NM> &B, int &b)
+__device__ __forceinline__ Grid block_domain(const Grid &t, const BatchT<NM> &B, int &b, int x)
 {
     if constexpr (NM == 1) {
         // a single domain has zero offsets; stating them lets them fold away
-        b = blockIdx.x;
+        b = x;
         Grid g = t;
         g.cell0 = 0; g.c2 = 0; g.z0 = 0; g.x0 = 0; g.y0 = 0;
         return g;
     } else {
-        const int x = blockIdx.x;
         int lo = 0;
 #pragma unroll
         for (int step = NM / 2; step > 0; step >>= 1)
@@ -111,6 +111,12 @@ __device__ __forceinline__ Grid block_domain(const Grid &t, const BatchT<NM> &B,
         b = x - B.first[lo];
         return member_grid(t, B.m[lo]);
     }
+}
+// this block's domain (block blockIdx.x of the launch)
+template <int NM>
+__device__ __forceinline__ Grid block_domain(const Grid &t, const BatchT<NM> &B, int &b)
+{
+    return block_domain(t, B, b, (int)blockIdx.x);
 }
 
 constexpr double GRAV = 9.80665;      // scale_const.F90:46
@@ -257,13 +263,22 @@ __device__ __forceinline__ R zface(R vel, int m, int KS, int KE, const V &v)
 }
 
 // read-only load through the non-coherent cache
+#if HEVI_COHERENT_LOADS
+// ordinary global loads: the persistent short step reads fields that earlier
+// phases of the same launch wrote (after a grid barrier), which the read-only
+// path may not serve
+template <typename T>
+__device__ __forceinline__ T ld(const T *p) { return *p; }
+#else
 template <typename T>
 __device__ __forceinline__ T ld(const T *p) { return __ldg(p); }
+#endif
 
 // device status word bits, read by the host after each call
 enum StatusBits : unsigned {
     ST_NONFINITE = 1u << 0,   // a prognostic output is NaN/Inf
     ST_TMA_TIMEOUT = 1u << 1, // a bulk tensor copy did not complete within its wait limit
+    ST_BARRIER_TIMEOUT = 1u << 2, // a grid barrier of the persistent short step did not complete within its wait limit
 };
 
 }  // namespace hevi

@@ -184,4 +184,27 @@ void mflx_average(const Grid &g, double *mflx, const double *av, int nstep, cuda
 // message returned by scale_hevi_last_error() (capi.cu)
 void set_last_error(const char *msg);
 
+// ---- the persistent short step (persist.cu) ----
+// One short step of every member as one cooperative launch: the numerical
+// filter (ND_ORDER = 1), the four RK4 HEVI stages with the halo of stages 1-3,
+// the vertical boundary values and the halo of the state. Flat terrain, no
+// divergence damping, the fused stage's default tile width.
+template <typename R>
+struct PersistStepT {
+    NdCoef ndc;
+    NdArgsT<R> nd;
+    StageArgsT<R> st[4];
+    double *rk[3][5];  // outputs of stages 1-3 (the inputs of stages 2-4)
+    double *X[5];      // the state, written by stage 4
+    unsigned *bar;     // PERSIST_WORDS device words: the grid barriers' arrival count, then per-phase work counters
+    unsigned *status;
+    int raster;        // rows of tiles per raster group of the stage phases
+    double wait_s;     // time limit of each grid barrier
+    unsigned extra;    // arrivals each barrier waits for beyond the grid's own (0; a test of the limit sets 1)
+};
+constexpr int PERSIST_WORDS = 64;
+template <typename R>
+cudaError_t launch_short_step_persistent(const Grid &g, const Members &mem, const PersistStepT<R> &p, int scheme,
+                                         cudaStream_t st, int *grid);
+
 }  // namespace hevi

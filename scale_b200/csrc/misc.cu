@@ -1,55 +1,26 @@
 // Halo fill, vertical boundary fill, large-step preparation, metric check and
 // budget reduction kernels.
-#include "hevi_kernels.cuh"
+#include "fill_body.cuh"
 
 namespace hevi {
-
-// ---- periodic halo fill: COMM_vars8 + COMM_wait on a single periodic rank ----
-// (scalelib/src/communication/scale_comm_cartesC.F90:345-397, 1600-2043). Every
-// halo column takes all KA levels of its periodic image; corners included.
-template <typename T>
-struct FieldList {
-    T *f[16];
-};
 
 template <typename T, int NM>
 __global__ void k_halo(const Grid gt, const FieldList<T> fl, const BatchT<NM> B)
 {
-    int b;
-    const Grid g = block_domain(gt, B, b);
-    const int nA = 2 * g.JHALO * g.IA;      // halo rows j < JS and j > JE, all i
-    const int nB = 2 * g.IHALO * g.JMAX;    // halo columns i < IS and i > IE, interior j
-    const int h = b * blockDim.y + threadIdx.y;
-    if (h >= nA + nB) return;
-    int i, j;
-    if (h < nA) {
-        const int r = h / g.IA;
-        i = 1 + h % g.IA;
-        j = r < g.JHALO ? 1 + r : g.JE + 1 + (r - g.JHALO);
-    } else {
-        const int q = h - nA;
-        const int r = q / g.JMAX;
-        j = g.JS + q % g.JMAX;
-        i = r < g.IHALO ? 1 + r : g.IE + 1 + (r - g.IHALO);
-    }
-    const int si = i < g.IS ? i + g.IMAX : (i > g.IE ? i - g.IMAX : i);
-    const int sj = j < g.JS ? j + g.JMAX : (j > g.JE ? j - g.JMAX : j);
-    T *v = fl.f[blockIdx.y];
-    const size_t dst = idx3(g, 1, i, j), src = idx3(g, 1, si, sj);
-    for (int k = threadIdx.x; k < g.KA; k += 32) v[dst + k] = v[src + k];
+    halo_column(gt, fl.f[blockIdx.y], B, (int)blockIdx.x, (int)threadIdx.y, (int)threadIdx.x);
 }
 
 template <typename T>
 void periodic_halo(const Grid &g, const Members &mem, T *const *fields, int nf, cudaStream_t st)
 {
-    auto nblocks = [](const Grid &m) { return (2 * m.JHALO * m.IA + 2 * m.IHALO * m.JMAX + 3) / 4; };
+    auto nblocks = [](const Grid &m) { return halo_blocks(m); };
     for (int base = 0; base < nf; base += 16) {
         FieldList<T> fl;
         const int n = (nf - base) < 16 ? (nf - base) : 16;
         for (int q = 0; q < n; ++q) fl.f[q] = fields[base + q];
         with_batch(g, mem, nblocks, [&](const auto &B, int nb) {
             constexpr int NM = std::decay_t<decltype(B)>::NMAX;
-            k_halo<T, NM><<<dim3(nb, n), dim3(32, 4), 0, st>>>(g, fl, B);
+            k_halo<T, NM><<<dim3(nb, n), dim3(32, FILL_WARPS), 0, st>>>(g, fl, B);
             return cudaSuccess;
         });
     }
@@ -57,36 +28,20 @@ void periodic_halo(const Grid &g, const Members &mem, T *const *fields, int nf, 
 template void periodic_halo<double>(const Grid &, const Members &, double *const *, int, cudaStream_t);
 template void periodic_halo<float>(const Grid &, const Members &, float *const *, int, cudaStream_t);
 
-// ---- vertical boundary values after a short step (scale_atmos_dyn_tstep_large_fvm_heve.F90:910-926) ----
 template <int NM>
 __global__ void k_vbc(const Grid gt, double *DENS, double *MOMZ, double *MOMX, double *MOMY, double *RHOT,
                       const BatchT<NM> B)
 {
-    int b;
-    const Grid g = block_domain(gt, B, b);
-    const Block2 p = split_block(b, (g.IMAX + 3) / 4);
-    const int i = g.IS + p.x * blockDim.y + threadIdx.y;
-    const int j = g.JS + p.y;
-    if (i > g.IE) return;
-    const size_t c = idx3(g, 1, i, j);
-    const int k = 1 + threadIdx.x;
-    if (k <= g.KS - 1) {
-        const size_t s = c + g.KS - 1, d = c + k - 1;
-        DENS[d] = DENS[s]; MOMZ[d] = 0.0; MOMX[d] = MOMX[s]; MOMY[d] = MOMY[s]; RHOT[d] = RHOT[s];
-    } else if (k <= g.KS - 1 + (g.KA - g.KE)) {
-        const int kk = g.KE + (k - (g.KS - 1));
-        const size_t s = c + g.KE - 1, d = c + kk - 1;
-        DENS[d] = DENS[s]; MOMZ[d] = 0.0; MOMX[d] = MOMX[s]; MOMY[d] = MOMY[s]; RHOT[d] = RHOT[s];
-    }
+    vbc_column(gt, DENS, MOMZ, MOMX, MOMY, RHOT, B, (int)blockIdx.x, (int)threadIdx.y, (int)threadIdx.x);
 }
 
 void vertical_bc(const Grid &g, const Members &mem, double *DENS, double *MOMZ, double *MOMX, double *MOMY, double *RHOT,
                  cudaStream_t st)
 {
-    auto nblocks = [](const Grid &m) { return ((m.IMAX + 3) / 4) * m.JMAX; };
+    auto nblocks = [](const Grid &m) { return vbc_blocks(m); };
     with_batch(g, mem, nblocks, [&](const auto &B, int nb) {
         constexpr int NM = std::decay_t<decltype(B)>::NMAX;
-        k_vbc<NM><<<nb, dim3(32, 4), 0, st>>>(g, DENS, MOMZ, MOMX, MOMY, RHOT, B);
+        k_vbc<NM><<<nb, dim3(32, FILL_WARPS), 0, st>>>(g, DENS, MOMZ, MOMX, MOMY, RHOT, B);
         return cudaSuccess;
     });
 }

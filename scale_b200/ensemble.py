@@ -4,7 +4,10 @@ The members (domains of different sizes, each with its own initial state) live
 in pooled device arrays, and one library state advances all of them: every
 kernel of the short step (numerical filter, the four RK4 stages, halo and
 boundary fills) covers all members in a single launch, and the short-step
-sequence can be recorded once as a CUDA graph and replayed. This has no
+sequence can be recorded once as a CUDA graph and replayed. With
+persistent=True the whole short step is ONE cooperative launch
+(scale_hevi_short_step_persistent_dev) whose CTAs take the blocks of each
+phase in turn and meet at bounded grid barriers between the phases. This has no
 counterpart in the reference, where each member is a separate run of
 scale-rm; per member the arithmetic is that of the single-domain short step
 (scale_atmos_dyn_tinteg_short_rk4.F90, scale_atmos_dyn_tstep_short_fvm_hevi.F90),
@@ -30,14 +33,14 @@ class Ensemble:
     """Members given as mkinit.Case objects (same time step, filter coefficient
     and flux schemes), resident on cuda:0 from construction to close()."""
 
-    def __init__(self, cases: list, mixed: bool = False, device: int = 0):
+    def __init__(self, cases: list, mixed: bool = False, device: int = 0, persistent: bool = False):
         import torch
 
         c0 = cases[0]
         for c in cases:
             if (c.dt, c.nd_coef, c.scheme, c.scheme_tracer) != (c0.dt, c0.nd_coef, c0.scheme, c0.scheme_tracer):
                 raise ValueError(f"{c.name}: members must share dt, ND_COEF and the flux schemes")
-        self.cases, self.mixed = cases, mixed
+        self.cases, self.mixed, self.persistent = cases, mixed, persistent
         self.dt, self.nd_coef = c0.dt, c0.nd_coef
         self.shapes = [c.g.shape for c in cases]
         self.layout = L = hevi.ensemble_setup([c.g.index_dict() for c in cases], c0.scheme, c0.scheme_tracer, device)
@@ -76,6 +79,14 @@ class Ensemble:
     # ---- one short step: numerical filter, RK4, boundary values and halos ----
     def step(self) -> None:
         gr = self.grid
+        if self.persistent:
+            # the whole step as one persistent launch over all members
+            fn = hevi.short_step_persistent_mixed_dev if self.mixed else hevi.short_step_persistent_dev
+            fn(mflx_hi=self.mflx, tflx_hi=self.tflx, num_diff=self.num_diff, DPRES0=self.DPRES0, RT2P=self.RT2P,
+               CORIOLI=self.CORIOLI, wdamp_coef=self.wdamp, REF_dens=self.ref["REF_dens"],
+               REF_pott=self.ref["REF_pott"], REF_rhot=self.REF_rhot, ND_COEF=self.nd_coef, ND_SFC_FACT=1.0,
+               dt=self.dt, **self.X, **self.tend, **gr)
+            return
         nf = hevi.ATMOS_DYN_numfilter_coef_mixed_dev if self.mixed else hevi.ATMOS_DYN_numfilter_coef_dev
         rk = hevi.ATMOS_DYN_Tinteg_short_rk4_mixed_dev if self.mixed else hevi.ATMOS_DYN_Tinteg_short_rk4_dev
         nf(num_diff=self.num_diff, CDZ=gr["CDZ"], CDX=gr["CDX"], CDY=gr["CDY"], FDZ=gr["FDZ"], FDX=gr["FDX"],

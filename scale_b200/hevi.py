@@ -148,7 +148,7 @@ class _Args:
 
 
 INT_ARGS = {"FLAG_FCT_MOMENTUM", "FLAG_FCT_T", "FLAG_FCT_ALONG_STREAM", "FLAG_FCT_TRACER", "BND_W", "BND_E",
-            "BND_S", "BND_N", "last", "ND_ORDER", "ND_USE_RS", "QA", "nfields", "n"}
+            "BND_S", "BND_N", "last", "ND_ORDER", "ND_USE_RS", "QA", "nfields", "n", "extra_arrivals"}
 # arguments passed as they are (an address, a C string or a stream handle), not by reference
 RAW_ARGS = {"idx", "flux_type", "stream"}
 
@@ -397,6 +397,29 @@ def ATMOS_DYN_Tinteg_short_rk3_dev(**kw):
 
 def ATMOS_DYN_numfilter_coef_dev(**kw):
     call("ATMOS_DYN_numfilter_coef_b200_dev", **kw)
+
+
+def short_step_persistent_dev(**kw):
+    """Numerical filter + RK4 HEVI + boundary values and halo of every member
+    as one persistent launch (scale_hevi_short_step_persistent_dev)."""
+    call("scale_hevi_short_step_persistent_dev", **kw)
+
+
+def short_step_persistent_mixed_dev(**kw):
+    call("scale_hevi_short_step_persistent_mixed_dev", **kw)
+
+
+def persistent_wait(seconds: float, extra_arrivals: int = 0) -> None:
+    """Time limit of the persistent step's grid barriers; extra_arrivals = 1
+    makes them wait for a CTA that does not exist (a test of the limit)."""
+    call("scale_hevi_persistent_wait", seconds=seconds, extra_arrivals=extra_arrivals)
+
+
+def persistent_grid() -> int:
+    """CTAs of the last persistent launch."""
+    n = C.c_int(0)
+    _check(load().scale_hevi_persistent_grid(C.byref(n)))
+    return n.value
 
 
 def ATMOS_DYN_Tstep_tracer_fvm_heve_dev(**kw):

@@ -1,9 +1,11 @@
 """Uneven ensembles: members of different sizes advanced together (every
-kernel launch covers all members) give, member by member, the same state bit
-for bit as each member advanced alone by the single-domain path, which the
-parity tests compare with the oracle. Also across the stage kernel's tile
-shapes, with the step replayed as a CUDA graph, and on the mixed-precision
-path."""
+kernel launch covers all members, or the whole short step is one persistent
+launch) give, member by member, the same state bit for bit as each member
+advanced alone by the single-domain path, which the parity tests compare with
+the oracle. Also across the stage kernel's tile shapes, with the step replayed
+as a CUDA graph, and on the mixed-precision path. The persistent step's grid
+barriers are bounded: a barrier made to wait for a CTA that does not exist
+ends the launch with an error status, and the library stays usable."""
 import numpy as np
 import pytest
 
@@ -29,8 +31,8 @@ def _alone(cases, nsteps, mixed=False, tile_x=0):
     return out
 
 
-def _together(cases, nsteps, mixed=False, tile_x=0, raster=0, graph=False):
-    e = Ensemble(cases, mixed=mixed)
+def _together(cases, nsteps, mixed=False, tile_x=0, raster=0, graph=False, persistent=False):
+    e = Ensemble(cases, mixed=mixed, persistent=persistent)
     try:
         hevi.stage_shape(tile_x, raster)
         if graph:
@@ -134,3 +136,69 @@ def test_six_point_ensemble_matches_members_alone(scheme):
     cases = mkinit.ensemble(sizes=SIZES[:3], scheme=scheme)
     assert all(c.g.IS == 4 for c in cases)
     _same(_together(cases, 4)[0], _alone(cases, 4))
+
+
+# ---- the whole short step as one persistent launch ----
+def test_persistent_step_matches_members_alone(cases, alone):
+    got, launches = _together(cases, NSTEPS, persistent=True)
+    _same(got, alone)
+    assert launches == NSTEPS  # one launch per short step
+
+
+def test_persistent_step_graph_replay(cases, alone):
+    got, _ = _together(cases, NSTEPS, graph=True, persistent=True)
+    _same(got, alone)
+
+
+def test_persistent_step_single_domain(cases, alone):
+    got, launches = _together(cases[1:2], NSTEPS, persistent=True)
+    _same(got, alone[1:2])
+    assert launches == NSTEPS
+
+
+@pytest.mark.parametrize("scheme", ["UD5", "CD6"])
+def test_persistent_six_point(scheme):
+    cases = mkinit.ensemble(sizes=SIZES[:3], scheme=scheme)
+    _same(_together(cases, 4, persistent=True)[0], _alone(cases, 4))
+
+
+def test_persistent_mixed_matches_members_alone(cases):
+    got = _together(cases, 4, mixed=True, persistent=True)[0]
+    want = _alone(cases, 4, mixed=True, tile_x=16)
+    for m, (x, y) in enumerate(zip(got, want)):
+        for n in STATE:
+            scale = np.max(np.abs(y[n]))
+            err = np.max(np.abs(x[n] - y[n])) / scale if scale else np.max(np.abs(x[n]))
+            # the same FP32 kernels' code; FMA contraction may differ between the two compiled forms
+            assert err <= 1e-6, f"member {m} {n}: {err:.3e}"
+
+
+def test_persistent_barrier_wait_is_bounded(cases):
+    # every barrier waits for one CTA more than the grid has: the first one
+    # expires after 50 ms, the launch ends and the status reports it
+    e = Ensemble(cases[:2], persistent=True)
+    try:
+        e.run(1)
+        hevi.check()
+        assert hevi.persistent_grid() > 0
+        hevi.persistent_wait(0.05, extra_arrivals=1)
+        e.run(1)
+        with pytest.raises(hevi.HeviError, match="grid barrier") as err:
+            hevi.check()
+        assert err.value.code == 3
+        # the limit back to its default and no extra arrival: the next step completes
+        hevi.persistent_wait(2.0, extra_arrivals=0)
+        e.run(1)
+        hevi.check()
+    finally:
+        e.close()
+
+
+def test_persistent_step_refuses_other_integrators(cases):
+    e = Ensemble(cases[:2], persistent=True)
+    try:
+        hevi.tinteg_short_type("RK3")
+        with pytest.raises(hevi.HeviError, match="RK4 of HEVI"):
+            e.run(1)
+    finally:
+        e.close()
