@@ -194,14 +194,15 @@ int ATMOS_DYN_Tinteg_short_rk3_b200_dev(SCALE_HEVI_TINTEG_SHORT_ARGS);
  * periodic self-exchange of COMM_vars8/COMM_wait
  * (scale_comm_cartesC.F90:1600-2043, 2787-3023) that the library does on one
  * rank. When fn is set, every lateral halo fill of the short step and the
- * large step (the RK stage buffers, the state, num_diff, mflx_hi and the
- * tracers) calls fn instead: fn receives the device addresses of nfields
- * (KA,IA,JA) fields with elements of elem_bytes (8 or 4) and must have filled
- * their lateral halos (IHALO columns, JHALO rows, corners included) when it
- * returns 0 (a nonzero return is reported as an error). The library's stream is idle during the call.
- * NULL restores the periodic fill. One domain only; the filter at ND_ORDER > 1
- * and the FCT tracer limiter, whose inner halo fills are not routed through
- * the hook, return SCALE_HEVI_ERR_UNSUPPORTED while it is set.
+ * large step (the RK stage buffers, the state, num_diff, mflx_hi, the
+ * tracers and their RK stages, the FCT limiter's R+/R-
+ * (scale_atmos_dyn_common.F90:2558-2561) and the work arrays of the filter at
+ * ND_ORDER > 1 (:1557-1563)) calls fn instead: fn receives the device
+ * addresses of nfields (KA,IA,JA) fields with elements of elem_bytes (8 or 4)
+ * and must have filled their lateral halos (IHALO columns, JHALO rows,
+ * corners included) when it returns 0 (a nonzero return is reported as an
+ * error). The library's stream is idle during the call. NULL restores the
+ * periodic fill. One domain only; the persistent short step does not take it.
  * ------------------------------------------------------------------------- */
 typedef int (*scale_hevi_halo_fn)(void *const *fields, int nfields, int elem_bytes, void *user);
 int scale_hevi_set_halo_exchange(scale_hevi_halo_fn fn, void *user);

@@ -69,6 +69,8 @@ def load() -> C.CDLL:
         f = getattr(lib, name)
         f.argtypes = [kinds[k] for k in sig.split()]
         f.restype = _RESTYPE.get(name, C.c_int)
+    lib.og_set_halo_exchange.argtypes = [HALO_FN, C.c_void_p]
+    lib.og_set_halo_exchange.restype = None
     _lib = lib
     return lib
 
@@ -165,6 +167,33 @@ def tinteg_short_rk3(g, scheme, x, a, ws2002=True, short="HEVI"):
 
 def halo(g, var, nfields=1):
     _call("og_halo_periodic", g, var, int(nfields))
+
+
+# int (*)(double *var, int nfields, void *user)
+HALO_FN = C.CFUNCTYPE(C.c_int, C.POINTER(C.c_double), C.c_int, C.c_void_p)
+_halo_cb = None  # the registered callback, kept alive while set
+
+
+def set_halo_exchange(g, fn) -> None:
+    """While fn is set, every halo fill of the oracle calls fn(fields) with
+    fields a list of the nfields (KA,IA,JA) arrays (1-D float64 views of the
+    oracle's memory, in the grid g's Fortran order), to be filled in place;
+    None restores the periodic fill (og_set_halo_exchange)."""
+    global _halo_cb
+    lib = load()
+    if fn is None:
+        lib.og_set_halo_exchange(HALO_FN(), None)
+        _halo_cb = None
+        return
+    n3 = g.KA * g.IA * g.JA
+
+    def tramp(var, nfields, user):
+        flat = np.ctypeslib.as_array(var, shape=(nfields * n3,))
+        fn([flat[q * n3:(q + 1) * n3] for q in range(nfields)])
+        return 0
+
+    _halo_cb = HALO_FN(tramp)
+    lib.og_set_halo_exchange(_halo_cb, None)
 
 
 def numfilter(g, num_diff, st, ref, DT, ND_COEF=1e-4, ND_ORDER=1, ND_SFC_FACT=1.0, ND_USE_RS=1):

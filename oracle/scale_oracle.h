@@ -142,6 +142,11 @@ void og_tinteg_short_type(int type);
 
 /* ---- periodic 8-neighbour halo fill, scale_comm_cartesC.F90 (COMM_vars8 on a periodic 1x1 grid) ---- */
 void og_halo_periodic(const og_dims *d, double *var, int nfields);
+/* ---- a decomposed domain (the tests' ranks): while fn is set, every halo fill of the
+ *      oracle, og_halo_periodic included, calls fn(var, nfields, user) instead, with
+ *      nfields consecutive (KA,IA,JA) arrays at var; NULL restores the periodic fill ---- */
+typedef int (*og_halo_fn)(double *var, int nfields, void *user);
+void og_set_halo_exchange(og_halo_fn fn, void *user);
 
 /* ---- numerical filter: scale_atmos_dyn_common.F90:385-985 (ND_ORDER=1 path) + filter_setup :100-330 ---- */
 int og_numfilter_coef(

@@ -469,6 +469,17 @@ int halo(T *const *f, int n)
     });
 }
 
+// the halo fill that launch_tracer_stage and launch_numfilter_high call between
+// their kernels while a halo exchange hook is set; ctx: the int that receives
+// halo()'s status
+static int hook_fill(void *ctx, void *const *f, int n, int elem)
+{
+    const int rc = elem == (int)sizeof(double) ? halo(reinterpret_cast<double *const *>(f), n)
+                                               : halo(reinterpret_cast<float *const *>(f), n);
+    *static_cast<int *>(ctx) = rc;
+    return rc;
+}
+
 // ---- one stage ---------------------------------------------------------------
 // F: type of the flux-like arrays (double: plain path, float: mixed precision)
 template <typename F>
@@ -702,14 +713,16 @@ int run_numfilter(R *num_diff, const double *DENS, const double *MOMZ, const dou
         if (sizeof(R) != sizeof(double))
             return fail(SCALE_HEVI_ERR_UNSUPPORTED, "ND_ORDER > 1 is supported on the FP64 path only");
         if (C.members.size() > 1) return fail(SCALE_HEVI_ERR_UNSUPPORTED, "ND_ORDER > 1 is not available for an ensemble");
-        if (C.halo_fn) return fail(SCALE_HEVI_ERR_UNSUPPORTED, "ND_ORDER > 1 is not available with a halo exchange hook");
         if (!C.ndw) CK(dalloc(&C.ndw, 30 * C.N3));
         NdArgs ah{reinterpret_cast<double *>(num_diff), DENS, MOMZ, MOMX, MOMY, RHOT, REF_dens, REF_pott,
                   reinterpret_cast<double *>(phi)};
-        CK(timed("numfilter", [&] {
-            CU(launch_numfilter_high(C.g, C.ndc, ah, C.ndw, C.ndw + 15 * C.N3, C.stream));
-            return SCALE_HEVI_OK;
-        }));
+        // a decomposed domain exchanges the work arrays through the hook
+        int hrc = SCALE_HEVI_OK;
+        const HaloFill hf{hook_fill, &hrc};
+        const cudaError_t e = launch_numfilter_high(C.g, C.ndc, ah, C.ndw, C.ndw + 15 * C.N3, C.stream,
+                                                    C.halo_fn ? &hf : nullptr);
+        if (hrc != SCALE_HEVI_OK) return hrc;
+        CU(e);
         C.launches += 3 + 2 * (C.ndc.order - 1);
         R *f[15];
         for (int q = 0; q < 15; ++q) f[q] = num_diff + (size_t)q * C.N3;
@@ -756,8 +769,6 @@ template <typename R>
 int run_tracer_rk3(double *QTRC, const double *QTRC0, const R *RHOQ_t, const double *DENS0, const double *DENS,
                    const R *mflx, const R *ndq, double dtl, bool fct, bool along)
 {
-    if (fct && C.halo_fn)
-        return fail(SCALE_HEVI_ERR_UNSUPPORTED, "the FCT tracer limiter is not available with a halo exchange hook");
     TracerArgsT<R> a{};
     a.QTRC0 = QTRC0; a.RHOQ_t = RHOQ_t; a.DENS0 = DENS0; a.DENS = DENS; a.mflx = mflx; a.ndq = ndq;
     limiter_scratch(a);
@@ -780,7 +791,16 @@ int run_tracer_rk3(double *QTRC, const double *QTRC0, const R *RHOQ_t, const dou
     CK(halo(&rk2, 1));
     // stage 3: dt with DENS, FCT when requested
     a.QTRCo = QTRC; a.QTRC = rk2; a.dens_mode = 0; a.dtl = dtl;
-    CK(timed(fct ? sec_fct : sec, [&] { CU(launch_tracer_stage(C.g, a, C.scheme_tracer, fct, C.stream)); return SCALE_HEVI_OK; }));
+    if (fct && C.halo_fn) {
+        // a decomposed domain: R+/R- go through the exchange between the limiter's kernels
+        int hrc = SCALE_HEVI_OK;
+        const HaloFill hf{hook_fill, &hrc};
+        const cudaError_t e = launch_tracer_stage(C.g, a, C.scheme_tracer, fct, C.stream, &hf);
+        if (hrc != SCALE_HEVI_OK) return hrc;
+        CU(e);
+    } else {
+        CK(timed(fct ? sec_fct : sec, [&] { CU(launch_tracer_stage(C.g, a, C.scheme_tracer, fct, C.stream)); return SCALE_HEVI_OK; }));
+    }
     C.launches += fct ? 4 : 1;
     return SCALE_HEVI_OK;
 }
@@ -1450,9 +1470,11 @@ int ATMOS_DYN_Tstep_tracer_fvm_heve_b200_dev(SCALE_HEVI_TSTEP_TRACER_ARGS)
     a.GS = dGS;
     a.MAPF = dMAPF;
     const bool fct = *FLAG_FCT_TRACER != 0;
-    if (fct && C.halo_fn)
-        return fail(SCALE_HEVI_ERR_UNSUPPORTED, "the FCT tracer limiter is not available with a halo exchange hook");
-    CU(launch_tracer_stage(C.g, a, C.scheme_tracer, fct, C.stream));
+    int hrc = SCALE_HEVI_OK;
+    const HaloFill hf{hook_fill, &hrc};
+    const cudaError_t e = launch_tracer_stage(C.g, a, C.scheme_tracer, fct, C.stream, C.halo_fn ? &hf : nullptr);
+    if (hrc != SCALE_HEVI_OK) return hrc;
+    CU(e);
     C.launches += fct ? 4 : 1;
     return SCALE_HEVI_OK;
 }

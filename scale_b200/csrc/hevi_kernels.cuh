@@ -7,6 +7,16 @@
 namespace hevi {
 
 // ---- ensemble members on the host ----
+// A lateral halo fill that the launchers below call between their own kernels
+// in place of the periodic fill: fn(ctx, fields, n, elem_bytes) fills n
+// (KA,IA,JA) fields of elem_bytes-sized values and returns 0, or a nonzero
+// status that makes the launcher return cudaErrorUnknown. Used for the
+// exchange of a decomposed domain; null: the periodic fill on the device.
+struct HaloFill {
+    int (*fn)(void *ctx, void *const *fields, int n, int elem_bytes);
+    void *ctx;
+};
+
 // The members that share the pooled arrays of one library state; a single
 // domain is one member with zero offsets (or no list at all). The launchers
 // below run every member in the same launch. A view: the caller owns the array.
@@ -90,7 +100,7 @@ cudaError_t launch_numfilter(const Grid &g, const Members &mem, const NdCoef &c,
 // 1 x, 2 y) and ND_ORDER-1 applications of calc_diff4 with the periodic halo
 // before each; num_diff is then formed from the last one
 cudaError_t launch_numfilter_high(const Grid &g, const NdCoef &c, const NdArgs &a, double *w1, double *w2,
-                                  cudaStream_t st);
+                                  cudaStream_t st, const HaloFill *fill = nullptr);
 // the member's coefficient tables in the pooled ones (per member: CN*3 hold
 // 6 values per level or point, the nd_coef_* vectors one)
 __host__ __device__ __forceinline__ NdCoef member_nd(const NdCoef &c, const Grid &g)
@@ -126,7 +136,8 @@ struct TracerArgsT {
 };
 using TracerArgs = TracerArgsT<double>;
 template <typename R>
-cudaError_t launch_tracer_stage(const Grid &g, const TracerArgsT<R> &a, int scheme, bool fct, cudaStream_t st);
+cudaError_t launch_tracer_stage(const Grid &g, const TracerArgsT<R> &a, int scheme, bool fct, cudaStream_t st,
+                                const HaloFill *fill = nullptr);
 // ATMOS_DYN_divergence with every metric term (misc.cu)
 void divergence_terrain(const Grid &g, double *DDIV, const double *MOMZ, const double *MOMX, const double *MOMY,
                         const Metrics &M, double J33G, cudaStream_t st);

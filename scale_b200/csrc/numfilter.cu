@@ -101,7 +101,7 @@ __global__ void __launch_bounds__(128) k_nd_diff4(const Grid g, const NdCoef c, 
 }
 
 cudaError_t launch_numfilter_high(const Grid &g, const NdCoef &c, const NdArgs &a, double *w1, double *w2,
-                                  cudaStream_t st)
+                                  cudaStream_t st, const HaloFill *fill)
 {
     dim3 b(32, 4), gr((g.IMAX + 3) / 4, g.JMAX);
     const int nphi = (int)(((long)g.KA * g.IA * g.JA + PHI_THREADS - 1) / PHI_THREADS);
@@ -112,7 +112,13 @@ cudaError_t launch_numfilter_high(const Grid &g, const NdCoef &c, const NdArgs &
     for (int no = 2; no <= c.order; ++no) {
         double *f[15];
         for (int q = 0; q < 15; ++q) f[q] = in + (size_t)q * n3(g);
-        periodic_halo(g, Members{}, f, 15, st); // COMM_vars8 of the work (:1557-1563)
+        if (fill) { // COMM_vars8 of the work (:1557-1563)
+            cudaError_t e = cudaGetLastError();
+            if (e != cudaSuccess) return e;
+            if (fill->fn(fill->ctx, reinterpret_cast<void *const *>(f), 15, (int)sizeof(double))) return cudaErrorUnknown;
+        } else {
+            periodic_halo(g, Members{}, f, 15, st);
+        }
         k_nd_diff4<<<gr, b, 0, st>>>(g, c, in, out);
         double *t = in;
         in = out;

@@ -326,7 +326,7 @@ __global__ void __launch_bounds__(128) k_fct_apply(const Grid g, const TracerArg
 }
 
 template <int S, typename R>
-static cudaError_t tracer_stage(const Grid &g, const TracerArgsT<R> &a, bool fct, cudaStream_t st)
+static cudaError_t tracer_stage(const Grid &g, const TracerArgsT<R> &a, bool fct, cudaStream_t st, const HaloFill *fill)
 {
     dim3 b(32, 4), gr((g.IMAX + 3) / 4, g.JMAX);
     if (!fct) {
@@ -337,28 +337,37 @@ static cudaError_t tracer_stage(const Grid &g, const TracerArgsT<R> &a, bool fct
     k_fct_lo<S, R><<<gl, b, 0, st>>>(g, a);
     k_fct_r<R><<<gr, b, 0, st>>>(g, a);
     R *rr[2] = {a.rjp, a.rjm};
-    periodic_halo(g, Members{}, rr, 2, st);
+    if (fill) {
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+        if (fill->fn(fill->ctx, reinterpret_cast<void *const *>(rr), 2, (int)sizeof(R))) return cudaErrorUnknown;
+    } else {
+        periodic_halo(g, Members{}, rr, 2, st);
+    }
     k_fct_apply<S, R><<<gr, b, 0, st>>>(g, a);
     return cudaGetLastError();
 }
 
 template <typename R>
-cudaError_t launch_tracer_stage(const Grid &g, const TracerArgsT<R> &a, int scheme, bool fct, cudaStream_t st)
+cudaError_t launch_tracer_stage(const Grid &g, const TracerArgsT<R> &a, int scheme, bool fct, cudaStream_t st,
+                                const HaloFill *fill)
 {
     switch (scheme) {
-    case UD3: return tracer_stage<UD3, R>(g, a, fct, st);
-    case CD4: return tracer_stage<CD4, R>(g, a, fct, st);
-    case KOREN: return tracer_stage<KOREN, R>(g, a, fct, st);
-    case CD2: return tracer_stage<CD2, R>(g, a, fct, st);
-    case UD5: return tracer_stage<UD5, R>(g, a, fct, st);
-    case CD6: return tracer_stage<CD6, R>(g, a, fct, st);
+    case UD3: return tracer_stage<UD3, R>(g, a, fct, st, fill);
+    case CD4: return tracer_stage<CD4, R>(g, a, fct, st, fill);
+    case KOREN: return tracer_stage<KOREN, R>(g, a, fct, st, fill);
+    case CD2: return tracer_stage<CD2, R>(g, a, fct, st, fill);
+    case UD5: return tracer_stage<UD5, R>(g, a, fct, st, fill);
+    case CD6: return tracer_stage<CD6, R>(g, a, fct, st, fill);
     default: return cudaErrorInvalidValue;
     }
 }
 #ifdef HEVI_FLOAT_TU
-template cudaError_t launch_tracer_stage<float>(const Grid &, const TracerArgsT<float> &, int, bool, cudaStream_t);
+template cudaError_t launch_tracer_stage<float>(const Grid &, const TracerArgsT<float> &, int, bool, cudaStream_t,
+                                                const HaloFill *);
 #else
-template cudaError_t launch_tracer_stage<double>(const Grid &, const TracerArgsT<double> &, int, bool, cudaStream_t);
+template cudaError_t launch_tracer_stage<double>(const Grid &, const TracerArgsT<double> &, int, bool, cudaStream_t,
+                                                 const HaloFill *);
 #endif
 
 }  // namespace hevi

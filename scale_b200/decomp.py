@@ -133,3 +133,39 @@ def attach(lib, dec: Decomposition, KA: int, group=None) -> None:
         torch.cuda.synchronize()
 
     lib.set_halo_exchange(exchange)
+
+
+def budget_sums(partials, group=None) -> list[float]:
+    """The domain totals of a decomposed domain's budgets: every rank gives its
+    subdomain's FP64 partial sums (scale_hevi_domain_sum_dev for the mass,
+    scale_hevi_energy_sum_dev for ENGT/ENGP/ENGK/ENGI, the reference's
+    MONITOR totals of scale_atmos_dyn.F90:530-688 and mod_atmos_vars.F90:768-777,
+    which reduce over ranks with MPI_ALLREDUCE). The partials are gathered and
+    added in rank order on every rank, so every rank holds the same bits
+    whatever the transport does (a reduction inside the transport may
+    associate the additions differently from one call to the next)."""
+    import torch.distributed as dist
+
+    v = torch.tensor([float(x) for x in partials], dtype=torch.float64)
+    if dist.get_backend(group) == "nccl":
+        v = v.cuda()
+    world = dist.get_world_size(group)
+    got = [torch.empty_like(v) for _ in range(world)]
+    dist.all_gather(got, v, group)
+    tot = [0.0] * len(partials)
+    for r in range(world):  # rank order
+        row = got[r].cpu().tolist()
+        for q in range(len(tot)):
+            tot[q] += row[q]
+    return tot
+
+
+def domain_budgets(lib, X, grid, group=None) -> dict[str, float]:
+    """Mass and energy totals of the decomposed domain from this rank's state X
+    (DENS, MOMZ, MOMX, MOMY, RHOT device arrays of its subdomain) and its grid
+    vectors (CZ, CDZ, CDX, CDY)."""
+    mass = lib.domain_sum_dev(X["DENS"], grid["CDZ"], grid["CDX"], grid["CDY"])
+    eng = lib.energy_sum_dev(**X, CZ=grid["CZ"], CDZ=grid["CDZ"], CDX=grid["CDX"], CDY=grid["CDY"])
+    names = ("ENGT", "ENGP", "ENGK", "ENGI")
+    tot = budget_sums([mass] + [eng[n] for n in names], group)
+    return {"mass": tot[0], **{n: tot[1 + q] for q, n in enumerate(names)}}

@@ -229,3 +229,159 @@ def test_decomposed_rk4_matches_global_run():
             p.join(300)
             assert p.exitcode == 0
         assert all(out[r] for r in range(world)), dict(out)
+
+
+# ---- exchanges inside the oracle's own call sequences: the FCT limiter's R+/R-
+# (scale_atmos_dyn_common.F90:2526-2561) and the filter's work arrays at
+# ND_ORDER > 1 (:1557-1563), through og_set_halo_exchange ----
+def _block(dec, g, v):
+    """This rank's block (halo included) of a global array: 3-D and more by its
+    lateral block, (IA,JA) 2-D arrays likewise."""
+    H = dec.halo
+    isl = slice(dec.i0, dec.i0 + dec.imax + 2 * H)
+    jsl = slice(dec.j0, dec.j0 + dec.jmax + 2 * H)
+    if v.ndim >= 3 and v.shape[:3] == g.shape:
+        return np.asfortranarray(v[:, isl, jsl])
+    return np.asfortranarray(v[isl, jsl])
+
+
+def _interior_equal(dec, g, glob, loc):
+    H = dec.halo
+    want = glob[:, dec.i0 + H: dec.i0 + H + dec.imax, dec.j0 + H: dec.j0 + H + dec.jmax]
+    return bool(np.array_equal(loc[:, H:-H, H:-H], want))
+
+
+def _inner_worker(rank, world, port, nx, ny, what, out):
+    import datetime
+
+    import torch.distributed as dist
+
+    sys.path.insert(0, str(ROOT / "tests"))
+    import helpers
+    import oracle
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=120))
+    try:
+        g = helpers.small_grid(IMAX=12, JMAX=10, KMAX=12, stretched=True)
+        c = helpers.small_case(g, "CD4")
+        helpers.perturb_state(c)
+        dec = Decomposition(g.IMAX, g.JMAX, nx, ny, rank, g.halo)
+        g_loc = helpers.small_grid(IMAX=dec.imax, JMAX=dec.jmax, KMAX=12, stretched=True)
+        exchange = lambda fields: dec.exchange([torch.from_numpy(f) for f in fields])  # noqa: E731
+        ok = True
+        if what == "fct":
+            from test_gpu_parity import _tracer_inputs
+
+            q0, q, d0, d, mflx, rhoq, GS, MAPF = _tracer_inputs(g, c)
+            ndq = np.asfortranarray(1e-6 * np.random.default_rng(9).normal(size=g.shape + (3,)))
+            for n in range(3):
+                oracle.halo(g, np.asfortranarray(ndq[..., n]))
+            for along in (True, False):
+                qg = q.copy(order="F")
+                oracle.tinteg_tracer_rk3(g, "UD3", qg, q0, rhoq, d0, d, mflx, ndq, GS, MAPF, 5.0, True, along)
+                ql = _block(dec, g, q)
+                oracle.set_halo_exchange(g_loc, exchange)
+                try:
+                    oracle.tinteg_tracer_rk3(g_loc, "UD3", ql, _block(dec, g, q0), _block(dec, g, rhoq),
+                                             _block(dec, g, d0), _block(dec, g, d), _block(dec, g, mflx),
+                                             _block(dec, g, ndq), _block(dec, g, GS), _block(dec, g, MAPF), 5.0,
+                                             True, along)
+                finally:
+                    oracle.set_halo_exchange(g_loc, None)
+                ok &= _interior_equal(dec, g, qg, ql)
+        else:  # the filter at ND_ORDER = 2 and 3
+            for order in (2, 3):
+                ndg = g.zeros(5, 3)
+                oracle.numfilter(g, ndg, c.state, c.ref, DT=0.5, ND_COEF=1e-3, ND_ORDER=order, ND_SFC_FACT=0.7)
+                ndl = g_loc.zeros(5, 3)
+                st = {n: _block(dec, g, v) for n, v in c.state.items()}
+                ref = {n: _block(dec, g, v) for n, v in c.ref.items() if isinstance(v, np.ndarray) and v.ndim >= 3}
+                oracle.set_halo_exchange(g_loc, exchange)
+                try:
+                    oracle.numfilter(g_loc, ndl, st, ref, DT=0.5, ND_COEF=1e-3, ND_ORDER=order, ND_SFC_FACT=0.7)
+                finally:
+                    oracle.set_halo_exchange(g_loc, None)
+                for v in range(5):
+                    for dd in range(3):
+                        ok &= _interior_equal(dec, g, ndg[..., v, dd], ndl[..., v, dd])
+        out[rank] = ok
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("what", ["fct", "nd_order"])
+def test_decomposed_limiter_and_filter_match_global_run(what):
+    """The tracer RK3 with the FCT limiter (its R+/R- exchanged between the
+    limiter's passes) and the numerical filter at ND_ORDER 2 and 3 (its work
+    arrays exchanged between the calc_diff4 applications), each rank running
+    the oracle on its subdomain of a 2x1 layout with every halo fill replaced
+    by the exchange, equal the global runs on every rank's interior, bit for
+    bit."""
+    world, nx, ny = 2, 2, 1
+    ctx = mp.get_context("spawn")
+    with ctx.Manager() as m:
+        out = m.dict()
+        port = _free_port()
+        procs = [ctx.Process(target=_inner_worker, args=(r, world, port, nx, ny, what, out)) for r in range(world)]
+        for p in procs:
+            p.start()
+        for p in procs:
+            p.join(300)
+            assert p.exitcode == 0
+        assert all(out[r] for r in range(world)), dict(out)
+
+
+def _budget_worker(rank, world, port, nx, ny, out):
+    import datetime
+
+    import torch.distributed as dist
+
+    sys.path.insert(0, str(ROOT / "tests"))
+    import helpers
+    import oracle
+    from scale_b200.decomp import budget_sums
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=120))
+    try:
+        g = helpers.small_grid(IMAX=12, JMAX=10, KMAX=12, stretched=True)
+        c = helpers.small_case(g, "CD4")
+        helpers.perturb_state(c)
+        dec = Decomposition(g.IMAX, g.JMAX, nx, ny, rank, g.halo)
+        g_loc = helpers.small_grid(IMAX=dec.imax, JMAX=dec.jmax, KMAX=12, stretched=True)
+        st = {n: _block(dec, g, v) for n, v in c.state.items()}
+        names = ("ENGT", "ENGP", "ENGK", "ENGI")
+        e_loc, e_glob = oracle.energy_sum(g_loc, st, g_loc.CZ), oracle.energy_sum(g, c.state, g.CZ)
+        tot = budget_sums([oracle.domain_sum(g_loc, st["DENS"])] + [e_loc[n] for n in names])
+        want = [oracle.domain_sum(g, c.state["DENS"])] + [e_glob[n] for n in names]
+        # every rank holds the same bits
+        allt = [None] * world
+        dist.all_gather_object(allt, tot)
+        out[rank] = {"same_on_ranks": all(t == tot for t in allt),
+                     "rel": max(abs(a - b) / abs(b) for a, b in zip(tot, want))}
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("nx,ny", [(2, 1), (2, 2)])
+def test_budget_sums_over_ranks(nx, ny):
+    """The FP64 mass and energy totals of a decomposed domain (each rank's
+    subdomain sum, gathered and added in rank order) are the same bits on
+    every rank and agree with the global domain's sums to rounding."""
+    world = nx * ny
+    ctx = mp.get_context("spawn")
+    with ctx.Manager() as m:
+        out = m.dict()
+        port = _free_port()
+        procs = [ctx.Process(target=_budget_worker, args=(r, world, port, nx, ny, out)) for r in range(world)]
+        for p in procs:
+            p.start()
+        for p in procs:
+            p.join(300)
+            assert p.exitcode == 0
+        for r in range(world):
+            assert out[r]["same_on_ranks"], dict(out)
+            assert out[r]["rel"] <= 1e-13, dict(out)

@@ -2,8 +2,9 @@
 the decomposition's exchange (scale_b200/decomp.py) on one GPU: a 1x1
 decomposition, whose exchange is the periodic fill done by torch copies, must
 give the results of the library's own periodic halo bit for bit, through the
-RK4 short step and the large step; the cases the hook does not route
-(FCT tracers, the higher-order filter) are refused."""
+RK4 short step, the large step, the FCT tracer limiter (R+/R- exchanged
+between its kernels) and the filter at ND_ORDER > 1 (its work arrays
+exchanged between the calc_diff4 applications)."""
 import numpy as np
 import pytest
 
@@ -85,18 +86,51 @@ def test_hook_large_step_matches_periodic_halo(lib):
         assert np.array_equal(res[0][n], res[1][n], equal_nan=True), n
 
 
-def test_hook_refuses_unrouted_halo_fills(lib):
-    g = helpers.small_grid()
+@pytest.mark.parametrize("order", [2, 3])
+def test_hook_high_order_filter_matches_periodic_halo(lib, order):
+    g = helpers.small_grid(IMAX=13, JMAX=11, KMAX=17, stretched=True)
     c = helpers.small_case(g)
-    lib.setup(g.index_dict(), "UD3", "UD3")
-    _attach(g)
-    with pytest.raises(hevi.HeviError, match="halo exchange hook") as e:
-        lib.ATMOS_DYN_numfilter_coef(num_diff=g.zeros(5, 3), DENS=c.state["DENS"], MOMZ=c.state["MOMZ"],
-                                     MOMX=c.state["MOMX"], MOMY=c.state["MOMY"], RHOT=c.state["RHOT"], CDZ=g.CDZ,
-                                     CDX=g.CDX, CDY=g.CDY, FDZ=g.FDZ, FDX=g.FDX, FDY=g.FDY, DT=0.5,
-                                     REF_dens=c.ref["REF_dens"], REF_pott=c.ref["REF_pott"], ND_COEF=1e-3,
-                                     ND_ORDER=2, ND_SFC_FACT=0.7, ND_USE_RS=True)
-    assert e.value.code == 5
+    helpers.perturb_state(c)
+    res = []
+    for hook in (False, True):
+        nd = np.full(g.shape + (5, 3), np.nan, order="F")
+        lib.setup(g.index_dict(), "UD3", "UD3")
+        if hook:
+            _attach(g)
+        lib.ATMOS_DYN_numfilter_coef(num_diff=nd, DENS=c.state["DENS"], MOMZ=c.state["MOMZ"], MOMX=c.state["MOMX"],
+                                     MOMY=c.state["MOMY"], RHOT=c.state["RHOT"], CDZ=g.CDZ, CDX=g.CDX, CDY=g.CDY,
+                                     FDZ=g.FDZ, FDX=g.FDX, FDY=g.FDY, DT=0.5, REF_dens=c.ref["REF_dens"],
+                                     REF_pott=c.ref["REF_pott"], ND_COEF=1e-3, ND_ORDER=order, ND_SFC_FACT=0.7,
+                                     ND_USE_RS=True)
+        res.append(nd)
+        lib.set_halo_exchange(None)
+        lib.finalize()
+    assert np.array_equal(res[0], res[1], equal_nan=True)
+
+
+@pytest.mark.parametrize("along", [True, False])
+def test_hook_fct_tracer_matches_periodic_halo(lib, along):
+    from test_gpu_parity import _tracer_inputs
+
+    g = helpers.small_grid(IMAX=14, JMAX=12, KMAX=16, stretched=True)
+    c = helpers.small_case(g)
+    helpers.perturb_state(c)
+    q0, q, d0, d, mflx, rhoq, GS, MAPF = _tracer_inputs(g, c)
+    ndq = np.asfortranarray(1e-6 * np.random.default_rng(9).normal(size=g.shape + (3,)))
+    res = []
+    for hook in (False, True):
+        qq = q.copy(order="F")
+        lib.setup(g.index_dict(), "UD3", "UD3")
+        if hook:
+            _attach(g)
+        lib.ATMOS_DYN_Tinteg_tracer_rk3(QTRC=qq, QTRC0=q0, RHOQ_t=rhoq, DENS0=d0, DENS=d, mflx_hi=mflx,
+                                        num_diff=ndq, GSQRT=GS, MAPF=MAPF, CDZ=g.CDZ, RCDZ=g.RCDZ, RCDX=g.RCDX,
+                                        RCDY=g.RCDY, BND_W=False, BND_E=False, BND_S=False, BND_N=False, dtl=5.0,
+                                        FLAG_FCT_TRACER=True, FLAG_FCT_ALONG_STREAM=along)
+        res.append(qq)
+        lib.set_halo_exchange(None)
+        lib.finalize()
+    assert np.array_equal(res[0], res[1], equal_nan=True)
 
 
 def test_hook_mixed_precision_matches_periodic_halo(lib):
