@@ -10,9 +10,10 @@
 // separate kernels run (phi_point, numfilter_column, halo_column,
 // hevi_stage_block, vbc_column), applied to the blocks of that phase's launch
 // over all members, whose block maps are kernel parameters: a CTA takes the
-// blocks x = blockIdx.x, blockIdx.x + gridDim.x, ... of a small body in
-// sub-blocks of 4 or 8 warps, and the stage tiles one at a time from a
-// counter. Between phases a grid barrier: CTA
+// blocks x = blockIdx.x, blockIdx.x + gridDim.x, ... of a fill or of phi in
+// sub-blocks of 4 or 8 warps, the filter's blocks four at a time and the stage
+// tiles one at a time from counters (columns of different heights cost
+// different times). Between phases a grid barrier: CTA
 // arrivals counted on a device word with a release, polled with an acquire,
 // and bounded in time; a barrier that does not complete within the wait limit
 // sets ST_BARRIER_TIMEOUT in the status word and the CTA returns (so does
@@ -42,7 +43,7 @@ struct Args {
     StageArgsT<R> st[4];
     double *rk[3][5];  // the outputs of stages 1-3, halo-filled after each
     double *X[5];      // the state: stage 4 writes it, then its vertical and lateral halo
-    unsigned *bar;     // [0] arrival counter, [1 + s] tiles taken in stage s; zero at launch
+    unsigned *bar;     // [0] arrival counter, [1 + s] tiles taken in stage s, [5] filter blocks taken; zero at launch
     unsigned *status;
     long long wait;    // clock cycles a barrier waits at most
     unsigned extra;    // arrivals a barrier waits for beyond the grid's own (0)
@@ -93,6 +94,26 @@ __device__ __forceinline__ void for_blocks(int nvb, F f)
     }
 }
 
+// the same, taking WARPS / VW blocks at a time from the counter *next (zero at
+// launch), so that blocks of different cost even out across the CTAs; s_x is
+// a shared word of the CTA
+template <int VW, class F>
+__device__ __forceinline__ void take_blocks(unsigned *next, int nvb, int *s_x, F f)
+{
+    constexpr int PER = WARPS / VW;
+    static_assert(PER * VW == WARPS, "a sub-block must divide the CTA");
+    const int sub = threadIdx.y / VW, wy = threadIdx.y % VW;
+    for (;;) {
+        if (threadIdx.x == 0 && threadIdx.y == 0) *s_x = (int)atomicAdd(next, (unsigned)PER);
+        __syncthreads();
+        const int base = *s_x; // block-uniform
+        __syncthreads();       // every thread has read it before the next take
+        if (base >= nvb) break;
+        const int x = base + sub;
+        if (x < nvb) f(x, wy, (int)threadIdx.x);
+    }
+}
+
 template <int S, typename R, int TX>
 __global__ void __launch_bounds__(32 * WARPS, HEVI_COL_MINB) k_short_step(const Grid gt, const __grid_constant__ Args<R> a)
 {
@@ -117,7 +138,7 @@ __global__ void __launch_bounds__(32 * WARPS, HEVI_COL_MINB) k_short_step(const 
     for_blocks<PHI_THREADS / 32>(P.bphi.first[P.bphi.n],
                                  [&](int x, int wy, int lane) { phi_point(gt, a.nd, P.bphi, x, wy * 32 + lane); });
     if (!barrier()) return;
-    for_blocks<ND_WARPS>(P.bnd.first[P.bnd.n], [&](int x, int wy, int lane) {
+    take_blocks<ND_WARPS>(a.bar + 5, P.bnd.first[P.bnd.n], &s_x, [&](int x, int wy, int lane) {
         numfilter_column<R, NM, false>(gt, a.ndc, a.nd, P.bnd, nullptr, x, wy, lane);
     });
     if (!barrier()) return;
