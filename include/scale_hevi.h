@@ -486,6 +486,13 @@ int scale_hevi_ensemble_layout(long long *cell0, long long *col0, long long *z0,
     const double *REF_dens, const double *REF_pott, const double *REF_rhot,                                    \
     const double *ND_COEF, const double *ND_SFC_FACT, const double *dt
 
+/* The numerical filter's form for one domain (no counterpart in the
+ * reference): 1, the default after setup, forms num_diff from tiles of the
+ * filtered quantities staged in shared memory by bulk tensor copies wherever
+ * the arrays admit tensor maps (16-byte aligned bases and strides); 0 keeps the
+ * column kernel. The results are identical. */
+int scale_hevi_numfilter_form(int tiled);
+
 int scale_hevi_short_step_persistent_dev(SCALE_HEVI_SHORT_STEP_ARGS);
 int scale_hevi_short_step_persistent_mixed_dev(SCALE_HEVI_SHORT_STEP_MIXED_ARGS);
 int scale_hevi_persistent_wait(const double *seconds, const int *extra_arrivals);

@@ -112,6 +112,7 @@ struct Ctx {
     double pwait_s = 2.0;
     unsigned pextra = 0;
     int pgrid = 0; // CTAs of the last persistent launch
+    bool nd_tiled = true; // the filter's tiled form where it applies (scale_hevi_numfilter_form)
 };
 
 Ctx C;
@@ -730,7 +731,7 @@ int run_numfilter(R *num_diff, const double *DENS, const double *MOMZ, const dou
     }
     NdArgsT<R> a{num_diff, DENS, MOMZ, MOMX, MOMY, RHOT, REF_dens, REF_pott, phi};
     CK(timed(sizeof(R) == sizeof(double) ? "numfilter" : "numfilter_mixed", [&] {
-        CU(launch_numfilter(C.g, mem(), C.ndc, a, C.stream));
+        CU(launch_numfilter(C.g, mem(), C.ndc, a, C.stream, C.nd_tiled ? C.status : nullptr));
         return SCALE_HEVI_OK;
     }));
     C.launches += 2;
@@ -1364,6 +1365,13 @@ int scale_hevi_persistent_wait(const double *seconds, const int *extra_arrivals)
     if (*extra_arrivals < 0 || *extra_arrivals > 1) return fail(SCALE_HEVI_ERR_ARG, "extra_arrivals must be 0 or 1");
     C.pwait_s = *seconds;
     C.pextra = (unsigned)*extra_arrivals;
+    return SCALE_HEVI_OK;
+}
+
+int scale_hevi_numfilter_form(int tiled)
+{
+    CK(need_setup());
+    C.nd_tiled = tiled != 0;
     return SCALE_HEVI_OK;
 }
 

@@ -93,8 +93,16 @@ struct NdArgsT {
     R *phi; // 5*N3 scratch: the five filtered quantities at every point
 };
 using NdArgs = NdArgsT<double>;
+// status: the library's status word, which also lets one domain use the tiled
+// form (launch_numfilter_tiled); null keeps the column form k_numfilter
 template <typename R>
-cudaError_t launch_numfilter(const Grid &g, const Members &mem, const NdCoef &c, const NdArgsT<R> &a, cudaStream_t st);
+cudaError_t launch_numfilter(const Grid &g, const Members &mem, const NdCoef &c, const NdArgsT<R> &a, cudaStream_t st,
+                             unsigned *status = nullptr);
+// num_diff from the phi scratch by the tiled kernel (hevi_tma.cu) after k_phi has
+// filled it; cudaErrorNotSupported where the tiled form does not apply
+template <typename R>
+cudaError_t launch_numfilter_tiled(const Grid &g, const Members &mem, const NdCoef &c, const NdArgsT<R> &a,
+                                   unsigned *status, cudaStream_t st);
 // ND_ORDER > 1 (FP64, one domain): the differences of the five quantities go
 // through work buffers w1/w2 (15 fields each; component 3*q + dir, dir 0 z,
 // 1 x, 2 y) and ND_ORDER-1 applications of calc_diff4 with the periodic halo

@@ -38,6 +38,7 @@
 
 #include "hevi_epilogue.cuh"
 #include "hevi_kernels.cuh"
+#include "numfilter_body.cuh"
 
 namespace hevi {
 namespace tma {
@@ -674,6 +675,114 @@ __global__ void __launch_bounds__(32 * CWARPS, 4) k_hevi_column(const Grid gt, c
 }
 
 // =============================================================================
+// k_numfilter_tiled: the 15 num_diff components (ND_ORDER = 1) of a 4 x 4 tile
+// of columns from shared memory
+// =============================================================================
+// One warp per column, lanes along k, chunks of 32 levels as in
+// k_hevi_explicit. Per chunk one thread copies the five filtered quantities
+// (phi, written by k_phi) and DENS over the tile, a lateral halo of 2 and the
+// levels L0-2..L0+33 into shared memory (six bulk tensor copies completing on
+// an mbarrier, bounded wait); numfilter_cell then forms every component from
+// there, with the arithmetic of k_numfilter, so the two give identical bits.
+// The vertical halo levels of each column follow with global loads.
+#ifndef HEVI_ND_TX
+#define HEVI_ND_TX 4
+#define HEVI_ND_TY 4
+#endif
+constexpr int NTX = HEVI_ND_TX, NTY = HEVI_ND_TY, NWARPS = NTX * NTY; // tile columns; one warp each
+constexpr int NKLO = 2;                        // box levels below the chunk's first
+constexpr int NBK = KC + 4;                    // box levels: L0-2 .. L0+33
+constexpr int NBW = NTX + 4, NBH = NTY + 4;    // lateral halo of 2
+constexpr int NPL = NBK * NBW * NBH;           // one staged field
+template <typename R> constexpr size_t nd_smem_bytes() { return (size_t)NPL * (5 * sizeof(R) + sizeof(double)) + 16; }
+
+struct NdMaps {
+    CUtensorMap m[6]; // phi q = 0..4 (type R), DENS (FP64), as (KA, IA, JA) tensors
+};
+
+// the staged filtered quantities; box element 0 is level k0, column i0, row j0
+template <typename R>
+struct PhiS {
+    using type = R;
+    const R *base;
+    int k0, i0, j0;
+    __device__ R operator()(int q, int k, int i, int j) const
+    {
+        return base[q * NPL + ((j - j0) * NBW + (i - i0)) * NBK + (k - k0)];
+    }
+};
+// the staged density around a cell
+struct DensS {
+    const double *p;
+    __device__ double operator()(int dk, int di, int dj) const { return p[dk + di * NBK + dj * NBK * NBW]; }
+};
+
+template <typename R>
+__global__ void __launch_bounds__(32 * NWARPS, 1024 / (32 * NWARPS) > 1 ? 2 : 1)
+    k_numfilter_tiled(const Grid g, const NdCoef c, const NdArgsT<R> a, unsigned *status,
+                      const __grid_constant__ NdMaps maps)
+{
+    extern __shared__ __align__(1024) double sm[];
+    R *sphi = reinterpret_cast<R *>(sm); // 5 fields, [j][i][k] each
+    double *sdn = reinterpret_cast<double *>(reinterpret_cast<char *>(sm) + (size_t)5 * NPL * sizeof(R));
+    uint64_t *bar = reinterpret_cast<uint64_t *>(sdn + NPL);
+    __shared__ int s_ok;
+    const int lane = threadIdx.x, w = threadIdx.y, tid = w * 32 + lane;
+    const int tx = w % NTX, ty = w / NTX;
+    const int nti = (g.IMAX + NTX - 1) / NTX;
+    const int i0 = g.IS + ((int)blockIdx.x % nti) * NTX, j0 = g.JS + ((int)blockIdx.x / nti) * NTY;
+    const int i = i0 + tx, j = j0 + ty;
+    const bool col_ok = i <= g.IE && j <= g.JE;
+    const size_t N3 = n3(g);
+    const int KS = g.KS, KE = g.KE;
+    const int NC = (g.KMAX + KC - 1) / KC;
+    constexpr unsigned BYTES = (unsigned)(NPL * (5 * sizeof(R) + sizeof(double)));
+
+    auto issue = [&](int ch) {
+        // box origin (0-based): level L0-2 = 32*ch (KS = 3), column i0-2, row j0-2
+        const int x = KC * ch + (KS - 1) - NKLO, y = i0 - 2 - 1, z = j0 - 2 - 1;
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        mbar_expect_tx(bar, BYTES);
+        for (int q = 0; q < 5; ++q) tma_load_3d(sphi + (size_t)q * NPL, &maps.m[q], x, y, z, bar);
+        tma_load_3d(sdn, &maps.m[5], x, y, z, bar);
+    };
+    if (tid == 0) {
+        mbar_init(bar, 1);
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        issue(0);
+    }
+    __syncthreads();
+
+    const R ncx = col_ok ? R(ld(c.cdx + i - 1)) : R(0.0), nfx = col_ok ? R(ld(c.fdx + i - 1)) : R(0.0);
+    const R ncy = col_ok ? R(ld(c.cdy + j - 1)) : R(0.0), nfy = col_ok ? R(ld(c.fdy + j - 1)) : R(0.0);
+    const R sfc = R(c.sfc);
+    for (int ch = 0; ch < NC; ++ch) {
+        if (tid == 0) {
+            const bool ok = mbar_wait(bar, ch & 1);
+            // on a timeout, wait once more (bounded) for the copies still in flight
+            if (!ok) (void)mbar_wait(bar, ch & 1);
+            s_ok = ok ? 1 : 0;
+        }
+        __syncthreads();
+        if (!s_ok) {
+            if (tid == 0) atomicOr(status, ST_TMA_TIMEOUT);
+            return; // block-uniform
+        }
+        (void)mbar_try(bar, ch & 1); // completed phase: makes the copied data visible to this thread
+        const int L0 = KS + KC * ch, k = L0 + lane;
+        if (col_ok && k <= KE) {
+            const PhiS<R> phi{sphi, L0 - NKLO, i0 - 2, j0 - 2};
+            const DensS dn{sdn + ((ty + 2) * NBW + (tx + 2)) * NBK + (k - (L0 - NKLO))};
+            numfilter_cell<false>(g, c, phi, dn, nullptr, a.num_diff, N3, idx3(g, k, i, j), k, i, j, ncx, nfx, ncy,
+                                  nfy, sfc);
+        }
+        __syncthreads(); // every read of the staged box is done
+        if (tid == 0 && ch + 1 < NC) issue(ch + 1);
+    }
+    if (col_ok) numfilter_halo_levels<false>(g, c, Phi<R>{g, a}, nullptr, a.num_diff, N3, a.DENS, i, j, lane);
+}
+
+// =============================================================================
 // host side
 // =============================================================================
 static PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
@@ -691,17 +800,21 @@ static PFN_cuTensorMapEncodeTiled_v12000 encode_fn()
     return fn;
 }
 
-// FP64 (KA, IA, JA) tensor with a box of bk x bw x bh elements
-static bool encode(CUtensorMap *m, const double *base, const Grid &g, int bk, int bw, int bh)
+// FP64 or FP32 (KA, IA, JA) tensor with a box of bk x bw x bh elements; false
+// unless the base address and the strides are multiples of 16 bytes
+template <typename T>
+static bool encode(CUtensorMap *m, const T *base, const Grid &g, int bk, int bw, int bh)
 {
     auto fn = encode_fn();
-    if (!fn || ((uintptr_t)base & 15u)) return false;
+    const size_t sk = (size_t)g.KA * sizeof(T), sj = (size_t)g.KA * g.IA * sizeof(T);
+    if (!fn || ((uintptr_t)base & 15u) || (sk & 15u) || (sj & 15u) || ((size_t)bk * sizeof(T)) % 16u) return false;
     const cuuint64_t dims[3] = {(cuuint64_t)g.KA, (cuuint64_t)g.IA, (cuuint64_t)g.JA};
-    const cuuint64_t strides[2] = {(cuuint64_t)g.KA * sizeof(double), (cuuint64_t)g.KA * g.IA * sizeof(double)};
+    const cuuint64_t strides[2] = {(cuuint64_t)sk, (cuuint64_t)sj};
     const cuuint32_t box[3] = {(cuuint32_t)bk, (cuuint32_t)bw, (cuuint32_t)bh};
     const cuuint32_t estr[3] = {1, 1, 1};
-    return fn(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, const_cast<double *>(base), dims, strides, box, estr,
-              CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+    const CUtensorMapDataType dt = sizeof(T) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+    return fn(m, dt, 3, const_cast<T *>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+              CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
@@ -748,7 +861,40 @@ cudaError_t launch_s(const Grid &g, StageArgsT<R> a, int raster, cudaStream_t st
     return cudaGetLastError();
 }
 
+template <typename R>
+cudaError_t launch_numfilter_s(const Grid &g, const NdCoef &c, const NdArgsT<R> &a, unsigned *status, cudaStream_t st)
+{
+    NdMaps maps;
+    for (int q = 0; q < 5; ++q)
+        if (!encode(&maps.m[q], a.phi + (size_t)q * n3(g), g, NBK, NBW, NBH)) return cudaErrorNotSupported;
+    if (!encode(&maps.m[5], a.DENS, g, NBK, NBW, NBH)) return cudaErrorNotSupported;
+    auto k = k_numfilter_tiled<R>;
+    cudaError_t e = open_smem(k, nd_smem_bytes<R>());
+    if (e != cudaSuccess) return e;
+    const int ntiles = ((g.IMAX + NTX - 1) / NTX) * ((g.JMAX + NTY - 1) / NTY);
+    k<<<ntiles, dim3(32, NWARPS), nd_smem_bytes<R>(), st>>>(g, c, a, status, maps);
+    return cudaGetLastError();
+}
+
 }  // namespace tma
+
+// The numerical filter's components from staged tiles where they apply: one
+// domain of KHALO = 2 whose filtered quantities and density admit tensor maps
+// (16-byte aligned bases and strides). cudaErrorNotSupported otherwise.
+template <typename R>
+cudaError_t launch_numfilter_tiled(const Grid &g, const Members &mem, const NdCoef &c, const NdArgsT<R> &a,
+                                   unsigned *status, cudaStream_t st)
+{
+    if (mem.n > 1 || g.KS != 3 || c.order != 1 || !status) return cudaErrorNotSupported;
+    return tma::launch_numfilter_s<R>(g, c, a, status, st);
+}
+#ifndef HEVI_FLOAT_TU
+template cudaError_t launch_numfilter_tiled<double>(const Grid &, const Members &, const NdCoef &,
+                                                    const NdArgsT<double> &, unsigned *, cudaStream_t);
+#else
+template cudaError_t launch_numfilter_tiled<float>(const Grid &, const Members &, const NdCoef &,
+                                                   const NdArgsT<float> &, unsigned *, cudaStream_t);
+#endif
 
 // The tiled stage where it applies: one domain, even KA, KA <= MAXKA_TILED,
 // the column scratch of the tiled kernels present and every staged field on a

@@ -131,7 +131,8 @@ cudaError_t launch_numfilter_high(const Grid &g, const NdCoef &c, const NdArgs &
 #endif
 
 template <typename R>
-cudaError_t launch_numfilter(const Grid &g, const Members &mem, const NdCoef &c, const NdArgsT<R> &a, cudaStream_t st)
+cudaError_t launch_numfilter(const Grid &g, const Members &mem, const NdCoef &c, const NdArgsT<R> &a, cudaStream_t st,
+                             unsigned *status)
 {
     auto nb_phi = [](const Grid &m) { return (int)(((long)m.KA * m.IA * m.JA + PHI_THREADS - 1) / PHI_THREADS); };
     auto nb_nd = [](const Grid &m) { return ((m.IMAX + 3) / 4) * m.JMAX; };
@@ -139,6 +140,11 @@ cudaError_t launch_numfilter(const Grid &g, const Members &mem, const NdCoef &c,
         k_phi<R, std::decay_t<decltype(B)>::NMAX><<<nb, PHI_THREADS, 0, st>>>(g, a, B);
         return cudaSuccess;
     });
+    if (status) {
+        // one domain: the components from staged tiles where the tensor maps apply
+        const cudaError_t e = launch_numfilter_tiled(g, mem, c, a, status, st);
+        if (e != cudaErrorNotSupported) return e;
+    }
     with_batch(g, mem, nb_nd, [&](const auto &B, int nb) {
         k_numfilter<R, std::decay_t<decltype(B)>::NMAX><<<nb, dim3(32, 4), 0, st>>>(g, c, a, B, nullptr);
         return cudaSuccess;
@@ -147,10 +153,10 @@ cudaError_t launch_numfilter(const Grid &g, const Members &mem, const NdCoef &c,
 }
 #ifdef HEVI_FLOAT_TU
 template cudaError_t launch_numfilter<float>(const Grid &, const Members &, const NdCoef &, const NdArgsT<float> &,
-                                             cudaStream_t);
+                                             cudaStream_t, unsigned *);
 #else
 template cudaError_t launch_numfilter<double>(const Grid &, const Members &, const NdCoef &, const NdArgsT<double> &,
-                                              cudaStream_t);
+                                              cudaStream_t, unsigned *);
 #endif
 
 }  // namespace hevi

@@ -100,7 +100,7 @@ def load(path: str | os.PathLike | None = None) -> C.CDLL:
             f.argtypes = [C.c_char_p]
         elif name == "scale_hevi_set_halo_exchange":
             f.argtypes = [HALO_FN, C.c_void_p]
-        elif name == "scale_hevi_stage_autotune":
+        elif name in ("scale_hevi_stage_autotune", "scale_hevi_numfilter_form"):
             f.argtypes = [C.c_int]
         elif name == "scale_hevi_stage_shape_get":
             f.argtypes = [C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_int]
@@ -413,6 +413,11 @@ def persistent_wait(seconds: float, extra_arrivals: int = 0) -> None:
     """Time limit of the persistent step's grid barriers; extra_arrivals = 1
     makes them wait for a CTA that does not exist (a test of the limit)."""
     call("scale_hevi_persistent_wait", seconds=seconds, extra_arrivals=extra_arrivals)
+
+
+def numfilter_form(tiled: bool) -> None:
+    """The filter's tiled form (True, the default) or the column kernel for one domain."""
+    _check(load().scale_hevi_numfilter_form(int(bool(tiled))))
 
 
 def persistent_grid() -> int:

@@ -149,3 +149,34 @@ def test_mixed_tracer_rk3_matches_fp64(fct, along):
     if fct:
         # no new minimum beyond FP32 rounding of the FP64 run's own
         assert a32.min() >= a64.min() - 1e-6 * np.max(np.abs(a64))
+
+
+def test_mixed_numfilter_tiled_form_matches_column_form():
+    """The FP32 filter from staged tiles against the FP32 column kernel on the
+    same inputs (two FP32 builds: FMA contraction may differ, so to 1e-6 of
+    each component's largest value)."""
+    import torch
+
+    import helpers
+
+    g = helpers.small_grid(IMAX=13, JMAX=10, KMAX=36, stretched=True)
+    c = helpers.small_case(g)
+    helpers.perturb_state(c)
+    dev = lambda x: torch.from_numpy(np.ravel(x, order="K").copy()).cuda()  # noqa: E731
+    out = []
+    for tiled in (True, False):
+        hevi.setup(g.index_dict(), "UD3", "UD3")
+        try:
+            hevi.numfilter_form(tiled)
+            nd = torch.zeros(15 * int(np.prod(g.shape)), dtype=torch.float32, device="cuda")
+            hevi.ATMOS_DYN_numfilter_coef_mixed_dev(
+                num_diff=nd, CDZ=g.CDZ, CDX=g.CDX, CDY=g.CDY, FDZ=g.FDZ, FDX=g.FDX, FDY=g.FDY, DT=0.5,
+                REF_dens=dev(c.ref["REF_dens"]), REF_pott=dev(c.ref["REF_pott"]), ND_COEF=1e-3, ND_ORDER=1,
+                ND_SFC_FACT=0.7, ND_USE_RS=True, **{n: dev(c.state[n]) for n in STATE})
+            hevi.check()
+            out.append(nd.cpu().numpy().reshape(g.shape + (15,), order="F"))
+        finally:
+            hevi.finalize()
+    for q in range(15):
+        scale = np.max(np.abs(out[1][..., q]))
+        assert np.max(np.abs(out[0][..., q] - out[1][..., q])) <= 1e-6 * max(scale, 1e-30), q

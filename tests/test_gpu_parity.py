@@ -119,6 +119,34 @@ def test_numfilter_bit_exact(lib, stretched, order, halo):
             assert helpers.same(got[..., v, d], ref_nd[..., v, d]), f"num_diff(:,:,:,{v+1},{d+1})"
 
 
+@pytest.mark.parametrize("kmax,halo", [(20, 2), (36, 2), (64, 3), (96, 2)])
+def test_numfilter_tiled_form_bit_exact(lib, kmax, halo):
+    """The filter's tiled form (num_diff from tiles staged by bulk tensor
+    copies; KA a multiple of 4 admits the tensor maps) against the column form
+    and the oracle, bit for bit, with ragged tiles and chunks."""
+    g = helpers.small_grid(IMAX=13, JMAX=10, KMAX=kmax, stretched=True, halo=halo)
+    c = helpers.small_case(g)
+    helpers.perturb_state(c)
+    ref_nd = g.zeros(5, 3)
+    oracle.numfilter(g, ref_nd, c.state, c.ref, DT=0.5, ND_COEF=1e-3, ND_ORDER=1, ND_SFC_FACT=0.7)
+    res = []
+    for tiled in (True, False):
+        got = np.full(g.shape + (5, 3), np.nan, order="F")
+        lib.setup(g.index_dict(), "UD3", "UD3")
+        lib.numfilter_form(tiled)
+        lib.ATMOS_DYN_numfilter_coef(num_diff=got, DENS=c.state["DENS"], MOMZ=c.state["MOMZ"], MOMX=c.state["MOMX"],
+                                     MOMY=c.state["MOMY"], RHOT=c.state["RHOT"], CDZ=g.CDZ, CDX=g.CDX, CDY=g.CDY,
+                                     FDZ=g.FDZ, FDX=g.FDX, FDY=g.FDY, DT=0.5, REF_dens=c.ref["REF_dens"],
+                                     REF_pott=c.ref["REF_pott"], ND_COEF=1e-3, ND_ORDER=1, ND_SFC_FACT=0.7,
+                                     ND_USE_RS=True)
+        lib.finalize()
+        res.append(got)
+    assert np.array_equal(res[0], res[1], equal_nan=True)
+    for v in range(5):
+        for d in range(3):
+            assert helpers.same(res[0][..., v, d], ref_nd[..., v, d]), f"num_diff(:,:,:,{v+1},{d+1})"
+
+
 def _tracer_inputs(g, c, seed=5):
     rng = np.random.Generator(np.random.PCG64(seed))
     q0 = np.asfortranarray(np.clip(1e-3 + 5e-4 * rng.normal(size=g.shape), 0.0, None))
