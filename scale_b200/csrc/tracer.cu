@@ -204,7 +204,7 @@ __device__ __forceinline__ void fact_fct(R f[2][3][3], R rw, R ru, R rv)
 
 // ---- FCT part 2: limiting factors R+ and R- (common.F90:2079-2553) ----------
 template <typename R>
-__global__ void __launch_bounds__(128) k_fct_r(const Grid g, const TracerArgsT<R> a)
+__global__ void __launch_bounds__(128, 4) k_fct_r(const Grid g, const TracerArgsT<R> a)
 {
     const int i = g.IS + blockIdx.x * blockDim.y + threadIdx.y;
     const int j = g.JS + blockIdx.y;
