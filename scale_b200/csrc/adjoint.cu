@@ -182,13 +182,21 @@ struct AdjIO {
     int fid[N];
     size_t off[N];
     __device__ AdjIO(const Ctx &c) : x(c) {}
+    // The slots are indexed by compile-time constants only (an unrolled loop
+    // with a select), so the jets and the slot table stay in registers rather
+    // than in local memory.
     __device__ Jet<N> in(int f, size_t c)
     {
         Jet<N> r(x.val[f][c]);
         if (n < N) {
-            r.d[n] = 1.0;
-            fid[n] = f;
-            off[n] = c;
+#pragma unroll
+            for (int q = 0; q < N; ++q) {
+                if (q == n) {
+                    r.d[q] = 1.0;
+                    fid[q] = f;
+                    off[q] = c;
+                }
+            }
             ++n;
         } else {
             atomicOr(x.status, ST_JET_OVERFLOW);
@@ -200,8 +208,9 @@ struct AdjIO {
     {
         const double l = x.aux[f][c];
         if (l == 0.0) return;
-        for (int q = 0; q < n; ++q)
-            if (v.d[q] != 0.0) atomicAdd(x.aux[fid[q]] + off[q], l * v.d[q]);
+#pragma unroll
+        for (int q = 0; q < N; ++q)
+            if (q < n && v.d[q] != 0.0) atomicAdd(x.aux[fid[q]] + off[q], l * v.d[q]);
     }
 };
 
@@ -248,12 +257,19 @@ struct PassPhi {
     __device__ void operator()(IO &io, const Ctx &x, int k, int i, int j) const
     {
         PASS_BEGIN
+        // every input is loaded unconditionally and in one order (the neighbour
+        // of the last point of the array in a direction is replaced by the point
+        // itself, whose value is then unused), so each keeps one derivative slot
         const T D = IN(XD, c);
+        const T W = IN(XW, c), Dk = IN(XD, k < g.KA ? c + 1 : c);
+        const T U = IN(XU, c), Di = IN(XD, i < g.IA ? c + sI : c);
+        const T V = IN(XV, c), Dj = IN(XD, j < g.JA ? c + sJ : c);
+        const T RT = IN(XR, c);
         io.out(PH0 + 0, c, D - CS(REFDENS, c));
-        io.out(PH0 + 1, c, k < g.KA ? T(2.0) * IN(XW, c) / (IN(XD, c + 1) + D) : T(0.0));
-        io.out(PH0 + 2, c, i < g.IA ? T(2.0) * IN(XU, c) / (IN(XD, c + sI) + D) : T(0.0));
-        io.out(PH0 + 3, c, j < g.JA ? T(2.0) * IN(XV, c) / (IN(XD, c + sJ) + D) : T(0.0));
-        io.out(PH0 + 4, c, IN(XR, c) / D - CS(REFPOTT, c));
+        io.out(PH0 + 1, c, k < g.KA ? T(2.0) * W / (Dk + D) : T(0.0));
+        io.out(PH0 + 2, c, i < g.IA ? T(2.0) * U / (Di + D) : T(0.0));
+        io.out(PH0 + 3, c, j < g.JA ? T(2.0) * V / (Dj + D) : T(0.0));
+        io.out(PH0 + 4, c, RT / D - CS(REFPOTT, c));
     }
 };
 
@@ -421,9 +437,11 @@ struct PassMFLX {
     __device__ void operator()(IO &io, const Ctx &x, int k, int i, int j) const
     {
         PASS_BEGIN
-        if (j >= g.JS && i >= g.IS) io.out(MZ, c, (k == KS - 1 || k == KE) ? T(0.0) : IN(NDF(1, 1), c));
-        if (j >= g.JS && k >= KS) io.out(MX, c, IN(XU, c) + IN(NDF(1, 2), c));
-        if (i >= g.IS && k >= KS) io.out(MY, c, IN(XV, c) + IN(NDF(1, 3), c));
+        // the inputs are loaded unconditionally and in one order (one slot each)
+        const T nz = IN(NDF(1, 1), c), U = IN(XU, c), nx = IN(NDF(1, 2), c), V = IN(XV, c), ny = IN(NDF(1, 3), c);
+        if (j >= g.JS && i >= g.IS) io.out(MZ, c, (k == KS - 1 || k == KE) ? T(0.0) : nz);
+        if (j >= g.JS && k >= KS) io.out(MX, c, U + nx);
+        if (i >= g.IS && k >= KS) io.out(MY, c, V + ny);
     }
 };
 
@@ -451,7 +469,8 @@ struct PassQWZ {
         }
         const T Mk = IN(XW, c), Mk1 = IN(XW, c + 1);
         const T vel = (T(0.5) * (Mk + Mk1)) / IN(XD, c + 1);
-        const T q = (k == KS) ? ipL<S>(vel, Mk, Mk1, IN(XW, c + 2)) : ip4<S>(vel, IN(XW, c - 1), Mk, Mk1, IN(XW, c + 2));
+        const T Mm1 = IN(XW, c - 1), Mk2 = IN(XW, c + 2); // both branches' points, loaded in one order
+        const T q = (k == KS) ? ipL<S>(vel, Mk, Mk1, Mk2) : ip4<S>(vel, Mm1, Mk, Mk1, Mk2);
         io.out(QWZ, c, T(x.J33G) * vel * q + IN(NDF(2, 1), c + 1));
     }
 };
@@ -507,11 +526,15 @@ struct PassTZ {
             io.out(TZ, c, T(0.0));
             return;
         }
+        // every branch's points are loaded first, in one order, so that each
+        // input keeps one derivative slot whatever the branch (KS-1 and KE+1 are
+        // in the array; an unused point contributes nothing)
         const T mZ = IN(MZ, c);
+        const T Pm1 = IN(POTT, c - 1), P0 = IN(POTT, c), P1 = IN(POTT, c + 1), P2 = IN(POTT, c + 2);
         T ti;
-        if (k == KS) ti = ipL<S>(mZ, IN(POTT, c), IN(POTT, c + 1), IN(POTT, c + 2));
-        else if (k == KE - 1) ti = ipH<S>(mZ, IN(POTT, c + 1), IN(POTT, c), IN(POTT, c - 1));
-        else ti = ip4<S>(mZ, IN(POTT, c - 1), IN(POTT, c), IN(POTT, c + 1), IN(POTT, c + 2));
+        if (k == KS) ti = ipL<S>(mZ, P0, P1, P2);
+        else if (k == KE - 1) ti = ipH<S>(mZ, P1, P0, Pm1);
+        else ti = ip4<S>(mZ, Pm1, P0, P1, P2);
         io.out(TZ, c, mZ * ti + IN(NDF(5, 1), c));
     }
 };
@@ -760,10 +783,11 @@ struct PassQHZ {
         const T h = T(0.5);
         const T den = TB(g.F2H1, k - 1) * h * (IN(XD, c + 1) + IN(XD, c + 1 + s)) + TB(g.F2H2, k - 1) * h * (IN(XD, c) + IN(XD, c + s));
         const T vel = (h * (IN(XW, c) + IN(XW, c + s))) / den;
+        const T Vm1 = IN(val, c - 1), V0 = IN(val, c), V1 = IN(val, c + 1), V2 = IN(val, c + 2); // one order
         T q;
-        if (k == KS) q = ipL<S>(vel, IN(val, c), IN(val, c + 1), IN(val, c + 2));
-        else if (k == KE - 1) q = ipH<S>(vel, IN(val, c + 1), IN(val, c), IN(val, c - 1));
-        else q = ip4<S>(vel, IN(val, c - 1), IN(val, c), IN(val, c + 1), IN(val, c + 2));
+        if (k == KS) q = ipL<S>(vel, V0, V1, V2);
+        else if (k == KE - 1) q = ipH<S>(vel, V1, V0, Vm1);
+        else q = ip4<S>(vel, Vm1, V0, V1, V2);
         io.out(out, c, T(x.J33G) * vel * q + IN(NDF(DIRY ? 4 : 3, 1), c));
     }
 };
