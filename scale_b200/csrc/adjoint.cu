@@ -224,7 +224,7 @@ struct Box {
 };
 
 template <class P, class IOT>
-__global__ void __launch_bounds__(128) k_pass(const Ctx x, const Box b)
+__global__ void __launch_bounds__(128) k_pass(const __grid_constant__ Ctx x, const Box b)
 {
     long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= b.count()) return;
@@ -1003,7 +1003,8 @@ cudaError_t numfilter(Mode m, const Ctx &x, cudaStream_t st)
     const Grid &g = x.g;
     const Box all{1, g.KA, 1, g.IA, 1, g.JA}, col{1, g.KA, g.IS, g.IE, g.JS, g.JE};
     auto nd = [&](auto v, auto d) -> cudaError_t {
-        return run<PassND<decltype(v)::value, decltype(d)::value>, 12>(m, x, col, st);
+        // at most 8 inputs per component: 4 filtered quantities and 4 densities
+        return run<PassND<decltype(v)::value, decltype(d)::value>, 8>(m, x, col, st);
     };
 #define ND_(v, d) RUN(nd(std::integral_constant<int, v>{}, std::integral_constant<int, d>{}))
     if (m != M_ADJ) {
