@@ -832,8 +832,17 @@ def run_adjoint(args, hevi, torch):
                 fd[f"{e:g}"] = {"max": errs[-1], "median": errs[len(errs) // 2]}
             out[scheme] = {"J": J, "gradient_s": t_grad, "steps": args.adjoint_steps, "checkpoint_every": 10,
                            "ms_per_adjoint_step": ms_adj, "ms_per_forward_step": ms_fwd,
+                           "adjoint_cost_vs_forward": ms_adj / ms_fwd,
                            "fd_rel_err_by_eps": fd, "directions": len(r["directions"]),
                            "dot_product_rel_diff": dp["rel_diff"]}
+            # the same directions with both perturbed runs in double-double
+            # arithmetic (scale_hevi_short_step_dd_dev), at the configuration's eps
+            w0 = time.time()
+            rdd = adjoint.gradient_check(p, ndirs=8, eps=1e-6, dd=True)
+            errs = sorted(d["rel_err"] for d in rdd["directions"])
+            out[scheme]["fd_rel_err_double_double"] = {
+                "eps": 1e-6, "max": errs[-1], "median": errs[len(errs) // 2], "seconds": time.time() - w0,
+                "forward": "pass-form short step in double-double arithmetic (about 32 digits)"}
         finally:
             hevi.finalize()
     out["workload"] = "warm bubble 128x128x64, dx=500 m, dt=1 s; J over x,y in [20,44] km, z in [2,6] km"

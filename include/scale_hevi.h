@@ -542,6 +542,12 @@ const char *scale_hevi_autotune_report(void);
  *   scale_hevi_boundary_adjoint_dev
  *                                 adjoint of scale_hevi_boundary_dev (on the
  *                                 5 fields of lam)
+ *   scale_hevi_short_step_dd_dev  the pass-form step in double-double
+ *                                 arithmetic (about 32 significant digits): the
+ *                                 state is X_hi + X_lo. A finite-difference
+ *                                 check of the adjoint runs it so that the
+ *                                 rounding of the forward model stays far below
+ *                                 the perturbation's effect
  * ------------------------------------------------------------------------- */
 int scale_hevi_adjoint_setup(const double *DPRES0, const double *RT2P, const double *REF_rhot, const double *REF_dens,
                              const double *REF_pott, const double *PHI, const double *CORIOLI, const double *CDZ,
@@ -552,6 +558,7 @@ int scale_hevi_adjoint_setup(const double *DPRES0, const double *RT2P, const dou
 int scale_hevi_short_step_dev(double *X);
 int scale_hevi_short_step_passes_dev(double *X);
 int scale_hevi_short_step_tlm_dev(double *X, double *dX);
+int scale_hevi_short_step_dd_dev(double *X_hi, double *X_lo);
 int scale_hevi_short_step_adjoint_dev(const double *X, double *lam);
 int scale_hevi_boundary_adjoint_dev(double *lam);
 

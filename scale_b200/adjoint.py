@@ -55,6 +55,10 @@ class Model:
     def tlm(self, X, dX) -> None:
         hevi.call("scale_hevi_short_step_tlm_dev", X=X, dX=dX)
 
+    def step_dd(self, X_hi, X_lo) -> None:
+        """One step in double-double arithmetic; the state is X_hi + X_lo."""
+        hevi.call("scale_hevi_short_step_dd_dev", X_hi=X_hi, X_lo=X_lo)
+
     def adjoint(self, X, lam) -> None:
         hevi.call("scale_hevi_short_step_adjoint_dev", X=X, lam=lam)
 
@@ -202,6 +206,46 @@ class Problem:
             n = self.n3
             return X[4 * n:] / X[:n]
 
+    def theta_of_dd(self, d, eps):
+        """theta_of in double-double arithmetic (scale_hevi_short_step_dd_dev):
+        the perturbed start state is formed exactly, every step rounds at about
+        1e-32, and theta = RHOT/DENS comes back as a (hi, lo) pair of numpy arrays."""
+        import torch
+
+        n = self.n3
+        host = lambda t: t.detach().cpu().numpy()  # noqa: E731
+        D0, W0 = host(self.DENS0), host(self.MOMZ0)
+        th_h, th_l = _two_sum(host(self.theta0), host(eps * d[0]))
+        u_h, u_l = _two_sum(host(self.MOMX0), host(eps * d[1]))
+        v_h, v_l = _two_sum(host(self.MOMY0), host(eps * d[2]))
+        r_h, r_l = dd_mul(D0, 0.0 * D0, th_h, th_l)
+        z = np.zeros_like(D0)
+        hi = torch.from_numpy(np.concatenate([D0, W0, u_h, v_h, r_h])).cuda()
+        lo = torch.from_numpy(np.concatenate([z, z, u_l, v_l, r_l])).cuda()
+        self.model.boundary(hi)
+        self.model.boundary(lo)
+        for _ in range(self.nsteps):
+            self.model.step_dd(hi, lo)
+        hevi.check()
+        h, l = host(hi), host(lo)
+        with np.errstate(divide="ignore", invalid="ignore"):
+            return dd_div(h[4 * n:], l[4 * n:], h[:n], l[:n])
+
+    def J_diff_dd(self, d, eps):
+        """J_diff with both runs in double-double arithmetic: the difference of
+        the two trajectories then carries no rounding of the forward model (FP64
+        leaves about 1e-16 of theta per operation, which divided by 2 eps sets a
+        floor of 1e-6..1e-5 on the finite difference at eps = 1e-6)."""
+        tph, tpl = self.theta_of_dd(d, eps)
+        tmh, tml = self.theta_of_dd(d, -eps)
+        dh, dl = dd_add(tph, tpl, -tmh, -tml)
+        diff = dh + dl
+        base = self.theta_base.cpu().numpy()
+        w = self.w.cpu().numpy()
+        m = w > 0.0
+        terms = diff[m] * (((tph[m] - base[m]) + tpl[m]) + ((tmh[m] - base[m]) + tml[m])) * w[m]
+        return 0.5 * float(np.sum(terms))
+
     def J_diff(self, d, eps):
         """J(X + eps d) - J(X - eps d), differenced cell by cell before the sum:
         a^2 - b^2 = (a - b)(a + b) with a, b the deviations from the base state of
@@ -212,6 +256,54 @@ class Problem:
         with torch.no_grad():
             tp, tm = self.theta_of(d, eps), self.theta_of(d, -eps)
             return float(0.5 * torch.sum((tp - tm) * ((tp - self.theta_base) + (tm - self.theta_base)) * self.w))
+
+
+# ---- double-double arithmetic on the host (error-free transforms in numpy's
+# IEEE float64: Knuth's two-sum, Veltkamp's split and Dekker's product) ----
+def _fast_sum(a, b):
+    s = a + b
+    return s, b - (s - a)
+
+
+def _two_sum(a, b):
+    s = a + b
+    v = s - a
+    return s, (a - (s - v)) + (b - v)
+
+
+def _split(a):
+    c = 134217729.0 * a  # 2^27 + 1
+    hi = c - (c - a)
+    return hi, a - hi
+
+
+def _two_prod(a, b):
+    p = a * b
+    ah, al = _split(a)
+    bh, bl = _split(b)
+    return p, ((ah * bh - p) + ah * bl + al * bh) + al * bl
+
+
+def dd_add(ah, al, bh, bl):
+    s, e = _two_sum(ah, bh)
+    t, f = _two_sum(al, bl)
+    s, e = _fast_sum(s, e + t)
+    return _fast_sum(s, e + f)
+
+
+def dd_mul(ah, al, bh, bl):
+    p, e = _two_prod(ah, bh)
+    return _fast_sum(p, e + (ah * bl + al * bh))
+
+
+def dd_div(ah, al, bh, bl):
+    q1 = ah / bh
+    rh, rl = dd_add(ah, al, *(-x for x in dd_mul(bh, bl, q1, 0.0 * q1)))
+    q2 = rh / bh
+    rh, rl = dd_add(rh, rl, *(-x for x in dd_mul(bh, bl, q2, 0.0 * q2)))
+    q3 = rh / bh
+    s, e = _fast_sum(q1, q2)
+    return dd_add(s, e, q3, 0.0 * q3)
 
 
 def interior_direction(g, rng, device="cuda"):
@@ -227,10 +319,11 @@ def interior_direction(g, rng, device="cuda"):
     return out
 
 
-def gradient_check(problem: Problem, ndirs: int = 8, eps=1e-6, seed: int = 0) -> dict:
+def gradient_check(problem: Problem, ndirs: int = 8, eps=1e-6, seed: int = 0, dd: bool = False) -> dict:
     """Adjoint gradient against central finite differences along ndirs
     seeded random directions: relative error |FD - <grad, d>| / |FD| for each
-    step size in eps (a number or a sequence); max_rel_err is over the first."""
+    step size in eps (a number or a sequence); max_rel_err is over the first.
+    dd: the finite differences from double-double forward runs (J_diff_dd)."""
     eps_list = [eps] if np.isscalar(eps) else list(eps)
     J0, grad = problem.value_and_grad()
     rng = np.random.default_rng(seed)
@@ -240,7 +333,7 @@ def gradient_check(problem: Problem, ndirs: int = 8, eps=1e-6, seed: int = 0) ->
         ad = float(sum((gq * dq).sum() for gq, dq in zip(grad, d)))
         row = {"adjoint": ad}
         for e in eps_list:
-            fd = problem.J_diff(d, e) / (2 * e)
+            fd = (problem.J_diff_dd(d, e) if dd else problem.J_diff(d, e)) / (2 * e)
             row[f"fd_{e:g}"] = fd
             row[f"rel_err_{e:g}"] = abs(fd - ad) / max(abs(fd), 1e-300)
         row["rel_err"] = row[f"rel_err_{eps_list[0]:g}"]

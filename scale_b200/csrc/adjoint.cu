@@ -124,6 +124,63 @@ struct Jet {
     }
 };
 
+// Double-double numbers (an unevaluated sum hi + lo, about 106 significant
+// bits) for a forward model whose rounding lies far below the differences that
+// a finite-difference check of the adjoint takes. The error-free transforms
+// are Knuth's two-sum, the fast two-sum for |a| >= |b| and the product error
+// through a fused multiply-add; sums, products and quotients renormalise their
+// results. The unit is compiled without FMA contraction, so every expression
+// here is evaluated as written.
+struct DD {
+    double hi, lo;
+    __device__ DD() : hi(0.0), lo(0.0) {}
+    __device__ DD(double x) : hi(x), lo(0.0) {}
+    __device__ DD(double h, double l) : hi(h), lo(l) {}
+};
+__device__ __forceinline__ DD dd_two_sum(double a, double b)
+{
+    const double s = a + b, v = s - a;
+    return {s, (a - (s - v)) + (b - v)};
+}
+__device__ __forceinline__ DD dd_fast_sum(double a, double b) // |a| >= |b| or a == 0
+{
+    const double s = a + b;
+    return {s, b - (s - a)};
+}
+__device__ __forceinline__ DD dd_two_prod(double a, double b)
+{
+    const double p = a * b;
+    return {p, fma(a, b, -p)};
+}
+__device__ __forceinline__ DD operator+(const DD &a, const DD &b)
+{
+    DD s = dd_two_sum(a.hi, b.hi);
+    const DD t = dd_two_sum(a.lo, b.lo);
+    s = dd_fast_sum(s.hi, s.lo + t.hi);
+    return dd_fast_sum(s.hi, s.lo + t.lo);
+}
+__device__ __forceinline__ DD operator-(const DD &a) { return {-a.hi, -a.lo}; }
+__device__ __forceinline__ DD operator+(const DD &a) { return a; }
+__device__ __forceinline__ DD operator-(const DD &a, const DD &b) { return a + (-b); }
+__device__ __forceinline__ DD operator*(const DD &a, const DD &b)
+{
+    const DD p = dd_two_prod(a.hi, b.hi);
+    return dd_fast_sum(p.hi, p.lo + (a.hi * b.lo + a.lo * b.hi));
+}
+__device__ __forceinline__ DD operator/(const DD &a, const DD &b)
+{
+    // three quotient digits, each from the remainder of the previous ones
+    const double q1 = a.hi / b.hi;
+    DD r = a - b * DD(q1);
+    const double q2 = r.hi / b.hi;
+    r = r - b * DD(q2);
+    const double q3 = r.hi / b.hi;
+    return dd_fast_sum(q1, q2) + DD(q3);
+}
+__device__ __forceinline__ double vof(const DD &a) { return a.hi; }
+__device__ __forceinline__ DD fabs(const DD &a) { return signbit(a.hi) ? -a : a; }
+__device__ __forceinline__ DD copysign(const DD &a, const DD &b) { return signbit(a.hi) != signbit(b.hi) ? -a : a; }
+
 // ---- field table ---------------------------------------------------------------------
 // Every array a pass touches is a field of the table; val[f] holds its values,
 // aux[f] its tangent (TlmIO) or adjoint (AdjIO), null for constants.
@@ -172,6 +229,19 @@ struct TlmIO {
     {
         x.val[f][c] = v.v;
         x.aux[f][c] = v.t;
+    }
+};
+// double-double values: hi in val, lo in aux
+struct DdIO {
+    using T = DD;
+    const Ctx &x;
+    __device__ DdIO(const Ctx &c) : x(c) {}
+    __device__ DD in(int f, size_t c) { return DD(x.val[f][c], x.aux[f][c]); }
+    __device__ DD cst(int f, size_t c) { return DD(x.val[f][c]); }
+    __device__ void out(int f, size_t c, const DD &v)
+    {
+        x.val[f][c] = v.hi;
+        x.aux[f][c] = v.lo;
     }
 };
 template <int N>
@@ -888,6 +958,28 @@ __global__ void k_combine(const Grid g, const Combine a)
     }
     if (k == g.KE) a.X[1][c] = a.S4[1][c];
 }
+// the same combine in double-double arithmetic (hi parts in a, lo parts in l)
+__global__ void k_combine_dd(const Grid g, const Combine a, const Combine l)
+{
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int n = g.KMAX * g.IMAX * g.JMAX;
+    if (t >= n) return;
+    const int k = g.KS + t % g.KMAX, i = g.IS + (t / g.KMAX) % g.IMAX, j = g.JS + t / (g.KMAX * g.IMAX);
+    const size_t c = idx3(g, k, i, j);
+    for (int v = 0; v < 5; ++v) {
+        if (v == 1 && k == g.KE) continue;
+        const DD s1(a.S1[v][c], l.S1[v][c]), s2(a.S2[v][c], l.S2[v][c]), s3(a.S3[v][c], l.S3[v][c]);
+        const DD s4(a.S4[v][c], l.S4[v][c]), x0(a.X[v][c], l.X[v][c]);
+        const DD acc = ((s1 * DD(2.0)) + s2 * DD(4.0)) + s3 * DD(2.0);
+        const DD r = ((acc + s4) - x0 * DD(3.0)) / DD(6.0);
+        a.X[v][c] = r.hi;
+        l.X[v][c] = r.lo;
+    }
+    if (k == g.KE) {
+        a.X[1][c] = a.S4[1][c];
+        l.X[1][c] = l.S4[1][c];
+    }
+}
 // its adjoint: lam(Xs) = w_s lam(X)/6 and lam(X) = -3 lam(X)/6 on the interior
 struct CombineAdj {
     double *L[5];
@@ -970,7 +1062,7 @@ __global__ void k_vbc_adj(const Grid g, const FieldPtrs fl)
 // ============================================================================
 namespace {
 
-enum Mode { M_FWD, M_TLM, M_ADJ };
+enum Mode { M_FWD, M_TLM, M_ADJ, M_DD };
 
 template <class P, class IOT>
 cudaError_t pass(const Ctx &x, Box b, cudaStream_t st)
@@ -988,6 +1080,7 @@ cudaError_t run(Mode m, const Ctx &x, Box b, cudaStream_t st)
     switch (m) {
     case M_FWD: return pass<P, FwdIO>(x, b, st);
     case M_TLM: return pass<P, TlmIO>(x, b, st);
+    case M_DD: return pass<P, DdIO>(x, b, st);
     default: return pass<P, AdjIO<NJ>>(x, b, st);
     }
 }
@@ -1040,6 +1133,7 @@ cudaError_t stage_fwd(Mode m, const Ctx &x, cudaStream_t st)
     {
         const int n = g.IMAX * g.JMAX;
         if (m == M_TLM) k_column<S, TlmIO><<<(n + 127) / 128, 128, 0, st>>>(x);
+        else if (m == M_DD) k_column<S, DdIO><<<(n + 127) / 128, 128, 0, st>>>(x);
         else k_column<S, FwdIO><<<(n + 127) / 128, 128, 0, st>>>(x);
         RUN(cudaGetLastError());
     }
@@ -1178,14 +1272,16 @@ static void bind_state(Ctx &x, int first, double *v, double *a, size_t N3)
     }
 }
 
+// one forward (M_FWD), tangent-linear (M_TLM: dX the tangent) or double-double
+// (M_DD: dX the lo parts of X) short step in pass form
 template <int S>
-static cudaError_t step_tlm_impl(const Model &M, double *X, double *dX, bool tangent)
+static cudaError_t step_tlm_impl(const Model &M, double *X, double *dX, Mode m)
 {
     cudaStream_t st = M.stream;
     const size_t N3 = n3(M.g);
     Bind b = make_bind(M);
     Ctx &x = b.x;
-    const Mode m = tangent ? M_TLM : M_FWD;
+    const bool tangent = m != M_FWD; // the aux arrays are bound and carried
     const Members one{};
     // numerical filter of the step's start state, then the halo of num_diff
     bind_state(x, XD, X, dX, N3);
@@ -1218,8 +1314,7 @@ static cudaError_t step_tlm_impl(const Model &M, double *X, double *dX, bool tan
         }
     }
     const int n = M.g.KMAX * M.g.IMAX * M.g.JMAX;
-    for (int pass_ = 0; pass_ < (tangent ? 2 : 1); ++pass_) {
-        double *Xp = pass_ ? dX : X, *Sp = pass_ ? b.xs_a : b.xs_v;
+    auto combine_of = [&](double *Xp, double *Sp) {
         Combine cb{};
         for (int q = 0; q < 5; ++q) {
             cb.X[q] = Xp + (size_t)q * N3;
@@ -1228,8 +1323,18 @@ static cudaError_t step_tlm_impl(const Model &M, double *X, double *dX, bool tan
             cb.S3[q] = Sp + (size_t)(10 + q) * N3;
             cb.S4[q] = Sp + (size_t)(15 + q) * N3;
         }
-        k_combine<<<(n + 127) / 128, 128, 0, st>>>(M.g, cb);
+        return cb;
+    };
+    if (m == M_DD) {
+        k_combine_dd<<<(n + 127) / 128, 128, 0, st>>>(M.g, combine_of(X, b.xs_v), combine_of(dX, b.xs_a));
         RUN(cudaGetLastError());
+    }
+    for (int pass_ = 0; pass_ < (tangent ? 2 : 1); ++pass_) {
+        double *Xp = pass_ ? dX : X, *Sp = pass_ ? b.xs_a : b.xs_v;
+        if (m != M_DD) {
+            k_combine<<<(n + 127) / 128, 128, 0, st>>>(M.g, combine_of(Xp, Sp));
+            RUN(cudaGetLastError());
+        }
         double *f[5];
         for (int q = 0; q < 5; ++q) f[q] = Xp + (size_t)q * N3;
         vertical_bc(M.g, one, f[0], f[1], f[2], f[3], f[4], st);
@@ -1334,11 +1439,15 @@ static cudaError_t by_scheme(int scheme, F f)
 }
 cudaError_t step_forward(const Model &M, double *X)
 {
-    return by_scheme(M.scheme, [&](auto s) { return step_tlm_impl<decltype(s)::value>(M, X, nullptr, false); });
+    return by_scheme(M.scheme, [&](auto s) { return step_tlm_impl<decltype(s)::value>(M, X, nullptr, M_FWD); });
 }
 cudaError_t step_tlm(const Model &M, double *X, double *dX)
 {
-    return by_scheme(M.scheme, [&](auto s) { return step_tlm_impl<decltype(s)::value>(M, X, dX, true); });
+    return by_scheme(M.scheme, [&](auto s) { return step_tlm_impl<decltype(s)::value>(M, X, dX, M_TLM); });
+}
+cudaError_t step_dd(const Model &M, double *X_hi, double *X_lo)
+{
+    return by_scheme(M.scheme, [&](auto s) { return step_tlm_impl<decltype(s)::value>(M, X_hi, X_lo, M_DD); });
 }
 cudaError_t step_adjoint(const Model &M, const double *X, double *lam)
 {

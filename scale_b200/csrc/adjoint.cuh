@@ -27,6 +27,8 @@ size_t scratch_fields();
 cudaError_t step_forward(const Model &M, double *X);
 // X and its tangent dX advanced one step
 cudaError_t step_tlm(const Model &M, double *X, double *dX);
+// one short step in double-double arithmetic: X_hi + X_lo in and out
+cudaError_t step_dd(const Model &M, double *X_hi, double *X_lo);
 // lam (adjoint of the state after the step) replaced by the adjoint of the
 // state X at the step's start
 cudaError_t step_adjoint(const Model &M, const double *X, double *lam);

@@ -1943,6 +1943,14 @@ int scale_hevi_short_step_tlm_dev(double *X, double *dX)
     return SCALE_HEVI_OK;
 }
 
+int scale_hevi_short_step_dd_dev(double *X_hi, double *X_lo)
+{
+    CK(ad_prepare());
+    if (!X_hi || !X_lo) return fail(SCALE_HEVI_ERR_ARG, "X_hi or X_lo is NULL");
+    CU(ad::step_dd(C.adm, X_hi, X_lo));
+    return SCALE_HEVI_OK;
+}
+
 int scale_hevi_short_step_adjoint_dev(const double *X, double *lam)
 {
     CK(ad_prepare());

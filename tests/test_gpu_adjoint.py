@@ -131,3 +131,40 @@ def test_gradient_against_finite_differences_with_checkpoints(scheme):
             assert (a - c_).abs().max().item() <= 1e-12 * scale
     finally:
         hevi.finalize()
+
+
+def test_double_double_step_agrees_with_the_pass_form(model):
+    """The double-double step (hi + lo) rounds to the FP64 pass-form step: the
+    two differ by the FP64 model's own rounding, far below 1e-10 of each field."""
+    import torch
+
+    X = model.state()
+    model.boundary(X)
+    hi, lo = X.clone(), torch.zeros_like(X)
+    Y = X.clone()
+    for _ in range(3):
+        model.step_passes(Y)
+        model.step_dd(hi, lo)
+    hevi.check()
+    n = model.n3
+    for q in range(5):
+        a, b = Y[q * n:(q + 1) * n], hi[q * n:(q + 1) * n] + lo[q * n:(q + 1) * n]
+        scale = max(b.abs().max().item(), 1e-300)
+        assert (a - b).abs().max().item() <= 1e-10 * scale, q
+        # the lo parts are small next to the hi parts
+        assert lo[q * n:(q + 1) * n].abs().max().item() <= 1e-15 * scale, q
+
+
+def test_gradient_against_double_double_differences():
+    """With both perturbed runs in double-double arithmetic the central
+    difference at eps = 1e-6 carries no FP64 rounding of the forward model:
+    the adjoint gradient (CD4) agrees with it to 1e-6."""
+    c = _case("CD4", 24, 24, 20)
+    hevi.setup(c.g.index_dict(), c.scheme, c.scheme_tracer)
+    try:
+        p = adjoint.Problem(c, nsteps=12, K=4, box=((3e3, 9e3), (3e3, 9e3), (1e3, 3e3)), spinup=5)
+        r = adjoint.gradient_check(p, ndirs=4, eps=1e-6, dd=True)
+        print("gradient vs double-double central differences:", [f"{row['rel_err']:.2e}" for row in r["directions"]])
+        assert r["max_rel_err"] < 1e-6, r
+    finally:
+        hevi.finalize()
