@@ -539,8 +539,28 @@ def run_tracer(args, c, hevi, torch, X, mflx, g, cells, stream, t0, t1, dist, wo
     rq = [hevi.domain_sum_dev(X["DENS"] * qt[n * N3:(n + 1) * N3], g.CDZ, g.CDX, g.CDY) for n in range(c.QA)]
     rq0 = [hevi.domain_sum_dev(dens0 * q_start[n], g.CDZ, g.CDX, g.CDY) for n in range(c.QA)]
 
-    # the same large steps with FP32 flux and limiter arithmetic, from the same start
+    # the same large steps with the three-kernel limiter (phi_lo and the
+    # anti-diffusive fluxes through HBM), from the same start: its time, and
+    # the fused form's result against it (identical bits expected)
     q64 = qt.clone()
+    hevi.tracer_fct_form(False)
+    try:
+        qt.copy_(q0)
+        torch.cuda.synchronize()
+        t0.record(stream)
+        for _ in range(k):
+            large_step()
+        t1.record(stream)
+        torch.cuda.synchronize()
+        hevi.check()
+    finally:
+        hevi.tracer_fct_form(True)
+    ms3 = max_over_ranks(t0.elapsed_time(t1), dist, "cuda") / k / c.QA
+    three_kernel = {"ms_per_tracer_large_step": ms3, "fused_speedup": ms3 / ms_tracer,
+                    "fused_result_identical": bool(torch.equal(qt, q64))}
+    qt.copy_(q64)
+
+    # the same large steps with FP32 flux and limiter arithmetic, from the same start
     kw32 = dict(kw, RHOQ_t=zero.float(), mflx_hi=mflx.float(), num_diff=ndq.float())
 
     def large_step_mixed():
@@ -570,12 +590,14 @@ def run_tracer(args, c, hevi, torch, X, mflx, g, cells, stream, t0, t1, dist, wo
         "value": aggregate_rate(cells, world, 1, ms_tracer), "unit": "cell-updates/s per tracer",
         "ms_per_tracer_large_step": ms_tracer, "ms_per_large_step": ms, "tracers": c.QA, "large_steps": k,
         "step": "ATMOS_DYN_Tinteg_tracer_rk3 (3 RK stages, UD3 fluxes, FCT along-stream), dtl = 2.5 s, FP64",
-        "roofline": {"bound": "hbm", "kernel": "tracer RK3 with FCT (k_tracer_plain x2, k_fct_lo, k_fct_r, "
-                     "k_fct_apply, halos)", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
+        "roofline": {"bound": "hbm", "kernel": "tracer RK3 with FCT (k_tracer_plain x2, k_fct_limit, R+/R- halo, "
+                     "k_fct_update, halos)", "achieved": ach, "peak": hbm, "unit": "GB/s", "frac": ach / hbm,
                      "algorithmic_bytes_per_cell": TRACER_BYTES},
         "kernel_launches_per_tracer_step": launches / (k * c.QA),
         "min_tracer_after": qmin, "tracer_mass_change_rel": [(a - b) / b if b else 0.0 for a, b in zip(rq, rq0)],
         "sections_ms_per_large_step": {kk: v[1] / k for kk, v in prof.items()},
+        "limiter_form": "fused (k_fct_limit, R+/R- halo, k_fct_update)",
+        "three_kernel_limiter": three_kernel,
         "mixed": mixed,
     }
 

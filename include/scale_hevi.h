@@ -493,6 +493,16 @@ int scale_hevi_ensemble_layout(long long *cell0, long long *col0, long long *z0,
  * column kernel. The results are identical. */
 int scale_hevi_numfilter_form(int tiled);
 
+/* The form of the FCT-limited tracer stage (ATMOS_DYN_fct inside
+ * ATMOS_DYN_Tstep_tracer_fvm_heve, scale_atmos_dyn_common.F90:1922-2734; no
+ * counterpart switch in the reference): 1, the default after setup, runs the
+ * limiter fused with the fluxes (one kernel forms phi_lo, the anti-diffusive
+ * fluxes and R+/R- from QTRC0 rows staged by bulk tensor copies, a second
+ * limits and updates) wherever QTRC0 admits a tensor map (16-byte aligned
+ * base, even KA); 0 keeps the three-kernel form (phi_lo and the
+ * anti-diffusive fluxes through HBM). The FP64 results are identical. */
+int scale_hevi_tracer_fct_form(int fused);
+
 int scale_hevi_short_step_persistent_dev(SCALE_HEVI_SHORT_STEP_ARGS);
 int scale_hevi_short_step_persistent_mixed_dev(SCALE_HEVI_SHORT_STEP_MIXED_ARGS);
 int scale_hevi_persistent_wait(const double *seconds, const int *extra_arrivals);

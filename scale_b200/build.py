@@ -39,7 +39,7 @@ CPP_SOURCES = ["grid_coef.cpp"]
 # held to a tolerance against the FP64 path, not bit for bit, so a*b+c may fuse.
 FLOAT_SOURCES = ["hevi_stage.cu", "hevi_tma.cu", "numfilter.cu", "tracer.cu", "persist.cu"]
 HEADERS = ["hevi_common.cuh", "hevi_stage.cuh", "hevi_kernels.cuh", "hevi_epilogue.cuh", "adjoint.cuh",
-           "numfilter_body.cuh", "fill_body.cuh", "hevi_stage_body.cuh", "grid_coef.h"]
+           "numfilter_body.cuh", "fill_body.cuh", "hevi_stage_body.cuh", "tma_util.cuh", "grid_coef.h"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 

@@ -113,6 +113,7 @@ struct Ctx {
     unsigned pextra = 0;
     int pgrid = 0; // CTAs of the last persistent launch
     bool nd_tiled = true; // the filter's tiled form where it applies (scale_hevi_numfilter_form)
+    bool fct_fused = true; // the limiter's fused form where it applies (scale_hevi_tracer_fct_form)
 };
 
 Ctx C;
@@ -792,17 +793,22 @@ int run_tracer_rk3(double *QTRC, const double *QTRC0, const R *RHOQ_t, const dou
     CK(halo(&rk2, 1));
     // stage 3: dt with DENS, FCT when requested
     a.QTRCo = QTRC; a.QTRC = rk2; a.dens_mode = 0; a.dtl = dtl;
+    a.status = C.fct_fused ? C.status : nullptr;
+    int nk = 0;
     if (fct && C.halo_fn) {
         // a decomposed domain: R+/R- go through the exchange between the limiter's kernels
         int hrc = SCALE_HEVI_OK;
         const HaloFill hf{hook_fill, &hrc};
-        const cudaError_t e = launch_tracer_stage(C.g, a, C.scheme_tracer, fct, C.stream, &hf);
+        const cudaError_t e = launch_tracer_stage(C.g, a, C.scheme_tracer, fct, C.stream, &hf, &nk);
         if (hrc != SCALE_HEVI_OK) return hrc;
         CU(e);
     } else {
-        CK(timed(fct ? sec_fct : sec, [&] { CU(launch_tracer_stage(C.g, a, C.scheme_tracer, fct, C.stream)); return SCALE_HEVI_OK; }));
+        CK(timed(fct ? sec_fct : sec, [&] {
+            CU(launch_tracer_stage(C.g, a, C.scheme_tracer, fct, C.stream, nullptr, &nk));
+            return SCALE_HEVI_OK;
+        }));
     }
-    C.launches += fct ? 4 : 1;
+    C.launches += nk;
     return SCALE_HEVI_OK;
 }
 
@@ -1375,6 +1381,13 @@ int scale_hevi_numfilter_form(int tiled)
     return SCALE_HEVI_OK;
 }
 
+int scale_hevi_tracer_fct_form(int fused)
+{
+    CK(need_setup());
+    C.fct_fused = fused != 0;
+    return SCALE_HEVI_OK;
+}
+
 int scale_hevi_persistent_grid(int *ctas)
 {
     CK(need_setup());
@@ -1477,13 +1490,14 @@ int ATMOS_DYN_Tstep_tracer_fvm_heve_b200_dev(SCALE_HEVI_TSTEP_TRACER_ARGS)
     a.along_stream = *FLAG_FCT_ALONG_STREAM ? 1 : 0;
     a.GS = dGS;
     a.MAPF = dMAPF;
+    a.status = C.fct_fused ? C.status : nullptr;
     const bool fct = *FLAG_FCT_TRACER != 0;
-    int hrc = SCALE_HEVI_OK;
+    int hrc = SCALE_HEVI_OK, nk = 0;
     const HaloFill hf{hook_fill, &hrc};
-    const cudaError_t e = launch_tracer_stage(C.g, a, C.scheme_tracer, fct, C.stream, C.halo_fn ? &hf : nullptr);
+    const cudaError_t e = launch_tracer_stage(C.g, a, C.scheme_tracer, fct, C.stream, C.halo_fn ? &hf : nullptr, &nk);
     if (hrc != SCALE_HEVI_OK) return hrc;
     CU(e);
-    C.launches += fct ? 4 : 1;
+    C.launches += nk;
     return SCALE_HEVI_OK;
 }
 

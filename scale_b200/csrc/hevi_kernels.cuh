@@ -141,11 +141,16 @@ struct TracerArgsT {
     // terrain-following metrics, null on flat terrain: GSQRT (KA,IA,JA,7) and
     // the MAPF slice (IA,JA,2) of the mass points (FP64 path only)
     const double *GS, *MAPF;
+    // device status word: with it, a limited stage runs the fused form
+    // (k_fct_limit, R+/R- halo, k_fct_update) where QTRC0 admits a tensor map
+    // and records a staging timeout there; null keeps the three-kernel form
+    unsigned *status;
 };
 using TracerArgs = TracerArgsT<double>;
+// one stage; *nk (when given) receives the number of kernels it launched
 template <typename R>
 cudaError_t launch_tracer_stage(const Grid &g, const TracerArgsT<R> &a, int scheme, bool fct, cudaStream_t st,
-                                const HaloFill *fill = nullptr);
+                                const HaloFill *fill = nullptr, int *nk = nullptr);
 // ATMOS_DYN_divergence with every metric term (misc.cu)
 void divergence_terrain(const Grid &g, double *DDIV, const double *MOMZ, const double *MOMX, const double *MOMY,
                         const Metrics &M, double J33G, cudaStream_t st);

@@ -5,14 +5,24 @@
 //
 // A stage without FCT is one kernel (every cell forms its six face fluxes and
 // updates). With FCT the limiter needs the low-order solution and the
-// limiting factors of the neighbours, so it runs as three kernels around the
-// halo fill of R+/R- (the reference's mid-limiter COMM_vars8, :2558-2561):
-//   k_fct_lo    low-order update phi_lo on the halo-extended region and the
-//               raw anti-diffusive fluxes of every face an interior cell owns
-//   k_fct_r     P+/P-, the along-stream (or 7-point) bounds Q+/Q-, R+/R-
-//   k_fct_apply limit the anti-diffusive fluxes and update the tracer
-// Terrain-following metrics (TracerArgsT::GS, MAPF) enter the num_diff terms and
-// the metric factor of every flux divergence; null pointers mean flat terrain.
+// limiting factors of the neighbours, so the stage splits at the halo fill of
+// R+/R- (the reference's mid-limiter COMM_vars8, :2558-2561). Its fused form:
+//   k_fct_limit   a CTA owns 8 columns x 32 levels and marches along j over a
+//                 strip of rows; QTRC0 rows come into a ring in shared memory
+//                 by bulk tensor copies (TMA, two rows ahead, bounded mbarrier
+//                 waits). Per row it forms the low-order solution phi_lo of the
+//                 tile and a halo of one in shared memory, the high- and
+//                 low-order fluxes of every face of the tile and their
+//                 differences (the anti-diffusive fluxes, z by warp shuffle, y
+//                 carried from the row before), and from them P+/P-, the
+//                 along-stream or 7-point bounds Q+/Q- and R+/R-. Only R+/R-
+//                 leave the kernel.
+//   k_fct_update  forms each face's high- and low-order fluxes again, limits
+//                 their difference with R+/R- and updates the tracer.
+// The three-kernel form (k_fct_lo: phi_lo and the anti-diffusive fluxes to
+// HBM; k_fct_r: R+/R-; k_fct_apply) runs where QTRC0 admits no tensor map or
+// no status word is given. Both forms evaluate every value with the same
+// operations in the same order: on the FP64 path they give identical bits.
 //
 // R is the type of the flux and limiter arithmetic and of the flux-like arrays:
 // double on the plain path (bit-identical to the oracle), float on the
@@ -24,6 +34,7 @@
 // at the resolution of the FP64 state, and FP32's own epsilon would switch off
 // the limiting of every change below 1.2e-7 that the FP64 path limits.
 #include "hevi_kernels.cuh"
+#include "tma_util.cuh"
 
 namespace hevi {
 
@@ -82,13 +93,18 @@ __device__ __forceinline__ R hflux_h(const TracerArgsT<R> &a, size_t N3, int dir
                         W6 ? R(ld(q + 3 * s)) : R(0.0))
            + ndq_at(a, N3, dir, c);
 }
-// donor-cell flux at the face between c and c+s (ud1.F90:155-165)
+// donor-cell flux of mass flux vel between the values lo (below / west /
+// south) and hi (ud1.F90:155-165)
+template <typename R>
+__device__ __forceinline__ R lflux_v(R vel, R lo, R hi)
+{
+    return vel * (R(0.5) * (hi + lo) - fsign(R(0.5), vel) * (hi - lo));
+}
+// donor-cell flux at the face between c and c+s
 template <typename R>
 __device__ __forceinline__ R lflux(const TracerArgsT<R> &a, size_t N3, int dir, size_t c, long s)
 {
-    const R vel = ld(a.mflx + (size_t)dir * N3 + c);
-    const R lo = R(ld(a.QTRC0 + c)), hi = R(ld(a.QTRC0 + c + s));
-    return vel * (R(0.5) * (hi + lo) - fsign(R(0.5), vel) * (hi - lo));
+    return lflux_v(ld(a.mflx + (size_t)dir * N3 + c), R(ld(a.QTRC0 + c)), R(ld(a.QTRC0 + c + s)));
 }
 
 // ---- stage without FCT, tstep_tracer_fvm_heve.F90:214-236 -------------------
@@ -325,17 +341,319 @@ __global__ void __launch_bounds__(128) k_fct_apply(const Grid g, const TracerArg
     }
 }
 
-template <int S, typename R>
-static cudaError_t tracer_stage(const Grid &g, const TracerArgsT<R> &a, bool fct, cudaStream_t st, const HaloFill *fill)
+// =============================================================================
+// fused form: k_fct_limit, k_fct_update
+// =============================================================================
+namespace fct {
+#ifndef HEVI_FCT_JB
+#define HEVI_FCT_JB 16
+#endif
+// tile width and CTAs per SM (measured on 512x512x128, UD3, along-stream):
+// FP64 8 columns, 4 CTAs (64 registers); FP32 4 columns, 8 CTAs
+#ifndef HEVI_FCT_FW
+#ifdef HEVI_FLOAT_TU
+#define HEVI_FCT_FW 4
+#define HEVI_FCT_MINB 8
+#else
+#define HEVI_FCT_FW 8
+#define HEVI_FCT_MINB 4
+#endif
+#endif
+constexpr int FW = HEVI_FCT_FW;  // tile columns along i, one warp each
+constexpr int KC = 32;           // levels of a CTA, one per lane
+constexpr int BK = 38;           // staged levels of a QTRC0 row (a 16-byte multiple) from L0-2 or one below
+constexpr int BW = FW + 4;       // staged columns: i0-2 .. i0+FW+1
+constexpr int SLOT = (BK * BW + 15) / 16 * 16; // doubles per staged row, padded to 128 bytes
+constexpr int NS = 6;            // staged rows in the ring
+constexpr int PK = KC + 2;       // phi_lo levels: L0-1 .. L0+KC
+constexpr int PW = FW + 2;       // phi_lo columns: i0-1 .. i0+FW
+constexpr int NP = 4;            // phi_lo rows in the ring
+constexpr int JB = HEVI_FCT_JB;  // rows of a CTA's strip
+constexpr unsigned ROW_BYTES = BK * BW * sizeof(double);
+template <typename R> constexpr size_t smem_bytes()
 {
-    dim3 b(32, 4), gr((g.IMAX + 3) / 4, g.JMAX);
-    if (!fct) {
-        k_tracer_plain<S, R><<<gr, b, 0, st>>>(g, a);
-        return cudaGetLastError();
+    return (size_t)NS * SLOT * sizeof(double) + NS * sizeof(uint64_t) + (size_t)NP * PW * PK * sizeof(R)
+           + (size_t)(FW + 1) * KC * sizeof(R);
+}
+}  // namespace fct
+
+// the along-stream weighted sums qa and qb of one field around a cell
+// (common.F90:2143-2170; the same terms at KS and KE with ka, kb clamped);
+// v(dk, di, dj) is the field at (k+dk, i+di, j+dj). qb reads (k, i-1, j-1)
+// for fact(0,1,-1) and (k-1, i, j-1) for fact(1,0,-1) as the reference does.
+template <typename R, class V>
+__device__ __forceinline__ R qa_sum(const R (&f)[2][3][3], int ka, const V &v)
+{
+#define FA(x, y, z) f[x][(y) + 1][(z) + 1]
+    return FA(1, 1, 1) * v(ka, 1, 1) + FA(0, 1, 1) * v(0, 1, 1) + FA(1, 0, 1) * v(ka, 0, 1) + FA(0, 0, 1) * v(0, 0, 1)
+           + FA(1, -1, 1) * v(ka, -1, 1) + FA(1, 1, 0) * v(ka, 1, 0) + FA(0, 1, 0) * v(0, 1, 0)
+           + FA(1, 0, 0) * v(ka, 0, 0) + FA(1, -1, 0) * v(ka, -1, 0) + FA(1, 1, -1) * v(ka, 1, -1)
+           + FA(0, 1, -1) * v(0, 1, -1) + FA(1, 0, -1) * v(ka, 0, -1) + FA(1, -1, -1) * v(ka, -1, -1)
+           + FA(0, 0, 0) * v(0, 0, 0);
+}
+template <typename R, class V>
+__device__ __forceinline__ R qb_sum(const R (&f)[2][3][3], int kb, const V &v)
+{
+    return FA(1, 1, 1) * v(kb, -1, -1) + FA(0, 1, 1) * v(0, -1, -1) + FA(1, 0, 1) * v(kb, 0, -1)
+           + FA(0, 0, 1) * v(0, 0, -1) + FA(1, -1, 1) * v(kb, 1, -1) + FA(1, 1, 0) * v(kb, -1, 0)
+           + FA(0, 1, 0) * v(0, -1, 0) + FA(1, 0, 0) * v(kb, 0, 0) + FA(1, -1, 0) * v(kb, 1, 0)
+           + FA(1, 1, -1) * v(kb, -1, 1) + FA(0, 1, -1) * v(0, -1, -1) + FA(1, 0, -1) * v(kb, 0, -1)
+           + FA(1, -1, -1) * v(kb, 1, 1) + FA(0, 0, 0) * v(0, 0, 0);
+#undef FA
+}
+
+// R+/R- of the cells of a strip (common.F90:1990-2553 without the halo fill),
+// and R(QTRC0) of the cells and their lateral halo ring into the phi_lo
+// scratch for k_fct_update (phi_lo itself stays in shared memory).
+// Block (32, FW): lane = level L0+lane, warp w = column i0+w; the CTA marches
+// over rows jb0 .. jb0+nrow-1. Iteration t forms phi_lo of row r = jb0-1+t and,
+// from t = 2, R+/R- of row o = r-1. QTRC0 row jb0-2+rr sits in ring slot
+// rr % NS (mbarrier rr % NS, phase rr / NS); rows rr = 0..3 are copied before
+// the march and row t+4 after the first barrier of iteration t, so a slot is
+// refilled only after the iteration that last read it has ended everywhere.
+template <int S, typename R>
+__global__ void __launch_bounds__(32 * fct::FW, HEVI_FCT_MINB)
+    k_fct_limit(const Grid g, const TracerArgsT<R> a, const __grid_constant__ CUtensorMap map)
+{
+    using namespace fct;
+    using namespace tma;
+    extern __shared__ __align__(1024) double fsm[];
+    double *spi = fsm;                                               // QTRC0 rows [slot][i][k]
+    uint64_t *bar = reinterpret_cast<uint64_t *>(spi + NS * SLOT);   // one mbarrier per slot
+    R *spl = reinterpret_cast<R *>(bar + NS);                        // phi_lo rows [slot][i][k]
+    R *sax = spl + NP * PW * PK;                                     // x anti-diffusive flux [face][lane]
+    __shared__ int s_ok;
+    const int lane = threadIdx.x, w = threadIdx.y, tid = w * 32 + lane;
+    const int nti = (g.IMAX + FW - 1) / FW;
+    const int i0 = g.IS + ((int)blockIdx.x % nti) * FW, L0 = g.KS + ((int)blockIdx.x / nti) * KC;
+    const int jb0 = g.JS + (int)blockIdx.y * JB;
+    const int nrow = min(JB, g.JE - jb0 + 1);
+    const int rlast = nrow + 3;        // last ring row: QTRC0 rows jb0-2 .. jb0+nrow+1
+    const int kx = (L0 - 3) & ~1;      // 0-based first staged level (level L0-2 or one below): even, a 16-byte start
+    const int KS = g.KS, KE = g.KE;
+    const size_t N3 = n3(g);
+    const long sI = g.KA, sJ = (long)g.KA * g.IA;
+    const R *mZ = a.mflx, *mX = a.mflx + N3, *mY = a.mflx + 2 * N3;
+
+    auto issue = [&](int rr) { // thread 0
+        uint64_t *b = bar + rr % NS;
+        mbar_expect_tx(b, ROW_BYTES);
+        tma_load_3d(spi + (rr % NS) * SLOT, &map, kx, i0 - 3, jb0 - 3 + rr, b);
+    };
+    auto wait_row = [&](int rr) { return mbar_wait(bar + rr % NS, (unsigned)(rr / NS) & 1u); };
+    // staged QTRC0 and phi_lo at level kk, column ii of row j
+    auto PI = [&](int j, int kk, int ii) -> double {
+        return spi[((j - jb0 + 2) % NS) * SLOT + (ii - i0 + 2) * BK + (kk - 1 - kx)];
+    };
+    auto PL = [&](int j, int kk, int ii) -> R { return spl[((j - jb0 + 1) % NP) * (PW * PK) + (ii - i0 + 1) * PK + (kk - L0 + 1)]; };
+
+    if (tid == 0) {
+        for (int q = 0; q < NS; ++q) mbar_init(bar + q, 1);
+        fence_mbar_init();
+        for (int rr = 0; rr < 4; ++rr) issue(rr);
+        const bool ok = wait_row(0) && wait_row(1) && wait_row(2);
+        if (!ok)
+            for (int rr = 0; rr < 4; ++rr) (void)wait_row(rr); // bounded: the copies still in flight
+        s_ok = ok ? 1 : 0;
     }
-    dim3 gl((g.IMAX + 2 + 3) / 4, g.JMAX + 2);
-    k_fct_lo<S, R><<<gl, b, 0, st>>>(g, a);
-    k_fct_r<R><<<gr, b, 0, st>>>(g, a);
+    __syncthreads();
+    if (!s_ok) {
+        if (tid == 0) atomicOr(a.status, ST_TMA_TIMEOUT);
+        return; // block-uniform
+    }
+    for (int rr = 0; rr < 3; ++rr) (void)mbar_try(bar + rr, 0u); // completed phases: the copies are visible here
+
+    const int i = i0 + w, k = L0 + lane;
+    const bool cell = i <= g.IE && k <= KE;
+    const R zero = R(0.0), one = R(1.0), h = R(0.5), eps = eps_of<R>(), dtl = R(a.dtl);
+    const R rdx = cell ? R(ld(g.RCDX + i - 1)) : zero;
+    const R rdz = cell ? R(ld(g.RCDZ + k - 1)) : zero;
+    R ay_prev = zero; // anti-diffusive y flux through the face j+1/2 of the row before
+
+    for (int t = 0; t <= nrow + 1; ++t) {
+        const int r = jb0 - 1 + t;
+        // (a) phi_lo of row r on the tile and a halo of one (common.F90:1990-2073)
+        {
+            R *pl = spl + (t % NP) * (PW * PK);
+            const R rcdy = R(ld(g.RCDY + r - 1));
+            for (int p = tid; p < PW * PK; p += 32 * FW) {
+                const int ii = i0 - 1 + p / PK, kk = L0 - 1 + p % PK;
+                if (ii > g.IE + 1 || kk < KS || kk > KE) continue;
+                const size_t c = idx3(g, kk, ii, r);
+                const R q = R(PI(r, kk, ii));
+                const R lz = kk <= KE - 1 ? lflux_v(ld(mZ + c), q, R(PI(r, kk + 1, ii))) : zero;
+                const R lzm = kk >= KS + 1 ? lflux_v(ld(mZ + c - 1), R(PI(r, kk - 1, ii)), q) : zero;
+                const R lx = lflux_v(ld(mX + c), q, R(PI(r, kk, ii + 1)));
+                const R lxm = lflux_v(ld(mX + c - sI), R(PI(r, kk, ii - 1)), q);
+                const R ly = lflux_v(ld(mY + c), q, R(PI(r + 1, kk, ii)));
+                const R lym = lflux_v(ld(mY + c - sJ), R(PI(r - 1, kk, ii)), q);
+                pl[p] = R((PI(r, kk, ii) * ld(a.DENS0 + c)
+                           + a.dtl * (double)mfac(g, a, -((lz - lzm) * R(ld(g.RCDZ + kk - 1)) + (lx - lxm) * R(ld(g.RCDX + ii - 1))
+                                                          + (ly - lym) * rcdy),
+                                                  ii, r, c))
+                          / ld(a.DENS + c));
+            }
+        }
+        __syncthreads(); // phi_lo of row r in place; every read of iteration t-1 done
+        if (tid == 0 && t + 4 <= rlast) {
+            fence_proxy_async();
+            issue(t + 4);
+        }
+        // (b) anti-diffusive fluxes of the faces of row o's cells (common.F90:2050-2073)
+        const int o = r - 1;
+        const bool out = t >= 2; // block-uniform
+        const size_t c = idx3(g, min(k, KE), min(i, g.IE), o);
+        const size_t col = c - (size_t)(min(k, KE) - 1);
+        R az = zero, azm = zero, ax = zero, ay = zero, aym = zero;
+        if (out) {
+            if (cell && k <= KE - 1)
+                az = hflux_z<S>(g, a, N3, col, k) - lflux_v(ld(mZ + c), R(PI(o, k, i)), R(PI(o, k + 1, i)));
+            azm = __shfl_up_sync(0xffffffffu, az, 1);
+            if (lane == 0)
+                azm = (cell && L0 > KS)
+                          ? hflux_z<S>(g, a, N3, col, L0 - 1) - lflux_v(ld(mZ + c - 1), R(PI(o, L0 - 1, i)), R(PI(o, L0, i)))
+                          : zero;
+            if (cell) {
+                // R(QTRC0) for k_fct_update: this cell and the halo ring its faces reach
+                a.phi_lo[c] = R(PI(o, k, i));
+                if (i == g.IS) a.phi_lo[c - sI] = R(PI(o, k, i - 1));
+                if (i == g.IE) a.phi_lo[c + sI] = R(PI(o, k, i + 1));
+                if (o == g.JS) a.phi_lo[c - sJ] = R(PI(o - 1, k, i));
+                if (o == g.JE) a.phi_lo[c + sJ] = R(PI(o + 1, k, i));
+                ax = hflux_h<S>(a, N3, 1, c, sI) - lflux_v(ld(mX + c), R(PI(o, k, i)), R(PI(o, k, i + 1)));
+                sax[(w + 1) * KC + lane] = ax;
+                if (w == 0)
+                    sax[lane] = hflux_h<S>(a, N3, 1, c - sI, sI) - lflux_v(ld(mX + c - sI), R(PI(o, k, i - 1)), R(PI(o, k, i)));
+                ay = hflux_h<S>(a, N3, 2, c, sJ) - lflux_v(ld(mY + c), R(PI(o, k, i)), R(PI(o + 1, k, i)));
+                aym = t == 2 ? hflux_h<S>(a, N3, 2, c - sJ, sJ) - lflux_v(ld(mY + c - sJ), R(PI(o - 1, k, i)), R(PI(o, k, i)))
+                             : ay_prev;
+                ay_prev = ay;
+            }
+        }
+        if (tid == 0 && t + 3 <= rlast) {
+            const bool ok = wait_row(t + 3);
+            if (!ok)
+                for (int rr = t + 3; rr <= min(t + 4, rlast); ++rr) (void)wait_row(rr); // bounded
+            s_ok = ok ? 1 : 0;
+        }
+        __syncthreads(); // x fluxes in place; QTRC0 row t+3 arrived (or timed out)
+        if (!s_ok) {
+            if (tid == 0) atomicOr(a.status, ST_TMA_TIMEOUT);
+            return; // block-uniform
+        }
+        if (t + 3 <= rlast) (void)mbar_try(bar + (t + 3) % NS, (unsigned)((t + 3) / NS) & 1u);
+        if (!out || !cell) continue;
+
+        // (c) P+/P-, the bounds Q+/Q- and R+/R- of cell (k, i, o) (common.F90:2077-2553)
+        const R axm = sax[w * KC + lane];
+        const R pz = rmax(zero, azm) - rmin(zero, az);
+        const R px = rmax(zero, axm) - rmin(zero, ax);
+        const R py = rmax(zero, aym) - rmin(zero, ay);
+        const R rdy = R(ld(g.RCDY + o - 1));
+        const R pjpls = mfac(g, a, dtl * (pz * rdz + px * rdx + py * rdy), i, o, c);
+        const R mz = rmax(zero, az) - rmin(zero, azm);
+        const R mx = rmax(zero, ax) - rmin(zero, axm);
+        const R my = rmax(zero, ay) - rmin(zero, aym);
+        const R pjmns = mfac(g, a, dtl * (mz * rdz + mx * rdx + my * rdy), i, o, c);
+        const auto vin = [&](int dk, int di, int dj) { return R(PI(o + dj, k + dk, i + di)); };
+        const auto vlo = [&](int dk, int di, int dj) { return PL(o + dj, k + dk, i + di); };
+        const R pin = vin(0, 0, 0), plo = vlo(0, 0, 0);
+        R qmax, qmin;
+        if (a.along_stream) {
+            R rw;
+            int ka, kb;
+            if (k == KS) { rw = ld(mZ + c) * rdz; ka = 1; kb = 0; }
+            else if (k == KE) { rw = ld(mZ + c - 1) * rdz; ka = 0; kb = -1; }
+            else { rw = (ld(mZ + c) + ld(mZ + c - 1)) * rdz; ka = 1; kb = -1; }
+            const R ru = (ld(mX + c) + ld(mX + c - sI)) * rdx;
+            const R rv = (ld(mY + c) + ld(mY + c - sJ)) * rdy;
+            R f[2][3][3];
+            fact_fct(f, rw, ru, rv);
+            const R qa_in = qa_sum(f, ka, vin), qb_in = qb_sum(f, kb, vin);
+            const R qa_lo = qa_sum(f, ka, vlo), qb_lo = qb_sum(f, kb, vlo);
+            qmax = rmax(rmax(rmax(rmax(rmax(pin, qa_in), qb_in), plo), qa_lo), qb_lo);
+            qmin = rmin(rmin(rmin(rmin(rmin(pin, qa_in), qb_in), plo), qa_lo), qb_lo);
+        } else {
+            qmax = rmax(pin, plo);
+            qmin = rmin(pin, plo);
+            const int nb[6][3] = {{1, 0, 0}, {-1, 0, 0}, {0, 1, 0}, {0, -1, 0}, {0, 0, 1}, {0, 0, -1}};
+#pragma unroll
+            for (int n = 0; n < 6; ++n) {
+                if ((k == KS && nb[n][0] == -1) || (k == KE && nb[n][0] == 1)) continue;
+                const R x = vin(nb[n][0], nb[n][1], nb[n][2]), y = vlo(nb[n][0], nb[n][1], nb[n][2]);
+                qmax = rmax(rmax(qmax, x), y);
+                qmin = rmin(rmin(qmin, x), y);
+            }
+        }
+        const R dn = R(ld(a.DENS + c));
+        const R qjpls = (qmax - plo) * dn;
+        const R qjmns = (plo - qmin) * dn;
+        R zerosw = h - fsign(h, pjpls - eps);
+        a.rjp[c] = rmin(one, qjpls * (one - zerosw) / (pjpls - zerosw));
+        zerosw = h - fsign(h, pjmns - eps);
+        a.rjm[c] = rmin(one, qjmns * (one - zerosw) / (pjmns - zerosw));
+    }
+}
+
+// limit and update (tstep_tracer_fvm_heve.F90:188-210) with the anti-diffusive
+// fluxes formed again from the high- and low-order fluxes; the z fluxes of
+// the face below a level come from the previous lane (lane 0: the previous
+// pass's lane 31; zero below KS). The low-order fluxes read R(QTRC0) from the
+// copy k_fct_limit left in the phi_lo scratch, not QTRC0 itself: QTRCo may be
+// QTRC0 (the RK3 integrator updates the tracer in place), and a neighbour's
+// value there may already be the new one. Each cell's own QTRC0 is read
+// before its own write.
+template <int S, typename R>
+__global__ void __launch_bounds__(128) k_fct_update(const Grid g, const TracerArgsT<R> a)
+{
+    const int i = g.IS + blockIdx.x * blockDim.y + threadIdx.y;
+    const int j = g.JS + blockIdx.y;
+    if (i > g.IE) return;
+    const size_t N3 = n3(g);
+    const long sI = g.KA, sJ = (long)g.KA * g.IA;
+    const size_t col = idx3(g, 1, i, j);
+    const R rcdx = R(ld(g.RCDX + i - 1)), rcdy = R(ld(g.RCDY + j - 1));
+    const R *q0 = a.phi_lo; // R(QTRC0)
+    // donor-cell flux at the face between c and c+s
+    auto lf = [&](int dir, size_t c, long s) {
+        return lflux_v(ld(a.mflx + (size_t)dir * N3 + c), ld(q0 + c), ld(q0 + c + s));
+    };
+    R carry_h = R(0.0), carry_a = R(0.0);
+    for (int k0 = g.KS; k0 <= g.KE; k0 += 32) {
+        const int k = k0 + threadIdx.x;
+        const bool ok = k <= g.KE;
+        const size_t c = col + k - 1;
+        R hz = R(0.0), az = R(0.0);
+        if (ok) {
+            hz = hflux_z<S>(g, a, N3, col, k);
+            if (k <= g.KE - 1) az = limit(a, hz - lf(0, c, 1), c, 1);
+        }
+        R hzm = __shfl_up_sync(0xffffffffu, hz, 1), azm = __shfl_up_sync(0xffffffffu, az, 1);
+        if (threadIdx.x == 0) {
+            hzm = carry_h;
+            azm = carry_a;
+        }
+        carry_h = __shfl_sync(0xffffffffu, hz, 31);
+        carry_a = __shfl_sync(0xffffffffu, az, 31);
+        if (!ok) continue;
+        const R hx = hflux_h<S>(a, N3, 1, c, sI), hxm = hflux_h<S>(a, N3, 1, c - sI, sI);
+        const R hy = hflux_h<S>(a, N3, 2, c, sJ), hym = hflux_h<S>(a, N3, 2, c - sJ, sJ);
+        const R ax = limit(a, hx - lf(1, c, sI), c, sI);
+        const R axm = limit(a, hxm - lf(1, c - sI, sI), c - sI, sI);
+        const R ay = limit(a, hy - lf(2, c, sJ), c, sJ);
+        const R aym = limit(a, hym - lf(2, c - sJ, sJ), c - sJ, sJ);
+        const R div = (hz - az - hzm + azm) * R(ld(g.RCDZ + k - 1)) + (hx - ax - hxm + axm) * rcdx
+                      + (hy - ay - hym + aym) * rcdy;
+        a.QTRCo[c] = (ld(a.QTRC0 + c) * ld(a.DENS0 + c) + a.dtl * (double)(mfac(g, a, -div, i, j, c) + ld(a.RHOQ_t + c)))
+                     / ld(a.DENS + c);
+    }
+}
+
+// the halo of R+/R- between the limiter's kernels: the exchange hook of a
+// decomposed domain, else the periodic fill (one launch)
+template <typename R>
+static cudaError_t fill_r(const Grid &g, const TracerArgsT<R> &a, cudaStream_t st, const HaloFill *fill, int &nk)
+{
     R *rr[2] = {a.rjp, a.rjm};
     if (fill) {
         cudaError_t e = cudaGetLastError();
@@ -343,31 +661,80 @@ static cudaError_t tracer_stage(const Grid &g, const TracerArgsT<R> &a, bool fct
         if (fill->fn(fill->ctx, reinterpret_cast<void *const *>(rr), 2, (int)sizeof(R))) return cudaErrorUnknown;
     } else {
         periodic_halo(g, Members{}, rr, 2, st);
+        ++nk;
     }
+    return cudaSuccess;
+}
+
+// the fused form of a limited stage; cudaErrorNotSupported (nothing launched)
+// without a status word or where QTRC0 admits no tensor map (even KA, a
+// 16-byte aligned base)
+template <int S, typename R>
+static cudaError_t fct_fused(const Grid &g, const TracerArgsT<R> &a, cudaStream_t st, const HaloFill *fill, int &nk)
+{
+    CUtensorMap map;
+    if (!a.status || !tma::encode(&map, a.QTRC0, g, fct::BK, fct::BW, 1)) return cudaErrorNotSupported;
+    const dim3 gf((unsigned)(((g.IMAX + fct::FW - 1) / fct::FW) * ((g.KMAX + fct::KC - 1) / fct::KC)),
+                  (unsigned)((g.JMAX + fct::JB - 1) / fct::JB));
+    auto kl = k_fct_limit<S, R>;
+    cudaError_t e = tma::open_smem(kl, fct::smem_bytes<R>());
+    if (e != cudaSuccess) return e;
+    kl<<<gf, dim3(32, fct::FW), fct::smem_bytes<R>(), st>>>(g, a, map);
+    ++nk;
+    e = fill_r(g, a, st, fill, nk);
+    if (e != cudaSuccess) return e;
+    k_fct_update<S, R><<<dim3((g.IMAX + 3) / 4, g.JMAX), dim3(32, 4), 0, st>>>(g, a);
+    ++nk;
+    return cudaGetLastError();
+}
+
+template <int S, typename R>
+static cudaError_t tracer_stage(const Grid &g, const TracerArgsT<R> &a, bool fct, cudaStream_t st, const HaloFill *fill,
+                                int &nk)
+{
+    dim3 b(32, 4), gr((g.IMAX + 3) / 4, g.JMAX);
+    if (!fct) {
+        k_tracer_plain<S, R><<<gr, b, 0, st>>>(g, a);
+        ++nk;
+        return cudaGetLastError();
+    }
+    const cudaError_t ef = fct_fused<S, R>(g, a, st, fill, nk);
+    if (ef != cudaErrorNotSupported) return ef;
+    dim3 gl((g.IMAX + 2 + 3) / 4, g.JMAX + 2);
+    k_fct_lo<S, R><<<gl, b, 0, st>>>(g, a);
+    k_fct_r<R><<<gr, b, 0, st>>>(g, a);
+    nk += 2;
+    cudaError_t e = fill_r(g, a, st, fill, nk);
+    if (e != cudaSuccess) return e;
     k_fct_apply<S, R><<<gr, b, 0, st>>>(g, a);
+    ++nk;
     return cudaGetLastError();
 }
 
 template <typename R>
 cudaError_t launch_tracer_stage(const Grid &g, const TracerArgsT<R> &a, int scheme, bool fct, cudaStream_t st,
-                                const HaloFill *fill)
+                                const HaloFill *fill, int *nk)
 {
+    int n = 0;
+    cudaError_t e;
     switch (scheme) {
-    case UD3: return tracer_stage<UD3, R>(g, a, fct, st, fill);
-    case CD4: return tracer_stage<CD4, R>(g, a, fct, st, fill);
-    case KOREN: return tracer_stage<KOREN, R>(g, a, fct, st, fill);
-    case CD2: return tracer_stage<CD2, R>(g, a, fct, st, fill);
-    case UD5: return tracer_stage<UD5, R>(g, a, fct, st, fill);
-    case CD6: return tracer_stage<CD6, R>(g, a, fct, st, fill);
-    default: return cudaErrorInvalidValue;
+    case UD3: e = tracer_stage<UD3, R>(g, a, fct, st, fill, n); break;
+    case CD4: e = tracer_stage<CD4, R>(g, a, fct, st, fill, n); break;
+    case KOREN: e = tracer_stage<KOREN, R>(g, a, fct, st, fill, n); break;
+    case CD2: e = tracer_stage<CD2, R>(g, a, fct, st, fill, n); break;
+    case UD5: e = tracer_stage<UD5, R>(g, a, fct, st, fill, n); break;
+    case CD6: e = tracer_stage<CD6, R>(g, a, fct, st, fill, n); break;
+    default: e = cudaErrorInvalidValue;
     }
+    if (nk) *nk = n;
+    return e;
 }
 #ifdef HEVI_FLOAT_TU
 template cudaError_t launch_tracer_stage<float>(const Grid &, const TracerArgsT<float> &, int, bool, cudaStream_t,
-                                                const HaloFill *);
+                                                const HaloFill *, int *);
 #else
 template cudaError_t launch_tracer_stage<double>(const Grid &, const TracerArgsT<double> &, int, bool, cudaStream_t,
-                                                 const HaloFill *);
+                                                 const HaloFill *, int *);
 #endif
 
 }  // namespace hevi

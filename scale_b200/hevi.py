@@ -100,7 +100,7 @@ def load(path: str | os.PathLike | None = None) -> C.CDLL:
             f.argtypes = [C.c_char_p]
         elif name == "scale_hevi_set_halo_exchange":
             f.argtypes = [HALO_FN, C.c_void_p]
-        elif name in ("scale_hevi_stage_autotune", "scale_hevi_numfilter_form"):
+        elif name in ("scale_hevi_stage_autotune", "scale_hevi_numfilter_form", "scale_hevi_tracer_fct_form"):
             f.argtypes = [C.c_int]
         elif name == "scale_hevi_stage_shape_get":
             f.argtypes = [C.POINTER(C.c_int), C.POINTER(C.c_int), C.c_int]
@@ -418,6 +418,12 @@ def persistent_wait(seconds: float, extra_arrivals: int = 0) -> None:
 def numfilter_form(tiled: bool) -> None:
     """The filter's tiled form (True, the default) or the column kernel for one domain."""
     _check(load().scale_hevi_numfilter_form(int(bool(tiled))))
+
+
+def tracer_fct_form(fused: bool) -> None:
+    """The FCT-limited tracer stage's fused form (True, the default) or the
+    three-kernel form."""
+    _check(load().scale_hevi_tracer_fct_form(int(bool(fused))))
 
 
 def persistent_grid() -> int:

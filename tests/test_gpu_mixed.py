@@ -126,19 +126,26 @@ def test_mixed_tracer_rk3_matches_fp64(fct, along):
     dev = lambda x, t=torch.float64: torch.from_numpy(np.ravel(x, order="K").copy()).to("cuda", t)  # noqa: E731
     out = {}
     hevi.setup(g.index_dict(), "UD3", "UD3")
+
+    def run(mixed):
+        ft = torch.float32 if mixed else torch.float64
+        q = dev(q0)
+        kw = dict(QTRC=q, QTRC0=q, RHOQ_t=dev(rhoq, ft), DENS0=dev(d0), DENS=dev(d), mflx_hi=dev(mflx, ft),
+                  num_diff=dev(ndq, ft), GSQRT=dev(GS), MAPF=dev(MAPF), CDZ=g.CDZ, RCDZ=g.RCDZ, RCDX=g.RCDX,
+                  RCDY=g.RCDY, BND_W=False, BND_E=False, BND_S=False, BND_N=False, dtl=5.0,
+                  FLAG_FCT_TRACER=fct, FLAG_FCT_ALONG_STREAM=along)
+        for _ in range(3):
+            (hevi.ATMOS_DYN_Tinteg_tracer_rk3_mixed_dev if mixed else hevi.ATMOS_DYN_Tinteg_tracer_rk3_dev)(**kw)
+            hevi.COMM_vars8_dev(q, 1)
+        hevi.check()
+        return q.cpu().numpy().reshape(g.shape, order="F")
+
     try:
         for mixed in (False, True):
-            ft = torch.float32 if mixed else torch.float64
-            q = dev(q0)
-            kw = dict(QTRC=q, QTRC0=q, RHOQ_t=dev(rhoq, ft), DENS0=dev(d0), DENS=dev(d), mflx_hi=dev(mflx, ft),
-                      num_diff=dev(ndq, ft), GSQRT=dev(GS), MAPF=dev(MAPF), CDZ=g.CDZ, RCDZ=g.RCDZ, RCDX=g.RCDX,
-                      RCDY=g.RCDY, BND_W=False, BND_E=False, BND_S=False, BND_N=False, dtl=5.0,
-                      FLAG_FCT_TRACER=fct, FLAG_FCT_ALONG_STREAM=along)
-            for _ in range(3):
-                (hevi.ATMOS_DYN_Tinteg_tracer_rk3_mixed_dev if mixed else hevi.ATMOS_DYN_Tinteg_tracer_rk3_dev)(**kw)
-                hevi.COMM_vars8_dev(q, 1)
-            hevi.check()
-            out[mixed] = q.cpu().numpy().reshape(g.shape, order="F")
+            out[mixed] = run(mixed)
+        # the three-kernel limiter in FP32 (FMA contractions may differ from the fused form's)
+        hevi.tracer_fct_form(False)
+        out["three_kernel"] = run(True)
     finally:
         hevi.finalize()
     sl = (slice(g.KS - 1, g.KE), slice(g.IS - 1, g.IE), slice(g.JS - 1, g.JE))
@@ -146,6 +153,8 @@ def test_mixed_tracer_rk3_matches_fp64(fct, along):
     assert np.isfinite(a32).all()
     err = np.max(np.abs(a32 - a64)) / np.max(np.abs(a64))
     assert err <= 1e-5, f"max relative error {err:.3e}"
+    err3 = np.max(np.abs(out["three_kernel"][sl] - a32)) / np.max(np.abs(a64))
+    assert err3 <= 1e-6, f"fused against three-kernel FP32 limiter: {err3:.3e}"
     if fct:
         # no new minimum beyond FP32 rounding of the FP64 run's own
         assert a32.min() >= a64.min() - 1e-6 * np.max(np.abs(a64))

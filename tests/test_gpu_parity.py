@@ -185,6 +185,36 @@ def test_tracer_step_bit_exact(lib, scheme, fct, along):
     assert helpers.same(got, ref), f"max rel diff {helpers.max_rel(got, ref):.3e}"
 
 
+@pytest.mark.parametrize("scheme", ["UD3", "CD6"])
+@pytest.mark.parametrize("along", [True, False])
+@pytest.mark.parametrize("kmax", [40, 17])
+def test_tracer_fct_forms_bit_exact(lib, scheme, along, kmax):
+    """The fused limiter (strips of 16 rows, tiles of 8 columns x 32 levels)
+    and the three-kernel form on a domain that fills neither: 13 x 37 columns,
+    40 levels (a second chunk of 8) or 17 (odd KA: no tensor map, so both
+    settings run the three-kernel form)."""
+    g = helpers.small_grid(IMAX=13, JMAX=37, KMAX=kmax, halo=helpers.halo_of(scheme), stretched=True)
+    c = helpers.small_case(g)
+    helpers.perturb_state(c)
+    q0, q, d0, d, mflx, rhoq, GS, MAPF = _tracer_inputs(g, c)
+    ref = np.full(g.shape, np.nan, order="F")
+    oracle.tstep_tracer(g, scheme, ref, q, q0, rhoq, d0, d, mflx, g.zeros(3), GS, MAPF, 2.5, True, along)
+    res = []
+    for fused in (True, False):
+        got = np.full(g.shape, np.nan, order="F")
+        lib.setup(g.index_dict(), scheme, scheme)
+        lib.tracer_fct_form(fused)
+        lib.ATMOS_DYN_Tstep_tracer_fvm_heve(QTRCo=got, QTRC=q, QTRC0=q0, RHOQ_t=rhoq, DENS0=d0, DENS=d,
+                                            mflx_hi=mflx, num_diff=g.zeros(3), GSQRT=GS, MAPF=MAPF, CDZ=g.CDZ,
+                                            RCDZ=g.RCDZ, RCDX=g.RCDX, RCDY=g.RCDY, dtl=2.5, FLAG_FCT_TRACER=True,
+                                            FLAG_FCT_ALONG_STREAM=along)
+        lib.check()
+        lib.finalize()
+        res.append(got)
+        assert helpers.same(got, ref), f"fused={fused}: max rel diff {helpers.max_rel(got, ref):.3e}"
+    assert np.array_equal(res[0], res[1], equal_nan=True)
+
+
 @pytest.mark.parametrize("tscheme", ["UD3", "UD3KOREN1993"])
 @pytest.mark.parametrize("fct", [False, True])
 def test_tracer_rk3_bit_exact(lib, fct, tscheme):
