@@ -372,8 +372,7 @@ constexpr int JB = HEVI_FCT_JB;  // rows of a CTA's strip
 constexpr unsigned ROW_BYTES = BK * BW * sizeof(double);
 template <typename R> constexpr size_t smem_bytes()
 {
-    return (size_t)NS * SLOT * sizeof(double) + NS * sizeof(uint64_t) + (size_t)NP * PW * PK * sizeof(R)
-           + (size_t)(FW + 1) * KC * sizeof(R);
+    return (size_t)NS * SLOT * sizeof(double) + NS * sizeof(uint64_t) + (size_t)NP * PW * PK * sizeof(R);
 }
 }  // namespace fct
 
@@ -407,10 +406,13 @@ __device__ __forceinline__ R qb_sum(const R (&f)[2][3][3], int kb, const V &v)
 // scratch for k_fct_update (phi_lo itself stays in shared memory).
 // Block (32, FW): lane = level L0+lane, warp w = column i0+w; the CTA marches
 // over rows jb0 .. jb0+nrow-1. Iteration t forms phi_lo of row r = jb0-1+t and,
-// from t = 2, R+/R- of row o = r-1. QTRC0 row jb0-2+rr sits in ring slot
-// rr % NS (mbarrier rr % NS, phase rr / NS); rows rr = 0..3 are copied before
-// the march and row t+4 after the first barrier of iteration t, so a slot is
-// refilled only after the iteration that last read it has ended everywhere.
+// from t = 2, R+/R- of row o = r-1, with one CTA barrier per iteration (after
+// phi_lo; each warp forms both x faces of its column). QTRC0 row jb0-2+rr
+// sits in ring slot rr % NS (mbarrier rr % NS, phase rr / NS); rows rr = 0..3
+// are copied before the march, row t+3 is waited for before the barrier of
+// iteration t and row t+4 is copied after it, so a slot is refilled only after
+// the iteration that last read it has ended everywhere, and a phi_lo slot is
+// rewritten only after the barrier that follows its last reads.
 template <int S, typename R>
 __global__ void __launch_bounds__(32 * fct::FW, HEVI_FCT_MINB)
     k_fct_limit(const Grid g, const TracerArgsT<R> a, const __grid_constant__ CUtensorMap map)
@@ -421,8 +423,9 @@ __global__ void __launch_bounds__(32 * fct::FW, HEVI_FCT_MINB)
     double *spi = fsm;                                               // QTRC0 rows [slot][i][k]
     uint64_t *bar = reinterpret_cast<uint64_t *>(spi + NS * SLOT);   // one mbarrier per slot
     R *spl = reinterpret_cast<R *>(bar + NS);                        // phi_lo rows [slot][i][k]
-    R *sax = spl + NP * PW * PK;                                     // x anti-diffusive flux [face][lane]
-    __shared__ int s_ok;
+    // staging status, double-buffered: with one barrier per iteration, thread 0
+    // writes iteration t+1's word while others may still read iteration t's
+    __shared__ int s_ok[2];
     const int lane = threadIdx.x, w = threadIdx.y, tid = w * 32 + lane;
     const int nti = (g.IMAX + FW - 1) / FW;
     const int i0 = g.IS + ((int)blockIdx.x % nti) * FW, L0 = g.KS + ((int)blockIdx.x / nti) * KC;
@@ -454,10 +457,10 @@ __global__ void __launch_bounds__(32 * fct::FW, HEVI_FCT_MINB)
         const bool ok = wait_row(0) && wait_row(1) && wait_row(2);
         if (!ok)
             for (int rr = 0; rr < 4; ++rr) (void)wait_row(rr); // bounded: the copies still in flight
-        s_ok = ok ? 1 : 0;
+        s_ok[1] = ok ? 1 : 0;
     }
     __syncthreads();
-    if (!s_ok) {
+    if (!s_ok[1]) {
         if (tid == 0) atomicOr(a.status, ST_TMA_TIMEOUT);
         return; // block-uniform
     }
@@ -494,7 +497,19 @@ __global__ void __launch_bounds__(32 * fct::FW, HEVI_FCT_MINB)
                           / ld(a.DENS + c));
             }
         }
+        if (tid == 0 && t + 3 <= rlast) {
+            const bool ok = wait_row(t + 3);
+            if (!ok) (void)wait_row(t + 3); // bounded: the copy still in flight
+            s_ok[t & 1] = ok ? 1 : 0;
+        } else if (tid == 0) {
+            s_ok[t & 1] = 1;
+        }
         __syncthreads(); // phi_lo of row r in place; every read of iteration t-1 done
+        if (!s_ok[t & 1]) {
+            if (tid == 0) atomicOr(a.status, ST_TMA_TIMEOUT);
+            return; // block-uniform
+        }
+        if (t + 3 <= rlast) (void)mbar_try(bar + (t + 3) % NS, (unsigned)((t + 3) / NS) & 1u);
         if (tid == 0 && t + 4 <= rlast) {
             fence_proxy_async();
             issue(t + 4);
@@ -504,7 +519,7 @@ __global__ void __launch_bounds__(32 * fct::FW, HEVI_FCT_MINB)
         const bool out = t >= 2; // block-uniform
         const size_t c = idx3(g, min(k, KE), min(i, g.IE), o);
         const size_t col = c - (size_t)(min(k, KE) - 1);
-        R az = zero, azm = zero, ax = zero, ay = zero, aym = zero;
+        R az = zero, azm = zero, ax = zero, ay = zero, aym = zero, axm = zero;
         if (out) {
             if (cell && k <= KE - 1)
                 az = hflux_z<S>(g, a, N3, col, k) - lflux_v(ld(mZ + c), R(PI(o, k, i)), R(PI(o, k + 1, i)));
@@ -521,31 +536,16 @@ __global__ void __launch_bounds__(32 * fct::FW, HEVI_FCT_MINB)
                 if (o == g.JS) a.phi_lo[c - sJ] = R(PI(o - 1, k, i));
                 if (o == g.JE) a.phi_lo[c + sJ] = R(PI(o + 1, k, i));
                 ax = hflux_h<S>(a, N3, 1, c, sI) - lflux_v(ld(mX + c), R(PI(o, k, i)), R(PI(o, k, i + 1)));
-                sax[(w + 1) * KC + lane] = ax;
-                if (w == 0)
-                    sax[lane] = hflux_h<S>(a, N3, 1, c - sI, sI) - lflux_v(ld(mX + c - sI), R(PI(o, k, i - 1)), R(PI(o, k, i)));
+                axm = hflux_h<S>(a, N3, 1, c - sI, sI) - lflux_v(ld(mX + c - sI), R(PI(o, k, i - 1)), R(PI(o, k, i)));
                 ay = hflux_h<S>(a, N3, 2, c, sJ) - lflux_v(ld(mY + c), R(PI(o, k, i)), R(PI(o + 1, k, i)));
                 aym = t == 2 ? hflux_h<S>(a, N3, 2, c - sJ, sJ) - lflux_v(ld(mY + c - sJ), R(PI(o - 1, k, i)), R(PI(o, k, i)))
                              : ay_prev;
                 ay_prev = ay;
             }
         }
-        if (tid == 0 && t + 3 <= rlast) {
-            const bool ok = wait_row(t + 3);
-            if (!ok)
-                for (int rr = t + 3; rr <= min(t + 4, rlast); ++rr) (void)wait_row(rr); // bounded
-            s_ok = ok ? 1 : 0;
-        }
-        __syncthreads(); // x fluxes in place; QTRC0 row t+3 arrived (or timed out)
-        if (!s_ok) {
-            if (tid == 0) atomicOr(a.status, ST_TMA_TIMEOUT);
-            return; // block-uniform
-        }
-        if (t + 3 <= rlast) (void)mbar_try(bar + (t + 3) % NS, (unsigned)((t + 3) / NS) & 1u);
         if (!out || !cell) continue;
 
         // (c) P+/P-, the bounds Q+/Q- and R+/R- of cell (k, i, o) (common.F90:2077-2553)
-        const R axm = sax[w * KC + lane];
         const R pz = rmax(zero, azm) - rmin(zero, az);
         const R px = rmax(zero, axm) - rmin(zero, ax);
         const R py = rmax(zero, aym) - rmin(zero, ay);
