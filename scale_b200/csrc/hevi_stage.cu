@@ -300,8 +300,15 @@ template cudaError_t launch_hevi_stage<double>(const Grid &, const Members &, co
 // put_state/put_flux, so the RK4/RK3 folds of the fused kernel apply unchanged.
 // FP64, one domain.
 // =============================================================================
+// at least 10 CTAs per SM (51 registers): the loop nests are bound by load
+// latency, and unbounded they took 29-90 registers (5 CTAs per SM for the
+// largest); 512x512x128 CD4 terrain short step 81.1 -> 75.4 ms (8 CTAs 77.4,
+// 12 CTAs 78.9)
+#ifndef HEVI_GCOLS_MINB
+#define HEVI_GCOLS_MINB 10
+#endif
 template <class F>
-__global__ void __launch_bounds__(128) k_gcols(int i0, int ni, int j0, int ncol, F f)
+__global__ void __launch_bounds__(128, HEVI_GCOLS_MINB) k_gcols(int i0, int ni, int j0, int ncol, F f)
 {
     const int col = blockIdx.x * 4 + threadIdx.y;
     if (col >= ncol) return;

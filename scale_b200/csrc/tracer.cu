@@ -108,8 +108,21 @@ __device__ __forceinline__ R lflux(const TracerArgsT<R> &a, size_t N3, int dir, 
 }
 
 // ---- stage without FCT, tstep_tracer_fvm_heve.F90:214-236 -------------------
+// CTAs per SM of the two warp-per-column tracer kernels, which are bound by
+// load latency: 16 (32 registers) for k_tracer_plain and 12 (40 registers)
+// for k_fct_update, against 48 and 64 registers unbounded (512x512x128, UD3:
+// 6.69 -> 5.92 ms per FP64 tracer step, 5.19 -> 4.68 ms mixed; 16 CTAs for
+// k_fct_update spill 400 B and took 7.80 ms)
+#ifndef HEVI_TR_MINB
+#define HEVI_TR_MINB 16
+#endif
+#ifndef HEVI_UPD_MINB
+#define HEVI_UPD_MINB 12
+#endif
+#define HEVI_TR_BOUNDS __launch_bounds__(128, HEVI_TR_MINB)
+#define HEVI_UPD_BOUNDS __launch_bounds__(128, HEVI_UPD_MINB)
 template <int S, typename R>
-__global__ void __launch_bounds__(128) k_tracer_plain(const Grid g, const TracerArgsT<R> a)
+__global__ void HEVI_TR_BOUNDS k_tracer_plain(const Grid g, const TracerArgsT<R> a)
 {
     const int i = g.IS + blockIdx.x * blockDim.y + threadIdx.y;
     const int j = g.JS + blockIdx.y;
@@ -604,7 +617,7 @@ __global__ void __launch_bounds__(32 * fct::FW, HEVI_FCT_MINB)
 // value there may already be the new one. Each cell's own QTRC0 is read
 // before its own write.
 template <int S, typename R>
-__global__ void __launch_bounds__(128) k_fct_update(const Grid g, const TracerArgsT<R> a)
+__global__ void HEVI_UPD_BOUNDS k_fct_update(const Grid g, const TracerArgsT<R> a)
 {
     const int i = g.IS + blockIdx.x * blockDim.y + threadIdx.y;
     const int j = g.JS + blockIdx.y;
