@@ -7,16 +7,17 @@
 // updates). With FCT the limiter needs the low-order solution and the
 // limiting factors of the neighbours, so the stage splits at the halo fill of
 // R+/R- (the reference's mid-limiter COMM_vars8, :2558-2561). Its fused form:
-//   k_fct_limit   a CTA owns 8 columns x 32 levels and marches along j over a
-//                 strip of rows; QTRC0 rows come into a ring in shared memory
-//                 by bulk tensor copies (TMA, two rows ahead, bounded mbarrier
-//                 waits). Per row it forms the low-order solution phi_lo of the
-//                 tile and a halo of one in shared memory, the high- and
-//                 low-order fluxes of every face of the tile and their
-//                 differences (the anti-diffusive fluxes, z by warp shuffle, y
-//                 carried from the row before), and from them P+/P-, the
-//                 along-stream or 7-point bounds Q+/Q- and R+/R-. Only R+/R-
-//                 leave the kernel.
+//   k_fct_limit   a CTA owns 8 columns (4 in FP32) x 32 levels and marches
+//                 along j over a strip of rows; QTRC0 rows come into a ring in
+//                 shared memory by bulk tensor copies (TMA, two rows ahead,
+//                 bounded mbarrier waits). Per row it forms the low-order
+//                 solution phi_lo of the tile and a halo of one in shared
+//                 memory, the high- and low-order fluxes of every face of the
+//                 tile and their differences (the anti-diffusive fluxes: z by
+//                 warp shuffle, both x faces by each column's warp, y carried
+//                 from the row before), and from them P+/P-, the along-stream
+//                 or 7-point bounds Q+/Q- and R+/R-. Only R+/R- and a copy of
+//                 R(QTRC0) for k_fct_update leave the kernel.
 //   k_fct_update  forms each face's high- and low-order fluxes again, limits
 //                 their difference with R+/R- and updates the tracer.
 // The three-kernel form (k_fct_lo: phi_lo and the anti-diffusive fluxes to
